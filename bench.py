@@ -1,0 +1,339 @@
+"""Benchmark of the DS2D hot path on B200: elastic RTM with random boundaries.
+
+Workload (one step): elastic RTM of a batch of 60 shots evenly spread along the surface of a
+1201 x 401 model (dx = dz = 10 m, 40-cell random band -> 1281 x 481 padded cells, nt = 4000,
+dt = 0.8 ms, 15 Hz Ricker), receivers on every column two cells below the surface: background
+forward pass, interior reconstruction, adjoint pass and zero-lag imaging (3 propagations per
+shot).  The true model is synthetic (8 dipping layers 2000-6000 m/s + 3 Gaussian lenses, seeded),
+the migration model is it smoothed with sigma = 15 cells; observed data come from PML forward
+modelling on the true model (untimed set-up).
+
+Metric: Gcell-updates/s = shots * 1281 * 481 * 4000 * 3 / time, whole job (all ranks).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank runs its own 60-shot batch (weak scaling) and the three images
+are summed over ranks with one NCCL all-reduce per step (SURVEY-style gradient reduction).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CFG = dict(allnx=1201, allnz=401, pml=40, nt=4000, dx=10.0, dz=10.0, dt=0.0008, f0=15.0,
+           shots=60, sz=0, gz=2, seed=2024)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--shots", type=int, default=CFG["shots"])
+    p.add_argument("--nt", type=int, default=CFG["nt"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-profile", action="store_true")
+    p.add_argument("--ref-shots", type=int, default=2, help="shots per reference-arm step")
+    return p.parse_args()
+
+
+class Clocks:
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.stop = threading.Event()
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=6)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def workload(args, rank):
+    from ds2d_b200 import synth
+    c = dict(CFG)
+    c["nt"] = args.nt
+    c["shots"] = args.shots
+    vp, vs = synth.dipping_lenses(c["allnx"], c["allnz"], seed=c["seed"] + rank)
+    vpm, vsm = synth.smooth(vp, 15.0), synth.smooth(vs, 15.0)
+    w = synth.ricker(c["nt"], c["f0"], c["dt"])
+    shots = synth.surface_shots(c["allnx"], c["allnx"], c["pml"], c["shots"], sz=c["sz"], gz=c["gz"])
+    return c, vp, vs, vpm, vsm, w, shots
+
+
+def cells(c):
+    return (c["allnx"] + 2 * c["pml"]) * (c["allnz"] + 2 * c["pml"])
+
+
+def cpu_baseline(c, vpm, vsm, w, shot, obs_z, obs_x):
+    """Oracle FP32 RTM of one shot on a bounded number of steps, all host cores."""
+    from oracle import pyoracle as po
+    nt = 120
+    st = po.Setup(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    m = po.build_model(st, vpm, vsm, None, shot.win_left, rbc=1, seed=c["seed"], shot_id=0)
+    t0 = time.perf_counter()
+    po.rtm(st, m, w[:nt], shot, obs_z[:, :nt], obs_x[:, :nt], 1, "f32")
+    dt = time.perf_counter() - t0
+    upd = 3.0 * cells(c) * nt
+    return {"value": upd / dt / 1e9, "unit": "Gcell-updates/s", "cores": os.cpu_count(),
+            "kind": "port",
+            "sample": f"1 shot x {nt} steps of the 1281x481 RTM (3 propagations), oracle FP32, "
+                      f"OpenMP on {os.cpu_count()} threads, {dt:.1f} s"}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_for(kernel):
+    """DRAM bytes per launch of `kernel` from a committed ncu capture summary, else None."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except Exception:
+        return None
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from ds2d_b200 import Elastic2D
+    c, vp, vs, vpm, vsm, w, shots = workload(args, rank)
+    dev = torch.cuda.current_device()
+    ntr = shots[0].ntr
+    # Observed data: PML forward modelling on the true model (set-up, untimed).
+    with Elastic2D(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                   boundary="pml", max_shots=min(20, c["shots"]), max_ntr=ntr, device=dev) as fm:
+        fm.set_models(vp, vs)
+        fm.set_wavelet(w)
+        obs_z, obs_x = fm.forward(shots)
+    e = Elastic2D(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                  boundary="random", max_shots=c["shots"], max_ntr=ntr, seed=c["seed"], device=dev)
+    e.set_models(vpm, vsm)
+    e.set_wavelet(w)
+    stream = torch.cuda.current_stream()
+    e.set_stream(stream.cuda_stream)
+    d_z = torch.from_numpy(obs_z).to(dev)
+    d_x = torch.from_numpy(obs_x).to(dev)
+    h_z = torch.from_numpy(obs_z).pin_memory()
+    h_x = torch.from_numpy(obs_x).pin_memory()
+    h2d = int(h_z.numel() + h_x.numel()) * 4
+    img_bytes = 3 * c["allnx"] * c["allnz"] * 4
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allreduce_images():
+        if dist is not None:
+            imgs = e.read_images(reset=True, which=("pp_grad", "ps_grad", "illumination"))
+            t = torch.from_numpy(np.stack(list(imgs.values()))).to(dev)
+            dist.all_reduce(t)
+            return t
+        return None
+
+    # warm-up
+    for _ in range(args.warmup):
+        e.rtm_device(shots, d_z.data_ptr(), d_x.data_ptr())
+    allreduce_images()
+    e.read_images(reset=True)
+    launches = e.last_launches
+    upd = e.last_cell_updates
+    # timed device-resident steps
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            e.rtm_device(shots, d_z.data_ptr(), d_x.data_ptr())
+            allreduce_images()
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_upd = upd * world * args.steps
+    value = total_upd / (ms / 1e3) / 1e9
+    # end-to-end: host (pinned) data in, images out, through the public API
+    e.read_images(reset=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e.rtm(shots, h_z.numpy(), h_x.numpy())
+        if dist is not None:
+            allreduce_images()
+        e.read_images(reset=True, which=("pp_grad", "ps_grad", "illumination"))
+    e1.record(stream)
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = total_upd / (ms_e2e / 1e3) / 1e9
+    # per-kernel roofline from a profiled step (rank 0 only; profiling adds event overhead)
+    roof = None
+    if rank == 0 and not args.no_profile:
+        e.profile(True)
+        e.rtm_device(shots, d_z.data_ptr(), d_x.data_ptr())
+        rep = e.profile_report()
+        e.profile(False)
+        tot = sum(v[1] for v in rep.values())
+        name, (n, kms, by) = max(rep.items(), key=lambda kv: kv[1][1])
+        peak, src = measured_peak()
+        achieved = by / n / (kms / n / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": src,
+                "traffic": traffic_for(name), "share": round(kms / tot, 4),
+                "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
+                                "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else None}
+                            for k, v in rep.items()}}
+    out = None
+    if rank == 0:
+        out = {"metric": "Gcell-updates/s (elastic RTM, random boundary)", "value": round(value, 3),
+               "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded dipping-layer + lens model, PML-modelled observed data)",
+               "config": {"workload": "elastic RTM, random boundary, 60 shots per GPU",
+                          "model": f"{c['allnx']}x{c['allnz']} (+{c['pml']} band) "
+                                   f"-> {cells(c)} padded cells",
+                          "nt": c["nt"], "shots_per_gpu": c["shots"], "propagations_per_shot": 3,
+                          "cell_updates_per_step": upd * world, "parallelism": f"shots x{world}",
+                          "l2": "inputs larger than L2 (wavefields of 60 shots ~3 GB)"},
+               "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s",
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": img_bytes},
+               "gpu_launches": int(launches * args.steps),
+               "clocks": clk.summary(), "roofline": roof}
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline(c, vpm, vsm, w, shots[0], obs_z[:ntr], obs_x[:ntr])
+    e.close()
+    return out
+
+
+def run_reference(args, rank, world):
+    """The reference's own CUDA build (oracle/_ref) on a bounded sample of the same workload."""
+    from oracle import pyoracle as po
+    if rank != 0:
+        return None
+    if not po.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libds2dref.so was not built"}
+    import torch  # noqa: F401
+    c, vp, vs, vpm, vsm, w, shots = workload(args, 0)
+    sample = shots[:: max(1, len(shots) // args.ref_shots)][:args.ref_shots]
+    st = po.Setup(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    # observed data with the reference's own PML forward modelling
+    obs = [po.ref_forward(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["nt"], c["dx"], c["dz"],
+                          c["dt"], vp, vs, w, s) for s in sample]
+    az = np.stack([o[0] for o in obs])
+    ax = np.stack([o[1] for o in obs])
+    pads = [po.build_model(st, vpm, vsm, None, s.win_left, rbc=1, seed=c["seed"], shot_id=i)
+            for i, s in enumerate(sample)]
+    vpp, vsp = np.stack([p[0] for p in pads]), np.stack([p[1] for p in pads])
+    g = (c["allnx"], c["allnz"], c["allnx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"])
+    for _ in range(args.warmup):
+        po.ref_rtm(*g, vpm, vsm, w, sample, az, ax, rbc=1, vp_pad=vpp, vs_pad=vsp)
+    tot = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, ms = po.ref_rtm(*g, vpm, vsm, w, sample, az, ax, rbc=1, vp_pad=vpp, vs_pad=vsp)
+        tot += ms
+    wall = time.perf_counter() - t0
+    upd = 3.0 * cells(c) * c["nt"] * len(sample) * args.steps
+    v = upd / (tot / 1e3) / 1e9
+    ve = upd / wall / 1e9
+    return {"impl": "reference", "metric": "Gcell-updates/s (elastic RTM, random boundary)",
+            "value": round(v, 3), "unit": "Gcell-updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(tot / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": "elastic RTM, random boundary",
+                                            "shots_per_step": len(sample), "nt": c["nt"]},
+            "cpu_baseline": {"value": round(v, 3), "unit": "Gcell-updates/s", "cores": 1,
+                             "kind": "reference",
+                             "sample": f"{len(sample)} of the 60 shots per step, full nt, run by "
+                                       "the reference's own CUDA kernels (FD2DGPU.cu / born.cu "
+                                       "built for sm_100a) on the same B200, driven in the "
+                                       "reference driver's order; random band injected"},
+            "e2e": {"value": round(ve, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = td
+    out = run_ours(args, rank, world, dist)
+    if out is not None:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

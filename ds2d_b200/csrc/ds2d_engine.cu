@@ -1,0 +1,924 @@
+// Host engine and C ABI (include/ds2d.h) of the B200 DS2D time-stepping path.
+//
+// The engine owns all device memory of a run: the full models and images, and a batch of
+// "slots" (one per resident shot) with the shot's padded parameters, wavefields, strips and
+// window images.  One call (ds2d_forward / ds2d_elsrtm / ds2d_rtm) processes its shots in
+// batches of opts.max_shots; every kernel launch covers all shots of the batch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ds2d.h"
+#include "ds2d_step.cuh"
+
+using namespace ds2d;
+
+namespace {
+
+// Setup of one batch of slots: window of the full model with edge replication
+// (FD2DGPU.cu:122-138, :234-250), optional project random band, PML damping (:444-494, profile
+// ((pml-i)/pml)^4 scaled by log10(1/rr) * 5 vp / (2 pml)), moduli with the reference's rho
+// (:1117-1125), imaging weights -2 vp^2 rho and -2 vs^2 rho (:3257-3258), image windows
+// (:1324-1333).
+struct SetupArgs {
+  Dims d;
+  const float *vp_all, *vs_all, *rho_all, *pp_all, *ps_all;
+  const ShotDev *shots;
+  float *b, *lam, *mu, *dampx, *dampz, *kpp, *kps, *dmp, *dms;
+  double L;  // log10(1/rr)
+  unsigned long long seed;
+  int shot_base;
+};
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+  // SplitMix64 finalizer (Steele, Lea, Flood 2014).
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ float band_factor(unsigned long long seed, int shot, int ix, int iz) {
+  unsigned long long h =
+      splitmix64(seed ^ (0xD1B54A32D192ED03ull * (unsigned long long)(unsigned)(shot + 1)));
+  h = splitmix64(h ^ (((unsigned long long)(unsigned)ix << 32) | (unsigned)iz));
+  const float u = (float)(h >> 40) * (1.0f / 16777216.0f);
+  return fmaf(0.4f, u, 0.6f);
+}
+
+__global__ void k_setup(SetupArgs a) {
+  const Dims &d = a.d;
+  const int s = blockIdx.z;
+  const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ix = blockIdx.y;
+  if (iz >= d.ld) return;
+  const long long k = d.slot * s + (long long)ix * d.ld + iz;
+  if (iz >= d.nzp) {
+    a.b[k] = 0.f; a.lam[k] = 0.f; a.mu[k] = 0.f;
+    if (a.dampx) { a.dampx[k] = 0.f; a.dampz[k] = 0.f; }
+    a.kpp[k] = 0.f; a.kps[k] = 0.f;
+    if (a.dmp) { a.dmp[k] = 0.f; a.dms[k] = 0.f; }
+    return;
+  }
+  const int pml = d.pml;
+  const int jx = min(max(ix - pml, 0), d.wnx - 1), jz = min(max(iz - pml, 0), d.wnz - 1);
+  const long long src = (long long)(a.shots[s].win_left + jx) * d.allnz + jz;
+  float p = a.vp_all[src], sv = a.vs_all[src];
+  const bool band = ix < pml || ix >= d.nxp - pml || iz < pml || iz >= d.nzp - pml;
+  if (d.rbc && band) {
+    const float f = band_factor(a.seed, a.shot_base + s, ix, iz);
+    p = __fmul_rn(p, f);
+    sv = __fmul_rn(sv, f);
+  }
+  const float r = a.rho_all ? a.rho_all[src] : 2000.0f;
+  const float vp2 = __fmul_rn(p, p), vs2 = __fmul_rn(sv, sv);
+  const float lam = __fmul_rn(r, __fsub_rn(vp2, __fmul_rn(2.0f, vs2)));
+  const float mu = __fmul_rn(r, vs2);
+  a.b[k] = (float)(1.0 / (double)r);
+  a.lam[k] = lam;
+  a.mu[k] = mu;
+  a.kpp[k] = __fmul_rn(__fmul_rn(__fmul_rn(-2.0f, p), p), r);
+  a.kps[k] = __fmul_rn(__fmul_rn(__fmul_rn(-2.0f, sv), sv), r);
+  if (a.dampx) {
+    double dx = 0, dz = 0;
+    if (!d.rbc) {
+      const double c = __dmul_rn(a.L, __ddiv_rn(__dmul_rn(5.0, (double)p), 2.0 * pml));
+      auto prof = [&](int n) {
+        const double t = (double)n / pml;
+        const double t2 = __dmul_rn(t, t);
+        return __dmul_rn(c, __dmul_rn(t2, t2));
+      };
+      if (ix < pml) dx = prof(pml - ix);
+      if (ix > d.nxp - pml) dx = prof(ix - (d.nxp - pml));
+      if (iz < pml) dz = prof(pml - iz);
+      if (iz > d.nzp - pml) dz = prof(iz - (d.nzp - pml));
+    }
+    a.dampx[k] = (float)dx;
+    a.dampz[k] = (float)dz;
+  }
+  if (a.dmp) {
+    a.dmp[k] = a.pp_all[src];
+    a.dms[k] = a.ps_all[src];
+  }
+}
+
+struct Arena {
+  std::vector<void *> ptrs;
+  ~Arena() { release(); }
+  void release() {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+// Per-launch device timing (profiling mode): one event pair per launch, folded per kernel name.
+struct ProfRec {
+  const char *name;
+  int ev;
+  double bytes;
+};
+
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  std::vector<ProfRec> recs;
+  int used = 0;
+  ~Profiler() {
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+  }
+  int take() {
+    if (used + 2 > (int)pool.size()) {
+      for (int i = 0; i < 256; i++) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        pool.push_back(e);
+      }
+    }
+    used += 2;
+    return used - 2;
+  }
+};
+
+}  // namespace
+
+struct ds2d_ctx {
+  ds2d_grid g{};
+  ds2d_opts o{};
+  Dims d{};
+  int B = 1;
+  cudaStream_t own = nullptr, stream = nullptr;
+  std::string err;
+  double last_updates = 0;
+  long long last_launches = 0;
+
+  // full-size arrays
+  float *vp_all = nullptr, *vs_all = nullptr, *rho_all = nullptr;
+  float *pp_all = nullptr, *ps_all = nullptr, *wavelet = nullptr;
+  float *images = nullptr;  // [7][allnx][allnz]
+  bool models_set = false, wavelet_set = false, image_set = false;
+
+  // per-slot arrays
+  Par par{};
+  float *p_b = nullptr, *p_lam = nullptr, *p_mu = nullptr, *p_dampx = nullptr, *p_dampz = nullptr;
+  float *p_kpp = nullptr, *p_kps = nullptr, *p_dmp = nullptr, *p_dms = nullptr;
+  Wave fw{}, b1{}, b2{}, abk{}, bbk{};
+  Strain e{}, be{};
+  float *ov_s[3] = {nullptr, nullptr, nullptr}, *ov_v[2] = {nullptr, nullptr};
+  Strips st_a{}, st_b{};
+  ShotDev *d_shots = nullptr;
+  int *d_rmap = nullptr;
+  float *rec[8] = {};          // obs/adj z,x | scattered z,x | scattered2 z,x | residual z,x
+  float *img_slot = nullptr;   // [7][B][wnx][wnz]
+  double *d_mis = nullptr;
+  bool have_elsrtm = false, have_rtm = false;
+  Profiler prof;
+  Arena arena;
+};
+
+namespace {
+
+thread_local std::string g_create_err = "";  // reported by ds2d_last_error(NULL)
+
+int fail(ds2d_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                           \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(c, DS2D_E_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),  \
+                  __FILE__, __LINE__);                                                     \
+  } while (0)
+
+int alloc(ds2d_ctx *c, void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(c, DS2D_E_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  c->arena.ptrs.push_back(*p);
+  return DS2D_OK;
+}
+
+int alloc_slots(ds2d_ctx *c, float **p) {
+  return alloc(c, (void **)p, sizeof(float) * (size_t)c->d.slot * c->B);
+}
+
+int alloc_wave(ds2d_ctx *c, Wave &w, bool adjoint) {
+  int rc;
+  float **sums[5] = {&w.vx, &w.vz, &w.txx, &w.tzz, &w.txz};
+  for (float **p : sums)
+    if ((rc = alloc_slots(c, p))) return rc;
+  if (c->d.rbc) return DS2D_OK;
+  // Split memory variables (only PML cells are touched).  The adjoint's txx / tzz are single
+  // variables (FD2DGPU.cu:754-755 txx = txx_x, tzz = tzz_z).
+  float **split_f[10] = {&w.vx_x, &w.vx_z, &w.vz_x, &w.vz_z, &w.txx_x,
+                         &w.txx_z, &w.tzz_x, &w.tzz_z, &w.txz_x, &w.txz_z};
+  float **split_a[6] = {&w.vx_x, &w.vx_z, &w.vz_x, &w.vz_z, &w.txz_x, &w.txz_z};
+  if (adjoint) {
+    for (float **p : split_a)
+      if ((rc = alloc_slots(c, p))) return rc;
+  } else {
+    for (float **p : split_f)
+      if ((rc = alloc_slots(c, p))) return rc;
+  }
+  return DS2D_OK;
+}
+
+int zero_wave(ds2d_ctx *c, const Wave &w, int nslots) {
+  size_t bytes = sizeof(float) * (size_t)c->d.slot * nslots;
+  const float *all[15] = {w.vx, w.vz, w.txx, w.tzz, w.txz, w.vx_x, w.vx_z, w.vz_x,
+                          w.vz_z, w.txx_x, w.txx_z, w.tzz_x, w.tzz_z, w.txz_x, w.txz_z};
+  for (const float *p : all)
+    if (p) CK(cudaMemsetAsync((void *)p, 0, bytes, c->stream));
+  return DS2D_OK;
+}
+
+int alloc_strips(ds2d_ctx *c, Strips &st) {
+  int rc;
+  st.prec = c->o.strip_precision;
+  size_t elems = (size_t)c->B * c->d.nt * 2 * c->d.lb;
+  size_t esz = st.prec == DS2D_STRIPS_F32 ? 4 : 2;
+  if ((rc = alloc(c, &st.data, elems * esz))) return rc;
+  if (st.prec != DS2D_STRIPS_F32) {
+    size_t ns = (size_t)c->B * c->d.nt * 2 * c->d.nseg;
+    if ((rc = alloc(c, (void **)&st.scale, ns * sizeof(float)))) return rc;
+  }
+  return DS2D_OK;
+}
+
+int ensure_common(ds2d_ctx *c) {
+  if (c->p_b) return DS2D_OK;
+  int rc;
+  float **ps[5] = {&c->p_b, &c->p_lam, &c->p_mu, &c->p_kpp, &c->p_kps};
+  for (float **p : ps)
+    if ((rc = alloc_slots(c, p))) return rc;
+  if (!c->d.rbc) {
+    if ((rc = alloc_slots(c, &c->p_dampx))) return rc;
+    if ((rc = alloc_slots(c, &c->p_dampz))) return rc;
+  }
+  if ((rc = alloc_wave(c, c->fw, false))) return rc;
+  if ((rc = alloc(c, (void **)&c->d_shots, sizeof(ShotDev) * c->B))) return rc;
+  if ((rc = alloc(c, (void **)&c->d_rmap, sizeof(int) * (size_t)c->B * c->d.nxp))) return rc;
+  size_t nrec = (size_t)c->B * c->d.max_ntr * c->d.nt;
+  for (int i = 0; i < 2; i++)
+    if ((rc = alloc(c, (void **)&c->rec[i], nrec * sizeof(float)))) return rc;
+  c->par.b = c->p_b; c->par.lam = c->p_lam; c->par.mu = c->p_mu;
+  c->par.dampx = c->p_dampx; c->par.dampz = c->p_dampz;
+  c->par.kpp = c->p_kpp; c->par.kps = c->p_kps;
+  return DS2D_OK;
+}
+
+int ensure_rtm(ds2d_ctx *c) {
+  int rc;
+  if ((rc = ensure_common(c))) return rc;
+  if (c->have_rtm) return DS2D_OK;
+  if ((rc = alloc_wave(c, c->abk, true))) return rc;
+  float **es[4] = {&c->e.gx_vx, &c->e.gz_vz, &c->e.gz_vx, &c->e.gx_vz};
+  for (float **p : es)
+    if ((rc = alloc_slots(c, p))) return rc;
+  if (!c->d.rbc && (rc = alloc_strips(c, c->st_a))) return rc;
+  if (!c->img_slot) {
+    size_t n = (size_t)7 * c->B * c->d.wnx * c->d.wnz;
+    if ((rc = alloc(c, (void **)&c->img_slot, n * sizeof(float)))) return rc;
+  }
+  c->have_rtm = true;
+  return DS2D_OK;
+}
+
+int ensure_elsrtm(ds2d_ctx *c) {
+  int rc;
+  if ((rc = ensure_rtm(c))) return rc;
+  if (c->have_elsrtm) return DS2D_OK;
+  if ((rc = alloc_slots(c, &c->p_dmp))) return rc;
+  if ((rc = alloc_slots(c, &c->p_dms))) return rc;
+  c->par.dmp = c->p_dmp;
+  c->par.dms = c->p_dms;
+  if ((rc = alloc_wave(c, c->b1, false))) return rc;
+  if ((rc = alloc_wave(c, c->b2, false))) return rc;
+  if ((rc = alloc_wave(c, c->bbk, true))) return rc;
+  float **es[4] = {&c->be.gx_vx, &c->be.gz_vz, &c->be.gz_vx, &c->be.gx_vz};
+  for (float **p : es)
+    if ((rc = alloc_slots(c, p))) return rc;
+  for (int i = 0; i < 3; i++)
+    if ((rc = alloc_slots(c, &c->ov_s[i]))) return rc;
+  for (int i = 0; i < 2; i++)
+    if ((rc = alloc_slots(c, &c->ov_v[i]))) return rc;
+  if (!c->d.rbc && (rc = alloc_strips(c, c->st_b))) return rc;
+  size_t nrec = (size_t)c->B * c->d.max_ntr * c->d.nt;
+  for (int i = 2; i < 8; i++)
+    if ((rc = alloc(c, (void **)&c->rec[i], nrec * sizeof(float)))) return rc;
+  if ((rc = alloc(c, (void **)&c->d_mis, sizeof(double) * (size_t)c->B * c->d.max_ntr))) return rc;
+  c->have_elsrtm = true;
+  return DS2D_OK;
+}
+
+// Validates shots [first, first + n) and uploads their descriptors and receiver maps.
+int upload_batch(ds2d_ctx *c, const ds2d_shot *shots, int n) {
+  const Dims &d = c->d;
+  std::vector<ShotDev> sd(n);
+  std::vector<int> rmap((size_t)n * d.nxp, -1);
+  for (int s = 0; s < n; s++) {
+    const ds2d_shot &sh = shots[s];
+    if (sh.win_left < 0 || sh.win_left + d.wnx > d.allnx)
+      return fail(c, DS2D_E_ARG, "shot %d: window [%d, %d) outside the model (allnx = %d)", s,
+                  sh.win_left, sh.win_left + d.wnx, d.allnx);
+    if (sh.isx < d.nop || sh.isx >= d.nxp - d.nop || sh.isz < d.nop || sh.isz >= d.nzp - d.nop)
+      return fail(c, DS2D_E_ARG, "shot %d: source cell (%d, %d) outside the updated grid", s,
+                  sh.isx, sh.isz);
+    if (sh.ntr < 0 || sh.ntr > d.max_ntr || (sh.ntr > 0 && !sh.igx))
+      return fail(c, DS2D_E_ARG, "shot %d: ntr = %d (max_ntr = %d)", s, sh.ntr, d.max_ntr);
+    if (sh.ntr > 0 && (sh.igz < d.pml || sh.igz >= d.nzp - d.pml))
+      return fail(c, DS2D_E_ARG, "shot %d: receiver row %d outside the interior", s, sh.igz);
+    for (int t = 0; t < sh.ntr; t++) {
+      int gx = sh.igx[t];
+      if (gx < d.pml || gx >= d.nxp - d.pml)
+        return fail(c, DS2D_E_ARG, "shot %d trace %d: receiver column %d outside the interior", s,
+                    t, gx);
+      int &slot = rmap[(size_t)s * d.nxp + gx];
+      if (slot >= 0)
+        return fail(c, DS2D_E_ARG, "shot %d: receivers %d and %d share column %d", s, slot, t, gx);
+      slot = t;
+    }
+    sd[s] = ShotDev{sh.win_left, sh.isx, sh.isz, sh.igz, sh.ntr, 0, 0, 0};
+  }
+  CK(cudaMemcpyAsync(c->d_shots, sd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_rmap, rmap.data(), sizeof(int) * rmap.size(), cudaMemcpyHostToDevice,
+                     c->stream));
+  return DS2D_OK;
+}
+
+int setup_batch(ds2d_ctx *c, int n, int shot_base, bool with_image) {
+  SetupArgs a{};
+  a.d = c->d;
+  a.vp_all = c->vp_all; a.vs_all = c->vs_all; a.rho_all = c->rho_all;
+  a.pp_all = c->pp_all; a.ps_all = c->ps_all;
+  a.shots = c->d_shots;
+  a.b = c->p_b; a.lam = c->p_lam; a.mu = c->p_mu; a.dampx = c->p_dampx; a.dampz = c->p_dampz;
+  a.kpp = c->p_kpp; a.kps = c->p_kps;
+  a.dmp = with_image ? c->p_dmp : nullptr;
+  a.dms = with_image ? c->p_dms : nullptr;
+  a.L = std::log10((double)(1.0f / 0.001f));  // rr = 0.001 (FD2DGPU.cu:1299)
+  a.seed = c->o.seed;
+  a.shot_base = shot_base;
+  dim3 grid((c->d.ld + 127) / 128, c->d.nxp, n);
+  k_setup<<<grid, 128, 0, c->stream>>>(a);
+  CK(cudaGetLastError());
+  c->last_launches++;
+  return DS2D_OK;
+}
+
+dim3 cell_grid(const Dims &d, int n) { return dim3((d.nzp + kBX - 1) / kBX, (d.nxp + kBY - 1) / kBY, n); }
+
+VelArgs vel_args(ds2d_ctx *c, const Wave &w, int it) {
+  VelArgs v{};
+  v.d = c->d; v.w = w; v.p = c->par; v.shots = c->d_shots; v.wavelet = c->wavelet; v.it = it;
+  v.rmap = c->d_rmap;
+  return v;
+}
+
+StrArgs str_args(ds2d_ctx *c, const Wave &w, int it) {
+  StrArgs s{};
+  s.d = c->d; s.w = w; s.p = c->par; s.it = it; s.shots = c->d_shots; s.rmap = c->d_rmap;
+  return s;
+}
+
+// Launch on the context stream; in profiling mode bracket it with an event pair and record the
+// launch's algorithmic bytes (cells * bytes per cell of that kernel).
+#define LAUNCHP(pname, pbytes, kernel, grid, block, args)                       \
+  do {                                                                          \
+    int ev_ = -1;                                                               \
+    if (c->prof.on) {                                                           \
+      ev_ = c->prof.take();                                                     \
+      cudaEventRecord(c->prof.pool[ev_], c->stream);                            \
+    }                                                                           \
+    kernel<<<grid, block, 0, c->stream>>>(args);                                \
+    c->last_launches++;                                                         \
+    if (ev_ >= 0) {                                                             \
+      cudaEventRecord(c->prof.pool[ev_ + 1], c->stream);                        \
+      c->prof.recs.push_back(ProfRec{pname, ev_, (double)(pbytes)});           \
+    }                                                                           \
+  } while (0)
+
+// Algorithmic bytes per padded cell of each half-step kernel (FP32): every array the update
+// needs read once and every array it produces written once.
+constexpr double kBytesVel = 32;     // S (12) + V (8) + b (4) read, V (8) written
+constexpr double kBytesStr = 40;     // V (8) + S (12) + lam, mu (8) read, S (12) written
+constexpr double kBytesStrRev = 56;  // + four strains written
+constexpr double kBytesVelAdj = 40;  // S (12) + lam, mu (8) + b (4) + V (8) read, V written
+constexpr double kBytesStrAdj = 32;  // V (8) + S (12) read, S (12) written
+constexpr double kBytesImage = 68;   // strains 16 + S 12 + weights 8 + V 8 read, 3 images r/w 24
+#define CELLS(n) ((double)(n) * c->d.nxp * c->d.nzp)
+#define WCELLS(n) ((double)(n) * c->d.wnx * c->d.wnz)
+#define LAUNCH(kernel, grid, block, args) LAUNCHP(#kernel, 0, kernel, grid, block, args)
+
+int strip_save(ds2d_ctx *c, const Wave &w, Strips &st, int it, int n) {
+  StripSaveArgs a{c->d, w.vx, w.vz, st, it};
+  dim3 grid((c->d.lb + 255) / 256, 2, n);
+  LAUNCH(k_strip_save, grid, 256, a);
+  return DS2D_OK;
+}
+
+// Background forward pass with optional recording and strip saving.
+int run_forward_pass(ds2d_ctx *c, int n, bool record, bool strips) {
+  const Dims &d = c->d;
+  dim3 grid = cell_grid(d, n), blk(kBX, kBY);
+  for (int it = 0; it < d.nt; it++) {
+    VelArgs v = vel_args(c, c->fw, it);
+    v.src_on = 1;
+    if (record) { v.rec_on = 1; v.rec_vz = c->rec[0]; v.rec_vx = c->rec[1]; }
+    LAUNCHP("vel_fwd", kBytesVel * CELLS(n), k_vel<kFwd>, grid, blk, v);
+    StrArgs s = str_args(c, c->fw, it);
+    LAUNCHP("str_fwd", kBytesStr * CELLS(n), k_str<kFwd>, grid, blk, s);
+    if (strips) strip_save(c, c->fw, c->st_a, it, n);
+  }
+  CK(cudaGetLastError());
+  return DS2D_OK;
+}
+
+int reduce_images(ds2d_ctx *c, int n, int nimg) {
+  const Dims &d = c->d;
+  dim3 grid((d.allnz + 255) / 256, d.allnx);
+  long long plane = (long long)c->B * d.wnx * d.wnz;
+  k_image_reduce<<<grid, 256, 0, c->stream>>>(d, c->img_slot, plane, nimg, n, c->d_shots, c->images,
+                                              (long long)d.allnx * d.allnz);
+  c->last_launches++;
+  CK(cudaGetLastError());
+  return DS2D_OK;
+}
+
+int check_ready(ds2d_ctx *c, bool need_image) {
+  if (!c) return DS2D_E_ARG;
+  if (!c->models_set) return fail(c, DS2D_E_STATE, "models not set (ds2d_set_models)");
+  if (!c->wavelet_set) return fail(c, DS2D_E_STATE, "wavelet not set (ds2d_set_wavelet)");
+  if (need_image && !c->image_set) return fail(c, DS2D_E_STATE, "image not set (ds2d_set_image)");
+  return DS2D_OK;
+}
+
+int copy_records_in(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *src_z,
+                    const float *src_x, long long trace_base, float *dz, float *dx,
+                    cudaMemcpyKind kind) {
+  const Dims &d = c->d;
+  size_t nrec = (size_t)n * d.max_ntr * d.nt;
+  CK(cudaMemsetAsync(dz, 0, nrec * sizeof(float), c->stream));
+  CK(cudaMemsetAsync(dx, 0, nrec * sizeof(float), c->stream));
+  long long tb = trace_base;
+  for (int s = 0; s < n; s++) {
+    size_t cnt = (size_t)shots[s].ntr * d.nt;
+    size_t dst = (size_t)s * d.max_ntr * d.nt;
+    if (cnt) {
+      CK(cudaMemcpyAsync(dz + dst, src_z + tb * d.nt, cnt * sizeof(float), kind, c->stream));
+      CK(cudaMemcpyAsync(dx + dst, src_x + tb * d.nt, cnt * sizeof(float), kind, c->stream));
+    }
+    tb += shots[s].ntr;
+  }
+  return DS2D_OK;
+}
+
+int copy_records_out(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *sz,
+                     const float *sx, long long trace_base, float *out_z, float *out_x) {
+  const Dims &d = c->d;
+  long long tb = trace_base;
+  for (int s = 0; s < n; s++) {
+    size_t cnt = (size_t)shots[s].ntr * d.nt;
+    size_t src = (size_t)s * d.max_ntr * d.nt;
+    if (cnt) {
+      if (out_z) CK(cudaMemcpyAsync(out_z + tb * d.nt, sz + src, cnt * 4, cudaMemcpyDeviceToHost, c->stream));
+      if (out_x) CK(cudaMemcpyAsync(out_x + tb * d.nt, sx + src, cnt * 4, cudaMemcpyDeviceToHost, c->stream));
+    }
+    tb += shots[s].ntr;
+  }
+  return DS2D_OK;
+}
+
+int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
+  const Dims &d = c->d;
+  int rc;
+  if ((rc = setup_batch(c, n, shot_base, false))) return rc;
+  if ((rc = zero_wave(c, c->fw, n))) return rc;
+  if ((rc = zero_wave(c, c->abk, n))) return rc;
+  size_t plane = (size_t)c->B * d.wnx * d.wnz;
+  CK(cudaMemsetAsync(c->img_slot, 0, 7 * plane * sizeof(float), c->stream));
+  const bool strips = !d.rbc;
+  if ((rc = run_forward_pass(c, n, false, strips))) return rc;
+  dim3 grid = cell_grid(d, n), blk(kBX, kBY);
+  dim3 igrid((d.wnz + kBX - 1) / kBX, (d.wnx + kBY - 1) / kBY, n);
+  for (int it = d.nt - 1; it >= 0; --it) {
+    StrArgs sr = str_args(c, c->fw, it);
+    sr.e = c->e;
+    sr.st = c->st_a;
+    sr.strips_on = strips;
+    LAUNCHP("str_rev", kBytesStrRev * CELLS(n), k_str<kRev>, grid, blk, sr);
+    VelArgs vr = vel_args(c, c->fw, it);
+    vr.st = c->st_a;
+    vr.strips_outer = strips;
+    LAUNCHP("vel_rev", kBytesVel * CELLS(n), k_vel<kRev>, grid, blk, vr);
+    StrArgs sa = str_args(c, c->abk, it);
+    sa.res_on = 1; sa.res_vz = c->rec[0]; sa.res_vx = c->rec[1];
+    LAUNCHP("str_adj", kBytesStrAdj * CELLS(n), k_str<kAdj>, grid, blk, sa);
+    VelArgs va = vel_args(c, c->abk, it);
+    LAUNCHP("vel_adj", kBytesVelAdj * CELLS(n), k_vel<kAdj>, grid, blk, va);
+    ImgArgs im{};
+    im.d = d; im.p = c->par; im.e = c->e;
+    im.atxx = c->abk.txx; im.atzz = c->abk.tzz; im.atxz = c->abk.txz;
+    im.vx = c->fw.vx; im.vz = c->fw.vz;
+    im.img = c->img_slot; im.img_plane = (long long)plane; im.full = 0;
+    LAUNCHP("image", kBytesImage * WCELLS(n), k_image, igrid, blk, im);
+  }
+  CK(cudaGetLastError());
+  return reduce_images(c, n, 3);
+}
+
+int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int iter,
+                 double *mis_host) {
+  const Dims &d = c->d;
+  int rc;
+  if ((rc = setup_batch(c, n, shot_base, true))) return rc;
+  for (const Wave *w : {&c->fw, &c->b1, &c->b2, &c->abk, &c->bbk})
+    if ((rc = zero_wave(c, *w, n))) return rc;
+  size_t bytes = sizeof(float) * (size_t)d.slot * n;
+  for (int i = 0; i < 3; i++) CK(cudaMemsetAsync(c->ov_s[i], 0, bytes, c->stream));
+  for (int i = 0; i < 2; i++) CK(cudaMemsetAsync(c->ov_v[i], 0, bytes, c->stream));
+  size_t plane = (size_t)c->B * d.wnx * d.wnz;
+  CK(cudaMemsetAsync(c->img_slot, 0, 7 * plane * sizeof(float), c->stream));
+  size_t nrec = (size_t)n * d.max_ntr * d.nt;
+  for (int i = 2; i < 6; i++) CK(cudaMemsetAsync(c->rec[i], 0, nrec * sizeof(float), c->stream));
+  const bool strips = !d.rbc;
+  dim3 grid = cell_grid(d, n), blk(kBX, kBY);
+  // Forward pass, FD2DGPU.cu:4396-4478: background, first- and second-order scattered sets.
+  for (int it = 0; it < d.nt; it++) {
+    VelArgs v = vel_args(c, c->fw, it);
+    v.src_on = 1;
+    LAUNCH(k_vel<kFwd>, grid, blk, v);
+    StrArgs s = str_args(c, c->fw, it);
+    LAUNCH(k_str<kFwd>, grid, blk, s);
+    BornArgs bs{d, c->fw.vx, c->fw.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
+    LAUNCH(k_born, grid, blk, bs);
+    VelArgs v1 = vel_args(c, c->b1, it);
+    v1.ov_txx = c->ov_s[0]; v1.ov_tzz = c->ov_s[1]; v1.ov_txz = c->ov_s[2];
+    v1.rec_on = 1; v1.rec_vz = c->rec[2]; v1.rec_vx = c->rec[3];
+    LAUNCH(k_vel<kFwd>, grid, blk, v1);
+    StrArgs s1 = str_args(c, c->b1, it);
+    LAUNCH(k_str<kFwd>, grid, blk, s1);
+    BornArgs bs2{d, c->b1.vx, c->b1.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
+    LAUNCH(k_born, grid, blk, bs2);
+    VelArgs v2 = vel_args(c, c->b2, it);
+    v2.ov_txx = c->ov_s[0]; v2.ov_tzz = c->ov_s[1]; v2.ov_txz = c->ov_s[2];
+    v2.rec_on = 1; v2.rec_vz = c->rec[4]; v2.rec_vx = c->rec[5];
+    LAUNCH(k_vel<kFwd>, grid, blk, v2);
+    StrArgs s2 = str_args(c, c->b2, it);
+    LAUNCH(k_str<kFwd>, grid, blk, s2);
+    if (strips) {
+      strip_save(c, c->fw, c->st_a, it, n);
+      strip_save(c, c->b1, c->st_b, it, n);
+    }
+  }
+  // Lm + Lm2 and the NCC adjoint source (FD2DGPU.cu:4532, 4556-4664).
+  k_lm_add<<<(unsigned)((nrec + 255) / 256), 256, 0, c->stream>>>(c->rec[2], c->rec[3], c->rec[4],
+                                                                   c->rec[5], (long long)nrec);
+  c->last_launches++;
+  k_ncc<<<dim3(d.max_ntr, n), 256, 0, c->stream>>>(d, c->d_shots, c->rec[2], c->rec[3], c->rec[0],
+                                                   c->rec[1], c->rec[6], c->rec[7], c->d_mis, iter);
+  c->last_launches++;
+  CK(cudaGetLastError());
+  dim3 igrid((d.wnz + kBX - 1) / kBX, (d.wnx + kBY - 1) / kBY, n);
+  // Backward pass, FD2DGPU.cu:4685-4807.
+  for (int it = d.nt - 1; it >= 0; --it) {
+    StrArgs sr = str_args(c, c->fw, it);
+    sr.e = c->e; sr.st = c->st_a; sr.strips_on = strips;
+    LAUNCH(k_str<kRev>, grid, blk, sr);
+    VelArgs vr = vel_args(c, c->fw, it);
+    vr.st = c->st_a; vr.strips_outer = strips;
+    LAUNCH(k_vel<kRev>, grid, blk, vr);
+    StrArgs sb = str_args(c, c->b1, it);
+    sb.e = c->be; sb.st = c->st_b; sb.strips_on = strips;
+    LAUNCH(k_str<kRev>, grid, blk, sb);
+    BornArgs bs{d, c->fw.vx, c->fw.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
+    LAUNCH(k_born, grid, blk, bs);
+    VelArgs vb = vel_args(c, c->b1, it);
+    vb.ov_txx = c->ov_s[0]; vb.ov_tzz = c->ov_s[1]; vb.ov_txz = c->ov_s[2];
+    vb.st = c->st_b; vb.strips_outer = strips;
+    LAUNCH(k_vel<kRev>, grid, blk, vb);
+    StrArgs sa = str_args(c, c->abk, it);
+    sa.res_on = 1; sa.res_vz = c->rec[6]; sa.res_vx = c->rec[7];
+    LAUNCH(k_str<kAdj>, grid, blk, sa);
+    VelArgs va = vel_args(c, c->abk, it);
+    LAUNCH(k_vel<kAdj>, grid, blk, va);
+    VelArgs vbb = vel_args(c, c->bbk, it);
+    LAUNCH(k_vel<kAdj>, grid, blk, vbb);
+    BornAdjArgs ba{d, c->abk.txx, c->abk.tzz, c->abk.txz, c->par, c->ov_v[0], c->ov_v[1]};
+    LAUNCH(k_born_adj, grid, blk, ba);
+    StrArgs sbb = str_args(c, c->bbk, it);
+    sbb.ov_vx = c->ov_v[0]; sbb.ov_vz = c->ov_v[1];
+    LAUNCH(k_str<kAdj>, grid, blk, sbb);
+    ImgArgs im{};
+    im.d = d; im.p = c->par; im.e = c->e; im.be = c->be;
+    im.atxx = c->abk.txx; im.atzz = c->abk.tzz; im.atxz = c->abk.txz;
+    im.btxx = c->bbk.txx; im.btzz = c->bbk.tzz; im.btxz = c->bbk.txz;
+    im.vx = c->fw.vx; im.vz = c->fw.vz;
+    im.img = c->img_slot; im.img_plane = (long long)plane; im.full = 1;
+    LAUNCH(k_image, igrid, blk, im);
+  }
+  CK(cudaGetLastError());
+  if ((rc = reduce_images(c, n, 7))) return rc;
+  std::vector<double> terms((size_t)n * d.max_ntr);
+  CK(cudaMemcpyAsync(terms.data(), c->d_mis, terms.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (mis_host && iter != 0)
+    for (int s = 0; s < n; s++)
+      for (int t = 0; t < shots[s].ntr; t++) *mis_host -= terms[(size_t)s * d.max_ntr + t];
+  return DS2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
+  if (!grid || !opts || !out) return DS2D_E_ARG;
+  *out = nullptr;
+  ds2d_ctx *c = new ds2d_ctx();
+  c->g = *grid;
+  c->o = *opts;
+  const ds2d_grid &g = *grid;
+  const int nop = 4;
+  auto bad = [&](const char *m) {
+    g_create_err = m;
+    delete c;
+    return DS2D_E_ARG;
+  };
+  if (g.allnx <= 0 || g.allnz <= 0 || g.nx <= 0 || g.nx > g.allnx || g.nt <= 0)
+    return bad("grid sizes must be positive with nx <= allnx");
+  if (g.pml < 2 * nop) return bad("pml must be at least 8 cells (2 * nop) for the strip bands");
+  if (!(g.dx > 0 && g.dz > 0 && g.dt > 0)) return bad("dx, dz, dt must be positive");
+  if (opts->max_shots <= 0 || opts->max_shots > 65535) return bad("max_shots out of range");
+  if (opts->max_ntr < 0) return bad("max_ntr must be >= 0");
+  if (opts->strip_precision < 0 || opts->strip_precision > 2) return bad("strip_precision");
+  if (opts->boundary != DS2D_BOUNDARY_PML && opts->boundary != DS2D_BOUNDARY_RANDOM)
+    return bad("boundary");
+  cudaError_t e = cudaSetDevice(opts->device);
+  if (e != cudaSuccess) {
+    g_create_err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+    delete c;
+    return DS2D_E_CUDA;
+  }
+  Dims &d = c->d;
+  d.nxp = g.nx + 2 * g.pml;
+  d.nzp = g.allnz + 2 * g.pml;
+  d.ld = (d.nzp + 31) / 32 * 32;
+  d.pml = g.pml;
+  d.nop = nop;
+  d.wnx = g.nx;
+  d.wnz = g.allnz;
+  d.nt = g.nt;
+  d.allnx = g.allnx;
+  d.allnz = g.allnz;
+  d.slot = (long long)d.nxp * d.ld;
+  d.dx = g.dx; d.dz = g.dz; d.dt = g.dt;
+  d.rbc = opts->boundary == DS2D_BOUNDARY_RANDOM;
+  d.lb = 4 * nop * (d.wnx + d.wnz);
+  d.nseg = (d.lb + 31) / 32;
+  d.max_ntr = std::max(opts->max_ntr, 1);
+  c->B = opts->max_shots;
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+    fail(c, DS2D_E_CUDA, "cudaStreamCreate failed");
+    delete c;
+    return DS2D_E_CUDA;
+  }
+  c->stream = c->own;
+  size_t nall = (size_t)g.allnx * g.allnz;
+  int rc = 0;
+  if ((rc = alloc(c, (void **)&c->vp_all, nall * 4)) || (rc = alloc(c, (void **)&c->vs_all, nall * 4)) ||
+      (rc = alloc(c, (void **)&c->pp_all, nall * 4)) || (rc = alloc(c, (void **)&c->ps_all, nall * 4)) ||
+      (rc = alloc(c, (void **)&c->images, 7 * nall * 4)) ||
+      (rc = alloc(c, (void **)&c->wavelet, (size_t)g.nt * 4))) {
+    ds2d_destroy(c);
+    return rc;
+  }
+  if (cudaMemsetAsync(c->images, 0, 7 * nall * 4, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    ds2d_destroy(c);
+    return DS2D_E_CUDA;
+  }
+  *out = c;
+  return DS2D_OK;
+}
+
+int ds2d_destroy(ds2d_ctx *c) {
+  if (!c) return DS2D_OK;
+  if (c->own) cudaStreamSynchronize(c->own);
+  c->arena.release();
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return DS2D_OK;
+}
+
+const char *ds2d_last_error(const ds2d_ctx *c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+
+int ds2d_set_stream(ds2d_ctx *c, void *stream) {
+  if (!c) return DS2D_E_ARG;
+  c->stream = stream ? (cudaStream_t)stream : c->own;
+  return DS2D_OK;
+}
+
+int ds2d_set_models(ds2d_ctx *c, const float *vp, const float *vs, const float *rho) {
+  if (!c || !vp || !vs) return DS2D_E_ARG;
+  size_t n = (size_t)c->g.allnx * c->g.allnz;
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(vp[i]) || !std::isfinite(vs[i]) || vp[i] <= 0.f || vs[i] < 0.f)
+      return fail(c, DS2D_E_ARG, "model value at %zu is not a valid velocity (vp %g, vs %g)", i,
+                  vp[i], vs[i]);
+  CK(cudaMemcpyAsync(c->vp_all, vp, n * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->vs_all, vs, n * 4, cudaMemcpyHostToDevice, c->stream));
+  if (rho) {
+    for (size_t i = 0; i < n; i++)
+      if (!std::isfinite(rho[i]) || rho[i] <= 0.f)
+        return fail(c, DS2D_E_ARG, "density at %zu is not positive", i);
+    if (!c->rho_all) {
+      int rc = alloc(c, (void **)&c->rho_all, n * 4);
+      if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(c->rho_all, rho, n * 4, cudaMemcpyHostToDevice, c->stream));
+  } else {
+    c->rho_all = nullptr;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->models_set = true;
+  return DS2D_OK;
+}
+
+int ds2d_set_wavelet(ds2d_ctx *c, const float *w) {
+  if (!c || !w) return DS2D_E_ARG;
+  CK(cudaMemcpyAsync(c->wavelet, w, (size_t)c->g.nt * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->wavelet_set = true;
+  return DS2D_OK;
+}
+
+int ds2d_set_image(ds2d_ctx *c, const float *pp, const float *ps) {
+  if (!c || !pp || !ps) return DS2D_E_ARG;
+  size_t n = (size_t)c->g.allnx * c->g.allnz;
+  CK(cudaMemcpyAsync(c->pp_all, pp, n * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->ps_all, ps, n * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->image_set = true;
+  return DS2D_OK;
+}
+
+int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, float *rec_vx) {
+  int rc;
+  if ((rc = check_ready(c, false))) return rc;
+  if (n < 0 || (n > 0 && (!shots || !rec_vz || !rec_vx))) return fail(c, DS2D_E_ARG, "bad arguments");
+  if ((rc = ensure_common(c))) return rc;
+  c->last_launches = 0;
+  c->last_updates = 0;
+  long long tb = 0;
+  for (int f = 0; f < n; f += c->B) {
+    int m = std::min(c->B, n - f);
+    if ((rc = upload_batch(c, shots + f, m))) return rc;
+    if ((rc = setup_batch(c, m, f, false))) return rc;
+    if ((rc = zero_wave(c, c->fw, m))) return rc;
+    size_t nrec = (size_t)m * c->d.max_ntr * c->d.nt;
+    CK(cudaMemsetAsync(c->rec[0], 0, nrec * 4, c->stream));
+    CK(cudaMemsetAsync(c->rec[1], 0, nrec * 4, c->stream));
+    if ((rc = run_forward_pass(c, m, true, false))) return rc;
+    if ((rc = copy_records_out(c, shots + f, m, c->rec[0], c->rec[1], tb, rec_vz, rec_vx))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
+    c->last_updates += (double)m * c->d.nxp * c->d.nzp * c->d.nt;
+  }
+  return DS2D_OK;
+}
+
+static int rtm_common(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *az,
+                      const float *ax, cudaMemcpyKind kind) {
+  int rc;
+  if ((rc = check_ready(c, false))) return rc;
+  if (n < 0 || (n > 0 && (!shots || !az || !ax))) return fail(c, DS2D_E_ARG, "bad arguments");
+  if ((rc = ensure_rtm(c))) return rc;
+  c->last_launches = 0;
+  c->last_updates = 0;
+  long long tb = 0;
+  for (int f = 0; f < n; f += c->B) {
+    int m = std::min(c->B, n - f);
+    if ((rc = upload_batch(c, shots + f, m))) return rc;
+    if ((rc = copy_records_in(c, shots + f, m, az, ax, tb, c->rec[0], c->rec[1], kind))) return rc;
+    if ((rc = rtm_batch(c, shots + f, m, f))) return rc;
+    for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
+    c->last_updates += 3.0 * m * c->d.nxp * c->d.nzp * c->d.nt;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+int ds2d_rtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *adj_vz, const float *adj_vx) {
+  return rtm_common(c, shots, n, adj_vz, adj_vx, cudaMemcpyHostToDevice);
+}
+
+int ds2d_rtm_device(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *adj_vz,
+                    const float *adj_vx) {
+  return rtm_common(c, shots, n, adj_vz, adj_vx, cudaMemcpyDeviceToDevice);
+}
+
+int ds2d_elsrtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *obs_vz,
+                const float *obs_vx, int iter, double *misfit, float *lm_vz, float *lm_vx,
+                float *res_vz, float *res_vx) {
+  int rc;
+  if ((rc = check_ready(c, true))) return rc;
+  if (n < 0 || (n > 0 && (!shots || !obs_vz || !obs_vx))) return fail(c, DS2D_E_ARG, "bad arguments");
+  if ((rc = ensure_elsrtm(c))) return rc;
+  c->last_launches = 0;
+  c->last_updates = 0;
+  long long tb = 0;
+  for (int f = 0; f < n; f += c->B) {
+    int m = std::min(c->B, n - f);
+    if ((rc = upload_batch(c, shots + f, m))) return rc;
+    if ((rc = copy_records_in(c, shots + f, m, obs_vz, obs_vx, tb, c->rec[0], c->rec[1],
+                              cudaMemcpyHostToDevice)))
+      return rc;
+    if ((rc = elsrtm_batch(c, shots + f, m, f, iter, misfit))) return rc;
+    if (lm_vz || lm_vx)
+      if ((rc = copy_records_out(c, shots + f, m, c->rec[2], c->rec[3], tb, lm_vz, lm_vx))) return rc;
+    if (res_vz || res_vx)
+      if ((rc = copy_records_out(c, shots + f, m, c->rec[6], c->rec[7], tb, res_vz, res_vx))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
+    c->last_updates += 7.0 * m * c->d.nxp * c->d.nzp * c->d.nt;
+  }
+  return DS2D_OK;
+}
+
+int ds2d_read_images(ds2d_ctx *c, float *const images[7], int reset) {
+  if (!c || !images) return DS2D_E_ARG;
+  size_t n = (size_t)c->g.allnx * c->g.allnz;
+  for (int a = 0; a < 7; a++)
+    if (images[a])
+      CK(cudaMemcpyAsync(images[a], c->images + a * n, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (reset) CK(cudaMemsetAsync(c->images, 0, 7 * n * 4, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+int ds2d_profile(ds2d_ctx *c, int enable) {
+  if (!c) return DS2D_E_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  c->prof.on = enable != 0;
+  c->prof.recs.clear();
+  c->prof.used = 0;
+  return DS2D_OK;
+}
+
+int ds2d_profile_report(ds2d_ctx *c, char *buf, int len) {
+  if (!c || !buf || len <= 0) return DS2D_E_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  struct Agg {
+    std::string name;
+    long long n = 0;
+    double ms = 0, bytes = 0;
+  };
+  std::vector<Agg> agg;
+  for (const ProfRec &r : c->prof.recs) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->prof.pool[r.ev], c->prof.pool[r.ev + 1]));
+    Agg *a = nullptr;
+    for (Agg &x : agg)
+      if (x.name == r.name) a = &x;
+    if (!a) {
+      agg.push_back(Agg{r.name});
+      a = &agg.back();
+    }
+    a->n++;
+    a->ms += ms;
+    a->bytes += r.bytes;
+  }
+  std::string out;
+  for (const Agg &a : agg) {
+    char line[256];
+    snprintf(line, sizeof line, "%s %lld %.6f %.6e\n", a.name.c_str(), a.n, a.ms, a.bytes);
+    out += line;
+  }
+  snprintf(buf, len, "%s", out.c_str());
+  c->prof.recs.clear();
+  c->prof.used = 0;
+  return (int)out.size() < len ? DS2D_OK : DS2D_E_ARG;
+}
+
+double ds2d_last_cell_updates(const ds2d_ctx *c) { return c ? c->last_updates : 0.0; }
+long long ds2d_last_launches(const ds2d_ctx *c) { return c ? c->last_launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,130 @@
+/*
+ * ds2d.h -- C ABI of the B200-native DS2D time-stepping path.
+ *
+ * The reference exposes this path as the C++ class FD2DGPU_ELASTIC (FD2DGPU.cuh:124-422) plus
+ * the per-shot driver ELSRTM_ROT_EXP_IMAGE_SINGLESHOT (FD2DGPU.cuh:429-430), called by
+ * lsrtm_all_iteration (main.cpp:939-1035).  The entry points below replace that surface with a
+ * plain C ABI: plain pointers and sizes, every call returns an int status (0 = DS2D_OK,
+ * negative = DS2D_E_*), ds2d_last_error() gives the message.  Host arrays belong to the caller
+ * and are copied in; the context owns all device memory.  One context per host thread.
+ *
+ * Array conventions follow the reference (idx = ix*nz + iz, z fastest):
+ *   models / images   [allnx][allnz] float
+ *   records           [ntr][nt] float per shot, shots concatenated in call order
+ * Geometry is given in cells of the padded shot window: nxpml = nx + 2*pml, nzpml = allnz +
+ * 2*pml, the window's first interior column sits at model column win_left.
+ */
+#ifndef DS2D_H
+#define DS2D_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DS2D_OK 0
+#define DS2D_E_ARG -1     /* invalid argument / geometry outside the model */
+#define DS2D_E_CUDA -2    /* CUDA runtime error (message in ds2d_last_error) */
+#define DS2D_E_NOMEM -3   /* device allocation failed */
+#define DS2D_E_STATE -4   /* call order violated (e.g. models not set) */
+#define DS2D_E_NUMERIC -5 /* non-finite value detected in a result */
+
+enum { DS2D_BOUNDARY_PML = 0, DS2D_BOUNDARY_RANDOM = 1 };
+enum { DS2D_STRIPS_F32 = 0, DS2D_STRIPS_F16 = 1, DS2D_STRIPS_BF16 = 2 };
+
+typedef struct ds2d_ctx ds2d_ctx;
+
+/* Grid of one run.  Replaces the constructor arguments of FD2DGPU_ELASTIC
+ * (FD2DGPU.cu:1350-1352: dx, dz, dt, nxpml, nzpml, allnx, allnz, pml, nt; nop is fixed to 4 as
+ * in main.cpp:1490). */
+typedef struct {
+  int allnx, allnz; /* full model */
+  int nx;           /* shot window width in cells (all shots share it, main.cpp:1421-1423) */
+  int pml;          /* PML width, or random-band width when boundary = RANDOM */
+  int nt;           /* time steps */
+  float dx, dz, dt;
+} ds2d_grid;
+
+typedef struct {
+  int boundary;           /* DS2D_BOUNDARY_PML (strips saved) or _RANDOM (parameters line 9 rbc) */
+  int strip_precision;    /* DS2D_STRIPS_*: storage of the saved boundary strips */
+  int max_shots;          /* shots resident on the device at once (batch size) */
+  int max_ntr;            /* upper bound of receivers per shot */
+  unsigned long long seed;/* random-band seed */
+  int device;             /* CUDA device ordinal */
+} ds2d_opts;
+
+/* One shot.  Replaces the public fields the reference sets before each driver call
+ * (main.cpp:1019-1025: isx, isz, igz, delta_left + record_left_in_v) and the trace coordinates
+ * of record_copytoGPU (FD2DGPU.cu:3537), already mapped to cells as
+ * GPUrecord_scatterwavefield does (FD2DGPU.cu:3097: igx = pml + (gc - ngx_left)/dx). */
+typedef struct {
+  int win_left;   /* model column of the first interior column of the window */
+  int isx, isz;   /* source cell (padded window coordinates) */
+  int igz;        /* receiver row */
+  int ntr;        /* receivers of this shot (<= max_ntr) */
+  const int *igx; /* ntr distinct receiver columns (padded window coordinates) */
+} ds2d_shot;
+
+/* FD2DGPU_ELASTIC::FD2DGPU_ELASTIC (FD2DGPU.cu:1350). */
+int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out);
+/* FD2DGPU_ELASTIC::~FD2DGPU_ELASTIC (FD2DGPU.cu:1640). */
+int ds2d_destroy(ds2d_ctx *ctx);
+const char *ds2d_last_error(const ds2d_ctx *ctx);
+
+/* Launch stream (cudaStream_t; NULL = the context's own stream).  The reference uses the
+ * default stream throughout (FD2DGPU.cuh:282 stream parameters receive 0). */
+int ds2d_set_stream(ds2d_ctx *ctx, void *stream);
+
+/* FD2DGPU_ELASTIC::GPUbufferVPVS (FD2DGPU.cu:1310).  rho may be NULL: the reference hard-wires
+ * rho = 2000 (FD2DGPU.cu:1121). */
+int ds2d_set_models(ds2d_ctx *ctx, const float *vp, const float *vs, const float *rho);
+/* Source wavelet, nt samples (constructor argument `sou`, FD2DGPU.cu:55; main.cpp:1476). */
+int ds2d_set_wavelet(ds2d_ctx *ctx, const float *wavelet);
+/* FD2DGPU_ELASTIC::GPUbufferM (FD2DGPU.cu:1316): reflectivity images used by the Born source. */
+int ds2d_set_image(ds2d_ctx *ctx, const float *image_pp, const float *image_ps);
+
+/* Background forward modelling of n shots (FD2DGPU.cu:4398-4400 addS + born_modeling mode 0),
+ * recording vz / vx at the receivers after every step.  rec_* receive [sum ntr][nt]. */
+int ds2d_forward(ds2d_ctx *ctx, const ds2d_shot *shots, int n, float *rec_vz, float *rec_vx);
+
+/* Reference-mode ELSRTM of n shots: ELSRTM_ROT_EXP_IMAGE_SINGLESHOT (FD2DGPU.cu:4184) per shot,
+ * with record_copytoGPU (:3537) and bufferVpVsHtoD (:1336) folded in.  obs_* are the observed
+ * records [sum ntr][nt].  Gradients accumulate in the context's seven images (read them with
+ * ds2d_read_images); *misfit accumulates like the reference's double& argument.  lm_* / res_*
+ * may be NULL; when given they receive Lm + Lm2 and the injected adjoint source. */
+int ds2d_elsrtm(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *obs_vz,
+                const float *obs_vx, int iter, double *misfit, float *lm_vz, float *lm_vx,
+                float *res_vz, float *res_vx);
+
+/* Elastic RTM of n shots: background forward pass, then interior reconstruction
+ * (FD2DGPU.cu:4769-4772), adjoint propagation of adj_* injected at the receivers (:3306,
+ * stack = true; :4775-4778) and zero-lag imaging (:3245 doimage_gradient, :3235 doimage_illum)
+ * into images 0 (pp), 1 (ps) and 2 (illumination).  adj_* are host arrays [sum ntr][nt]. */
+int ds2d_rtm(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *adj_vz,
+             const float *adj_vx);
+/* Same as ds2d_rtm with adj_* already in device memory (no host copies). */
+int ds2d_rtm_device(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *adj_vz_dev,
+                    const float *adj_vx_dev);
+
+/* FD2DGPU_ELASTIC::imagebuffer_resettozero (FD2DGPU.cu:3478): copies the seven accumulated
+ * images (pp_grad, ps_grad, illumination, b_pp, b_ps, b_pp2, b_ps2; each [allnx][allnz]) to the
+ * host arrays that are not NULL, then zeroes them when reset != 0. */
+int ds2d_read_images(ds2d_ctx *ctx, float *const images[7], int reset);
+
+/* Cell-updates performed by the last ds2d_forward / ds2d_elsrtm / ds2d_rtm call (padded cells x
+ * steps x propagations), for throughput reporting. */
+double ds2d_last_cell_updates(const ds2d_ctx *ctx);
+
+/* Number of kernel launches issued by the last forward / elsrtm / rtm call. */
+long long ds2d_last_launches(const ds2d_ctx *ctx);
+
+/* Profiling (no counterpart in the reference, which has only a commented-out host timer,
+ * FD2DGPU.cu:3554-3583): when enabled, every launch is bracketed by CUDA events on the launch
+ * stream.  ds2d_profile_report writes one line per kernel, "name launches total_ms
+ * algorithmic_bytes", for the launches since the last report, and clears them. */
+int ds2d_profile(ds2d_ctx *ctx, int enable);
+int ds2d_profile_report(ds2d_ctx *ctx, char *buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,17 @@
+#!/usr/bin/env bash
+# Builds the reference's own CUDA path (FD2DGPU.cu + born.cu, compiled where they lie in the
+# reference tree) plus oracle/ref_harness.cu into oracle/_ref/libds2dref.so.  Test
+# infrastructure only: the library is the parity checker, never the product.  Flags follow the
+# reference Makefile (nvcc -O3 -w -DELASTIC -DORDER=12) with an explicit sm_100a target.
+set -euo pipefail
+REF="${DS2D_REFERENCE:-/root/reference}"
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+mkdir -p "$OUT"
+FLAGS="-O3 -w -DELASTIC -DORDER=12 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC"
+nvcc $FLAGS -I"$REF" -c "$REF/born.cu" -o "$OUT/born.o"
+nvcc $FLAGS -I"$REF" -c "$HERE/ref_harness.cu" -o "$OUT/ref_harness.o"
+nvcc -shared -gencode arch=compute_100a,code=sm_100a -o "$OUT/libds2dref.so" \
+  "$OUT/ref_harness.o" "$OUT/born.o" -lcublas -lcufft
+rm -f "$OUT/born.o" "$OUT/ref_harness.o"
+echo "built $OUT/libds2dref.so"

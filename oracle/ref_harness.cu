@@ -1,0 +1,243 @@
+// Harness around the reference's own CUDA build -- TEST INFRASTRUCTURE ONLY.
+//
+// Compiles the reference translation unit FD2DGPU.cu in place (it is #included from the
+// reference tree by oracle/build_ref.sh; nothing is copied) and drives its FD2DGPU_ELASTIC class
+// through the call sequence of main.cpp:939-1035 without MPI.  The resulting library
+// (oracle/_ref/libds2dref.so) produces the golden outputs that pin the CPU oracle and the
+// B200 kernels.  Members the reference declares private (lamda, miu) are needed to inject a
+// pre-randomised model, hence the access override below.
+#define private public
+#include "FD2DGPU.cu"
+#undef private
+
+#include <cstdint>
+#include <vector>
+
+namespace {
+
+struct RefGeom {
+  int allnx, allnz, nx, pml, nt;
+  float dx, dz, dt;
+};
+
+// Receiver sampling of the background field (the reference records only scattered fields;
+// forward modelling for observed data reads the public vx / vz, as the survey describes).
+__global__ void harness_record(const float *vz, const float *vx, float *rz, float *rx,
+                               const int *igx, int igz, int nzpml, int ntr, int nt, int it) {
+  int tr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tr >= ntr) return;
+  size_t k = (size_t)igx[tr] * nzpml + igz;
+  rz[(size_t)tr * nt + it] = vz[k];
+  rx[(size_t)tr * nt + it] = vx[k];
+}
+
+FD2DGPU_ELASTIC *make(const RefGeom &g, const float *wavelet, int ntr) {
+  int nxpml = g.nx + 2 * g.pml, nzpml = g.allnz + 2 * g.pml;
+  return new FD2DGPU_ELASTIC(wavelet, g.dx, g.dz, g.dt, nxpml, nzpml, g.allnx, g.allnz, 1, g.pml,
+                             g.nt, 4, ntr);
+}
+
+// Receiver coordinates such that pml + (int)((float)(gc - ngx_left)/dx) == igx exactly.
+std::vector<int> coords_from_cells(const RefGeom &g, const int *igx, int ntr) {
+  std::vector<int> gc(ntr);
+  for (int i = 0; i < ntr; i++) gc[i] = (int)((igx[i] - g.pml) * g.dx);
+  return gc;
+}
+
+int last_error() { return (int)cudaDeviceSynchronize(); }
+
+}  // namespace
+
+extern "C" {
+
+// Background forward modelling (FD2DGPU.cu:4398-4400: addS + born_modeling mode 0).
+int ref_forward(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz, float dt,
+                const float *vp_all, const float *vs_all, const float *wavelet, int win_left,
+                int isx, int isz, int igz, int ntr, const int *igx, float *rec_vz,
+                float *rec_vx) {
+  RefGeom g{allnx, allnz, nx, pml, nt, dx, dz, dt};
+  FD2DGPU_ELASTIC *f = make(g, wavelet, ntr);
+  std::vector<float> vp(vp_all, vp_all + (size_t)allnx * allnz), vs(vs_all, vs_all + (size_t)allnx * allnz);
+  f->GPUbufferVPVS(vp.data(), vs.data());
+  f->bufferVpVsHtoD(win_left);
+  f->isx = isx;
+  f->isz = isz;
+  f->igz = igz;
+  int nDim = f->nxpml * f->nzpml;
+  f->FD_ELASTIC_initial(nDim);
+  f->calculate_elastic_damp_C();
+  int *d_igx;
+  float *d_rz, *d_rx;
+  cudaMalloc(&d_igx, ntr * sizeof(int));
+  cudaMalloc(&d_rz, (size_t)ntr * nt * sizeof(float));
+  cudaMalloc(&d_rx, (size_t)ntr * nt * sizeof(float));
+  cudaMemcpy(d_igx, igx, ntr * sizeof(int), cudaMemcpyHostToDevice);
+  for (int it = 0; it < nt; ++it) {
+    f->elastic_rotation_addS_for(it, 0);
+    f->born_modeling(1, 0);
+    harness_record<<<(ntr + 127) / 128, 128>>>(f->vz, f->vx, d_rz, d_rx, d_igx, igz, f->nzpml,
+                                                ntr, nt, it);
+  }
+  cudaMemcpy(rec_vz, d_rz, (size_t)ntr * nt * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(rec_vx, d_rx, (size_t)ntr * nt * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(d_igx);
+  cudaFree(d_rz);
+  cudaFree(d_rx);
+  int rc = last_error();
+  delete f;
+  return rc;
+}
+
+// One reference-mode ELSRTM shot through the reference driver itself (rbc = 0, cpu_mem = 0),
+// followed by imagebuffer_resettozero.  img7 receives seven full-size images [allnx][allnz].
+int ref_elsrtm(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz, float dt,
+               const float *vp_all, const float *vs_all, const float *wavelet,
+               const float *image_pp, const float *image_ps, int win_left, int isx, int isz,
+               int igz, int ntr, const int *igx, const float *obs_vz, const float *obs_vx,
+               int iter, float *res_vz, float *res_vx, float *const img7[7], double *misfit) {
+  RefGeom g{allnx, allnz, nx, pml, nt, dx, dz, dt};
+  size_t nall = (size_t)allnx * allnz, nrec = (size_t)ntr * nt;
+  FD2DGPU_ELASTIC *f = make(g, wavelet, ntr);
+  std::vector<float> vp(vp_all, vp_all + nall), vs(vs_all, vs_all + nall);
+  std::vector<float> ipp(image_pp, image_pp + nall), ips(image_ps, image_ps + nall);
+  std::vector<float> rz(obs_vz, obs_vz + nrec), rx(obs_vx, obs_vx + nrec);
+  std::vector<int> gc = coords_from_cells(g, igx, ntr);
+  f->GPUbufferVPVS(vp.data(), vs.data());
+  f->GPUbufferM(ipp.data(), ips.data());
+  f->record_copytoGPU(rz.data(), rx.data(), gc.data());
+  f->bufferVpVsHtoD(win_left);
+  f->delta_left = win_left;
+  f->record_left_in_v = 0;
+  f->isx = isx;
+  f->isz = isz;
+  f->igz = igz;
+  f->cmin = (float)win_left;
+  f->ngx_left = 0;
+  int nDim = f->nxpml * f->nzpml;
+  double mis = 0;
+  std::vector<float> pg(nall), sg(nall);
+  char snapdir[] = ".";
+  ELSRTM_ROT_EXP_IMAGE_SINGLESHOT(*f, 1, nDim, 1, rz.data(), rx.data(), gc.data(), false, false,
+                                  1000, iter, snapdir, ipp.data(), ips.data(), pg.data(),
+                                  sg.data(), mis);
+  if (res_vz) cudaMemcpy(res_vz, f->GPUrecord_scatter_z, nrec * sizeof(float), cudaMemcpyDeviceToHost);
+  if (res_vx) cudaMemcpy(res_vx, f->GPUrecord_scatter_x, nrec * sizeof(float), cudaMemcpyDeviceToHost);
+  f->imagebuffer_resettozero(img7[0], img7[1], img7[2], img7[3], img7[4], img7[5], img7[6]);
+  if (misfit) *misfit = mis;
+  int rc = last_error();
+  delete f;
+  return rc;
+}
+
+// Elastic RTM with the reference's kernels in the reference driver's order (forward:
+// :4396-4400 mode 0; backward: :4769-4778 reconstruction + adjoint, :3335 + :3341 imaging).
+// rbc = 0 saves / reloads boundary strips with the reference's 2-field kernels (:3674-3731).
+// rbc = 1 takes a pre-randomised padded model (vp_pad / vs_pad, [nxpml][nzpml]) instead of the
+// reference's cuRAND generator, whose index arithmetic writes past the end of vp / vs
+// (FD2DGPU.cu:172, :177) and is therefore not run; lambda / mu are rebuilt by the reference's
+// GPUcalculate_elastic_rho_C.  img3 receives pp, ps, illumination, full size [allnx][allnz].
+// Shots run one after another on the default stream, as the reference does.
+int ref_rtm(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz, float dt,
+            const float *vp_all, const float *vs_all, const float *wavelet, int nshots,
+            const int *win_left, const int *isx, int isz, int igz, int ntr, const int *igx,
+            const float *adj_vz, const float *adj_vx, int rbc, const float *vp_pad,
+            const float *vs_pad, float *const img3[3], float *elapsed_ms) {
+  RefGeom g{allnx, allnz, nx, pml, nt, dx, dz, dt};
+  size_t nall = (size_t)allnx * allnz, nrec = (size_t)ntr * nt;
+  FD2DGPU_ELASTIC *f = make(g, wavelet, ntr);
+  std::vector<float> vp(vp_all, vp_all + nall), vs(vs_all, vs_all + nall);
+  f->GPUbufferVPVS(vp.data(), vs.data());
+  int nxpml = f->nxpml, nzpml = f->nzpml, N = f->nop, nDim = nxpml * nzpml;
+  size_t ud = (size_t)2 * N * nx * nt, lr = (size_t)2 * N * allnz * nt;
+  float *up_x = nullptr, *up_z = nullptr, *dn_x = nullptr, *dn_z = nullptr;
+  float *lf_x = nullptr, *lf_z = nullptr, *rt_x = nullptr, *rt_z = nullptr;
+  if (!rbc) {
+    cudaMalloc(&up_x, ud * 4); cudaMalloc(&up_z, ud * 4);
+    cudaMalloc(&dn_x, ud * 4); cudaMalloc(&dn_z, ud * 4);
+    cudaMalloc(&lf_x, lr * 4); cudaMalloc(&lf_z, lr * 4);
+    cudaMalloc(&rt_x, lr * 4); cudaMalloc(&rt_z, lr * 4);
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaMemset(f->pp_gradient, 0, nall * 4);
+  cudaMemset(f->ps_gradient, 0, nall * 4);
+  cudaMemset(f->allimageGPU_denominator, 0, nall * 4);
+  cudaEventRecord(e0);
+  for (int s = 0; s < nshots; s++) {
+    std::vector<int> gc = coords_from_cells(g, igx + (size_t)s * ntr, ntr);
+    cudaMemcpy(f->GPUgc, gc.data(), ntr * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(f->GPUrecord_scatter_z, adj_vz + (size_t)s * nrec, nrec * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(f->GPUrecord_scatter_x, adj_vx + (size_t)s * nrec, nrec * 4, cudaMemcpyHostToDevice);
+    f->bufferVpVsHtoD(win_left[s]);
+    f->delta_left = win_left[s];
+    f->record_left_in_v = 0;
+    f->isx = isx[s];
+    f->isz = isz;
+    f->igz = igz;
+    f->ngx_left = 0;
+    f->FD_ELASTIC_initial(nDim);
+    f->BK_ELASTIC_initial(nDim);
+    if (rbc) {
+      cudaMemcpy(f->vp, vp_pad + (size_t)s * nDim, nDim * 4, cudaMemcpyHostToDevice);
+      cudaMemcpy(f->vs, vs_pad + (size_t)s * nDim, nDim * 4, cudaMemcpyHostToDevice);
+      cudaMemset(f->d_damp, 0, nDim * 4);
+      cudaMemset(f->d_dampz, 0, nDim * 4);
+      GPUcalculate_elastic_rho_C<<<f->Grid_Block.grid, f->Grid_Block.block>>>(
+          f->d_rho, f->vp, f->vs, f->lamda, f->miu, nxpml, nzpml);
+    } else {
+      f->calculate_elastic_damp_C();
+    }
+    for (int it = 0; it < nt; ++it) {
+      f->elastic_rotation_addS_for(it, 0);
+      f->born_modeling(1, 0);
+      if (!rbc)
+        record_edge_wavefield<<<f->Grid_Block.grid, f->Grid_Block.block>>>(
+            f->vx, f->vz, up_x, up_z, dn_x, dn_z, lf_x, lf_z, rt_x, rt_z, pml, nzpml, nxpml, nx,
+            allnz, N, it);
+    }
+    for (int it = nt - 1; it >= 0; --it) {
+      if (!rbc)
+        load_edge_wavefield<<<f->Grid_Block.grid, f->Grid_Block.block>>>(
+            f->vx, f->vz, up_x, up_z, dn_x, dn_z, lf_x, lf_z, rt_x, rt_z, pml, nzpml, nxpml, nx,
+            allnz, N, it);
+      f->calculateTxz(-1, true);
+      f->calculateTxxzz(-1, true);
+      f->calculateVz(-1, true);
+      f->calculateVx(-1, true);
+      f->elastic_rotation_addS_bac(it, 0, true);
+      f->calculateTxz(-1, false);
+      f->calculateTxxzz(-1, false);
+      f->calculateVz(-1, false);
+      f->calculateVx(-1, false);
+      doimage_gradient<<<f->imagesize.grid, f->imagesize.block>>>(
+          f->pp_gradient, f->ps_gradient, f->vx_gx, f->vz_gz, f->vx_gz, f->vz_gx, f->txx_bk,
+          f->tzz_bk, f->txz_bk, f->vp, f->vs, f->d_rho, f->nx, f->nz, f->delta_left,
+          f->record_left_in_v, pml, nzpml);
+      doimage_illum<<<f->imagesize.grid, f->imagesize.block>>>(
+          f->allimageGPU_denominator, f->vx, f->vz, f->nx, f->nz, f->delta_left,
+          f->record_left_in_v, pml, nzpml);
+    }
+  }
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  if (elapsed_ms) *elapsed_ms = ms;
+  if (img3) {
+    if (img3[0]) cudaMemcpy(img3[0], f->pp_gradient, nall * 4, cudaMemcpyDeviceToHost);
+    if (img3[1]) cudaMemcpy(img3[1], f->ps_gradient, nall * 4, cudaMemcpyDeviceToHost);
+    if (img3[2]) cudaMemcpy(img3[2], f->allimageGPU_denominator, nall * 4, cudaMemcpyDeviceToHost);
+  }
+  if (!rbc) {
+    cudaFree(up_x); cudaFree(up_z); cudaFree(dn_x); cudaFree(dn_z);
+    cudaFree(lf_x); cudaFree(lf_z); cudaFree(rt_x); cudaFree(rt_z);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int rc = last_error();
+  delete f;
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,173 @@
+"""Parity of the sm_100a path (through the C ABI) with the reference's CUDA build (golden fixtures
+and, when oracle/_ref is present, live runs) and with the FP64 CPU oracle."""
+import numpy as np
+import pytest
+
+from ds2d_b200 import Elastic2D, synth
+from oracle import pyoracle as po
+from tests.helpers import case_of, gate, load, rel, shots_of, small_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(c, shots, **kw):
+    return Elastic2D(c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                     max_shots=kw.pop("max_shots", len(shots)), max_ntr=max(s.ntr for s in shots), **kw)
+
+
+def _need(name):
+    fx = load(name)
+    if fx is None:
+        pytest.fail(f"golden fixture {name} missing")
+    return fx
+
+
+def test_forward_vs_golden(cuda_device):
+    fx = _need("forward_pml.npz")
+    c = case_of(fx)
+    shots = shots_of(fx)
+    with _ctx(c, shots) as e:
+        e.set_models(fx["vp"], fx["vs"])
+        e.set_wavelet(fx["wavelet"])
+        rz, rx = e.forward(shots)
+    ntr = shots[0].ntr
+    for i in range(len(shots)):
+        assert rel(rz[i * ntr:(i + 1) * ntr], fx["rec_vz"][i]) < gate()
+        assert rel(rx[i * ntr:(i + 1) * ntr], fx["rec_vx"][i]) < gate()
+
+
+def test_forward_batch_vs_oracle_f64(cuda_device):
+    c, vp, vs, w, shots = small_case()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    rho = synth.gardner(vp)
+    with _ctx(c, shots) as e:
+        e.set_models(vp, vs, rho)
+        e.set_wavelet(w)
+        rz, rx = e.forward(shots)
+        assert e.last_cell_updates == len(shots) * (c["nx"] + 2 * c["pml"]) * (c["allnz"] + 2 * c["pml"]) * c["nt"]
+    ntr = shots[0].ntr
+    for i, s in enumerate(shots):
+        m = po.build_model(st, vp, vs, rho, s.win_left)
+        oz, ox = po.forward(st, m, w, s, "f64")
+        assert rel(rz[i * ntr:(i + 1) * ntr], oz) < gate()
+        assert rel(rx[i * ntr:(i + 1) * ntr], ox) < gate()
+
+
+@pytest.mark.parametrize("name", ["rtm_pml.npz", "rtm_random.npz"])
+def test_rtm_vs_golden_and_oracle(cuda_device, name):
+    fx = _need(name)
+    c = case_of(fx)
+    shots = shots_of(fx)
+    rbc = int(fx["rbc"])
+    seed = int(fx.get("seed", 0))
+    with _ctx(c, shots, boundary="random" if rbc else "pml", seed=seed) as e:
+        e.set_models(fx["vp"], fx["vs"])
+        e.set_wavelet(fx["wavelet"])
+        e.rtm(shots, fx["adj_vz"].reshape(-1, c["nt"]), fx["adj_vx"].reshape(-1, c["nt"]))
+        imgs = e.read_images()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    tot64 = np.zeros((3, c["allnx"], c["allnz"]))
+    tot32 = np.zeros((3, c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left, rbc=rbc, seed=seed, shot_id=i)
+        for tot, prec in ((tot64, "f64"), (tot32, "f32")):
+            o = po.rtm(st, m, fx["wavelet"], s, fx["adj_vz"][i], fx["adj_vx"][i], rbc, prec)
+            for k in range(3):
+                tot[k] += po.place(o[k], c["allnx"], c["allnz"], s.win_left)
+    for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
+        floor = rel(tot32[k], tot64[k])
+        assert rel(imgs[key], fx["images"][k]) < gate(floor), (key, rel(imgs[key], fx["images"][k]))
+        assert rel(imgs[key], tot64[k]) < gate(floor), (key, rel(imgs[key], tot64[k]))
+
+
+@pytest.mark.parametrize("it", [0, 1])
+def test_elsrtm_vs_golden_and_oracle(cuda_device, it):
+    fx = _need(f"elsrtm_iter{it}.npz")
+    c = case_of(fx)
+    s = shots_of(fx)[0]
+    with _ctx(c, [s]) as e:
+        e.set_models(fx["vp"], fx["vs"])
+        e.set_wavelet(fx["wavelet"])
+        e.set_image(fx["img_pp"], fx["img_ps"])
+        mis, (lz, lx, rz, rx) = e.elsrtm([s], fx["obs_vz"], fx["obs_vx"], it, want_records=True)
+        imgs = e.read_images()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left)
+    dmp = po.window_image(st, fx["img_pp"], s.win_left)
+    dms = po.window_image(st, fx["img_ps"], s.win_left)
+    args = (st, m, dmp, dms, fx["wavelet"], s, fx["obs_vz"], fx["obs_vx"], it)
+    r64 = po.elsrtm(*args, precision="f64")
+    r32 = po.elsrtm(*args, precision="f32")
+    for got, key in ((rz, "res_vz"), (rx, "res_vx")):
+        floor = rel(r32[key], r64[key])
+        assert rel(got, fx[key]) < gate(floor), (key, rel(got, fx[key]), floor)
+        assert rel(got, r64[key]) < gate(floor)
+    floor = rel(r32["lm_vz"], r64["lm_vz"])
+    assert rel(lz, r64["lm_vz"]) < gate(floor)
+    for k, key in enumerate(Elastic2D.IMAGE_NAMES):
+        full64 = po.place(r64["images"][k], c["allnx"], c["allnz"], s.win_left)
+        full32 = po.place(r32["images"][k], c["allnx"], c["allnz"], s.win_left)
+        floor = rel(full32, full64)
+        assert rel(imgs[key], fx["images"][k]) < gate(floor), (key, rel(imgs[key], fx["images"][k]), floor)
+        assert rel(imgs[key], full64) < gate(floor), (key, rel(imgs[key], full64), floor)
+    if it > 0:
+        assert mis == pytest.approx(fx["misfit"], rel=1e-4)
+
+
+def test_batched_equals_one_by_one(cuda_device):
+    c, vp, vs, w, shots = small_case(nt=200)
+    rz, rx = None, None
+    with _ctx(c, shots) as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        rz, rx = e.forward(shots)
+        e.rtm(shots, rz, rx)
+        batched = e.read_images()
+    with _ctx(c, shots, max_shots=1) as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        ntr = shots[0].ntr
+        for i, s in enumerate(shots):
+            e.rtm([s], rz[i * ntr:(i + 1) * ntr], rx[i * ntr:(i + 1) * ntr])
+        single = e.read_images()
+    for key in ("pp_grad", "ps_grad", "illumination"):
+        np.testing.assert_array_equal(batched[key], single[key])
+
+
+@pytest.mark.parametrize("strips", ["f16", "bf16"])
+def test_half_precision_strips(cuda_device, strips):
+    fx = _need("rtm_pml.npz")
+    c = case_of(fx)
+    shots = shots_of(fx)
+    out = {}
+    for prec in ("f32", strips):
+        with _ctx(c, shots, strips=prec) as e:
+            e.set_models(fx["vp"], fx["vs"])
+            e.set_wavelet(fx["wavelet"])
+            e.rtm(shots, fx["adj_vz"].reshape(-1, c["nt"]), fx["adj_vx"].reshape(-1, c["nt"]))
+            out[prec] = e.read_images()
+    tol = 2e-3 if strips == "f16" else 2e-2
+    for key in ("pp_grad", "ps_grad", "illumination"):
+        assert rel(out[strips][key], out["f32"][key]) < tol, (key, rel(out[strips][key], out["f32"][key]))
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_live_reference_rtm_random(cuda_device):
+    c, vp, vs, w, shots = small_case(nt=250)
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    m0 = po.build_model(st, vp, vs, None, shots[0].win_left)
+    obs = [po.forward(st, po.build_model(st, vp, vs, None, s.win_left), w, s) for s in shots]
+    az = np.concatenate([o[0] for o in obs]).astype(np.float32)
+    ax = np.concatenate([o[1] for o in obs]).astype(np.float32)
+    vpm, vsm = synth.smooth(vp, 2.0), synth.smooth(vs, 2.0)
+    pads = [po.build_model(st, vpm, vsm, None, s.win_left, rbc=1, seed=77, shot_id=i) for i, s in enumerate(shots)]
+    ref_imgs, _ = po.ref_rtm(c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                             vpm, vsm, w, shots, az, ax, rbc=1,
+                             vp_pad=np.stack([p[0] for p in pads]), vs_pad=np.stack([p[1] for p in pads]))
+    with _ctx(c, shots, boundary="random", seed=77) as e:
+        e.set_models(vpm, vsm)
+        e.set_wavelet(w)
+        e.rtm(shots, az, ax)
+        imgs = e.read_images()
+    for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
+        assert rel(imgs[key], ref_imgs[k]) < 2e-5, (key, rel(imgs[key], ref_imgs[k]))

@@ -1,0 +1,73 @@
+"""Pins the CPU oracle against the reference's own CUDA build: every golden fixture in
+tests/golden/ (made by tests/golden/make_golden.py on a B200) is replayed by the oracle in FP64
+and FP32 on the same inputs."""
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from tests.helpers import case_of, gate, load, rel, shots_of
+
+
+def _setup(fx):
+    c = case_of(fx)
+    return c, po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+
+
+def _need(name):
+    fx = load(name)
+    if fx is None:
+        pytest.fail(f"golden fixture {name} missing (run tests/golden/make_golden.py on a GPU)")
+    return fx
+
+
+def test_forward_golden():
+    fx = _need("forward_pml.npz")
+    c, st = _setup(fx)
+    for i, s in enumerate(shots_of(fx)):
+        m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left)
+        rz, rx = po.forward(st, m, fx["wavelet"], s, "f64")
+        assert rel(fx["rec_vz"][i], rz) < gate() and rel(fx["rec_vx"][i], rx) < gate()
+
+
+@pytest.mark.parametrize("it", [0, 1])
+def test_elsrtm_golden(it):
+    fx = _need(f"elsrtm_iter{it}.npz")
+    c, st = _setup(fx)
+    s = shots_of(fx)[0]
+    m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left)
+    dmp = po.window_image(st, fx["img_pp"], s.win_left)
+    dms = po.window_image(st, fx["img_ps"], s.win_left)
+    args = (st, m, dmp, dms, fx["wavelet"], s, fx["obs_vz"], fx["obs_vx"], it)
+    r64 = po.elsrtm(*args, precision="f64")
+    r32 = po.elsrtm(*args, precision="f32")
+    for key in ("res_vz", "res_vx"):
+        floor = rel(r32[key], r64[key])
+        assert rel(fx[key], r64[key]) < gate(floor), key
+    for k in range(7):
+        full64 = po.place(r64["images"][k], c["allnx"], c["allnz"], s.win_left)
+        full32 = po.place(r32["images"][k], c["allnx"], c["allnz"], s.win_left)
+        floor = rel(full32, full64)
+        assert rel(fx["images"][k], full64) < gate(floor), (k, rel(fx["images"][k], full64), floor)
+    if it > 0:
+        assert fx["misfit"] == pytest.approx(r64["misfit"], rel=1e-4)
+
+
+@pytest.mark.parametrize("name", ["rtm_pml.npz", "rtm_random.npz"])
+def test_rtm_golden(name):
+    fx = _need(name)
+    c, st = _setup(fx)
+    rbc = int(fx["rbc"])
+    tot64 = np.zeros((3, c["allnx"], c["allnz"]))
+    tot32 = np.zeros((3, c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots_of(fx)):
+        m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left, rbc=rbc,
+                           seed=int(fx.get("seed", 0)), shot_id=i)
+        if rbc:
+            np.testing.assert_array_equal(m[0], fx["vp_pad"][i])
+        for tot, prec in ((tot64, "f64"), (tot32, "f32")):
+            imgs = po.rtm(st, m, fx["wavelet"], s, fx["adj_vz"][i], fx["adj_vx"][i], rbc, prec)
+            for k in range(3):
+                tot[k] += po.place(imgs[k], c["allnx"], c["allnz"], s.win_left)
+    for k in range(3):
+        floor = rel(tot32[k], tot64[k])
+        assert rel(fx["images"][k], tot64[k]) < gate(floor), (k, rel(fx["images"][k], tot64[k]), floor)
