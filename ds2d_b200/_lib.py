@@ -24,7 +24,7 @@ EXPORTS = [
     "ds2d_create", "ds2d_destroy", "ds2d_last_error", "ds2d_set_stream", "ds2d_set_models",
     "ds2d_set_wavelet", "ds2d_set_image", "ds2d_forward", "ds2d_elsrtm", "ds2d_rtm",
     "ds2d_rtm_device", "ds2d_read_images", "ds2d_last_cell_updates", "ds2d_last_launches",
-    "ds2d_profile", "ds2d_profile_report",
+    "ds2d_profile", "ds2d_profile_report", "ds2d_set_option",
 ]
 
 
@@ -43,7 +43,7 @@ class Opts(ctypes.Structure):
 class Shot(ctypes.Structure):
     _fields_ = [("win_left", ctypes.c_int), ("isx", ctypes.c_int), ("isz", ctypes.c_int),
                 ("igz", ctypes.c_int), ("ntr", ctypes.c_int),
-                ("igx", ctypes.POINTER(ctypes.c_int))]
+                ("igx", ctypes.POINTER(ctypes.c_int)), ("nx", ctypes.c_int)]
 
 
 class DS2DError(RuntimeError):
@@ -84,6 +84,7 @@ def load():
         "ds2d_last_cell_updates": ([P], ctypes.c_double),
         "ds2d_last_launches": ([P], ctypes.c_longlong),
         "ds2d_profile": ([P, ctypes.c_int], ctypes.c_int),
+        "ds2d_set_option": ([P, ctypes.c_char_p, ctypes.c_longlong], ctypes.c_int),
         "ds2d_profile_report": ([P, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
     }
     for name, (args, res) in sig.items():

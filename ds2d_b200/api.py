@@ -18,13 +18,15 @@ class ShotGeom:
     """One shot in cells of the padded window (reference main.cpp:1019-1025).
 
     win_left: model column of the window's first interior column (delta_left + record_left_in_v)
-    isx, isz: source cell; igz: receiver row; igx: receiver columns (distinct).
+    isx, isz: source cell; igz: receiver row; igx: receiver columns (distinct);
+    nx: this shot's window width (0 = the context's nx).
     """
     win_left: int
     isx: int
     isz: int
     igz: int
     igx: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    nx: int = 0
 
     @property
     def ntr(self):
@@ -112,7 +114,8 @@ class Elastic2D:
             gx = np.ascontiguousarray(s.igx, dtype=np.int32)
             keep.append(gx)
             arr[i] = _lib.Shot(int(s.win_left), int(s.isx), int(s.isz), int(s.igz), len(gx),
-                               gx.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+                               gx.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                               int(getattr(s, "nx", 0)))
         return arr, keep
 
     def _rec(self, shots):
@@ -166,6 +169,10 @@ class Elastic2D:
             ptrs[i] = _fptr(out[k]) if k in out else ctypes.POINTER(ctypes.c_float)()
         self._check(self.lib.ds2d_read_images(self.h, ptrs, int(bool(reset))))
         return out
+
+    def set_option(self, key, value):
+        """Tuning knob: "fused" (0/1) or "xr" (rows per CTA of the fused kernels)."""
+        self._check(self.lib.ds2d_set_option(self.h, key.encode(), int(value)))
 
     def profile(self, enable=True):
         """Per-launch CUDA-event timing of every kernel from now on (adds small overhead)."""

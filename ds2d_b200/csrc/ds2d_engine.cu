@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/ds2d.h"
+#include "ds2d_fused.cuh"
 #include "ds2d_step.cuh"
 
 using namespace ds2d;
@@ -53,13 +54,13 @@ __device__ __forceinline__ float band_factor(unsigned long long seed, int shot, 
 }
 
 __global__ void k_setup(SetupArgs a) {
-  const Dims &d = a.d;
   const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
   const int iz = blockIdx.x * blockDim.x + threadIdx.x;
   const int ix = blockIdx.y;
   if (iz >= d.ld) return;
   const long long k = d.slot * s + (long long)ix * d.ld + iz;
-  if (iz >= d.nzp) {
+  if (iz >= d.nzp || ix >= d.nxp) {  // row padding, or beyond this slot's (narrower) window
     a.b[k] = 0.f; a.lam[k] = 0.f; a.mu[k] = 0.f;
     if (a.dampx) { a.dampx[k] = 0.f; a.dampz[k] = 0.f; }
     a.kpp[k] = 0.f; a.kps[k] = 0.f;
@@ -177,6 +178,12 @@ struct ds2d_ctx {
   float *img_slot = nullptr;   // [7][B][wnx][wnz]
   double *d_mis = nullptr;
   bool have_elsrtm = false, have_rtm = false;
+  // Tuning knobs (ds2d_set_option): fused single-pass forward step, rows per CTA of the fused
+  // kernels.
+  int opt_fused = 1, opt_xr = 64;
+  Wave fw2{}, abk2{};  // ping-pong partners of fw / abk for the fused kernels
+  Wave *fw_cur = nullptr;  // buffer holding the latest forward state
+  double batch_cells = 0, batch_wcells = 0;  // padded / interior cells of the current batch
   Profiler prof;
   Arena arena;
 };
@@ -334,10 +341,14 @@ int upload_batch(ds2d_ctx *c, const ds2d_shot *shots, int n) {
   std::vector<int> rmap((size_t)n * d.nxp, -1);
   for (int s = 0; s < n; s++) {
     const ds2d_shot &sh = shots[s];
-    if (sh.win_left < 0 || sh.win_left + d.wnx > d.allnx)
+    const int wnx = sh.nx > 0 ? sh.nx : d.wnx;
+    const int nxp = wnx + 2 * d.pml;
+    if (wnx > d.wnx)
+      return fail(c, DS2D_E_ARG, "shot %d: window width %d exceeds grid.nx = %d", s, wnx, d.wnx);
+    if (sh.win_left < 0 || sh.win_left + wnx > d.allnx)
       return fail(c, DS2D_E_ARG, "shot %d: window [%d, %d) outside the model (allnx = %d)", s,
-                  sh.win_left, sh.win_left + d.wnx, d.allnx);
-    if (sh.isx < d.nop || sh.isx >= d.nxp - d.nop || sh.isz < d.nop || sh.isz >= d.nzp - d.nop)
+                  sh.win_left, sh.win_left + wnx, d.allnx);
+    if (sh.isx < d.nop || sh.isx >= nxp - d.nop || sh.isz < d.nop || sh.isz >= d.nzp - d.nop)
       return fail(c, DS2D_E_ARG, "shot %d: source cell (%d, %d) outside the updated grid", s,
                   sh.isx, sh.isz);
     if (sh.ntr < 0 || sh.ntr > d.max_ntr || (sh.ntr > 0 && !sh.igx))
@@ -346,7 +357,7 @@ int upload_batch(ds2d_ctx *c, const ds2d_shot *shots, int n) {
       return fail(c, DS2D_E_ARG, "shot %d: receiver row %d outside the interior", s, sh.igz);
     for (int t = 0; t < sh.ntr; t++) {
       int gx = sh.igx[t];
-      if (gx < d.pml || gx >= d.nxp - d.pml)
+      if (gx < d.pml || gx >= nxp - d.pml)
         return fail(c, DS2D_E_ARG, "shot %d trace %d: receiver column %d outside the interior", s,
                     t, gx);
       int &slot = rmap[(size_t)s * d.nxp + gx];
@@ -354,7 +365,13 @@ int upload_batch(ds2d_ctx *c, const ds2d_shot *shots, int n) {
         return fail(c, DS2D_E_ARG, "shot %d: receivers %d and %d share column %d", s, slot, t, gx);
       slot = t;
     }
-    sd[s] = ShotDev{sh.win_left, sh.isx, sh.isz, sh.igz, sh.ntr, 0, 0, 0};
+    sd[s] = ShotDev{sh.win_left, sh.isx, sh.isz, sh.igz, sh.ntr, nxp, wnx,
+                    4 * d.nop * (wnx + d.wnz)};
+  }
+  c->batch_cells = c->batch_wcells = 0;
+  for (const ShotDev &x : sd) {
+    c->batch_cells += (double)x.nxp * d.nzp;
+    c->batch_wcells += (double)x.wnx * d.wnz;
   }
   CK(cudaMemcpyAsync(c->d_shots, sd.data(), sizeof(ShotDev) * n, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_rmap, rmap.data(), sizeof(int) * rmap.size(), cudaMemcpyHostToDevice,
@@ -422,20 +439,54 @@ constexpr double kBytesStrRev = 56;  // + four strains written
 constexpr double kBytesVelAdj = 40;  // S (12) + lam, mu (8) + b (4) + V (8) read, V written
 constexpr double kBytesStrAdj = 32;  // V (8) + S (12) read, S (12) written
 constexpr double kBytesImage = 68;   // strains 16 + S 12 + weights 8 + V 8 read, 3 images r/w 24
-#define CELLS(n) ((double)(n) * c->d.nxp * c->d.nzp)
-#define WCELLS(n) ((double)(n) * c->d.wnx * c->d.wnz)
+constexpr double kBytesFused = 52;   // one fused elastic step: 5 fields r/w + b, lam, mu read
+// Fused backward RTM step per padded cell: source and adjoint fields r/w (2 x 40), b, lam, mu
+// (12), imaging weights (8) and three image accumulators r/w (24).
+constexpr double kBytesBwdFused = 124;
+#define CELLS(n) (c->batch_cells)
+#define WCELLS(n) (c->batch_wcells)
 #define LAUNCH(kernel, grid, block, args) LAUNCHP(#kernel, 0, kernel, grid, block, args)
 
 int strip_save(ds2d_ctx *c, const Wave &w, Strips &st, int it, int n) {
-  StripSaveArgs a{c->d, w.vx, w.vz, st, it};
+  StripSaveArgs a{c->d, c->d_shots, w.vx, w.vz, st, it};
   dim3 grid((c->d.lb + 255) / 256, 2, n);
   LAUNCH(k_strip_save, grid, 256, a);
   return DS2D_OK;
 }
 
+// Fused forward pass: one k_fwd_fused launch per step, ping-ponging fw <-> fw2.
+int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
+  const Dims &d = c->d;
+  int rc;
+  if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
+  if ((rc = zero_wave(c, c->fw2, n))) return rc;
+  const int nstrips = (d.nzp + kFTZ - 1) / kFTZ;
+  const int tz = (d.nzp + nstrips - 1) / nstrips;
+  const int xr = std::max(8, c->opt_xr);
+  dim3 grid(nstrips, (d.nxp + xr - 1) / xr, n);
+  Wave *cur = &c->fw, *nxt = &c->fw2;
+  for (int it = 0; it < d.nt; it++) {
+    FwdFusedArgs a{};
+    a.d = d; a.a = *cur; a.b = *nxt; a.p = c->par; a.shots = c->d_shots; a.wavelet = c->wavelet;
+    a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
+    if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
+    if (d.rbc)
+      LAUNCHP("fwd_fused", kBytesFused * CELLS(n), k_fwd_fused<false>, grid, kFB, a);
+    else
+      LAUNCHP("fwd_fused", kBytesFused * CELLS(n), k_fwd_fused<true>, grid, kFB, a);
+    if (strips) strip_save(c, *nxt, c->st_a, it, n);
+    std::swap(cur, nxt);
+  }
+  c->fw_cur = cur;
+  CK(cudaGetLastError());
+  return DS2D_OK;
+}
+
 // Background forward pass with optional recording and strip saving.
 int run_forward_pass(ds2d_ctx *c, int n, bool record, bool strips) {
+  if (c->opt_fused) return run_forward_fused(c, n, record, strips);
   const Dims &d = c->d;
+  c->fw_cur = &c->fw;
   dim3 grid = cell_grid(d, n), blk(kBX, kBY);
   for (int it = 0; it < d.nt; it++) {
     VelArgs v = vel_args(c, c->fw, it);
@@ -515,15 +566,47 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
   CK(cudaMemsetAsync(c->img_slot, 0, 7 * plane * sizeof(float), c->stream));
   const bool strips = !d.rbc;
   if ((rc = run_forward_pass(c, n, false, strips))) return rc;
+  if (c->opt_fused) {
+    // Both buffers of the source field start from the final forward state, so the cells the
+    // interior reconstruction never updates (PML / random band) stay frozen in both.
+    Wave *cur = c->fw_cur, *nxt = (cur == &c->fw) ? &c->fw2 : &c->fw;
+    size_t bytes = sizeof(float) * (size_t)d.slot * n;
+    const float *src[5] = {cur->vx, cur->vz, cur->txx, cur->tzz, cur->txz};
+    float *dst[5] = {nxt->vx, nxt->vz, nxt->txx, nxt->tzz, nxt->txz};
+    for (int i = 0; i < 5; i++)
+      CK(cudaMemcpyAsync(dst[i], src[i], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
+    if ((rc = zero_wave(c, c->abk2, n))) return rc;
+    Wave *acur = &c->abk, *anxt = &c->abk2;
+    const int nstrips = (d.nzp + kFTZ - 1) / kFTZ;
+    const int tz = (d.nzp + nstrips - 1) / nstrips;
+    const int xr = std::max(8, c->opt_xr);
+    dim3 fgrid(nstrips, (d.nxp + xr - 1) / xr, n);
+    for (int it = d.nt - 1; it >= 0; --it) {
+      BwdFusedArgs a{};
+      a.d = d; a.ra = *cur; a.rb = *nxt; a.aa = *acur; a.ab = *anxt; a.p = c->par;
+      a.shots = c->d_shots; a.rmap = c->d_rmap; a.res_vz = c->rec[0]; a.res_vx = c->rec[1];
+      a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
+      a.img = c->img_slot; a.img_plane = (long long)plane;
+      if (d.rbc)
+        LAUNCHP("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_fused<false>, fgrid, kFB, a);
+      else
+        LAUNCHP("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_fused<true>, fgrid, kFB, a);
+      std::swap(cur, nxt);
+      std::swap(acur, anxt);
+    }
+    CK(cudaGetLastError());
+    return reduce_images(c, n, 3);
+  }
   dim3 grid = cell_grid(d, n), blk(kBX, kBY);
   dim3 igrid((d.wnz + kBX - 1) / kBX, (d.wnx + kBY - 1) / kBY, n);
   for (int it = d.nt - 1; it >= 0; --it) {
-    StrArgs sr = str_args(c, c->fw, it);
+    StrArgs sr = str_args(c, *c->fw_cur, it);
     sr.e = c->e;
     sr.st = c->st_a;
     sr.strips_on = strips;
     LAUNCHP("str_rev", kBytesStrRev * CELLS(n), k_str<kRev>, grid, blk, sr);
-    VelArgs vr = vel_args(c, c->fw, it);
+    VelArgs vr = vel_args(c, *c->fw_cur, it);
     vr.st = c->st_a;
     vr.strips_outer = strips;
     LAUNCHP("vel_rev", kBytesVel * CELLS(n), k_vel<kRev>, grid, blk, vr);
@@ -533,9 +616,9 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     VelArgs va = vel_args(c, c->abk, it);
     LAUNCHP("vel_adj", kBytesVelAdj * CELLS(n), k_vel<kAdj>, grid, blk, va);
     ImgArgs im{};
-    im.d = d; im.p = c->par; im.e = c->e;
+    im.d = d; im.shots = c->d_shots; im.p = c->par; im.e = c->e;
     im.atxx = c->abk.txx; im.atzz = c->abk.tzz; im.atxz = c->abk.txz;
-    im.vx = c->fw.vx; im.vz = c->fw.vz;
+    im.vx = c->fw_cur->vx; im.vz = c->fw_cur->vz;
     im.img = c->img_slot; im.img_plane = (long long)plane; im.full = 0;
     LAUNCHP("image", kBytesImage * WCELLS(n), k_image, igrid, blk, im);
   }
@@ -566,7 +649,7 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
     LAUNCH(k_vel<kFwd>, grid, blk, v);
     StrArgs s = str_args(c, c->fw, it);
     LAUNCH(k_str<kFwd>, grid, blk, s);
-    BornArgs bs{d, c->fw.vx, c->fw.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
+    BornArgs bs{d, c->d_shots, c->fw.vx, c->fw.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
     LAUNCH(k_born, grid, blk, bs);
     VelArgs v1 = vel_args(c, c->b1, it);
     v1.ov_txx = c->ov_s[0]; v1.ov_tzz = c->ov_s[1]; v1.ov_txz = c->ov_s[2];
@@ -574,7 +657,7 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
     LAUNCH(k_vel<kFwd>, grid, blk, v1);
     StrArgs s1 = str_args(c, c->b1, it);
     LAUNCH(k_str<kFwd>, grid, blk, s1);
-    BornArgs bs2{d, c->b1.vx, c->b1.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
+    BornArgs bs2{d, c->d_shots, c->b1.vx, c->b1.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
     LAUNCH(k_born, grid, blk, bs2);
     VelArgs v2 = vel_args(c, c->b2, it);
     v2.ov_txx = c->ov_s[0]; v2.ov_tzz = c->ov_s[1]; v2.ov_txz = c->ov_s[2];
@@ -607,7 +690,7 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
     StrArgs sb = str_args(c, c->b1, it);
     sb.e = c->be; sb.st = c->st_b; sb.strips_on = strips;
     LAUNCH(k_str<kRev>, grid, blk, sb);
-    BornArgs bs{d, c->fw.vx, c->fw.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
+    BornArgs bs{d, c->d_shots, c->fw.vx, c->fw.vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
     LAUNCH(k_born, grid, blk, bs);
     VelArgs vb = vel_args(c, c->b1, it);
     vb.ov_txx = c->ov_s[0]; vb.ov_tzz = c->ov_s[1]; vb.ov_txz = c->ov_s[2];
@@ -620,13 +703,13 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
     LAUNCH(k_vel<kAdj>, grid, blk, va);
     VelArgs vbb = vel_args(c, c->bbk, it);
     LAUNCH(k_vel<kAdj>, grid, blk, vbb);
-    BornAdjArgs ba{d, c->abk.txx, c->abk.tzz, c->abk.txz, c->par, c->ov_v[0], c->ov_v[1]};
+    BornAdjArgs ba{d, c->d_shots, c->abk.txx, c->abk.tzz, c->abk.txz, c->par, c->ov_v[0], c->ov_v[1]};
     LAUNCH(k_born_adj, grid, blk, ba);
     StrArgs sbb = str_args(c, c->bbk, it);
     sbb.ov_vx = c->ov_v[0]; sbb.ov_vz = c->ov_v[1];
     LAUNCH(k_str<kAdj>, grid, blk, sbb);
     ImgArgs im{};
-    im.d = d; im.p = c->par; im.e = c->e; im.be = c->be;
+    im.d = d; im.shots = c->d_shots; im.p = c->par; im.e = c->e; im.be = c->be;
     im.atxx = c->abk.txx; im.atzz = c->abk.tzz; im.atxz = c->abk.txz;
     im.btxx = c->bbk.txx; im.btzz = c->bbk.tzz; im.btxz = c->bbk.txz;
     im.vx = c->fw.vx; im.vz = c->fw.vz;
@@ -694,6 +777,10 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
   d.lb = 4 * nop * (d.wnx + d.wnz);
   d.nseg = (d.lb + 31) / 32;
   d.max_ntr = std::max(opts->max_ntr, 1);
+  d.nxp_max = d.nxp;
+  d.wnx_max = d.wnx;
+  d.lb_max = d.lb;
+  d.nseg_max = d.nseg;
   c->B = opts->max_shots;
   if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
     fail(c, DS2D_E_CUDA, "cudaStreamCreate failed");
@@ -800,7 +887,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     if ((rc = copy_records_out(c, shots + f, m, c->rec[0], c->rec[1], tb, rec_vz, rec_vx))) return rc;
     CK(cudaStreamSynchronize(c->stream));
     for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
-    c->last_updates += (double)m * c->d.nxp * c->d.nzp * c->d.nt;
+    c->last_updates += c->batch_cells * c->d.nt;
   }
   return DS2D_OK;
 }
@@ -820,7 +907,7 @@ static int rtm_common(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *a
     if ((rc = copy_records_in(c, shots + f, m, az, ax, tb, c->rec[0], c->rec[1], kind))) return rc;
     if ((rc = rtm_batch(c, shots + f, m, f))) return rc;
     for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
-    c->last_updates += 3.0 * m * c->d.nxp * c->d.nzp * c->d.nt;
+    c->last_updates += 3.0 * c->batch_cells * c->d.nt;
   }
   CK(cudaStreamSynchronize(c->stream));
   return DS2D_OK;
@@ -858,7 +945,7 @@ int ds2d_elsrtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *obs_vz,
       if ((rc = copy_records_out(c, shots + f, m, c->rec[6], c->rec[7], tb, res_vz, res_vx))) return rc;
     CK(cudaStreamSynchronize(c->stream));
     for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
-    c->last_updates += 7.0 * m * c->d.nxp * c->d.nzp * c->d.nt;
+    c->last_updates += 7.0 * c->batch_cells * c->d.nt;
   }
   return DS2D_OK;
 }
@@ -871,6 +958,20 @@ int ds2d_read_images(ds2d_ctx *c, float *const images[7], int reset) {
       CK(cudaMemcpyAsync(images[a], c->images + a * n, n * 4, cudaMemcpyDeviceToHost, c->stream));
   if (reset) CK(cudaMemsetAsync(c->images, 0, 7 * n * 4, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
+  if (!c || !key) return DS2D_E_ARG;
+  std::string k(key);
+  if (k == "fused") {
+    c->opt_fused = value != 0;
+  } else if (k == "xr") {
+    if (value < 8 || value > 4096) return fail(c, DS2D_E_ARG, "xr must be in [8, 4096]");
+    c->opt_xr = (int)value;
+  } else {
+    return fail(c, DS2D_E_ARG, "unknown option '%s'", key);
+  }
   return DS2D_OK;
 }
 

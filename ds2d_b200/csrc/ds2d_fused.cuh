@@ -1,0 +1,442 @@
+// Fused single-pass elastic time step for sm_100a: one launch advances the velocities AND the
+// stresses of every resident shot by one step (reference update_vx, update_vz, update_txx_tzz,
+// update_txz, born.cu:215-349, four launches per step there).
+//
+// Shape: each CTA owns a z-strip of tz <= 112 output columns (128 threads: one thread per column
+// of the strip plus an 8-column halo on each side) and marches along x over xr output rows.  At
+// row step r it
+//   1. loads the old stresses of row r (coalesced rows of 128 floats),
+//   2. computes the new velocities of row r-4 for the strip plus a 4-column halo,
+//   3. computes the new stresses of row r-8 for the strip.
+// The 8-tap x-derivatives come from per-thread register windows of the last 9 rows; the z-taps of
+// the current row come from one shared-memory row per field.  State ping-pongs between two
+// buffers (a -> b), so neighbouring CTAs never see a half-updated halo.  DRAM traffic per cell is
+// the algorithmic 52 bytes (5 fields read + written, b, lam, mu read); halo re-reads hit L2.
+//
+// Injections keep the reference's transient semantics (see ds2d_kernels.cuh): the explosive
+// source is added to the stress values that enter the stencil windows; the one cell that carries
+// it reloads its own old state from memory for the stress update.
+#pragma once
+#include "ds2d_kernels.cuh"
+
+namespace ds2d {
+
+constexpr int kFB = 128;        // threads per CTA
+constexpr int kFTZ = kFB - 16;  // max output columns of one strip
+
+struct FwdFusedArgs {
+  Dims d;
+  Wave a, b;  // state at t-1 (read) and t (written)
+  Par p;
+  const ShotDev *shots;
+  const float *wavelet;
+  int it;
+  int tz, xr;  // output columns per strip, output rows per CTA
+  const int *rmap;
+  float *rec_vz, *rec_vx;
+  int rec_on;
+};
+
+template <int N>
+__device__ __forceinline__ void push(float (&w)[N], float v) {
+#pragma unroll
+  for (int i = 0; i < N - 1; i++) w[i] = w[i + 1];
+  w[N - 1] = v;
+}
+
+// Window of 9 rows, w[8] = newest row q0; row q sits at index 8 - (q0 - q).
+// Dx+ at row q0 - 4 (taps q+i, q-i+1) and Dx- at row q0 - 4 (taps q+i-1, q-i).
+__device__ __forceinline__ float dxp_mid(const float (&w)[9]) {
+  return stencil4([&](int i) { return w[4 + i] - w[5 - i]; });
+}
+__device__ __forceinline__ float dxm_mid(const float (&w)[9]) {
+  return stencil4([&](int i) { return w[3 + i] - w[4 - i]; });
+}
+
+template <bool kPML>
+__global__ void __launch_bounds__(kFB) k_fwd_fused(FwdFusedArgs a) {
+  __shared__ float s_txz[kFB], s_tzz[kFB], s_vx[kFB], s_vz[kFB];
+  const int s = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int z = blockIdx.x * a.tz - 8 + t;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  const long long base = d.slot * s;
+  const int ld = d.ld;
+  const bool zin = z >= 0 && z < d.nzp;
+  const bool zupd = z >= d.nop && z < d.nzp - d.nop;
+  const bool vcol = t >= 4 && t < a.tz + 12 && zupd;
+  const bool scol = t >= 8 && t < a.tz + 8 && zupd;
+  const ShotDev sh = a.shots[s];
+  const float sval = a.wavelet[a.it];
+  const bool src_col = z == sh.isz;
+  const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+  const float *Atxx = a.a.txx, *Atzz = a.a.tzz, *Atxz = a.a.txz;
+
+  float w_txx[9], w_tzz[9], w_txz[9], w_vx[9], w_vz[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_txx[i] = w_tzz[i] = w_txz[i] = w_vx[i] = w_vz[i] = 0.f;
+
+  float n_txx = 0.f, n_tzz = 0.f, n_txz = 0.f;
+  auto load_s = [&](int r) {
+    n_txx = n_tzz = n_txz = 0.f;
+    if (r >= 0 && r < d.nxp && zin) {
+      const long long k = base + (long long)r * ld + z;
+      n_txx = __ldg(Atxx + k);
+      n_tzz = __ldg(Atzz + k);
+      n_txz = __ldg(Atxz + k);
+      if (src_col && r == sh.isx) {  // FD2DGPU.cu:2039-2049 (transient)
+        n_txx += sval;
+        n_tzz += sval;
+      }
+    }
+  };
+  load_s(x0 - 8);
+  for (int r = x0 - 8; r < x1 + 8; r++) {
+    push(w_txx, n_txx);
+    push(w_tzz, n_tzz);
+    push(w_txz, n_txz);
+    load_s(r + 1);
+    // ---- velocities of row rv = r - 4 --------------------------------------------------
+    const int rv = r - 4;
+    s_txz[t] = w_txz[4];
+    s_tzz[t] = w_tzz[4];
+    __syncthreads();
+    float vxn = 0.f, vzn = 0.f;
+    if (vcol && r >= x0 && rv >= d.nop && rv < d.nxp - d.nop) {
+      const long long k = base + (long long)rv * ld + z;
+      const float ax = dxp_mid(w_txx);
+      const float fx = dxm_mid(w_txz);
+      const float bz = stencil4([&](int i) { return s_txz[t + i - 1] - s_txz[t - i]; });
+      const float ez = stencil4([&](int i) { return s_tzz[t + i] - s_tzz[t - i + 1]; });
+      const float bb = __ldg(a.p.b + k);
+      const float cbx = bb * dtdx, cbz = bb * dtdz;
+      const float ux_x = cbx * ax, ux_z = cbz * bz, uz_x = cbx * fx, uz_z = cbz * ez;
+      const bool own = rv >= x0 && rv < x1 && t >= 8 && t < a.tz + 8;
+      if (kPML && pml_cell(d, rv, z)) {
+        const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+        const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
+        const float vxx = __fdiv_rn(fmaf(d1, a.a.vx_x[k], ux_x), d2);
+        const float vxz = __fdiv_rn(fmaf(d3, a.a.vx_z[k], ux_z), d4);
+        const float vzx = __fdiv_rn(fmaf(d1, a.a.vz_x[k], uz_x), d2);
+        const float vzz = __fdiv_rn(fmaf(d3, a.a.vz_z[k], uz_z), d4);
+        if (own) {
+          a.b.vx_x[k] = vxx; a.b.vx_z[k] = vxz; a.b.vz_x[k] = vzx; a.b.vz_z[k] = vzz;
+        }
+        vxn = vxx + vxz;
+        vzn = vzx + vzz;
+      } else {
+        vxn = __ldg(a.a.vx + k) + (ux_x + ux_z);
+        vzn = __ldg(a.a.vz + k) + (uz_x + uz_z);
+      }
+      if (own) {
+        a.b.vx[k] = vxn;
+        a.b.vz[k] = vzn;
+        if (a.rec_on && z == sh.igz) {
+          const int tr = a.rmap[(long long)s * d.nxp_max + rv];
+          if (tr >= 0) {
+            const long long q = ((long long)s * d.max_ntr + tr) * d.nt + a.it;
+            a.rec_vz[q] = vzn;
+            a.rec_vx[q] = vxn;
+          }
+        }
+      }
+    }
+    push(w_vx, vxn);
+    push(w_vz, vzn);
+    // ---- stresses of row rs = r - 8 -----------------------------------------------------
+    const int rs = r - 8;
+    s_vx[t] = w_vx[4];
+    s_vz[t] = w_vz[4];
+    __syncthreads();
+    if (scol && rs >= x0 && rs < x1 && rs >= d.nop && rs < d.nxp - d.nop) {
+      const long long k = base + (long long)rs * ld + z;
+      const float sa = dxm_mid(w_vx);
+      const float sf = dxp_mid(w_vz);
+      const float sb = stencil4([&](int i) { return s_vz[t + i - 1] - s_vz[t - i]; });
+      const float se = stencil4([&](int i) { return s_vx[t + i] - s_vx[t - i + 1]; });
+      const float lam = __ldg(a.p.lam + k), mu = __ldg(a.p.mu + k);
+      const float l2m = lam + 2.0f * mu;
+      const float xx_x = l2m * dtdx * sa, xx_z = lam * dtdz * sb;
+      const float zz_x = lam * dtdx * sa, zz_z = l2m * dtdz * sb;
+      const float xz_x = dtdx * mu * sf, xz_z = dtdz * mu * se;
+      if (kPML && pml_cell(d, rs, z)) {
+        const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+        const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
+        const float a1 = __fdiv_rn(fmaf(d1, a.a.txx_x[k], xx_x), d2);
+        const float a2 = __fdiv_rn(fmaf(d3, a.a.txx_z[k], xx_z), d4);
+        const float b1 = __fdiv_rn(fmaf(d1, a.a.tzz_x[k], zz_x), d2);
+        const float b2 = __fdiv_rn(fmaf(d3, a.a.tzz_z[k], zz_z), d4);
+        const float c1 = __fdiv_rn(fmaf(d1, a.a.txz_x[k], xz_x), d2);
+        const float c2 = __fdiv_rn(fmaf(d3, a.a.txz_z[k], xz_z), d4);
+        a.b.txx_x[k] = a1; a.b.txx_z[k] = a2;
+        a.b.tzz_x[k] = b1; a.b.tzz_z[k] = b2;
+        a.b.txz_x[k] = c1; a.b.txz_z[k] = c2;
+        a.b.txx[k] = a1 + a2;
+        a.b.tzz[k] = b1 + b2;
+        a.b.txz[k] = c1 + c2;
+      } else {
+        float oxx = w_txx[0], ozz = w_tzz[0];
+        if (src_col && rs == sh.isx) {  // the injected cell: state without the source
+          oxx = __ldg(Atxx + k);
+          ozz = __ldg(Atzz + k);
+        }
+        a.b.txx[k] = oxx + (xx_x + xx_z);
+        a.b.tzz[k] = ozz + (zz_x + zz_z);
+        a.b.txz[k] = w_txz[0] + (xz_x + xz_z);
+      }
+    }
+    // No third barrier: the next step writes s_txz / s_tzz only after every thread has passed
+    // this step's second barrier (V stage done) and s_vx / s_vz only after its first barrier.
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused backward RTM step: interior reconstruction of the source wavefield (stress then
+// velocity, direction -1, FD2DGPU.cu:903-1082 via calculateTxz/Txxzz/Vz/Vx at :4769-4772), the
+// adjoint step (modulus-free stresses, moduli inside the velocity divergence, FD2DGPU.cu:591-895
+// via :4775-4778) with the receiver-side injection (:3306-3322), and the imaging condition
+// (doimage_gradient :3245, doimage_illum :3235) in one pass.  Same strip/row-march shape as
+// k_fwd_fused; both field sets ping-pong a -> b.  At row step r: stage 1 updates the stresses of
+// row r-4 (strip + 4-column halo) and images them, stage 2 updates the velocities of row r-8.
+// Strains never leave registers.  Strip values (PML mode) enter only the stage-1 windows; the
+// inner-band cells reload their own state, as the reference's split update recomputes them.
+struct BwdFusedArgs {
+  Dims d;
+  Wave ra, rb;   // reconstructed source field: state at t (read), t-1 (written)
+  Wave aa, ab;   // adjoint field
+  Par p;
+  const ShotDev *shots;
+  const int *rmap;
+  const float *res_vz, *res_vx;  // [slot][max_ntr][nt]
+  Strips st;
+  int strips_on;
+  int it;
+  int tz, xr;
+  float *img;        // [3][slot][wnx][wnz]: pp, ps, illumination
+  long long img_plane;
+};
+
+template <bool kPML>
+__global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
+  __shared__ float s_bvx[kFB], s_bvz[kFB], s_avx[kFB], s_avz[kFB];          // stage-1 z-taps
+  __shared__ float s_btxz[kFB], s_btzz[kFB], s_m[kFB], s_pz[kFB], s_lx[kFB];  // stage-2 z-taps
+  const int s = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int z = blockIdx.x * a.tz - 8 + t;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  const long long base = d.slot * s;
+  const int ld = d.ld, pml = d.pml;
+  const bool zin = z >= 0 && z < d.nzp;
+  const bool c1 = t >= 4 && t < a.tz + 12;  // stage-1 columns (strip + halo)
+  const bool c2 = t >= 8 && t < a.tz + 8;   // stage-2 / output columns
+  const bool z_int = z >= pml && z < d.nzp - pml;
+  const bool z_upd = z >= d.nop && z < d.nzp - d.nop;
+  const ShotDev sh = a.shots[s];
+  const bool rec_col = z == sh.igz;
+  const float *res_z = a.res_vz + (long long)s * d.max_ntr * d.nt + a.it;
+  const float *res_x = a.res_vx + (long long)s * d.max_ntr * d.nt + a.it;
+  const int *rmap = a.rmap + (long long)s * d.nxp_max;
+  const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+
+  // stage-1 inputs (velocities at t, rows r-8..r)
+  float w_bvx[9], w_bvz[9], w_avx[9], w_avz[9];
+  // stage-2 inputs (stresses at t-1 and adjoint products, rows r-12..r-4 / r-8..r-4)
+  float w_btxx[9], w_btxz[9], w_btzz[5], w_P[9], w_L[9], w_M[9], w_Pz[5], w_Lx[5];
+#pragma unroll
+  for (int i = 0; i < 9; i++)
+    w_bvx[i] = w_bvz[i] = w_avx[i] = w_avz[i] = w_btxx[i] = w_btxz[i] = w_P[i] = w_L[i] = w_M[i] = 0.f;
+#pragma unroll
+  for (int i = 0; i < 5; i++) w_btzz[i] = w_Pz[i] = w_Lx[i] = 0.f;
+
+  float n_bvx = 0.f, n_bvz = 0.f, n_avx = 0.f, n_avz = 0.f;
+  auto load_v = [&](int r) {
+    n_bvx = n_bvz = n_avx = n_avz = 0.f;
+    if (r < 0 || r >= d.nxp || !zin) return;
+    const long long k = base + (long long)r * ld + z;
+    int bo = -1;
+    if (a.strips_on) bo = band_offset(d, r, z);
+    if (bo >= 0) {
+      n_bvx = strip_get(a.st, d, s, a.it, 0, bo);
+      n_bvz = strip_get(a.st, d, s, a.it, 1, bo);
+    } else {
+      n_bvx = __ldg(a.ra.vx + k);
+      n_bvz = __ldg(a.ra.vz + k);
+    }
+    n_avx = __ldg(a.aa.vx + k);
+    n_avz = __ldg(a.aa.vz + k);
+    if (rec_col) {
+      const int tr = rmap[r];
+      if (tr >= 0) {
+        n_avz += res_z[(long long)tr * d.nt];
+        n_avx += res_x[(long long)tr * d.nt];
+      }
+    }
+  };
+  load_v(x0 - 8);
+  for (int r = x0 - 8; r < x1 + 8; r++) {
+    push(w_bvx, n_bvx);
+    push(w_bvz, n_bvz);
+    push(w_avx, n_avx);
+    push(w_avz, n_avz);
+    load_v(r + 1);
+    // ---- stage 1: stresses of row r1 = r - 4 -----------------------------------------------
+    const int r1 = r - 4;
+    s_bvx[t] = w_bvx[4];
+    s_bvz[t] = w_bvz[4];
+    s_avx[t] = w_avx[4];
+    s_avz[t] = w_avz[4];
+    __syncthreads();
+    float btxx = 0.f, btzz = 0.f, btxz = 0.f, P = 0.f, L = 0.f, M = 0.f, Pz = 0.f, Lx = 0.f;
+    if (c1 && zin && r >= x0 && r1 >= 0 && r1 < d.nxp) {
+      const long long k = base + (long long)r1 * ld + z;
+      const bool own = c2 && r1 >= x0 && r1 < x1;
+      btxx = __ldg(a.ra.txx + k);
+      btzz = __ldg(a.ra.tzz + k);
+      btxz = __ldg(a.ra.txz + k);
+      const bool x_int = r1 >= pml && r1 < d.nxp - pml;
+      float gx_vx = 0.f, gz_vz = 0.f, gz_vx = 0.f, gx_vz = 0.f;
+      const float lam = __ldg(a.p.lam + k), mu = __ldg(a.p.mu + k);
+      if (x_int && z_int) {
+        const float sa = dxm_mid(w_bvx);
+        const float sf = dxp_mid(w_bvz);
+        const float sb = stencil4([&](int i) { return s_bvz[t + i - 1] - s_bvz[t - i]; });
+        const float se = stencil4([&](int i) { return s_bvx[t + i] - s_bvx[t - i + 1]; });
+        const float l2m = lam + 2.0f * mu;
+        const float dir = -1.0f;
+        btxx = btxx + (dir * l2m * dtdx * sa + dir * lam * dtdz * sb);
+        btzz = btzz + (dir * lam * dtdx * sa + dir * l2m * dtdz * sb);
+        btxz = btxz + (dir * mu * dtdx * sf + dir * mu * dtdz * se);
+        gx_vx = sa / d.dx;
+        gz_vz = sb / d.dz;
+        gz_vx = se / d.dz;
+        gx_vz = sf / d.dx;
+        if (own) {
+          a.rb.txx[k] = btxx;
+          a.rb.tzz[k] = btzz;
+          a.rb.txz[k] = btxz;
+        }
+      }
+      // adjoint stresses (modulus-free; txx is txx_x, tzz is tzz_z)
+      float atxx = 0.f, atzz = 0.f, atxz = 0.f;
+      if (r1 >= d.nop && r1 < d.nxp - d.nop && z_upd) {
+        const float sa = dxm_mid(w_avx);
+        const float sf = dxp_mid(w_avz);
+        const float sb = stencil4([&](int i) { return s_avz[t + i - 1] - s_avz[t - i]; });
+        const float se = stencil4([&](int i) { return s_avx[t + i] - s_avx[t - i + 1]; });
+        const float xx = -dtdx * sa, zz = -dtdz * sb, xz_x = -dtdx * sf, xz_z = -dtdz * se;
+        const float oxx = __ldg(a.aa.txx + k), ozz = __ldg(a.aa.tzz + k);
+        if (kPML && pml_cell(d, r1, z)) {
+          const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+          const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
+          atxx = __fdiv_rn(fmaf(d1, oxx, xx), d2);
+          atzz = __fdiv_rn(fmaf(d3, ozz, zz), d4);
+          const float q1 = __fdiv_rn(fmaf(d1, a.aa.txz_x[k], xz_x), d2);
+          const float q2 = __fdiv_rn(fmaf(d3, a.aa.txz_z[k], xz_z), d4);
+          if (own) {
+            a.ab.txz_x[k] = q1;
+            a.ab.txz_z[k] = q2;
+          }
+          atxz = q1 + q2;
+        } else {
+          atxx = oxx + xx;
+          atzz = ozz + zz;
+          atxz = __ldg(a.aa.txz + k) + (xz_x + xz_z);
+        }
+        if (own) {
+          a.ab.txx[k] = atxx;
+          a.ab.tzz[k] = atzz;
+          a.ab.txz[k] = atxz;
+        }
+      }
+      const float l2m = lam + 2.0f * mu;
+      P = l2m * atxx;
+      L = lam * atzz;
+      M = mu * atxz;
+      Pz = l2m * atzz;
+      Lx = lam * atxx;
+      if (own && x_int && z_int) {
+        const long long o = ((long long)s * d.wnx_max + (r1 - pml)) * d.wnz + (z - pml);
+        const float kpp = __ldg(a.p.kpp + k), kps = __ldg(a.p.kps + k);
+        const float lamda_grad = (gx_vx + gz_vz) * (atxx + atzz);
+        const float miu_grad = -2.0f * (gx_vx * atzz + gz_vz * atxx) + (gz_vx + gx_vz) * atxz;
+        a.img[o] += kpp * lamda_grad;
+        a.img[a.img_plane + o] += kps * miu_grad;
+      }
+    }
+    push(w_btxx, btxx);
+    push(w_btxz, btxz);
+    push(w_btzz, btzz);
+    push(w_P, P);
+    push(w_L, L);
+    push(w_M, M);
+    push(w_Pz, Pz);
+    push(w_Lx, Lx);
+    // ---- stage 2: velocities of row r2 = r - 8 ---------------------------------------------
+    const int r2 = r - 8;
+    s_btxz[t] = w_btxz[4];
+    s_btzz[t] = w_btzz[0];
+    s_m[t] = w_M[4];
+    s_pz[t] = w_Pz[0];
+    s_lx[t] = w_Lx[0];
+    __syncthreads();
+    if (c2 && zin && r2 >= x0 && r2 < x1) {
+      const long long k = base + (long long)r2 * ld + z;
+      const bool x_int = r2 >= pml && r2 < d.nxp - pml;
+      const float bb = __ldg(a.p.b + k);
+      const float cbx = bb * dtdx, cbz = bb * dtdz;
+      if (x_int && z_int) {
+        const float ax = dxp_mid(w_btxx);
+        const float fx = dxm_mid(w_btxz);
+        const float bz = stencil4([&](int i) { return s_btxz[t + i - 1] - s_btxz[t - i]; });
+        const float ez = stencil4([&](int i) { return s_btzz[t + i] - s_btzz[t - i + 1]; });
+        float ovx = w_bvx[0], ovz = w_bvz[0];
+        if (a.strips_on && band_offset(d, r2, z) >= 0) {  // inner band: own state, not the strip
+          ovx = __ldg(a.ra.vx + k);
+          ovz = __ldg(a.ra.vz + k);
+        }
+        const float vx = ovx + (-cbx * ax + -cbz * bz);
+        const float vz = ovz + (-cbx * fx + -cbz * ez);
+        a.rb.vx[k] = vx;
+        a.rb.vz[k] = vz;
+        const long long o = ((long long)s * d.wnx_max + (r2 - pml)) * d.wnz + (z - pml);
+        a.img[2 * a.img_plane + o] += vx * vx + vz * vz;
+      }
+      if (r2 >= d.nop && r2 < d.nxp - d.nop && z_upd) {
+        const float t_xx = dxp_mid(w_P);
+        const float t_zx = dxp_mid(w_L);
+        const float s_xz = dxm_mid(w_M);
+        const float t_xz = stencil4([&](int i) { return s_m[t + i - 1] - s_m[t - i]; });
+        const float s_zz = stencil4([&](int i) { return s_pz[t + i] - s_pz[t - i + 1]; });
+        const float s_xx = stencil4([&](int i) { return s_lx[t + i] - s_lx[t - i + 1]; });
+        const float ux_x = fmaf(-cbx, t_zx, -cbx * t_xx), ux_z = -cbz * t_xz;
+        const float uz_x = -cbx * s_xz, uz_z = fmaf(-cbz, s_xx, -cbz * s_zz);
+        float vx, vz;
+        if (kPML && pml_cell(d, r2, z)) {
+          const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+          const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
+          const float vxx = __fdiv_rn(fmaf(d1, a.aa.vx_x[k], ux_x), d2);
+          const float vxz = __fdiv_rn(fmaf(d3, a.aa.vx_z[k], ux_z), d4);
+          const float vzx = __fdiv_rn(fmaf(d1, a.aa.vz_x[k], uz_x), d2);
+          const float vzz = __fdiv_rn(fmaf(d3, a.aa.vz_z[k], uz_z), d4);
+          a.ab.vx_x[k] = vxx; a.ab.vx_z[k] = vxz; a.ab.vz_x[k] = vzx; a.ab.vz_z[k] = vzz;
+          vx = vxx + vxz;
+          vz = vzx + vzz;
+        } else {
+          float ovx = w_avx[0], ovz = w_avz[0];
+          if (rec_col && rmap[r2] >= 0) {  // injected cell: state without the residual
+            ovx = __ldg(a.aa.vx + k);
+            ovz = __ldg(a.aa.vz + k);
+          }
+          vx = ovx + (ux_x + ux_z);
+          vz = ovz + (uz_x + uz_z);
+        }
+        a.ab.vx[k] = vx;
+        a.ab.vz[k] = vz;
+      }
+    }
+  }
+}
+
+}  // namespace ds2d

@@ -26,23 +26,35 @@ constexpr float kC2 = (float)(-245.0 / 3072.0);
 constexpr float kC3 = (float)(49.0 / 5120.0);
 constexpr float kC4 = (float)(-5.0 / 7168.0);
 
+// Grid of a batch.  nxp / wnx / lb / nseg describe ONE slot (kernels narrow them to the slot's
+// own window with slot_dims); the *_max fields are the allocation strides shared by all slots.
 struct Dims {
   int nxp, nzp, ld;  // padded window, leading dimension
   int pml, nop;
   int wnx, wnz;      // interior window (reference nx, nz)
   int nt;
   int allnx, allnz;
-  long long slot;    // floats per slot of one array (nxp * ld)
+  long long slot;    // floats per slot of one array (nxp_max * ld)
   float dx, dz, dt;
   int rbc;           // random boundary: no PML cells, no strips
   int lb;            // strip band cells per component per step
   int nseg;          // 32-cell scale segments per component per step
   int max_ntr;
+  int nxp_max, wnx_max, lb_max, nseg_max;  // strides
 };
 
 struct ShotDev {
-  int win_left, isx, isz, igz, ntr, pad0, pad1, pad2;
+  int win_left, isx, isz, igz, ntr, nxp, wnx, lb;
 };
+
+__host__ __device__ __forceinline__ Dims slot_dims(const Dims &d, const ShotDev &sh) {
+  Dims r = d;
+  r.nxp = sh.nxp;
+  r.wnx = sh.wnx;
+  r.lb = sh.lb;
+  r.nseg = (sh.lb + 31) / 32;
+  return r;
+}
 
 // One wavefield set (base pointers of slot 0).  Split arrays are null without a PML.
 struct Wave {
@@ -127,9 +139,9 @@ __device__ __forceinline__ void band_cell(const Dims &d, int bo, int &ix, int &i
 __device__ __forceinline__ float strip_get(const Strips &st, const Dims &d, int s, int it,
                                            int comp, int bo) {
   long long row = ((long long)s * d.nt + it) * 2 + comp;
-  long long e = row * d.lb + bo;
+  long long e = row * d.lb_max + bo;
   if (st.prec == 0) return ((const float *)st.data)[e];
-  float sc = st.scale[row * d.nseg + (bo >> 5)];
+  float sc = st.scale[row * d.nseg_max + (bo >> 5)];
   if (st.prec == 1) return __half2float(((const __half *)st.data)[e]) * sc;
   return __bfloat162float(((const __nv_bfloat16 *)st.data)[e]) * sc;
 }

@@ -29,8 +29,8 @@ struct VelArgs {
 
 template <int MODE>
 __global__ void __launch_bounds__(kBX *kBY) k_vel(VelArgs a) {
-  const Dims &d = a.d;
   const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
   const int iz = blockIdx.x * kBX + threadIdx.x;
   const int ix = blockIdx.y * kBY + threadIdx.y;
   if (ix >= d.nxp || iz >= d.nzp) return;
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kBX *kBY) k_vel(VelArgs a) {
   a.w.vx[k] = vx;
   a.w.vz[k] = vz;
   if (a.rec_on && iz == a.shots[s].igz) {
-    const int tr = a.rmap[(long long)s * d.nxp + ix];
+    const int tr = a.rmap[(long long)s * d.nxp_max + ix];
     if (tr >= 0) {
       const long long r = ((long long)s * d.max_ntr + tr) * d.nt + a.it;
       a.rec_vz[r] = vz;
@@ -163,8 +163,8 @@ struct StrArgs {
 
 template <int MODE>
 __global__ void __launch_bounds__(kBX *kBY) k_str(StrArgs a) {
-  const Dims &d = a.d;
   const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
   const int iz = blockIdx.x * kBX + threadIdx.x;
   const int ix = blockIdx.y * kBY + threadIdx.y;
   if (ix >= d.nxp || iz >= d.nzp) return;
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(kBX *kBY) k_str(StrArgs a) {
     igz = a.shots[s].igz;
     rz = a.res_vz + (long long)s * d.max_ntr * d.nt + a.it;
     rx = a.res_vx + (long long)s * d.max_ntr * d.nt + a.it;
-    rmap = a.rmap + (long long)s * d.nxp;
+    rmap = a.rmap + (long long)s * d.nxp_max;
   }
   auto rv = [&](int comp, int qx, int qz) {
     if (MODE == kRev && near_band) {
@@ -224,7 +224,10 @@ __global__ void __launch_bounds__(kBX *kBY) k_str(StrArgs a) {
     const float l2m = lam + 2.0f * mu;
     const float xx_x = dir * l2m * dtdx * sa, xx_z = dir * lam * dtdz * sb;
     const float zz_x = dir * lam * dtdx * sa, zz_z = dir * l2m * dtdz * sb;
-    const float xz_x = dir * dtdx * mu * sf, xz_z = dir * dtdz * mu * se;
+    // operand order of update_txz (born.cu:344-345) forward, of _txz_grad (FD2DGPU.cu:1067-1068)
+    // in reconstruction
+    const float xz_x = MODE == kRev ? dir * mu * dtdx * sf : dir * dtdx * mu * sf;
+    const float xz_z = MODE == kRev ? dir * mu * dtdz * se : dir * dtdz * mu * se;
     if (pml) {
       const float a1 = __fdiv_rn(fmaf(d1, a.w.txx_x[k], xx_x), d2);
       const float a2 = __fdiv_rn(fmaf(d3, a.w.txx_z[k], xx_z), d4);
@@ -272,14 +275,15 @@ __global__ void __launch_bounds__(kBX *kBY) k_str(StrArgs a) {
 // (interior cells only; the overlays stay zero elsewhere).
 struct BornArgs {
   Dims d;
+  const ShotDev *shots;
   const float *vx, *vz;  // source-side velocities
   Par p;
   float *ov_txx, *ov_tzz, *ov_txz;
 };
 
 __global__ void __launch_bounds__(kBX *kBY) k_born(BornArgs a) {
-  const Dims &d = a.d;
   const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
   const int iz = blockIdx.x * kBX + threadIdx.x;
   const int ix = blockIdx.y * kBY + threadIdx.y;
   const int lo = d.pml;
@@ -304,14 +308,15 @@ __global__ void __launch_bounds__(kBX *kBY) k_born(BornArgs a) {
 // velocities.  The txz x-term weights both samples with the modulus at ix+i-1 (born.cu:514).
 struct BornAdjArgs {
   Dims d;
+  const ShotDev *shots;
   const float *txx, *tzz, *txz;  // adjoint stresses of the background adjoint set
   Par p;
   float *ov_vx, *ov_vz;
 };
 
 __global__ void __launch_bounds__(kBX *kBY) k_born_adj(BornAdjArgs a) {
-  const Dims &d = a.d;
   const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
   const int iz = blockIdx.x * kBX + threadIdx.x;
   const int ix = blockIdx.y * kBY + threadIdx.y;
   const int lo = d.pml;
@@ -358,14 +363,15 @@ __global__ void __launch_bounds__(kBX *kBY) k_born_adj(BornAdjArgs a) {
 // per 32-element segment; 16-bit formats store q = v / scale with scale = segment max / 2^15.
 struct StripSaveArgs {
   Dims d;
+  const ShotDev *shots;
   const float *vx, *vz;
   Strips st;
   int it;
 };
 
 __global__ void __launch_bounds__(256) k_strip_save(StripSaveArgs a) {
-  const Dims &d = a.d;
   const int s = blockIdx.z, comp = blockIdx.y;
+  const Dims d = slot_dims(a.d, a.shots[s]);
   const int bo = blockIdx.x * 256 + threadIdx.x;
   const bool valid = bo < d.lb;
   float v = 0.f;
@@ -375,7 +381,7 @@ __global__ void __launch_bounds__(256) k_strip_save(StripSaveArgs a) {
     v = (comp ? a.vz : a.vx)[d.slot * s + (long long)ix * d.ld + iz];
   }
   const long long row = ((long long)s * d.nt + a.it) * 2 + comp;
-  const long long e = row * d.lb + bo;
+  const long long e = row * d.lb_max + bo;
   if (a.st.prec == 0) {
     if (valid) ((float *)a.st.data)[e] = v;
     return;
@@ -384,7 +390,7 @@ __global__ void __launch_bounds__(256) k_strip_save(StripSaveArgs a) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
   const float sc = m > 0.f ? m * (1.0f / 32768.0f) : 1.0f;
-  if ((threadIdx.x & 31) == 0 && bo < d.lb) a.st.scale[row * d.nseg + (bo >> 5)] = sc;
+  if ((threadIdx.x & 31) == 0 && bo < d.lb) a.st.scale[row * d.nseg_max + (bo >> 5)] = sc;
   if (!valid) return;
   const float q = v / sc;
   if (a.st.prec == 1) ((__half *)a.st.data)[e] = __float2half_rn(q);
@@ -395,6 +401,7 @@ __global__ void __launch_bounds__(256) k_strip_save(StripSaveArgs a) {
 // :3235-3242 doimage_illum, accumulated per slot over the interior window [wnx][wnz].
 struct ImgArgs {
   Dims d;
+  const ShotDev *shots;
   Par p;
   Strain e, be;
   const float *atxx, *atzz, *atxz;   // adjoint stresses
@@ -418,13 +425,13 @@ __device__ __forceinline__ void image_pair(const float *e0, const float *e1, con
 }
 
 __global__ void __launch_bounds__(kBX *kBY) k_image(ImgArgs a) {
-  const Dims &d = a.d;
   const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
   const int iz = blockIdx.x * kBX + threadIdx.x;
   const int ix = blockIdx.y * kBY + threadIdx.y;
   if (ix >= d.wnx || iz >= d.wnz) return;
   const long long k = d.slot * s + (long long)(ix + d.pml) * d.ld + iz + d.pml;
-  const long long o = ((long long)s * d.wnx + ix) * d.wnz + iz;
+  const long long o = ((long long)s * d.wnx_max + ix) * d.wnz + iz;
   const float kpp = a.p.kpp[k], kps = a.p.kps[k];
   float pp, ps;
   image_pair(a.e.gx_vx, a.e.gz_vz, a.e.gz_vx, a.e.gx_vz, a.atxx, a.atzz, a.atxz, k, kpp, kps, pp, ps);
@@ -454,7 +461,8 @@ __global__ void k_image_reduce(Dims d, const float *img, long long img_plane, in
     float acc = full[a * full_plane + (long long)col * d.allnz + iz];
     for (int s = 0; s < nslots; s++) {
       const int c = col - shots[s].win_left;
-      if (c >= 0 && c < d.wnx) acc += img[a * img_plane + ((long long)s * d.wnx + c) * d.wnz + iz];
+      if (c >= 0 && c < shots[s].wnx)
+        acc += img[a * img_plane + ((long long)s * d.wnx_max + c) * d.wnz + iz];
     }
     full[a * full_plane + (long long)col * d.allnz + iz] = acc;
   }

@@ -75,6 +75,21 @@ def reflectivity(allnx, allnz, seed, density=0.05, std=0.05):
     return m
 
 
+def uneven_shots(allnx, pml, nshots, wmin, wmax, seed, sz=0, gz=2):
+    """Shots with their own aperture: width ~ U[wmin, wmax] cells, centred on the source and
+    clipped to the model, receivers on every column of the window (batched-uneven workload)."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(0, allnx - 1, nshots).round().astype(int)
+    shots = []
+    for sx in xs:
+        w = int(min(rng.integers(wmin, wmax + 1), allnx))
+        wl = int(np.clip(sx - w // 2, 0, allnx - w))
+        igx = np.arange(pml, pml + w, dtype=np.int32)
+        shots.append(ShotGeom(win_left=wl, isx=pml + int(sx - wl), isz=pml + sz, igz=pml + gz,
+                              igx=igx, nx=w))
+    return shots
+
+
 def surface_shots(allnx, nx, pml, nshots, sz=0, gz=2, receivers_every=1, first=None, last=None):
     """Shots evenly spread along the surface, each with an nx-wide window centred on the source
     (clipped to the model), receivers on every `receivers_every`-th interior column at depth gz."""

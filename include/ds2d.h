@@ -37,7 +37,8 @@ typedef struct ds2d_ctx ds2d_ctx;
  * in main.cpp:1490). */
 typedef struct {
   int allnx, allnz; /* full model */
-  int nx;           /* shot window width in cells (all shots share it, main.cpp:1421-1423) */
+  int nx;           /* largest shot window width in cells (the reference's single nx,
+                       main.cpp:1421-1423); individual shots may be narrower (ds2d_shot.nx) */
   int pml;          /* PML width, or random-band width when boundary = RANDOM */
   int nt;           /* time steps */
   float dx, dz, dt;
@@ -62,6 +63,9 @@ typedef struct {
   int igz;        /* receiver row */
   int ntr;        /* receivers of this shot (<= max_ntr) */
   const int *igx; /* ntr distinct receiver columns (padded window coordinates) */
+  int nx;         /* this shot's window width (0 = grid.nx, the maximum).  The reference
+                     requires one width for all shots and proceeds with a wrong one otherwise
+                     (main.cpp:1010-1017); here shots of a batch may differ. */
 } ds2d_shot;
 
 /* FD2DGPU_ELASTIC::FD2DGPU_ELASTIC (FD2DGPU.cu:1350). */
@@ -116,6 +120,11 @@ double ds2d_last_cell_updates(const ds2d_ctx *ctx);
 
 /* Number of kernel launches issued by the last forward / elsrtm / rtm call. */
 long long ds2d_last_launches(const ds2d_ctx *ctx);
+
+/* Tuning knobs (no counterpart in the reference, whose launch shape is fixed at 32x32 blocks,
+ * FD2DGPU.cuh:8-9): "fused" (1 = single-pass fused time step, 0 = one launch per half step)
+ * and "xr" (rows marched by one CTA of the fused kernels). */
+int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
 
 /* Profiling (no counterpart in the reference, which has only a commented-out host timer,
  * FD2DGPU.cu:3554-3583): when enabled, every launch is bracketed by CUDA events on the launch

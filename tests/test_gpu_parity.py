@@ -114,6 +114,54 @@ def test_elsrtm_vs_golden_and_oracle(cuda_device, it):
         assert mis == pytest.approx(fx["misfit"], rel=1e-4)
 
 
+@pytest.mark.parametrize("boundary", ["pml", "random"])
+@pytest.mark.parametrize("xr", [16, 64])
+def test_fused_step_matches_half_steps(cuda_device, boundary, xr):
+    c, vp, vs, w, shots = small_case(nt=300)
+    out = {}
+    for fused in (0, 1):
+        with _ctx(c, shots, boundary=boundary, seed=5) as e:
+            e.set_option("fused", fused)
+            e.set_option("xr", xr)
+            e.set_models(vp, vs)
+            e.set_wavelet(w)
+            rz, rx = e.forward(shots)
+            e.rtm(shots, rz, rx)
+            out[fused] = (rz, rx, e.read_images())
+    assert rel(out[1][0], out[0][0]) < 1e-6 and rel(out[1][1], out[0][1]) < 1e-6
+    for key in ("pp_grad", "ps_grad", "illumination"):
+        assert rel(out[1][2][key], out[0][2][key]) < 1e-6, key
+
+
+@pytest.mark.parametrize("fused", [0, 1])
+def test_uneven_windows_vs_oracle(cuda_device, fused):
+    """Shots of different aperture widths in one batch (per-slot window sizes)."""
+    c, vp, vs, w, _ = small_case(nt=200)
+    shots = synth.uneven_shots(c["allnx"], c["pml"], 4, 20, c["allnx"], seed=9)
+    wmax = max(s.nx for s in shots)
+    with Elastic2D(c["allnx"], c["allnz"], wmax, c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                   max_shots=len(shots), max_ntr=wmax) as e:
+        e.set_option("fused", fused)
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        rz, rx = e.forward(shots)
+        e.rtm(shots, rz, rx)
+        imgs = e.read_images()
+    off = 0
+    tot = np.zeros((3, c["allnx"], c["allnz"]))
+    for s in shots:
+        st = po.Setup(c["allnx"], c["allnz"], s.nx, c["pml"], c["dx"], c["dz"], c["dt"])
+        m = po.build_model(st, vp, vs, None, s.win_left)
+        oz, ox = po.forward(st, m, w, s)
+        assert rel(rz[off:off + s.ntr], oz) < gate()
+        o = po.rtm(st, m, w, s, rz[off:off + s.ntr], rx[off:off + s.ntr], 0)
+        for k in range(3):
+            tot[k] += po.place(o[k], c["allnx"], c["allnz"], s.win_left)
+        off += s.ntr
+    for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
+        assert rel(imgs[key], tot[k]) < 1e-4, (key, rel(imgs[key], tot[k]))
+
+
 def test_batched_equals_one_by_one(cuda_device):
     c, vp, vs, w, shots = small_case(nt=200)
     rz, rx = None, None
