@@ -181,6 +181,7 @@ struct ds2d_ctx {
   // Tuning knobs (ds2d_set_option): fused single-pass forward step, rows per CTA of the fused
   // kernels.
   int opt_fused = 1, opt_xr = 64;
+  int opt_adjoint_born = 0;  // scattered adjoint of ELSRTM (off = the reference's observed runs)
   Wave fw2{}, abk2{};  // ping-pong partners of fw / abk for the fused kernels
   Wave *fw_cur = nullptr;  // buffer holding the latest forward state
   double batch_cells = 0, batch_wcells = 0;  // padded / interior cells of the current batch
@@ -701,19 +702,25 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
     LAUNCH(k_str<kAdj>, grid, blk, sa);
     VelArgs va = vel_args(c, c->abk, it);
     LAUNCH(k_vel<kAdj>, grid, blk, va);
-    VelArgs vbb = vel_args(c, c->bbk, it);
-    LAUNCH(k_vel<kAdj>, grid, blk, vbb);
-    BornAdjArgs ba{d, c->d_shots, c->abk.txx, c->abk.tzz, c->abk.txz, c->par, c->ov_v[0], c->ov_v[1]};
-    LAUNCH(k_born_adj, grid, blk, ba);
-    StrArgs sbb = str_args(c, c->bbk, it);
-    sbb.ov_vx = c->ov_v[0]; sbb.ov_vz = c->ov_v[1];
-    LAUNCH(k_str<kAdj>, grid, blk, sbb);
+    if (c->opt_adjoint_born) {
+      // pure_born_reconstruct_backward(-1, backward), FD2DGPU.cu:1881-1889, as written.  In the
+      // reference's own runs add_born_source_adjoint never executes (96 registers x 1024-thread
+      // blocks exceeds the 65,536-register limit and the launch error is never checked), so
+      // the scattered adjoint stays zero; that observed behaviour is the default.
+      VelArgs vbb = vel_args(c, c->bbk, it);
+      LAUNCH(k_vel<kAdj>, grid, blk, vbb);
+      BornAdjArgs ba{d, c->d_shots, c->abk.txx, c->abk.tzz, c->abk.txz, c->par, c->ov_v[0], c->ov_v[1]};
+      LAUNCH(k_born_adj, grid, blk, ba);
+      StrArgs sbb = str_args(c, c->bbk, it);
+      sbb.ov_vx = c->ov_v[0]; sbb.ov_vz = c->ov_v[1];
+      LAUNCH(k_str<kAdj>, grid, blk, sbb);
+    }
     ImgArgs im{};
     im.d = d; im.shots = c->d_shots; im.p = c->par; im.e = c->e; im.be = c->be;
     im.atxx = c->abk.txx; im.atzz = c->abk.tzz; im.atxz = c->abk.txz;
     im.btxx = c->bbk.txx; im.btzz = c->bbk.tzz; im.btxz = c->bbk.txz;
     im.vx = c->fw.vx; im.vz = c->fw.vz;
-    im.img = c->img_slot; im.img_plane = (long long)plane; im.full = 1;
+    im.img = c->img_slot; im.img_plane = (long long)plane; im.full = c->opt_adjoint_born ? 2 : 1;
     LAUNCH(k_image, igrid, blk, im);
   }
   CK(cudaGetLastError());
@@ -945,7 +952,7 @@ int ds2d_elsrtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *obs_vz,
       if ((rc = copy_records_out(c, shots + f, m, c->rec[6], c->rec[7], tb, res_vz, res_vx))) return rc;
     CK(cudaStreamSynchronize(c->stream));
     for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
-    c->last_updates += 7.0 * c->batch_cells * c->d.nt;
+    c->last_updates += (c->opt_adjoint_born ? 7.0 : 6.0) * c->batch_cells * c->d.nt;
   }
   return DS2D_OK;
 }
@@ -966,6 +973,8 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
   std::string k(key);
   if (k == "fused") {
     c->opt_fused = value != 0;
+  } else if (k == "adjoint_born") {
+    c->opt_adjoint_born = value != 0;
   } else if (k == "xr") {
     if (value < 8 || value > 4096) return fail(c, DS2D_E_ARG, "xr must be in [8, 4096]");
     c->opt_xr = (int)value;

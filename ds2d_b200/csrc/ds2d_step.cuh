@@ -389,7 +389,9 @@ __global__ void __launch_bounds__(256) k_strip_save(StripSaveArgs a) {
   float m = fabsf(v);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  const float sc = m > 0.f ? m * (1.0f / 32768.0f) : 1.0f;
+  // Leading wavefront tails reach subnormal magnitudes, where m / 2^15 would underflow to 0;
+  // clamping the scale at FLT_MIN keeps |q| <= 2^15 inside the fp16 range.
+  const float sc = m > 0.f ? fmaxf(m * (1.0f / 32768.0f), 1.17549435e-38f) : 1.0f;
   if ((threadIdx.x & 31) == 0 && bo < d.lb) a.st.scale[row * d.nseg_max + (bo >> 5)] = sc;
   if (!valid) return;
   const float q = v / sc;
@@ -409,7 +411,7 @@ struct ImgArgs {
   const float *vx, *vz;              // reconstructed source velocities (illumination)
   float *img;                        // [7][slot][wnx][wnz]
   long long img_plane;               // slots * wnx * wnz
-  int full;                          // 1: all seven images (reference ELSRTM), 0: pp, ps, illum
+  int full;  // 0: pp, ps, illum; 1: + scattered-strain images; 2: + scattered-adjoint images
 };
 
 __device__ __forceinline__ void image_pair(const float *e0, const float *e1, const float *e2,
@@ -439,10 +441,12 @@ __global__ void __launch_bounds__(kBX *kBY) k_image(ImgArgs a) {
   a.img[a.img_plane + o] += ps;
   const float vx = a.vx[k], vz = a.vz[k];
   a.img[2 * a.img_plane + o] += vx * vx + vz * vz;
-  if (a.full) {
+  if (a.full >= 1) {
     image_pair(a.be.gx_vx, a.be.gz_vz, a.be.gz_vx, a.be.gx_vz, a.atxx, a.atzz, a.atxz, k, kpp, kps, pp, ps);
     a.img[3 * a.img_plane + o] += pp;
     a.img[4 * a.img_plane + o] += ps;
+  }
+  if (a.full >= 2) {
     image_pair(a.e.gx_vx, a.e.gz_vz, a.e.gz_vx, a.e.gx_vz, a.btxx, a.btzz, a.btxz, k, kpp, kps, pp, ps);
     a.img[5 * a.img_plane + o] += pp;
     a.img[6 * a.img_plane + o] += ps;

@@ -484,7 +484,8 @@ void ncc_residual(int ntr, int nt, const std::vector<double> &sz, const std::vec
 template <class R>
 int elsrtm_impl(const orc_grid *gg, const float *const model[7], const float *dmp,
                 const float *dms, const float *wav, int nt, const orc_shot *s,
-                const float *obs_vz, const float *obs_vx, int iter, int rbc, double *lm_vz,
+                const float *obs_vz, const float *obs_vx, int iter, int rbc, int adjoint_born,
+                   double *lm_vz,
                 double *lm_vx, double *res_vz, double *res_vx, double *const img[7],
                 double *misfit) {
   Geo<R> g(gg);
@@ -562,12 +563,17 @@ int elsrtm_impl(const orc_grid *gg, const float *const model[7], const float *dm
     k_adj_txx_tzz(g, wbk, M, -1);
     k_adj_vz(g, wbk, M, -1);
     k_adj_vx(g, wbk, M, -1);
-    // pure_born_reconstruct_backward(-1, backward), FD2DGPU.cu:1881-1889
-    k_adj_vz(g, bbk, M, -1);
-    k_adj_vx(g, bbk, M, -1);
-    k_born_source_adjoint(g, wbk, bbk, M, -1);
-    k_adj_txx_tzz(g, bbk, M, -1);
-    k_adj_txz(g, bbk, M, -1);
+    // pure_born_reconstruct_backward(-1, backward), FD2DGPU.cu:1881-1889.  On a GPU the
+    // reference's add_born_source_adjoint launch fails (96 registers x 1024 threads per block >
+    // 65,536; the error is never checked), so its runs leave the scattered adjoint at zero:
+    // adjoint_born = 0 reproduces that, 1 evaluates the term as written.
+    if (adjoint_born) {
+      k_adj_vz(g, bbk, M, -1);
+      k_adj_vx(g, bbk, M, -1);
+      k_born_source_adjoint(g, wbk, bbk, M, -1);
+      k_adj_txx_tzz(g, bbk, M, -1);
+      k_adj_txz(g, bbk, M, -1);
+    }
     // image_gradient, FD2DGPU.cu:3333-3342
     k_image(g, M, e, wbk, im[0], im[1]);
     k_image(g, M, be, wbk, im[3], im[4]);
@@ -724,19 +730,21 @@ int orc_forward_f32(const orc_grid *g, const float *const model[7], const float 
 
 int orc_elsrtm_f64(const orc_grid *g, const float *const model[7], const float *dm_p,
                    const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
-                   const float *obs_vz, const float *obs_vx, int iter, int rbc, double *lm_vz,
+                   const float *obs_vz, const float *obs_vx, int iter, int rbc, int adjoint_born,
+                   double *lm_vz,
                    double *lm_vx, double *res_vz, double *res_vx, double *const img[7],
                    double *misfit) {
   return elsrtm_impl<double>(g, model, dm_p, dm_s, wavelet, nt, s, obs_vz, obs_vx, iter, rbc,
-                             lm_vz, lm_vx, res_vz, res_vx, img, misfit);
+                             adjoint_born, lm_vz, lm_vx, res_vz, res_vx, img, misfit);
 }
 int orc_elsrtm_f32(const orc_grid *g, const float *const model[7], const float *dm_p,
                    const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
-                   const float *obs_vz, const float *obs_vx, int iter, int rbc, double *lm_vz,
+                   const float *obs_vz, const float *obs_vx, int iter, int rbc, int adjoint_born,
+                   double *lm_vz,
                    double *lm_vx, double *res_vz, double *res_vx, double *const img[7],
                    double *misfit) {
   return elsrtm_impl<float>(g, model, dm_p, dm_s, wavelet, nt, s, obs_vz, obs_vx, iter, rbc,
-                            lm_vz, lm_vx, res_vz, res_vx, img, misfit);
+                            adjoint_born, lm_vz, lm_vx, res_vz, res_vx, img, misfit);
 }
 
 int orc_rtm_f64(const orc_grid *g, const float *const model[7], const float *wavelet, int nt,

@@ -74,12 +74,14 @@ int orc_forward_f32(const orc_grid *g, const float *const model[7], const float 
  *   misfit             accumulated exactly as FD2DGPU.cu:4615-4618 (iter > 0 only) */
 int orc_elsrtm_f64(const orc_grid *g, const float *const model[7], const float *dm_p,
                    const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
-                   const float *obs_vz, const float *obs_vx, int iter, int rbc, double *lm_vz,
+                   const float *obs_vz, const float *obs_vx, int iter, int rbc, int adjoint_born,
+                   double *lm_vz,
                    double *lm_vx, double *res_vz, double *res_vx, double *const img[7],
                    double *misfit);
 int orc_elsrtm_f32(const orc_grid *g, const float *const model[7], const float *dm_p,
                    const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
-                   const float *obs_vz, const float *obs_vx, int iter, int rbc, double *lm_vz,
+                   const float *obs_vz, const float *obs_vx, int iter, int rbc, int adjoint_born,
+                   double *lm_vz,
                    double *lm_vx, double *res_vz, double *res_vx, double *const img[7],
                    double *misfit);
 

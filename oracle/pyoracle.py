@@ -53,8 +53,8 @@ def lib():
         for p in ("f64", "f32"):
             getattr(L, f"orc_forward_{p}").argtypes = [G, M, fp, ctypes.c_int, S, dp, dp]
             getattr(L, f"orc_elsrtm_{p}").argtypes = [G, M, fp, fp, fp, ctypes.c_int, S, fp, fp,
-                                                       ctypes.c_int, ctypes.c_int, dp, dp, dp, dp,
-                                                       ctypes.POINTER(dp), dp]
+                                                       ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                       dp, dp, dp, dp, ctypes.POINTER(dp), dp]
             getattr(L, f"orc_rtm_{p}").argtypes = [G, M, fp, ctypes.c_int, S, fp, fp, ctypes.c_int,
                                                     ctypes.POINTER(dp)]
         L.orc_ncc_residual.argtypes = [ctypes.c_int, ctypes.c_int, fp, fp, fp, fp, ctypes.c_int,
@@ -134,8 +134,9 @@ def forward(st, model, wavelet, shot, precision="f64"):
 
 
 def elsrtm(st, model, dm_p, dm_s, wavelet, shot, obs_vz, obs_vx, iteration, rbc=0,
-           precision="f64"):
-    """Returns dict with lm_vz, lm_vx, res_vz, res_vx, images (7 window images), misfit."""
+           precision="f64", adjoint_born=0):
+    """Returns dict with lm_vz, lm_vx, res_vz, res_vx, images (7 window images), misfit.
+    adjoint_born = 0 reproduces the reference's runs (scattered adjoint never excited)."""
     sh, keep = _shot(shot)
     mp, keep2 = _model_ptrs(model)
     w = _f(wavelet)
@@ -146,7 +147,7 @@ def elsrtm(st, model, dm_p, dm_s, wavelet, shot, obs_vz, obs_vx, iteration, rbc=
     mis = ctypes.c_double(0.0)
     getattr(lib(), f"orc_elsrtm_{precision}")(
         ctypes.byref(st.g), mp, _p(_f(dm_p)), _p(_f(dm_s)), _p(w), nt, ctypes.byref(sh),
-        _p(_f(obs_vz)), _p(_f(obs_vx)), iteration, rbc, *[_p(r, dp) for r in recs], iptr,
+        _p(_f(obs_vz)), _p(_f(obs_vx)), iteration, rbc, adjoint_born, *[_p(r, dp) for r in recs], iptr,
         ctypes.byref(mis))
     return dict(lm_vz=recs[0], lm_vx=recs[1], res_vz=recs[2], res_vx=recs[3], images=imgs,
                 misfit=mis.value)

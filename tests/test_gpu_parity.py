@@ -114,6 +114,34 @@ def test_elsrtm_vs_golden_and_oracle(cuda_device, it):
         assert mis == pytest.approx(fx["misfit"], rel=1e-4)
 
 
+def test_elsrtm_adjoint_born_as_written(cuda_device):
+    """The scattered-adjoint term the reference's runs never execute (its launch exceeds the
+    register limit), evaluated as written, against the FP64 oracle doing the same."""
+    fx = _need("elsrtm_iter1.npz")
+    c = case_of(fx)
+    s = shots_of(fx)[0]
+    with _ctx(c, [s]) as e:
+        e.set_option("adjoint_born", 1)
+        e.set_models(fx["vp"], fx["vs"])
+        e.set_wavelet(fx["wavelet"])
+        e.set_image(fx["img_pp"], fx["img_ps"])
+        e.elsrtm([s], fx["obs_vz"], fx["obs_vx"], 1)
+        imgs = e.read_images()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left)
+    dmp = po.window_image(st, fx["img_pp"], s.win_left)
+    dms = po.window_image(st, fx["img_ps"], s.win_left)
+    args = (st, m, dmp, dms, fx["wavelet"], s, fx["obs_vz"], fx["obs_vx"], 1)
+    r64 = po.elsrtm(*args, precision="f64", adjoint_born=1)
+    r32 = po.elsrtm(*args, precision="f32", adjoint_born=1)
+    for k in (5, 6):
+        key = Elastic2D.IMAGE_NAMES[k]
+        full64 = po.place(r64["images"][k], c["allnx"], c["allnz"], s.win_left)
+        full32 = po.place(r32["images"][k], c["allnx"], c["allnz"], s.win_left)
+        assert np.abs(full64).max() > 0
+        assert rel(imgs[key], full64) < gate(rel(full32, full64)), key
+
+
 @pytest.mark.parametrize("boundary", ["pml", "random"])
 @pytest.mark.parametrize("xr", [16, 64])
 def test_fused_step_matches_half_steps(cuda_device, boundary, xr):
