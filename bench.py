@@ -158,7 +158,10 @@ def run_ours(args, rank, world, dist):
                   boundary="random", max_shots=c["shots"], max_ntr=ntr, seed=c["seed"], device=dev)
     e.set_models(vpm, vsm)
     e.set_wavelet(w)
-    stream = torch.cuda.current_stream()
+    # A non-default stream: the library captures each batch (time loops included) into a CUDA
+    # graph, which the legacy default stream does not allow.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     e.set_stream(stream.cuda_stream)
     d_z = torch.from_numpy(obs_z).to(dev)
     d_x = torch.from_numpy(obs_x).to(dev)

@@ -1,0 +1,216 @@
+// Acoustic Born operator pair for CG-LSRTM on sm_100a.
+//
+// The acoustic scheme is the reference's elastic one with mu = 0 (txx = tzz = s, txz = 0;
+// born.cu:215-349 with miu = 0) and its Born source is add_born_source with mu = 0
+// (born.cu:394-400): e = -2 lam m (Dx- vx / dx + Dz- vz / dz) on the interior, applied as a
+// transient read overlay of the scattered stress.  L m records the scattered vz, vx after every
+// step; L^T is its exact discrete transpose (no reference counterpart: the reference's adjoint is
+// not the transpose of its Born modelling and its CG helpers, main.cpp:1224-1320, are unused).
+// The boundary is the random band without damping, so the background field is rebuilt by exact
+// time reversal of the whole grid (source included) instead of saved strips.
+#pragma once
+#include "ds2d_kernels.cuh"
+
+namespace ds2d {
+
+struct AcArgs {
+  Dims d;
+  const ShotDev *shots;
+  Par p;
+  float *vx, *vz, *s;      // state updated in place
+  const float *e;          // additive stress overlay (Born source) or null
+  const float *wavelet;
+  int it;
+  int src_on;              // explosive source overlay on s
+  float dir;               // +1 forward, -1 exact reversal
+  const int *rmap;
+  float *rec_vz, *rec_vx;  // [slot][max_ntr][nt]
+  int rec_on;
+};
+
+__device__ __forceinline__ bool in_upd(const Dims &d, int ix, int iz) {
+  return ix >= d.nop && ix < d.nxp - d.nop && iz >= d.nop && iz < d.nzp - d.nop;
+}
+__device__ __forceinline__ bool in_int(const Dims &d, int ix, int iz) {
+  return ix >= d.pml && ix < d.nxp - d.pml && iz >= d.pml && iz < d.nzp - d.pml;
+}
+
+// v += dir * b dt/d * D+(s + e + source)
+__global__ void __launch_bounds__(256) k_ac_vel(AcArgs a) {
+  const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y;
+  if (ix >= d.nxp || iz >= d.nzp || !in_upd(d, ix, iz)) return;
+  const int ld = d.ld;
+  const long long base = d.slot * s, k = base + (long long)ix * ld + iz;
+  long long ksrc = -1;
+  float sval = 0.f;
+  if (a.src_on) {
+    const ShotDev sh = a.shots[s];
+    ksrc = base + (long long)sh.isx * ld + sh.isz;
+    sval = a.wavelet[a.it];
+  }
+  const float *S = a.s, *E = a.e;
+  auto rd = [&](long long q) {
+    float v = __ldg(S + q);
+    if (E) v += __ldg(E + q);
+    if (q == ksrc) v += sval;
+    return v;
+  };
+  const float ax = stencil4([&](int i) { return rd(k + (long long)i * ld) - rd(k + (long long)(1 - i) * ld); });
+  const float az = stencil4([&](int i) { return rd(k + i) - rd(k - i + 1); });
+  const float bb = a.p.b[k];
+  const float vx = a.vx[k] + a.dir * (bb * (d.dt / d.dx)) * ax;
+  const float vz = a.vz[k] + a.dir * (bb * (d.dt / d.dz)) * az;
+  a.vx[k] = vx;
+  a.vz[k] = vz;
+  if (a.rec_on && iz == a.shots[s].igz) {
+    const int tr = a.rmap[(long long)s * d.nxp_max + ix];
+    if (tr >= 0) {
+      const long long r = ((long long)s * d.max_ntr + tr) * d.nt + a.it;
+      a.rec_vz[r] = vz;
+      a.rec_vx[r] = vx;
+    }
+  }
+}
+
+// s += dir * lam (dt/dx Dx- vx + dt/dz Dz- vz)
+__global__ void __launch_bounds__(256) k_ac_str(AcArgs a) {
+  const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y;
+  if (ix >= d.nxp || iz >= d.nzp || !in_upd(d, ix, iz)) return;
+  const int ld = d.ld;
+  const long long k = d.slot * s + (long long)ix * ld + iz;
+  const float *VX = a.vx, *VZ = a.vz;
+  const float sx = stencil4([&](int i) { return __ldg(VX + k + (long long)(i - 1) * ld) - __ldg(VX + k - (long long)i * ld); });
+  const float sz = stencil4([&](int i) { return __ldg(VZ + k + i - 1) - __ldg(VZ + k - i); });
+  a.s[k] = a.s[k] + a.dir * a.p.lam[k] * ((d.dt / d.dx) * sx + (d.dt / d.dz) * sz);
+}
+
+// e = -2 lam m (Dx- vx / dx + Dz- vz / dz) on the interior (m = the windowed model in p.dmp).
+__global__ void __launch_bounds__(256) k_ac_born(Dims d0, const ShotDev *shots, Par p,
+                                                 const float *vx, const float *vz, float *e) {
+  const int s = blockIdx.z;
+  const Dims d = slot_dims(d0, shots[s]);
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y;
+  if (ix >= d.nxp || iz >= d.nzp || !in_int(d, ix, iz)) return;
+  const int ld = d.ld;
+  const long long k = d.slot * s + (long long)ix * ld + iz;
+  const float sx = stencil4([&](int i) { return __ldg(vx + k + (long long)(i - 1) * ld) - __ldg(vx + k - (long long)i * ld); });
+  const float sz = stencil4([&](int i) { return __ldg(vz + k + i - 1) - __ldg(vz + k - i); });
+  e[k] = -2.0f * p.lam[k] * p.dmp[k] * (sx / d.dx + sz / d.dz);
+}
+
+// Adjoint, part 1 (transpose of the stress stage) with the transpose of the recording:
+// y_v += r (receivers), yx -= dt/dx Dx+(lam ys), yz -= dt/dz Dz+(lam ys).
+struct AcAdjArgs {
+  Dims d;
+  const ShotDev *shots;
+  Par p;
+  float *yx, *yz, *ys;
+  const int *rmap;
+  const float *res_vz, *res_vx;  // [slot][max_ntr][nt]
+  int it;
+  const float *bvx, *bvz;        // background velocities at this step (gradient)
+  float *grad;                   // [slot][wnx][wnz] (wnx_max stride)
+};
+
+__global__ void __launch_bounds__(256) k_ac_adj_v(AcAdjArgs a) {
+  const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y;
+  if (ix >= d.nxp || iz >= d.nzp || !in_upd(d, ix, iz)) return;
+  const int ld = d.ld;
+  const long long k = d.slot * s + (long long)ix * ld + iz;
+  const float *lam = a.p.lam, *ys = a.ys;
+  auto w = [&](long long q) { return __ldg(lam + q) * __ldg(ys + q); };
+  const float tx = stencil4([&](int i) { return w(k + (long long)i * ld) - w(k + (long long)(1 - i) * ld); });
+  const float tz = stencil4([&](int i) { return w(k + i) - w(k - i + 1); });
+  float yx = a.yx[k], yz = a.yz[k];
+  if (iz == a.shots[s].igz) {
+    const int tr = a.rmap[(long long)s * d.nxp_max + ix];
+    if (tr >= 0) {
+      const long long r = ((long long)s * d.max_ntr + tr) * d.nt + a.it;
+      yz += a.res_vz[r];
+      yx += a.res_vx[r];
+    }
+  }
+  a.yx[k] = yx - (d.dt / d.dx) * tx;
+  a.yz[k] = yz - (d.dt / d.dz) * tz;
+}
+
+// Adjoint, part 2 (transpose of the velocity stage): gs = -Dx-(b dt/dx yx) - Dz-(b dt/dz yz),
+// ys += gs, and the transpose of the Born source: grad += -2 lam (Dx- vx/dx + Dz- vz/dz) gs.
+__global__ void __launch_bounds__(256) k_ac_adj_s(AcAdjArgs a) {
+  const int s = blockIdx.z;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y;
+  if (ix >= d.nxp || iz >= d.nzp || !in_upd(d, ix, iz)) return;
+  const int ld = d.ld;
+  const long long k = d.slot * s + (long long)ix * ld + iz;
+  const float *b = a.p.b, *yx = a.yx, *yz = a.yz;
+  const float cx = d.dt / d.dx, cz = d.dt / d.dz;
+  auto ux = [&](long long q) { return __ldg(b + q) * cx * __ldg(yx + q); };
+  auto uz = [&](long long q) { return __ldg(b + q) * cz * __ldg(yz + q); };
+  const float gx = stencil4([&](int i) { return ux(k + (long long)(i - 1) * ld) - ux(k - (long long)i * ld); });
+  const float gz = stencil4([&](int i) { return uz(k + i - 1) - uz(k - i); });
+  const float gs = -gx - gz;
+  a.ys[k] = a.ys[k] + gs;
+  if (in_int(d, ix, iz)) {
+    const float *VX = a.bvx, *VZ = a.bvz;
+    const float sx = stencil4([&](int i) { return __ldg(VX + k + (long long)(i - 1) * ld) - __ldg(VX + k - (long long)i * ld); });
+    const float sz = stencil4([&](int i) { return __ldg(VZ + k + i - 1) - __ldg(VZ + k - i); });
+    const long long o = ((long long)s * d.wnx_max + (ix - d.pml)) * d.wnz + (iz - d.pml);
+    a.grad[o] += -2.0f * a.p.lam[k] * (sx / d.dx + sz / d.dz) * gs;
+  }
+}
+
+// FP64 inner product <a, b> over n floats: per-block partial sums (scratch), then one block adds
+// the partials in a fixed order (deterministic).  Warp shuffles for the in-block reduction.
+constexpr int kDotBlocks = 592;  // 4 x 148 SMs
+constexpr int kDotThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(kDotThreads) k_dot_partial(const float *a, const float *b,
+                                                             long long n, double *partial) {
+  __shared__ double sh[kDotThreads / 32];
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * kDotThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kDotThreads)
+    acc = fma((double)a[i], (double)b[i], acc);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < kDotThreads / 32 ? sh[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+  }
+}
+
+__global__ void __launch_bounds__(32) k_dot_final(const double *partial, int np, double *out) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < np; i += 32) v += partial[i];
+  v = warp_sum(v);
+  if (threadIdx.x == 0) *out = v;
+}
+
+// y = alpha * x + y and y = x + beta * y on float vectors with FP64 scalars (CG updates).
+__global__ void k_axpy(long long n, double alpha, const float *x, float *y) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = (float)((double)y[i] + alpha * (double)x[i]);
+}
+__global__ void k_xpby(long long n, const float *x, double beta, float *y) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = (float)((double)x[i] + beta * (double)y[i]);
+}
+
+}  // namespace ds2d

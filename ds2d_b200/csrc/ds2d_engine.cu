@@ -182,9 +182,18 @@ struct ds2d_ctx {
   // kernels.
   int opt_fused = 1, opt_xr = 64;
   int opt_adjoint_born = 0;  // scattered adjoint of ELSRTM (off = the reference's observed runs)
+  int opt_ring = 1;          // cp.async ring-fed fused kernels
   Wave fw2{}, abk2{};  // ping-pong partners of fw / abk for the fused kernels
   Wave *fw_cur = nullptr;  // buffer holding the latest forward state
   double batch_cells = 0, batch_wcells = 0;  // padded / interior cells of the current batch
+  // CUDA graphs of whole batches (time loops included), keyed by everything baked into them.
+  int opt_graph = 1;
+  struct GraphEntry {
+    long long key[6];
+    cudaGraphExec_t exec;
+    long long launches;
+  };
+  std::vector<GraphEntry> graphs;
   Profiler prof;
   Arena arena;
 };
@@ -447,6 +456,21 @@ constexpr double kBytesBwdFused = 124;
 #define CELLS(n) (c->batch_cells)
 #define WCELLS(n) (c->batch_wcells)
 #define LAUNCH(kernel, grid, block, args) LAUNCHP(#kernel, 0, kernel, grid, block, args)
+// Same with dynamic shared memory.
+#define LAUNCHS(pname, pbytes, kernel, grid, block, smem, args)                 \
+  do {                                                                          \
+    int ev_ = -1;                                                               \
+    if (c->prof.on) {                                                           \
+      ev_ = c->prof.take();                                                     \
+      cudaEventRecord(c->prof.pool[ev_], c->stream);                            \
+    }                                                                           \
+    kernel<<<grid, block, smem, c->stream>>>(args);                             \
+    c->last_launches++;                                                         \
+    if (ev_ >= 0) {                                                             \
+      cudaEventRecord(c->prof.pool[ev_ + 1], c->stream);                        \
+      c->prof.recs.push_back(ProfRec{pname, ev_, (double)(pbytes)});           \
+    }                                                                           \
+  } while (0)
 
 int strip_save(ds2d_ctx *c, const Wave &w, Strips &st, int it, int n) {
   StripSaveArgs a{c->d, c->d_shots, w.vx, w.vz, st, it};
@@ -471,10 +495,17 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
     a.d = d; a.a = *cur; a.b = *nxt; a.p = c->par; a.shots = c->d_shots; a.wavelet = c->wavelet;
     a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
     if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
-    if (d.rbc)
+    if (c->opt_ring) {
+      const size_t sm = sizeof(float) * kRing * kFwdRingFields * kFB;
+      if (d.rbc)
+        LAUNCHS("fwd_fused", kBytesFused * CELLS(n), k_fwd_ring<false>, grid, kFB, sm, a);
+      else
+        LAUNCHS("fwd_fused", kBytesFused * CELLS(n), k_fwd_ring<true>, grid, kFB, sm, a);
+    } else if (d.rbc) {
       LAUNCHP("fwd_fused", kBytesFused * CELLS(n), k_fwd_fused<false>, grid, kFB, a);
-    else
+    } else {
       LAUNCHP("fwd_fused", kBytesFused * CELLS(n), k_fwd_fused<true>, grid, kFB, a);
+    }
     if (strips) strip_save(c, *nxt, c->st_a, it, n);
     std::swap(cur, nxt);
   }
@@ -557,7 +588,52 @@ int copy_records_out(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *sz
   return DS2D_OK;
 }
 
+int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base);
+
+// Runs `body` (device work only: launches, async device copies and memsets on c->stream) as a
+// CUDA graph: captured on first use for `key`, replayed afterwards.  Direct launches when
+// graphs are off, when profiling, or on the legacy default stream (which cannot be captured).
+template <class F>
+int run_graph(ds2d_ctx *c, const long long (&key)[6], F &&body) {
+  if (!c->opt_graph || c->prof.on || c->stream == nullptr) return body();
+  for (const auto &g : c->graphs)
+    if (std::equal(key, key + 6, g.key)) {
+      CK(cudaGraphLaunch(g.exec, c->stream));
+      c->last_launches += g.launches;
+      return DS2D_OK;
+    }
+  const long long before = c->last_launches;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = body();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  CK(e);
+  ds2d_ctx::GraphEntry g{};
+  std::copy(key, key + 6, g.key);
+  const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  CK(ie);
+  g.launches = c->last_launches - before;
+  c->graphs.push_back(g);
+  CK(cudaGraphLaunch(g.exec, c->stream));
+  return DS2D_OK;
+}
+
 int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
+  int rc;
+  if (c->opt_fused) {  // allocations must precede any graph capture
+    if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
+    if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
+  }
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring, c->opt_xr, (long long)(size_t)c->stream};
+  return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
+}
+
+int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
   const Dims &d = c->d;
   int rc;
   if ((rc = setup_batch(c, n, shot_base, false))) return rc;
@@ -589,10 +665,17 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
       a.shots = c->d_shots; a.rmap = c->d_rmap; a.res_vz = c->rec[0]; a.res_vx = c->rec[1];
       a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
       a.img = c->img_slot; a.img_plane = (long long)plane;
-      if (d.rbc)
+      if (c->opt_ring) {
+        const size_t sm = sizeof(float) * kRing * kBwdRingFields * kFB;
+        if (d.rbc)
+          LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_ring<false>, fgrid, kFB, sm, a);
+        else
+          LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_ring<true>, fgrid, kFB, sm, a);
+      } else if (d.rbc) {
         LAUNCHP("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_fused<false>, fgrid, kFB, a);
-      else
+      } else {
         LAUNCHP("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_fused<true>, fgrid, kFB, a);
+      }
       std::swap(cur, nxt);
       std::swap(acur, anxt);
     }
@@ -789,6 +872,24 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
   d.lb_max = d.lb;
   d.nseg_max = d.nseg;
   c->B = opts->max_shots;
+  {
+    // Ring-fed kernels use more than the default 48 KB of dynamic shared memory.
+    const int fwd_sm = (int)(sizeof(float) * kRing * kFwdRingFields * kFB);
+    cudaError_t ea = cudaFuncSetAttribute(k_fwd_ring<true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_sm);
+    cudaError_t eb = cudaFuncSetAttribute(k_fwd_ring<false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_sm);
+    const int bwd_sm = (int)(sizeof(float) * kRing * kBwdRingFields * kFB);
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_bwd_ring<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sm);
+    if (eb == cudaSuccess)
+      eb = cudaFuncSetAttribute(k_bwd_ring<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sm);
+    if (ea != cudaSuccess || eb != cudaSuccess) {
+      g_create_err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea != cudaSuccess ? ea : eb);
+      delete c;
+      return DS2D_E_CUDA;
+    }
+  }
   if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
     fail(c, DS2D_E_CUDA, "cudaStreamCreate failed");
     delete c;
@@ -816,6 +917,9 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
 int ds2d_destroy(ds2d_ctx *c) {
   if (!c) return DS2D_OK;
   if (c->own) cudaStreamSynchronize(c->own);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
+  c->graphs.clear();
   c->arena.release();
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
@@ -885,12 +989,18 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
   for (int f = 0; f < n; f += c->B) {
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
-    if ((rc = setup_batch(c, m, f, false))) return rc;
-    if ((rc = zero_wave(c, c->fw, m))) return rc;
-    size_t nrec = (size_t)m * c->d.max_ntr * c->d.nt;
-    CK(cudaMemsetAsync(c->rec[0], 0, nrec * 4, c->stream));
-    CK(cudaMemsetAsync(c->rec[1], 0, nrec * 4, c->stream));
-    if ((rc = run_forward_pass(c, m, true, false))) return rc;
+    if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring, c->opt_xr, (long long)(size_t)c->stream};
+    rc = run_graph(c, key, [&]() {
+      int r;
+      if ((r = setup_batch(c, m, f, false))) return r;
+      if ((r = zero_wave(c, c->fw, m))) return r;
+      size_t nrec = (size_t)m * c->d.max_ntr * c->d.nt;
+      CK(cudaMemsetAsync(c->rec[0], 0, nrec * 4, c->stream));
+      CK(cudaMemsetAsync(c->rec[1], 0, nrec * 4, c->stream));
+      return run_forward_pass(c, m, true, false);
+    });
+    if (rc) return rc;
     if ((rc = copy_records_out(c, shots + f, m, c->rec[0], c->rec[1], tb, rec_vz, rec_vx))) return rc;
     CK(cudaStreamSynchronize(c->stream));
     for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
@@ -975,6 +1085,10 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     c->opt_fused = value != 0;
   } else if (k == "adjoint_born") {
     c->opt_adjoint_born = value != 0;
+  } else if (k == "graph") {
+    c->opt_graph = value != 0;
+  } else if (k == "ring") {
+    c->opt_ring = value != 0;
   } else if (k == "xr") {
     if (value < 8 || value > 4096) return fail(c, DS2D_E_ARG, "xr must be in [8, 4096]");
     c->opt_xr = (int)value;

@@ -192,6 +192,182 @@ __global__ void __launch_bounds__(kFB) k_fwd_fused(FwdFusedArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Asynchronous row prefetch for the row-marching kernels.  Every per-row operand of a thread's
+// column is copied global -> shared with cp.async (LDGSTS) kRingAhead row steps before it is
+// used.  Ring slot q (q mod kRing) holds everything row step q consumes: the stage-1 stencil
+// inputs of row q, the stage-1 own-cell operands of row q-4 and the stage-2 operands of row q-8,
+// issued together as one commit group at step q - kRingAhead.  A thread only ever reads ring
+// entries it copied itself, so cp.async.wait_group alone orders them (no barrier), and the ring
+// only needs kRingAhead + 1 slots however long the lags are.
+constexpr int kRing = 8;
+constexpr int kRingAhead = 6;
+
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Forward step fed by the ring: same arithmetic as k_fwd_fused.  Fields of ring slot q:
+// 0 txx, 1 tzz, 2 txz of row q (stencil windows); 3 vx, 4 vz, 5 b of row q-4 (velocity stage);
+// 6 lam, 7 mu of row q-8 (stress stage).
+constexpr int kFwdRingFields = 8;
+
+template <bool kPML>
+__global__ void __launch_bounds__(kFB) k_fwd_ring(FwdFusedArgs a) {
+  extern __shared__ float ring[];  // [kRing][kFwdRingFields][kFB]
+  __shared__ float s_txz[kFB], s_tzz[kFB], s_vx[kFB], s_vz[kFB];
+  const int s = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int z = blockIdx.x * a.tz - 8 + t;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  const long long base = d.slot * s;
+  const int ld = d.ld;
+  const bool zin = z >= 0 && z < d.nzp;
+  const bool zupd = z >= d.nop && z < d.nzp - d.nop;
+  const bool vcol = t >= 4 && t < a.tz + 12 && zupd;
+  const bool scol = t >= 8 && t < a.tz + 8 && zupd;
+  const ShotDev sh = a.shots[s];
+  const float sval = a.wavelet[a.it];
+  const bool src_col = z == sh.isz;
+  const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+  const float *src[kFwdRingFields] = {a.a.txx, a.a.tzz, a.a.txz, a.a.vx,
+                                      a.a.vz, a.p.b,   a.p.lam, a.p.mu};
+  // R(q, f): field f of ring slot q (row q for f < 3, row q-4 for f < 6, row q-8 otherwise)
+  auto R = [&](int q, int f) -> float & {
+    return ring[((q & (kRing - 1)) * kFwdRingFields + f) * kFB + t];
+  };
+  auto issue = [&](int q) {
+#pragma unroll
+    for (int f = 0; f < kFwdRingFields; f++) {
+      const int row = q - (f < 3 ? 0 : (f < 6 ? 4 : 8));
+      if (row >= 0 && row < d.nxp && zin)
+        cp_async4(&R(q, f), src[f] + base + (long long)row * ld + z);
+      else
+        R(q, f) = 0.f;
+    }
+    cp_async_commit();
+  };
+
+  float w_txx[9], w_tzz[9], w_txz[9], w_vx[9], w_vz[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_txx[i] = w_tzz[i] = w_txz[i] = w_vx[i] = w_vz[i] = 0.f;
+
+#pragma unroll
+  for (int j = 0; j < kRingAhead; j++) issue(x0 - 8 + j);
+  for (int r = x0 - 8; r < x1 + 8; r++) {
+    cp_async_wait<kRingAhead - 1>();  // row r has landed (this thread's copies)
+    float n_txx = R(r, 0), n_tzz = R(r, 1);
+    const float n_txz = R(r, 2);
+    if (src_col && r == sh.isx) {  // FD2DGPU.cu:2039-2049 (transient)
+      n_txx += sval;
+      n_tzz += sval;
+    }
+    push(w_txx, n_txx);
+    push(w_tzz, n_tzz);
+    push(w_txz, n_txz);
+    issue(r + kRingAhead);
+    // ---- velocities of row rv = r - 4 --------------------------------------------------
+    const int rv = r - 4;
+    s_txz[t] = w_txz[4];
+    s_tzz[t] = w_tzz[4];
+    __syncthreads();
+    float vxn = 0.f, vzn = 0.f;
+    if (vcol && r >= x0 && rv >= d.nop && rv < d.nxp - d.nop) {
+      const long long k = base + (long long)rv * ld + z;
+      const float ax = dxp_mid(w_txx);
+      const float fx = dxm_mid(w_txz);
+      const float bz = stencil4([&](int i) { return s_txz[t + i - 1] - s_txz[t - i]; });
+      const float ez = stencil4([&](int i) { return s_tzz[t + i] - s_tzz[t - i + 1]; });
+      const float bb = R(r, 5);
+      const float cbx = bb * dtdx, cbz = bb * dtdz;
+      const float ux_x = cbx * ax, ux_z = cbz * bz, uz_x = cbx * fx, uz_z = cbz * ez;
+      const bool own = rv >= x0 && rv < x1 && t >= 8 && t < a.tz + 8;
+      if (kPML && pml_cell(d, rv, z)) {
+        const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+        const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
+        const float vxx = __fdiv_rn(fmaf(d1, a.a.vx_x[k], ux_x), d2);
+        const float vxz = __fdiv_rn(fmaf(d3, a.a.vx_z[k], ux_z), d4);
+        const float vzx = __fdiv_rn(fmaf(d1, a.a.vz_x[k], uz_x), d2);
+        const float vzz = __fdiv_rn(fmaf(d3, a.a.vz_z[k], uz_z), d4);
+        if (own) {
+          a.b.vx_x[k] = vxx; a.b.vx_z[k] = vxz; a.b.vz_x[k] = vzx; a.b.vz_z[k] = vzz;
+        }
+        vxn = vxx + vxz;
+        vzn = vzx + vzz;
+      } else {
+        vxn = R(r, 3) + (ux_x + ux_z);
+        vzn = R(r, 4) + (uz_x + uz_z);
+      }
+      if (own) {
+        a.b.vx[k] = vxn;
+        a.b.vz[k] = vzn;
+        if (a.rec_on && z == sh.igz) {
+          const int tr = a.rmap[(long long)s * d.nxp_max + rv];
+          if (tr >= 0) {
+            const long long q = ((long long)s * d.max_ntr + tr) * d.nt + a.it;
+            a.rec_vz[q] = vzn;
+            a.rec_vx[q] = vxn;
+          }
+        }
+      }
+    }
+    push(w_vx, vxn);
+    push(w_vz, vzn);
+    // ---- stresses of row rs = r - 8 -----------------------------------------------------
+    const int rs = r - 8;
+    s_vx[t] = w_vx[4];
+    s_vz[t] = w_vz[4];
+    __syncthreads();
+    if (scol && rs >= x0 && rs < x1 && rs >= d.nop && rs < d.nxp - d.nop) {
+      const long long k = base + (long long)rs * ld + z;
+      const float sa = dxm_mid(w_vx);
+      const float sf = dxp_mid(w_vz);
+      const float sb = stencil4([&](int i) { return s_vz[t + i - 1] - s_vz[t - i]; });
+      const float se = stencil4([&](int i) { return s_vx[t + i] - s_vx[t - i + 1]; });
+      const float lam = R(r, 6), mu = R(r, 7);
+      const float l2m = lam + 2.0f * mu;
+      const float xx_x = l2m * dtdx * sa, xx_z = lam * dtdz * sb;
+      const float zz_x = lam * dtdx * sa, zz_z = l2m * dtdz * sb;
+      const float xz_x = dtdx * mu * sf, xz_z = dtdz * mu * se;
+      if (kPML && pml_cell(d, rs, z)) {
+        const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+        const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
+        const float a1 = __fdiv_rn(fmaf(d1, a.a.txx_x[k], xx_x), d2);
+        const float a2 = __fdiv_rn(fmaf(d3, a.a.txx_z[k], xx_z), d4);
+        const float b1 = __fdiv_rn(fmaf(d1, a.a.tzz_x[k], zz_x), d2);
+        const float b2 = __fdiv_rn(fmaf(d3, a.a.tzz_z[k], zz_z), d4);
+        const float c1 = __fdiv_rn(fmaf(d1, a.a.txz_x[k], xz_x), d2);
+        const float c2 = __fdiv_rn(fmaf(d3, a.a.txz_z[k], xz_z), d4);
+        a.b.txx_x[k] = a1; a.b.txx_z[k] = a2;
+        a.b.tzz_x[k] = b1; a.b.tzz_z[k] = b2;
+        a.b.txz_x[k] = c1; a.b.txz_z[k] = c2;
+        a.b.txx[k] = a1 + a2;
+        a.b.tzz[k] = b1 + b2;
+        a.b.txz[k] = c1 + c2;
+      } else {
+        float oxx = w_txx[0], ozz = w_tzz[0];
+        if (src_col && rs == sh.isx) {  // the injected cell: state without the source
+          oxx = __ldg(a.a.txx + k);
+          ozz = __ldg(a.a.tzz + k);
+        }
+        a.b.txx[k] = oxx + (xx_x + xx_z);
+        a.b.tzz[k] = ozz + (zz_x + zz_z);
+        a.b.txz[k] = w_txz[0] + (xz_x + xz_z);
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------------------------
 // Fused backward RTM step: interior reconstruction of the source wavefield (stress then
 // velocity, direction -1, FD2DGPU.cu:903-1082 via calculateTxz/Txxzz/Vz/Vx at :4769-4772), the
 // adjoint step (modulus-free stresses, moduli inside the velocity divergence, FD2DGPU.cu:591-895
@@ -437,6 +613,260 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
       }
     }
   }
+}
+
+// Backward RTM step fed by the ring (same arithmetic as k_bwd_fused).  Fields of ring slot q:
+//  0-3   bvx, bvz, avx, avz of row q            (stage-1 stencil windows)
+//  4-15  btxx, btzz, btxz, atxx, atzz, atxz, lam, mu, kpp, kps, img pp, img ps of row q-4
+//  16-17 b, img illumination of row q-8          (stage 2)
+constexpr int kBwdRingFields = 18;
+
+template <bool kPML>
+__global__ void __launch_bounds__(kFB) k_bwd_ring(BwdFusedArgs a) {
+  extern __shared__ float ring[];  // [kRing][kBwdRingFields][kFB]
+  __shared__ float s_bvx[kFB], s_bvz[kFB], s_avx[kFB], s_avz[kFB];
+  __shared__ float s_btxz[kFB], s_btzz[kFB], s_m[kFB], s_pz[kFB], s_lx[kFB];
+  const int s = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int z = blockIdx.x * a.tz - 8 + t;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  const long long base = d.slot * s;
+  const int ld = d.ld, pml = d.pml;
+  const bool zin = z >= 0 && z < d.nzp;
+  const bool c1 = t >= 4 && t < a.tz + 12;
+  const bool c2 = t >= 8 && t < a.tz + 8;
+  const bool z_int = z >= pml && z < d.nzp - pml;
+  const bool z_upd = z >= d.nop && z < d.nzp - d.nop;
+  const ShotDev sh = a.shots[s];
+  const bool rec_col = z == sh.igz;
+  const float *res_z = a.res_vz + (long long)s * d.max_ntr * d.nt + a.it;
+  const float *res_x = a.res_vx + (long long)s * d.max_ntr * d.nt + a.it;
+  const int *rmap = a.rmap + (long long)s * d.nxp_max;
+  const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+  const long long img_row = (long long)s * d.wnx_max;  // image row of model row r: img_row + r - pml
+  float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
+  const float *grid_src[16] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.txx, a.ra.tzz,
+                               a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz, a.p.lam,  a.p.mu,
+                               a.p.kpp,  a.p.kps,  a.p.b,    nullptr};
+  auto R = [&](int q, int f) -> float & {
+    return ring[((q & (kRing - 1)) * kBwdRingFields + f) * kFB + t];
+  };
+  auto issue = [&](int q) {
+#pragma unroll
+    for (int f = 0; f < kBwdRingFields; f++) {
+      const int lag = f < 4 ? 0 : (f < 16 ? 4 : 8);
+      const int row = q - lag;
+      const bool img = f == 14 || f == 15 || f == 17;
+      float *dst = &R(q, f);
+      if (img) {
+        if (row >= pml && row < d.nxp - pml && z_int && zin) {
+          float *src = f == 14 ? img_pp : (f == 15 ? img_ps : img_il);
+          cp_async4(dst, src + (img_row + row - pml) * d.wnz + (z - pml));
+        } else {
+          *dst = 0.f;
+        }
+      } else if (row >= 0 && row < d.nxp && zin) {
+        const float *src = grid_src[f < 14 ? f : 14];
+        cp_async4(dst, src + base + (long long)row * ld + z);
+      } else {
+        *dst = 0.f;
+      }
+    }
+    cp_async_commit();
+  };
+
+  float w_bvx[9], w_bvz[9], w_avx[9], w_avz[9];
+  float w_btxx[9], w_btxz[9], w_btzz[5], w_P[9], w_L[9], w_M[9], w_Pz[5], w_Lx[5];
+#pragma unroll
+  for (int i = 0; i < 9; i++)
+    w_bvx[i] = w_bvz[i] = w_avx[i] = w_avz[i] = w_btxx[i] = w_btxz[i] = w_P[i] = w_L[i] = w_M[i] = 0.f;
+#pragma unroll
+  for (int i = 0; i < 5; i++) w_btzz[i] = w_Pz[i] = w_Lx[i] = 0.f;
+
+#pragma unroll
+  for (int j = 0; j < kRingAhead; j++) issue(x0 - 8 + j);
+  for (int r = x0 - 8; r < x1 + 8; r++) {
+    cp_async_wait<kRingAhead - 1>();  // slot r has landed (this thread's copies)
+    {
+      float n_bvx = R(r, 0), n_bvz = R(r, 1), n_avx = R(r, 2), n_avz = R(r, 3);
+      if (r >= 0 && r < d.nxp && zin) {
+        if (a.strips_on) {
+          const int bo = band_offset(d, r, z);
+          if (bo >= 0) {
+            n_bvx = strip_get(a.st, d, s, a.it, 0, bo);
+            n_bvz = strip_get(a.st, d, s, a.it, 1, bo);
+          }
+        }
+        if (rec_col) {
+          const int tr = rmap[r];
+          if (tr >= 0) {
+            n_avz += res_z[(long long)tr * d.nt];
+            n_avx += res_x[(long long)tr * d.nt];
+          }
+        }
+      }
+      push(w_bvx, n_bvx);
+      push(w_bvz, n_bvz);
+      push(w_avx, n_avx);
+      push(w_avz, n_avz);
+    }
+    // ---- stage 1: stresses of row r1 = r - 4 -----------------------------------------------
+    const int r1 = r - 4;
+    s_bvx[t] = w_bvx[4];
+    s_bvz[t] = w_bvz[4];
+    s_avx[t] = w_avx[4];
+    s_avz[t] = w_avz[4];
+    __syncthreads();
+    float btxx = 0.f, btzz = 0.f, btxz = 0.f, P = 0.f, L = 0.f, M = 0.f, Pz = 0.f, Lx = 0.f;
+    if (c1 && zin && r >= x0 && r1 >= 0 && r1 < d.nxp) {
+      const long long k = base + (long long)r1 * ld + z;
+      const bool own = c2 && r1 >= x0 && r1 < x1;
+      btxx = R(r, 4);
+      btzz = R(r, 5);
+      btxz = R(r, 6);
+      const bool x_int = r1 >= pml && r1 < d.nxp - pml;
+      float gx_vx = 0.f, gz_vz = 0.f, gz_vx = 0.f, gx_vz = 0.f;
+      const float lam = R(r, 10), mu = R(r, 11);
+      if (x_int && z_int) {
+        const float sa = dxm_mid(w_bvx);
+        const float sf = dxp_mid(w_bvz);
+        const float sb = stencil4([&](int i) { return s_bvz[t + i - 1] - s_bvz[t - i]; });
+        const float se = stencil4([&](int i) { return s_bvx[t + i] - s_bvx[t - i + 1]; });
+        const float l2m = lam + 2.0f * mu;
+        const float dir = -1.0f;
+        btxx = btxx + (dir * l2m * dtdx * sa + dir * lam * dtdz * sb);
+        btzz = btzz + (dir * lam * dtdx * sa + dir * l2m * dtdz * sb);
+        btxz = btxz + (dir * mu * dtdx * sf + dir * mu * dtdz * se);
+        gx_vx = sa / d.dx;
+        gz_vz = sb / d.dz;
+        gz_vx = se / d.dz;
+        gx_vz = sf / d.dx;
+        if (own) {
+          a.rb.txx[k] = btxx;
+          a.rb.tzz[k] = btzz;
+          a.rb.txz[k] = btxz;
+        }
+      }
+      float atxx = 0.f, atzz = 0.f, atxz = 0.f;
+      if (r1 >= d.nop && r1 < d.nxp - d.nop && z_upd) {
+        const float sa = dxm_mid(w_avx);
+        const float sf = dxp_mid(w_avz);
+        const float sb = stencil4([&](int i) { return s_avz[t + i - 1] - s_avz[t - i]; });
+        const float se = stencil4([&](int i) { return s_avx[t + i] - s_avx[t - i + 1]; });
+        const float xx = -dtdx * sa, zz = -dtdz * sb, xz_x = -dtdx * sf, xz_z = -dtdz * se;
+        const float oxx = R(r, 7), ozz = R(r, 8);
+        if (kPML && pml_cell(d, r1, z)) {
+          const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+          const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
+          atxx = __fdiv_rn(fmaf(d1, oxx, xx), d2);
+          atzz = __fdiv_rn(fmaf(d3, ozz, zz), d4);
+          const float q1 = __fdiv_rn(fmaf(d1, a.aa.txz_x[k], xz_x), d2);
+          const float q2 = __fdiv_rn(fmaf(d3, a.aa.txz_z[k], xz_z), d4);
+          if (own) {
+            a.ab.txz_x[k] = q1;
+            a.ab.txz_z[k] = q2;
+          }
+          atxz = q1 + q2;
+        } else {
+          atxx = oxx + xx;
+          atzz = ozz + zz;
+          atxz = R(r, 9) + (xz_x + xz_z);
+        }
+        if (own) {
+          a.ab.txx[k] = atxx;
+          a.ab.tzz[k] = atzz;
+          a.ab.txz[k] = atxz;
+        }
+      }
+      const float l2m = lam + 2.0f * mu;
+      P = l2m * atxx;
+      L = lam * atzz;
+      M = mu * atxz;
+      Pz = l2m * atzz;
+      Lx = lam * atxx;
+      if (own && x_int && z_int) {
+        const long long o = (img_row + (r1 - pml)) * d.wnz + (z - pml);
+        const float kpp = R(r, 12), kps = R(r, 13);
+        const float lamda_grad = (gx_vx + gz_vz) * (atxx + atzz);
+        const float miu_grad = -2.0f * (gx_vx * atzz + gz_vz * atxx) + (gz_vx + gx_vz) * atxz;
+        img_pp[o] = R(r, 14) + kpp * lamda_grad;
+        img_ps[o] = R(r, 15) + kps * miu_grad;
+      }
+    }
+    push(w_btxx, btxx);
+    push(w_btxz, btxz);
+    push(w_btzz, btzz);
+    push(w_P, P);
+    push(w_L, L);
+    push(w_M, M);
+    push(w_Pz, Pz);
+    push(w_Lx, Lx);
+    // ---- stage 2: velocities of row r2 = r - 8 ---------------------------------------------
+    const int r2 = r - 8;
+    s_btxz[t] = w_btxz[4];
+    s_btzz[t] = w_btzz[0];
+    s_m[t] = w_M[4];
+    s_pz[t] = w_Pz[0];
+    s_lx[t] = w_Lx[0];
+    __syncthreads();
+    if (c2 && zin && r2 >= x0 && r2 < x1) {
+      const long long k = base + (long long)r2 * ld + z;
+      const bool x_int = r2 >= pml && r2 < d.nxp - pml;
+      const float bb = R(r, 16);
+      const float cbx = bb * dtdx, cbz = bb * dtdz;
+      if (x_int && z_int) {
+        const float ax = dxp_mid(w_btxx);
+        const float fx = dxm_mid(w_btxz);
+        const float bz = stencil4([&](int i) { return s_btxz[t + i - 1] - s_btxz[t - i]; });
+        const float ez = stencil4([&](int i) { return s_btzz[t + i] - s_btzz[t - i + 1]; });
+        float ovx = w_bvx[0], ovz = w_bvz[0];
+        if (a.strips_on && band_offset(d, r2, z) >= 0) {  // inner band: own state, not the strip
+          ovx = __ldg(a.ra.vx + k);
+          ovz = __ldg(a.ra.vz + k);
+        }
+        const float vx = ovx + (-cbx * ax + -cbz * bz);
+        const float vz = ovz + (-cbx * fx + -cbz * ez);
+        a.rb.vx[k] = vx;
+        a.rb.vz[k] = vz;
+        const long long o = (img_row + (r2 - pml)) * d.wnz + (z - pml);
+        img_il[o] = R(r, 17) + (vx * vx + vz * vz);
+      }
+      if (r2 >= d.nop && r2 < d.nxp - d.nop && z_upd) {
+        const float t_xx = dxp_mid(w_P);
+        const float t_zx = dxp_mid(w_L);
+        const float s_xz = dxm_mid(w_M);
+        const float t_xz = stencil4([&](int i) { return s_m[t + i - 1] - s_m[t - i]; });
+        const float s_zz = stencil4([&](int i) { return s_pz[t + i] - s_pz[t - i + 1]; });
+        const float s_xx = stencil4([&](int i) { return s_lx[t + i] - s_lx[t - i + 1]; });
+        const float ux_x = fmaf(-cbx, t_zx, -cbx * t_xx), ux_z = -cbz * t_xz;
+        const float uz_x = -cbx * s_xz, uz_z = fmaf(-cbz, s_xx, -cbz * s_zz);
+        float vx, vz;
+        if (kPML && pml_cell(d, r2, z)) {
+          const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+          const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
+          const float vxx = __fdiv_rn(fmaf(d1, a.aa.vx_x[k], ux_x), d2);
+          const float vxz = __fdiv_rn(fmaf(d3, a.aa.vx_z[k], ux_z), d4);
+          const float vzx = __fdiv_rn(fmaf(d1, a.aa.vz_x[k], uz_x), d2);
+          const float vzz = __fdiv_rn(fmaf(d3, a.aa.vz_z[k], uz_z), d4);
+          a.ab.vx_x[k] = vxx; a.ab.vx_z[k] = vxz; a.ab.vz_x[k] = vzx; a.ab.vz_z[k] = vzz;
+          vx = vxx + vxz;
+          vz = vzx + vzz;
+        } else {
+          float ovx = w_avx[0], ovz = w_avz[0];
+          if (rec_col && rmap[r2] >= 0) {  // injected cell: state without the residual
+            ovx = __ldg(a.aa.vx + k);
+            ovz = __ldg(a.aa.vz + k);
+          }
+          vx = ovx + (ux_x + ux_z);
+          vz = ovz + (uz_x + uz_z);
+        }
+        a.ab.vx[k] = vx;
+        a.ab.vz[k] = vz;
+      }
+    }
+  }
+  cp_async_wait<0>();
 }
 
 }  // namespace ds2d

@@ -628,6 +628,156 @@ int rtm_impl(const orc_grid *gg, const float *const model[7], const float *wav, 
   return 0;
 }
 
+// ---- acoustic Born operator pair (exact discrete adjoint), FP64 -----------------------------
+// Fields vx, vz, s (s = txx = tzz of the mu = 0 elastic scheme).  U = [nop, n-nop)^2 is the
+// updated set, I = [pml, n-pml)^2 the interior carrying the Born source.
+struct AcOp {
+  Geo<double> g;
+  Vec<double> b, lam;
+  double cx, cz;  // dt/dx, dt/dz
+  explicit AcOp(const orc_grid *gg, const float *const model[7]) : g(gg) {
+    b.resize(g.n);
+    lam.resize(g.n);
+    for (size_t k = 0; k < g.n; k++) {
+      b[k] = 1.0 / (double)model[2][k];
+      lam[k] = model[3][k];
+    }
+    cx = g.dt / g.dx;
+    cz = g.dt / g.dz;
+  }
+  size_t I(int ix, int iz) const { return g.I(ix, iz); }
+  // Dx+ f = sum c_i (f[x+i] - f[x-i+1]); Dx- f = sum c_i (f[x+i-1] - f[x-i]); same in z.
+  template <class F> double dxp(F f, int ix, int iz) const {
+    double t = 0;
+    for (int i = 1; i <= 4; i++) t += g.c[i] * (f(I(ix + i, iz)) - f(I(ix - i + 1, iz)));
+    return t;
+  }
+  template <class F> double dxm(F f, int ix, int iz) const {
+    double t = 0;
+    for (int i = 1; i <= 4; i++) t += g.c[i] * (f(I(ix + i - 1, iz)) - f(I(ix - i, iz)));
+    return t;
+  }
+  template <class F> double dzp(F f, int ix, int iz) const {
+    double t = 0;
+    for (int i = 1; i <= 4; i++) t += g.c[i] * (f(I(ix, iz + i)) - f(I(ix, iz - i + 1)));
+    return t;
+  }
+  template <class F> double dzm(F f, int ix, int iz) const {
+    double t = 0;
+    for (int i = 1; i <= 4; i++) t += g.c[i] * (f(I(ix, iz + i - 1)) - f(I(ix, iz - i)));
+    return t;
+  }
+  // One step: v += b dt/d D+ (s + e + source), then s += lam (dt/dx Dx- vx + dt/dz Dz- vz).
+  // dir = -1 undoes a dir = +1 step exactly (stress first, then velocities).
+  void step(Vec<double> &vx, Vec<double> &vz, Vec<double> &s, const Vec<double> *e, long ksrc,
+            double sval, int dir) const {
+    const int lo = g.nop;
+    auto S = [&](size_t q) {
+      double v = s[q];
+      if (e) v += (*e)[q];
+      if ((long)q == ksrc) v += sval;
+      return v;
+    };
+    auto vstage = [&]() {
+      FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {
+        size_t k = I(ix, iz);
+        vx[k] += dir * b[k] * cx * dxp(S, ix, iz);
+        vz[k] += dir * b[k] * cz * dzp(S, ix, iz);
+      }
+    };
+    auto sstage = [&]() {
+      auto VX = [&](size_t q) { return vx[q]; };
+      auto VZ = [&](size_t q) { return vz[q]; };
+      FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {
+        size_t k = I(ix, iz);
+        s[k] += dir * lam[k] * (cx * dxm(VX, ix, iz) + cz * dzm(VZ, ix, iz));
+      }
+    };
+    if (dir > 0) { vstage(); sstage(); } else { sstage(); vstage(); }
+  }
+  // Born source e = -2 lam m (Dx- vx / dx + Dz- vz / dz) on I.
+  void born(const Vec<double> &vx, const Vec<double> &vz, const double *m, Vec<double> &e) const {
+    auto VX = [&](size_t q) { return vx[q]; };
+    auto VZ = [&](size_t q) { return vz[q]; };
+    FOR_CELLS(g.pml, g.nx - g.pml, g.pml, g.nz - g.pml) {
+      size_t k = I(ix, iz);
+      e[k] = -2.0 * lam[k] * m[k] * (dxm(VX, ix, iz) / g.dx + dzm(VZ, ix, iz) / g.dz);
+    }
+  }
+  // Transpose of one dir = +1 step acting on the adjoint state; returns the gradient with
+  // respect to the injected e in ge (on U).
+  void adj_step(Vec<double> &yx, Vec<double> &yz, Vec<double> &ys, Vec<double> &ge) const {
+    const int lo = g.nop;
+    Vec<double> w(g.n, 0.0), ux(g.n, 0.0), uz(g.n, 0.0);
+    FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) { size_t k = I(ix, iz); w[k] = lam[k] * ys[k]; }
+    auto W = [&](size_t q) { return w[q]; };
+    FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {  // transpose of the stress stage
+      size_t k = I(ix, iz);
+      yx[k] -= cx * dxp(W, ix, iz);
+      yz[k] -= cz * dzp(W, ix, iz);
+    }
+    FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {
+      size_t k = I(ix, iz);
+      ux[k] = b[k] * cx * yx[k];
+      uz[k] = b[k] * cz * yz[k];
+    }
+    auto UX = [&](size_t q) { return ux[q]; };
+    auto UZ = [&](size_t q) { return uz[q]; };
+    FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {  // transpose of the velocity stage
+      size_t k = I(ix, iz);
+      const double gs = -dxm(UX, ix, iz) - dzm(UZ, ix, iz);
+      ys[k] += gs;
+      ge[k] = gs;
+    }
+  }
+};
+
+int ac_born(const orc_grid *gg, const float *const model[7], const float *wav, int nt,
+            const orc_shot *s, const double *m, double *rz, double *rx) {
+  AcOp op(gg, model);
+  const Geo<double> &g = op.g;
+  Vec<double> vx(g.n, 0), vz(g.n, 0), sg(g.n, 0), dvx(g.n, 0), dvz(g.n, 0), ds(g.n, 0), e(g.n, 0);
+  const long ks = (long)g.I(s->isx, s->isz);
+  for (int it = 0; it < nt; it++) {
+    op.step(vx, vz, sg, nullptr, ks, wav[it], 1);
+    op.born(vx, vz, m, e);
+    op.step(dvx, dvz, ds, &e, -1, 0.0, 1);
+    for (int tr = 0; tr < s->ntr; tr++) {
+      size_t k = g.I(s->igx[tr], s->igz);
+      rz[(size_t)tr * nt + it] = dvz[k];
+      rx[(size_t)tr * nt + it] = dvx[k];
+    }
+  }
+  return 0;
+}
+
+int ac_born_adj(const orc_grid *gg, const float *const model[7], const float *wav, int nt,
+                const orc_shot *s, const double *rz, const double *rx, double *grad) {
+  AcOp op(gg, model);
+  const Geo<double> &g = op.g;
+  Vec<double> vx(g.n, 0), vz(g.n, 0), sg(g.n, 0), yx(g.n, 0), yz(g.n, 0), ys(g.n, 0), ge(g.n, 0);
+  const long ks = (long)g.I(s->isx, s->isz);
+  for (int it = 0; it < nt; it++) op.step(vx, vz, sg, nullptr, ks, wav[it], 1);
+  std::fill(grad, grad + g.n, 0.0);
+  auto VX = [&](size_t q) { return vx[q]; };
+  auto VZ = [&](size_t q) { return vz[q]; };
+  for (int it = nt - 1; it >= 0; --it) {
+    for (int tr = 0; tr < s->ntr; tr++) {  // transpose of the recording after step it
+      size_t k = g.I(s->igx[tr], s->igz);
+      yz[k] += rz[(size_t)tr * nt + it];
+      yx[k] += rx[(size_t)tr * nt + it];
+    }
+    op.adj_step(yx, yz, ys, ge);
+    for (int ix = g.pml; ix < g.nx - g.pml; ix++)  // transpose of the Born source at step it
+      for (int iz = g.pml; iz < g.nz - g.pml; iz++) {
+        size_t k = g.I(ix, iz);
+        grad[k] += -2.0 * op.lam[k] * (op.dxm(VX, ix, iz) / g.dx + op.dzm(VZ, ix, iz) / g.dz) * ge[k];
+      }
+    op.step(vx, vz, sg, nullptr, ks, wav[it], -1);  // background back to step it-1
+  }
+  return 0;
+}
+
 inline uint64_t splitmix64(uint64_t z) {
   // SplitMix64 finalizer (Steele, Lea, Flood 2014).
   z += 0x9E3779B97F4A7C15ull;
@@ -756,6 +906,16 @@ int orc_rtm_f32(const orc_grid *g, const float *const model[7], const float *wav
                 const orc_shot *s, const float *adj_vz, const float *adj_vx, int rbc,
                 double *const img[3]) {
   return rtm_impl<float>(g, model, wavelet, nt, s, adj_vz, adj_vx, rbc, img);
+}
+
+int orc_ac_born(const orc_grid *g, const float *const model[7], const float *wavelet, int nt,
+                const orc_shot *s, const double *m, double *rec_vz, double *rec_vx) {
+  return ac_born(g, model, wavelet, nt, s, m, rec_vz, rec_vx);
+}
+
+int orc_ac_born_adj(const orc_grid *g, const float *const model[7], const float *wavelet, int nt,
+                    const orc_shot *s, const double *rec_vz, const double *rec_vx, double *grad) {
+  return ac_born_adj(g, model, wavelet, nt, s, rec_vz, rec_vx, grad);
 }
 
 void orc_ncc_residual(int ntr, int nt, const float *syn_vz, const float *syn_vx,

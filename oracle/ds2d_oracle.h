@@ -106,6 +106,21 @@ void orc_ncc_residual(int ntr, int nt, const float *syn_vz, const float *syn_vx,
 void orc_adam_update(int n, int iter, const float *const grads[6], float *image_pp,
                      float *image_ps, double *s_p, double *s_s, double *r_p, double *r_s);
 
+/* Acoustic Born operator pair for CG-LSRTM (no reference counterpart: the reference's CG
+ * helpers, main.cpp:1224-1320, are never called and its adjoint is not the transpose of its
+ * Born modelling).  The acoustic scheme is the elastic one with mu = 0 (txx = tzz = sigma,
+ * txz = 0; born.cu:282-349 with miu = 0); the Born source is add_born_source with mu = 0
+ * (born.cu:394-400: sigma += -2 lam m (Dx- vx / dx + Dz- vz / dz), interior only, transient).
+ * Boundary: random band (model as built by orc_build_model with rbc = 1) and NO damping, so the
+ * background field is reconstructed by exact time reversal over the whole grid (source
+ * included).  model[] = vp, vs(unused), rho, lam, mu(unused), dampx, dampz (unused).
+ *   orc_ac_born:  m (padded [nxpml][nzpml], zero outside the interior) -> rec_vz, rec_vx [ntr][nt]
+ *   orc_ac_born_adj: rec_vz, rec_vx -> g (padded), the exact transpose of orc_ac_born. */
+int orc_ac_born(const orc_grid *g, const float *const model[7], const float *wavelet, int nt,
+                const orc_shot *s, const double *m, double *rec_vz, double *rec_vx);
+int orc_ac_born_adj(const orc_grid *g, const float *const model[7], const float *wavelet, int nt,
+                    const orc_shot *s, const double *rec_vz, const double *rec_vx, double *grad);
+
 /* Project random-band factor in [0.6, 1.0): shared bit-for-bit with the CUDA setup kernel. */
 float orc_random_band_factor(uint64_t seed, int shot_id, int ix, int iz);
 

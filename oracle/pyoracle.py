@@ -57,6 +57,8 @@ def lib():
                                                        dp, dp, dp, dp, ctypes.POINTER(dp), dp]
             getattr(L, f"orc_rtm_{p}").argtypes = [G, M, fp, ctypes.c_int, S, fp, fp, ctypes.c_int,
                                                     ctypes.POINTER(dp)]
+        L.orc_ac_born.argtypes = [G, M, fp, ctypes.c_int, S, dp, dp, dp]
+        L.orc_ac_born_adj.argtypes = [G, M, fp, ctypes.c_int, S, dp, dp, dp]
         L.orc_ncc_residual.argtypes = [ctypes.c_int, ctypes.c_int, fp, fp, fp, fp, ctypes.c_int,
                                        dp, dp, dp]
         L.orc_ncc_residual.restype = None
@@ -164,6 +166,32 @@ def rtm(st, model, wavelet, shot, adj_vz, adj_vx, rbc=0, precision="f64"):
     getattr(lib(), f"orc_rtm_{precision}")(ctypes.byref(st.g), mp, _p(w), nt, ctypes.byref(sh),
                                            _p(_f(adj_vz)), _p(_f(adj_vx)), rbc, iptr)
     return imgs
+
+
+def ac_born(st, model, wavelet, shot, m_pad):
+    """Acoustic Born modelling L m of one shot (FP64): (rec_vz, rec_vx) [ntr][nt]."""
+    sh, keep = _shot(shot)
+    mp, keep2 = _model_ptrs(model)
+    w = _f(wavelet)
+    nt = len(w)
+    m = np.ascontiguousarray(m_pad, np.float64)
+    rz, rx = np.zeros((shot.ntr, nt)), np.zeros((shot.ntr, nt))
+    lib().orc_ac_born(ctypes.byref(st.g), mp, _p(w), nt, ctypes.byref(sh), _p(m, dp), _p(rz, dp),
+                      _p(rx, dp))
+    return rz, rx
+
+
+def ac_born_adj(st, model, wavelet, shot, rz, rx):
+    """Exact transpose L^T of ac_born for one shot: padded gradient [nxpml][nzpml] (FP64)."""
+    sh, keep = _shot(shot)
+    mp, keep2 = _model_ptrs(model)
+    w = _f(wavelet)
+    nt = len(w)
+    g = np.zeros(st.shape)
+    lib().orc_ac_born_adj(ctypes.byref(st.g), mp, _p(w), nt, ctypes.byref(sh),
+                          _p(np.ascontiguousarray(rz, np.float64), dp),
+                          _p(np.ascontiguousarray(rx, np.float64), dp), _p(g, dp))
+    return g
 
 
 def ricker(nt, f0, dt):

@@ -144,12 +144,14 @@ def test_elsrtm_adjoint_born_as_written(cuda_device):
 
 @pytest.mark.parametrize("boundary", ["pml", "random"])
 @pytest.mark.parametrize("xr", [16, 64])
-def test_fused_step_matches_half_steps(cuda_device, boundary, xr):
+@pytest.mark.parametrize("ring", [0, 1])
+def test_fused_step_matches_half_steps(cuda_device, boundary, xr, ring):
     c, vp, vs, w, shots = small_case(nt=300)
     out = {}
     for fused in (0, 1):
         with _ctx(c, shots, boundary=boundary, seed=5) as e:
             e.set_option("fused", fused)
+            e.set_option("ring", ring)
             e.set_option("xr", xr)
             e.set_models(vp, vs)
             e.set_wavelet(w)
@@ -188,6 +190,32 @@ def test_uneven_windows_vs_oracle(cuda_device, fused):
         off += s.ntr
     for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
         assert rel(imgs[key], tot[k]) < 1e-4, (key, rel(imgs[key], tot[k]))
+
+
+def test_graph_replay_matches_direct_launches(cuda_device):
+    """Batches captured into CUDA graphs (first call) and replayed (later calls) give the same
+    bits as direct launches."""
+    import torch
+    c, vp, vs, w, shots = small_case(nt=150)
+    stream = torch.cuda.Stream()
+    out = {}
+    for graph in (0, 1):
+        with _ctx(c, shots, boundary="random", seed=3) as e:
+            e.set_option("graph", graph)
+            e.set_stream(stream.cuda_stream)
+            e.set_models(vp, vs)
+            e.set_wavelet(w)
+            rz, rx = e.forward(shots)
+            rz2, rx2 = e.forward(shots)  # replay
+            np.testing.assert_array_equal(rz, rz2)
+            for _ in range(2):  # capture, then replay
+                e.rtm(shots, rz, rx)
+                out[graph, _] = e.read_images()
+            out[graph, "rec"] = rz
+    np.testing.assert_array_equal(out[0, "rec"], out[1, "rec"])
+    for key in ("pp_grad", "ps_grad", "illumination"):
+        np.testing.assert_array_equal(out[1, 0][key], out[0, 0][key])
+        np.testing.assert_array_equal(out[1, 1][key], out[0, 0][key])
 
 
 def test_batched_equals_one_by_one(cuda_device):
