@@ -158,6 +158,43 @@ class Elastic2D:
         self._check(self.lib.ds2d_rtm_device(self.h, arr, len(shots), ctypes.c_void_p(adj_vz_ptr),
                                              ctypes.c_void_p(adj_vx_ptr)))
 
+    def dot_f64(self, a_ptr, b_ptr, n):
+        """FP64 <a, b> of two float device vectors (integer device pointers)."""
+        out = ctypes.c_double(0.0)
+        self._check(self.lib.ds2d_dot_f64(self.h, ctypes.c_void_p(a_ptr), ctypes.c_void_p(b_ptr),
+                                          int(n), ctypes.byref(out)))
+        return out.value
+
+    # -- acoustic Born pair and CG-LSRTM (context built with boundary="random", vs = 0) ------
+    def ac_born(self, shots, m):
+        """d = L m: scattered vz, vx of the acoustic Born operator, each [sum ntr][nt]."""
+        arr, keep = self._shots(shots)
+        m = _f32(m)
+        rz, rx = self._rec(shots), self._rec(shots)
+        self._check(self.lib.ds2d_ac_born(self.h, arr, len(shots), _fptr(m), _fptr(rz), _fptr(rx)))
+        return rz, rx
+
+    def ac_born_adj(self, shots, rec_vz, rec_vx):
+        """g = L^T d, the exact transpose of ac_born ([allnx][allnz])."""
+        arr, keep = self._shots(shots)
+        rz, rx = _f32(rec_vz), _f32(rec_vx)
+        g = np.zeros((self.allnx, self.allnz), np.float32)
+        self._check(self.lib.ds2d_ac_born_adj(self.h, arr, len(shots), _fptr(rz), _fptr(rx), _fptr(g)))
+        return g
+
+    def lsrtm(self, shots, obs_vz, obs_vx, niter, target=0.0):
+        """CGLS on ||L m - d||^2 from m = 0: returns (m, relative residual after each iteration)."""
+        arr, keep = self._shots(shots)
+        oz, ox = _f32(obs_vz), _f32(obs_vx)
+        m = np.zeros((self.allnx, self.allnz), np.float32)
+        hist = np.zeros(max(niter, 1))
+        done = ctypes.c_int(0)
+        self._check(self.lib.ds2d_lsrtm(self.h, arr, len(shots), _fptr(oz), _fptr(ox), int(niter),
+                                        float(target), _fptr(m),
+                                        hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                        ctypes.byref(done)))
+        return m, hist[:done.value]
+
     IMAGE_NAMES = ("pp_grad", "ps_grad", "illumination", "b_pp", "b_ps", "b_pp2", "b_ps2")
 
     def read_images(self, reset=True, which=None):

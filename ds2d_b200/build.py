@@ -25,13 +25,24 @@ def stale():
     return any(os.path.getmtime(p) > t for p in DEPS if os.path.exists(p))
 
 
+HOST_MAIN = os.path.join(HERE, "csrc", "host", "ds2d_main.cpp")
+HOST_BIN = os.path.join(HERE, "ds2d_elsrtm")
+
+
 def build(force=False, verbose=False):
-    if not force and not stale():
-        return LIB
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", LIB] + SOURCES
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+    if force or stale():
+        cmd = [_nvcc()] + NVCC_FLAGS + ["-o", LIB] + SOURCES
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    if force or not os.path.exists(HOST_BIN) or os.path.getmtime(HOST_BIN) < max(
+            os.path.getmtime(LIB), os.path.getmtime(HOST_MAIN)):
+        # C++ host driver (parameters file, SU I/O, shot loop) linked against the library.
+        cmd = ["g++", "-O2", "-std=c++17", "-o", HOST_BIN, HOST_MAIN, "-L" + HERE, "-lds2d_b200",
+               "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
     return LIB
 
 

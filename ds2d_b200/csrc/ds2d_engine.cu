@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/ds2d.h"
+#include "ds2d_acoustic.cuh"
 #include "ds2d_fused.cuh"
 #include "ds2d_step.cuh"
 
@@ -183,6 +184,15 @@ struct ds2d_ctx {
   int opt_fused = 1, opt_xr = 64;
   int opt_adjoint_born = 0;  // scattered adjoint of ELSRTM (off = the reference's observed runs)
   int opt_ring = 1;          // cp.async ring-fed fused kernels
+  // Acoustic Born pair (LSRTM): background, scattered and adjoint states, Born overlay.
+  float *ac[10] = {};        // bvx bvz bs | dvx dvz ds | yx yz ys | e
+  double *dot_part = nullptr, *dot_out = nullptr;  // FP64 inner-product scratch
+  // Work vectors of the LSRTM solver (model- and data-space), grown on demand.
+  struct Vec {
+    float *p = nullptr;
+    size_t n = 0;
+  };
+  Vec vecs[12];
   Wave fw2{}, abk2{};  // ping-pong partners of fw / abk for the fused kernels
   Wave *fw_cur = nullptr;  // buffer holding the latest forward state
   double batch_cells = 0, batch_wcells = 0;  // padded / interior cells of the current batch
@@ -818,6 +828,161 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
   return DS2D_OK;
 }
 
+// ---- acoustic Born pair and CG-LSRTM ---------------------------------------------------------
+
+int ensure_acoustic(ds2d_ctx *c) {
+  int rc;
+  if ((rc = ensure_common(c))) return rc;
+  if (!c->d.rbc)
+    return fail(c, DS2D_E_STATE,
+                "the acoustic LSRTM operators need boundary = DS2D_BOUNDARY_RANDOM (exact time "
+                "reversal of an undamped grid)");
+  if (!c->p_dmp) {
+    if ((rc = alloc_slots(c, &c->p_dmp))) return rc;
+    if ((rc = alloc_slots(c, &c->p_dms))) return rc;
+    c->par.dmp = c->p_dmp;
+    c->par.dms = c->p_dms;
+  }
+  for (float *&p : c->ac)
+    if (!p && (rc = alloc_slots(c, &p))) return rc;
+  if (!c->dot_part) {
+    if ((rc = alloc(c, (void **)&c->dot_part, sizeof(double) * kDotBlocks))) return rc;
+    if ((rc = alloc(c, (void **)&c->dot_out, sizeof(double)))) return rc;
+  }
+  return DS2D_OK;
+}
+
+AcArgs ac_args(ds2d_ctx *c, int set, int it, float dir) {
+  AcArgs a{};
+  a.d = c->d; a.shots = c->d_shots; a.p = c->par;
+  a.vx = c->ac[3 * set]; a.vz = c->ac[3 * set + 1]; a.s = c->ac[3 * set + 2];
+  a.wavelet = c->wavelet; a.it = it; a.dir = dir; a.rmap = c->d_rmap;
+  return a;
+}
+
+// L m for the uploaded batch: scattered vz / vx into rec[0] / rec[1] (m = the window p_dmp).
+int ac_L_batch(ds2d_ctx *c, int n) {
+  const Dims &d = c->d;
+  size_t bytes = sizeof(float) * (size_t)d.slot * n;
+  for (int i = 0; i < 10; i++)
+    if (i < 6 || i == 9) CK(cudaMemsetAsync(c->ac[i], 0, bytes, c->stream));
+  size_t nrec = (size_t)n * d.max_ntr * d.nt;
+  CK(cudaMemsetAsync(c->rec[0], 0, nrec * 4, c->stream));
+  CK(cudaMemsetAsync(c->rec[1], 0, nrec * 4, c->stream));
+  dim3 grid = cell_grid(d, n), blk(32, 8);
+  for (int it = 0; it < d.nt; it++) {
+    AcArgs b = ac_args(c, 0, it, 1.f);
+    b.src_on = 1;
+    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
+    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+    k_ac_born<<<grid, blk, 0, c->stream>>>(d, c->d_shots, c->par, c->ac[0], c->ac[1], c->ac[9]);
+    c->last_launches++;
+    AcArgs s = ac_args(c, 1, it, 1.f);
+    s.e = c->ac[9];
+    s.rec_on = 1; s.rec_vz = c->rec[0]; s.rec_vx = c->rec[1];
+    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, s);
+    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, s);
+  }
+  CK(cudaGetLastError());
+  return DS2D_OK;
+}
+
+// L^T r for the uploaded batch (r in rec[0] / rec[1]); the windowed gradients are added into
+// the model-size image 0.
+int ac_LT_batch(ds2d_ctx *c, int n) {
+  const Dims &d = c->d;
+  size_t bytes = sizeof(float) * (size_t)d.slot * n;
+  for (int i = 0; i < 9; i++)
+    if (i < 3 || i >= 6) CK(cudaMemsetAsync(c->ac[i], 0, bytes, c->stream));
+  size_t plane = (size_t)c->B * d.wnx * d.wnz;
+  CK(cudaMemsetAsync(c->img_slot, 0, plane * sizeof(float), c->stream));
+  dim3 grid = cell_grid(d, n), blk(32, 8);
+  for (int it = 0; it < d.nt; it++) {
+    AcArgs b = ac_args(c, 0, it, 1.f);
+    b.src_on = 1;
+    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
+    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+  }
+  for (int it = d.nt - 1; it >= 0; --it) {
+    AcAdjArgs y{};
+    y.d = d; y.shots = c->d_shots; y.p = c->par;
+    y.yx = c->ac[6]; y.yz = c->ac[7]; y.ys = c->ac[8];
+    y.rmap = c->d_rmap; y.res_vz = c->rec[0]; y.res_vx = c->rec[1]; y.it = it;
+    y.bvx = c->ac[0]; y.bvz = c->ac[1]; y.grad = c->img_slot;
+    LAUNCHP("ac_adj_v", 0, k_ac_adj_v, grid, blk, y);
+    LAUNCHP("ac_adj_s", 0, k_ac_adj_s, grid, blk, y);
+    AcArgs b = ac_args(c, 0, it, -1.f);  // background back to step it-1: stress, then velocity
+    b.src_on = 1;
+    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
+  }
+  CK(cudaGetLastError());
+  return reduce_images(c, n, 1);
+}
+
+// Applies L (m_dev -> data vector [n][max_ntr][nt] x {z, x}) or L^T (data -> grad_dev) over all
+// shots in batches.  m_dev / grad_dev are model-size device arrays.
+int ac_apply(ds2d_ctx *c, const ds2d_shot *shots, int n, bool adjoint, const float *m_dev,
+             float *dz, float *dx, float *grad_dev) {
+  const Dims &d = c->d;
+  int rc;
+  size_t nall = (size_t)d.allnx * d.allnz;
+  if (!adjoint) CK(cudaMemcpyAsync(c->pp_all, m_dev, nall * 4, cudaMemcpyDeviceToDevice, c->stream));
+  else CK(cudaMemsetAsync(c->images, 0, nall * 4, c->stream));
+  const size_t per = (size_t)d.max_ntr * d.nt;
+  for (int f = 0; f < n; f += c->B) {
+    const int m = std::min(c->B, n - f);
+    if ((rc = upload_batch(c, shots + f, m))) return rc;
+    if ((rc = setup_batch(c, m, f, !adjoint))) return rc;
+    if (!adjoint) {
+      if ((rc = ac_L_batch(c, m))) return rc;
+      CK(cudaMemcpyAsync(dz + f * per, c->rec[0], m * per * 4, cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(dx + f * per, c->rec[1], m * per * 4, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+      CK(cudaMemcpyAsync(c->rec[0], dz + f * per, m * per * 4, cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->rec[1], dx + f * per, m * per * 4, cudaMemcpyDeviceToDevice, c->stream));
+      if ((rc = ac_LT_batch(c, m))) return rc;
+    }
+    // upload_batch of the next batch overwrites d_shots / rmap: finish this batch first.
+    CK(cudaStreamSynchronize(c->stream));
+    c->last_updates += 2.0 * c->batch_cells * d.nt;
+  }
+  if (adjoint) CK(cudaMemcpyAsync(grad_dev, c->images, nall * 4, cudaMemcpyDeviceToDevice, c->stream));
+  return DS2D_OK;
+}
+
+// Work vector `i` with room for n floats (zeroed when (re)allocated).
+int work_vec(ds2d_ctx *c, int i, size_t n, float **out) {
+  ds2d_ctx::Vec &v = c->vecs[i];
+  if (v.n < n) {
+    if (v.p) cudaFree(v.p);
+    v.p = nullptr;
+    v.n = 0;
+    cudaError_t e = cudaMalloc(&v.p, n * sizeof(float));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      v.p = nullptr;
+      return fail(c, DS2D_E_NOMEM, "cudaMalloc(%zu floats) for a solver vector: %s", n,
+                  cudaGetErrorString(e));
+    }
+    v.n = n;
+    CK(cudaMemsetAsync(v.p, 0, n * sizeof(float), c->stream));
+  }
+  *out = v.p;
+  return DS2D_OK;
+}
+
+// FP64 <a, b> over n floats (device), result on the host.
+int dot64(ds2d_ctx *c, const float *a, const float *b, long long n, double *out) {
+  k_dot_partial<<<kDotBlocks, kDotThreads, 0, c->stream>>>(a, b, n, c->dot_part);
+  k_dot_final<<<1, 32, 0, c->stream>>>(c->dot_part, kDotBlocks, c->dot_out);
+  c->last_launches += 2;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, c->dot_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -920,6 +1085,8 @@ int ds2d_destroy(ds2d_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
   c->graphs.clear();
+  for (auto &v : c->vecs)
+    if (v.p) cudaFree(v.p);
   c->arena.release();
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
@@ -1076,6 +1243,147 @@ int ds2d_read_images(ds2d_ctx *c, float *const images[7], int reset) {
   if (reset) CK(cudaMemsetAsync(c->images, 0, 7 * n * 4, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return DS2D_OK;
+}
+
+static int data_io(ds2d_ctx *c, const ds2d_shot *shots, int n, float *dev, float *host,
+                   bool to_dev) {
+  const size_t per = (size_t)c->d.max_ntr * c->d.nt;
+  long long tb = 0;
+  for (int s = 0; s < n; s++) {
+    const size_t cnt = (size_t)shots[s].ntr * c->d.nt;
+    if (cnt) {
+      if (to_dev)
+        CK(cudaMemcpyAsync(dev + s * per, host + tb * c->d.nt, cnt * 4, cudaMemcpyHostToDevice, c->stream));
+      else
+        CK(cudaMemcpyAsync(host + tb * c->d.nt, dev + s * per, cnt * 4, cudaMemcpyDeviceToHost, c->stream));
+    }
+    tb += shots[s].ntr;
+  }
+  return DS2D_OK;
+}
+
+static int check_shots(ds2d_ctx *c, const ds2d_shot *shots, int n) {
+  for (int s = 0; s < n; s++)
+    if (shots[s].ntr > c->d.max_ntr) return fail(c, DS2D_E_ARG, "shot %d: ntr > max_ntr", s);
+  return DS2D_OK;
+}
+
+int ds2d_ac_born(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *m, float *rec_vz,
+                 float *rec_vx) {
+  int rc;
+  if ((rc = check_ready(c, false))) return rc;
+  if (n <= 0 || !shots || !m || !rec_vz || !rec_vx) return fail(c, DS2D_E_ARG, "bad arguments");
+  if ((rc = ensure_acoustic(c)) || (rc = check_shots(c, shots, n))) return rc;
+  c->last_launches = 0;
+  c->last_updates = 0;
+  const size_t nall = (size_t)c->d.allnx * c->d.allnz, nd = (size_t)n * c->d.max_ntr * c->d.nt;
+  float *mv, *dz, *dx;
+  if ((rc = work_vec(c, 0, nall, &mv)) || (rc = work_vec(c, 7, nd, &dz)) || (rc = work_vec(c, 8, nd, &dx)))
+    return rc;
+  CK(cudaMemcpyAsync(mv, m, nall * 4, cudaMemcpyHostToDevice, c->stream));
+  if ((rc = ac_apply(c, shots, n, false, mv, dz, dx, nullptr))) return rc;
+  if ((rc = data_io(c, shots, n, dz, rec_vz, false)) || (rc = data_io(c, shots, n, dx, rec_vx, false)))
+    return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+int ds2d_ac_born_adj(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *rec_vz,
+                     const float *rec_vx, float *grad) {
+  int rc;
+  if ((rc = check_ready(c, false))) return rc;
+  if (n <= 0 || !shots || !grad || !rec_vz || !rec_vx) return fail(c, DS2D_E_ARG, "bad arguments");
+  if ((rc = ensure_acoustic(c)) || (rc = check_shots(c, shots, n))) return rc;
+  c->last_launches = 0;
+  c->last_updates = 0;
+  const size_t nall = (size_t)c->d.allnx * c->d.allnz, nd = (size_t)n * c->d.max_ntr * c->d.nt;
+  float *gv, *dz, *dx;
+  if ((rc = work_vec(c, 1, nall, &gv)) || (rc = work_vec(c, 5, nd, &dz)) || (rc = work_vec(c, 6, nd, &dx)))
+    return rc;
+  CK(cudaMemsetAsync(dz, 0, nd * 4, c->stream));
+  CK(cudaMemsetAsync(dx, 0, nd * 4, c->stream));
+  if ((rc = data_io(c, shots, n, dz, (float *)rec_vz, true)) ||
+      (rc = data_io(c, shots, n, dx, (float *)rec_vx, true)))
+    return rc;
+  if ((rc = ac_apply(c, shots, n, true, nullptr, dz, dx, gv))) return rc;
+  CK(cudaMemcpyAsync(grad, gv, nall * 4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+int ds2d_lsrtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *obs_vz,
+               const float *obs_vx, int niter, double target, float *m_out, double *resid,
+               int *iters_done) {
+  int rc;
+  if ((rc = check_ready(c, false))) return rc;
+  if (n <= 0 || !shots || !obs_vz || !obs_vx || !m_out || niter < 0)
+    return fail(c, DS2D_E_ARG, "bad arguments");
+  if ((rc = ensure_acoustic(c)) || (rc = check_shots(c, shots, n))) return rc;
+  c->last_launches = 0;
+  c->last_updates = 0;
+  const size_t nall = (size_t)c->d.allnx * c->d.allnz, nd = (size_t)n * c->d.max_ntr * c->d.nt;
+  float *m, *sv, *p, *rz, *rx, *qz, *qx;
+  if ((rc = work_vec(c, 0, nall, &m)) || (rc = work_vec(c, 1, nall, &sv)) ||
+      (rc = work_vec(c, 2, nall, &p)) || (rc = work_vec(c, 5, nd, &rz)) ||
+      (rc = work_vec(c, 6, nd, &rx)) || (rc = work_vec(c, 7, nd, &qz)) ||
+      (rc = work_vec(c, 8, nd, &qx)))
+    return rc;
+  CK(cudaMemsetAsync(m, 0, nall * 4, c->stream));
+  CK(cudaMemsetAsync(rz, 0, nd * 4, c->stream));
+  CK(cudaMemsetAsync(rx, 0, nd * 4, c->stream));
+  if ((rc = data_io(c, shots, n, rz, (float *)obs_vz, true)) ||
+      (rc = data_io(c, shots, n, rx, (float *)obs_vx, true)))
+    return rc;
+  // CGLS on || L m - d ||^2 with m0 = 0: r = d, s = L^T r, p = s (FP64 scalars throughout).
+  double dd, tz, tx;
+  if ((rc = dot64(c, rz, rz, nd, &tz)) || (rc = dot64(c, rx, rx, nd, &tx))) return rc;
+  dd = tz + tx;
+  if (!(dd > 0)) return fail(c, DS2D_E_NUMERIC, "observed data are zero or not finite");
+  if ((rc = ac_apply(c, shots, n, true, nullptr, rz, rx, sv))) return rc;
+  CK(cudaMemcpyAsync(p, sv, nall * 4, cudaMemcpyDeviceToDevice, c->stream));
+  double gamma;
+  if ((rc = dot64(c, sv, sv, nall, &gamma))) return rc;
+  const int nb = 4 * 148;
+  int k = 0;
+  for (; k < niter; k++) {
+    if ((rc = ac_apply(c, shots, n, false, p, qz, qx, nullptr))) return rc;
+    if ((rc = dot64(c, qz, qz, nd, &tz)) || (rc = dot64(c, qx, qx, nd, &tx))) return rc;
+    const double delta = tz + tx;
+    if (!(delta > 0) || !std::isfinite(gamma)) return fail(c, DS2D_E_NUMERIC, "CG breakdown at %d", k);
+    const double alpha = gamma / delta;
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nall, alpha, p, m);
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -alpha, qz, rz);
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -alpha, qx, rx);
+    c->last_launches += 3;
+    if ((rc = dot64(c, rz, rz, nd, &tz)) || (rc = dot64(c, rx, rx, nd, &tx))) return rc;
+    const double rel = std::sqrt((tz + tx) / dd);
+    if (resid) resid[k] = rel;
+    if (rel <= target) {
+      k++;
+      break;
+    }
+    if ((rc = ac_apply(c, shots, n, true, nullptr, rz, rx, sv))) return rc;
+    double gnew;
+    if ((rc = dot64(c, sv, sv, nall, &gnew))) return rc;
+    const double beta = gnew / gamma;
+    gamma = gnew;
+    k_xpby<<<nb, 256, 0, c->stream>>>((long long)nall, sv, beta, p);
+    c->last_launches++;
+  }
+  if (iters_done) *iters_done = k;
+  CK(cudaMemcpyAsync(m_out, m, nall * 4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+int ds2d_dot_f64(ds2d_ctx *c, const float *a, const float *b, long long n, double *result) {
+  if (!c || !a || !b || !result || n < 0) return DS2D_E_ARG;
+  if (!c->dot_part) {
+    int rc;
+    if ((rc = alloc(c, (void **)&c->dot_part, sizeof(double) * kDotBlocks))) return rc;
+    if ((rc = alloc(c, (void **)&c->dot_out, sizeof(double)))) return rc;
+  }
+  return dot64(c, a, b, n, result);
 }
 
 int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {

@@ -121,6 +121,31 @@ double ds2d_last_cell_updates(const ds2d_ctx *ctx);
 /* Number of kernel launches issued by the last forward / elsrtm / rtm call. */
 long long ds2d_last_launches(const ds2d_ctx *ctx);
 
+/* Acoustic Born operator pair and CG-LSRTM (north-star extension; the reference ships unused
+ * CG helpers, main.cpp:1224-1320 sjcgsolver / FD2DGPU.cu:4885 ELSRTM_CALCULATE_ALPHA, and runs
+ * NCC + Adam instead).  The acoustic scheme is the elastic one with mu = 0 (pass vs = 0 to
+ * ds2d_set_models); the context must use DS2D_BOUNDARY_RANDOM (undamped grid, exact time
+ * reversal).  m / grad are [allnx][allnz]; records [sum ntr][nt].
+ *   ds2d_ac_born      d = L m  (scattered vz, vx; Born source of add_born_source with mu = 0)
+ *   ds2d_ac_born_adj  g = L^T d, the exact discrete transpose of ds2d_ac_born
+ *   ds2d_lsrtm        CGLS on ||L m - d||^2 from m = 0 with FP64 inner products and step
+ *                     lengths; stops after niter iterations or when ||d - L m|| / ||d|| <=
+ *                     target; resid[k] receives that ratio after iteration k. */
+int ds2d_ac_born(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *m, float *rec_vz,
+                 float *rec_vx);
+int ds2d_ac_born_adj(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *rec_vz,
+                     const float *rec_vx, float *grad);
+int ds2d_lsrtm(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *obs_vz,
+               const float *obs_vx, int niter, double target, float *m_out, double *resid,
+               int *iters_done);
+
+/* FP64 inner product <a, b> of two float vectors of n elements in device memory, the
+ * reduction the CG-LSRTM uses for its dot products and step lengths (the reference sums its CG
+ * products in float on the host, main.cpp:1232-1276).  Per-block partial sums go to scratch
+ * owned by the context, then one block adds them in a fixed order, so the result is
+ * deterministic.  Runs on the context stream and returns after the result is on the host. */
+int ds2d_dot_f64(ds2d_ctx *ctx, const float *a, const float *b, long long n, double *result);
+
 /* Tuning knobs (no counterpart in the reference, whose launch shape is fixed at 32x32 blocks,
  * FD2DGPU.cuh:8-9): "fused" (1 = single-pass fused time step, 0 = one launch per half step)
  * and "xr" (rows marched by one CTA of the fused kernels). */
