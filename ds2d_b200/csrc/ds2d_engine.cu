@@ -845,6 +845,10 @@ int ensure_acoustic(ds2d_ctx *c) {
   }
   for (float *&p : c->ac)
     if (!p && (rc = alloc_slots(c, &p))) return rc;
+  if (!c->img_slot) {  // per-shot gradient planes (same 7-plane size as the RTM images)
+    size_t n = (size_t)7 * c->B * c->d.wnx * c->d.wnz;
+    if ((rc = alloc(c, (void **)&c->img_slot, n * sizeof(float)))) return rc;
+  }
   if (!c->dot_part) {
     if ((rc = alloc(c, (void **)&c->dot_part, sizeof(double) * kDotBlocks))) return rc;
     if ((rc = alloc(c, (void **)&c->dot_out, sizeof(double)))) return rc;

@@ -711,6 +711,9 @@ __global__ void __launch_bounds__(kFB) k_bwd_ring(BwdFusedArgs a) {
       push(w_avx, n_avx);
       push(w_avz, n_avz);
     }
+    // Refill slot r + kRingAhead (= slot r - 2, last read two rows ago); only slot r is read
+    // below.
+    issue(r + kRingAhead);
     // ---- stage 1: stresses of row r1 = r - 4 -----------------------------------------------
     const int r1 = r - 4;
     s_bvx[t] = w_bvx[4];
