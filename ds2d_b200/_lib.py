@@ -25,7 +25,7 @@ EXPORTS = [
     "ds2d_set_wavelet", "ds2d_set_image", "ds2d_forward", "ds2d_elsrtm", "ds2d_rtm",
     "ds2d_rtm_device", "ds2d_read_images", "ds2d_last_cell_updates", "ds2d_last_launches",
     "ds2d_profile", "ds2d_profile_report", "ds2d_set_option", "ds2d_ac_born",
-    "ds2d_ac_born_adj", "ds2d_lsrtm", "ds2d_dot_f64",
+    "ds2d_ac_born_adj", "ds2d_lsrtm", "ds2d_dot_f64", "ds2d_dot_f64_noalloc",
 ]
 
 
@@ -87,6 +87,7 @@ def load():
         "ds2d_profile": ([P, ctypes.c_int], ctypes.c_int),
         "ds2d_set_option": ([P, ctypes.c_char_p, ctypes.c_longlong], ctypes.c_int),
         "ds2d_dot_f64": ([P, P, P, ctypes.c_longlong, dp], ctypes.c_int),
+        "ds2d_dot_f64_noalloc": ([P, P, ctypes.c_longlong, P, dp], ctypes.c_int),
         "ds2d_ac_born": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, fp], ctypes.c_int),
         "ds2d_ac_born_adj": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, fp], ctypes.c_int),
         "ds2d_lsrtm": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, ctypes.c_int,

@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1458,3 +1459,120 @@ double ds2d_last_cell_updates(const ds2d_ctx *c) { return c ? c->last_updates : 
 long long ds2d_last_launches(const ds2d_ctx *c) { return c ? c->last_launches : 0; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// FP64 inner product that allocates nothing.
+//
+// ds2d_dot_f64 keeps its per-block partial sums in scratch that the context allocates on first
+// use, and a context itself allocates the whole wavefield arena when it is created.  Some
+// callers cannot allocate device memory at the moment they need a dot product:
+//  - a host framework that owns the device memory budget and hands libraries only the buffers
+//    they work on (a pool that is already at its limit, or a policy that forbids a library
+//    from calling cudaMalloc behind its back);
+//  - a caller that has no ds2d context at all (a CG or convergence check on the host
+//    application's own vectors), for which creating one would allocate hundreds of MB;
+//  - a caller running when the HBM is full, e.g. between batches that sized the arena to what
+//    was left, where any new allocation fails with out-of-memory.
+// For them the scratch lives in this module's static device memory: the CUDA runtime reserves
+// it when it loads the module, so a call makes no allocation.  The price is that the scratch is
+// shared by every call on a device: calls on the same device that overlap in time (two host
+// threads, or two streams whose work runs concurrently) race on it and return wrong sums.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kNaPerThread = 64;                               // elements per thread
+constexpr long long kNaChunk = (long long)kDotThreads * kNaPerThread;  // 16384 per block
+constexpr int kNaMaxPartials = 32768;                          // 256 KiB of partial sums
+constexpr long long kNaMaxElems = kNaChunk * kNaMaxPartials;   // 2^29 = 536,870,912 elements
+constexpr int kNaMaxDevices = 64;
+
+// Partial sums [0, kNaMaxPartials) and the result slot [kNaMaxPartials].  Nothing here has to
+// start at zero: a call writes every partial it later reads, and the result before reading it.
+static __device__ __align__(256) double g_na_scratch[kNaMaxPartials + 1];
+
+// Same per-block reduction as k_dot_partial, but each block owns one contiguous chunk of
+// kNaChunk elements instead of a grid stride, so the block count (and the scratch a call needs)
+// follows n and is bounded by the static array.
+__global__ void __launch_bounds__(kDotThreads) k_dot_chunk(const float *a, const float *b,
+                                                           long long n, double *partial) {
+  __shared__ double sh[kDotThreads / 32];
+  const long long lo = (long long)blockIdx.x * kNaChunk;
+  const long long hi = lo + kNaChunk < n ? lo + kNaChunk : n;
+  double acc = 0.0;
+  for (long long i = lo + threadIdx.x; i < hi; i += kDotThreads)
+    acc = fma((double)a[i], (double)b[i], acc);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < kDotThreads / 32 ? sh[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+  }
+}
+
+std::mutex g_na_mu;
+double *g_na_ptr[kNaMaxDevices] = {};
+
+// Device address of g_na_scratch on the current device, looked up once per device (with that
+// device current, as cudaGetSymbolAddress requires) and cached.  The first call on a device
+// may load this module there, so it should come before any stream capture on that device.
+int na_scratch(double **out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    g_create_err = std::string("ds2d_dot_f64_noalloc: cudaGetDevice: ") + cudaGetErrorString(e);
+    return DS2D_E_CUDA;
+  }
+  if (dev < 0 || dev >= kNaMaxDevices) {
+    g_create_err = "ds2d_dot_f64_noalloc: device ordinal " + std::to_string(dev) +
+                   " is beyond the table of " + std::to_string(kNaMaxDevices) + " devices";
+    return DS2D_E_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  if (!g_na_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_na_scratch);
+    if (e != cudaSuccess || !p) {
+      g_create_err = std::string("ds2d_dot_f64_noalloc: cudaGetSymbolAddress: ") +
+                     cudaGetErrorString(e);
+      return DS2D_E_CUDA;
+    }
+    g_na_ptr[dev] = static_cast<double *>(p);
+  }
+  *out = g_na_ptr[dev];
+  return DS2D_OK;
+}
+
+}  // namespace
+
+extern "C" int ds2d_dot_f64_noalloc(const float *a, const float *b, long long n, void *stream,
+                                    double *result) {
+  if (!a || !b || !result || n < 0) {
+    g_create_err = "ds2d_dot_f64_noalloc: null vector/result pointer or negative length";
+    return DS2D_E_ARG;
+  }
+  if (n > kNaMaxElems) {
+    g_create_err = "ds2d_dot_f64_noalloc: n = " + std::to_string(n) +
+                   " exceeds the static scratch limit of " + std::to_string(kNaMaxElems) +
+                   " elements (" + std::to_string(kNaMaxPartials) + " partial sums of " +
+                   std::to_string(kNaChunk) + " elements); use ds2d_dot_f64";
+    return DS2D_E_ARG;
+  }
+  double *scratch = nullptr;
+  int rc = na_scratch(&scratch);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nb = n == 0 ? 1 : (int)((n + kNaChunk - 1) / kNaChunk);
+  k_dot_chunk<<<nb, kDotThreads, 0, st>>>(a, b, n, scratch);
+  k_dot_final<<<1, 32, 0, st>>>(scratch, nb, scratch + kNaMaxPartials);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(result, scratch + kNaMaxPartials, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    g_create_err = std::string("ds2d_dot_f64_noalloc: ") + cudaGetErrorString(e);
+    return DS2D_E_CUDA;
+  }
+  return DS2D_OK;
+}

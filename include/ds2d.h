@@ -146,6 +146,24 @@ int ds2d_lsrtm(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *obs_vz
  * deterministic.  Runs on the context stream and returns after the result is on the host. */
 int ds2d_dot_f64(ds2d_ctx *ctx, const float *a, const float *b, long long n, double *result);
 
+/* The same FP64 inner product with no context and no device allocation (no counterpart in the
+ * reference, which has no device-side reduction).  For callers that cannot allocate device
+ * memory when they need the product: a host framework that owns the device memory budget, a
+ * caller with no ds2d context, or one running with the HBM already full.  The partial sums live
+ * in a static device array of the library (256 KiB per device), so:
+ *  - n is limited to 536,870,912 elements (32768 partial sums of 16384 elements each); a larger
+ *    n returns DS2D_E_ARG with a message, and nothing is launched;
+ *  - the first call on a device looks up that array's address with the device current (and may
+ *    load the library's module there), so make it before any stream capture on that device;
+ *  - calls on the same device that overlap in time (other host threads, or streams whose work
+ *    runs concurrently) share the array and race: serialise them.
+ * Runs on `stream` (NULL = the legacy default stream) of the current device and returns after
+ * the result is on the host.  Errors are reported by ds2d_last_error(NULL).  Summation order
+ * differs from ds2d_dot_f64 (contiguous chunks instead of a grid stride), so the two agree to
+ * FP64 rounding, not bit for bit. */
+int ds2d_dot_f64_noalloc(const float *a, const float *b, long long n, void *stream,
+                         double *result);
+
 /* Tuning knobs (no counterpart in the reference, whose launch shape is fixed at 32x32 blocks,
  * FD2DGPU.cuh:8-9): "fused" (1 = single-pass fused time step, 0 = one launch per half step)
  * and "xr" (rows marched by one CTA of the fused kernels). */
