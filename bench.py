@@ -132,12 +132,15 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_for(kernel):
-    """DRAM bytes per launch of `kernel` from a committed ncu capture summary, else None."""
+def traffic_for(kernel, shots):
+    """DRAM bytes (read + write) per launch of `kernel` over `shots` resident shots, from the
+    per-shot figure of a committed ncu capture (profiles/traffic.json), else None.  A launch
+    advances every resident shot by one step, so its traffic scales with the shot count."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(kernel)
+            per_shot = json.load(f)[kernel]["dram_bytes_per_shot"]
+        return round(per_shot * shots)
     except Exception:
         return None
 
@@ -238,7 +241,7 @@ def run_ours(args, rank, world, dist):
         achieved = by / n / (kms / n / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": src,
-                "traffic": traffic_for(name), "share": round(kms / tot, 4),
+                "traffic": traffic_for(name, c["shots"]), "share": round(kms / tot, 4),
                 "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
                                 "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else None}
                             for k, v in rep.items()}}
