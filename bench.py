@@ -92,15 +92,21 @@ class Clocks:
                 "samples": len(self.rows)}
 
 
-def workload(args, rank):
+def workload(args, rank, world=1):
+    """One model for all ranks; a survey of `shots` x world shots, of which this rank takes its
+    cost-balanced shard (weak scaling: `shots` per GPU)."""
     from ds2d_b200 import synth
+    from ds2d_b200.shard import shard_shots
     c = dict(CFG)
     c["nt"] = args.nt
     c["shots"] = args.shots
-    vp, vs = synth.dipping_lenses(c["allnx"], c["allnz"], seed=c["seed"] + rank)
+    vp, vs = synth.dipping_lenses(c["allnx"], c["allnz"], seed=c["seed"])
     vpm, vsm = synth.smooth(vp, 15.0), synth.smooth(vs, 15.0)
     w = synth.ricker(c["nt"], c["f0"], c["dt"])
-    shots = synth.surface_shots(c["allnx"], c["allnx"], c["pml"], c["shots"], sz=c["sz"], gz=c["gz"])
+    survey = synth.surface_shots(c["allnx"], c["allnx"], c["pml"], c["shots"] * world, sz=c["sz"],
+                                 gz=c["gz"])
+    mine = shard_shots(survey, world, rank, c["allnx"], c["pml"], c["allnz"] + 2 * c["pml"], c["nt"])
+    shots = [survey[i] for i in mine]
     return c, vp, vs, vpm, vsm, w, shots
 
 
@@ -148,7 +154,7 @@ def traffic_for(kernel, shots):
 def run_ours(args, rank, world, dist):
     import torch
     from ds2d_b200 import Elastic2D
-    c, vp, vs, vpm, vsm, w, shots = workload(args, rank)
+    c, vp, vs, vpm, vsm, w, shots = workload(args, rank, world)
     dev = torch.cuda.current_device()
     ntr = shots[0].ntr
     # Observed data: PML forward modelling on the true model (set-up, untimed).
@@ -179,11 +185,11 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize()
 
     def allreduce_images():
+        # the one exchange step of the path: the images summed over every rank's shots
         if dist is not None:
+            from ds2d_b200.shard import reduce_images
             imgs = e.read_images(reset=True, which=("pp_grad", "ps_grad", "illumination"))
-            t = torch.from_numpy(np.stack(list(imgs.values()))).to(dev)
-            dist.all_reduce(t)
-            return t
+            return reduce_images(imgs, dist, device=dev)
         return None
 
     # warm-up
