@@ -24,6 +24,42 @@ using namespace ds2d;
 
 namespace {
 
+// Ring depths the fused kernels are instantiated for, and the default (option "ring").
+constexpr int kRingDepths[3] = {2, 4, 8};
+constexpr int kDefaultRing = 4;
+
+using FwdFn = void (*)(FwdFusedArgs);
+using BwdFn = void (*)(BwdFusedArgs);
+
+// Fused ring kernels by boundary, ring depth and occupancy target (option "occ": 0 = registers
+// for 6 forward / 3 backward CTAs per SM, 1 = capped for 8 forward / 4 backward CTAs per SM).
+template <int kD, int kF, int kB>
+FwdFn fwd_pick(bool rbc) { return rbc ? k_fwd_ring<false, kD, kF> : k_fwd_ring<true, kD, kF>; }
+template <int kD, int kF, int kB>
+BwdFn bwd_pick(bool rbc) { return rbc ? k_bwd_ring<false, kD, kB> : k_bwd_ring<true, kD, kB>; }
+
+FwdFn fwd_ring_fn(bool rbc, int depth, int occ = 0) {
+  switch (depth * 2 + (occ ? 1 : 0)) {
+    case 4: return fwd_pick<2, 6, 3>(rbc);
+    case 5: return fwd_pick<2, 8, 4>(rbc);
+    case 8: return fwd_pick<4, 6, 3>(rbc);
+    case 9: return fwd_pick<4, 8, 4>(rbc);
+    case 17: return fwd_pick<8, 8, 4>(rbc);
+    default: return fwd_pick<8, 6, 3>(rbc);
+  }
+}
+
+BwdFn bwd_ring_fn(bool rbc, int depth, int occ = 0) {
+  switch (depth * 2 + (occ ? 1 : 0)) {
+    case 4: return bwd_pick<2, 6, 3>(rbc);
+    case 5: return bwd_pick<2, 8, 4>(rbc);
+    case 8: return bwd_pick<4, 6, 3>(rbc);
+    case 9: return bwd_pick<4, 8, 4>(rbc);
+    case 17: return bwd_pick<8, 8, 4>(rbc);
+    default: return bwd_pick<8, 6, 3>(rbc);
+  }
+}
+
 // Setup of one batch of slots: window of the full model with edge replication
 // (FD2DGPU.cu:122-138, :234-250), optional project random band, PML damping (:444-494, profile
 // ((pml-i)/pml)^4 scaled by log10(1/rr) * 5 vp / (2 pml)), moduli with the reference's rho
@@ -182,9 +218,10 @@ struct ds2d_ctx {
   bool have_elsrtm = false, have_rtm = false;
   // Tuning knobs (ds2d_set_option): fused single-pass forward step, rows per CTA of the fused
   // kernels.
-  int opt_fused = 1, opt_xr = 64;
+  int opt_fused = 1, opt_xr = 128;
   int opt_adjoint_born = 0;  // scattered adjoint of ELSRTM (off = the reference's observed runs)
-  int opt_ring = 1;          // cp.async ring-fed fused kernels
+  int opt_ring = kDefaultRing;  // cp.async ring depth of the fused kernels (0 = no ring)
+  int opt_occ = 0;           // occupancy target of the ring kernels (see fwd_ring_fn)
   // Acoustic Born pair (LSRTM): background, scattered and adjoint states, Born overlay.
   float *ac[10] = {};        // bvx bvz bs | dvx dvz ds | yx yz ys | e
   double *dot_part = nullptr, *dot_out = nullptr;  // FP64 inner-product scratch
@@ -507,11 +544,9 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
     a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
     if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
     if (c->opt_ring) {
-      const size_t sm = sizeof(float) * kRing * kFwdRingFields * kFB;
-      if (d.rbc)
-        LAUNCHS("fwd_fused", kBytesFused * CELLS(n), k_fwd_ring<false>, grid, kFB, sm, a);
-      else
-        LAUNCHS("fwd_fused", kBytesFused * CELLS(n), k_fwd_ring<true>, grid, kFB, sm, a);
+      const size_t sm = sizeof(float) * c->opt_ring * kFwdRingFields * kFB;
+      FwdFn kfn = fwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ);
+      LAUNCHS("fwd_fused", kBytesFused * CELLS(n), kfn, grid, kFB, sm, a);
     } else if (d.rbc) {
       LAUNCHP("fwd_fused", kBytesFused * CELLS(n), k_fwd_fused<false>, grid, kFB, a);
     } else {
@@ -640,7 +675,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring, c->opt_xr, (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ, c->opt_xr, (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -677,11 +712,9 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
       a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
       a.img = c->img_slot; a.img_plane = (long long)plane;
       if (c->opt_ring) {
-        const size_t sm = sizeof(float) * kRing * kBwdRingFields * kFB;
-        if (d.rbc)
-          LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_ring<false>, fgrid, kFB, sm, a);
-        else
-          LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_ring<true>, fgrid, kFB, sm, a);
+        const size_t sm = sizeof(float) * c->opt_ring * kBwdRingFields * kFB;
+        BwdFn kfn = bwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ);
+        LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, fgrid, kFB, sm, a);
       } else if (d.rbc) {
         LAUNCHP("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_fused<false>, fgrid, kFB, a);
       } else {
@@ -1043,19 +1076,23 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
   d.nseg_max = d.nseg;
   c->B = opts->max_shots;
   {
-    // Ring-fed kernels use more than the default 48 KB of dynamic shared memory.
-    const int fwd_sm = (int)(sizeof(float) * kRing * kFwdRingFields * kFB);
-    cudaError_t ea = cudaFuncSetAttribute(k_fwd_ring<true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_sm);
-    cudaError_t eb = cudaFuncSetAttribute(k_fwd_ring<false>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_sm);
-    const int bwd_sm = (int)(sizeof(float) * kRing * kBwdRingFields * kFB);
-    if (ea == cudaSuccess)
-      ea = cudaFuncSetAttribute(k_bwd_ring<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sm);
-    if (eb == cudaSuccess)
-      eb = cudaFuncSetAttribute(k_bwd_ring<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sm);
-    if (ea != cudaSuccess || eb != cudaSuccess) {
-      g_create_err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea != cudaSuccess ? ea : eb);
+    // Ring-fed kernels may use more than the default 48 KB of dynamic shared memory.
+    cudaError_t e = cudaSuccess;
+    for (int depth : kRingDepths) {
+      const int fwd_sm = (int)(sizeof(float) * depth * kFwdRingFields * kFB);
+      const int bwd_sm = (int)(sizeof(float) * depth * kBwdRingFields * kFB);
+      for (bool rbc : {false, true})
+        for (int occ : {0, 1}) {
+          if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(fwd_ring_fn(rbc, depth, occ),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_sm);
+          if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(bwd_ring_fn(rbc, depth, occ),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sm);
+        }
+    }
+    if (e != cudaSuccess) {
+      g_create_err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
       delete c;
       return DS2D_E_CUDA;
     }
@@ -1162,7 +1199,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring, c->opt_xr, (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ, c->opt_xr, (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -1401,7 +1438,13 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
   } else if (k == "graph") {
     c->opt_graph = value != 0;
   } else if (k == "ring") {
-    c->opt_ring = value != 0;
+    if (value == 1) value = kDefaultRing;
+    if (value != 0 && value != 2 && value != 4 && value != 8)
+      return fail(c, DS2D_E_ARG, "ring must be 0 (off), 1 (default depth) or a depth of 2, 4 or 8");
+    c->opt_ring = (int)value;
+  } else if (k == "occ") {
+    if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "occ must be 0 or 1");
+    c->opt_occ = (int)value;
   } else if (k == "xr") {
     if (value < 8 || value > 4096) return fail(c, DS2D_E_ARG, "xr must be in [8, 4096]");
     c->opt_xr = (int)value;

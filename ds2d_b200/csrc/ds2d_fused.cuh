@@ -193,14 +193,15 @@ __global__ void __launch_bounds__(kFB) k_fwd_fused(FwdFusedArgs a) {
 
 // ---------------------------------------------------------------------------------------------
 // Asynchronous row prefetch for the row-marching kernels.  Every per-row operand of a thread's
-// column is copied global -> shared with cp.async (LDGSTS) kRingAhead row steps before it is
-// used.  Ring slot q (q mod kRing) holds everything row step q consumes: the stage-1 stencil
-// inputs of row q, the stage-1 own-cell operands of row q-4 and the stage-2 operands of row q-8,
-// issued together as one commit group at step q - kRingAhead.  A thread only ever reads ring
-// entries it copied itself, so cp.async.wait_group alone orders them (no barrier), and the ring
-// only needs kRingAhead + 1 slots however long the lags are.
-constexpr int kRing = 8;
-constexpr int kRingAhead = 6;
+// column is copied global -> shared with cp.async (LDGSTS) kD - 1 row steps before it is used
+// (kD = ring depth, a power of two, a template parameter of the kernels).  Ring slot q (q mod kD)
+// holds everything row step q consumes: the stage-1 stencil inputs of row q, the stage-1
+// own-cell operands of row q-4 and the stage-2 operands of row q-8, issued together as one commit
+// group at step q - (kD - 1), into the slot row step q - 1 has just finished with.  A thread only
+// ever reads ring entries it copied itself, so cp.async.wait_group alone orders them (no
+// barrier), and kD slots suffice however long the lags are.  The prefetch distance needed is a
+// few microseconds of DRAM latency; one row step of a CTA takes about as long, so a shallow ring
+// (kD = 4) hides it while leaving shared memory for more resident CTAs.
 
 __device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -219,9 +220,10 @@ __device__ __forceinline__ void cp_async_wait() {
 // 6 lam, 7 mu of row q-8 (stress stage).
 constexpr int kFwdRingFields = 8;
 
-template <bool kPML>
-__global__ void __launch_bounds__(kFB) k_fwd_ring(FwdFusedArgs a) {
-  extern __shared__ float ring[];  // [kRing][kFwdRingFields][kFB]
+template <bool kPML, int kD, int kMinB>
+__global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
+  static_assert(kD >= 2 && (kD & (kD - 1)) == 0, "ring depth: a power of two");
+  extern __shared__ float ring[];  // [kD][kFwdRingFields][kFB]
   __shared__ float s_txz[kFB], s_tzz[kFB], s_vx[kFB], s_vz[kFB];
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(kFB) k_fwd_ring(FwdFusedArgs a) {
                                       a.a.vz, a.p.b,   a.p.lam, a.p.mu};
   // R(q, f): field f of ring slot q (row q for f < 3, row q-4 for f < 6, row q-8 otherwise)
   auto R = [&](int q, int f) -> float & {
-    return ring[((q & (kRing - 1)) * kFwdRingFields + f) * kFB + t];
+    return ring[((q & (kD - 1)) * kFwdRingFields + f) * kFB + t];
   };
   auto issue = [&](int q) {
 #pragma unroll
@@ -261,9 +263,9 @@ __global__ void __launch_bounds__(kFB) k_fwd_ring(FwdFusedArgs a) {
   for (int i = 0; i < 9; i++) w_txx[i] = w_tzz[i] = w_txz[i] = w_vx[i] = w_vz[i] = 0.f;
 
 #pragma unroll
-  for (int j = 0; j < kRingAhead; j++) issue(x0 - 8 + j);
+  for (int j = 0; j < kD - 1; j++) issue(x0 - 8 + j);
   for (int r = x0 - 8; r < x1 + 8; r++) {
-    cp_async_wait<kRingAhead - 1>();  // row r has landed (this thread's copies)
+    cp_async_wait<kD - 2>();  // row r has landed (this thread's copies)
     float n_txx = R(r, 0), n_tzz = R(r, 1);
     const float n_txz = R(r, 2);
     if (src_col && r == sh.isx) {  // FD2DGPU.cu:2039-2049 (transient)
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(kFB) k_fwd_ring(FwdFusedArgs a) {
     push(w_txx, n_txx);
     push(w_tzz, n_tzz);
     push(w_txz, n_txz);
-    issue(r + kRingAhead);
+    issue(r + kD - 1);  // into the slot of row r - 1 (mod kD), finished last step
     // ---- velocities of row rv = r - 4 --------------------------------------------------
     const int rv = r - 4;
     s_txz[t] = w_txz[4];
@@ -415,6 +417,7 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
   const float *res_x = a.res_vx + (long long)s * d.max_ntr * d.nt + a.it;
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
 
   // stage-1 inputs (velocities at t, rows r-8..r)
   float w_bvx[9], w_bvz[9], w_avx[9], w_avz[9];
@@ -484,10 +487,10 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
         btxx = btxx + (dir * l2m * dtdx * sa + dir * lam * dtdz * sb);
         btzz = btzz + (dir * lam * dtdx * sa + dir * l2m * dtdz * sb);
         btxz = btxz + (dir * mu * dtdx * sf + dir * mu * dtdz * se);
-        gx_vx = sa / d.dx;
-        gz_vz = sb / d.dz;
-        gz_vx = se / d.dz;
-        gx_vz = sf / d.dx;
+        gx_vx = sa * rdx;  // strains; reciprocal multiply (the division's slow path is taken
+        gz_vz = sb * rdz;  // for the tiny amplitudes ahead of a wavefront)
+        gz_vx = se * rdz;
+        gx_vz = sf * rdx;
         if (own) {
           a.rb.txx[k] = btxx;
           a.rb.tzz[k] = btzz;
@@ -621,9 +624,10 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
 //  16-17 b, img illumination of row q-8          (stage 2)
 constexpr int kBwdRingFields = 18;
 
-template <bool kPML>
-__global__ void __launch_bounds__(kFB) k_bwd_ring(BwdFusedArgs a) {
-  extern __shared__ float ring[];  // [kRing][kBwdRingFields][kFB]
+template <bool kPML, int kD, int kMinB>
+__global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
+  static_assert(kD >= 2 && (kD & (kD - 1)) == 0, "ring depth: a power of two");
+  extern __shared__ float ring[];  // [kD][kBwdRingFields][kFB]
   __shared__ float s_bvx[kFB], s_bvz[kFB], s_avx[kFB], s_avz[kFB];
   __shared__ float s_btxz[kFB], s_btzz[kFB], s_m[kFB], s_pz[kFB], s_lx[kFB];
   const int s = blockIdx.z, t = threadIdx.x;
@@ -644,13 +648,14 @@ __global__ void __launch_bounds__(kFB) k_bwd_ring(BwdFusedArgs a) {
   const float *res_x = a.res_vx + (long long)s * d.max_ntr * d.nt + a.it;
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
   const long long img_row = (long long)s * d.wnx_max;  // image row of model row r: img_row + r - pml
   float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
   const float *grid_src[16] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.txx, a.ra.tzz,
                                a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz, a.p.lam,  a.p.mu,
                                a.p.kpp,  a.p.kps,  a.p.b,    nullptr};
   auto R = [&](int q, int f) -> float & {
-    return ring[((q & (kRing - 1)) * kBwdRingFields + f) * kFB + t];
+    return ring[((q & (kD - 1)) * kBwdRingFields + f) * kFB + t];
   };
   auto issue = [&](int q) {
 #pragma unroll
@@ -685,9 +690,9 @@ __global__ void __launch_bounds__(kFB) k_bwd_ring(BwdFusedArgs a) {
   for (int i = 0; i < 5; i++) w_btzz[i] = w_Pz[i] = w_Lx[i] = 0.f;
 
 #pragma unroll
-  for (int j = 0; j < kRingAhead; j++) issue(x0 - 8 + j);
+  for (int j = 0; j < kD - 1; j++) issue(x0 - 8 + j);
   for (int r = x0 - 8; r < x1 + 8; r++) {
-    cp_async_wait<kRingAhead - 1>();  // slot r has landed (this thread's copies)
+    cp_async_wait<kD - 2>();  // slot r has landed (this thread's copies)
     {
       float n_bvx = R(r, 0), n_bvz = R(r, 1), n_avx = R(r, 2), n_avz = R(r, 3);
       if (r >= 0 && r < d.nxp && zin) {
@@ -711,9 +716,8 @@ __global__ void __launch_bounds__(kFB) k_bwd_ring(BwdFusedArgs a) {
       push(w_avx, n_avx);
       push(w_avz, n_avz);
     }
-    // Refill slot r + kRingAhead (= slot r - 2, last read two rows ago); only slot r is read
-    // below.
-    issue(r + kRingAhead);
+    // Refill the slot of row r - 1 (mod kD) with row r + kD - 1; only slot r is read below.
+    issue(r + kD - 1);
     // ---- stage 1: stresses of row r1 = r - 4 -----------------------------------------------
     const int r1 = r - 4;
     s_bvx[t] = w_bvx[4];
@@ -741,10 +745,10 @@ __global__ void __launch_bounds__(kFB) k_bwd_ring(BwdFusedArgs a) {
         btxx = btxx + (dir * l2m * dtdx * sa + dir * lam * dtdz * sb);
         btzz = btzz + (dir * lam * dtdx * sa + dir * l2m * dtdz * sb);
         btxz = btxz + (dir * mu * dtdx * sf + dir * mu * dtdz * se);
-        gx_vx = sa / d.dx;
-        gz_vz = sb / d.dz;
-        gz_vx = se / d.dz;
-        gx_vz = sf / d.dx;
+        gx_vx = sa * rdx;  // strains; reciprocal multiply (the division's slow path is taken
+        gz_vz = sb * rdz;  // for the tiny amplitudes ahead of a wavefront)
+        gz_vx = se * rdz;
+        gx_vz = sf * rdx;
         if (own) {
           a.rb.txx[k] = btxx;
           a.rb.tzz[k] = btzz;

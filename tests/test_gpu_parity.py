@@ -144,7 +144,7 @@ def test_elsrtm_adjoint_born_as_written(cuda_device):
 
 @pytest.mark.parametrize("boundary", ["pml", "random"])
 @pytest.mark.parametrize("xr", [16, 64])
-@pytest.mark.parametrize("ring", [0, 1])
+@pytest.mark.parametrize("ring", [0, 2, 4, 8])
 def test_fused_step_matches_half_steps(cuda_device, boundary, xr, ring):
     c, vp, vs, w, shots = small_case(nt=300)
     out = {}
@@ -158,6 +158,24 @@ def test_fused_step_matches_half_steps(cuda_device, boundary, xr, ring):
             rz, rx = e.forward(shots)
             e.rtm(shots, rz, rx)
             out[fused] = (rz, rx, e.read_images())
+    assert rel(out[1][0], out[0][0]) < 1e-6 and rel(out[1][1], out[0][1]) < 1e-6
+    for key in ("pp_grad", "ps_grad", "illumination"):
+        assert rel(out[1][2][key], out[0][2][key]) < 1e-6, key
+
+
+@pytest.mark.parametrize("boundary", ["pml", "random"])
+def test_ring_occupancy_variants_agree(cuda_device, boundary):
+    """Register-capped ring kernels (8 forward / 4 backward CTAs per SM) against the default."""
+    c, vp, vs, w, shots = small_case(nt=300)
+    out = {}
+    for occ in (0, 1):
+        with _ctx(c, shots, boundary=boundary, seed=5) as e:
+            e.set_option("occ", occ)
+            e.set_models(vp, vs)
+            e.set_wavelet(w)
+            rz, rx = e.forward(shots)
+            e.rtm(shots, rz, rx)
+            out[occ] = (rz, rx, e.read_images())
     assert rel(out[1][0], out[0][0]) < 1e-6 and rel(out[1][1], out[0][1]) < 1e-6
     for key in ("pp_grad", "ps_grad", "illumination"):
         assert rel(out[1][2][key], out[0][2][key]) < 1e-6, key
