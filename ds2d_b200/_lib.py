@@ -26,6 +26,9 @@ EXPORTS = [
     "ds2d_rtm_device", "ds2d_read_images", "ds2d_last_cell_updates", "ds2d_last_launches",
     "ds2d_profile", "ds2d_profile_report", "ds2d_set_option", "ds2d_ac_born",
     "ds2d_ac_born_adj", "ds2d_lsrtm", "ds2d_dot_f64", "ds2d_dot_f64_noalloc",
+    "ds2d_ac_normal", "ds2d_lsrtm_pcg", "ds2d_unet_create", "ds2d_unet_destroy", "ds2d_unet_last_error", "ds2d_unet_set_stream",
+    "ds2d_unet_num_params", "ds2d_unet_set_params", "ds2d_unet_get_params", "ds2d_unet_forward",
+    "ds2d_unet_loss_grad", "ds2d_unet_adam_step",
 ]
 
 
@@ -88,6 +91,19 @@ def load():
         "ds2d_set_option": ([P, ctypes.c_char_p, ctypes.c_longlong], ctypes.c_int),
         "ds2d_dot_f64": ([P, P, P, ctypes.c_longlong, dp], ctypes.c_int),
         "ds2d_dot_f64_noalloc": ([P, P, ctypes.c_longlong, P, dp], ctypes.c_int),
+        "ds2d_ac_normal": ([P, ctypes.POINTER(Shot), ctypes.c_int, P, P], ctypes.c_int),
+        "ds2d_lsrtm_pcg": ([P, P, ctypes.POINTER(Shot), ctypes.c_int, P, P, ctypes.c_int,
+                            ctypes.c_double, P, dp, dp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "ds2d_unet_create": ([ctypes.c_int] * 5 + [ctypes.POINTER(P)], ctypes.c_int),
+        "ds2d_unet_destroy": ([P], ctypes.c_int),
+        "ds2d_unet_last_error": ([P], ctypes.c_char_p),
+        "ds2d_unet_set_stream": ([P, P], ctypes.c_int),
+        "ds2d_unet_num_params": ([P], ctypes.c_longlong),
+        "ds2d_unet_set_params": ([P, fp, ctypes.c_longlong], ctypes.c_int),
+        "ds2d_unet_get_params": ([P, fp, ctypes.c_longlong], ctypes.c_int),
+        "ds2d_unet_forward": ([P, P, P] + [ctypes.c_int] * 3, ctypes.c_int),
+        "ds2d_unet_loss_grad": ([P, P, P] + [ctypes.c_int] * 3 + [dp, fp], ctypes.c_int),
+        "ds2d_unet_adam_step": ([P] + [ctypes.c_float] * 4, ctypes.c_int),
         "ds2d_ac_born": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, fp], ctypes.c_int),
         "ds2d_ac_born_adj": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, fp], ctypes.c_int),
         "ds2d_lsrtm": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, ctypes.c_int,

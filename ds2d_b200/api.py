@@ -195,7 +195,33 @@ class Elastic2D:
                                         ctypes.byref(done)))
         return m, hist[:done.value]
 
-    IMAGE_NAMES = ("pp_grad", "ps_grad", "illumination", "b_pp", "b_ps", "b_pp2", "b_ps2")
+    def ac_normal_device(self, shots, m_ptr, img_ptr):
+        """img = L^T L m on model-size device arrays (integer device pointers)."""
+        arr, keep = self._shots(shots)
+        self._check(self.lib.ds2d_ac_normal(self.h, arr, len(shots), ctypes.c_void_p(m_ptr),
+                                            ctypes.c_void_p(img_ptr)))
+
+    def ac_born_device(self, shots, m_ptr, rz_ptr, rx_ptr):
+        """d = L m with m and the records [sum ntr][nt] in device memory."""
+        arr, keep = self._shots(shots)
+        self._check(self.lib.ds2d_ac_born(self.h, arr, len(shots), ctypes.c_void_p(m_ptr),
+                                          ctypes.c_void_p(rz_ptr), ctypes.c_void_p(rx_ptr)))
+
+    def lsrtm_pcg(self, shots, obs_vz_ptr, obs_vx_ptr, m_ptr, niter, target=0.0, net=None):
+        """Flexible preconditioned CG-LSRTM on device arrays; net = ds2d_b200.unet.UNet or None
+        (plain CG).  Returns (relative residual per iteration, wall ms per iteration)."""
+        arr, keep = self._shots(shots)
+        hist = np.zeros(max(niter, 1))
+        ms = np.zeros(max(niter, 1))
+        done = ctypes.c_int(0)
+        dp = ctypes.POINTER(ctypes.c_double)
+        self._check(self.lib.ds2d_lsrtm_pcg(
+            self.h, net.h if net is not None else None, arr, len(shots), ctypes.c_void_p(obs_vz_ptr),
+            ctypes.c_void_p(obs_vx_ptr), int(niter), float(target), ctypes.c_void_p(m_ptr),
+            hist.ctypes.data_as(dp), ms.ctypes.data_as(dp), ctypes.byref(done)))
+        return hist[:done.value], ms[:done.value]
+
+    IMAGE_NAMES =("pp_grad", "ps_grad", "illumination", "b_pp", "b_ps", "b_pp2", "b_ps2")
 
     def read_images(self, reset=True, which=None):
         """imagebuffer_resettozero: the accumulated images as [allnx][allnz] arrays."""

@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libds2d_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "ds2d_engine.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "ds2d_engine.cu"), os.path.join(HERE, "csrc", "ds2d_unet.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
     os.path.join(ROOT, "include", "ds2d.h")]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -1294,10 +1295,11 @@ static int data_io(ds2d_ctx *c, const ds2d_shot *shots, int n, float *dev, float
   for (int s = 0; s < n; s++) {
     const size_t cnt = (size_t)shots[s].ntr * c->d.nt;
     if (cnt) {
+      // cudaMemcpyDefault: the caller's records may live in host or device memory
       if (to_dev)
-        CK(cudaMemcpyAsync(dev + s * per, host + tb * c->d.nt, cnt * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(dev + s * per, host + tb * c->d.nt, cnt * 4, cudaMemcpyDefault, c->stream));
       else
-        CK(cudaMemcpyAsync(host + tb * c->d.nt, dev + s * per, cnt * 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(host + tb * c->d.nt, dev + s * per, cnt * 4, cudaMemcpyDefault, c->stream));
     }
     tb += shots[s].ntr;
   }
@@ -1322,7 +1324,7 @@ int ds2d_ac_born(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *m, flo
   float *mv, *dz, *dx;
   if ((rc = work_vec(c, 0, nall, &mv)) || (rc = work_vec(c, 7, nd, &dz)) || (rc = work_vec(c, 8, nd, &dx)))
     return rc;
-  CK(cudaMemcpyAsync(mv, m, nall * 4, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(mv, m, nall * 4, cudaMemcpyDefault, c->stream));
   if ((rc = ac_apply(c, shots, n, false, mv, dz, dx, nullptr))) return rc;
   if ((rc = data_io(c, shots, n, dz, rec_vz, false)) || (rc = data_io(c, shots, n, dx, rec_vx, false)))
     return rc;
@@ -1348,7 +1350,7 @@ int ds2d_ac_born_adj(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *re
       (rc = data_io(c, shots, n, dx, (float *)rec_vx, true)))
     return rc;
   if ((rc = ac_apply(c, shots, n, true, nullptr, dz, dx, gv))) return rc;
-  CK(cudaMemcpyAsync(grad, gv, nall * 4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(grad, gv, nall * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return DS2D_OK;
 }
@@ -1413,7 +1415,157 @@ int ds2d_lsrtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *obs_vz,
     c->last_launches++;
   }
   if (iters_done) *iters_done = k;
-  CK(cudaMemcpyAsync(m_out, m, nall * 4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(m_out, m, nall * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+int ds2d_ac_normal(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *m, float *img) {
+  int rc;
+  if ((rc = check_ready(c, false))) return rc;
+  if (n <= 0 || !shots || !m || !img) return fail(c, DS2D_E_ARG, "bad arguments");
+  if ((rc = ensure_acoustic(c)) || (rc = check_shots(c, shots, n))) return rc;
+  c->last_launches = 0;
+  c->last_updates = 0;
+  const size_t nall = (size_t)c->d.allnx * c->d.allnz, nd = (size_t)n * c->d.max_ntr * c->d.nt;
+  float *mv, *gv, *dz, *dx;
+  if ((rc = work_vec(c, 0, nall, &mv)) || (rc = work_vec(c, 1, nall, &gv)) ||
+      (rc = work_vec(c, 7, nd, &dz)) || (rc = work_vec(c, 8, nd, &dx)))
+    return rc;
+  CK(cudaMemcpyAsync(mv, m, nall * 4, cudaMemcpyDefault, c->stream));
+  if ((rc = ac_apply(c, shots, n, false, mv, dz, dx, nullptr))) return rc;
+  if ((rc = ac_apply(c, shots, n, true, nullptr, dz, dx, gv))) return rc;
+  CK(cudaMemcpyAsync(img, gv, nall * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+__global__ void k_scale_f(long long n, float s, float *x) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] *= s;
+}
+
+// z = P(g): the U-Net applied to g / rms(g) on the model grid zero-padded to multiples of 8
+// (images [allnx][allnz] are the network's [h][w]); z = g without a network.
+int precondition(ds2d_ctx *c, ds2d_unet *net, const float *g, float *z) {
+  const Dims &d = c->d;
+  const size_t nall = (size_t)d.allnx * d.allnz;
+  if (!net) {
+    CK(cudaMemcpyAsync(z, g, nall * 4, cudaMemcpyDeviceToDevice, c->stream));
+    return DS2D_OK;
+  }
+  const int hp = (d.allnx + 7) / 8 * 8, wp = (d.allnz + 7) / 8 * 8;
+  int rc;
+  float *xin, *xout;
+  if ((rc = work_vec(c, 9, (size_t)hp * wp, &xin)) || (rc = work_vec(c, 10, (size_t)hp * wp, &xout)))
+    return rc;
+  double gg;
+  if ((rc = dot64(c, g, g, (long long)nall, &gg))) return rc;
+  if (!(gg > 0)) {
+    CK(cudaMemsetAsync(z, 0, nall * 4, c->stream));
+    return DS2D_OK;
+  }
+  CK(cudaMemsetAsync(xin, 0, (size_t)hp * wp * 4, c->stream));
+  CK(cudaMemcpy2DAsync(xin, (size_t)wp * 4, g, (size_t)d.allnz * 4, (size_t)d.allnz * 4, d.allnx,
+                       cudaMemcpyDeviceToDevice, c->stream));
+  k_scale_f<<<4 * 148, 256, 0, c->stream>>>((long long)hp * wp, (float)(1.0 / std::sqrt(gg / nall)), xin);
+  c->last_launches++;
+  if (ds2d_unet_set_stream(net, c->stream) || ds2d_unet_forward(net, xin, xout, 1, hp, wp))
+    return fail(c, DS2D_E_CUDA, "preconditioner: %s", ds2d_unet_last_error(net));
+  CK(cudaMemcpy2DAsync(z, (size_t)d.allnz * 4, xout, (size_t)wp * 4, (size_t)d.allnz * 4, d.allnx,
+                       cudaMemcpyDeviceToDevice, c->stream));
+  return DS2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ds2d_lsrtm_pcg(ds2d_ctx *c, ds2d_unet *net, const ds2d_shot *shots, int n, const float *obs_vz,
+                   const float *obs_vx, int niter, double target, float *m_out, double *resid,
+                   double *elapsed_ms, int *iters_done) {
+  int rc;
+  if ((rc = check_ready(c, false))) return rc;
+  if (n <= 0 || !shots || !obs_vz || !obs_vx || !m_out || niter < 0)
+    return fail(c, DS2D_E_ARG, "bad arguments");
+  if ((rc = ensure_acoustic(c)) || (rc = check_shots(c, shots, n))) return rc;
+  c->last_launches = 0;
+  c->last_updates = 0;
+  const auto t0 = std::chrono::steady_clock::now();
+  const size_t nall = (size_t)c->d.allnx * c->d.allnz, nd = (size_t)n * c->d.max_ntr * c->d.nt;
+  float *m, *g, *p, *gn, *z, *rz, *rx, *qz, *qx;
+  if ((rc = work_vec(c, 0, nall, &m)) || (rc = work_vec(c, 1, nall, &g)) ||
+      (rc = work_vec(c, 2, nall, &p)) || (rc = work_vec(c, 3, nall, &gn)) ||
+      (rc = work_vec(c, 4, nall, &z)) || (rc = work_vec(c, 5, nd, &rz)) ||
+      (rc = work_vec(c, 6, nd, &rx)) || (rc = work_vec(c, 7, nd, &qz)) ||
+      (rc = work_vec(c, 8, nd, &qx)))
+    return rc;
+  CK(cudaMemsetAsync(m, 0, nall * 4, c->stream));
+  CK(cudaMemsetAsync(rz, 0, nd * 4, c->stream));
+  CK(cudaMemsetAsync(rx, 0, nd * 4, c->stream));
+  if ((rc = data_io(c, shots, n, rz, (float *)obs_vz, true)) ||
+      (rc = data_io(c, shots, n, rx, (float *)obs_vx, true)))
+    return rc;
+  // Flexible preconditioned CG on || d - L m ||^2 from m = 0 (FP64 scalars):
+  //   g = L^T r, z = P(g), p = z + beta p with Polak-Ribiere+ beta = max(0, <z, g - g_prev>) /
+  //   <z_prev, g_prev>, and the exact step alpha = <r, L p> / ||L p||^2 along p.  With P = I this
+  //   is CG (Polak-Ribiere equals Fletcher-Reeves on a quadratic with exact line search); with
+  //   the network it stays a descent method whatever P does, since alpha is exact.
+  double dd, tz, tx;
+  if ((rc = dot64(c, rz, rz, nd, &tz)) || (rc = dot64(c, rx, rx, nd, &tx))) return rc;
+  dd = tz + tx;
+  if (!(dd > 0)) return fail(c, DS2D_E_NUMERIC, "observed data are zero or not finite");
+  if ((rc = ac_apply(c, shots, n, true, nullptr, rz, rx, g))) return rc;
+  if ((rc = precondition(c, net, g, z))) return rc;
+  CK(cudaMemcpyAsync(p, z, nall * 4, cudaMemcpyDeviceToDevice, c->stream));
+  double zg;
+  if ((rc = dot64(c, z, g, nall, &zg))) return rc;
+  const int nb = 4 * 148;
+  int k = 0;
+  for (; k < niter; k++) {
+    if ((rc = ac_apply(c, shots, n, false, p, qz, qx, nullptr))) return rc;
+    double rq_z, rq_x;
+    if ((rc = dot64(c, qz, qz, nd, &tz)) || (rc = dot64(c, qx, qx, nd, &tx)) ||
+        (rc = dot64(c, rz, qz, nd, &rq_z)) || (rc = dot64(c, rx, qx, nd, &rq_x)))
+      return rc;
+    const double qq = tz + tx;
+    if (!(qq > 0) || !std::isfinite(rq_z + rq_x))
+      return fail(c, DS2D_E_NUMERIC, "PCG breakdown at %d", k);
+    const double alpha = (rq_z + rq_x) / qq;
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nall, alpha, p, m);
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -alpha, qz, rz);
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -alpha, qx, rx);
+    c->last_launches += 3;
+    if ((rc = dot64(c, rz, rz, nd, &tz)) || (rc = dot64(c, rx, rx, nd, &tx))) return rc;
+    const double rel = std::sqrt((tz + tx) / dd);
+    if (resid) resid[k] = rel;
+    if (elapsed_ms)
+      elapsed_ms[k] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (rel <= target) {
+      k++;
+      break;
+    }
+    if (k + 1 == niter) {
+      k++;
+      break;
+    }
+    if ((rc = ac_apply(c, shots, n, true, nullptr, rz, rx, gn))) return rc;
+    if ((rc = precondition(c, net, gn, z))) return rc;
+    double zgn, zgo;
+    if ((rc = dot64(c, z, gn, nall, &zgn)) || (rc = dot64(c, z, g, nall, &zgo))) return rc;
+    const double beta = std::max(0.0, (zgn - zgo) / zg);
+    zg = zgn;
+    k_xpby<<<nb, 256, 0, c->stream>>>((long long)nall, z, beta, p);
+    c->last_launches++;
+    std::swap(g, gn);
+  }
+  if (iters_done) *iters_done = k;
+  CK(cudaMemcpyAsync(m_out, m, nall * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return DS2D_OK;
 }

@@ -1,0 +1,855 @@
+// Image-domain U-Net preconditioner on sm_100a: BF16 tensor-core (mma.sync m16n8k16, FP32
+// accumulate) convolution kernels for inference and training, with the host orchestration of the
+// network, its Adam optimiser and its C ABI (include/ds2d.h, ds2d_unet_*).
+//
+// The reference has no learned component; the network approximates the inverse Hessian of the
+// Born operator (maps an RTM image to reflectivity) and preconditions CG-LSRTM.  Architecture
+// (identical to the FP64 oracle that checks it): 4-level encoder-decoder, base 32 channels,
+// conv3x3 + ReLU pairs, 2x2 average pooling, nearest 2x upsampling, skip concatenation, 1x1 output
+// convolution.  Activations and gradients are BF16 NHWC (channels last); weights keep an FP32
+// master copy (Adam) and BF16 copies laid out [tap][cout][cin] for the forward product and
+// [tap][cin][cout] (spatially flipped) for the backward-data product.
+//
+// Every 3x3 convolution, forward and both backward products, is an implicit GEMM on the tensor
+// cores:
+//   forward      out[p][co]  = sum_{tap,ci} in[p + tap][ci] * W[tap][co][ci]
+//   backward     dx[p][ci]   = sum_{tap,co} dz[p - tap][co] * W[tap][co][ci]  (= forward with the
+//                              flipped, transposed weights)
+//   weight grad  dW[tap][co][ci] = sum_p dz[p][co] * x[p + tap][ci]   (K = pixels, split over CTAs)
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ds2d.h"
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+// ---------------------------------------------------------------------------------------------
+// Tensor-core primitive: D = A(16x16, row) * B(16x8, col) + C, BF16 in, FP32 accumulate.
+// Fragment ownership (lane = 4 g + t): A regs {(g,2t..), (g+8,2t..), (g,2t+8..), (g+8,2t+8..)};
+// B regs {(k 2t.., n g), (k 2t+8.., n g)}; C {(g, 2t), (g, 2t+1), (g+8, 2t), (g+8, 2t+1)}.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void mma16816(float (&c)[4], const unsigned (&a)[4], unsigned b0,
+                                         unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ unsigned ld32(const bf16 *p) {
+  return *reinterpret_cast<const unsigned *>(p);
+}
+
+// ---------------------------------------------------------------------------------------------
+// 3x3 'same' convolution as an implicit GEMM.  CTA tile: 32 pixels of one image row x kCo output
+// channels; warps 2 (pixels) x kCo/32 (channels), each warp 16 pixels x 32 channels (4 MMA n-tiles).
+// K loop: input channels in chunks of 16, 9 taps per chunk.  Staging through shared memory with a
+// 24-half row stride (conflict-free 32-bit fragment loads).
+// ---------------------------------------------------------------------------------------------
+constexpr int kPx = 32;  // pixels per CTA tile
+constexpr int kSS = 24;  // shared row stride in halves (16 channels + 8 pad)
+
+struct ConvArgs {
+  const bf16 *in;   // [N][H][W][cin]
+  const bf16 *wt;   // [9][cout][cin]
+  const float *bias;  // [cout] or null
+  bf16 *out;        // [N][H][W][ocs], channels [oco, oco + cout)
+  float *out_f32;   // optional FP32 copy, same indexing as out
+  const bf16 *mask; // optional: out *= (mask > 0), mask [N][H][W][ocs] at the same channels
+  int n, h, w, cin, cout, ocs, oco, relu;
+};
+
+template <int kCo>
+__global__ void __launch_bounds__(64 * (kCo / 32)) k_conv3x3(ConvArgs a) {
+  __shared__ __align__(16) bf16 s_in[3][kPx + 2][kSS];
+  __shared__ __align__(16) bf16 s_w[9][kCo][kSS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wp = warp & 1, wc = warp >> 1;
+  const int w0 = blockIdx.x * kPx, row = blockIdx.y;
+  const int ngrp = a.cout / kCo;
+  const int img = blockIdx.z / ngrp, co0 = (blockIdx.z % ngrp) * kCo;
+  constexpr int kThreads = 64 * (kCo / 32);
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+
+  for (int ci0 = 0; ci0 < a.cin; ci0 += 16) {
+    // input halo tile: 3 rows x 34 pixels x 16 channels (two 16-byte vectors per pixel)
+    for (int i = tid; i < 3 * (kPx + 2) * 2; i += kThreads) {
+      const int half = i & 1, px = (i >> 1) % (kPx + 2), r = (i >> 1) / (kPx + 2);
+      const int hh = row + r - 1, ww = w0 + px - 1;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (hh >= 0 && hh < a.h && ww >= 0 && ww < a.w)
+        v = *reinterpret_cast<const uint4 *>(
+            a.in + (((long long)img * a.h + hh) * a.w + ww) * a.cin + ci0 + half * 8);
+      *reinterpret_cast<uint4 *>(&s_in[r][px][half * 8]) = v;
+    }
+    // weights: 9 taps x kCo couts x 16 channels
+    for (int i = tid; i < 9 * kCo * 2; i += kThreads) {
+      const int half = i & 1, co = (i >> 1) % kCo, tap = (i >> 1) / kCo;
+      const uint4 v = *reinterpret_cast<const uint4 *>(
+          a.wt + ((long long)tap * a.cout + co0 + co) * a.cin + ci0 + half * 8);
+      *reinterpret_cast<uint4 *>(&s_w[tap][co][half * 8]) = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int tap = 0; tap < 9; tap++) {
+      const int ky = tap / 3, kx = tap % 3;
+      const int p = wp * 16 + g + kx;
+      unsigned fa[4];
+      fa[0] = ld32(&s_in[ky][p][2 * t]);
+      fa[1] = ld32(&s_in[ky][p + 8][2 * t]);
+      fa[2] = ld32(&s_in[ky][p][2 * t + 8]);
+      fa[3] = ld32(&s_in[ky][p + 8][2 * t + 8]);
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) {
+        const int co = wc * 32 + nt * 8 + g;
+        mma16816(acc[nt], fa, ld32(&s_w[tap][co][2 * t]), ld32(&s_w[tap][co][2 * t + 8]));
+      }
+    }
+    __syncthreads();
+  }
+  // epilogue: bias, ReLU, mask, BF16 (and optional FP32) store
+#pragma unroll
+  for (int nt = 0; nt < 4; nt++) {
+    const int co = co0 + wc * 32 + nt * 8 + 2 * t;
+    const float b0 = a.bias ? a.bias[co] : 0.f, b1 = a.bias ? a.bias[co + 1] : 0.f;
+#pragma unroll
+    for (int hlf = 0; hlf < 2; hlf++) {
+      const int ww = w0 + wp * 16 + g + 8 * hlf;
+      if (ww >= a.w) continue;
+      float v0 = acc[nt][2 * hlf] + b0, v1 = acc[nt][2 * hlf + 1] + b1;
+      if (a.relu) {
+        v0 = fmaxf(v0, 0.f);
+        v1 = fmaxf(v1, 0.f);
+      }
+      const long long o = (((long long)img * a.h + row) * a.w + ww) * a.ocs + a.oco + co;
+      if (a.mask) {
+        const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162 *>(a.mask + o);
+        if (!(__bfloat162float(m.x) > 0.f)) v0 = 0.f;
+        if (!(__bfloat162float(m.y) > 0.f)) v1 = 0.f;
+      }
+      *reinterpret_cast<__nv_bfloat162 *>(a.out + o) = __floats2bfloat162_rn(v0, v1);
+      if (a.out_f32) {
+        a.out_f32[o] = v0;
+        a.out_f32[o + 1] = v1;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Weight gradient dW[tap][co][ci] += sum_p dz[p][co] x[p + tap][ci] and bias gradient.  CTA:
+// 32 couts x 16*kCiT input channels, all 9 taps, over a contiguous range of 32-pixel row chunks
+// (split-K over CTAs, FP32 atomics at the end).  Operands are staged transposed (channel-major,
+// pixels contiguous) so both MMA fragments are 32-bit shared loads; x is staged once per
+// horizontal tap shift so every fragment load is aligned.
+// ---------------------------------------------------------------------------------------------
+constexpr int kWS = kPx + 8;  // transposed pixel stride (halves)
+
+struct WgradArgs {
+  const bf16 *dz;  // [N][H][W][zcs] at channel offset 0, cout channels
+  const bf16 *x;   // [N][H][W][cin]
+  float *dw;       // [9][cout][cin] FP32 (accumulated)
+  float *db;       // [cout] FP32 (accumulated) or null
+  int n, h, w, cin, cout, zcs;
+  int chunks_per_cta;
+};
+
+template <int kCiT>
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad(WgradArgs a) {
+  constexpr int kCi = 16 * kCiT;
+  __shared__ __align__(16) bf16 s_dz[32][kWS];            // [co][px]
+  __shared__ __align__(16) bf16 s_x[3][kCi][3][kWS];      // [kx shift][ci][row][px]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int co0 = blockIdx.x * 32, ci0 = blockIdx.y * kCi;
+  const int mt = warp & 1;                 // co block of 16
+  constexpr int kNT = kCi / 8;             // n-tiles of 8 channels
+  constexpr int kNTw = kNT / 2;            // n-tiles per warp (warps 0/1 vs 2/3 split them)
+  const int nt0 = (warp >> 1) * kNTw;
+  float acc[9][kNTw][4];
+#pragma unroll
+  for (int i = 0; i < 9; i++)
+#pragma unroll
+    for (int j = 0; j < kNTw; j++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) acc[i][j][k] = 0.f;
+  float bsum = 0.f;
+  const int wchunks = (a.w + kPx - 1) / kPx;
+  const long long total = (long long)a.n * a.h * wchunks;
+  const long long c_begin = (long long)blockIdx.z * a.chunks_per_cta;
+  const long long c_end = c_begin + a.chunks_per_cta < total ? c_begin + a.chunks_per_cta : total;
+  for (long long cidx = c_begin; cidx < c_end; cidx++) {
+    const int wc = (int)(cidx % wchunks);
+    const long long rr = cidx / wchunks;
+    const int row = (int)(rr % a.h), img = (int)(rr / a.h);
+    const int w0 = wc * kPx;
+    // dz chunk, transposed: 32 pixels x 32 couts
+    for (int i = tid; i < kPx * 32; i += 128) {
+      const int co = i & 31, px = i >> 5;
+      const int ww = w0 + px;
+      bf16 v = __float2bfloat16(0.f);
+      if (ww < a.w) v = a.dz[(((long long)img * a.h + row) * a.w + ww) * a.zcs + co0 + co];
+      s_dz[co][px] = v;
+    }
+    // x rows row-1..row+1, pixels w0-1 .. w0+kPx, staged for each kx shift
+    for (int i = tid; i < 3 * (kPx + 2) * kCi; i += 128) {
+      const int ci = i % kCi, px = (i / kCi) % (kPx + 2), r = i / (kCi * (kPx + 2));
+      const int hh = row + r - 1, ww = w0 + px - 1;
+      bf16 v = __float2bfloat16(0.f);
+      if (hh >= 0 && hh < a.h && ww >= 0 && ww < a.w)
+        v = a.x[(((long long)img * a.h + hh) * a.w + ww) * a.cin + ci0 + ci];
+      // pixel px of the halo row serves output pixel px - kx for shift kx
+#pragma unroll
+      for (int kx = 0; kx < 3; kx++) {
+        const int q = px - kx;
+        if (q >= 0 && q < kPx) s_x[kx][ci][r][q] = v;
+      }
+    }
+    __syncthreads();
+    if (a.db && tid < 32) {
+      float s = 0.f;
+      for (int px = 0; px < kPx; px++) s += __bfloat162float(s_dz[tid][px]);
+      bsum += s;
+    }
+#pragma unroll
+    for (int ks = 0; ks < 2; ks++) {
+      unsigned fa[4];
+      const int m = mt * 16 + g, k = ks * 16 + 2 * t;
+      fa[0] = ld32(&s_dz[m][k]);
+      fa[1] = ld32(&s_dz[m + 8][k]);
+      fa[2] = ld32(&s_dz[m][k + 8]);
+      fa[3] = ld32(&s_dz[m + 8][k + 8]);
+#pragma unroll
+      for (int tap = 0; tap < 9; tap++) {
+        const int ky = tap / 3, kx = tap % 3;
+#pragma unroll
+        for (int j = 0; j < kNTw; j++) {
+          const int ci = (nt0 + j) * 8 + g;
+          mma16816(acc[tap][j], fa, ld32(&s_x[kx][ci][ky][k]), ld32(&s_x[kx][ci][ky][k + 8]));
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int tap = 0; tap < 9; tap++)
+#pragma unroll
+    for (int j = 0; j < kNTw; j++) {
+      const int ci = ci0 + (nt0 + j) * 8 + 2 * t;
+#pragma unroll
+      for (int hlf = 0; hlf < 2; hlf++) {
+        const int co = co0 + mt * 16 + g + 8 * hlf;
+        float *p = a.dw + ((long long)tap * a.cout + co) * a.cin + ci;
+        atomicAdd(p, acc[tap][j][2 * hlf]);
+        atomicAdd(p + 1, acc[tap][j][2 * hlf + 1]);
+      }
+    }
+  if (a.db && tid < 32 && blockIdx.y == 0) atomicAdd(a.db + co0 + tid, bsum);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Element-wise and small kernels
+// ---------------------------------------------------------------------------------------------
+// FP32 image [N][H][W] -> BF16 [N][H][W][16] (channel 0 = value, 1..15 = 0)
+__global__ void k_pack_input(const float *x, bf16 *out, long long npx) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npx * 16) return;
+  out[i] = __float2bfloat16((i & 15) == 0 ? x[i >> 4] : 0.f);
+}
+
+// 2x2 average pooling, [N][H][W][C] -> [N][H/2][W/2][C]
+__global__ void k_pool(const bf16 *x, bf16 *y, int n, int h, int w, int c) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int h2 = h / 2, w2 = w / 2;
+  if (i >= (long long)n * h2 * w2 * c) return;
+  const int ch = (int)(i % c);
+  long long r = i / c;
+  const int xx = (int)(r % w2), yy = (int)((r / w2) % h2), im = (int)(r / ((long long)w2 * h2));
+  const long long b = (((long long)im * h + 2 * yy) * w + 2 * xx) * c + ch;
+  const float s = __bfloat162float(x[b]) + __bfloat162float(x[b + c]) +
+                  __bfloat162float(x[b + (long long)w * c]) + __bfloat162float(x[b + (long long)w * c + c]);
+  y[i] = __float2bfloat16(0.25f * s);
+}
+
+// d(skip) = pool_grad(dy) * (s > 0) + extra, where extra (the skip's gradient through the
+// decoder concatenation, already masked) is read at channel offset `eco` of stride `ecs`.
+__global__ void k_pool_grad(const bf16 *dy, const bf16 *s, const bf16 *extra, int ecs, int eco,
+                            bf16 *dx, int n, int h, int w, int c) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)n * h * w * c) return;
+  const int ch = (int)(i % c);
+  long long r = i / c;
+  const int xx = (int)(r % w), yy = (int)((r / w) % h), im = (int)(r / ((long long)w * h));
+  const long long j = (((long long)im * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c + ch;
+  float v = __bfloat162float(s[i]) > 0.f ? 0.25f * __bfloat162float(dy[j]) : 0.f;
+  if (extra) v += __bfloat162float(extra[r * ecs + eco + ch]);
+  dx[i] = __float2bfloat16(v);
+}
+
+// Decoder input: out[.., 0:cu] = up2(u) (nearest), out[.., cu:cu+cs] = s; out [N][H][W][cu+cs]
+__global__ void k_up_concat(const bf16 *u, int cu, const bf16 *s, int cs, bf16 *out, int n, int h,
+                            int w) {
+  const int c = cu + cs;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)n * h * w * c) return;
+  const int ch = (int)(i % c);
+  long long r = i / c;
+  const int xx = (int)(r % w), yy = (int)((r / w) % h), im = (int)(r / ((long long)w * h));
+  if (ch < cu)
+    out[i] = u[(((long long)im * (h / 2) + yy / 2) * (w / 2) + xx / 2) * cu + ch];
+  else
+    out[i] = s[r * cs + ch - cu];
+}
+
+// d(u) = up2_grad(d(cat)[.., 0:cu]): sum of the 4 children
+__global__ void k_up_grad(const bf16 *dcat, int c, bf16 *du, int cu, int n, int h, int w) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int h2 = h / 2, w2 = w / 2;
+  if (i >= (long long)n * h2 * w2 * cu) return;
+  const int ch = (int)(i % cu);
+  long long r = i / cu;
+  const int xx = (int)(r % w2), yy = (int)((r / w2) % h2), im = (int)(r / ((long long)w2 * h2));
+  const long long b = (((long long)im * h + 2 * yy) * w + 2 * xx) * c + ch;
+  const float s = __bfloat162float(dcat[b]) + __bfloat162float(dcat[b + c]) +
+                  __bfloat162float(dcat[b + (long long)w * c]) +
+                  __bfloat162float(dcat[b + (long long)w * c + c]);
+  du[i] = __float2bfloat16(s);
+}
+
+// 1x1 output convolution (c -> 1): y[p] = b + sum_c x[p][c] w[c]
+__global__ void k_out_fwd(const bf16 *x, const float *w, const float *b, float *y, long long npx,
+                          int c) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npx) return;
+  float s = b[0];
+  for (int ch = 0; ch < c; ch++) s = fmaf(__bfloat162float(x[p * c + ch]), w[ch], s);
+  y[p] = s;
+}
+
+// MSE loss gradient dy = 2 (y - t) / count, and per-block partial loss sums (FP64)
+__global__ void k_mse(const float *y, const float *t, float *dy, long long npx, double *part) {
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npx;
+       p += (long long)gridDim.x * blockDim.x) {
+    const float d = y[p] - t[p];
+    dy[p] = 2.0f * d / (float)npx;
+    acc += (double)d * d;
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// Backward of the 1x1 output convolution: dx[p][c] = dy[p] w[c] (x > 0), dw[c] += dy x, db += dy
+__global__ void k_out_bwd(const bf16 *x, const float *dy, const float *w, bf16 *dx, float *dw,
+                          float *db, long long npx, int c) {
+  __shared__ float s_dw[64];
+  __shared__ float s_db;
+  if (threadIdx.x < c) s_dw[threadIdx.x] = 0.f;
+  if (threadIdx.x == 0) s_db = 0.f;
+  __syncthreads();
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < npx) {
+    const float d = dy[p];
+    for (int ch = 0; ch < c; ch++) {
+      const float xv = __bfloat162float(x[p * c + ch]);
+      dx[p * c + ch] = __float2bfloat16(xv > 0.f ? d * w[ch] : 0.f);
+      atomicAdd(&s_dw[ch], d * xv);
+    }
+    atomicAdd(&s_db, d);
+  }
+  __syncthreads();
+  if (threadIdx.x < c) atomicAdd(dw + threadIdx.x, s_dw[threadIdx.x]);
+  if (threadIdx.x == 0) atomicAdd(db, s_db);
+}
+
+// Adam step on the FP32 master parameters (bias-corrected, as Kingma & Ba 2015).
+__global__ void k_adam(float *p, const float *g, float *m, float *v, long long n, float lr,
+                       float b1, float b2, float eps, float c1, float c2) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// BF16 weight copies from the FP32 master [tap][co][ci_real]: forward [tap][co][cin_pad] and
+// backward-data [tap'][ci][co] with tap' = 8 - tap (spatial flip).
+__global__ void k_weights_bf16(const float *w, int k2, int co_n, int ci_real, int cin_pad,
+                               bf16 *wf, bf16 *wb) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)k2 * co_n * cin_pad) return;
+  const int ci = (int)(i % cin_pad);
+  const int co = (int)((i / cin_pad) % co_n);
+  const int tap = (int)(i / ((long long)cin_pad * co_n));
+  const float v = ci < ci_real ? w[((long long)tap * co_n + co) * ci_real + ci] : 0.f;
+  wf[i] = __float2bfloat16(v);
+  if (wb && ci < ci_real) wb[((long long)(k2 - 1 - tap) * ci_real + ci) * co_n + co] = __float2bfloat16(v);
+}
+
+constexpr int kRedBlocks = 296;
+
+// Channel 0 of the padded first-layer weight gradient [9*cout][cin_pad] -> [9*cout][1].
+__global__ void k_fold_first(const float *g0, float *g, int rows, int cin_pad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < rows) g[i] = g0[(long long)i * cin_pad];
+}
+
+inline unsigned nblk(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------------------
+struct ds2d_unet {
+  struct Layer {
+    std::string name;
+    int cin, cout, k, cin_pad;
+    long long w_off, b_off, nw;  // offsets into the flat FP32 parameter vector
+    bf16 *wf = nullptr, *wb = nullptr;  // BF16 forward / backward-data weights
+  };
+  struct Act {
+    bf16 *p = nullptr;
+    int h = 0, w = 0, c = 0;
+  };
+  int base = 32, max_n = 0, max_h = 0, max_w = 0, device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<Layer> layers;
+  long long nparam = 0;
+  float *params = nullptr, *grads = nullptr, *m = nullptr, *v = nullptr;
+  long long adam_t = 0;
+  // activations (forward) and their gradients (backward), per named slot
+  enum {
+    IN, E1A, E1B, P1, E2A, E2B, P2, E3A, E3B, P3, E4A, E4B, C3, D3A, D3B, C2, D2A, D2B, C1, D1A,
+    D1B, NACT
+  };
+  Act act[NACT], grad[NACT];
+  float *y = nullptr, *dy = nullptr;
+  float *g0 = nullptr;  // padded [9][cout][16] weight gradient of the first layer (cin 1 -> 16)
+  double *part = nullptr, *h_part = nullptr;
+  std::string err;
+  bool weights_dirty = true;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+thread_local std::string g_unet_err;
+
+int unet_fail(ds2d_unet *u, int code, const std::string &msg) {
+  if (u) u->err = msg;
+  else g_unet_err = msg;
+  return code;
+}
+
+#define UCK(call)                                                                        \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return unet_fail(u, DS2D_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+int ualloc(ds2d_unet *u, void **p, size_t bytes) {
+  UCK(cudaMalloc(p, bytes));
+  UCK(cudaMemsetAsync(*p, 0, bytes, u->stream));
+  u->allocs.push_back(*p);
+  return DS2D_OK;
+}
+
+int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w, int cin, int cout,
+         const float *bias, bf16 *out, int ocs, int oco, float *out_f32, const bf16 *mask, int relu,
+         int n, int h, int wd) {
+  ConvArgs a{in, w, bias, out, out_f32, mask, n, h, wd, cin, cout, ocs, oco, relu};
+  (void)L;
+  if (cout % 64 == 0) {
+    dim3 grid((wd + kPx - 1) / kPx, h, n * (cout / 64));
+    k_conv3x3<64><<<grid, 128, 0, u->stream>>>(a);
+  } else if (cout % 32 == 0) {
+    dim3 grid((wd + kPx - 1) / kPx, h, n * (cout / 32));
+    k_conv3x3<32><<<grid, 64, 0, u->stream>>>(a);
+  } else {
+    return unet_fail(u, DS2D_E_ARG, "conv: output channels must be a multiple of 32");
+  }
+  UCK(cudaGetLastError());
+  return DS2D_OK;
+}
+
+int wgrad(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *dz, int zcs, const bf16 *x, int n,
+          int h, int wd, float *dw_padded = nullptr) {
+  WgradArgs a{};
+  a.dz = dz; a.x = x; a.dw = dw_padded ? dw_padded : u->grads + L.w_off; a.db = u->grads + L.b_off;
+  a.n = n; a.h = h; a.w = wd; a.cin = L.cin_pad; a.cout = L.cout; a.zcs = zcs;
+  const long long chunks = (long long)n * h * ((wd + kPx - 1) / kPx);
+  const int kci = L.cin_pad >= 32 ? 32 : 16;
+  const long long tiles = (long long)(L.cout / 32) * (L.cin_pad / kci);
+  long long splits = (4 * 148 + tiles - 1) / tiles;
+  if (splits > chunks) splits = chunks;
+  if (splits < 1) splits = 1;
+  a.chunks_per_cta = (int)((chunks + splits - 1) / splits);
+  splits = (chunks + a.chunks_per_cta - 1) / a.chunks_per_cta;
+  // the FP32 gradient is [tap][cout][cin]; a channel-padded layer (the first) accumulates into a
+  // padded scratch that the caller folds
+  if (L.cin_pad != L.cin && !dw_padded)
+    return unet_fail(u, DS2D_E_STATE, "wgrad of a channel-padded layer needs a padded scratch");
+  dim3 grid(L.cout / 32, L.cin_pad / kci, (unsigned)splits);
+  if (kci == 32)
+    k_conv3x3_wgrad<2><<<grid, 128, 0, u->stream>>>(a);
+  else
+    k_conv3x3_wgrad<1><<<grid, 128, 0, u->stream>>>(a);
+  UCK(cudaGetLastError());
+  return DS2D_OK;
+}
+
+int refresh_weights(ds2d_unet *u) {
+  if (!u->weights_dirty) return DS2D_OK;
+  for (auto &L : u->layers) {
+    if (L.k != 3) continue;
+    const long long n = 9LL * L.cout * L.cin_pad;
+    k_weights_bf16<<<nblk(n), 256, 0, u->stream>>>(u->params + L.w_off, 9, L.cout, L.cin,
+                                                   L.cin_pad, L.wf, L.wb);
+  }
+  UCK(cudaGetLastError());
+  u->weights_dirty = false;
+  return DS2D_OK;
+}
+
+int check_shape(ds2d_unet *u, int n, int h, int w) {
+  if (n < 1 || n > u->max_n || h < 8 || w < 8 || h > u->max_h || w > u->max_w || h % 8 || w % 8)
+    return unet_fail(u, DS2D_E_ARG,
+                     "unet: need 1 <= n <= max_n, 8 <= h <= max_h, 8 <= w <= max_w, h and w "
+                     "multiples of 8");
+  return DS2D_OK;
+}
+
+// Forward pass: x [n][h][w] FP32 (device) -> u->y [n][h][w] FP32.
+int forward(ds2d_unet *u, const float *x, int n, int h, int w) {
+  int rc;
+  if ((rc = refresh_weights(u))) return rc;
+  using U = ds2d_unet;
+  const long long npx = (long long)n * h * w;
+  k_pack_input<<<nblk(npx * 16), 256, 0, u->stream>>>(x, u->act[U::IN].p, npx);
+  const int c[4] = {u->base, 2 * u->base, 4 * u->base, 8 * u->base};
+  const int ea[4] = {U::E1A, U::E2A, U::E3A, U::E4A}, eb[4] = {U::E1B, U::E2B, U::E3B, U::E4B};
+  const int pl[3] = {U::P1, U::P2, U::P3};
+  int src = U::IN, cin = 16, hh = h, ww = w;
+  for (int l = 0; l < 4; l++) {
+    const auto &La = u->layers[2 * l], &Lb = u->layers[2 * l + 1];
+    if ((rc = conv(u, La, u->act[src].p, La.wf, cin, c[l], u->params + La.b_off, u->act[ea[l]].p,
+                   c[l], 0, nullptr, nullptr, 1, n, hh, ww)))
+      return rc;
+    if ((rc = conv(u, Lb, u->act[ea[l]].p, Lb.wf, c[l], c[l], u->params + Lb.b_off,
+                   u->act[eb[l]].p, c[l], 0, nullptr, nullptr, 1, n, hh, ww)))
+      return rc;
+    if (l < 3) {
+      const long long np = (long long)n * (hh / 2) * (ww / 2) * c[l];
+      k_pool<<<nblk(np), 256, 0, u->stream>>>(u->act[eb[l]].p, u->act[pl[l]].p, n, hh, ww, c[l]);
+      src = pl[l];
+      hh /= 2;
+      ww /= 2;
+    }
+    cin = c[l];
+  }
+  const int ca[3] = {U::C1, U::C2, U::C3}, da[3] = {U::D1A, U::D2A, U::D3A},
+            db[3] = {U::D1B, U::D2B, U::D3B};
+  int prev = U::E4B, cprev = c[3];
+  for (int l = 2; l >= 0; l--) {
+    hh *= 2;
+    ww *= 2;
+    const int cc = cprev + c[l];
+    const long long np = (long long)n * hh * ww * cc;
+    k_up_concat<<<nblk(np), 256, 0, u->stream>>>(u->act[prev].p, cprev, u->act[eb[l]].p, c[l],
+                                                 u->act[ca[l]].p, n, hh, ww);
+    const int li = 8 + 2 * (2 - l);
+    const auto &La = u->layers[li], &Lb = u->layers[li + 1];
+    if ((rc = conv(u, La, u->act[ca[l]].p, La.wf, cc, c[l], u->params + La.b_off, u->act[da[l]].p,
+                   c[l], 0, nullptr, nullptr, 1, n, hh, ww)))
+      return rc;
+    if ((rc = conv(u, Lb, u->act[da[l]].p, Lb.wf, c[l], c[l], u->params + Lb.b_off,
+                   u->act[db[l]].p, c[l], 0, nullptr, nullptr, 1, n, hh, ww)))
+      return rc;
+    prev = db[l];
+    cprev = c[l];
+  }
+  const auto &Lo = u->layers.back();
+  k_out_fwd<<<nblk(npx), 256, 0, u->stream>>>(u->act[U::D1B].p, u->params + Lo.w_off,
+                                              u->params + Lo.b_off, u->y, npx, c[0]);
+  UCK(cudaGetLastError());
+  return DS2D_OK;
+}
+
+// Backward pass from u->dy (dLoss/dy, FP32 [n][h][w]); parameter gradients into u->grads.
+int backward(ds2d_unet *u, int n, int h, int w) {
+  using U = ds2d_unet;
+  int rc;
+  const long long npx = (long long)n * h * w;
+  const int c[4] = {u->base, 2 * u->base, 4 * u->base, 8 * u->base};
+  UCK(cudaMemsetAsync(u->grads, 0, sizeof(float) * u->nparam, u->stream));
+  const auto &Lo = u->layers.back();
+  k_out_bwd<<<nblk(npx), 256, 0, u->stream>>>(u->act[U::D1B].p, u->dy, u->params + Lo.w_off,
+                                              u->grad[U::D1B].p, u->grads + Lo.w_off,
+                                              u->grads + Lo.b_off, npx, c[0]);
+  const int ca[3] = {U::C1, U::C2, U::C3}, da[3] = {U::D1A, U::D2A, U::D3A},
+            db[3] = {U::D1B, U::D2B, U::D3B};
+  const int ea[4] = {U::E1A, U::E2A, U::E3A, U::E4A}, eb[4] = {U::E1B, U::E2B, U::E3B, U::E4B};
+  const int pl[3] = {U::P1, U::P2, U::P3};
+  int hh = h, ww = w;
+  // decoder, level 1 up to 3; the gradient arriving at db[l] is already ReLU-masked
+  for (int l = 0; l < 3; l++) {
+    const int li = 8 + 2 * (2 - l);
+    const auto &La = u->layers[li], &Lb = u->layers[li + 1];
+    const int cprev = l == 2 ? c[3] : c[l + 1];
+    const int cc = cprev + c[l];
+    // d(d_la output) = conv_bwd(d(db)) masked by d_la's output
+    if ((rc = wgrad(u, Lb, u->grad[db[l]].p, c[l], u->act[da[l]].p, n, hh, ww))) return rc;
+    if ((rc = conv(u, Lb, u->grad[db[l]].p, Lb.wb, c[l], c[l], nullptr, u->grad[da[l]].p, c[l], 0,
+                   nullptr, u->act[da[l]].p, 0, n, hh, ww)))
+      return rc;
+    if ((rc = wgrad(u, La, u->grad[da[l]].p, c[l], u->act[ca[l]].p, n, hh, ww))) return rc;
+    // d(concat) masked by the concat input (up(prev) and skip are both ReLU outputs)
+    if ((rc = conv(u, La, u->grad[da[l]].p, La.wb, c[l], cc, nullptr, u->grad[ca[l]].p, cc, 0,
+                   nullptr, u->act[ca[l]].p, 0, n, hh, ww)))
+      return rc;
+    // up part -> gradient of the coarser level's output
+    const int prev = l == 2 ? U::E4B : db[l + 1];
+    const long long np = (long long)n * (hh / 2) * (ww / 2) * cprev;
+    k_up_grad<<<nblk(np), 256, 0, u->stream>>>(u->grad[ca[l]].p, cc, u->grad[prev].p, cprev, n,
+                                                hh, ww);
+    hh /= 2;
+    ww /= 2;
+  }
+  // encoder, level 4 down to 1; grad[eb[l]] holds the masked gradient of e{l}b's output
+  for (int l = 3; l >= 0; l--) {
+    const auto &La = u->layers[2 * l], &Lb = u->layers[2 * l + 1];
+    if (l < 3) {
+      // skip gradient: pool path (from level l+1's input) + concat path (channels cprev..)
+      const int cprev = l == 2 ? c[3] : c[l + 1];
+      const long long np = (long long)n * hh * ww * c[l];
+      k_pool_grad<<<nblk(np), 256, 0, u->stream>>>(u->grad[pl[l]].p, u->act[eb[l]].p,
+                                                   u->grad[ca[l]].p, cprev + c[l], cprev,
+                                                   u->grad[eb[l]].p, n, hh, ww, c[l]);
+    }
+    const int src = l == 0 ? U::IN : pl[l - 1];
+    const int cin = l == 0 ? 16 : c[l - 1];
+    if ((rc = wgrad(u, Lb, u->grad[eb[l]].p, c[l], u->act[ea[l]].p, n, hh, ww))) return rc;
+    if ((rc = conv(u, Lb, u->grad[eb[l]].p, Lb.wb, c[l], c[l], nullptr, u->grad[ea[l]].p, c[l], 0,
+                   nullptr, u->act[ea[l]].p, 0, n, hh, ww)))
+      return rc;
+    if (l == 0) {
+      // first layer: cin padded 1 -> 16; weight gradient through the padded scratch, then
+      // channel 0 of it is the real gradient
+      UCK(cudaMemsetAsync(u->g0, 0, sizeof(float) * 9 * La.cout * La.cin_pad, u->stream));
+      if ((rc = wgrad(u, La, u->grad[ea[l]].p, c[l], u->act[src].p, n, hh, ww, u->g0))) return rc;
+      k_fold_first<<<nblk(9LL * La.cout), 256, 0, u->stream>>>(u->g0, u->grads + La.w_off,
+                                                               9 * La.cout, La.cin_pad);
+      break;
+    }
+    if ((rc = wgrad(u, La, u->grad[ea[l]].p, c[l], u->act[src].p, n, hh, ww))) return rc;
+    // gradient of the pooled input (no mask: pooling output is not a ReLU output)
+    if ((rc = conv(u, La, u->grad[ea[l]].p, La.wb, c[l], cin, nullptr, u->grad[src].p, cin, 0,
+                   nullptr, nullptr, 0, n, hh, ww)))
+      return rc;
+    hh *= 2;
+    ww *= 2;
+  }
+  UCK(cudaGetLastError());
+  return DS2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d_unet **out) {
+  if (!out) return DS2D_E_ARG;
+  *out = nullptr;
+  if (base != 32 && base != 64)
+    return unet_fail(nullptr, DS2D_E_ARG, "unet base channels must be 32 or 64");
+  if (max_n < 1 || max_h < 8 || max_w < 8 || max_h % 8 || max_w % 8)
+    return unet_fail(nullptr, DS2D_E_ARG, "unet: max_n >= 1, max_h / max_w multiples of 8");
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess)
+    return unet_fail(nullptr, DS2D_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  ds2d_unet *u = new ds2d_unet();
+  u->base = base; u->max_n = max_n; u->max_h = max_h; u->max_w = max_w; u->device = device;
+  const int c[4] = {base, 2 * base, 4 * base, 8 * base};
+  // layer table, same order as the oracle's layer_specs()
+  auto add = [&](const char *name, int cin, int cout, int k) {
+    ds2d_unet::Layer L;
+    L.name = name; L.cin = cin; L.cout = cout; L.k = k;
+    L.cin_pad = (cin + 15) / 16 * 16;
+    L.nw = (long long)k * k * cout * cin;
+    L.w_off = u->nparam;
+    L.b_off = L.w_off + L.nw;
+    u->nparam = L.b_off + cout;
+    u->layers.push_back(L);
+  };
+  static const char *en[8] = {"e1a", "e1b", "e2a", "e2b", "e3a", "e3b", "e4a", "e4b"};
+  int prev = 1;
+  for (int l = 0; l < 4; l++) {
+    add(en[2 * l], prev, c[l], 3);
+    add(en[2 * l + 1], c[l], c[l], 3);
+    prev = c[l];
+  }
+  static const char *dn[6] = {"d3a", "d3b", "d2a", "d2b", "d1a", "d1b"};
+  for (int i = 0, l = 2; l >= 0; l--, i++) {
+    add(dn[2 * i], prev + c[l], c[l], 3);
+    add(dn[2 * i + 1], c[l], c[l], 3);
+    prev = c[l];
+  }
+  add("out", c[0], 1, 1);
+  int rc = DS2D_OK;
+  auto A = [&](void **p, size_t bytes) {
+    if (rc == DS2D_OK) rc = ualloc(u, p, bytes);
+  };
+  A((void **)&u->params, sizeof(float) * u->nparam);
+  A((void **)&u->grads, sizeof(float) * u->nparam);
+  A((void **)&u->m, sizeof(float) * u->nparam);
+  A((void **)&u->v, sizeof(float) * u->nparam);
+  for (auto &L : u->layers)
+    if (L.k == 3) {
+      A((void **)&L.wf, sizeof(bf16) * 9 * L.cout * L.cin_pad);
+      A((void **)&L.wb, sizeof(bf16) * 9 * L.cout * L.cin);
+    }
+  using U = ds2d_unet;
+  const long long px0 = (long long)max_n * max_h * max_w;
+  auto act = [&](int slot, int lev, int ch) {
+    const long long px = px0 >> (2 * lev);
+    u->act[slot].c = ch;
+    u->grad[slot].c = ch;
+    A((void **)&u->act[slot].p, sizeof(bf16) * px * ch);
+    A((void **)&u->grad[slot].p, sizeof(bf16) * px * ch);
+  };
+  act(U::IN, 0, 16);
+  act(U::E1A, 0, c[0]); act(U::E1B, 0, c[0]); act(U::P1, 1, c[0]);
+  act(U::E2A, 1, c[1]); act(U::E2B, 1, c[1]); act(U::P2, 2, c[1]);
+  act(U::E3A, 2, c[2]); act(U::E3B, 2, c[2]); act(U::P3, 3, c[2]);
+  act(U::E4A, 3, c[3]); act(U::E4B, 3, c[3]);
+  act(U::C3, 2, c[3] + c[2]); act(U::D3A, 2, c[2]); act(U::D3B, 2, c[2]);
+  act(U::C2, 1, c[2] + c[1]); act(U::D2A, 1, c[1]); act(U::D2B, 1, c[1]);
+  act(U::C1, 0, c[1] + c[0]); act(U::D1A, 0, c[0]); act(U::D1B, 0, c[0]);
+  A((void **)&u->y, sizeof(float) * px0);
+  A((void **)&u->dy, sizeof(float) * px0);
+  A((void **)&u->part, sizeof(double) * kRedBlocks);
+  A((void **)&u->g0, sizeof(float) * 9 * c[0] * 16);
+  if (rc == DS2D_OK && cudaMallocHost((void **)&u->h_part, sizeof(double) * kRedBlocks) != cudaSuccess)
+    rc = unet_fail(u, DS2D_E_NOMEM, "cudaMallocHost");
+  if (rc != DS2D_OK) {
+    g_unet_err = u->err;
+    ds2d_unet_destroy(u);
+    return rc;
+  }
+  *out = u;
+  return DS2D_OK;
+}
+
+int ds2d_unet_destroy(ds2d_unet *u) {
+  if (!u) return DS2D_OK;
+  cudaSetDevice(u->device);
+  if (u->stream) cudaStreamSynchronize(u->stream);
+  for (void *p : u->allocs) cudaFree(p);
+  if (u->h_part) cudaFreeHost(u->h_part);
+  delete u;
+  return DS2D_OK;
+}
+
+const char *ds2d_unet_last_error(const ds2d_unet *u) { return u ? u->err.c_str() : g_unet_err.c_str(); }
+
+int ds2d_unet_set_stream(ds2d_unet *u, void *stream) {
+  if (!u) return DS2D_E_ARG;
+  u->stream = static_cast<cudaStream_t>(stream);
+  return DS2D_OK;
+}
+
+long long ds2d_unet_num_params(const ds2d_unet *u) { return u ? u->nparam : 0; }
+
+int ds2d_unet_set_params(ds2d_unet *u, const float *host, long long n) {
+  if (!u || !host || n != u->nparam) return unet_fail(u, DS2D_E_ARG, "set_params: size mismatch");
+  cudaSetDevice(u->device);
+  UCK(cudaMemcpyAsync(u->params, host, sizeof(float) * n, cudaMemcpyHostToDevice, u->stream));
+  UCK(cudaMemsetAsync(u->m, 0, sizeof(float) * n, u->stream));
+  UCK(cudaMemsetAsync(u->v, 0, sizeof(float) * n, u->stream));
+  UCK(cudaStreamSynchronize(u->stream));
+  u->adam_t = 0;
+  u->weights_dirty = true;
+  return DS2D_OK;
+}
+
+int ds2d_unet_get_params(ds2d_unet *u, float *host, long long n) {
+  if (!u || !host || n != u->nparam) return unet_fail(u, DS2D_E_ARG, "get_params: size mismatch");
+  cudaSetDevice(u->device);
+  UCK(cudaMemcpyAsync(host, u->params, sizeof(float) * n, cudaMemcpyDeviceToHost, u->stream));
+  UCK(cudaStreamSynchronize(u->stream));
+  return DS2D_OK;
+}
+
+int ds2d_unet_forward(ds2d_unet *u, const float *x, float *y, int n, int h, int w) {
+  if (!u || !x || !y) return unet_fail(u, DS2D_E_ARG, "forward: null pointer");
+  int rc;
+  if ((rc = check_shape(u, n, h, w))) return rc;
+  cudaSetDevice(u->device);
+  if ((rc = forward(u, x, n, h, w))) return rc;
+  UCK(cudaMemcpyAsync(y, u->y, sizeof(float) * n * h * w, cudaMemcpyDeviceToDevice, u->stream));
+  return DS2D_OK;
+}
+
+int ds2d_unet_loss_grad(ds2d_unet *u, const float *x, const float *target, int n, int h, int w,
+                        double *loss, float *grads_host) {
+  if (!u || !x || !target) return unet_fail(u, DS2D_E_ARG, "loss_grad: null pointer");
+  int rc;
+  if ((rc = check_shape(u, n, h, w))) return rc;
+  cudaSetDevice(u->device);
+  if ((rc = forward(u, x, n, h, w))) return rc;
+  const long long npx = (long long)n * h * w;
+  k_mse<<<kRedBlocks, 256, 0, u->stream>>>(u->y, target, u->dy, npx, u->part);
+  if ((rc = backward(u, n, h, w))) return rc;
+  UCK(cudaMemcpyAsync(u->h_part, u->part, sizeof(double) * kRedBlocks, cudaMemcpyDeviceToHost,
+                      u->stream));
+  if (grads_host)
+    UCK(cudaMemcpyAsync(grads_host, u->grads, sizeof(float) * u->nparam, cudaMemcpyDeviceToHost,
+                        u->stream));
+  UCK(cudaStreamSynchronize(u->stream));
+  if (loss) {
+    double s = 0;
+    for (int i = 0; i < kRedBlocks; i++) s += u->h_part[i];
+    *loss = s / (double)npx;
+  }
+  return DS2D_OK;
+}
+
+int ds2d_unet_adam_step(ds2d_unet *u, float lr, float beta1, float beta2, float eps) {
+  if (!u) return DS2D_E_ARG;
+  cudaSetDevice(u->device);
+  u->adam_t++;
+  const float c1 = 1.f - (float)std::pow((double)beta1, (double)u->adam_t);
+  const float c2 = 1.f - (float)std::pow((double)beta2, (double)u->adam_t);
+  k_adam<<<nblk(u->nparam), 256, 0, u->stream>>>(u->params, u->grads, u->m, u->v, u->nparam, lr,
+                                                 beta1, beta2, eps, c1, c2);
+  UCK(cudaGetLastError());
+  u->weights_dirty = true;
+  return DS2D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,120 @@
+"""Learned preconditioner for acoustic CG-LSRTM (no counterpart in the reference).
+
+Pipeline, all on the GPU through this package's own kernels:
+  1. training pairs: seeded random reflectivity m (sparse spikes plus dipping reflectors) on a
+     smooth background -> Born data L m -> RTM image L^T L m (ds2d_ac_normal);
+  2. training: the U-Net (ds2d_b200.unet, BF16 tensor-core kernels) learns image -> reflectivity
+     on per-sample RMS-normalised pairs with Adam;
+  3. application: ds2d_lsrtm_pcg with the trained network as the preconditioner P against the
+     same call with P = I (plain CG), both judged by the relative Born-data residual.
+"""
+import time
+
+import numpy as np
+
+from . import synth
+
+
+def background(allnx, allnz, vtop=1800.0, vbot=4500.0, seed=0, lateral=0.03, sigma=20.0):
+    """Smooth vp increasing linearly with depth plus a smooth +-`lateral` lateral variation."""
+    rng = np.random.default_rng(seed)
+    z = np.linspace(0.0, 1.0, allnz)[None, :]
+    vp = vtop + (vbot - vtop) * z + np.zeros((allnx, 1))
+    pert = synth.smooth(rng.uniform(-1, 1, (allnx, allnz)).astype(np.float32), sigma)
+    pert = pert / max(float(np.abs(pert).max()), 1e-12)
+    return (vp * (1.0 + lateral * pert)).astype(np.float32)
+
+
+def random_reflectivity(allnx, allnz, rng, density=0.05, amp=0.05, reflectors=4, top=8):
+    """Sparse spikes (`density` of the cells, N(0, amp)) plus `reflectors` dipping reflector
+    lines of random amplitude; zero in the top `top` rows (source and receiver depth)."""
+    m = np.zeros((allnx, allnz), np.float32)
+    mask = rng.random((allnx, allnz)) < density
+    m[mask] = rng.normal(0.0, amp, int(mask.sum()))
+    x = np.arange(allnx)
+    for _ in range(reflectors):
+        z0 = rng.uniform(top + 4, allnz - 4)
+        dip = rng.uniform(-0.25, 0.25)
+        zz = np.round(z0 + dip * (x - allnx / 2)).astype(int)
+        ok = (zz >= top) & (zz < allnz)
+        m[x[ok], zz[ok]] += rng.normal(0.0, 2 * amp)
+    m[:, :top] = 0.0
+    return m
+
+
+def make_pairs(ctx, shots, npairs, seed, device="cuda", log=None):
+    """(images, reflectivities) as torch FP32 tensors [npairs][allnx][allnz] on the device."""
+    import torch
+    rng = np.random.default_rng(seed)
+    nx, nz = ctx.allnx, ctx.allnz
+    X = torch.zeros((npairs, nx, nz), dtype=torch.float32, device=device)
+    Y = torch.zeros_like(X)
+    t0 = time.perf_counter()
+    for i in range(npairs):
+        m = torch.from_numpy(random_reflectivity(nx, nz, rng)).to(device)
+        Y[i] = m
+        ctx.ac_normal_device(shots, Y[i].data_ptr(), X[i].data_ptr())
+        if log and (i + 1) % max(1, npairs // 8) == 0:
+            log(f"pairs {i + 1}/{npairs} {time.perf_counter() - t0:.1f} s")
+    return X, Y
+
+
+def normalise(t):
+    """Per-sample RMS normalisation of a [n][h][w] tensor."""
+    r = t.pow(2).mean(dim=(1, 2), keepdim=True).sqrt().clamp_min(1e-30)
+    return t / r
+
+
+def pad8(t):
+    """Zero-pad the last two dims of [n][h][w] to multiples of 8 (the network's constraint)."""
+    import torch.nn.functional as F
+    h, w = t.shape[-2:]
+    return F.pad(t, (0, (-w) % 8, 0, (-h) % 8))
+
+
+def train(net, X, Y, epochs=20, batch=4, lr=1e-3, seed=0, log=None):
+    """Adam on MSE(net(X_i / rms), Y_i / rms) over shuffled mini-batches with random lateral
+    flips.  Returns the mean loss of every epoch."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    Xn, Yn = pad8(normalise(X)).contiguous(), pad8(normalise(Y)).contiguous()
+    n, h, w = Xn.shape
+    hist = []
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=g)
+        tot, cnt = 0.0, 0
+        for b0 in range(0, n - batch + 1, batch):
+            idx = perm[b0:b0 + batch].to(Xn.device)
+            xb, yb = Xn[idx], Yn[idx]
+            if torch.rand(1, generator=g).item() < 0.5:  # lateral flip (x is the first image axis)
+                xb, yb = xb.flip(1), yb.flip(1)
+            xb, yb = xb.contiguous(), yb.contiguous()
+            loss = net.loss_grad(xb.data_ptr(), yb.data_ptr(), batch, h, w)
+            net.adam_step(lr=lr)
+            tot += loss
+            cnt += 1
+        hist.append(tot / max(cnt, 1))
+        if log:
+            log(f"epoch {ep + 1}/{epochs} loss {hist[-1]:.4f}")
+    return hist
+
+
+def evaluate(net, X, Y):
+    """Relative L2 error against the normalised reflectivity of (a) the network's estimate and
+    (b) the best scalar multiple of the RTM image (the method without the network), both after
+    an optimal scalar fit, averaged over the samples."""
+    import torch
+    Xn, Yn = pad8(normalise(X)).contiguous(), pad8(normalise(Y)).contiguous()
+    n, h, w = Xn.shape
+    out = torch.zeros_like(Xn)
+    for i in range(n):
+        net.forward(Xn[i].data_ptr(), out[i].data_ptr(), 1, h, w)
+    torch.cuda.synchronize()
+
+    def fit_err(a, b):
+        s = (a * b).sum() / (a * a).sum().clamp_min(1e-30)
+        return float(((s * a - b).norm() / b.norm()).item())
+
+    e_net = np.mean([fit_err(out[i], Yn[i]) for i in range(n)])
+    e_rtm = np.mean([fit_err(Xn[i], Yn[i]) for i in range(n)])
+    return {"net": e_net, "rtm": e_rtm}

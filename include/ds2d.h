@@ -125,12 +125,19 @@ long long ds2d_last_launches(const ds2d_ctx *ctx);
  * CG helpers, main.cpp:1224-1320 sjcgsolver / FD2DGPU.cu:4885 ELSRTM_CALCULATE_ALPHA, and runs
  * NCC + Adam instead).  The acoustic scheme is the elastic one with mu = 0 (pass vs = 0 to
  * ds2d_set_models); the context must use DS2D_BOUNDARY_RANDOM (undamped grid, exact time
- * reversal).  m / grad are [allnx][allnz]; records [sum ntr][nt].
+ * reversal).  m / grad are [allnx][allnz]; records [sum ntr][nt]; these arrays may be in host
+ * or device memory (copies use unified addressing).
  *   ds2d_ac_born      d = L m  (scattered vz, vx; Born source of add_born_source with mu = 0)
  *   ds2d_ac_born_adj  g = L^T d, the exact discrete transpose of ds2d_ac_born
+ *   ds2d_ac_normal    img = L^T L m: the RTM image of the Born data of m, records kept on the
+ *                     device (training pairs of the learned preconditioner)
  *   ds2d_lsrtm        CGLS on ||L m - d||^2 from m = 0 with FP64 inner products and step
  *                     lengths; stops after niter iterations or when ||d - L m|| / ||d|| <=
- *                     target; resid[k] receives that ratio after iteration k. */
+ *                     target; resid[k] receives that ratio after iteration k.
+ *   ds2d_lsrtm_pcg    the same problem by flexible preconditioned CG: direction z = P(L^T r)
+ *                     with P the U-Net `net` (NULL: P = I, plain CG), Polak-Ribiere+ conjugation
+ *                     and the exact step <r, L p> / ||L p||^2; elapsed_ms[k] (may be NULL) is the
+ *                     wall time from the call's start to the end of iteration k. */
 int ds2d_ac_born(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *m, float *rec_vz,
                  float *rec_vx);
 int ds2d_ac_born_adj(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *rec_vz,
@@ -138,6 +145,11 @@ int ds2d_ac_born_adj(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *
 int ds2d_lsrtm(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *obs_vz,
                const float *obs_vx, int niter, double target, float *m_out, double *resid,
                int *iters_done);
+int ds2d_ac_normal(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *m, float *img);
+struct ds2d_unet;
+int ds2d_lsrtm_pcg(ds2d_ctx *ctx, struct ds2d_unet *net, const ds2d_shot *shots, int n,
+                   const float *obs_vz, const float *obs_vx, int niter, double target,
+                   float *m_out, double *resid, double *elapsed_ms, int *iters_done);
 
 /* FP64 inner product <a, b> of two float vectors of n elements in device memory, the
  * reduction the CG-LSRTM uses for its dot products and step lengths (the reference sums its CG
@@ -165,8 +177,11 @@ int ds2d_dot_f64_noalloc(const float *a, const float *b, long long n, void *stre
                          double *result);
 
 /* Tuning knobs (no counterpart in the reference, whose launch shape is fixed at 32x32 blocks,
- * FD2DGPU.cuh:8-9): "fused" (1 = single-pass fused time step, 0 = one launch per half step)
- * and "xr" (rows marched by one CTA of the fused kernels). */
+ * FD2DGPU.cuh:8-9): "fused" (1 = single-pass fused time step, 0 = one launch per half step),
+ * "xr" (rows marched by one CTA of the fused kernels), "ring" (cp.async prefetch ring depth of
+ * the fused kernels: 0 off, 1 default, or 2 / 4 / 8), "occ" (0 / 1: register budget for 6 / 8
+ * forward and 3 / 4 backward CTAs per SM), "graph" (0 / 1: capture batches in CUDA graphs),
+ * "adjoint_born" (see ds2d_elsrtm). */
 int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
 
 /* Profiling (no counterpart in the reference, which has only a commented-out host timer,
@@ -175,6 +190,32 @@ int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
  * algorithmic_bytes", for the launches since the last report, and clears them. */
 int ds2d_profile(ds2d_ctx *ctx, int enable);
 int ds2d_profile_report(ds2d_ctx *ctx, char *buf, int len);
+
+/* ---- Learned preconditioner: image-domain U-Net (no counterpart in the reference) --------
+ * Maps an RTM image to an estimate of the reflectivity (an approximate inverse Hessian of the
+ * Born operator) to precondition CG-LSRTM.  4-level encoder-decoder, `base` (32) channels at the
+ * first level doubling per level, conv3x3 + ReLU pairs, 2x2 average pooling, nearest 2x
+ * upsampling with skip concatenation, 1x1 output convolution; BF16 activations and weights on
+ * the tensor cores with FP32 accumulation and FP32 master weights.  Images are FP32 [n][h][w] in
+ * device memory with h and w multiples of 8.  Parameters are one flat FP32 vector: per layer (in
+ * the order e1a e1b e2a e2b e3a e3b e4a e4b d3a d3b d2a d2b d1a d1b out) the weights
+ * [ky][kx][cout][cin] followed by the biases [cout]. */
+typedef struct ds2d_unet ds2d_unet;
+int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d_unet **out);
+int ds2d_unet_destroy(ds2d_unet *net);
+const char *ds2d_unet_last_error(const ds2d_unet *net); /* NULL: error of the last create */
+int ds2d_unet_set_stream(ds2d_unet *net, void *stream);
+long long ds2d_unet_num_params(const ds2d_unet *net);
+int ds2d_unet_set_params(ds2d_unet *net, const float *params, long long n); /* host; resets Adam */
+int ds2d_unet_get_params(ds2d_unet *net, float *params, long long n);                /* host */
+/* y = net(x), both device [n][h][w] FP32. */
+int ds2d_unet_forward(ds2d_unet *net, const float *x, float *y, int n, int h, int w);
+/* Mean-squared-error loss of net(x) against target (device arrays) and the gradient of every
+ * parameter (kept on the device for ds2d_unet_adam_step; copied to grads_host when non-NULL). */
+int ds2d_unet_loss_grad(ds2d_unet *net, const float *x, const float *target, int n, int h, int w,
+                        double *loss, float *grads_host);
+/* One Adam step (bias-corrected) with the gradients of the last ds2d_unet_loss_grad. */
+int ds2d_unet_adam_step(ds2d_unet *net, float lr, float beta1, float beta2, float eps);
 
 #ifdef __cplusplus
 }
