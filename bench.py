@@ -43,6 +43,16 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-profile", action="store_true")
     p.add_argument("--ref-shots", type=int, default=2, help="shots per reference-arm step")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="skip the launch-shape autotuner (library defaults)")
+    p.add_argument("--workload", default="rtm", choices=["rtm", "lsrtm"],
+                   help="rtm: elastic RTM throughput (default); lsrtm: learned vs plain CG-LSRTM")
+    p.add_argument("--lsrtm-size", default="full", choices=["small", "full"],
+                   help="full: 2001x601, 80 shots, nt 5000; small: 512x256, 40 shots, nt 2000")
+    p.add_argument("--pairs", type=int, default=192, help="training pairs of the preconditioner")
+    p.add_argument("--train-steps", type=int, default=2000)
+    p.add_argument("--cg-iters", type=int, default=10)
+    p.add_argument("--target", type=float, default=1e-2)
     return p.parse_args()
 
 
@@ -163,8 +173,16 @@ def run_ours(args, rank, world, dist):
         fm.set_models(vp, vs)
         fm.set_wavelet(w)
         obs_z, obs_x = fm.forward(shots)
+    tuned = None
+    if not args.no_autotune:
+        # launch shape chosen by the project's autotuner on a short probe of the same batch
+        from ds2d_b200.autotune import apply, tune_rtm
+        tuned, _ = tune_rtm(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["dx"], c["dz"], c["dt"],
+                            vpm, vsm, w, shots, max_ntr=ntr, seed=c["seed"], device=dev)
     e = Elastic2D(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
                   boundary="random", max_shots=c["shots"], max_ntr=ntr, seed=c["seed"], device=dev)
+    if tuned:
+        apply(e, tuned)
     e.set_models(vpm, vsm)
     e.set_wavelet(w)
     # A non-default stream: the library captures each batch (time loops included) into a CUDA
@@ -263,7 +281,8 @@ def run_ours(args, rank, world, dist):
                                    f"-> {cells(c)} padded cells",
                           "nt": c["nt"], "shots_per_gpu": c["shots"], "propagations_per_shot": 3,
                           "cell_updates_per_step": upd * world, "parallelism": f"shots x{world}",
-                          "l2": "inputs larger than L2 (wavefields of 60 shots ~3 GB)"},
+                          "l2": "inputs larger than L2 (wavefields of 60 shots ~3 GB)",
+                          "launch_shape": tuned or "library defaults (autotuner skipped)"},
                "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s",
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": img_bytes},
                "gpu_launches": int(launches * args.steps),
@@ -321,6 +340,102 @@ def run_reference(args, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_lsrtm(args):
+    """Learned vs plain acoustic CG-LSRTM on one GPU: training pairs (random reflectivity -> Born
+    data -> RTM image, 512x256, 40 shots) made by this code, U-Net training on the GPU, then
+    ds2d_lsrtm_pcg with and without the network on the application grid."""
+    import torch
+    from ds2d_b200 import Elastic2D, precond, synth
+    from ds2d_b200.unet import UNet, flatten
+    from oracle import unet_oracle
+
+    def log(msg):
+        print(msg, file=sys.stderr, flush=True)
+
+    dev = torch.cuda.current_device()
+    f0, dt, dx, band = 15.0, 0.0008, 10.0, 20
+    # ---- training pairs and training -------------------------------------------------------
+    tnx, tnz, tnt, tshots = 512, 256, 2000, 40
+    tr_shots = synth.surface_shots(tnx, tnx, band, tshots)
+    et = Elastic2D(tnx, tnz, tnx, band, tnt, dx, dx, dt, boundary="random", max_shots=tshots,
+                   max_ntr=tnx, seed=7, device=dev)
+    vpt = precond.background(tnx, tnz, seed=1)
+    et.set_models(vpt, np.zeros_like(vpt))
+    et.set_wavelet(synth.ricker(tnt, f0, dt))
+    t0 = time.perf_counter()
+    X, Y = precond.make_pairs(et, tr_shots, args.pairs + 16, seed=11, log=log)
+    t_pairs = time.perf_counter() - t0
+    cells_pair = 5.0 * tshots * (tnx + 2 * band) * (tnz + 2 * band) * tnt
+    et.close()
+    anx, anz, ant, ashots = (2001, 601, 5000, 80) if args.lsrtm_size == "full" else (512, 256, 2000, 40)
+    hp, wp = (anx + 7) // 8 * 8, (anz + 7) // 8 * 8
+    net = UNet(base=32, max_n=8, max_h=max(256, hp), max_w=max(128, wp), device=dev)
+    net.set_params(flatten(unet_oracle.init_params(5)))
+    t0 = time.perf_counter()
+    hist = precond.train(net, X[:args.pairs], Y[:args.pairs], steps=args.train_steps, batch=8,
+                         lr=1e-3, log=log)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    ev = precond.evaluate(net, X[args.pairs:], Y[args.pairs:])
+    log(f"held-out fit error: network {ev['net']:.3f}, scaled RTM image {ev['rtm']:.3f}")
+    del X, Y
+    # ---- application: observed Born data of a sparse random reflectivity -------------------
+    shots = synth.surface_shots(anx, anx, band, ashots)
+    ea = Elastic2D(anx, anz, anx, band, ant, dx, dx, dt, boundary="random", max_shots=ashots,
+                   max_ntr=anx, seed=9, device=dev)
+    vpa = precond.background(anx, anz, seed=2)
+    ea.set_models(vpa, np.zeros_like(vpa))
+    ea.set_wavelet(synth.ricker(ant, f0, dt))
+    rng = np.random.default_rng(17)
+    m_true = torch.from_numpy(precond.random_reflectivity(anx, anz, rng, reflectors=0)).to(dev)
+    ntr = sum(s.ntr for s in shots)
+    dz = torch.zeros((ntr, ant), dtype=torch.float32, device=dev)
+    dxr = torch.zeros_like(dz)
+    ea.ac_born_device(shots, m_true.data_ptr(), dz.data_ptr(), dxr.data_ptr())
+    res = {}
+    for name, p in (("plain", None), ("learned", net)):
+        m = torch.zeros_like(m_true)
+        r, ms = ea.lsrtm_pcg(shots, dz.data_ptr(), dxr.data_ptr(), m.data_ptr(), args.cg_iters,
+                             target=args.target, net=p)
+        err = float(((m - m_true).norm() / m_true.norm()).item())
+        hit = [t for t, v in zip(ms, r) if v <= args.target]
+        res[name] = {"time_to_target_s": round(hit[0] / 1e3, 3) if hit else None,
+                     "iterations": len(r), "residual": [round(float(v), 5) for v in r],
+                     "elapsed_s": [round(float(t) / 1e3, 2) for t in ms],
+                     "image_rel_error_vs_true": round(err, 4)}
+        log(f"{name}: residual {r[-1]:.4f} after {len(r)} iterations, {ms[-1] / 1e3:.1f} s")
+    tp, tl = res["plain"]["time_to_target_s"], res["learned"]["time_to_target_s"]
+    # equal-residual speed-up when both reach the target; otherwise the time the learned run needs
+    # to reach the plain run's final residual, against the plain run's total time
+    if tp is not None and tl is not None:
+        speedup = tp / tl
+        basis = "time to the target residual, plain / learned"
+    else:
+        rp = res["plain"]["residual"][-1]
+        tl_eq = next((t for t, v in zip(res["learned"]["elapsed_s"], res["learned"]["residual"])
+                      if v <= rp), None)
+        speedup = res["plain"]["elapsed_s"][-1] / tl_eq if tl_eq else None
+        basis = (f"target {args.target} not reached by both; time to the plain run's final "
+                 f"residual {rp:.4g}, plain / learned")
+    upd = 5.0 * ashots * (anx + 2 * band) * (anz + 2 * band) * ant
+    return {"metric": "LSRTM time to 1e-2 relative data residual, learned vs plain (speed-up)",
+            "value": round(speedup, 3) if speedup else None, "unit": "x", "basis": basis,
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f32 stencils, bf16 network, f64 CG",
+            "data": "synthetic (seeded sparse reflectivity on a smooth 1800-4500 m/s background)",
+            "config": {"workload": "acoustic CG-LSRTM", "grid": f"{anx}x{anz} (+{band} band)",
+                       "shots": ashots, "nt": ant, "cg_iterations": args.cg_iters,
+                       "target": args.target},
+            "plain": res["plain"], "learned": res["learned"],
+            "training": {"pairs": args.pairs, "grid": f"{tnx}x{tnz}", "shots": tshots, "nt": tnt,
+                         "pair_generation_s": round(t_pairs, 1),
+                         "pair_gcell_updates_per_s": round(cells_pair * (args.pairs + 16) / t_pairs / 1e9, 2),
+                         "steps": args.train_steps, "batch": 8, "crop": "256x128",
+                         "training_s": round(t_train, 1),
+                         "loss_first_last": [round(hist[0], 4), round(hist[-1], 4)],
+                         "heldout_fit_error": {k: round(v, 4) for k, v in ev.items()}},
+            "cg_iteration_cell_updates": upd}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -334,6 +449,10 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
+    if args.workload == "lsrtm":
+        if rank == 0:
+            print(json.dumps(run_lsrtm(args)))
+        return
     if world > 1:
         import datetime
 

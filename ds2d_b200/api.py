@@ -204,8 +204,9 @@ class Elastic2D:
     def ac_born_device(self, shots, m_ptr, rz_ptr, rx_ptr):
         """d = L m with m and the records [sum ntr][nt] in device memory."""
         arr, keep = self._shots(shots)
-        self._check(self.lib.ds2d_ac_born(self.h, arr, len(shots), ctypes.c_void_p(m_ptr),
-                                          ctypes.c_void_p(rz_ptr), ctypes.c_void_p(rx_ptr)))
+        fpp = ctypes.POINTER(ctypes.c_float)
+        self._check(self.lib.ds2d_ac_born(self.h, arr, len(shots), ctypes.cast(m_ptr, fpp),
+                                          ctypes.cast(rz_ptr, fpp), ctypes.cast(rx_ptr, fpp)))
 
     def lsrtm_pcg(self, shots, obs_vz_ptr, obs_vx_ptr, m_ptr, niter, target=0.0, net=None):
         """Flexible preconditioned CG-LSRTM on device arrays; net = ds2d_b200.unet.UNet or None

@@ -1,0 +1,64 @@
+"""Autotuner of the fused elastic kernels' launch shape (no counterpart in the reference, whose
+launches are fixed 32x32 blocks).
+
+The knobs are the rows marched per CTA (`xr`), the depth of the cp.async prefetch ring (`ring`)
+and the register / occupancy target (`occ`).  Their best values depend on the grid, the number of
+resident shots and the boundary, so the tuner times each candidate on a probe context with the
+caller's grid and batch but only `probe_nt` time steps (an RTM of the same shots: one forward and
+one backward fused launch per step), and returns the fastest setting; `apply` copies it onto the
+production context.  Everything runs through the public API on the GPU."""
+import numpy as np
+
+from .api import Elastic2D
+
+DEFAULT_SPACE = [
+    {"ring": 4, "xr": 128, "occ": 0}, {"ring": 4, "xr": 64, "occ": 0},
+    {"ring": 4, "xr": 256, "occ": 0}, {"ring": 2, "xr": 128, "occ": 0},
+    {"ring": 8, "xr": 128, "occ": 0}, {"ring": 4, "xr": 128, "occ": 1},
+]
+
+
+def tune_rtm(allnx, allnz, nx, pml, dx, dz, dt, vp, vs, wavelet, shots, boundary="random",
+             max_ntr=None, seed=0, device=0, probe_nt=48, space=None, repeats=2):
+    """Times every setting of `space` on an RTM of `shots` with probe_nt steps; returns
+    (best setting, {setting key: ms per step})."""
+    import torch
+    space = space or DEFAULT_SPACE
+    max_ntr = max_ntr or max(s.ntr for s in shots)
+    w = np.asarray(wavelet, np.float32)[:probe_nt]
+    timings = {}
+    with Elastic2D(allnx, allnz, nx, pml, probe_nt, dx, dz, dt, boundary=boundary,
+                   max_shots=len(shots), max_ntr=max_ntr, seed=seed, device=device) as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        stream = torch.cuda.Stream(device=device)
+        e.set_stream(stream.cuda_stream)
+        ntr = sum(s.ntr for s in shots)
+        az = torch.zeros((ntr, probe_nt), dtype=torch.float32, device=f"cuda:{device}")
+        for cfg in space:
+            for k, v in cfg.items():
+                e.set_option(k, v)
+            e.rtm_device(shots, az.data_ptr(), az.data_ptr())  # warm-up (and graph capture)
+            torch.cuda.synchronize(device)
+            best = float("inf")
+            for _ in range(repeats):
+                ev0 = torch.cuda.Event(enable_timing=True)
+                ev1 = torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                e.rtm_device(shots, az.data_ptr(), az.data_ptr())
+                ev1.record(stream)
+                torch.cuda.synchronize(device)
+                best = min(best, ev0.elapsed_time(ev1) / probe_nt)
+            timings[key(cfg)] = best
+            e.read_images(reset=True)
+    best_cfg = min(space, key=lambda c: timings[key(c)])
+    return dict(best_cfg), timings
+
+
+def key(cfg):
+    return ",".join(f"{k}={cfg[k]}" for k in sorted(cfg))
+
+
+def apply(ctx, cfg):
+    for k, v in cfg.items():
+        ctx.set_option(k, v)

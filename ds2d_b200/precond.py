@@ -3,8 +3,8 @@
 Pipeline, all on the GPU through this package's own kernels:
   1. training pairs: seeded random reflectivity m (sparse spikes plus dipping reflectors) on a
      smooth background -> Born data L m -> RTM image L^T L m (ds2d_ac_normal);
-  2. training: the U-Net (ds2d_b200.unet, BF16 tensor-core kernels) learns image -> reflectivity
-     on per-sample RMS-normalised pairs with Adam;
+  2. training: the U-Net (ds2d_b200.unet, BF16 tensor-core kernels) learns image -> band-limited
+     reflectivity on random crops of per-sample RMS-normalised pairs with Adam;
   3. application: ds2d_lsrtm_pcg with the trained network as the preconditioner P against the
      same call with P = I (plain CG), both judged by the relative Born-data residual.
 """
@@ -72,39 +72,62 @@ def pad8(t):
     return F.pad(t, (0, (-w) % 8, 0, (-h) % 8))
 
 
-def train(net, X, Y, epochs=20, batch=4, lr=1e-3, seed=0, log=None):
-    """Adam on MSE(net(X_i / rms), Y_i / rms) over shuffled mini-batches with random lateral
-    flips.  Returns the mean loss of every epoch."""
+def band_limit(Y, sigma=1.0):
+    """Training target: the reflectivity smoothed by a Gaussian of `sigma` cells, i.e. the part of
+    it a 15 Hz survey can resolve (the network is not asked to invent unrecoverable spikes)."""
+    import torch
+    import torch.nn.functional as F
+    r = int(3 * sigma + 0.5)
+    k = torch.exp(-0.5 * (torch.arange(-r, r + 1, dtype=torch.float32, device=Y.device) / sigma) ** 2)
+    k = k / k.sum()
+    y = Y[:, None]
+    y = F.conv2d(F.pad(y, (0, 0, r, r), mode="reflect"), k.view(1, 1, -1, 1))
+    y = F.conv2d(F.pad(y, (r, r, 0, 0), mode="reflect"), k.view(1, 1, 1, -1))
+    return y[:, 0].contiguous()
+
+
+def train(net, X, Y, steps=2000, batch=8, crop=(256, 128), lr=1e-3, seed=0, log=None):
+    """Adam on MSE(net(x), y) over random crops (with random lateral flips) of the per-sample
+    RMS-normalised pairs (x = image, y = band-limited reflectivity); the learning rate decays
+    linearly to lr/10.  Returns the mean loss of every tenth of the run."""
     import torch
     g = torch.Generator(device="cpu").manual_seed(seed)
-    Xn, Yn = pad8(normalise(X)).contiguous(), pad8(normalise(Y)).contiguous()
+    Xn, Yn = normalise(X).contiguous(), normalise(band_limit(Y)).contiguous()
     n, h, w = Xn.shape
-    hist = []
-    for ep in range(epochs):
-        perm = torch.randperm(n, generator=g)
-        tot, cnt = 0.0, 0
-        for b0 in range(0, n - batch + 1, batch):
-            idx = perm[b0:b0 + batch].to(Xn.device)
-            xb, yb = Xn[idx], Yn[idx]
-            if torch.rand(1, generator=g).item() < 0.5:  # lateral flip (x is the first image axis)
-                xb, yb = xb.flip(1), yb.flip(1)
-            xb, yb = xb.contiguous(), yb.contiguous()
-            loss = net.loss_grad(xb.data_ptr(), yb.data_ptr(), batch, h, w)
-            net.adam_step(lr=lr)
-            tot += loss
-            cnt += 1
-        hist.append(tot / max(cnt, 1))
-        if log:
-            log(f"epoch {ep + 1}/{epochs} loss {hist[-1]:.4f}")
+    ch, cw = min(crop[0], h) // 8 * 8, min(crop[1], w) // 8 * 8
+    xb = torch.empty((batch, ch, cw), dtype=torch.float32, device=X.device)
+    yb = torch.empty_like(xb)
+    hist, tot, cnt = [], 0.0, 0
+    t0 = time.perf_counter()
+    for step in range(steps):
+        idx = torch.randint(0, n, (batch,), generator=g)
+        i0 = torch.randint(0, h - ch + 1, (batch,), generator=g)
+        j0 = torch.randint(0, w - cw + 1, (batch,), generator=g)
+        flip = torch.rand(batch, generator=g) < 0.5
+        for b in range(batch):
+            xs = Xn[idx[b], i0[b]:i0[b] + ch, j0[b]:j0[b] + cw]
+            ys = Yn[idx[b], i0[b]:i0[b] + ch, j0[b]:j0[b] + cw]
+            if flip[b]:
+                xs, ys = xs.flip(0), ys.flip(0)
+            xb[b].copy_(xs)
+            yb[b].copy_(ys)
+        tot += net.loss_grad(xb.data_ptr(), yb.data_ptr(), batch, ch, cw)
+        cnt += 1
+        net.adam_step(lr=lr * (1.0 - 0.9 * step / max(1, steps - 1)))
+        if (step + 1) % max(1, steps // 10) == 0:
+            hist.append(tot / cnt)
+            if log:
+                log(f"step {step + 1}/{steps} loss {hist[-1]:.4f} {time.perf_counter() - t0:.1f} s")
+            tot, cnt = 0.0, 0
     return hist
 
 
 def evaluate(net, X, Y):
-    """Relative L2 error against the normalised reflectivity of (a) the network's estimate and
+    """Relative L2 error against the normalised band-limited reflectivity of (a) the network's estimate and
     (b) the best scalar multiple of the RTM image (the method without the network), both after
     an optimal scalar fit, averaged over the samples."""
     import torch
-    Xn, Yn = pad8(normalise(X)).contiguous(), pad8(normalise(Y)).contiguous()
+    Xn, Yn = pad8(normalise(X)).contiguous(), pad8(normalise(band_limit(Y))).contiguous()
     n, h, w = Xn.shape
     out = torch.zeros_like(Xn)
     for i in range(n):
