@@ -208,6 +208,13 @@ class Elastic2D:
         self._check(self.lib.ds2d_ac_born(self.h, arr, len(shots), ctypes.cast(m_ptr, fpp),
                                           ctypes.cast(rz_ptr, fpp), ctypes.cast(rx_ptr, fpp)))
 
+    def ac_born_adj_device(self, shots, rz_ptr, rx_ptr, g_ptr):
+        """g = L^T d with the records [sum ntr][nt] and g in device memory."""
+        arr, keep = self._shots(shots)
+        fpp = ctypes.POINTER(ctypes.c_float)
+        self._check(self.lib.ds2d_ac_born_adj(self.h, arr, len(shots), ctypes.cast(rz_ptr, fpp),
+                                              ctypes.cast(rx_ptr, fpp), ctypes.cast(g_ptr, fpp)))
+
     def lsrtm_pcg(self, shots, obs_vz_ptr, obs_vx_ptr, m_ptr, niter, target=0.0, net=None):
         """Flexible preconditioned CG-LSRTM on device arrays; net = ds2d_b200.unet.UNet or None
         (plain CG).  Returns (relative residual per iteration, wall ms per iteration)."""

@@ -99,7 +99,9 @@ __global__ void __launch_bounds__(256) k_ac_born(Dims d0, const ShotDev *shots, 
   const long long k = d.slot * s + (long long)ix * ld + iz;
   const float sx = stencil4([&](int i) { return __ldg(vx + k + (long long)(i - 1) * ld) - __ldg(vx + k - (long long)i * ld); });
   const float sz = stencil4([&](int i) { return __ldg(vz + k + i - 1) - __ldg(vz + k - i); });
-  e[k] = -2.0f * p.lam[k] * p.dmp[k] * (sx / d.dx + sz / d.dz);
+  // reciprocal multiplies (same form as the transpose in k_ac_adj_s); a division would take its
+  // slow path for the tiny amplitudes ahead of a wavefront
+  e[k] = -2.0f * p.lam[k] * p.dmp[k] * (sx * (1.0f / d.dx) + sz * (1.0f / d.dz));
 }
 
 // Adjoint, part 1 (transpose of the stress stage) with the transpose of the recording:
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(256) k_ac_adj_s(AcAdjArgs a) {
     const float sx = stencil4([&](int i) { return __ldg(VX + k + (long long)(i - 1) * ld) - __ldg(VX + k - (long long)i * ld); });
     const float sz = stencil4([&](int i) { return __ldg(VZ + k + i - 1) - __ldg(VZ + k - i); });
     const long long o = ((long long)s * d.wnx_max + (ix - d.pml)) * d.wnz + (iz - d.pml);
-    a.grad[o] += -2.0f * a.p.lam[k] * (sx / d.dx + sz / d.dz) * gs;
+    a.grad[o] += -2.0f * a.p.lam[k] * (sx * (1.0f / d.dx) + sz * (1.0f / d.dz)) * gs;
   }
 }
 

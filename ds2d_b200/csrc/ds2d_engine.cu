@@ -223,6 +223,9 @@ struct ds2d_ctx {
   int opt_adjoint_born = 0;  // scattered adjoint of ELSRTM (off = the reference's observed runs)
   int opt_ring = kDefaultRing;  // cp.async ring depth of the fused kernels (0 = no ring)
   int opt_occ = 0;           // occupancy target of the ring kernels (see fwd_ring_fn)
+  bool ring_ok = true;       // batch arrays fit the ring kernels' 32-bit offsets
+  int opt_pcg_switch = 970;  // ds2d_lsrtm_pcg: per-mille residual ratio that ends the network phase
+  int opt_pcg_m = 8;         // ds2d_lsrtm_pcg: directions kept for explicit conjugation
   // Acoustic Born pair (LSRTM): background, scattered and adjoint states, Born overlay.
   float *ac[10] = {};        // bvx bvz bs | dvx dvz ds | yx yz ys | e
   double *dot_part = nullptr, *dot_out = nullptr;  // FP64 inner-product scratch
@@ -231,7 +234,7 @@ struct ds2d_ctx {
     float *p = nullptr;
     size_t n = 0;
   };
-  Vec vecs[12];
+  Vec vecs[64];  // 0-11 solver vectors, 16+ the flexible-CG direction window
   Wave fw2{}, abk2{};  // ping-pong partners of fw / abk for the fused kernels
   Wave *fw_cur = nullptr;  // buffer holding the latest forward state
   double batch_cells = 0, batch_wcells = 0;  // padded / interior cells of the current batch
@@ -544,7 +547,7 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
     a.d = d; a.a = *cur; a.b = *nxt; a.p = c->par; a.shots = c->d_shots; a.wavelet = c->wavelet;
     a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
     if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
-    if (c->opt_ring) {
+    if (c->opt_ring && c->ring_ok) {
       const size_t sm = sizeof(float) * c->opt_ring * kFwdRingFields * kFB;
       FwdFn kfn = fwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ);
       LAUNCHS("fwd_fused", kBytesFused * CELLS(n), kfn, grid, kFB, sm, a);
@@ -712,7 +715,7 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
       a.shots = c->d_shots; a.rmap = c->d_rmap; a.res_vz = c->rec[0]; a.res_vx = c->rec[1];
       a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
       a.img = c->img_slot; a.img_plane = (long long)plane;
-      if (c->opt_ring) {
+      if (c->opt_ring && c->ring_ok) {
         const size_t sm = sizeof(float) * c->opt_ring * kBwdRingFields * kFB;
         BwdFn kfn = bwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ);
         LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, fgrid, kFB, sm, a);
@@ -1076,6 +1079,10 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
   d.lb_max = d.lb;
   d.nseg_max = d.nseg;
   c->B = opts->max_shots;
+  // The ring-fed kernels index cells and image pixels with 32-bit offsets; batches whose arrays
+  // exceed 2^31 elements fall back to the 64-bit fused kernels.
+  c->ring_ok = (long long)c->B * d.slot < (1LL << 31) &&
+               (long long)c->B * d.wnx * d.wnz < (1LL << 31);
   {
     // Ring-fed kernels may use more than the default 48 KB of dynamic shared memory.
     cudaError_t e = cudaSuccess;
@@ -1498,71 +1505,89 @@ int ds2d_lsrtm_pcg(ds2d_ctx *c, ds2d_unet *net, const ds2d_shot *shots, int n, c
   c->last_updates = 0;
   const auto t0 = std::chrono::steady_clock::now();
   const size_t nall = (size_t)c->d.allnx * c->d.allnz, nd = (size_t)n * c->d.max_ntr * c->d.nt;
-  float *m, *g, *p, *gn, *z, *rz, *rx, *qz, *qx;
+  const int M = std::max(1, std::min(c->opt_pcg_m, 15));
+  float *m, *g, *z, *rz, *rx, *wz, *wx;
   if ((rc = work_vec(c, 0, nall, &m)) || (rc = work_vec(c, 1, nall, &g)) ||
-      (rc = work_vec(c, 2, nall, &p)) || (rc = work_vec(c, 3, nall, &gn)) ||
       (rc = work_vec(c, 4, nall, &z)) || (rc = work_vec(c, 5, nd, &rz)) ||
-      (rc = work_vec(c, 6, nd, &rx)) || (rc = work_vec(c, 7, nd, &qz)) ||
-      (rc = work_vec(c, 8, nd, &qx)))
+      (rc = work_vec(c, 6, nd, &rx)) || (rc = work_vec(c, 7, nd, &wz)) ||
+      (rc = work_vec(c, 8, nd, &wx)))
     return rc;
+  // direction window: p_j (model space) and q_j = L p_j (data space, two components)
+  std::vector<float *> P(M), QZ(M), QX(M);
+  std::vector<double> sig(M, 0.0);
+  for (int j = 0; j < M; j++)
+    if ((rc = work_vec(c, 16 + 3 * j, nall, &P[j])) || (rc = work_vec(c, 17 + 3 * j, nd, &QZ[j])) ||
+        (rc = work_vec(c, 18 + 3 * j, nd, &QX[j])))
+      return rc;
   CK(cudaMemsetAsync(m, 0, nall * 4, c->stream));
   CK(cudaMemsetAsync(rz, 0, nd * 4, c->stream));
   CK(cudaMemsetAsync(rx, 0, nd * 4, c->stream));
   if ((rc = data_io(c, shots, n, rz, (float *)obs_vz, true)) ||
       (rc = data_io(c, shots, n, rx, (float *)obs_vx, true)))
     return rc;
-  // Flexible preconditioned CG on || d - L m ||^2 from m = 0 (FP64 scalars):
-  //   g = L^T r, z = P(g), p = z + beta p with Polak-Ribiere+ beta = max(0, <z, g - g_prev>) /
-  //   <z_prev, g_prev>, and the exact step alpha = <r, L p> / ||L p||^2 along p.  With P = I this
-  //   is CG (Polak-Ribiere equals Fletcher-Reeves on a quadratic with exact line search); with
-  //   the network it stays a descent method whatever P does, since alpha is exact.
+  // Flexible CG with truncated explicit conjugation (Notay's FCG(M)) on || d - L m ||^2 from
+  // m = 0, FP64 scalars.  Each iteration: g = L^T r, z = P(g), w = L z, then z and w are made
+  // L^T L-conjugate to the last M directions (z -= beta_j p_j, w -= beta_j q_j with
+  // beta_j = <w, q_j> / <q_j, q_j>), and the exact step alpha = <r, q> / <q, q> is taken along
+  // p = z, q = w.  With P = I this is CG; with the network the explicit conjugation keeps its
+  // directions from undoing one another (an inexact, non-linear P breaks the short recurrence).
+  // When an iteration with the network reduces the residual by less than the "pcg_switch"
+  // ratio, the network phase ends and the solver continues with P = I and a fresh window.
   double dd, tz, tx;
   if ((rc = dot64(c, rz, rz, nd, &tz)) || (rc = dot64(c, rx, rx, nd, &tx))) return rc;
   dd = tz + tx;
   if (!(dd > 0)) return fail(c, DS2D_E_NUMERIC, "observed data are zero or not finite");
   if ((rc = ac_apply(c, shots, n, true, nullptr, rz, rx, g))) return rc;
-  if ((rc = precondition(c, net, g, z))) return rc;
-  CK(cudaMemcpyAsync(p, z, nall * 4, cudaMemcpyDeviceToDevice, c->stream));
-  double zg;
-  if ((rc = dot64(c, z, g, nall, &zg))) return rc;
   const int nb = 4 * 148;
-  int k = 0;
+  int k = 0, nwin = 0, head = 0;  // window: nwin entries, next slot `head`
+  double prev_rel = 1.0;
   for (; k < niter; k++) {
-    if ((rc = ac_apply(c, shots, n, false, p, qz, qx, nullptr))) return rc;
+    if ((rc = precondition(c, net, g, z))) return rc;
+    if ((rc = ac_apply(c, shots, n, false, z, wz, wx, nullptr))) return rc;
+    for (int i = 0; i < nwin; i++) {
+      const int j = (head - 1 - i + M) % M;
+      double bz, bx;
+      if ((rc = dot64(c, wz, QZ[j], nd, &bz)) || (rc = dot64(c, wx, QX[j], nd, &bx))) return rc;
+      const double beta = (bz + bx) / sig[j];
+      k_axpy<<<nb, 256, 0, c->stream>>>((long long)nall, -beta, P[j], z);
+      k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -beta, QZ[j], wz);
+      k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -beta, QX[j], wx);
+      c->last_launches += 3;
+    }
     double rq_z, rq_x;
-    if ((rc = dot64(c, qz, qz, nd, &tz)) || (rc = dot64(c, qx, qx, nd, &tx)) ||
-        (rc = dot64(c, rz, qz, nd, &rq_z)) || (rc = dot64(c, rx, qx, nd, &rq_x)))
+    if ((rc = dot64(c, wz, wz, nd, &tz)) || (rc = dot64(c, wx, wx, nd, &tx)) ||
+        (rc = dot64(c, rz, wz, nd, &rq_z)) || (rc = dot64(c, rx, wx, nd, &rq_x)))
       return rc;
     const double qq = tz + tx;
     if (!(qq > 0) || !std::isfinite(rq_z + rq_x))
       return fail(c, DS2D_E_NUMERIC, "PCG breakdown at %d", k);
     const double alpha = (rq_z + rq_x) / qq;
-    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nall, alpha, p, m);
-    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -alpha, qz, rz);
-    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -alpha, qx, rx);
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nall, alpha, z, m);
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -alpha, wz, rz);
+    k_axpy<<<nb, 256, 0, c->stream>>>((long long)nd, -alpha, wx, rx);
     c->last_launches += 3;
+    // keep (p, q) = (z, w) in the window
+    CK(cudaMemcpyAsync(P[head], z, nall * 4, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(QZ[head], wz, nd * 4, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(QX[head], wx, nd * 4, cudaMemcpyDeviceToDevice, c->stream));
+    sig[head] = qq;
+    head = (head + 1) % M;
+    nwin = std::min(nwin + 1, M);
     if ((rc = dot64(c, rz, rz, nd, &tz)) || (rc = dot64(c, rx, rx, nd, &tx))) return rc;
     const double rel = std::sqrt((tz + tx) / dd);
     if (resid) resid[k] = rel;
     if (elapsed_ms)
       elapsed_ms[k] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    if (rel <= target) {
+    if (rel <= target || k + 1 == niter) {
       k++;
       break;
     }
-    if (k + 1 == niter) {
-      k++;
-      break;
+    if (net && c->opt_pcg_switch > 0 && rel > prev_rel * (c->opt_pcg_switch / 1000.0)) {
+      net = nullptr;  // network phase over: plain CG from the current iterate
+      nwin = 0;
     }
-    if ((rc = ac_apply(c, shots, n, true, nullptr, rz, rx, gn))) return rc;
-    if ((rc = precondition(c, net, gn, z))) return rc;
-    double zgn, zgo;
-    if ((rc = dot64(c, z, gn, nall, &zgn)) || (rc = dot64(c, z, g, nall, &zgo))) return rc;
-    const double beta = std::max(0.0, (zgn - zgo) / zg);
-    zg = zgn;
-    k_xpby<<<nb, 256, 0, c->stream>>>((long long)nall, z, beta, p);
-    c->last_launches++;
-    std::swap(g, gn);
+    prev_rel = rel;
+    if ((rc = ac_apply(c, shots, n, true, nullptr, rz, rx, g))) return rc;
   }
   if (iters_done) *iters_done = k;
   CK(cudaMemcpyAsync(m_out, m, nall * 4, cudaMemcpyDefault, c->stream));
@@ -1594,6 +1619,12 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     if (value != 0 && value != 2 && value != 4 && value != 8)
       return fail(c, DS2D_E_ARG, "ring must be 0 (off), 1 (default depth) or a depth of 2, 4 or 8");
     c->opt_ring = (int)value;
+  } else if (k == "pcg_m") {
+    if (value < 1 || value > 15) return fail(c, DS2D_E_ARG, "pcg_m must be in [1, 15]");
+    c->opt_pcg_m = (int)value;
+  } else if (k == "pcg_switch") {
+    if (value < 0 || value > 1000) return fail(c, DS2D_E_ARG, "pcg_switch must be in [0, 1000]");
+    c->opt_pcg_switch = (int)value;
   } else if (k == "occ") {
     if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "occ must be 0 or 1");
     c->opt_occ = (int)value;

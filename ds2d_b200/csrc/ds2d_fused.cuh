@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
   const int z = blockIdx.x * a.tz - 8 + t;
   const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
   if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
-  const long long base = d.slot * s;
+  const int base = (int)(d.slot * s);  // cell offsets fit 32 bits (checked on the host)
   const int ld = d.ld;
   const bool zin = z >= 0 && z < d.nzp;
   const bool zupd = z >= d.nop && z < d.nzp - d.nop;
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
     for (int f = 0; f < kFwdRingFields; f++) {
       const int row = q - (f < 3 ? 0 : (f < 6 ? 4 : 8));
       if (row >= 0 && row < d.nxp && zin)
-        cp_async4(&R(q, f), src[f] + base + (long long)row * ld + z);
+        cp_async4(&R(q, f), src[f] + (base + row * ld + z));
       else
         R(q, f) = 0.f;
     }
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
     __syncthreads();
     float vxn = 0.f, vzn = 0.f;
     if (vcol && r >= x0 && rv >= d.nop && rv < d.nxp - d.nop) {
-      const long long k = base + (long long)rv * ld + z;
+      const int k = base + rv * ld + z;
       const float ax = dxp_mid(w_txx);
       const float fx = dxm_mid(w_txz);
       const float bz = stencil4([&](int i) { return s_txz[t + i - 1] - s_txz[t - i]; });
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
     s_vz[t] = w_vz[4];
     __syncthreads();
     if (scol && rs >= x0 && rs < x1 && rs >= d.nop && rs < d.nxp - d.nop) {
-      const long long k = base + (long long)rs * ld + z;
+      const int k = base + rs * ld + z;
       const float sa = dxm_mid(w_vx);
       const float sf = dxp_mid(w_vz);
       const float sb = stencil4([&](int i) { return s_vz[t + i - 1] - s_vz[t - i]; });
@@ -635,7 +635,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
   const int z = blockIdx.x * a.tz - 8 + t;
   const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
   if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
-  const long long base = d.slot * s;
+  const int base = (int)(d.slot * s);  // cell offsets fit 32 bits (checked on the host)
   const int ld = d.ld, pml = d.pml;
   const bool zin = z >= 0 && z < d.nzp;
   const bool c1 = t >= 4 && t < a.tz + 12;
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
   const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
-  const long long img_row = (long long)s * d.wnx_max;  // image row of model row r: img_row + r - pml
+  const int img_row = s * d.wnx_max;  // image row of model row r: img_row + r - pml
   float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
   const float *grid_src[16] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.txx, a.ra.tzz,
                                a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz, a.p.lam,  a.p.mu,
@@ -667,13 +667,13 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
       if (img) {
         if (row >= pml && row < d.nxp - pml && z_int && zin) {
           float *src = f == 14 ? img_pp : (f == 15 ? img_ps : img_il);
-          cp_async4(dst, src + (img_row + row - pml) * d.wnz + (z - pml));
+          cp_async4(dst, src + ((img_row + row - pml) * d.wnz + (z - pml)));
         } else {
           *dst = 0.f;
         }
       } else if (row >= 0 && row < d.nxp && zin) {
         const float *src = grid_src[f < 14 ? f : 14];
-        cp_async4(dst, src + base + (long long)row * ld + z);
+        cp_async4(dst, src + (base + row * ld + z));
       } else {
         *dst = 0.f;
       }
@@ -727,7 +727,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
     __syncthreads();
     float btxx = 0.f, btzz = 0.f, btxz = 0.f, P = 0.f, L = 0.f, M = 0.f, Pz = 0.f, Lx = 0.f;
     if (c1 && zin && r >= x0 && r1 >= 0 && r1 < d.nxp) {
-      const long long k = base + (long long)r1 * ld + z;
+      const int k = base + r1 * ld + z;
       const bool own = c2 && r1 >= x0 && r1 < x1;
       btxx = R(r, 4);
       btzz = R(r, 5);
@@ -793,7 +793,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
       Pz = l2m * atzz;
       Lx = lam * atxx;
       if (own && x_int && z_int) {
-        const long long o = (img_row + (r1 - pml)) * d.wnz + (z - pml);
+        const int o = (img_row + (r1 - pml)) * d.wnz + (z - pml);
         const float kpp = R(r, 12), kps = R(r, 13);
         const float lamda_grad = (gx_vx + gz_vz) * (atxx + atzz);
         const float miu_grad = -2.0f * (gx_vx * atzz + gz_vz * atxx) + (gz_vx + gx_vz) * atxz;
@@ -818,7 +818,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
     s_lx[t] = w_Lx[0];
     __syncthreads();
     if (c2 && zin && r2 >= x0 && r2 < x1) {
-      const long long k = base + (long long)r2 * ld + z;
+      const int k = base + r2 * ld + z;
       const bool x_int = r2 >= pml && r2 < d.nxp - pml;
       const float bb = R(r, 16);
       const float cbx = bb * dtdx, cbz = bb * dtdz;
@@ -836,7 +836,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float vz = ovz + (-cbx * fx + -cbz * ez);
         a.rb.vx[k] = vx;
         a.rb.vz[k] = vz;
-        const long long o = (img_row + (r2 - pml)) * d.wnz + (z - pml);
+        const int o = (img_row + (r2 - pml)) * d.wnz + (z - pml);
         img_il[o] = R(r, 17) + (vx * vx + vz * vz);
       }
       if (r2 >= d.nop && r2 < d.nxp - d.nop && z_upd) {

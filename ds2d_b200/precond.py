@@ -1,8 +1,8 @@
 """Learned preconditioner for acoustic CG-LSRTM (no counterpart in the reference).
 
 Pipeline, all on the GPU through this package's own kernels:
-  1. training pairs: seeded random reflectivity m (sparse spikes plus dipping reflectors) on a
-     smooth background -> Born data L m -> RTM image L^T L m (ds2d_ac_normal);
+  1. training pairs: seeded random reflectivity m (sparse spikes, dipping reflectors, band-limited
+     fields) on a smooth background -> Born data L m -> RTM image L^T L m (ds2d_ac_normal);
   2. training: the U-Net (ds2d_b200.unet, BF16 tensor-core kernels) learns image -> band-limited
      reflectivity on random crops of per-sample RMS-normalised pairs with Adam;
   3. application: ds2d_lsrtm_pcg with the trained network as the preconditioner P against the
@@ -42,21 +42,88 @@ def random_reflectivity(allnx, allnz, rng, density=0.05, amp=0.05, reflectors=4,
     return m
 
 
-def make_pairs(ctx, shots, npairs, seed, device="cuda", log=None):
+def training_reflectivity(allnx, allnz, rng, top=8):
+    """A varied training model: sparse spikes of random density, 0-6 dipping reflectors, and a
+    band-limited random field of random scale, under a random depth trend of the amplitude.  The
+    variety makes the network meet inputs like the CG gradients it preconditions later (the
+    remaining error of an iterate is smoother and deeper than a fresh reflectivity)."""
+    m = random_reflectivity(allnx, allnz, rng, density=rng.uniform(0.01, 0.08),
+                            reflectors=int(rng.integers(0, 7)), top=top)
+    if rng.random() < 0.7:
+        field = synth.smooth(rng.standard_normal((allnx, allnz)).astype(np.float32),
+                             rng.uniform(1.0, 6.0))
+        field *= rng.uniform(0.2, 1.0) * 0.05 / max(float(field.std()), 1e-12)
+        m += field
+    z = np.linspace(0.0, 1.0, allnz)[None, :]
+    m *= (1.0 + rng.uniform(-0.7, 2.0) * z).astype(np.float32)
+    m[:, :top] = 0.0
+    return m.astype(np.float32)
+
+
+def make_pairs(ctx, shots, npairs, seed, device="cuda", log=None, generator=None):
     """(images, reflectivities) as torch FP32 tensors [npairs][allnx][allnz] on the device."""
     import torch
     rng = np.random.default_rng(seed)
+    gen = generator or training_reflectivity
     nx, nz = ctx.allnx, ctx.allnz
     X = torch.zeros((npairs, nx, nz), dtype=torch.float32, device=device)
     Y = torch.zeros_like(X)
     t0 = time.perf_counter()
     for i in range(npairs):
-        m = torch.from_numpy(random_reflectivity(nx, nz, rng)).to(device)
+        m = torch.from_numpy(gen(nx, nz, rng)).to(device)
         Y[i] = m
         ctx.ac_normal_device(shots, Y[i].data_ptr(), X[i].data_ptr())
         if log and (i + 1) % max(1, npairs // 8) == 0:
             log(f"pairs {i + 1}/{npairs} {time.perf_counter() - t0:.1f} s")
     return X, Y
+
+
+def make_trajectory_pairs(ctx, shots, nmodels, iters, seed, device="cuda", log=None,
+                          generator=None):
+    """Training pairs along plain CG-LSRTM trajectories: for each seeded model m, run `iters`
+    iterations of CGLS on d = L m and keep, at every iterate m_k, the pair (g_k = L^T (d - L m_k),
+    e_k = m - m_k).  g_0 is the RTM image of m and e_0 = m itself; later pairs show the network the
+    smoother, deeper, poorly illuminated errors that the CG leaves behind, i.e. the inputs it meets
+    as a preconditioner.  Each iteration costs one L and one L^T, the price of one ordinary pair.
+    Returns (g, e) as torch FP32 tensors [nmodels * iters][allnx][allnz]."""
+    import torch
+    rng = np.random.default_rng(seed)
+    gen = generator or training_reflectivity
+    nx, nz = ctx.allnx, ctx.allnz
+    ntr = sum(s.ntr for s in shots)
+    G = torch.zeros((nmodels * iters, nx, nz), dtype=torch.float32, device=device)
+    E = torch.zeros_like(G)
+    dz = torch.zeros((ntr, ctx.nt), dtype=torch.float32, device=device)
+    dx = torch.zeros_like(dz)
+    qz, qx = torch.zeros_like(dz), torch.zeros_like(dz)
+    t0 = time.perf_counter()
+    for j in range(nmodels):
+        m_true = torch.from_numpy(gen(nx, nz, rng)).to(device)
+        ctx.ac_born_device(shots, m_true.data_ptr(), dz.data_ptr(), dx.data_ptr())
+        rz, rx = dz.clone(), dx.clone()
+        m = torch.zeros_like(m_true)
+        g = torch.zeros_like(m_true)
+        ctx.ac_born_adj_device(shots, rz.data_ptr(), rx.data_ptr(), g.data_ptr())
+        p = g.clone()
+        gamma = float(g.double().pow(2).sum())
+        for k in range(iters):
+            G[j * iters + k] = g
+            E[j * iters + k] = m_true - m
+            if k + 1 == iters:
+                break
+            ctx.ac_born_device(shots, p.data_ptr(), qz.data_ptr(), qx.data_ptr())
+            delta = float(qz.double().pow(2).sum() + qx.double().pow(2).sum())
+            alpha = gamma / delta
+            m += alpha * p
+            rz -= alpha * qz
+            rx -= alpha * qx
+            ctx.ac_born_adj_device(shots, rz.data_ptr(), rx.data_ptr(), g.data_ptr())
+            gnew = float(g.double().pow(2).sum())
+            p = g + (gnew / gamma) * p
+            gamma = gnew
+        if log:
+            log(f"trajectory {j + 1}/{nmodels} {time.perf_counter() - t0:.1f} s")
+    return G, E
 
 
 def normalise(t):
