@@ -132,3 +132,28 @@ def test_lsrtm_cg_matches_oracle_cgls(cuda_device):
     assert len(hist) == 4
     np.testing.assert_allclose(hist, ref, rtol=5e-3)
     assert hist[-1] < hist[0] < 1.0
+
+
+def test_lsrtm_pcg_plain_matches_cgls_and_net_descends(cuda_device):
+    """ds2d_lsrtm_pcg with P = I follows CGLS (same residuals up to rounding); with a U-Net as P
+    (untrained) the exact line search still makes every iteration decrease the residual."""
+    import torch
+    from ds2d_b200.unet import UNet, flatten
+    from oracle import unet_oracle as uo
+    c, vp, vs, w, shots, m = acoustic_case(nt=300, nshots=3)
+    with ctx(c, shots) as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        dz, dx = e.ac_born(shots, m)
+        _, hist_cgls = e.lsrtm(shots, dz, dx, 4)
+        tz, tx = torch.from_numpy(dz).cuda(), torch.from_numpy(dx).cuda()
+        mo = torch.zeros((c["allnx"], c["allnz"]), dtype=torch.float32, device="cuda")
+        hist, ms = e.lsrtm_pcg(shots, tz.data_ptr(), tx.data_ptr(), mo.data_ptr(), 4)
+        assert len(hist) == 4 and np.all(np.diff(ms) > 0)
+        np.testing.assert_allclose(hist, hist_cgls, rtol=2e-3)
+        hp, wp = (c["allnx"] + 7) // 8 * 8, (c["allnz"] + 7) // 8 * 8
+        with UNet(max_n=1, max_h=hp, max_w=wp) as net:
+            net.set_params(flatten(uo.init_params(1)))
+            mo.zero_()
+            hist_n, _ = e.lsrtm_pcg(shots, tz.data_ptr(), tx.data_ptr(), mo.data_ptr(), 4, net=net)
+    assert np.all(np.diff(np.concatenate([[1.0], hist_n])) < 0), hist_n
