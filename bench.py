@@ -399,7 +399,7 @@ def run_lsrtm(args):
     et.close()
     anx, anz, ant, ashots = (2001, 601, 5000, 80) if args.lsrtm_size == "full" else (512, 256, 2000, 40)
     hp, wp = (anx + 7) // 8 * 8, (anz + 7) // 8 * 8
-    net = UNet(base=32, max_n=8, max_h=max(256, hp), max_w=max(128, wp), device=dev)
+    net = UNet(base=32, max_n=8, max_h=max(128, hp), max_w=max(tnz, wp), device=dev)
     net.set_params(flatten(unet_oracle.init_params(5)))
     t0 = time.perf_counter()
     hist = precond.train(net, X[:args.pairs], Y[:args.pairs], steps=args.train_steps, batch=8,
@@ -429,7 +429,12 @@ def run_lsrtm(args):
                              target=args.target, net=p)
         err = float(((m - m_true).norm() / m_true.norm()).item())
         hit = [t for t, v in zip(ms, r) if v <= args.target]
+
+        def time_to(level):
+            h = [t for t, v in zip(ms, r) if v <= level]
+            return round(h[0] / 1e3, 2) if h else None
         res[name] = {"time_to_target_s": round(hit[0] / 1e3, 3) if hit else None,
+                     "time_to_residual_s": {str(lv): time_to(lv) for lv in (0.5, 0.3, 0.2, 0.15, 0.1)},
                      "iterations": len(r), "residual": [round(float(v), 5) for v in r],
                      "elapsed_s": [round(float(t) / 1e3, 2) for t in ms],
                      "image_rel_error_vs_true": round(err, 4)}
@@ -459,7 +464,7 @@ def run_lsrtm(args):
             "training": {"pairs": args.pairs, "grid": f"{tnx}x{tnz}", "shots": tshots, "nt": tnt,
                          "pair_generation_s": round(t_pairs, 1),
                          "pair_gcell_updates_per_s": round(cells_pair * (args.pairs + 16) / t_pairs / 1e9, 2),
-                         "steps": args.train_steps, "batch": 8, "crop": "256x128",
+                         "steps": args.train_steps, "batch": 8, "crop": "128 x full depth",
                          "training_s": round(t_train, 1),
                          "loss_first_last": [round(hist[0], 4), round(hist[-1], 4)],
                          "heldout_fit_error": {k: round(v, 4) for k, v in ev.items()}},

@@ -153,15 +153,17 @@ def band_limit(Y, sigma=1.0):
     return y[:, 0].contiguous()
 
 
-def train(net, X, Y, steps=2000, batch=8, crop=(256, 128), lr=1e-3, seed=0, log=None):
-    """Adam on MSE(net(x), y) over random crops (with random lateral flips) of the per-sample
-    RMS-normalised pairs (x = image, y = band-limited reflectivity); the learning rate decays
-    linearly to lr/10.  Returns the mean loss of every tenth of the run."""
+def train(net, X, Y, steps=2000, batch=8, crop=(128, None), lr=1e-3, seed=0, log=None):
+    """Adam on MSE(net(x), y) over random lateral crops (full depth by default, so the network
+    sees where a feature sits between the surface and the bottom, and with random lateral flips)
+    of the per-sample RMS-normalised pairs (x = image, y = band-limited reflectivity); the
+    learning rate decays linearly to lr/10.  Returns the mean loss of every tenth of the run."""
     import torch
     g = torch.Generator(device="cpu").manual_seed(seed)
     Xn, Yn = normalise(X).contiguous(), normalise(band_limit(Y)).contiguous()
     n, h, w = Xn.shape
-    ch, cw = min(crop[0], h) // 8 * 8, min(crop[1], w) // 8 * 8
+    ch = min(crop[0] or h, h) // 8 * 8
+    cw = min(crop[1] or w, w) // 8 * 8
     xb = torch.empty((batch, ch, cw), dtype=torch.float32, device=X.device)
     yb = torch.empty_like(xb)
     hist, tot, cnt = [], 0.0, 0
