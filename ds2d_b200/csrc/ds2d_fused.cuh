@@ -294,11 +294,12 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
       const bool own = rv >= x0 && rv < x1 && t >= 8 && t < a.tz + 8;
       if (kPML && pml_cell(d, rv, z)) {
         const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-        const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-        const float vxx = __fdiv_rn(fmaf(d1, a.a.vx_x[k], ux_x), d2);
-        const float vxz = __fdiv_rn(fmaf(d3, a.a.vx_z[k], ux_z), d4);
-        const float vzx = __fdiv_rn(fmaf(d1, a.a.vz_x[k], uz_x), d2);
-        const float vzz = __fdiv_rn(fmaf(d3, a.a.vz_z[k], uz_z), d4);
+        const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+        const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
+        const float vxx = fmaf(d1, a.a.vx_x[k], ux_x) * i2;
+        const float vxz = fmaf(d3, a.a.vx_z[k], ux_z) * i4;
+        const float vzx = fmaf(d1, a.a.vz_x[k], uz_x) * i2;
+        const float vzz = fmaf(d3, a.a.vz_z[k], uz_z) * i4;
         if (own) {
           a.b.vx_x[k] = vxx; a.b.vx_z[k] = vxz; a.b.vz_x[k] = vzx; a.b.vz_z[k] = vzz;
         }
@@ -341,13 +342,14 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
       const float xz_x = dtdx * mu * sf, xz_z = dtdz * mu * se;
       if (kPML && pml_cell(d, rs, z)) {
         const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-        const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-        const float a1 = __fdiv_rn(fmaf(d1, a.a.txx_x[k], xx_x), d2);
-        const float a2 = __fdiv_rn(fmaf(d3, a.a.txx_z[k], xx_z), d4);
-        const float b1 = __fdiv_rn(fmaf(d1, a.a.tzz_x[k], zz_x), d2);
-        const float b2 = __fdiv_rn(fmaf(d3, a.a.tzz_z[k], zz_z), d4);
-        const float c1 = __fdiv_rn(fmaf(d1, a.a.txz_x[k], xz_x), d2);
-        const float c2 = __fdiv_rn(fmaf(d3, a.a.txz_z[k], xz_z), d4);
+        const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+        const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
+        const float a1 = fmaf(d1, a.a.txx_x[k], xx_x) * i2;
+        const float a2 = fmaf(d3, a.a.txx_z[k], xx_z) * i4;
+        const float b1 = fmaf(d1, a.a.tzz_x[k], zz_x) * i2;
+        const float b2 = fmaf(d3, a.a.tzz_z[k], zz_z) * i4;
+        const float c1 = fmaf(d1, a.a.txz_x[k], xz_x) * i2;
+        const float c2 = fmaf(d3, a.a.txz_z[k], xz_z) * i4;
         a.b.txx_x[k] = a1; a.b.txx_z[k] = a2;
         a.b.tzz_x[k] = b1; a.b.tzz_z[k] = b2;
         a.b.txz_x[k] = c1; a.b.txz_z[k] = c2;
@@ -765,11 +767,12 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float oxx = R(r, 7), ozz = R(r, 8);
         if (kPML && pml_cell(d, r1, z)) {
           const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-          const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-          atxx = __fdiv_rn(fmaf(d1, oxx, xx), d2);
-          atzz = __fdiv_rn(fmaf(d3, ozz, zz), d4);
-          const float q1 = __fdiv_rn(fmaf(d1, a.aa.txz_x[k], xz_x), d2);
-          const float q2 = __fdiv_rn(fmaf(d3, a.aa.txz_z[k], xz_z), d4);
+          const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+          const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
+          atxx = fmaf(d1, oxx, xx) * i2;
+          atzz = fmaf(d3, ozz, zz) * i4;
+          const float q1 = fmaf(d1, a.aa.txz_x[k], xz_x) * i2;
+          const float q2 = fmaf(d3, a.aa.txz_z[k], xz_z) * i4;
           if (own) {
             a.ab.txz_x[k] = q1;
             a.ab.txz_z[k] = q2;
@@ -851,11 +854,12 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
         float vx, vz;
         if (kPML && pml_cell(d, r2, z)) {
           const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-          const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-          const float vxx = __fdiv_rn(fmaf(d1, a.aa.vx_x[k], ux_x), d2);
-          const float vxz = __fdiv_rn(fmaf(d3, a.aa.vx_z[k], ux_z), d4);
-          const float vzx = __fdiv_rn(fmaf(d1, a.aa.vz_x[k], uz_x), d2);
-          const float vzz = __fdiv_rn(fmaf(d3, a.aa.vz_z[k], uz_z), d4);
+          const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+          const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
+          const float vxx = fmaf(d1, a.aa.vx_x[k], ux_x) * i2;
+          const float vxz = fmaf(d3, a.aa.vx_z[k], ux_z) * i4;
+          const float vzx = fmaf(d1, a.aa.vz_x[k], uz_x) * i2;
+          const float vzz = fmaf(d3, a.aa.vz_z[k], uz_z) * i4;
           a.ab.vx_x[k] = vxx; a.ab.vx_z[k] = vxz; a.ab.vz_x[k] = vzx; a.ab.vz_z[k] = vzz;
           vx = vxx + vxz;
           vz = vzx + vzz;
