@@ -631,7 +631,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
   static_assert(kD >= 2 && (kD & (kD - 1)) == 0, "ring depth: a power of two");
   extern __shared__ float ring[];  // [kD][kBwdRingFields][kFB]
   __shared__ float s_bvx[kFB], s_bvz[kFB], s_avx[kFB], s_avz[kFB];
-  __shared__ float s_btxz[kFB], s_btzz[kFB], s_m[kFB], s_pz[kFB], s_lx[kFB];
+  __shared__ float s_btxz[kFB], s_btzz[kFB], s_m[kFB], s_pzlx[kFB];
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int z = blockIdx.x * a.tz - 8 + t;
@@ -684,12 +684,15 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
   };
 
   float w_bvx[9], w_bvz[9], w_avx[9], w_avz[9];
-  float w_btxx[9], w_btxz[9], w_btzz[5], w_P[9], w_L[9], w_M[9], w_Pz[5], w_Lx[5];
+  // Adjoint-velocity operands: the stage-2 update needs Dx+((l+2m) atxx) + Dx+(l atzz) and
+  // Dz+((l+2m) atzz) + Dz+(l atxx); by linearity each pair is one derivative of the summed
+  // product, so stage 1 keeps PL = (l+2m) atxx + l atzz and PzLx = (l+2m) atzz + l atxx.
+  float w_btxx[9], w_btxz[9], w_btzz[5], w_PL[9], w_M[9], w_PzLx[5];
 #pragma unroll
   for (int i = 0; i < 9; i++)
-    w_bvx[i] = w_bvz[i] = w_avx[i] = w_avz[i] = w_btxx[i] = w_btxz[i] = w_P[i] = w_L[i] = w_M[i] = 0.f;
+    w_bvx[i] = w_bvz[i] = w_avx[i] = w_avz[i] = w_btxx[i] = w_btxz[i] = w_PL[i] = w_M[i] = 0.f;
 #pragma unroll
-  for (int i = 0; i < 5; i++) w_btzz[i] = w_Pz[i] = w_Lx[i] = 0.f;
+  for (int i = 0; i < 5; i++) w_btzz[i] = w_PzLx[i] = 0.f;
 
 #pragma unroll
   for (int j = 0; j < kD - 1; j++) issue(x0 - 8 + j);
@@ -727,7 +730,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
     s_avx[t] = w_avx[4];
     s_avz[t] = w_avz[4];
     __syncthreads();
-    float btxx = 0.f, btzz = 0.f, btxz = 0.f, P = 0.f, L = 0.f, M = 0.f, Pz = 0.f, Lx = 0.f;
+    float btxx = 0.f, btzz = 0.f, btxz = 0.f, PL = 0.f, M = 0.f, PzLx = 0.f;
     if (c1 && zin && r >= x0 && r1 >= 0 && r1 < d.nxp) {
       const int k = base + r1 * ld + z;
       const bool own = c2 && r1 >= x0 && r1 < x1;
@@ -790,11 +793,9 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
         }
       }
       const float l2m = lam + 2.0f * mu;
-      P = l2m * atxx;
-      L = lam * atzz;
+      PL = l2m * atxx + lam * atzz;
       M = mu * atxz;
-      Pz = l2m * atzz;
-      Lx = lam * atxx;
+      PzLx = l2m * atzz + lam * atxx;
       if (own && x_int && z_int) {
         const int o = (img_row + (r1 - pml)) * d.wnz + (z - pml);
         const float kpp = R(r, 12), kps = R(r, 13);
@@ -807,18 +808,15 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
     push(w_btxx, btxx);
     push(w_btxz, btxz);
     push(w_btzz, btzz);
-    push(w_P, P);
-    push(w_L, L);
+    push(w_PL, PL);
     push(w_M, M);
-    push(w_Pz, Pz);
-    push(w_Lx, Lx);
+    push(w_PzLx, PzLx);
     // ---- stage 2: velocities of row r2 = r - 8 ---------------------------------------------
     const int r2 = r - 8;
     s_btxz[t] = w_btxz[4];
     s_btzz[t] = w_btzz[0];
     s_m[t] = w_M[4];
-    s_pz[t] = w_Pz[0];
-    s_lx[t] = w_Lx[0];
+    s_pzlx[t] = w_PzLx[0];
     __syncthreads();
     if (c2 && zin && r2 >= x0 && r2 < x1) {
       const int k = base + r2 * ld + z;
@@ -843,14 +841,12 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
         img_il[o] = R(r, 17) + (vx * vx + vz * vz);
       }
       if (r2 >= d.nop && r2 < d.nxp - d.nop && z_upd) {
-        const float t_xx = dxp_mid(w_P);
-        const float t_zx = dxp_mid(w_L);
+        const float t_x = dxp_mid(w_PL);
         const float s_xz = dxm_mid(w_M);
         const float t_xz = stencil4([&](int i) { return s_m[t + i - 1] - s_m[t - i]; });
-        const float s_zz = stencil4([&](int i) { return s_pz[t + i] - s_pz[t - i + 1]; });
-        const float s_xx = stencil4([&](int i) { return s_lx[t + i] - s_lx[t - i + 1]; });
-        const float ux_x = fmaf(-cbx, t_zx, -cbx * t_xx), ux_z = -cbz * t_xz;
-        const float uz_x = -cbx * s_xz, uz_z = fmaf(-cbz, s_xx, -cbz * s_zz);
+        const float s_z = stencil4([&](int i) { return s_pzlx[t + i] - s_pzlx[t - i + 1]; });
+        const float ux_x = -cbx * t_x, ux_z = -cbz * t_xz;
+        const float uz_x = -cbx * s_xz, uz_z = -cbz * s_z;
         float vx, vz;
         if (kPML && pml_cell(d, r2, z)) {
           const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;

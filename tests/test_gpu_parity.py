@@ -5,7 +5,7 @@ import pytest
 
 from ds2d_b200 import Elastic2D, synth
 from oracle import pyoracle as po
-from tests.helpers import case_of, gate, load, rel, shots_of, small_case
+from tests.helpers import GATE, case_of, gate, load, rel, shots_of, small_case
 
 pytestmark = pytest.mark.gpu
 
@@ -158,9 +158,16 @@ def test_fused_step_matches_half_steps(cuda_device, boundary, xr, ring):
             rz, rx = e.forward(shots)
             e.rtm(shots, rz, rx)
             out[fused] = (rz, rx, e.read_images())
-    assert rel(out[1][0], out[0][0]) < 1e-6 and rel(out[1][1], out[0][1]) < 1e-6
+    # The ring kernels multiply by 1 / (1 + dt d / 2) in PML cells where the half steps divide,
+    # take each pair of adjoint-velocity derivatives of one stencil as a single derivative of the
+    # summed operand (linearity) and form strains with reciprocal multiplies: they agree with the
+    # half-step path at the FP32 parity gate (1e-5), not bit for bit.  Without the ring the fused
+    # kernels keep the half steps' operation order.
+    tol = 1e-6 if ring == 0 else GATE
+    assert rel(out[1][0], out[0][0]) < tol and rel(out[1][1], out[0][1]) < tol
     for key in ("pp_grad", "ps_grad", "illumination"):
-        assert rel(out[1][2][key], out[0][2][key]) < 1e-6, key
+        err = rel(out[1][2][key], out[0][2][key])
+        assert err < tol, (key, err)
 
 
 @pytest.mark.parametrize("boundary", ["pml", "random"])
