@@ -380,7 +380,13 @@ def run_lsrtm(args):
     dev = torch.cuda.current_device()
     f0, dt, dx, band = 15.0, 0.0008, 10.0, 20
     # ---- training pairs and training -------------------------------------------------------
-    tnx, tnz, tnt, tshots = 512, 256, 2000, 40
+    # Training survey: 512 columns at the application's depth, record length and shot spacing
+    # (full: 600 deep, nt 5000, 20 shots ~ 25 cells apart like 80 shots over 2001 columns;
+    # small: the application grid itself, 512x256, nt 2000, 40 shots).
+    if args.lsrtm_size == "full":
+        tnx, tnz, tnt, tshots = 512, 600, 5000, 20
+    else:
+        tnx, tnz, tnt, tshots = 512, 256, 2000, 40
     tr_shots = synth.surface_shots(tnx, tnx, band, tshots)
     et = Elastic2D(tnx, tnz, tnx, band, tnt, dx, dx, dt, boundary="random", max_shots=tshots,
                    max_ntr=tnx, seed=7, device=dev)
