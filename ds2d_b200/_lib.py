@@ -28,7 +28,7 @@ EXPORTS = [
     "ds2d_ac_born_adj", "ds2d_lsrtm", "ds2d_dot_f64", "ds2d_dot_f64_noalloc",
     "ds2d_ac_normal", "ds2d_lsrtm_pcg", "ds2d_unet_create", "ds2d_unet_destroy", "ds2d_unet_last_error", "ds2d_unet_set_stream",
     "ds2d_unet_num_params", "ds2d_unet_set_params", "ds2d_unet_get_params", "ds2d_unet_forward",
-    "ds2d_unet_loss_grad", "ds2d_unet_adam_step",
+    "ds2d_unet_loss_grad", "ds2d_unet_adam_step", "ds2d_unet_set_option",
 ]
 
 
@@ -104,6 +104,7 @@ def load():
         "ds2d_unet_forward": ([P, P, P] + [ctypes.c_int] * 3, ctypes.c_int),
         "ds2d_unet_loss_grad": ([P, P, P] + [ctypes.c_int] * 3 + [dp, fp], ctypes.c_int),
         "ds2d_unet_adam_step": ([P] + [ctypes.c_float] * 4, ctypes.c_int),
+        "ds2d_unet_set_option": ([P, ctypes.c_char_p, ctypes.c_longlong], ctypes.c_int),
         "ds2d_ac_born": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, fp], ctypes.c_int),
         "ds2d_ac_born_adj": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, fp], ctypes.c_int),
         "ds2d_lsrtm": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, ctypes.c_int,

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -148,6 +149,177 @@ __global__ void __launch_bounds__(64 * (kCo / 32)) k_conv3x3(ConvArgs a) {
       }
     }
   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The same 3x3 convolution on the 5th-generation tensor cores (tcgen05, accumulators in TMEM).
+// CTA: 128 threads, tile M = 128 consecutive output pixels of one image row x N output channels;
+// K loop: input-channel chunks of 16, 9 taps per chunk, one UMMA (M 128, N, K 16) per tap issued by
+// one thread.  Operands sit in shared memory in the canonical K-major no-swizzle layout: 8-row core
+// matrices of 16 bytes per row, rows 16 bytes apart (SBO = 128 B between 8-row groups), the two
+// 8-channel halves of a 16-channel chunk in separate planes (LBO = plane stride).  With rows
+// uniformly 16 bytes apart, the tap shift kx is a 16-byte offset of the descriptor's start
+// address, so one staged halo row serves all three kx taps.  The accumulator tile (128 lanes x N
+// FP32 columns) is read back with tcgen05.ld by the warp owning each 32-lane quarter.
+// ---------------------------------------------------------------------------------------------
+constexpr int kTcM = 128;              // pixels per CTA (UMMA M)
+constexpr int kTcHalo = kTcM + 2;      // halo pixels per staged row
+constexpr int kTcPlaneA = kTcHalo * 16;  // bytes of one (row, channel-half) plane
+constexpr int kTcSpin = 1 << 24;       // bound on every mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle (SM100 descriptor version 1).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+template <int kN>
+__global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  // layout: A planes [3 rows][2 halves][130 px][16 B], B planes [9 taps][2 halves][kN][16 B]
+  unsigned char *sA = tc_smem;
+  unsigned char *sB = tc_smem + 6 * kTcPlaneA;
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int w0 = blockIdx.x * kTcM, row = blockIdx.y;
+  const int ngrp = a.cout / kN;
+  const int img = blockIdx.z / ngrp, co0 = (blockIdx.z % ngrp) * kN;
+  constexpr uint32_t kCols = kN < 32 ? 32 : kN;  // TMEM columns: a power of two >= 32
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base)), "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar)));
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t idesc = umma_idesc(kTcM, kN);
+  const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+  bool ok = true;
+  int phase = 0;
+  for (int ci0 = 0; ci0 < a.cin && ok; ci0 += 16) {
+    // stage the 3 halo rows: pixel px of row ky, channel half kh -> plane (ky, kh), offset 16 px
+    for (int i = tid; i < 3 * 2 * kTcHalo; i += 128) {
+      const int px = i % kTcHalo, kh = (i / kTcHalo) & 1, ky = i / (2 * kTcHalo);
+      const int hh = row + ky - 1, ww = w0 + px - 1;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (hh >= 0 && hh < a.h && ww >= 0 && ww < a.w)
+        v = *reinterpret_cast<const uint4 *>(
+            a.in + (((long long)img * a.h + hh) * a.w + ww) * a.cin + ci0 + kh * 8);
+      *reinterpret_cast<uint4 *>(sA + (ky * 2 + kh) * kTcPlaneA + px * 16) = v;
+    }
+    // stage the weights: tap, half, cout row
+    for (int i = tid; i < 9 * 2 * kN; i += 128) {
+      const int co = i % kN, kh = (i / kN) & 1, tap = i / (2 * kN);
+      const uint4 v = *reinterpret_cast<const uint4 *>(
+          a.wt + ((long long)tap * a.cout + co0 + co) * a.cin + ci0 + kh * 8);
+      *reinterpret_cast<uint4 *>(sB + (tap * 2 + kh) * (kN * 16) + co * 16) = v;
+    }
+    // generic-proxy writes -> visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+#pragma unroll
+      for (int tap = 0; tap < 9; tap++) {
+        const int ky = tap / 3, kx = tap % 3;
+        const uint64_t ad = umma_desc(a_base + (ky * 2) * kTcPlaneA + kx * 16, kTcPlaneA, 128);
+        const uint64_t bd = umma_desc(b_base + (tap * 2) * (kN * 16), kN * 16, 128);
+        const uint32_t acc = (ci0 > 0 || tap > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+          smem_u32(&mbar)));
+    }
+    // every thread waits until the MMAs of this chunk have read shared memory and finished
+    uint32_t done = 0;
+    for (int spin = 0; spin < kTcSpin && !done; spin++) {
+      asm volatile(
+          "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+          "selp.u32 %0, 1, 0, p;\n}\n"
+          : "=r"(done)
+          : "r"(smem_u32(&mbar)), "r"(phase)
+          : "memory");
+    }
+    if (!done) {
+      ok = false;
+      if (tid == 0) atomicExch(err, 1);
+    }
+    phase ^= 1;
+    __syncthreads();
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  if (ok) {
+    // epilogue: thread (warp w, lane l) owns output pixel 32 w + l, reads 8 columns at a time
+    const int m = warp * 32 + lane;
+    const int ww = w0 + m;
+    const long long obase = (((long long)img * a.h + row) * a.w + ww) * a.ocs + a.oco + co0;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kN; c0 += 8) {
+      uint32_t r[8];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+            "=r"(r[7])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (ww < a.w) {
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          v[j] = __uint_as_float(r[j]) + (a.bias ? a.bias[co0 + c0 + j] : 0.f);
+          if (a.relu) v[j] = fmaxf(v[j], 0.f);
+        }
+        const long long o = obase + c0;
+        if (a.mask) {
+#pragma unroll
+          for (int j = 0; j < 8; j++)
+            if (!(__bfloat162float(a.mask[o + j]) > 0.f)) v[j] = 0.f;
+        }
+        __nv_bfloat162 p[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) p[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        *reinterpret_cast<uint4 *>(a.out + o) = *reinterpret_cast<uint4 *>(p);
+        if (a.out_f32) {
+#pragma unroll
+          for (int j = 0; j < 8; j++) a.out_f32[o + j] = v[j];
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols));
+  }
+}
+
+template <int kN>
+constexpr int tc_smem_bytes() {
+  return 6 * kTcPlaneA + 9 * 2 * kN * 16;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -452,6 +624,8 @@ struct ds2d_unet {
   double *part = nullptr, *h_part = nullptr;
   std::string err;
   bool weights_dirty = true;
+  int use_tc = 0;          // 3x3 convolutions on tcgen05 (1) or mma.sync (0)
+  int *d_err = nullptr;    // device flag raised by a bounded wait that gave up
   std::vector<void *> allocs;
 };
 
@@ -484,7 +658,16 @@ int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w,
          int n, int h, int wd) {
   ConvArgs a{in, w, bias, out, out_f32, mask, n, h, wd, cin, cout, ocs, oco, relu};
   (void)L;
-  if (cout % 64 == 0) {
+  if (u->use_tc && cout % 32 == 0) {
+    const int kn = cout % 128 == 0 ? 128 : (cout % 64 == 0 ? 64 : 32);
+    dim3 grid((wd + kTcM - 1) / kTcM, h, n * (cout / kn));
+    if (kn == 128)
+      k_conv3x3_tc<128><<<grid, 128, tc_smem_bytes<128>(), u->stream>>>(a, u->d_err);
+    else if (kn == 64)
+      k_conv3x3_tc<64><<<grid, 128, tc_smem_bytes<64>(), u->stream>>>(a, u->d_err);
+    else
+      k_conv3x3_tc<32><<<grid, 128, tc_smem_bytes<32>(), u->stream>>>(a, u->d_err);
+  } else if (cout % 64 == 0) {
     dim3 grid((wd + kPx - 1) / kPx, h, n * (cout / 64));
     k_conv3x3<64><<<grid, 128, 0, u->stream>>>(a);
   } else if (cout % 32 == 0) {
@@ -533,6 +716,18 @@ int refresh_weights(ds2d_unet *u) {
   }
   UCK(cudaGetLastError());
   u->weights_dirty = false;
+  return DS2D_OK;
+}
+
+// Reads (and clears) the flag a tensor-core kernel raises when a bounded wait gave up.
+int check_wait_flag(ds2d_unet *u) {
+  int flag = 0;
+  UCK(cudaMemcpyAsync(&flag, u->d_err, sizeof(int), cudaMemcpyDeviceToHost, u->stream));
+  UCK(cudaStreamSynchronize(u->stream));
+  if (flag) {
+    UCK(cudaMemsetAsync(u->d_err, 0, sizeof(int), u->stream));
+    return unet_fail(u, DS2D_E_CUDA, "tensor-core convolution: a bounded wait gave up");
+  }
   return DS2D_OK;
 }
 
@@ -754,6 +949,19 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
   A((void **)&u->dy, sizeof(float) * px0);
   A((void **)&u->part, sizeof(double) * kRedBlocks);
   A((void **)&u->g0, sizeof(float) * 9 * c[0] * 16);
+  A((void **)&u->d_err, sizeof(int));
+  if (rc == DS2D_OK) {
+    cudaError_t ea = cudaFuncSetAttribute(k_conv3x3_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          tc_smem_bytes<128>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc_smem_bytes<64>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc_smem_bytes<32>());
+    if (ea != cudaSuccess)
+      rc = unet_fail(u, DS2D_E_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
+  }
   if (rc == DS2D_OK && cudaMallocHost((void **)&u->h_part, sizeof(double) * kRedBlocks) != cudaSuccess)
     rc = unet_fail(u, DS2D_E_NOMEM, "cudaMallocHost");
   if (rc != DS2D_OK) {
@@ -812,7 +1020,16 @@ int ds2d_unet_forward(ds2d_unet *u, const float *x, float *y, int n, int h, int 
   cudaSetDevice(u->device);
   if ((rc = forward(u, x, n, h, w))) return rc;
   UCK(cudaMemcpyAsync(y, u->y, sizeof(float) * n * h * w, cudaMemcpyDeviceToDevice, u->stream));
-  return DS2D_OK;
+  return u->use_tc ? check_wait_flag(u) : DS2D_OK;
+}
+
+int ds2d_unet_set_option(ds2d_unet *u, const char *key, long long value) {
+  if (!u || !key) return unet_fail(u, DS2D_E_ARG, "set_option: null argument");
+  if (std::string(key) == "tcgen05") {
+    u->use_tc = value != 0;
+    return DS2D_OK;
+  }
+  return unet_fail(u, DS2D_E_ARG, std::string("unknown option ") + key);
 }
 
 int ds2d_unet_loss_grad(ds2d_unet *u, const float *x, const float *target, int n, int h, int w,
@@ -831,6 +1048,7 @@ int ds2d_unet_loss_grad(ds2d_unet *u, const float *x, const float *target, int n
     UCK(cudaMemcpyAsync(grads_host, u->grads, sizeof(float) * u->nparam, cudaMemcpyDeviceToHost,
                         u->stream));
   UCK(cudaStreamSynchronize(u->stream));
+  if (u->use_tc && (rc = check_wait_flag(u))) return rc;
   if (loss) {
     double s = 0;
     for (int i = 0; i < kRedBlocks; i++) s += u->h_part[i];

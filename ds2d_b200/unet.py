@@ -76,6 +76,10 @@ class UNet:
         if rc:
             raise DS2DError(rc, self.lib.ds2d_unet_last_error(self.h).decode())
 
+    def set_option(self, key, value):
+        """"tcgen05": 1 = 3x3 convolutions on tcgen05 / TMEM, 0 = mma.sync."""
+        self._check(self.lib.ds2d_unet_set_option(self.h, key.encode(), int(value)))
+
     def set_stream(self, stream_handle):
         self._check(self.lib.ds2d_unet_set_stream(self.h, ctypes.c_void_p(stream_handle)))
 

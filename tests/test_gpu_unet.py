@@ -27,13 +27,15 @@ def _case(n=2, h=32, w=64, seed=0):
     return p, x, t
 
 
-def test_unet_forward_matches_oracle(cuda_device):
+@pytest.mark.parametrize("tcgen05", [0, 1])
+def test_unet_forward_matches_oracle(cuda_device, tcgen05):
     import torch
     from ds2d_b200.unet import UNet, flatten
     p, x, t = _case()
     n, h, w = x.shape[:3]
     want, _ = uo.forward(p, x)
     with UNet(max_n=n, max_h=h, max_w=w) as net:
+        net.set_option("tcgen05", tcgen05)
         net.set_params(flatten(p))
         dx = torch.from_numpy(x[..., 0].astype(np.float32)).cuda()
         dy = torch.zeros_like(dx)
@@ -45,13 +47,15 @@ def test_unet_forward_matches_oracle(cuda_device):
     assert rel(got, want[..., 0]) < FWD_GATE, rel(got, want[..., 0])
 
 
-def test_unet_gradients_match_oracle(cuda_device):
+@pytest.mark.parametrize("tcgen05", [0, 1])
+def test_unet_gradients_match_oracle(cuda_device, tcgen05):
     import torch
     from ds2d_b200.unet import UNet, flatten, unflatten
     p, x, t = _case(seed=1)
     n, h, w = x.shape[:3]
     loss_want, g_want, _ = uo.loss_and_grads(p, x, t)
     with UNet(max_n=n, max_h=h, max_w=w) as net:
+        net.set_option("tcgen05", tcgen05)
         net.set_params(flatten(p))
         dx = torch.from_numpy(x[..., 0].astype(np.float32)).cuda()
         dt = torch.from_numpy(t[..., 0].astype(np.float32)).cuda()
@@ -82,3 +86,24 @@ def test_unet_adam_training_reduces_loss(cuda_device):
             net.adam_step(lr=1e-3)
         last = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
     assert last < 0.3 * first, (first, last)
+
+
+def test_unet_tcgen05_and_mma_sync_agree_on_a_wide_image(cuda_device):
+    """Rows wider than one 128-pixel tensor-core tile, several channel groups: the two tensor-core
+    paths give the same forward output up to FP32 summation order and BF16 rounding."""
+    import torch
+    from ds2d_b200.unet import UNet, flatten
+    p = uo.init_params(4)
+    rng = np.random.default_rng(4)
+    n, h, w = 2, 24, 200
+    x = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32)).cuda()
+    out = []
+    with UNet(max_n=n, max_h=h, max_w=w) as net:
+        net.set_params(flatten(p))
+        for tc in (0, 1):
+            net.set_option("tcgen05", tc)
+            y = torch.zeros_like(x)
+            net.forward(x.data_ptr(), y.data_ptr(), n, h, w)
+            torch.cuda.synchronize()
+            out.append(y.cpu().numpy())
+    assert rel(out[1], out[0]) < 1e-2, rel(out[1], out[0])
