@@ -624,7 +624,7 @@ struct ds2d_unet {
   double *part = nullptr, *h_part = nullptr;
   std::string err;
   bool weights_dirty = true;
-  int use_tc = 0;          // 3x3 convolutions on tcgen05 (1) or mma.sync (0)
+  int use_tc = 1;          // 3x3 convolutions on tcgen05 (1, default) or mma.sync (0)
   int *d_err = nullptr;    // device flag raised by a bounded wait that gave up
   std::vector<void *> allocs;
 };
