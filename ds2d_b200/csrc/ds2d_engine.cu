@@ -228,6 +228,7 @@ struct ds2d_ctx {
   int opt_pcg_m = 8;         // ds2d_lsrtm_pcg: directions kept for explicit conjugation
   // Acoustic Born pair (LSRTM): background, scattered and adjoint states, Born overlay.
   float *ac[10] = {};        // bvx bvz bs | dvx dvz ds | yx yz ys | e
+  float *ac2[6] = {};        // second (ping-pong) buffers of bvx bvz bs | dvx dvz ds (fused steps)
   double *dot_part = nullptr, *dot_out = nullptr;  // FP64 inner-product scratch
   // Work vectors of the LSRTM solver (model- and data-space), grown on demand.
   struct Vec {
@@ -883,6 +884,9 @@ int ensure_acoustic(ds2d_ctx *c) {
   }
   for (float *&p : c->ac)
     if (!p && (rc = alloc_slots(c, &p))) return rc;
+  if (c->opt_fused && c->ring_ok)
+    for (float *&p : c->ac2)
+      if (!p && (rc = alloc_slots(c, &p))) return rc;
   if (!c->img_slot) {  // per-shot gradient planes (same 7-plane size as the RTM images)
     size_t n = (size_t)7 * c->B * c->d.wnx * c->d.wnz;
     if ((rc = alloc(c, (void **)&c->img_slot, n * sizeof(float)))) return rc;
@@ -902,10 +906,54 @@ AcArgs ac_args(ds2d_ctx *c, int set, int it, float dir) {
   return a;
 }
 
+// One fused acoustic forward step (k_ac_ring) of the buffer pair `set` (0 background, 1
+// scattered) from ping-pong side `cur` to 1 - cur.
+int ac_ring_step(ds2d_ctx *c, int n, int set, int cur, int it, bool born_out, bool record) {
+  const Dims &d = c->d;
+  const int nstrips = (d.nzp + kFTZ - 1) / kFTZ;
+  const int tz = (d.nzp + nstrips - 1) / nstrips;
+  const int xr = std::max(8, c->opt_xr);
+  dim3 grid(nstrips, (d.nxp + xr - 1) / xr, n);
+  float *side[2][3] = {{c->ac[3 * set], c->ac[3 * set + 1], c->ac[3 * set + 2]},
+                       {c->ac2[3 * set], c->ac2[3 * set + 1], c->ac2[3 * set + 2]}};
+  AcRingArgs a{};
+  a.d = d; a.shots = c->d_shots;
+  a.vx = side[cur][0]; a.vz = side[cur][1]; a.s = side[cur][2];
+  a.vx_n = side[1 - cur][0]; a.vz_n = side[1 - cur][1]; a.s_n = side[1 - cur][2];
+  a.b = c->par.b; a.lam = c->par.lam; a.m = c->par.dmp;
+  a.wavelet = c->wavelet; a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
+  if (set == 0) {
+    a.e_out = born_out ? c->ac[9] : nullptr;
+  } else {
+    a.e_in = c->ac[9];
+    if (record) { a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
+  }
+  const size_t sm = sizeof(float) * 4 * kAcRingFields * kFB;
+  void (*kfn)(AcRingArgs) = set == 0 ? k_ac_ring<0, 4> : k_ac_ring<1, 4>;
+  LAUNCHS("ac_ring", 0, kfn, grid, kFB, sm, a);
+  return DS2D_OK;
+}
+
 // L m for the uploaded batch: scattered vz / vx into rec[0] / rec[1] (m = the window p_dmp).
 int ac_L_batch(ds2d_ctx *c, int n) {
   const Dims &d = c->d;
   size_t bytes = sizeof(float) * (size_t)d.slot * n;
+  if (c->opt_fused && c->ring_ok && c->ac2[0]) {
+    // fused: per step one background launch (Born source out) and one scattered launch
+    for (int i = 0; i < 10; i++)
+      if (i < 6 || i == 9) CK(cudaMemsetAsync(c->ac[i], 0, bytes, c->stream));
+    for (float *p : c->ac2) CK(cudaMemsetAsync(p, 0, bytes, c->stream));
+    size_t nrec = (size_t)n * d.max_ntr * d.nt;
+    CK(cudaMemsetAsync(c->rec[0], 0, nrec * 4, c->stream));
+    CK(cudaMemsetAsync(c->rec[1], 0, nrec * 4, c->stream));
+    int rc;
+    for (int it = 0, cur = 0; it < d.nt; it++, cur ^= 1) {
+      if ((rc = ac_ring_step(c, n, 0, cur, it, true, false))) return rc;
+      if ((rc = ac_ring_step(c, n, 1, cur, it, false, true))) return rc;
+    }
+    CK(cudaGetLastError());
+    return DS2D_OK;
+  }
   for (int i = 0; i < 10; i++)
     if (i < 6 || i == 9) CK(cudaMemsetAsync(c->ac[i], 0, bytes, c->stream));
   size_t nrec = (size_t)n * d.max_ntr * d.nt;
@@ -939,11 +987,22 @@ int ac_LT_batch(ds2d_ctx *c, int n) {
   size_t plane = (size_t)c->B * d.wnx * d.wnz;
   CK(cudaMemsetAsync(c->img_slot, 0, plane * sizeof(float), c->stream));
   dim3 grid = cell_grid(d, n), blk(32, 8);
-  for (int it = 0; it < d.nt; it++) {
-    AcArgs b = ac_args(c, 0, it, 1.f);
-    b.src_on = 1;
-    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
-    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+  if (c->opt_fused && c->ring_ok && c->ac2[0]) {
+    // fused forward replay of the background; the reversal below runs in place on ac[0..2]
+    for (int i = 0; i < 3; i++) CK(cudaMemsetAsync(c->ac2[i], 0, bytes, c->stream));
+    int rc, cur = 0;
+    for (int it = 0; it < d.nt; it++, cur ^= 1)
+      if ((rc = ac_ring_step(c, n, 0, cur, it, false, false))) return rc;
+    if (cur == 1)
+      for (int i = 0; i < 3; i++)
+        CK(cudaMemcpyAsync(c->ac[i], c->ac2[i], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    for (int it = 0; it < d.nt; it++) {
+      AcArgs b = ac_args(c, 0, it, 1.f);
+      b.src_on = 1;
+      LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
+      LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+    }
   }
   for (int it = d.nt - 1; it >= 0; --it) {
     AcAdjArgs y{};

@@ -876,4 +876,132 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
   cp_async_wait<0>();
 }
 
+// ---------------------------------------------------------------------------------------------
+// Acoustic forward step fed by the ring (vs = 0: the stress is one field s = txx = tzz, txz = 0),
+// the fused counterpart of k_ac_vel + k_ac_str (+ k_ac_born).  Same x-march as k_fwd_ring: at row
+// step r the velocities of row r - 4 (from the window of S = s + overlay) and the stress of row
+// r - 8 (from the new velocities) are updated, state ping-pongs between two buffers.
+//   kMode 0 (background): the explosive source is the overlay on s; with `e` set, the stress
+//           stage also writes the Born source e = -2 lam m (Dx- vx / dx + Dz- vz / dz) of the new
+//           velocities on the interior (the k_ac_born of the same step).
+//   kMode 1 (scattered): the Born source e of the same step is the overlay on s; the new
+//           velocities are recorded at the receivers.
+// Ring fields of slot q: 0 s and 1 e (overlay, mode 1) of row q; 2 vx, 3 vz, 4 b of row q - 4;
+// 5 s (own state), 6 lam, 7 m of row q - 8.
+// ---------------------------------------------------------------------------------------------
+constexpr int kAcRingFields = 8;
+
+struct AcRingArgs {
+  Dims d;
+  const ShotDev *shots;
+  const float *vx, *vz, *s;  // state at t-1 (read)
+  float *vx_n, *vz_n, *s_n;  // state at t (written)
+  const float *b, *lam, *m;
+  const float *e_in;         // mode 1: Born source overlay
+  float *e_out;              // mode 0: Born source written (or null)
+  const float *wavelet;
+  int it, tz, xr;
+  const int *rmap;
+  float *rec_vz, *rec_vx;    // mode 1: records [slot][max_ntr][nt]
+};
+
+template <int kMode, int kD>
+__global__ void __launch_bounds__(kFB, 6) k_ac_ring(AcRingArgs a) {
+  static_assert(kD >= 2 && (kD & (kD - 1)) == 0, "ring depth: a power of two");
+  extern __shared__ float ring[];  // [kD][kAcRingFields][kFB]
+  __shared__ float s_S[kFB], s_vz[kFB];
+  const int sl = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[sl]);
+  const int z = blockIdx.x * a.tz - 8 + t;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  const int base = (int)(d.slot * sl);  // cell offsets fit 32 bits (checked on the host)
+  const int ld = d.ld;
+  const bool zin = z >= 0 && z < d.nzp;
+  const bool zupd = z >= d.nop && z < d.nzp - d.nop;
+  const bool z_int = z >= d.pml && z < d.nzp - d.pml;
+  const bool vcol = t >= 4 && t < a.tz + 12 && zupd;
+  const bool scol = t >= 8 && t < a.tz + 8 && zupd;
+  const ShotDev sh = a.shots[sl];
+  const float sval = kMode == 0 ? a.wavelet[a.it] : 0.f;
+  const bool src_col = kMode == 0 && z == sh.isz;
+  const float cx = d.dt / d.dx, cz = d.dt / d.dz;
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
+  const float *src[kAcRingFields] = {a.s, a.e_in, a.vx, a.vz, a.b, a.s, a.lam, a.m};
+  auto R = [&](int q, int f) -> float & {
+    return ring[((q & (kD - 1)) * kAcRingFields + f) * kFB + t];
+  };
+  auto used = [&](int f) {
+    return !(f == 1 && kMode != 1) && !(f == 7 && (kMode != 0 || !a.e_out));
+  };
+  auto issue = [&](int q) {
+#pragma unroll
+    for (int f = 0; f < kAcRingFields; f++) {
+      const int row = q - (f < 2 ? 0 : (f < 5 ? 4 : 8));
+      if (!used(f)) continue;
+      if (row >= 0 && row < d.nxp && zin)
+        cp_async4(&R(q, f), src[f] + (base + row * ld + z));
+      else
+        R(q, f) = 0.f;
+    }
+    cp_async_commit();
+  };
+
+  float w_S[9], w_vx[9], w_vz[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_S[i] = w_vx[i] = w_vz[i] = 0.f;
+
+#pragma unroll
+  for (int j = 0; j < kD - 1; j++) issue(x0 - 8 + j);
+  for (int r = x0 - 8; r < x1 + 8; r++) {
+    cp_async_wait<kD - 2>();  // row r has landed (this thread's copies)
+    float nS = R(r, 0);
+    if (kMode == 1) nS += R(r, 1);
+    if (src_col && r == sh.isx) nS += sval;  // FD2DGPU.cu:2039-2049 (transient)
+    push(w_S, nS);
+    issue(r + kD - 1);  // into the slot of row r - 1 (mod kD), finished last step
+    // ---- velocities of row rv = r - 4 ----------------------------------------------------
+    const int rv = r - 4;
+    s_S[t] = w_S[4];
+    __syncthreads();
+    float vxn = 0.f, vzn = 0.f;
+    if (vcol && r >= x0 && rv >= d.nop && rv < d.nxp - d.nop) {
+      const int k = base + rv * ld + z;
+      const float ax = dxp_mid(w_S);
+      const float az = stencil4([&](int i) { return s_S[t + i] - s_S[t - i + 1]; });
+      const float bb = R(r, 4);
+      vxn = R(r, 2) + 1.0f * (bb * cx) * ax;  // k_ac_vel: v + dir (b dt/d) D+ S, dir = +1
+      vzn = R(r, 3) + 1.0f * (bb * cz) * az;
+      if (rv >= x0 && rv < x1 && t >= 8 && t < a.tz + 8) {
+        a.vx_n[k] = vxn;
+        a.vz_n[k] = vzn;
+        if (kMode == 1 && z == sh.igz) {
+          const int tr = a.rmap[(long long)sl * d.nxp_max + rv];
+          if (tr >= 0) {
+            const long long q = ((long long)sl * d.max_ntr + tr) * d.nt + a.it;
+            a.rec_vz[q] = vzn;
+            a.rec_vx[q] = vxn;
+          }
+        }
+      }
+    }
+    push(w_vx, vxn);
+    push(w_vz, vzn);
+    // ---- stress of row rs = r - 8 --------------------------------------------------------
+    const int rs = r - 8;
+    s_vz[t] = w_vz[4];
+    __syncthreads();
+    if (scol && rs >= x0 && rs < x1 && rs >= d.nop && rs < d.nxp - d.nop) {
+      const int k = base + rs * ld + z;
+      const float sx = dxm_mid(w_vx);
+      const float sz = stencil4([&](int i) { return s_vz[t + i - 1] - s_vz[t - i]; });
+      const float lam = R(r, 6);
+      a.s_n[k] = R(r, 5) + 1.0f * lam * (cx * sx + cz * sz);  // k_ac_str, dir = +1
+      if (kMode == 0 && a.e_out && rs >= d.pml && rs < d.nxp - d.pml && z_int)
+        a.e_out[k] = -2.0f * lam * R(r, 7) * (sx * rdx + sz * rdz);  // k_ac_born
+    }
+  }
+  cp_async_wait<0>();
+}
+
 }  // namespace ds2d

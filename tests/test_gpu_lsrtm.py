@@ -157,3 +157,20 @@ def test_lsrtm_pcg_plain_matches_cgls_and_net_descends(cuda_device):
             mo.zero_()
             hist_n, _ = e.lsrtm_pcg(shots, tz.data_ptr(), tx.data_ptr(), mo.data_ptr(), 4, net=net)
     assert np.all(np.diff(np.concatenate([[1.0], hist_n])) < 0), hist_n
+
+
+def test_acoustic_fused_steps_match_half_steps(cuda_device):
+    """The fused acoustic step (velocity + stress + Born source in one x-march, ping-pong state)
+    against one launch per half step, for L and L^T."""
+    c, vp, vs, w, shots, m = acoustic_case(nt=300, nshots=3)
+    out = {}
+    for fused in (0, 1):
+        with ctx(c, shots) as e:
+            e.set_option("fused", fused)
+            e.set_models(vp, vs)
+            e.set_wavelet(w)
+            dz, dx = e.ac_born(shots, m)
+            g = e.ac_born_adj(shots, dz, dx)
+            out[fused] = (dz, dx, g)
+    for a, b in zip(out[1], out[0]):
+        assert rel(a, b) < 1e-6, rel(a, b)
