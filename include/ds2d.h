@@ -135,8 +135,9 @@ long long ds2d_last_launches(const ds2d_ctx *ctx);
  *                     lengths; stops after niter iterations or when ||d - L m|| / ||d|| <=
  *                     target; resid[k] receives that ratio after iteration k.
  *   ds2d_lsrtm_pcg    the same problem by flexible preconditioned CG: direction z = P(L^T r)
- *                     with P the U-Net `net` (NULL: P = I, plain CG), Polak-Ribiere+ conjugation
- *                     and the exact step <r, L p> / ||L p||^2; when an iteration with the
+ *                     with P the U-Net `net` (NULL: P = I, plain CG), explicit L^T L-conjugation
+ *                     against the last "pcg_m" directions (default 8; flexible CG, FCG(M)) and
+ *                     the exact step <r, L p> / ||L p||^2; when an iteration with the
  *                     network reduces the residual by less than the "pcg_switch" option (per
  *                     mille, default 970) the solver restarts as plain CG from the current
  *                     iterate.  elapsed_ms[k] (may be NULL) is the wall time from the call's start
@@ -184,7 +185,7 @@ int ds2d_dot_f64_noalloc(const float *a, const float *b, long long n, void *stre
  * "xr" (rows marched by one CTA of the fused kernels), "ring" (cp.async prefetch ring depth of
  * the fused kernels: 0 off, 1 default, or 2 / 4 / 8), "occ" (0 / 1: register budget for 6 / 8
  * forward and 3 / 4 backward CTAs per SM), "graph" (0 / 1: capture batches in CUDA graphs),
- * "adjoint_born" (see ds2d_elsrtm), "pcg_switch" (see ds2d_lsrtm_pcg). */
+ * "adjoint_born" (see ds2d_elsrtm), "pcg_switch" and "pcg_m" (1..15, see ds2d_lsrtm_pcg). */
 int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
 
 /* Profiling (no counterpart in the reference, which has only a commented-out host timer,
