@@ -549,7 +549,7 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
     a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
     if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
     if (c->opt_ring && c->ring_ok) {
-      const size_t sm = sizeof(float) * c->opt_ring * kFwdRingFields * kFB;
+      const size_t sm = sizeof(float) * c->opt_ring * fwd_ring_fields(!d.rbc) * kFB;
       FwdFn kfn = fwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ);
       LAUNCHS("fwd_fused", kBytesFused * CELLS(n), kfn, grid, kFB, sm, a);
     } else if (d.rbc) {
@@ -717,7 +717,7 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
       a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
       a.img = c->img_slot; a.img_plane = (long long)plane;
       if (c->opt_ring && c->ring_ok) {
-        const size_t sm = sizeof(float) * c->opt_ring * kBwdRingFields * kFB;
+        const size_t sm = sizeof(float) * c->opt_ring * bwd_ring_fields(!d.rbc) * kFB;
         BwdFn kfn = bwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ);
         LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, fgrid, kFB, sm, a);
       } else if (d.rbc) {
@@ -1146,10 +1146,10 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
     // Ring-fed kernels may use more than the default 48 KB of dynamic shared memory.
     cudaError_t e = cudaSuccess;
     for (int depth : kRingDepths) {
-      const int fwd_sm = (int)(sizeof(float) * depth * kFwdRingFields * kFB);
-      const int bwd_sm = (int)(sizeof(float) * depth * kBwdRingFields * kFB);
       for (bool rbc : {false, true})
         for (int occ : {0, 1}) {
+          const int fwd_sm = (int)(sizeof(float) * depth * fwd_ring_fields(!rbc) * kFB);
+          const int bwd_sm = (int)(sizeof(float) * depth * bwd_ring_fields(!rbc) * kFB);
           if (e == cudaSuccess)
             e = cudaFuncSetAttribute(fwd_ring_fn(rbc, depth, occ),
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_sm);

@@ -115,11 +115,12 @@ __global__ void __launch_bounds__(kFB) k_fwd_fused(FwdFusedArgs a) {
       const bool own = rv >= x0 && rv < x1 && t >= 8 && t < a.tz + 8;
       if (kPML && pml_cell(d, rv, z)) {
         const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-        const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-        const float vxx = __fdiv_rn(fmaf(d1, a.a.vx_x[k], ux_x), d2);
-        const float vxz = __fdiv_rn(fmaf(d3, a.a.vx_z[k], ux_z), d4);
-        const float vzx = __fdiv_rn(fmaf(d1, a.a.vz_x[k], uz_x), d2);
-        const float vzz = __fdiv_rn(fmaf(d3, a.a.vz_z[k], uz_z), d4);
+        const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+        const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
+        const float vxx = fmaf(d1, a.a.vx_x[k], ux_x) * i2;
+        const float vxz = fmaf(d3, a.a.vx_z[k], ux_z) * i4;
+        const float vzx = fmaf(d1, a.a.vz_x[k], uz_x) * i2;
+        const float vzz = fmaf(d3, a.a.vz_z[k], uz_z) * i4;
         if (own) {
           a.b.vx_x[k] = vxx; a.b.vx_z[k] = vxz; a.b.vz_x[k] = vzx; a.b.vz_z[k] = vzz;
         }
@@ -162,13 +163,14 @@ __global__ void __launch_bounds__(kFB) k_fwd_fused(FwdFusedArgs a) {
       const float xz_x = dtdx * mu * sf, xz_z = dtdz * mu * se;
       if (kPML && pml_cell(d, rs, z)) {
         const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-        const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-        const float a1 = __fdiv_rn(fmaf(d1, a.a.txx_x[k], xx_x), d2);
-        const float a2 = __fdiv_rn(fmaf(d3, a.a.txx_z[k], xx_z), d4);
-        const float b1 = __fdiv_rn(fmaf(d1, a.a.tzz_x[k], zz_x), d2);
-        const float b2 = __fdiv_rn(fmaf(d3, a.a.tzz_z[k], zz_z), d4);
-        const float c1 = __fdiv_rn(fmaf(d1, a.a.txz_x[k], xz_x), d2);
-        const float c2 = __fdiv_rn(fmaf(d3, a.a.txz_z[k], xz_z), d4);
+        const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+        const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
+        const float a1 = fmaf(d1, a.a.txx_x[k], xx_x) * i2;
+        const float a2 = fmaf(d3, a.a.txx_z[k], xx_z) * i4;
+        const float b1 = fmaf(d1, a.a.tzz_x[k], zz_x) * i2;
+        const float b2 = fmaf(d3, a.a.tzz_z[k], zz_z) * i4;
+        const float c1 = fmaf(d1, a.a.txz_x[k], xz_x) * i2;
+        const float c2 = fmaf(d3, a.a.txz_z[k], xz_z) * i4;
         a.b.txx_x[k] = a1; a.b.txx_z[k] = a2;
         a.b.tzz_x[k] = b1; a.b.tzz_z[k] = b2;
         a.b.txz_x[k] = c1; a.b.txz_z[k] = c2;
@@ -217,14 +219,23 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // Forward step fed by the ring: same arithmetic as k_fwd_fused.  Fields of ring slot q:
 // 0 txx, 1 tzz, 2 txz of row q (stencil windows); 3 vx, 4 vz, 5 b of row q-4 (velocity stage);
-// 6 lam, 7 mu of row q-8 (stress stage).
+// 6 lam, 7 mu of row q-8 (stress stage).  With PML the split operands of a PML cell come through
+// the ring too (a PML cell does not read its own vx, vz, so slots 3-4 carry vx_x, vx_z):
+// 8 vz_x, 9 vz_z, 10 dampx, 11 dampz of row q-4; 12 dampx, 13 dampz, 14 txx_x, 15 txx_z,
+// 16 tzz_x, 17 tzz_z, 18 txz_x, 19 txz_z of row q-8.
 constexpr int kFwdRingFields = 8;
+constexpr int kFwdRingFieldsPml = 20;
+__host__ __device__ constexpr int fwd_ring_fields(bool pml) {
+  return pml ? kFwdRingFieldsPml : kFwdRingFields;
+}
 
 template <bool kPML, int kD, int kMinB>
 __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
-  static_assert(kD >= 2 && (kD & (kD - 1)) == 0, "ring depth: a power of two");
-  extern __shared__ float ring[];  // [kD][kFwdRingFields][kFB]
+  static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
+  constexpr int NF = fwd_ring_fields(kPML);
+  extern __shared__ float ring[];  // [kD][NF][kFB]
   __shared__ float s_txz[kFB], s_tzz[kFB], s_vx[kFB], s_vz[kFB];
+  __shared__ int s_tr[16];  // receiver column: trace index of velocity row mod 16, 8 rows ahead
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int z = blockIdx.x * a.tz - 8 + t;
@@ -239,21 +250,54 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
   const ShotDev sh = a.shots[s];
   const float sval = a.wavelet[a.it];
   const bool src_col = z == sh.isz;
+  const bool rec_col = a.rec_on && z == sh.igz;
+  const int *rmap = a.rmap + (long long)s * d.nxp_max;
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
-  const float *src[kFwdRingFields] = {a.a.txx, a.a.tzz, a.a.txz, a.a.vx,
-                                      a.a.vz, a.p.b,   a.p.lam, a.p.mu};
   // R(q, f): field f of ring slot q (row q for f < 3, row q-4 for f < 6, row q-8 otherwise)
-  auto R = [&](int q, int f) -> float & {
-    return ring[((q & (kD - 1)) * kFwdRingFields + f) * kFB + t];
-  };
+  auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kFB + t]; };
   auto issue = [&](int q) {
-#pragma unroll
-    for (int f = 0; f < kFwdRingFields; f++) {
-      const int row = q - (f < 3 ? 0 : (f < 6 ? 4 : 8));
-      if (row >= 0 && row < d.nxp && zin)
-        cp_async4(&R(q, f), src[f] + (base + row * ld + z));
-      else
-        R(q, f) = 0.f;
+    const int r0 = q, r4 = q - 4, r8 = q - 8;
+    const bool in0 = r0 >= 0 && r0 < d.nxp && zin;
+    const bool in4 = r4 >= 0 && r4 < d.nxp && zin;
+    const bool in8 = r8 >= 0 && r8 < d.nxp && zin;
+    const int o0 = base + r0 * ld + z, o4 = base + r4 * ld + z, o8 = base + r8 * ld + z;
+    const bool pml4 = kPML && in4 && pml_cell(d, r4, z);
+    const bool pml8 = kPML && in8 && pml_cell(d, r8, z);
+    if (in0) {
+      cp_async4(&R(q, 0), a.a.txx + o0);
+      cp_async4(&R(q, 1), a.a.tzz + o0);
+      cp_async4(&R(q, 2), a.a.txz + o0);
+    } else {
+      R(q, 0) = R(q, 1) = R(q, 2) = 0.f;
+    }
+    if (in4) {
+      cp_async4(&R(q, 3), (pml4 ? a.a.vx_x : a.a.vx) + o4);
+      cp_async4(&R(q, 4), (pml4 ? a.a.vx_z : a.a.vz) + o4);
+      cp_async4(&R(q, 5), a.p.b + o4);
+    } else {
+      R(q, 3) = R(q, 4) = R(q, 5) = 0.f;
+    }
+    if (in8) {
+      cp_async4(&R(q, 6), a.p.lam + o8);
+      cp_async4(&R(q, 7), a.p.mu + o8);
+    } else {
+      R(q, 6) = R(q, 7) = 0.f;
+    }
+    if (kPML && pml4) {
+      cp_async4(&R(q, 8), a.a.vz_x + o4);
+      cp_async4(&R(q, 9), a.a.vz_z + o4);
+      cp_async4(&R(q, 10), a.p.dampx + o4);
+      cp_async4(&R(q, 11), a.p.dampz + o4);
+    }
+    if (kPML && pml8) {
+      cp_async4(&R(q, 12), a.p.dampx + o8);
+      cp_async4(&R(q, 13), a.p.dampz + o8);
+      cp_async4(&R(q, 14), a.a.txx_x + o8);
+      cp_async4(&R(q, 15), a.a.txx_z + o8);
+      cp_async4(&R(q, 16), a.a.tzz_x + o8);
+      cp_async4(&R(q, 17), a.a.tzz_z + o8);
+      cp_async4(&R(q, 18), a.a.txz_x + o8);
+      cp_async4(&R(q, 19), a.a.txz_z + o8);
     }
     cp_async_commit();
   };
@@ -266,6 +310,13 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
   for (int j = 0; j < kD - 1; j++) issue(x0 - 8 + j);
   for (int r = x0 - 8; r < x1 + 8; r++) {
     cp_async_wait<kD - 2>();  // row r has landed (this thread's copies)
+    if (rec_col) {  // trace index of velocity row r + 4 (read 8 steps on, landed by then)
+      const int q = r + 4;
+      if (q >= 0 && q < d.nxp)
+        cp_async4((float *)&s_tr[q & 15], (const float *)(rmap + q));
+      else
+        s_tr[q & 15] = -1;
+    }
     float n_txx = R(r, 0), n_tzz = R(r, 1);
     const float n_txz = R(r, 2);
     if (src_col && r == sh.isx) {  // FD2DGPU.cu:2039-2049 (transient)
@@ -293,13 +344,13 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
       const float ux_x = cbx * ax, ux_z = cbz * bz, uz_x = cbx * fx, uz_z = cbz * ez;
       const bool own = rv >= x0 && rv < x1 && t >= 8 && t < a.tz + 8;
       if (kPML && pml_cell(d, rv, z)) {
-        const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+        const float ddx = R(r, 10) * d.dt * 0.5f, ddz = R(r, 11) * d.dt * 0.5f;
         const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
         const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
-        const float vxx = fmaf(d1, a.a.vx_x[k], ux_x) * i2;
-        const float vxz = fmaf(d3, a.a.vx_z[k], ux_z) * i4;
-        const float vzx = fmaf(d1, a.a.vz_x[k], uz_x) * i2;
-        const float vzz = fmaf(d3, a.a.vz_z[k], uz_z) * i4;
+        const float vxx = fmaf(d1, R(r, 3), ux_x) * i2;
+        const float vxz = fmaf(d3, R(r, 4), ux_z) * i4;
+        const float vzx = fmaf(d1, R(r, 8), uz_x) * i2;
+        const float vzz = fmaf(d3, R(r, 9), uz_z) * i4;
         if (own) {
           a.b.vx_x[k] = vxx; a.b.vx_z[k] = vxz; a.b.vz_x[k] = vzx; a.b.vz_z[k] = vzz;
         }
@@ -312,8 +363,8 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
       if (own) {
         a.b.vx[k] = vxn;
         a.b.vz[k] = vzn;
-        if (a.rec_on && z == sh.igz) {
-          const int tr = a.rmap[(long long)s * d.nxp_max + rv];
+        if (rec_col) {
+          const int tr = s_tr[rv & 15];
           if (tr >= 0) {
             const long long q = ((long long)s * d.max_ntr + tr) * d.nt + a.it;
             a.rec_vz[q] = vzn;
@@ -341,15 +392,15 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
       const float zz_x = lam * dtdx * sa, zz_z = l2m * dtdz * sb;
       const float xz_x = dtdx * mu * sf, xz_z = dtdz * mu * se;
       if (kPML && pml_cell(d, rs, z)) {
-        const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+        const float ddx = R(r, 12) * d.dt * 0.5f, ddz = R(r, 13) * d.dt * 0.5f;
         const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
         const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
-        const float a1 = fmaf(d1, a.a.txx_x[k], xx_x) * i2;
-        const float a2 = fmaf(d3, a.a.txx_z[k], xx_z) * i4;
-        const float b1 = fmaf(d1, a.a.tzz_x[k], zz_x) * i2;
-        const float b2 = fmaf(d3, a.a.tzz_z[k], zz_z) * i4;
-        const float c1 = fmaf(d1, a.a.txz_x[k], xz_x) * i2;
-        const float c2 = fmaf(d3, a.a.txz_z[k], xz_z) * i4;
+        const float a1 = fmaf(d1, R(r, 14), xx_x) * i2;
+        const float a2 = fmaf(d3, R(r, 15), xx_z) * i4;
+        const float b1 = fmaf(d1, R(r, 16), zz_x) * i2;
+        const float b2 = fmaf(d3, R(r, 17), zz_z) * i4;
+        const float c1 = fmaf(d1, R(r, 18), xz_x) * i2;
+        const float c2 = fmaf(d3, R(r, 19), xz_z) * i4;
         a.b.txx_x[k] = a1; a.b.txx_z[k] = a2;
         a.b.tzz_x[k] = b1; a.b.tzz_z[k] = b2;
         a.b.txz_x[k] = c1; a.b.txz_z[k] = c2;
@@ -510,11 +561,12 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
         const float oxx = __ldg(a.aa.txx + k), ozz = __ldg(a.aa.tzz + k);
         if (kPML && pml_cell(d, r1, z)) {
           const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-          const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-          atxx = __fdiv_rn(fmaf(d1, oxx, xx), d2);
-          atzz = __fdiv_rn(fmaf(d3, ozz, zz), d4);
-          const float q1 = __fdiv_rn(fmaf(d1, a.aa.txz_x[k], xz_x), d2);
-          const float q2 = __fdiv_rn(fmaf(d3, a.aa.txz_z[k], xz_z), d4);
+          const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+          const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
+          atxx = fmaf(d1, oxx, xx) * i2;
+          atzz = fmaf(d3, ozz, zz) * i4;
+          const float q1 = fmaf(d1, a.aa.txz_x[k], xz_x) * i2;
+          const float q2 = fmaf(d3, a.aa.txz_z[k], xz_z) * i4;
           if (own) {
             a.ab.txz_x[k] = q1;
             a.ab.txz_z[k] = q2;
@@ -596,11 +648,12 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
         float vx, vz;
         if (kPML && pml_cell(d, r2, z)) {
           const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-          const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-          const float vxx = __fdiv_rn(fmaf(d1, a.aa.vx_x[k], ux_x), d2);
-          const float vxz = __fdiv_rn(fmaf(d3, a.aa.vx_z[k], ux_z), d4);
-          const float vzx = __fdiv_rn(fmaf(d1, a.aa.vz_x[k], uz_x), d2);
-          const float vzz = __fdiv_rn(fmaf(d3, a.aa.vz_z[k], uz_z), d4);
+          const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+          const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
+          const float vxx = fmaf(d1, a.aa.vx_x[k], ux_x) * i2;
+          const float vxz = fmaf(d3, a.aa.vx_z[k], ux_z) * i4;
+          const float vzx = fmaf(d1, a.aa.vz_x[k], uz_x) * i2;
+          const float vzz = fmaf(d3, a.aa.vz_z[k], uz_z) * i4;
           a.ab.vx_x[k] = vxx; a.ab.vx_z[k] = vxz; a.ab.vz_x[k] = vzx; a.ab.vz_z[k] = vzz;
           vx = vxx + vxz;
           vz = vzx + vzz;
@@ -624,14 +677,43 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
 //  0-3   bvx, bvz, avx, avz of row q            (stage-1 stencil windows)
 //  4-15  btxx, btzz, btxz, atxx, atzz, atxz, lam, mu, kpp, kps, img pp, img ps of row q-4
 //  16-17 b, img illumination of row q-8          (stage 2)
+// With PML and strips every operand that a cell of the band reads is prefetched the same way, so
+// no load waits inside the march.  A PML cell is never an imaging cell and never reads its own
+// atxz, so for it the slots of atxz, kpp, kps, img pp (row q-4) carry atxz_x, atxz_z, dampx,
+// dampz, and the slot of the illumination (row q-8) carries dampx; a strip-band cell takes its
+// velocities from the strips, so slots 0-1 carry the strip words of its row.  Extra fields:
+//  18-22 dampz, avx_x, avx_z, avz_x, avz_z of row q-8  (PML cells, stage 2)
+//  23-24 bvx, bvz of row q-8   (inner strip-band cells: their own state, stage 2)
+//  25-26 the FP32 scales of the two strip words of row q  (FP16 / BF16 strips)
 constexpr int kBwdRingFields = 18;
+constexpr int kBwdRingFieldsPml = 27;
+__host__ __device__ constexpr int bwd_ring_fields(bool pml) {
+  return pml ? kBwdRingFieldsPml : kBwdRingFields;
+}
+
+// Band value of strip element e from its ring copy: the FP32 element itself, or the aligned
+// 32-bit word holding the FP16 / BF16 element (upper half for odd e) times its segment's scale.
+// Same result as strip_get.
+__device__ __forceinline__ float strip_unpack(int prec, long long e, float word, float sc) {
+  if (prec == 0) return word;
+  const unsigned u = __float_as_uint(word);
+  const unsigned short h = (unsigned short)((e & 1) ? (u >> 16) : (u & 0xffffu));
+  if (prec == 1) return __half2float(__ushort_as_half(h)) * sc;
+  return __bfloat162float(__ushort_as_bfloat16(h)) * sc;
+}
 
 template <bool kPML, int kD, int kMinB>
 __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
-  static_assert(kD >= 2 && (kD & (kD - 1)) == 0, "ring depth: a power of two");
-  extern __shared__ float ring[];  // [kD][kBwdRingFields][kFB]
+  static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
+  constexpr int NF = bwd_ring_fields(kPML);
+  extern __shared__ float ring[];  // [kD][NF][kFB]
   __shared__ float s_bvx[kFB], s_bvz[kFB], s_avx[kFB], s_avz[kFB];
   __shared__ float s_btxz[kFB], s_btzz[kFB], s_m[kFB], s_pzlx[kFB];
+  // Receiver column (one thread of the CTA, if any): per row mod 16, the trace index (fetched 16
+  // rows ahead), whether a trace sits there and its residual at this step (fetched 8 rows ahead)
+  // and the cell's state without the residual (kept 8 rows for stage 2).
+  __shared__ int s_tr[16], s_has[16];
+  __shared__ float s_rz[16], s_rx[16], s_ownx[16], s_ownz[16];
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int z = blockIdx.x * a.tz - 8 + t;
@@ -646,6 +728,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
   const bool z_upd = z >= d.nop && z < d.nzp - d.nop;
   const ShotDev sh = a.shots[s];
   const bool rec_col = z == sh.igz;
+  const bool strips = kPML && a.strips_on;
   const float *res_z = a.res_vz + (long long)s * d.max_ntr * d.nt + a.it;
   const float *res_x = a.res_vx + (long long)s * d.max_ntr * d.nt + a.it;
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
@@ -653,32 +736,78 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
   const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
   const int img_row = s * d.wnx_max;  // image row of model row r: img_row + r - pml
   float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
-  const float *grid_src[16] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.txx, a.ra.tzz,
-                               a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz, a.p.lam,  a.p.mu,
-                               a.p.kpp,  a.p.kps,  a.p.b,    nullptr};
-  auto R = [&](int q, int f) -> float & {
-    return ring[((q & (kD - 1)) * kBwdRingFields + f) * kFB + t];
-  };
+  const long long strip_row0 = ((long long)s * d.nt + a.it) * 2;  // strip row of component 0
+  const float *grid_src[15] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.txx,
+                               a.ra.tzz, a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz,
+                               a.p.lam,  a.p.mu,   a.p.kpp,  a.p.kps,  a.p.b};
+  auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kFB + t]; };
+  auto strip_elem = [&](int comp, int bo) { return (strip_row0 + comp) * d.lb_max + bo; };
   auto issue = [&](int q) {
+    const int r0 = q, r4 = q - 4, r8 = q - 8;
+    const bool in0 = r0 >= 0 && r0 < d.nxp && zin;
+    const bool in4 = r4 >= 0 && r4 < d.nxp && zin;
+    const bool in8 = r8 >= 0 && r8 < d.nxp && zin;
+    const int o0 = base + r0 * ld + z, o4 = base + r4 * ld + z, o8 = base + r8 * ld + z;
+    const bool int4 = in4 && r4 >= pml && r4 < d.nxp - pml && z_int;
+    const bool int8 = in8 && r8 >= pml && r8 < d.nxp - pml && z_int;
+    const bool pml4 = kPML && in4 && pml_cell(d, r4, z);
+    const bool pml8 = kPML && in8 && pml_cell(d, r8, z);
+    const int bo0 = strips && in0 ? band_offset(d, r0, z) : -1;
+    // lag 0: stencil inputs (strip words in the band)
 #pragma unroll
-    for (int f = 0; f < kBwdRingFields; f++) {
-      const int lag = f < 4 ? 0 : (f < 16 ? 4 : 8);
-      const int row = q - lag;
-      const bool img = f == 14 || f == 15 || f == 17;
+    for (int f = 0; f < 4; f++) {
       float *dst = &R(q, f);
-      if (img) {
-        if (row >= pml && row < d.nxp - pml && z_int && zin) {
-          float *src = f == 14 ? img_pp : (f == 15 ? img_ps : img_il);
-          cp_async4(dst, src + ((img_row + row - pml) * d.wnz + (z - pml)));
+      if (!in0) {
+        *dst = 0.f;
+      } else if (kPML && f < 2 && bo0 >= 0) {
+        const long long e = strip_elem(f, bo0);
+        if (a.st.prec == 0) {
+          cp_async4(dst, (const float *)a.st.data + e);
         } else {
-          *dst = 0.f;
+          cp_async4(dst, (const float *)((const char *)a.st.data + ((e * 2) & ~3LL)));
+          cp_async4(&R(q, 25 + f), a.st.scale + (strip_row0 + f) * d.nseg_max + (bo0 >> 5));
         }
-      } else if (row >= 0 && row < d.nxp && zin) {
-        const float *src = grid_src[f < 14 ? f : 14];
-        cp_async4(dst, src + (base + row * ld + z));
+      } else {
+        cp_async4(dst, grid_src[f] + o0);
+      }
+    }
+    // lag 4: stage-1 own-cell operands
+#pragma unroll
+    for (int f = 4; f < 16; f++) {
+      float *dst = &R(q, f);
+      if (kPML && pml4 && (f == 9 || (f >= 12 && f <= 15))) {
+        if (f == 9) cp_async4(dst, a.aa.txz_x + o4);
+        if (f == 12) cp_async4(dst, a.aa.txz_z + o4);
+        if (f == 13) cp_async4(dst, a.p.dampx + o4);
+        if (f == 14) cp_async4(dst, a.p.dampz + o4);
+      } else if (f == 14 || f == 15) {
+        if (int4)
+          cp_async4(dst, (f == 14 ? img_pp : img_ps) + ((img_row + r4 - pml) * d.wnz + (z - pml)));
+        else
+          *dst = 0.f;
+      } else if (in4) {
+        cp_async4(dst, grid_src[f] + o4);
       } else {
         *dst = 0.f;
       }
+    }
+    // lag 8: stage-2 own-cell operands
+    if (in8) cp_async4(&R(q, 16), a.p.b + o8); else R(q, 16) = 0.f;
+    if (kPML && pml8) {
+      cp_async4(&R(q, 17), a.p.dampx + o8);
+      cp_async4(&R(q, 18), a.p.dampz + o8);
+      cp_async4(&R(q, 19), a.aa.vx_x + o8);
+      cp_async4(&R(q, 20), a.aa.vx_z + o8);
+      cp_async4(&R(q, 21), a.aa.vz_x + o8);
+      cp_async4(&R(q, 22), a.aa.vz_z + o8);
+    } else if (int8) {
+      cp_async4(&R(q, 17), img_il + ((img_row + r8 - pml) * d.wnz + (z - pml)));
+      if (strips && band_offset(d, r8, z) >= 0) {
+        cp_async4(&R(q, 23), a.ra.vx + o8);
+        cp_async4(&R(q, 24), a.ra.vz + o8);
+      }
+    } else {
+      R(q, 17) = 0.f;
     }
     cp_async_commit();
   };
@@ -696,23 +825,50 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
 
 #pragma unroll
   for (int j = 0; j < kD - 1; j++) issue(x0 - 8 + j);
+  if (rec_col) {  // trace indexes of the first 16 rows, residuals of the first 8 (direct loads)
+    for (int q = x0 - 8; q < x0 + 8; q++) s_tr[q & 15] = (q >= 0 && q < d.nxp) ? rmap[q] : -1;
+    for (int q = x0 - 8; q < x0; q++) {
+      const int tr = s_tr[q & 15];
+      s_has[q & 15] = tr >= 0;
+      if (tr >= 0) {
+        s_rz[q & 15] = res_z[(long long)tr * d.nt];
+        s_rx[q & 15] = res_x[(long long)tr * d.nt];
+      }
+    }
+  }
   for (int r = x0 - 8; r < x1 + 8; r++) {
     cp_async_wait<kD - 2>();  // slot r has landed (this thread's copies)
+    if (rec_col) {
+      // Residual of row r + 8 and trace index of row r + 16, copied asynchronously with this
+      // step's commit group (landed kD - 1 <= 7 steps later, before either is read).
+      const int q8 = r + 8, q16 = r + 16;
+      const int tr8 = s_tr[q8 & 15];
+      s_has[q8 & 15] = tr8 >= 0;
+      if (tr8 >= 0) {
+        cp_async4(&s_rz[q8 & 15], res_z + (long long)tr8 * d.nt);
+        cp_async4(&s_rx[q8 & 15], res_x + (long long)tr8 * d.nt);
+      }
+      if (q16 < d.nxp)
+        cp_async4((float *)&s_tr[q16 & 15], (const float *)(rmap + q16));
+      else
+        s_tr[q16 & 15] = -1;
+    }
     {
       float n_bvx = R(r, 0), n_bvz = R(r, 1), n_avx = R(r, 2), n_avz = R(r, 3);
       if (r >= 0 && r < d.nxp && zin) {
-        if (a.strips_on) {
+        if (strips) {
           const int bo = band_offset(d, r, z);
           if (bo >= 0) {
-            n_bvx = strip_get(a.st, d, s, a.it, 0, bo);
-            n_bvz = strip_get(a.st, d, s, a.it, 1, bo);
+            n_bvx = strip_unpack(a.st.prec, strip_elem(0, bo), n_bvx, R(r, 25));
+            n_bvz = strip_unpack(a.st.prec, strip_elem(1, bo), n_bvz, R(r, 26));
           }
         }
         if (rec_col) {
-          const int tr = rmap[r];
-          if (tr >= 0) {
-            n_avz += res_z[(long long)tr * d.nt];
-            n_avx += res_x[(long long)tr * d.nt];
+          s_ownx[r & 15] = n_avx;
+          s_ownz[r & 15] = n_avz;
+          if (s_has[r & 15]) {
+            n_avz += s_rz[r & 15];
+            n_avx += s_rx[r & 15];
           }
         }
       }
@@ -769,13 +925,14 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float xx = -dtdx * sa, zz = -dtdz * sb, xz_x = -dtdx * sf, xz_z = -dtdz * se;
         const float oxx = R(r, 7), ozz = R(r, 8);
         if (kPML && pml_cell(d, r1, z)) {
-          const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+          // ring slots 9, 12, 13, 14 of a PML cell: atxz_x, atxz_z, dampx, dampz
+          const float ddx = R(r, 13) * d.dt * 0.5f, ddz = R(r, 14) * d.dt * 0.5f;
           const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
           const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
           atxx = fmaf(d1, oxx, xx) * i2;
           atzz = fmaf(d3, ozz, zz) * i4;
-          const float q1 = fmaf(d1, a.aa.txz_x[k], xz_x) * i2;
-          const float q2 = fmaf(d3, a.aa.txz_z[k], xz_z) * i4;
+          const float q1 = fmaf(d1, R(r, 9), xz_x) * i2;
+          const float q2 = fmaf(d3, R(r, 12), xz_z) * i4;
           if (own) {
             a.ab.txz_x[k] = q1;
             a.ab.txz_z[k] = q2;
@@ -829,9 +986,9 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float bz = stencil4([&](int i) { return s_btxz[t + i - 1] - s_btxz[t - i]; });
         const float ez = stencil4([&](int i) { return s_btzz[t + i] - s_btzz[t - i + 1]; });
         float ovx = w_bvx[0], ovz = w_bvz[0];
-        if (a.strips_on && band_offset(d, r2, z) >= 0) {  // inner band: own state, not the strip
-          ovx = __ldg(a.ra.vx + k);
-          ovz = __ldg(a.ra.vz + k);
+        if (strips && band_offset(d, r2, z) >= 0) {  // inner band: own state, not the strip
+          ovx = R(r, 23);
+          ovz = R(r, 24);
         }
         const float vx = ovx + (-cbx * ax + -cbz * bz);
         const float vz = ovz + (-cbx * fx + -cbz * ez);
@@ -849,21 +1006,22 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float uz_x = -cbx * s_xz, uz_z = -cbz * s_z;
         float vx, vz;
         if (kPML && pml_cell(d, r2, z)) {
-          const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
+          // ring slots 17-22 of a PML cell: dampx, dampz, avx_x, avx_z, avz_x, avz_z
+          const float ddx = R(r, 17) * d.dt * 0.5f, ddz = R(r, 18) * d.dt * 0.5f;
           const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
           const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);  // no divide slow path
-          const float vxx = fmaf(d1, a.aa.vx_x[k], ux_x) * i2;
-          const float vxz = fmaf(d3, a.aa.vx_z[k], ux_z) * i4;
-          const float vzx = fmaf(d1, a.aa.vz_x[k], uz_x) * i2;
-          const float vzz = fmaf(d3, a.aa.vz_z[k], uz_z) * i4;
+          const float vxx = fmaf(d1, R(r, 19), ux_x) * i2;
+          const float vxz = fmaf(d3, R(r, 20), ux_z) * i4;
+          const float vzx = fmaf(d1, R(r, 21), uz_x) * i2;
+          const float vzz = fmaf(d3, R(r, 22), uz_z) * i4;
           a.ab.vx_x[k] = vxx; a.ab.vx_z[k] = vxz; a.ab.vz_x[k] = vzx; a.ab.vz_z[k] = vzz;
           vx = vxx + vxz;
           vz = vzx + vzz;
         } else {
           float ovx = w_avx[0], ovz = w_avz[0];
-          if (rec_col && rmap[r2] >= 0) {  // injected cell: state without the residual
-            ovx = __ldg(a.aa.vx + k);
-            ovz = __ldg(a.aa.vz + k);
+          if (rec_col) {  // receiver column: the state without the residual
+            ovx = s_ownx[r2 & 15];
+            ovz = s_ownz[r2 & 15];
           }
           vx = ovx + (ux_x + ux_z);
           vz = ovz + (uz_x + uz_z);

@@ -119,11 +119,14 @@ __global__ void __launch_bounds__(kBX *kBY) k_vel(VelArgs a) {
   float vx, vz;
   if (pml_cell(d, ix, iz)) {
     const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-    const float d1 = 1.0f - ddx, d2 = 1.0f + ddx, d3 = 1.0f - ddz, d4 = 1.0f + ddz;
-    const float vxx = __fdiv_rn(fmaf(d1, a.w.vx_x[k], ux_x), d2);
-    const float vxz = __fdiv_rn(fmaf(d3, a.w.vx_z[k], ux_z), d4);
-    const float vzx = __fdiv_rn(fmaf(d1, a.w.vz_x[k], uz_x), d2);
-    const float vzz = __fdiv_rn(fmaf(d3, a.w.vz_z[k], uz_z), d4);
+    const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
+    // (d1 v + u) / (1 + dt d / 2) as a multiply by the rounded reciprocal: a division takes its
+    // slow path for the tiny amplitudes ahead of a wavefront
+    const float i2 = __frcp_rn(1.0f + ddx), i4 = __frcp_rn(1.0f + ddz);
+    const float vxx = fmaf(d1, a.w.vx_x[k], ux_x) * i2;
+    const float vxz = fmaf(d3, a.w.vx_z[k], ux_z) * i4;
+    const float vzx = fmaf(d1, a.w.vz_x[k], uz_x) * i2;
+    const float vzz = fmaf(d3, a.w.vz_z[k], uz_z) * i4;
     a.w.vx_x[k] = vxx;
     a.w.vx_z[k] = vxz;
     a.w.vz_x[k] = vzx;
@@ -214,10 +217,10 @@ __global__ void __launch_bounds__(kBX *kBY) k_str(StrArgs a) {
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
   const float dir = (MODE == kFwd) ? 1.0f : -1.0f;
   const bool pml = pml_cell(d, ix, iz);
-  float d1 = 1.f, d2 = 1.f, d3 = 1.f, d4 = 1.f;
+  float d1 = 1.f, i2 = 1.f, d3 = 1.f, i4 = 1.f;  // damping factors; i2, i4 = 1 / (1 + dt d / 2)
   if (pml) {
     const float ddx = a.p.dampx[k] * d.dt * 0.5f, ddz = a.p.dampz[k] * d.dt * 0.5f;
-    d1 = 1.0f - ddx; d2 = 1.0f + ddx; d3 = 1.0f - ddz; d4 = 1.0f + ddz;
+    d1 = 1.0f - ddx; i2 = __frcp_rn(1.0f + ddx); d3 = 1.0f - ddz; i4 = __frcp_rn(1.0f + ddz);
   }
   if (MODE != kAdj) {
     const float lam = a.p.lam[k], mu = a.p.mu[k];
@@ -229,12 +232,12 @@ __global__ void __launch_bounds__(kBX *kBY) k_str(StrArgs a) {
     const float xz_x = MODE == kRev ? dir * mu * dtdx * sf : dir * dtdx * mu * sf;
     const float xz_z = MODE == kRev ? dir * mu * dtdz * se : dir * dtdz * mu * se;
     if (pml) {
-      const float a1 = __fdiv_rn(fmaf(d1, a.w.txx_x[k], xx_x), d2);
-      const float a2 = __fdiv_rn(fmaf(d3, a.w.txx_z[k], xx_z), d4);
-      const float b1 = __fdiv_rn(fmaf(d1, a.w.tzz_x[k], zz_x), d2);
-      const float b2 = __fdiv_rn(fmaf(d3, a.w.tzz_z[k], zz_z), d4);
-      const float c1 = __fdiv_rn(fmaf(d1, a.w.txz_x[k], xz_x), d2);
-      const float c2 = __fdiv_rn(fmaf(d3, a.w.txz_z[k], xz_z), d4);
+      const float a1 = fmaf(d1, a.w.txx_x[k], xx_x) * i2;
+      const float a2 = fmaf(d3, a.w.txx_z[k], xx_z) * i4;
+      const float b1 = fmaf(d1, a.w.tzz_x[k], zz_x) * i2;
+      const float b2 = fmaf(d3, a.w.tzz_z[k], zz_z) * i4;
+      const float c1 = fmaf(d1, a.w.txz_x[k], xz_x) * i2;
+      const float c2 = fmaf(d3, a.w.txz_z[k], xz_z) * i4;
       a.w.txx_x[k] = a1; a.w.txx_z[k] = a2;
       a.w.tzz_x[k] = b1; a.w.tzz_z[k] = b2;
       a.w.txz_x[k] = c1; a.w.txz_z[k] = c2;
@@ -247,20 +250,21 @@ __global__ void __launch_bounds__(kBX *kBY) k_str(StrArgs a) {
       a.w.txz[k] = a.w.txz[k] + (xz_x + xz_z);
     }
     if (MODE == kRev && a.e.gx_vx) {
-      a.e.gx_vx[k] = sa / d.dx;
-      a.e.gz_vz[k] = sb / d.dz;
-      a.e.gz_vx[k] = se / d.dz;
-      a.e.gx_vz[k] = sf / d.dx;
+      const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;  // reciprocal multiplies, as above
+      a.e.gx_vx[k] = sa * rdx;
+      a.e.gz_vz[k] = sb * rdz;
+      a.e.gz_vx[k] = se * rdz;
+      a.e.gx_vz[k] = sf * rdx;
     }
   } else {
     // FD2DGPU.cu:725-761, 860-895: no moduli; txx is txx_x, tzz is tzz_z.
     const float xx = dir * dtdx * sa, zz = dir * dtdz * sb;
     const float xz_x = dir * dtdx * sf, xz_z = dir * dtdz * se;
     if (pml) {
-      a.w.txx[k] = __fdiv_rn(fmaf(d1, a.w.txx[k], xx), d2);
-      a.w.tzz[k] = __fdiv_rn(fmaf(d3, a.w.tzz[k], zz), d4);
-      const float c1 = __fdiv_rn(fmaf(d1, a.w.txz_x[k], xz_x), d2);
-      const float c2 = __fdiv_rn(fmaf(d3, a.w.txz_z[k], xz_z), d4);
+      a.w.txx[k] = fmaf(d1, a.w.txx[k], xx) * i2;
+      a.w.tzz[k] = fmaf(d3, a.w.tzz[k], zz) * i4;
+      const float c1 = fmaf(d1, a.w.txz_x[k], xz_x) * i2;
+      const float c2 = fmaf(d3, a.w.txz_z[k], xz_z) * i4;
       a.w.txz_x[k] = c1; a.w.txz_z[k] = c2;
       a.w.txz[k] = c1 + c2;
     } else {
@@ -299,9 +303,10 @@ __global__ void __launch_bounds__(kBX *kBY) k_born(BornArgs a) {
   const float l2m = lam + 2.0f * mu;
   const float P = 2.0f * l2m * (-dmp);
   const float Q = 2.0f * (l2m * (-dmp) - 2.0f * mu * (-dms));
-  a.ov_txx[k] = P * vx_x / d.dx + Q * vz_z / d.dz;
-  a.ov_tzz[k] = Q * vx_x / d.dx + P * vz_z / d.dz;
-  a.ov_txz[k] = 2.0f * mu * (-dms) * (vz_x / d.dx + vx_z / d.dz);
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;  // reciprocal multiplies (no divide slow path)
+  a.ov_txx[k] = P * vx_x * rdx + Q * vz_z * rdz;
+  a.ov_tzz[k] = Q * vx_x * rdx + P * vz_z * rdz;
+  a.ov_txz[k] = 2.0f * mu * (-dms) * (vz_x * rdx + vx_z * rdz);
 }
 
 // born.cu:408-527 add_born_source_adjoint into read overlays of the scattered adjoint
@@ -355,8 +360,9 @@ __global__ void __launch_bounds__(kBX *kBY) k_born_adj(BornAdjArgs a) {
     return S(p) * __ldg(txz + p) - S(q) * __ldg(txz + q);
   });
   const float bb = -a.p.b[k];  // direction -1 (FD2DGPU.cu:1886)
-  a.ov_vx[k] = bb * (txx_x / d.dx + tzz_x / d.dx + txz_z / d.dz);
-  a.ov_vz[k] = bb * (tzz_z / d.dz + txx_z / d.dz + txz_x / d.dx);
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;  // reciprocal multiplies (no divide slow path)
+  a.ov_vx[k] = bb * (txx_x * rdx + tzz_x * rdx + txz_z * rdz);
+  a.ov_vz[k] = bb * (tzz_z * rdz + txx_z * rdz + txz_x * rdx);
 }
 
 // Saves the strip cells of (vx, vz) after forward step `it` (FD2DGPU.cu:4419-4444).  One warp

@@ -158,11 +158,11 @@ def test_fused_step_matches_half_steps(cuda_device, boundary, xr, ring):
             rz, rx = e.forward(shots)
             e.rtm(shots, rz, rx)
             out[fused] = (rz, rx, e.read_images())
-    # The ring kernels multiply by 1 / (1 + dt d / 2) in PML cells where the half steps divide,
-    # take each pair of adjoint-velocity derivatives of one stencil as a single derivative of the
-    # summed operand (linearity) and form strains with reciprocal multiplies: they agree with the
-    # half-step path at the FP32 parity gate (1e-5), not bit for bit.  Without the ring the fused
-    # kernels keep the half steps' operation order.
+    # Every path multiplies by 1 / (1 + dt d / 2) in PML cells and by 1 / dx, 1 / dz for strains.
+    # The ring kernels also take each pair of adjoint-velocity derivatives of one stencil as a
+    # single derivative of the summed operand (linearity): they agree with the half-step path at
+    # the FP32 parity gate (1e-5), not bit for bit.  Without the ring the fused kernels keep the
+    # half steps' operation order.
     tol = 1e-6 if ring == 0 else GATE
     assert rel(out[1][0], out[0][0]) < tol and rel(out[1][1], out[0][1]) < tol
     for key in ("pp_grad", "ps_grad", "illumination"):
