@@ -13,7 +13,8 @@ Metric: Gcell-updates/s = shots * 1281 * 481 * 4000 * 3 / time, whole job (all r
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU (torchrun): every rank runs its own 60-shot batch (weak scaling) and the three images
-are summed over ranks with one NCCL all-reduce per step (SURVEY-style gradient reduction).
+are summed over ranks with one NCCL all-reduce per step, as the reference sums its gradients
+over MPI ranks.
 """
 import argparse
 import json

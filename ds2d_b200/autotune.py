@@ -1,8 +1,8 @@
 """Autotuner of the fused elastic kernels' launch shape (no counterpart in the reference, whose
 launches are fixed 32x32 blocks).
 
-The knobs are the rows marched per CTA (`xr`), the depth of the cp.async prefetch ring (`ring`)
-and the register / occupancy target (`occ`).  Their best values depend on the grid, the number of
+The knobs are the rows marched per CTA (`xr`), the depth of the cp.async prefetch ring (`ring`),
+the register / occupancy target (`occ`) and the threads per CTA (`cta`, 128 or 192).  Their best values depend on the grid, the number of
 resident shots and the boundary, so the tuner times each candidate on a probe context with the
 caller's grid and batch but only `probe_nt` time steps (an RTM of the same shots: one forward and
 one backward fused launch per step), and returns the fastest setting; `apply` copies it onto the
@@ -12,9 +12,10 @@ import numpy as np
 from .api import Elastic2D
 
 DEFAULT_SPACE = [
-    {"ring": 4, "xr": 128, "occ": 0}, {"ring": 4, "xr": 64, "occ": 0},
-    {"ring": 4, "xr": 256, "occ": 0}, {"ring": 2, "xr": 128, "occ": 0},
-    {"ring": 8, "xr": 128, "occ": 0}, {"ring": 4, "xr": 128, "occ": 1},
+    {"ring": 4, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 0, "cta": 192},
+    {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 128},
+    {"ring": 4, "xr": 256, "occ": 0, "cta": 192}, {"ring": 2, "xr": 128, "occ": 0, "cta": 128},
+    {"ring": 8, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 1, "cta": 128},
 ]
 
 

@@ -39,7 +39,14 @@ FwdFn fwd_pick(bool rbc) { return rbc ? k_fwd_ring<false, kD, kF> : k_fwd_ring<t
 template <int kD, int kF, int kB>
 BwdFn bwd_pick(bool rbc) { return rbc ? k_bwd_ring<false, kD, kB> : k_bwd_ring<true, kD, kB>; }
 
-FwdFn fwd_ring_fn(bool rbc, int depth, int occ = 0) {
+// Wider CTAs (option "cta"): 192 threads = 176 output columns per z-strip, instantiated for the
+// default ring depth and occupancy target only (4 forward / 2 backward CTAs per SM, the same
+// warps per SM as 128-thread CTAs at 6 / 3).
+constexpr int kWideCta = 192;
+
+FwdFn fwd_ring_fn(bool rbc, int depth, int occ = 0, int cta = kFB) {
+  if (cta == kWideCta && depth == 4 && occ == 0)
+    return rbc ? k_fwd_ring<false, 4, 4, kWideCta> : k_fwd_ring<true, 4, 4, kWideCta>;
   switch (depth * 2 + (occ ? 1 : 0)) {
     case 4: return fwd_pick<2, 6, 3>(rbc);
     case 5: return fwd_pick<2, 8, 4>(rbc);
@@ -50,7 +57,9 @@ FwdFn fwd_ring_fn(bool rbc, int depth, int occ = 0) {
   }
 }
 
-BwdFn bwd_ring_fn(bool rbc, int depth, int occ = 0) {
+BwdFn bwd_ring_fn(bool rbc, int depth, int occ = 0, int cta = kFB) {
+  if (cta == kWideCta && depth == 4 && occ == 0)
+    return rbc ? k_bwd_ring<false, 4, 2, kWideCta> : k_bwd_ring<true, 4, 2, kWideCta>;
   switch (depth * 2 + (occ ? 1 : 0)) {
     case 4: return bwd_pick<2, 6, 3>(rbc);
     case 5: return bwd_pick<2, 8, 4>(rbc);
@@ -223,6 +232,7 @@ struct ds2d_ctx {
   int opt_adjoint_born = 0;  // scattered adjoint of ELSRTM (off = the reference's observed runs)
   int opt_ring = kDefaultRing;  // cp.async ring depth of the fused kernels (0 = no ring)
   int opt_occ = 0;           // occupancy target of the ring kernels (see fwd_ring_fn)
+  int opt_cta = 0;           // threads per CTA of the ring kernels: 0 auto, 128 or 192
   bool ring_ok = true;       // batch arrays fit the ring kernels' 32-bit offsets
   int opt_pcg_switch = 970;  // ds2d_lsrtm_pcg: per-mille residual ratio that ends the network phase
   int opt_pcg_m = 8;         // ds2d_lsrtm_pcg: directions kept for explicit conjugation
@@ -532,14 +542,36 @@ int strip_save(ds2d_ctx *c, const Wave &w, Strips &st, int it, int n) {
   return DS2D_OK;
 }
 
+// Threads per CTA of the fused elastic launches.  A CTA computes (threads - 16) columns of a
+// z-strip; the strips split nzp evenly, so the share of working threads depends on nzp (481:
+// 97 of 128 or 161 of 192; 441: 111 of 128 or 147 of 192).  Automatic choice: the wider CTA
+// when its share of working threads is at least 5 % higher.  Only the ring kernels at the default
+// depth and occupancy have the wide variant.
+int fused_cta(const ds2d_ctx *c) {
+  if (!(c->opt_ring && c->ring_ok) || c->opt_ring != 4 || c->opt_occ != 0) return kFB;
+  if (c->opt_cta) return c->opt_cta;
+  auto share = [&](int cta) {
+    const int ns = (c->d.nzp + cta - 17) / (cta - 16);
+    return (double)((c->d.nzp + ns - 1) / ns) / cta;
+  };
+  return share(kWideCta) > 1.05 * share(kFB) ? kWideCta : kFB;
+}
+
+// z-strip split of the fused launches for CTAs of `cta` threads: (strips, columns per strip).
+void strip_split(const Dims &d, int cta, int *nstrips, int *tz) {
+  *nstrips = (d.nzp + cta - 17) / (cta - 16);
+  *tz = (d.nzp + *nstrips - 1) / *nstrips;
+}
+
 // Fused forward pass: one k_fwd_fused launch per step, ping-ponging fw <-> fw2.
 int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
   const Dims &d = c->d;
   int rc;
   if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
   if ((rc = zero_wave(c, c->fw2, n))) return rc;
-  const int nstrips = (d.nzp + kFTZ - 1) / kFTZ;
-  const int tz = (d.nzp + nstrips - 1) / nstrips;
+  const int cta = fused_cta(c);
+  int nstrips, tz;
+  strip_split(d, cta, &nstrips, &tz);
   const int xr = std::max(8, c->opt_xr);
   dim3 grid(nstrips, (d.nxp + xr - 1) / xr, n);
   Wave *cur = &c->fw, *nxt = &c->fw2;
@@ -549,9 +581,9 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
     a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
     if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
     if (c->opt_ring && c->ring_ok) {
-      const size_t sm = sizeof(float) * c->opt_ring * fwd_ring_fields(!d.rbc) * kFB;
-      FwdFn kfn = fwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ);
-      LAUNCHS("fwd_fused", kBytesFused * CELLS(n), kfn, grid, kFB, sm, a);
+      const size_t sm = sizeof(float) * c->opt_ring * fwd_ring_fields(!d.rbc) * cta;
+      FwdFn kfn = fwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ, cta);
+      LAUNCHS("fwd_fused", kBytesFused * CELLS(n), kfn, grid, cta, sm, a);
     } else if (d.rbc) {
       LAUNCHP("fwd_fused", kBytesFused * CELLS(n), k_fwd_fused<false>, grid, kFB, a);
     } else {
@@ -680,7 +712,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ, c->opt_xr, (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr, (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -706,8 +738,9 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
     if ((rc = zero_wave(c, c->abk2, n))) return rc;
     Wave *acur = &c->abk, *anxt = &c->abk2;
-    const int nstrips = (d.nzp + kFTZ - 1) / kFTZ;
-    const int tz = (d.nzp + nstrips - 1) / nstrips;
+    const int cta = fused_cta(c);
+    int nstrips, tz;
+    strip_split(d, cta, &nstrips, &tz);
     const int xr = std::max(8, c->opt_xr);
     dim3 fgrid(nstrips, (d.nxp + xr - 1) / xr, n);
     for (int it = d.nt - 1; it >= 0; --it) {
@@ -717,9 +750,9 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
       a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
       a.img = c->img_slot; a.img_plane = (long long)plane;
       if (c->opt_ring && c->ring_ok) {
-        const size_t sm = sizeof(float) * c->opt_ring * bwd_ring_fields(!d.rbc) * kFB;
-        BwdFn kfn = bwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ);
-        LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, fgrid, kFB, sm, a);
+        const size_t sm = sizeof(float) * c->opt_ring * bwd_ring_fields(!d.rbc) * cta;
+        BwdFn kfn = bwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ, cta);
+        LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, fgrid, cta, sm, a);
       } else if (d.rbc) {
         LAUNCHP("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_fused<false>, fgrid, kFB, a);
       } else {
@@ -1156,6 +1189,17 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
           if (e == cudaSuccess)
             e = cudaFuncSetAttribute(bwd_ring_fn(rbc, depth, occ),
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_sm);
+          if (depth == 4 && occ == 0) {
+            // shared memory scales with the CTA width
+            if (e == cudaSuccess)
+              e = cudaFuncSetAttribute(fwd_ring_fn(rbc, depth, occ, kWideCta),
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       fwd_sm / kFB * kWideCta);
+            if (e == cudaSuccess)
+              e = cudaFuncSetAttribute(bwd_ring_fn(rbc, depth, occ, kWideCta),
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       bwd_sm / kFB * kWideCta);
+          }
         }
     }
     if (e != cudaSuccess) {
@@ -1266,7 +1310,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ, c->opt_xr, (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr, (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -1687,6 +1731,10 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
   } else if (k == "occ") {
     if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "occ must be 0 or 1");
     c->opt_occ = (int)value;
+  } else if (k == "cta") {
+    if (value != 0 && value != kFB && value != kWideCta)
+      return fail(c, DS2D_E_ARG, "cta must be 0 (automatic), 128 or 192");
+    c->opt_cta = (int)value;
   } else if (k == "xr") {
     if (value < 8 || value > 4096) return fail(c, DS2D_E_ARG, "xr must be in [8, 4096]");
     c->opt_xr = (int)value;

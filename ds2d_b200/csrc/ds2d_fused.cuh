@@ -21,6 +21,19 @@
 
 namespace ds2d {
 
+// Row steps per iteration of the ring kernels' x-march (compile-time tuning knob).  Two steps
+// per iteration let the compiler rename half of the window shifts away (60-shot RTM at
+// 1201x401 on a B200: forward 669 -> 643 us, backward 1596 -> 1572 us per launch); three or
+// four spill registers or overflow the instruction cache.
+#ifndef DS2D_RING_UNROLL_FWD
+#define DS2D_RING_UNROLL_FWD 2
+#endif
+#ifndef DS2D_RING_UNROLL_BWD
+#define DS2D_RING_UNROLL_BWD 2
+#endif
+constexpr int kRingUnrollFwd = DS2D_RING_UNROLL_FWD;
+constexpr int kRingUnrollBwd = DS2D_RING_UNROLL_BWD;
+
 constexpr int kFB = 128;        // threads per CTA
 constexpr int kFTZ = kFB - 16;  // max output columns of one strip
 
@@ -229,12 +242,12 @@ __host__ __device__ constexpr int fwd_ring_fields(bool pml) {
   return pml ? kFwdRingFieldsPml : kFwdRingFields;
 }
 
-template <bool kPML, int kD, int kMinB>
-__global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
+template <bool kPML, int kD, int kMinB, int kT = kFB>
+__global__ void __launch_bounds__(kT, kMinB) k_fwd_ring(FwdFusedArgs a) {
   static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
   constexpr int NF = fwd_ring_fields(kPML);
-  extern __shared__ float ring[];  // [kD][NF][kFB]
-  __shared__ float s_txz[kFB], s_tzz[kFB], s_vx[kFB], s_vz[kFB];
+  extern __shared__ float ring[];  // [kD][NF][kT]
+  __shared__ float s_txz[kT], s_tzz[kT], s_vx[kT], s_vz[kT];
   __shared__ int s_tr[16];  // receiver column: trace index of velocity row mod 16, 8 rows ahead
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
@@ -254,7 +267,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
   // R(q, f): field f of ring slot q (row q for f < 3, row q-4 for f < 6, row q-8 otherwise)
-  auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kFB + t]; };
+  auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kT + t]; };
   auto issue = [&](int q) {
     const int r0 = q, r4 = q - 4, r8 = q - 8;
     const bool in0 = r0 >= 0 && r0 < d.nxp && zin;
@@ -308,6 +321,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_fwd_ring(FwdFusedArgs a) {
 
 #pragma unroll
   for (int j = 0; j < kD - 1; j++) issue(x0 - 8 + j);
+#pragma unroll kRingUnrollFwd
   for (int r = x0 - 8; r < x1 + 8; r++) {
     cp_async_wait<kD - 2>();  // row r has landed (this thread's copies)
     if (rec_col) {  // trace index of velocity row r + 4 (read 8 steps on, landed by then)
@@ -702,13 +716,13 @@ __device__ __forceinline__ float strip_unpack(int prec, long long e, float word,
   return __bfloat162float(__ushort_as_bfloat16(h)) * sc;
 }
 
-template <bool kPML, int kD, int kMinB>
-__global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
+template <bool kPML, int kD, int kMinB, int kT = kFB>
+__global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
   static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
   constexpr int NF = bwd_ring_fields(kPML);
-  extern __shared__ float ring[];  // [kD][NF][kFB]
-  __shared__ float s_bvx[kFB], s_bvz[kFB], s_avx[kFB], s_avz[kFB];
-  __shared__ float s_btxz[kFB], s_btzz[kFB], s_m[kFB], s_pzlx[kFB];
+  extern __shared__ float ring[];  // [kD][NF][kT]
+  __shared__ float s_bvx[kT], s_bvz[kT], s_avx[kT], s_avz[kT];
+  __shared__ float s_btxz[kT], s_btzz[kT], s_m[kT], s_pzlx[kT];
   // Receiver column (one thread of the CTA, if any): per row mod 16, the trace index (fetched 16
   // rows ahead), whether a trace sits there and its residual at this step (fetched 8 rows ahead)
   // and the cell's state without the residual (kept 8 rows for stage 2).
@@ -740,7 +754,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
   const float *grid_src[15] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.txx,
                                a.ra.tzz, a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz,
                                a.p.lam,  a.p.mu,   a.p.kpp,  a.p.kps,  a.p.b};
-  auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kFB + t]; };
+  auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kT + t]; };
   auto strip_elem = [&](int comp, int bo) { return (strip_row0 + comp) * d.lb_max + bo; };
   auto issue = [&](int q) {
     const int r0 = q, r4 = q - 4, r8 = q - 8;
@@ -836,6 +850,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_ring(BwdFusedArgs a) {
       }
     }
   }
+#pragma unroll kRingUnrollBwd
   for (int r = x0 - 8; r < x1 + 8; r++) {
     cp_async_wait<kD - 2>();  // slot r has landed (this thread's copies)
     if (rec_col) {

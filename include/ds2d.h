@@ -121,7 +121,7 @@ double ds2d_last_cell_updates(const ds2d_ctx *ctx);
 /* Number of kernel launches issued by the last forward / elsrtm / rtm call. */
 long long ds2d_last_launches(const ds2d_ctx *ctx);
 
-/* Acoustic Born operator pair and CG-LSRTM (north-star extension; the reference ships unused
+/* Acoustic Born operator pair and CG-LSRTM (an extension of the path; the reference ships unused
  * CG helpers, main.cpp:1224-1320 sjcgsolver / FD2DGPU.cu:4885 ELSRTM_CALCULATE_ALPHA, and runs
  * NCC + Adam instead).  The acoustic scheme is the elastic one with mu = 0 (pass vs = 0 to
  * ds2d_set_models); the context must use DS2D_BOUNDARY_RANDOM (undamped grid, exact time
@@ -184,7 +184,9 @@ int ds2d_dot_f64_noalloc(const float *a, const float *b, long long n, void *stre
  * FD2DGPU.cuh:8-9): "fused" (1 = single-pass fused time step, 0 = one launch per half step),
  * "xr" (rows marched by one CTA of the fused kernels), "ring" (cp.async prefetch ring depth of
  * the fused kernels: 0 off, 1 default, or 2 / 4 / 8), "occ" (0 / 1: register budget for 6 / 8
- * forward and 3 / 4 backward CTAs per SM), "graph" (0 / 1: capture batches in CUDA graphs),
+ * forward and 3 / 4 backward CTAs per SM), "cta" (threads per CTA of the ring kernels: 128,
+ * 192, or 0 = the one whose z-strips leave fewer threads idle for this grid; 192 needs ring 4 and
+ * occ 0), "graph" (0 / 1: capture batches in CUDA graphs),
  * "adjoint_born" (see ds2d_elsrtm), "pcg_switch" and "pcg_m" (1..15, see ds2d_lsrtm_pcg). */
 int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
 

@@ -21,7 +21,7 @@ struct RefGeom {
 };
 
 // Receiver sampling of the background field (the reference records only scattered fields;
-// forward modelling for observed data reads the public vx / vz, as the survey describes).
+// forward modelling for observed data reads the public vx / vz after every step).
 __global__ void harness_record(const float *vz, const float *vx, float *rz, float *rx,
                                const int *igx, int igz, int nzpml, int ntr, int nt, int it) {
   int tr = blockIdx.x * blockDim.x + threadIdx.x;

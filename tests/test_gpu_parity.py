@@ -188,6 +188,30 @@ def test_ring_occupancy_variants_agree(cuda_device, boundary):
         assert rel(out[1][2][key], out[0][2][key]) < 1e-6, key
 
 
+@pytest.mark.parametrize("boundary", ["pml", "random"])
+def test_ring_cta_widths_agree(cuda_device, boundary):
+    """192-thread ring CTAs (2 z-strips of 160 columns) against 128-thread ones (3 strips of
+    107) on a 320-cell-deep grid: every cell does the same arithmetic, so the results are equal
+    bit for bit."""
+    c, _, _, w, _ = small_case(nt=200)
+    c["allnz"] = 300
+    vp, vs = synth.layered(c["allnx"], c["allnz"], seed=4)
+    shots = synth.surface_shots(c["allnx"], c["nx"], c["pml"], 3)
+    out = {}
+    for cta in (128, 192):
+        with _ctx(c, shots, boundary=boundary, seed=5) as e:
+            e.set_option("cta", cta)
+            e.set_models(vp, vs)
+            e.set_wavelet(w)
+            rz, rx = e.forward(shots)
+            e.rtm(shots, rz, rx)
+            out[cta] = (rz, rx, e.read_images())
+    assert np.abs(out[128][0]).max() > 0
+    assert np.array_equal(out[192][0], out[128][0]) and np.array_equal(out[192][1], out[128][1])
+    for key in ("pp_grad", "ps_grad", "illumination"):
+        assert np.array_equal(out[192][2][key], out[128][2][key]), key
+
+
 @pytest.mark.parametrize("fused", [0, 1])
 def test_uneven_windows_vs_oracle(cuda_device, fused):
     """Shots of different aperture widths in one batch (per-slot window sizes)."""
