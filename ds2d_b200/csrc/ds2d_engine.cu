@@ -57,6 +57,20 @@ FwdFn fwd_ring_fn(bool rbc, int depth, int occ = 0, int cta = kFB) {
   }
 }
 
+// Born-modelling modes of the forward ring kernel (1 background + Born source, 2 first-order
+// scattered set, 3 second-order set), default ring depth and CTA width; their larger rings allow
+// 3-4 CTAs per SM, so the register budget is set for 4.
+FwdFn fwd_mode_fn(bool rbc, int mode) {
+  switch (mode) {
+    case 1: return rbc ? k_fwd_ring<false, 4, 4, kFB, 1> : k_fwd_ring<true, 4, 4, kFB, 1>;
+    case 2: return rbc ? k_fwd_ring<false, 4, 4, kFB, 2> : k_fwd_ring<true, 4, 4, kFB, 2>;
+    default: return rbc ? k_fwd_ring<false, 4, 4, kFB, 3> : k_fwd_ring<true, 4, 4, kFB, 3>;
+  }
+}
+
+using ScatFn = void (*)(BwdScatArgs);
+ScatFn bwd_scat_fn(bool rbc) { return rbc ? k_bwd_scat_ring<false, 4, 4> : k_bwd_scat_ring<true, 4, 4>; }
+
 BwdFn bwd_ring_fn(bool rbc, int depth, int occ = 0, int cta = kFB) {
   if (cta == kWideCta && depth == 4 && occ == 0)
     return rbc ? k_bwd_ring<false, 4, 2, kWideCta> : k_bwd_ring<true, 4, 2, kWideCta>;
@@ -247,6 +261,8 @@ struct ds2d_ctx {
   };
   Vec vecs[64];  // 0-11 solver vectors, 16+ the flexible-CG direction window
   Wave fw2{}, abk2{};  // ping-pong partners of fw / abk for the fused kernels
+  Wave b1_2{}, b2_2{};  // ping-pong partners of the scattered sets (fused ELSRTM forward)
+  float *ov_s2[3] = {nullptr, nullptr, nullptr};  // Born source of b1 for b2 (fused forward)
   Wave *fw_cur = nullptr;  // buffer holding the latest forward state
   double batch_cells = 0, batch_wcells = 0;  // padded / interior cells of the current batch
   // CUDA graphs of whole batches (time loops included), keyed by everything baked into them.
@@ -513,6 +529,12 @@ constexpr double kBytesVelAdj = 40;  // S (12) + lam, mu (8) + b (4) + V (8) rea
 constexpr double kBytesStrAdj = 32;  // V (8) + S (12) read, S (12) written
 constexpr double kBytesImage = 68;   // strains 16 + S 12 + weights 8 + V 8 read, 3 images r/w 24
 constexpr double kBytesFused = 52;   // one fused elastic step: 5 fields r/w + b, lam, mu read
+// Fused Born-modelling steps (ring modes 1-3): the elastic step plus the overlay read (12), the
+// Born source written (12) and dmp, dms read (8) where the mode has them.
+constexpr double kBytesBornMode[4] = {52, 72, 84, 64};
+// Reverse step of the first-order scattered set (k_bwd_scat_ring): its 5 fields read and written,
+// b, lam, mu, kpp, kps, the adjoint stresses and the Born source read, images 3 and 4 updated.
+constexpr double kBytesBwdScat = 100;
 // Fused backward RTM step per padded cell: source and adjoint fields r/w (2 x 40), b, lam, mu
 // (12), imaging weights (8) and three image accumulators r/w (24).
 constexpr double kBytesBwdFused = 124;
@@ -792,6 +814,116 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
   return reduce_images(c, n, 3);
 }
 
+// ELSRTM forward pass on the ring kernels (FD2DGPU.cu:4396-4478): per step one launch per
+// wavefield set -- the background writing its Born source, the first-order set reading it as an
+// overlay, recording and writing its own Born source, the second-order set reading that and
+// recording -- each set ping-ponging between two buffers, then the strips of the background and
+// the first-order set.  The final states are copied back into fw, b1, b2 where the half-step
+// pass leaves them.
+int elsrtm_forward_fused(ds2d_ctx *c, int n, bool strips) {
+  const Dims &d = c->d;
+  int rc;
+  if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
+  if (!c->b1_2.vx && (rc = alloc_wave(c, c->b1_2, false))) return rc;
+  if (!c->b2_2.vx && (rc = alloc_wave(c, c->b2_2, false))) return rc;
+  for (int i = 0; i < 3; i++)
+    if (!c->ov_s2[i] && (rc = alloc_slots(c, &c->ov_s2[i]))) return rc;
+  for (const Wave *w : {&c->fw2, &c->b1_2, &c->b2_2})
+    if ((rc = zero_wave(c, *w, n))) return rc;
+  const size_t bytes = sizeof(float) * (size_t)d.slot * n;
+  for (int i = 0; i < 3; i++) CK(cudaMemsetAsync(c->ov_s2[i], 0, bytes, c->stream));
+  int nstrips, tz;
+  strip_split(d, kFB, &nstrips, &tz);
+  const int xr = std::max(8, c->opt_xr);
+  dim3 grid(nstrips, (d.nxp + xr - 1) / xr, n);
+  Wave *set[3][2] = {{&c->fw, &c->fw2}, {&c->b1, &c->b1_2}, {&c->b2, &c->b2_2}};
+  float *const *ov[2] = {c->ov_s, c->ov_s2};  // Born source of the background / of b1
+  int cur = 0;
+  for (int it = 0; it < d.nt; it++, cur ^= 1) {
+    for (int m = 0; m < 3; m++) {
+      FwdFusedArgs a{};
+      a.d = d; a.a = *set[m][cur]; a.b = *set[m][cur ^ 1]; a.p = c->par; a.shots = c->d_shots;
+      a.wavelet = c->wavelet; a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
+      if (m > 0) {
+        a.rec_on = 1; a.rec_vz = c->rec[2 * m]; a.rec_vx = c->rec[2 * m + 1];
+        a.ovi_txx = ov[m - 1][0]; a.ovi_tzz = ov[m - 1][1]; a.ovi_txz = ov[m - 1][2];
+      }
+      if (m < 2) { a.ovo_txx = ov[m][0]; a.ovo_tzz = ov[m][1]; a.ovo_txz = ov[m][2]; }
+      const int mode = m + 1;
+      const size_t sm = sizeof(float) * 4 * fwd_ring_fields(!d.rbc, mode) * kFB;
+      FwdFn kfn = fwd_mode_fn(d.rbc != 0, mode);
+      LAUNCHS("fwd_born", kBytesBornMode[mode] * CELLS(n), kfn, grid, kFB, sm, a);
+    }
+    if (strips) {
+      strip_save(c, *set[0][cur ^ 1], c->st_a, it, n);
+      strip_save(c, *set[1][cur ^ 1], c->st_b, it, n);
+    }
+  }
+  if (cur == 1)
+    for (int m = 0; m < 3; m++) {
+      const Wave &src = *set[m][1], &dst = *set[m][0];
+      const float *from[5] = {src.vx, src.vz, src.txx, src.tzz, src.txz};
+      float *to[5] = {dst.vx, dst.vz, dst.txx, dst.tzz, dst.txz};
+      for (int i = 0; i < 5; i++)
+        CK(cudaMemcpyAsync(to[i], from[i], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    }
+  CK(cudaGetLastError());
+  return DS2D_OK;
+}
+
+// ELSRTM backward pass on the ring kernels (FD2DGPU.cu:4685-4807): per step k_bwd_ring
+// (background reconstruction, adjoint with the NCC source, images 0-2), k_born of the
+// background's reconstructed velocities, then k_bwd_scat_ring (first-order set reconstruction
+// with that Born source, images 3-4).  Each set ping-pongs between two buffers that both start
+// from its final forward state, so the cells the interior reconstruction never updates stay
+// frozen in both.
+int elsrtm_backward_fused(ds2d_ctx *c, int n, bool strips) {
+  const Dims &d = c->d;
+  int rc;
+  if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
+  if ((rc = zero_wave(c, c->abk2, n))) return rc;
+  const size_t bytes = sizeof(float) * (size_t)d.slot * n;
+  for (int m = 0; m < 2; m++) {
+    const Wave &src = m ? c->b1 : c->fw, &dst = m ? c->b1_2 : c->fw2;
+    const float *from[5] = {src.vx, src.vz, src.txx, src.tzz, src.txz};
+    float *to[5] = {dst.vx, dst.vz, dst.txx, dst.tzz, dst.txz};
+    for (int i = 0; i < 5; i++)
+      CK(cudaMemcpyAsync(to[i], from[i], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  int nstrips, tz;
+  strip_split(d, kFB, &nstrips, &tz);
+  const int xr = std::max(8, c->opt_xr);
+  dim3 grid(nstrips, (d.nxp + xr - 1) / xr, n);
+  dim3 bgrid = cell_grid(d, n), blk(kBX, kBY);
+  const long long plane = (long long)c->B * d.wnx * d.wnz;
+  Wave *fc = &c->fw, *fn = &c->fw2, *ac = &c->abk, *an = &c->abk2, *bc = &c->b1, *bn = &c->b1_2;
+  const size_t sm = sizeof(float) * 4 * bwd_ring_fields(!d.rbc) * kFB;
+  const size_t sm2 = sizeof(float) * 4 * kBwdScatRingFields * kFB;
+  for (int it = d.nt - 1; it >= 0; --it) {
+    BwdFusedArgs a{};
+    a.d = d; a.ra = *fc; a.rb = *fn; a.aa = *ac; a.ab = *an; a.p = c->par;
+    a.shots = c->d_shots; a.rmap = c->d_rmap; a.res_vz = c->rec[6]; a.res_vx = c->rec[7];
+    a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
+    a.img = c->img_slot; a.img_plane = plane;
+    BwdFn kfn = bwd_ring_fn(d.rbc != 0, 4, 0, kFB);
+    LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, grid, kFB, sm, a);
+    BornArgs bs{d, c->d_shots, fn->vx, fn->vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
+    LAUNCH(k_born, bgrid, blk, bs);
+    BwdScatArgs b{};
+    b.d = d; b.ra = *bc; b.rb = *bn; b.atxx = an->txx; b.atzz = an->tzz; b.atxz = an->txz;
+    b.ov_txx = c->ov_s[0]; b.ov_tzz = c->ov_s[1]; b.ov_txz = c->ov_s[2]; b.p = c->par;
+    b.shots = c->d_shots; b.st = c->st_b; b.strips_on = strips; b.it = it; b.tz = tz; b.xr = xr;
+    b.img = c->img_slot; b.img_plane = plane;
+    ScatFn kfn2 = bwd_scat_fn(d.rbc != 0);
+    LAUNCHS("bwd_scat", kBytesBwdScat * CELLS(n), kfn2, grid, kFB, sm2, b);
+    std::swap(fc, fn);
+    std::swap(ac, an);
+    std::swap(bc, bn);
+  }
+  CK(cudaGetLastError());
+  return DS2D_OK;
+}
+
 int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int iter,
                  double *mis_host) {
   const Dims &d = c->d;
@@ -809,7 +941,11 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
   const bool strips = !d.rbc;
   dim3 grid = cell_grid(d, n), blk(kBX, kBY);
   // Forward pass, FD2DGPU.cu:4396-4478: background, first- and second-order scattered sets.
-  for (int it = 0; it < d.nt; it++) {
+  // The ring kernels compute the Born source from the new velocities inside their stress stage;
+  // that needs every interior cell inside the updated band (pml >= nop).
+  const bool fused_fwd = c->opt_fused && c->opt_ring == 4 && c->ring_ok && d.pml >= d.nop;
+  if (fused_fwd && (rc = elsrtm_forward_fused(c, n, strips))) return rc;
+  for (int it = 0; it < d.nt && !fused_fwd; it++) {
     VelArgs v = vel_args(c, c->fw, it);
     v.src_on = 1;
     LAUNCH(k_vel<kFwd>, grid, blk, v);
@@ -845,8 +981,10 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
   c->last_launches++;
   CK(cudaGetLastError());
   dim3 igrid((d.wnz + kBX - 1) / kBX, (d.wnx + kBY - 1) / kBY, n);
-  // Backward pass, FD2DGPU.cu:4685-4807.
-  for (int it = d.nt - 1; it >= 0; --it) {
+  // Backward pass, FD2DGPU.cu:4685-4807 (the fused path has no scattered-adjoint term).
+  const bool fused_bwd = fused_fwd && !c->opt_adjoint_born;
+  if (fused_bwd && (rc = elsrtm_backward_fused(c, n, strips))) return rc;
+  for (int it = d.nt - 1; it >= 0 && !fused_bwd; --it) {
     StrArgs sr = str_args(c, c->fw, it);
     sr.e = c->e; sr.st = c->st_a; sr.strips_on = strips;
     LAUNCH(k_str<kRev>, grid, blk, sr);
@@ -1202,6 +1340,14 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
           }
         }
     }
+    for (bool rbc : {false, true})
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(bwd_scat_fn(rbc), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(float) * 4 * kBwdScatRingFields * kFB));
+    for (bool rbc : {false, true})
+      for (int mode = 1; mode <= 3 && e == cudaSuccess; mode++)
+        e = cudaFuncSetAttribute(fwd_mode_fn(rbc, mode), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(float) * 4 * fwd_ring_fields(!rbc, mode) * kFB));
     if (e != cudaSuccess) {
       g_create_err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
       delete c;

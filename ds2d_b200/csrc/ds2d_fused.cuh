@@ -48,6 +48,11 @@ struct FwdFusedArgs {
   const int *rmap;
   float *rec_vz, *rec_vx;
   int rec_on;
+  // Born modelling sets (ring kernel modes 1-3): read overlay of the stresses (the Born source
+  // of the previous set, added to the stencil values only) and the Born source written from the
+  // new velocities for the next set.
+  const float *ovi_txx, *ovi_tzz, *ovi_txz;
+  float *ovo_txx, *ovo_tzz, *ovo_txz;
 };
 
 template <int N>
@@ -236,16 +241,35 @@ __device__ __forceinline__ void cp_async_wait() {
 // the ring too (a PML cell does not read its own vx, vz, so slots 3-4 carry vx_x, vx_z):
 // 8 vz_x, 9 vz_z, 10 dampx, 11 dampz of row q-4; 12 dampx, 13 dampz, 14 txx_x, 15 txx_z,
 // 16 tzz_x, 17 tzz_z, 18 txz_x, 19 txz_z of row q-8.
+//
+// Modes (the reference's born_modeling sequence, FD2DGPU.cu:1817-1862 with add_born_source,
+// born.cu:351-405, after each set):
+//   0  background step with the explosive source (modelling, RTM);
+//   1  background step that also writes the Born source of its new velocities (interior cells)
+//      into ovo_* for the first-order scattered set;
+//   2  scattered step without source, ovi_* added to the stress stencil values, Born source of
+//      its own new velocities written into ovo_* for the second-order set;
+//   3  scattered step with the ovi_* overlay only.
+// An overlay mode reads each cell's own stresses for the stress update from extra ring fields
+// (the windows hold stress + overlay), and a Born-source mode reads dmp, dms:
+//   NF0 + 0..2 ovi txx, tzz, txz of row q; NF0 + 3..5 txx, tzz, txz of row q-8 (overlay modes);
+//   then dmp, dms of row q-8 (Born-source modes), NF0 = fwd_ring_fields(kPML).
 constexpr int kFwdRingFields = 8;
 constexpr int kFwdRingFieldsPml = 20;
 __host__ __device__ constexpr int fwd_ring_fields(bool pml) {
   return pml ? kFwdRingFieldsPml : kFwdRingFields;
 }
+__host__ __device__ constexpr int fwd_ring_fields(bool pml, int mode) {
+  return fwd_ring_fields(pml) + (mode >= 2 ? 6 : 0) + (mode == 1 || mode == 2 ? 2 : 0);
+}
 
-template <bool kPML, int kD, int kMinB, int kT = kFB>
+template <bool kPML, int kD, int kMinB, int kT = kFB, int kMode = 0>
 __global__ void __launch_bounds__(kT, kMinB) k_fwd_ring(FwdFusedArgs a) {
   static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
-  constexpr int NF = fwd_ring_fields(kPML);
+  constexpr bool kOvIn = kMode >= 2, kBornOut = kMode == 1 || kMode == 2, kSrc = kMode < 2;
+  constexpr int NF0 = fwd_ring_fields(kPML);
+  constexpr int NF = fwd_ring_fields(kPML, kMode);
+  constexpr int FOV = NF0, FOWN = NF0 + 3, FBORN = NF0 + (kOvIn ? 6 : 0);
   extern __shared__ float ring[];  // [kD][NF][kT]
   __shared__ float s_txz[kT], s_tzz[kT], s_vx[kT], s_vz[kT];
   __shared__ int s_tr[16];  // receiver column: trace index of velocity row mod 16, 8 rows ahead
@@ -262,8 +286,9 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_ring(FwdFusedArgs a) {
   const bool scol = t >= 8 && t < a.tz + 8 && zupd;
   const ShotDev sh = a.shots[s];
   const float sval = a.wavelet[a.it];
-  const bool src_col = z == sh.isz;
+  const bool src_col = kSrc && z == sh.isz;
   const bool rec_col = a.rec_on && z == sh.igz;
+  const bool z_int = z >= d.pml && z < d.nzp - d.pml;
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
   // R(q, f): field f of ring slot q (row q for f < 3, row q-4 for f < 6, row q-8 otherwise)
@@ -312,6 +337,24 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_ring(FwdFusedArgs a) {
       cp_async4(&R(q, 18), a.a.txz_x + o8);
       cp_async4(&R(q, 19), a.a.txz_z + o8);
     }
+    if (kOvIn) {
+      if (in0) {
+        cp_async4(&R(q, FOV), a.ovi_txx + o0);
+        cp_async4(&R(q, FOV + 1), a.ovi_tzz + o0);
+        cp_async4(&R(q, FOV + 2), a.ovi_txz + o0);
+      } else {
+        R(q, FOV) = R(q, FOV + 1) = R(q, FOV + 2) = 0.f;
+      }
+      if (in8 && !pml8) {
+        cp_async4(&R(q, FOWN), a.a.txx + o8);
+        cp_async4(&R(q, FOWN + 1), a.a.tzz + o8);
+        cp_async4(&R(q, FOWN + 2), a.a.txz + o8);
+      }
+    }
+    if (kBornOut && in8 && r8 >= d.pml && r8 < d.nxp - d.pml && z_int) {
+      cp_async4(&R(q, FBORN), a.p.dmp + o8);
+      cp_async4(&R(q, FBORN + 1), a.p.dms + o8);
+    }
     cp_async_commit();
   };
 
@@ -331,8 +374,12 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_ring(FwdFusedArgs a) {
       else
         s_tr[q & 15] = -1;
     }
-    float n_txx = R(r, 0), n_tzz = R(r, 1);
-    const float n_txz = R(r, 2);
+    float n_txx = R(r, 0), n_tzz = R(r, 1), n_txz = R(r, 2);
+    if (kOvIn) {  // Born source of the previous set (read overlay, as k_vel)
+      n_txx += R(r, FOV);
+      n_tzz += R(r, FOV + 1);
+      n_txz += R(r, FOV + 2);
+    }
     if (src_col && r == sh.isx) {  // FD2DGPU.cu:2039-2049 (transient)
       n_txx += sval;
       n_tzz += sval;
@@ -422,14 +469,30 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_ring(FwdFusedArgs a) {
         a.b.tzz[k] = b1 + b2;
         a.b.txz[k] = c1 + c2;
       } else {
-        float oxx = w_txx[0], ozz = w_tzz[0];
+        float oxx = w_txx[0], ozz = w_tzz[0], oxz = w_txz[0];
+        if (kOvIn) {  // the windows carry the overlay: own state from the ring
+          oxx = R(r, FOWN);
+          ozz = R(r, FOWN + 1);
+          oxz = R(r, FOWN + 2);
+        }
         if (src_col && rs == sh.isx) {  // the injected cell: state without the source
           oxx = __ldg(a.a.txx + k);
           ozz = __ldg(a.a.tzz + k);
         }
         a.b.txx[k] = oxx + (xx_x + xx_z);
         a.b.tzz[k] = ozz + (zz_x + zz_z);
-        a.b.txz[k] = w_txz[0] + (xz_x + xz_z);
+        a.b.txz[k] = oxz + (xz_x + xz_z);
+      }
+      if (kBornOut && rs >= d.pml && rs < d.nxp - d.pml && z_int) {
+        // add_born_source of the new velocities (k_born): sa, sb, se, sf are Dx- vx, Dz- vz,
+        // Dz+ vx, Dx+ vz of this row
+        const float dmp = R(r, FBORN), dms = R(r, FBORN + 1);
+        const float P = 2.0f * l2m * (-dmp);
+        const float Q = 2.0f * (l2m * (-dmp) - 2.0f * mu * (-dms));
+        const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
+        a.ovo_txx[k] = P * sa * rdx + Q * sb * rdz;
+        a.ovo_tzz[k] = Q * sa * rdx + P * sb * rdz;
+        a.ovo_txz[k] = 2.0f * mu * (-dms) * (sf * rdx + se * rdz);
       }
     }
   }
@@ -1044,6 +1107,209 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
         a.ab.vx[k] = vx;
         a.ab.vz[k] = vz;
       }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Reverse step of the first-order scattered set of reference-mode ELSRTM (FD2DGPU.cu:4685-4807),
+// fed by the ring: interior reconstruction of b1 (stress then velocity, direction -1; strips st_b
+// in the band, as k_str<kRev> / k_vel<kRev>), with the Born source of the background's
+// reconstructed velocities (ov_*, written by k_born after k_bwd_ring) added to the stress stencil
+// values of the velocity stage, and the imaging condition of b1's strains with the adjoint
+// stresses of the same step into images 3 and 4 (k_image, b_pp / b_ps).  Same x-march as
+// k_bwd_ring: stage 1 updates the stresses of row r-4 and images them, stage 2 the velocities of
+// row r-8.  Fields of ring slot q:
+//  0-1   bvx, bvz of row q (strip words in the band)
+//  2-6   btxx, btzz, btxz, lam, mu of row q-4
+//  7-16  kpp, kps, image 3, image 4, atxx, atzz, atxz, ov txx, ov tzz, ov txz of row q-4 (interior)
+//  17    b of row q-8; 18-19 bvx, bvz of row q-8 (inner strip-band cells: their own state)
+//  20-21 the FP32 scales of the two strip words of row q (FP16 / BF16 strips)
+struct BwdScatArgs {
+  Dims d;
+  Wave ra, rb;                            // b1 state at t (read), t-1 (written)
+  const float *atxx, *atzz, *atxz;        // adjoint stresses of this step
+  const float *ov_txx, *ov_tzz, *ov_txz;  // Born source of the background's velocities
+  Par p;
+  const ShotDev *shots;
+  Strips st;
+  int strips_on;
+  int it;
+  int tz, xr;
+  float *img;  // [7][slot][wnx][wnz]; planes 3 and 4 are accumulated
+  long long img_plane;
+};
+constexpr int kBwdScatRingFields = 22;
+
+template <bool kPML, int kD, int kMinB>
+__global__ void __launch_bounds__(kFB, kMinB) k_bwd_scat_ring(BwdScatArgs a) {
+  static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
+  constexpr int NF = kBwdScatRingFields;
+  extern __shared__ float ring[];  // [kD][NF][kFB]
+  __shared__ float s_bvx[kFB], s_bvz[kFB], s_btxz[kFB], s_btzz[kFB];
+  const int s = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int z = blockIdx.x * a.tz - 8 + t;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  const int base = (int)(d.slot * s);  // cell offsets fit 32 bits (checked on the host)
+  const int ld = d.ld, pml = d.pml;
+  const bool zin = z >= 0 && z < d.nzp;
+  const bool c1 = t >= 4 && t < a.tz + 12;
+  const bool c2 = t >= 8 && t < a.tz + 8;
+  const bool z_int = z >= pml && z < d.nzp - pml;
+  const bool strips = kPML && a.strips_on;
+  const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
+  const int img_row = s * d.wnx_max;  // image row of model row r: img_row + r - pml
+  float *img_b = a.img + 3 * a.img_plane, *img_bs = a.img + 4 * a.img_plane;
+  const long long strip_row0 = ((long long)s * d.nt + a.it) * 2;
+  auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kFB + t]; };
+  auto strip_elem = [&](int comp, int bo) { return (strip_row0 + comp) * d.lb_max + bo; };
+  auto issue = [&](int q) {
+    const int r0 = q, r4 = q - 4, r8 = q - 8;
+    const bool in0 = r0 >= 0 && r0 < d.nxp && zin;
+    const bool in4 = r4 >= 0 && r4 < d.nxp && zin;
+    const bool in8 = r8 >= 0 && r8 < d.nxp && zin;
+    const int o0 = base + r0 * ld + z, o4 = base + r4 * ld + z, o8 = base + r8 * ld + z;
+    const bool int4 = in4 && r4 >= pml && r4 < d.nxp - pml && z_int;
+    const bool int8 = in8 && r8 >= pml && r8 < d.nxp - pml && z_int;
+    const int bo0 = strips && in0 ? band_offset(d, r0, z) : -1;
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      float *dst = &R(q, f);
+      if (!in0) {
+        *dst = 0.f;
+      } else if (kPML && bo0 >= 0) {
+        const long long e = strip_elem(f, bo0);
+        if (a.st.prec == 0) {
+          cp_async4(dst, (const float *)a.st.data + e);
+        } else {
+          cp_async4(dst, (const float *)((const char *)a.st.data + ((e * 2) & ~3LL)));
+          cp_async4(&R(q, 20 + f), a.st.scale + (strip_row0 + f) * d.nseg_max + (bo0 >> 5));
+        }
+      } else {
+        cp_async4(dst, (f == 0 ? a.ra.vx : a.ra.vz) + o0);
+      }
+    }
+    if (in4) {
+      cp_async4(&R(q, 2), a.ra.txx + o4);
+      cp_async4(&R(q, 3), a.ra.tzz + o4);
+      cp_async4(&R(q, 4), a.ra.txz + o4);
+      cp_async4(&R(q, 5), a.p.lam + o4);
+      cp_async4(&R(q, 6), a.p.mu + o4);
+    } else {
+      R(q, 2) = R(q, 3) = R(q, 4) = R(q, 5) = R(q, 6) = 0.f;
+    }
+    if (int4) {
+      const int io = (img_row + r4 - pml) * d.wnz + (z - pml);
+      cp_async4(&R(q, 7), a.p.kpp + o4);
+      cp_async4(&R(q, 8), a.p.kps + o4);
+      cp_async4(&R(q, 9), img_b + io);
+      cp_async4(&R(q, 10), img_bs + io);
+      cp_async4(&R(q, 11), a.atxx + o4);
+      cp_async4(&R(q, 12), a.atzz + o4);
+      cp_async4(&R(q, 13), a.atxz + o4);
+      cp_async4(&R(q, 14), a.ov_txx + o4);
+      cp_async4(&R(q, 15), a.ov_tzz + o4);
+      cp_async4(&R(q, 16), a.ov_txz + o4);
+    } else {
+      R(q, 14) = R(q, 15) = R(q, 16) = 0.f;  // the Born source is zero outside the interior
+    }
+    if (in8) cp_async4(&R(q, 17), a.p.b + o8); else R(q, 17) = 0.f;
+    if (strips && int8 && band_offset(d, r8, z) >= 0) {
+      cp_async4(&R(q, 18), a.ra.vx + o8);
+      cp_async4(&R(q, 19), a.ra.vz + o8);
+    }
+    cp_async_commit();
+  };
+
+  float w_bvx[9], w_bvz[9], w_btxx[9], w_btxz[9], w_btzz[5];
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_bvx[i] = w_bvz[i] = w_btxx[i] = w_btxz[i] = 0.f;
+#pragma unroll
+  for (int i = 0; i < 5; i++) w_btzz[i] = 0.f;
+
+#pragma unroll
+  for (int j = 0; j < kD - 1; j++) issue(x0 - 8 + j);
+#pragma unroll kRingUnrollBwd
+  for (int r = x0 - 8; r < x1 + 8; r++) {
+    cp_async_wait<kD - 2>();  // slot r has landed (this thread's copies)
+    {
+      float n_bvx = R(r, 0), n_bvz = R(r, 1);
+      if (strips && r >= 0 && r < d.nxp && zin) {
+        const int bo = band_offset(d, r, z);
+        if (bo >= 0) {
+          n_bvx = strip_unpack(a.st.prec, strip_elem(0, bo), n_bvx, R(r, 20));
+          n_bvz = strip_unpack(a.st.prec, strip_elem(1, bo), n_bvz, R(r, 21));
+        }
+      }
+      push(w_bvx, n_bvx);
+      push(w_bvz, n_bvz);
+    }
+    issue(r + kD - 1);
+    // ---- stage 1: stresses of row r1 = r - 4, strains, images 3 and 4 -------------------------
+    const int r1 = r - 4;
+    s_bvx[t] = w_bvx[4];
+    s_bvz[t] = w_bvz[4];
+    __syncthreads();
+    float pxx = 0.f, pzz = 0.f, pxz = 0.f;  // stress + Born source: the velocity stage's operand
+    if (c1 && zin && r >= x0 && r1 >= 0 && r1 < d.nxp) {
+      const int k = base + r1 * ld + z;
+      const bool own = c2 && r1 >= x0 && r1 < x1;
+      float btxx = R(r, 2), btzz = R(r, 3), btxz = R(r, 4);
+      if (r1 >= pml && r1 < d.nxp - pml && z_int) {
+        const float sa = dxm_mid(w_bvx);
+        const float sf = dxp_mid(w_bvz);
+        const float sb = stencil4([&](int i) { return s_bvz[t + i - 1] - s_bvz[t - i]; });
+        const float se = stencil4([&](int i) { return s_bvx[t + i] - s_bvx[t - i + 1]; });
+        const float lam = R(r, 5), mu = R(r, 6);
+        const float l2m = lam + 2.0f * mu;
+        const float dir = -1.0f;
+        btxx = btxx + (dir * l2m * dtdx * sa + dir * lam * dtdz * sb);
+        btzz = btzz + (dir * lam * dtdx * sa + dir * l2m * dtdz * sb);
+        btxz = btxz + (dir * mu * dtdx * sf + dir * mu * dtdz * se);
+        if (own) {
+          a.rb.txx[k] = btxx;
+          a.rb.tzz[k] = btzz;
+          a.rb.txz[k] = btxz;
+          const float gx_vx = sa * rdx, gz_vz = sb * rdz, gz_vx = se * rdz, gx_vz = sf * rdx;
+          const float atxx = R(r, 11), atzz = R(r, 12), atxz = R(r, 13);
+          const float lamda_grad = (gx_vx + gz_vz) * (atxx + atzz);
+          const float miu_grad = -2.0f * (gx_vx * atzz + gz_vz * atxx) + (gz_vx + gx_vz) * atxz;
+          const int o = (img_row + (r1 - pml)) * d.wnz + (z - pml);
+          img_b[o] = R(r, 9) + R(r, 7) * lamda_grad;
+          img_bs[o] = R(r, 10) + R(r, 8) * miu_grad;
+        }
+      }
+      pxx = btxx + R(r, 14);
+      pzz = btzz + R(r, 15);
+      pxz = btxz + R(r, 16);
+    }
+    push(w_btxx, pxx);
+    push(w_btxz, pxz);
+    push(w_btzz, pzz);
+    // ---- stage 2: velocities of row r2 = r - 8 ---------------------------------------------
+    const int r2 = r - 8;
+    s_btxz[t] = w_btxz[4];
+    s_btzz[t] = w_btzz[0];
+    __syncthreads();
+    if (c2 && zin && r2 >= x0 && r2 < x1 && r2 >= pml && r2 < d.nxp - pml && z_int) {
+      const int k = base + r2 * ld + z;
+      const float bb = R(r, 17);
+      const float cbx = bb * dtdx, cbz = bb * dtdz;
+      const float ax = dxp_mid(w_btxx);
+      const float fx = dxm_mid(w_btxz);
+      const float bz = stencil4([&](int i) { return s_btxz[t + i - 1] - s_btxz[t - i]; });
+      const float ez = stencil4([&](int i) { return s_btzz[t + i] - s_btzz[t - i + 1]; });
+      float ovx = w_bvx[0], ovz = w_bvz[0];
+      if (strips && band_offset(d, r2, z) >= 0) {  // inner band: own state, not the strip
+        ovx = R(r, 18);
+        ovz = R(r, 19);
+      }
+      a.rb.vx[k] = ovx + (-cbx * ax + -cbz * bz);
+      a.rb.vz[k] = ovz + (-cbx * fx + -cbz * ez);
     }
   }
   cp_async_wait<0>();

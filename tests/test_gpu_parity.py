@@ -114,6 +114,60 @@ def test_elsrtm_vs_golden_and_oracle(cuda_device, it):
         assert mis == pytest.approx(fx["misfit"], rel=1e-4)
 
 
+@pytest.mark.parametrize("boundary", ["pml", "random"])
+def test_elsrtm_fused_matches_half_steps(cuda_device, boundary):
+    """Reference-mode ELSRTM on the fused ring kernels (Born sources computed inside the
+    background and first-order steps) against the half-step path and the FP64 oracle, three
+    shots in one batch."""
+    c, vp, vs, w, shots = small_case(nt=300)
+    vpm, vsm = synth.smooth(vp, 3.0), synth.smooth(vs, 3.0)
+    img_pp = synth.reflectivity(c["allnx"], c["allnz"], seed=5, density=0.05, std=0.05)
+    img_ps = 0.5 * synth.reflectivity(c["allnx"], c["allnz"], seed=6, density=0.05, std=0.05)
+    with _ctx(c, shots) as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        oz, ox = e.forward(shots)
+    rbc = int(boundary == "random")
+    out = {}
+    for fused in (0, 1):
+        with _ctx(c, shots, boundary=boundary, seed=5) as e:
+            e.set_option("fused", fused)
+            e.set_models(vpm, vsm)
+            e.set_wavelet(w)
+            e.set_image(img_pp, img_ps)
+            mis, recs = e.elsrtm(shots, oz, ox, 1, want_records=True)
+            out[fused] = (mis, recs, e.read_images())
+    # Same formulas, but the ring kernels round a few products differently (their expressions
+    # contract into FMAs differently from the half-step kernels').  With the PML the two paths
+    # agree to about 1e-6; the undamped random band keeps every rounding difference in the grid,
+    # so there both are held to the FP32-vs-FP64 spread of the oracle.
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    ntr = shots[0].ntr
+    tot64 = np.zeros((5, c["allnx"], c["allnz"]))
+    tot32 = np.zeros((5, c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        m = po.build_model(st, vpm, vsm, None, s.win_left, rbc=rbc, seed=5, shot_id=i)
+        dmp = po.window_image(st, img_pp, s.win_left)
+        dms = po.window_image(st, img_ps, s.win_left)
+        sl = slice(i * ntr, (i + 1) * ntr)
+        args = (st, m, dmp, dms, w, s, oz[sl], ox[sl], 1)
+        r64 = po.elsrtm(*args, rbc=rbc, precision="f64")
+        r32 = po.elsrtm(*args, rbc=rbc, precision="f32")
+        for j, key in enumerate(("lm_vz", "lm_vx", "res_vz", "res_vx")):
+            tol = gate(rel(r32[key], r64[key]))
+            assert np.abs(r64[key]).max() > 0
+            for fused in (0, 1):
+                assert rel(out[fused][1][j][sl], r64[key]) < tol, (key, fused)
+            assert rel(out[1][1][j][sl], out[0][1][j][sl]) < tol, key
+        for k in range(5):
+            tot64[k] += po.place(r64["images"][k], c["allnx"], c["allnz"], s.win_left)
+            tot32[k] += po.place(r32["images"][k], c["allnx"], c["allnz"], s.win_left)
+    for k, key in enumerate(Elastic2D.IMAGE_NAMES[:5]):
+        tol = gate(rel(tot32[k], tot64[k]))
+        for fused in (0, 1):
+            assert rel(out[fused][2][key], tot64[k]) < tol, (key, fused)
+
+
 def test_elsrtm_adjoint_born_as_written(cuda_device):
     """The scattered-adjoint term the reference's runs never execute (its launch exceeds the
     register limit), evaluated as written, against the FP64 oracle doing the same."""
