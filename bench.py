@@ -31,6 +31,10 @@ sys.path.insert(0, ROOT)
 
 CFG = dict(allnx=1201, allnz=401, pml=40, nt=4000, dx=10.0, dz=10.0, dt=0.0008, f0=15.0,
            shots=60, sz=0, gz=2, seed=2024)
+# Reference-mode ELSRTM workload.  Counted propagations per shot: 6 (background, first- and
+# second-order Born sets forward; background and first-order reconstruction and the adjoint
+# backward); the reference also propagates a scattered adjoint that its runs leave at zero.
+ELSRTM_SHOTS, ELSRTM_NT, ELSRTM_PROPS = 16, 2000, 6
 
 
 def parse():
@@ -46,10 +50,12 @@ def parse():
     p.add_argument("--ref-shots", type=int, default=2, help="shots per reference-arm step")
     p.add_argument("--no-autotune", action="store_true",
                    help="skip the launch-shape autotuner (library defaults)")
-    p.add_argument("--workload", default="rtm", choices=["rtm", "uneven", "lsrtm"],
+    p.add_argument("--workload", default="rtm", choices=["rtm", "uneven", "lsrtm", "elsrtm"],
                    help="rtm: elastic RTM throughput, 60 shots 1201x401 (default); uneven: 256 "
                         "shots with their own aperture windows from a 4001x401 model; lsrtm: "
-                        "learned vs plain CG-LSRTM")
+                        "learned vs plain CG-LSRTM; elsrtm: reference-mode ELSRTM iteration "
+                        "(PML + boundary strips, Born modelling, NCC adjoint source), 16 shots "
+                        "1201x401, nt 2000")
     p.add_argument("--lsrtm-size", default="full", choices=["small", "full"],
                    help="full: 2001x601, 80 shots, nt 5000; small: 512x256, 40 shots, nt 2000")
     p.add_argument("--pairs", type=int, default=192, help="training pairs of the preconditioner")
@@ -121,6 +127,11 @@ def workload(args, rank, world=1):
         c.update(allnx=4001, pml=20, wmin=400, wmax=1500)
         if args.shots == CFG["shots"]:
             c["shots"] = 256
+    if getattr(args, "workload", "rtm") == "elsrtm":  # 40-cell PML, 16 shots, nt 2000 by default
+        if args.shots == CFG["shots"]:
+            c["shots"] = ELSRTM_SHOTS
+        if args.nt == CFG["nt"]:
+            c["nt"] = ELSRTM_NT
     vp, vs = synth.dipping_lenses(c["allnx"], c["allnz"], seed=c["seed"])
     vpm, vsm = synth.smooth(vp, 15.0), synth.smooth(vs, 15.0)
     w = synth.ricker(c["nt"], c["f0"], c["dt"])
@@ -315,6 +326,196 @@ def run_ours(args, rank, world, dist):
     return out
 
 
+def elsrtm_images(c):
+    """Seeded reflectivity images (the current model update) of the ELSRTM workload."""
+    from ds2d_b200 import synth
+    pp = synth.reflectivity(c["allnx"], c["allnz"], seed=5, density=0.05, std=0.05)
+    ps = 0.5 * synth.reflectivity(c["allnx"], c["allnz"], seed=6, density=0.05, std=0.05)
+    return pp, ps
+
+
+def run_elsrtm(args, rank, world, dist):
+    """Reference-mode ELSRTM iteration (PML, boundary strips, Born modelling of two orders, NCC
+    adjoint source, seven images) of this rank's shots, timed with CUDA events; the gradients
+    are summed over ranks like the reference's MPI reduction."""
+    import torch
+    from ds2d_b200 import Elastic2D
+    c, vp, vs, vpm, vsm, w, shots = workload(args, rank, world)
+    dev = torch.cuda.current_device()
+    ntr = max(s.ntr for s in shots)
+    g = (c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"])
+    with Elastic2D(*g, boundary="pml", max_shots=len(shots), max_ntr=ntr, device=dev) as fm:
+        fm.set_models(vp, vs)
+        fm.set_wavelet(w)
+        obs_z, obs_x = fm.forward(shots)
+    img_pp, img_ps = elsrtm_images(c)
+    e = Elastic2D(*g, boundary="pml", strips="f32", max_shots=len(shots), max_ntr=ntr, device=dev)
+    e.set_models(vpm, vsm)
+    e.set_wavelet(w)
+    e.set_image(img_pp, img_ps)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    e.set_stream(stream.cuda_stream)
+    d_z = torch.from_numpy(obs_z).to(dev)
+    d_x = torch.from_numpy(obs_x).to(dev)
+    h_z = torch.from_numpy(obs_z).pin_memory()
+    h_x = torch.from_numpy(obs_x).pin_memory()
+    h2d = int(h_z.numel() + h_x.numel()) * 4
+    names = ("pp_grad", "ps_grad")
+    img_bytes = len(names) * c["allnx"] * c["allnz"] * 4
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce_grads():
+        if dist is not None:
+            from ds2d_b200.shard import reduce_images
+            reduce_images(e.read_images(reset=True, which=names), dist, device=dev)
+
+    for _ in range(args.warmup):
+        e.elsrtm_device(shots, d_z.data_ptr(), d_x.data_ptr(), 1)
+    reduce_grads()
+    e.read_images(reset=True)
+    launches = e.last_launches
+    upd = e.last_cell_updates
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            e.elsrtm_device(shots, d_z.data_ptr(), d_x.data_ptr(), 1)
+            reduce_grads()
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_upd = upd * world * args.steps
+    value = total_upd / (ms / 1e3) / 1e9
+    # end to end: observed records from pinned host memory, gradients back to the host
+    e.read_images(reset=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e.elsrtm(shots, h_z.numpy(), h_x.numpy(), 1)
+        if dist is not None:
+            reduce_grads()
+        else:
+            e.read_images(reset=True, which=names)
+    e1.record(stream)
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = total_upd / (ms_e2e / 1e3) / 1e9
+    roof = None
+    if rank == 0 and not args.no_profile:
+        e.profile(True)
+        e.elsrtm_device(shots, d_z.data_ptr(), d_x.data_ptr(), 1)
+        rep = e.profile_report()
+        e.profile(False)
+        tot = sum(v[1] for v in rep.values())
+        name, (n, kms, by) = max(rep.items(), key=lambda kv: kv[1][1])
+        peak, src = measured_peak()
+        achieved = by / n / (kms / n / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": src,
+                "traffic": traffic_for(name, len(shots)), "share": round(kms / tot, 4),
+                "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
+                                "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[2] > 0 else None}
+                            for k, v in rep.items()}}
+    out = None
+    if rank == 0:
+        out = {"metric": "Gcell-updates/s (reference-mode ELSRTM)", "value": round(value, 3),
+               "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded dipping-layer + lens model, PML-modelled observed "
+                       "data, seeded reflectivity images)",
+               "config": {"workload": f"reference-mode ELSRTM, PML + FP32 strips, {len(shots)} "
+                                      "shots per GPU",
+                          "model": f"{c['allnx']}x{c['allnz']} (+{c['pml']} PML) -> "
+                                   f"{cells(c)} padded cells",
+                          "nt": c["nt"], "shots_per_gpu": len(shots),
+                          "propagations_per_shot": ELSRTM_PROPS,
+                          "cell_updates_per_step": upd * world, "parallelism": f"shots x{world}",
+                          "l2": "inputs larger than L2 (wavefields of all resident shots, GBs)"},
+               "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s",
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": img_bytes},
+               "gpu_launches": int(launches * args.steps),
+               "clocks": clk.summary(), "roofline": roof}
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline_elsrtm(c, vpm, vsm, w, shots[0], obs_z, obs_x,
+                                                      img_pp, img_ps)
+    e.close()
+    return out
+
+
+def cpu_baseline_elsrtm(c, vpm, vsm, w, shot, obs_z, obs_x, img_pp, img_ps):
+    """Oracle FP32 reference-mode ELSRTM of one shot on a bounded number of steps."""
+    from oracle import pyoracle as po
+    nt = 60
+    st = po.Setup(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    m = po.build_model(st, vpm, vsm, None, shot.win_left)
+    dmp = po.window_image(st, img_pp, shot.win_left)
+    dms = po.window_image(st, img_ps, shot.win_left)
+    n0 = shot.ntr
+    oz = np.ascontiguousarray(obs_z[:n0, :nt])
+    ox = np.ascontiguousarray(obs_x[:n0, :nt])
+    t0 = time.perf_counter()
+    po.elsrtm(st, m, dmp, dms, w[:nt], shot, oz, ox, 1, precision="f32")
+    dt = time.perf_counter() - t0
+    upd = ELSRTM_PROPS * cells(c) * nt
+    return {"value": upd / dt / 1e9, "unit": "Gcell-updates/s", "cores": os.cpu_count(),
+            "kind": "port",
+            "sample": f"1 shot x {nt} steps of the 1281x481 reference-mode ELSRTM, oracle FP32, "
+                      f"OpenMP on {os.cpu_count()} threads, {dt:.1f} s"}
+
+
+def run_reference_elsrtm(args, c, vp, vs, vpm, vsm, w, shots):
+    """The reference's per-shot ELSRTM driver (ELSRTM_ROT_EXP_IMAGE_SINGLESHOT, its own CUDA
+    kernels built for sm_100a) on a sample of the workload's shots; the driver call alone is
+    timed with CUDA events (the harness's set-up of its FD2DGPU_ELASTIC object is not)."""
+    from oracle import pyoracle as po
+    sample = shots[:: max(1, len(shots) // args.ref_shots)][:args.ref_shots]
+    img_pp, img_ps = elsrtm_images(c)
+    g = (c["allnx"], c["allnz"], c["allnx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"])
+    obs = [po.ref_forward(*g, vp, vs, w, s) for s in sample]
+    for _ in range(args.warmup):
+        po.ref_elsrtm(*g, vpm, vsm, w, img_pp, img_ps, sample[0], obs[0][0], obs[0][1], 1)
+    tot = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for s, (oz, ox) in zip(sample, obs):
+            tot += po.ref_elsrtm(*g, vpm, vsm, w, img_pp, img_ps, s, oz, ox, 1)["elapsed_ms"]
+    wall = time.perf_counter() - t0
+    upd = ELSRTM_PROPS * cells(c) * c["nt"] * len(sample) * args.steps
+    v = upd / (tot / 1e3) / 1e9
+    ve = upd / wall / 1e9
+    return {"impl": "reference", "metric": "Gcell-updates/s (reference-mode ELSRTM)",
+            "value": round(v, 3), "unit": "Gcell-updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(tot / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": "reference-mode ELSRTM, PML + strips",
+                                            "shots_per_step": len(sample), "nt": c["nt"],
+                                            "propagations_per_shot": ELSRTM_PROPS},
+            "cpu_baseline": {"value": round(v, 3), "unit": "Gcell-updates/s", "cores": 1,
+                             "kind": "reference",
+                             "sample": f"{len(sample)} of the {len(shots)} shots per step, full "
+                                       "nt, run by the reference's own per-shot driver and CUDA "
+                                       "kernels (FD2DGPU.cu / born.cu built for sm_100a) on the "
+                                       "same B200"},
+            "e2e": {"value": round(ve, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args, rank, world):
     """The reference's own CUDA build (oracle/_ref) on a bounded sample of the same workload."""
     from oracle import pyoracle as po
@@ -322,12 +523,14 @@ def run_reference(args, rank, world):
         return None
     if not po.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libds2dref.so was not built"}
-    if args.workload != "rtm":
+    if args.workload not in ("rtm", "elsrtm"):
         return {"impl": "reference", "unavailable": "the reference runs one window width for all "
                 "shots (main.cpp:1010-1017) and has no learned or CG-LSRTM path; its arm covers "
-                "the default RTM workload"}
+                "the RTM and ELSRTM workloads"}
     import torch  # noqa: F401
     c, vp, vs, vpm, vsm, w, shots = workload(args, 0)
+    if args.workload == "elsrtm":
+        return run_reference_elsrtm(args, c, vp, vs, vpm, vsm, w, shots)
     sample = shots[:: max(1, len(shots) // args.ref_shots)][:args.ref_shots]
     st = po.Setup(c["allnx"], c["allnz"], c["allnx"], c["pml"], c["dx"], c["dz"], c["dt"])
     # observed data with the reference's own PML forward modelling
@@ -501,7 +704,7 @@ def main():
         import torch.distributed as td
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         dist = td
-    out = run_ours(args, rank, world, dist)
+    out = (run_elsrtm if args.workload == "elsrtm" else run_ours)(args, rank, world, dist)
     if out is not None:
         print(json.dumps(out))
     if dist is not None:

@@ -146,6 +146,17 @@ class Elastic2D:
             return mis.value, (lz, lx, rz, rx)
         return mis.value
 
+    def elsrtm_device(self, shots, obs_vz_ptr, obs_vx_ptr, iteration):
+        """Reference-mode ELSRTM with the observed records in device memory (integer device
+        pointers, [sum ntr][nt] each); returns the misfit increment."""
+        arr, keep = self._shots(shots)
+        mis = ctypes.c_double(0.0)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self._check(self.lib.ds2d_elsrtm(self.h, arr, len(shots), ctypes.cast(obs_vz_ptr, fp),
+                                         ctypes.cast(obs_vx_ptr, fp), int(iteration),
+                                         ctypes.byref(mis), None, None, None, None))
+        return mis.value
+
     def rtm(self, shots, adj_vz, adj_vx):
         """Elastic RTM of the given shots with adj_* injected at the receivers."""
         arr, keep = self._shots(shots)

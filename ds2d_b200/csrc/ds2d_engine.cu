@@ -1519,7 +1519,7 @@ int ds2d_elsrtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *obs_vz,
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if ((rc = copy_records_in(c, shots + f, m, obs_vz, obs_vx, tb, c->rec[0], c->rec[1],
-                              cudaMemcpyHostToDevice)))
+                              cudaMemcpyDefault)))
       return rc;
     if ((rc = elsrtm_batch(c, shots + f, m, f, iter, misfit))) return rc;
     if (lm_vz || lm_vx)

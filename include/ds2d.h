@@ -92,9 +92,11 @@ int ds2d_forward(ds2d_ctx *ctx, const ds2d_shot *shots, int n, float *rec_vz, fl
 
 /* Reference-mode ELSRTM of n shots: ELSRTM_ROT_EXP_IMAGE_SINGLESHOT (FD2DGPU.cu:4184) per shot,
  * with record_copytoGPU (:3537) and bufferVpVsHtoD (:1336) folded in.  obs_* are the observed
- * records [sum ntr][nt].  Gradients accumulate in the context's seven images (read them with
- * ds2d_read_images); *misfit accumulates like the reference's double& argument.  lm_* / res_*
- * may be NULL; when given they receive Lm + Lm2 and the injected adjoint source. */
+ * records [sum ntr][nt], in host or device memory (copied with unified addressing; the reference
+ * takes host records, record_copytoGPU).  Gradients accumulate in the context's seven images
+ * (read them with ds2d_read_images); *misfit accumulates like the reference's double& argument.
+ * lm_* / res_* may be NULL; when given they receive Lm + Lm2 and the injected adjoint source
+ * (host arrays). */
 int ds2d_elsrtm(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *obs_vz,
                 const float *obs_vx, int iter, double *misfit, float *lm_vz, float *lm_vx,
                 float *res_vz, float *res_vx);

@@ -236,7 +236,7 @@ def ref_lib():
         I, F = ctypes.c_int, ctypes.c_float
         L.ref_forward.argtypes = [I, I, I, I, I, F, F, F, fp, fp, fp, I, I, I, I, I, ip, fp, fp]
         L.ref_elsrtm.argtypes = [I, I, I, I, I, F, F, F, fp, fp, fp, fp, fp, I, I, I, I, I, ip, fp,
-                                 fp, I, fp, fp, ctypes.POINTER(fp), dp]
+                                 fp, I, fp, fp, ctypes.POINTER(fp), dp, fp]
         L.ref_rtm.argtypes = [I, I, I, I, I, F, F, F, fp, fp, fp, I, ip, ip, I, I, I, ip, fp, fp, I,
                               fp, fp, ctypes.POINTER(fp), fp]
         _ref = L
@@ -263,14 +263,16 @@ def ref_elsrtm(allnx, allnz, nx, pml, nt, dx, dz, dt, vp, vs, wavelet, img_pp, i
     imgs = [np.zeros((allnx, allnz), np.float32) for _ in range(7)]
     iptr = (fp * 7)(*[_p(a) for a in imgs])
     mis = ctypes.c_double(0.0)
+    ms = ctypes.c_float(0)
     rc = ref_lib().ref_elsrtm(allnx, allnz, nx, pml, nt, dx, dz, dt, _p(_f(vp)), _p(_f(vs)),
                               _p(_f(wavelet)), _p(_f(img_pp)), _p(_f(img_ps)), shot.win_left,
                               shot.isx, shot.isz, shot.igz, len(gx), _p(gx, ip), _p(_f(obs_vz)),
                               _p(_f(obs_vx)), iteration, _p(res_z), _p(res_x), iptr,
-                              ctypes.byref(mis))
+                              ctypes.byref(mis), ctypes.byref(ms))
     if rc != 0:
         raise RuntimeError(f"ref_elsrtm: CUDA error {rc}")
-    return dict(res_vz=res_z, res_vx=res_x, images=imgs, misfit=mis.value)
+    # elapsed_ms: CUDA-event time of the reference's per-shot driver call alone
+    return dict(res_vz=res_z, res_vx=res_x, images=imgs, misfit=mis.value, elapsed_ms=ms.value)
 
 
 def ref_rtm(allnx, allnz, nx, pml, nt, dx, dz, dt, vp, vs, wavelet, shots, adj_vz, adj_vx,

@@ -94,7 +94,8 @@ int ref_elsrtm(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz
                const float *vp_all, const float *vs_all, const float *wavelet,
                const float *image_pp, const float *image_ps, int win_left, int isx, int isz,
                int igz, int ntr, const int *igx, const float *obs_vz, const float *obs_vx,
-               int iter, float *res_vz, float *res_vx, float *const img7[7], double *misfit) {
+               int iter, float *res_vz, float *res_vx, float *const img7[7], double *misfit,
+               float *elapsed_ms) {
   RefGeom g{allnx, allnz, nx, pml, nt, dx, dz, dt};
   size_t nall = (size_t)allnx * allnz, nrec = (size_t)ntr * nt;
   FD2DGPU_ELASTIC *f = make(g, wavelet, ntr);
@@ -117,9 +118,20 @@ int ref_elsrtm(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz
   double mis = 0;
   std::vector<float> pg(nall), sg(nall);
   char snapdir[] = ".";
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
   ELSRTM_ROT_EXP_IMAGE_SINGLESHOT(*f, 1, nDim, 1, rz.data(), rx.data(), gc.data(), false, false,
                                   1000, iter, snapdir, ipp.data(), ips.data(), pg.data(),
                                   sg.data(), mis);
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (elapsed_ms) *elapsed_ms = ms;
   if (res_vz) cudaMemcpy(res_vz, f->GPUrecord_scatter_z, nrec * sizeof(float), cudaMemcpyDeviceToHost);
   if (res_vx) cudaMemcpy(res_vx, f->GPUrecord_scatter_x, nrec * sizeof(float), cudaMemcpyDeviceToHost);
   f->imagebuffer_resettozero(img7[0], img7[1], img7[2], img7[3], img7[4], img7[5], img7[6]);

@@ -3,6 +3,8 @@ roofline inputs it reads from committed files."""
 import json
 import os
 
+import numpy as np
+
 import bench
 from ds2d_b200.shard import shard_shots
 
@@ -32,6 +34,14 @@ def test_uneven_workload_matches_its_config():
     assert all(0 <= s.win_left and s.win_left + s.nx <= 4001 for s in shots)
     parts = [shard_shots(shots, 4, r, c["nx"], 20, 441, 10) for r in range(4)]
     assert sorted(i for p in parts for i in p) == list(range(256))
+
+
+def test_elsrtm_workload_matches_its_config():
+    c, vp, vs, vpm, vsm, w, shots = bench.workload(_Args(workload="elsrtm"), 0, 1)
+    assert (c["allnx"], c["allnz"], c["pml"], c["nt"]) == (1201, 401, 40, bench.ELSRTM_NT)
+    assert len(shots) == c["shots"] == bench.ELSRTM_SHOTS and len(w) == bench.ELSRTM_NT
+    pp, ps = bench.elsrtm_images(c)
+    assert pp.shape == ps.shape == (1201, 401) and np.abs(pp).max() > 0
 
 
 def test_roofline_inputs():
