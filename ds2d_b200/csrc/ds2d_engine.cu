@@ -535,6 +535,9 @@ constexpr double kBytesBornMode[4] = {52, 72, 84, 64};
 // Reverse step of the first-order scattered set (k_bwd_scat_ring): its 5 fields read and written,
 // b, lam, mu, kpp, kps, the adjoint stresses and the Born source read, images 3 and 4 updated.
 constexpr double kBytesBwdScat = 100;
+// Fused acoustic reverse step (k_ac_rev_ring): adjoint state and background, 3 fields each read
+// and written, b and lam read, the gradient updated on the interior.
+constexpr double kBytesAcRev = 64;
 // Fused backward RTM step per padded cell: source and adjoint fields r/w (2 x 40), b, lam, mu
 // (12), imaging weights (8) and three image accumulators r/w (24).
 constexpr double kBytesBwdFused = 124;
@@ -1158,8 +1161,9 @@ int ac_LT_batch(ds2d_ctx *c, int n) {
   size_t plane = (size_t)c->B * d.wnx * d.wnz;
   CK(cudaMemsetAsync(c->img_slot, 0, plane * sizeof(float), c->stream));
   dim3 grid = cell_grid(d, n), blk(32, 8);
-  if (c->opt_fused && c->ring_ok && c->ac2[0]) {
-    // fused forward replay of the background; the reversal below runs in place on ac[0..2]
+  const bool fused = c->opt_fused && c->ring_ok && c->ac2[0];
+  if (fused) {
+    // fused forward replay of the background, final state left in ac[0..2]
     for (int i = 0; i < 3; i++) CK(cudaMemsetAsync(c->ac2[i], 0, bytes, c->stream));
     int rc, cur = 0;
     for (int it = 0; it < d.nt; it++, cur ^= 1)
@@ -1167,6 +1171,33 @@ int ac_LT_batch(ds2d_ctx *c, int n) {
     if (cur == 1)
       for (int i = 0; i < 3; i++)
         CK(cudaMemcpyAsync(c->ac[i], c->ac2[i], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    // fused reversal: one k_ac_rev_ring launch per step; the background ping-pongs between
+    // ac[0..2] and ac2[0..2], the adjoint state between ac[6..8] and ac2[3..5] (both start at
+    // zero; cells outside the updated band are never written in either)
+    for (int i = 3; i < 6; i++) CK(cudaMemsetAsync(c->ac2[i], 0, bytes, c->stream));
+    const int nstrips = (d.nzp + kAcRevTZ - 1) / kAcRevTZ;
+    const int tz = (d.nzp + nstrips - 1) / nstrips;
+    const int xr = std::max(8, c->opt_xr);
+    dim3 rgrid(nstrips, (d.nxp + xr - 1) / xr, n);
+    float *bk[2][3] = {{c->ac[0], c->ac[1], c->ac[2]}, {c->ac2[0], c->ac2[1], c->ac2[2]}};
+    float *yk[2][3] = {{c->ac[6], c->ac[7], c->ac[8]}, {c->ac2[3], c->ac2[4], c->ac2[5]}};
+    const size_t sm = sizeof(float) * 4 * kAcRevRingFields * kFB;
+    cur = 0;
+    for (int it = d.nt - 1; it >= 0; --it, cur ^= 1) {
+      AcRevArgs a{};
+      a.d = d; a.shots = c->d_shots;
+      a.yx = yk[cur][0]; a.yz = yk[cur][1]; a.ys = yk[cur][2];
+      a.yx_n = yk[cur ^ 1][0]; a.yz_n = yk[cur ^ 1][1]; a.ys_n = yk[cur ^ 1][2];
+      a.vx = bk[cur][0]; a.vz = bk[cur][1]; a.s = bk[cur][2];
+      a.vx_n = bk[cur ^ 1][0]; a.vz_n = bk[cur ^ 1][1]; a.s_n = bk[cur ^ 1][2];
+      a.b = c->par.b; a.lam = c->par.lam; a.grad = c->img_slot; a.wavelet = c->wavelet;
+      a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
+      a.res_vz = c->rec[0]; a.res_vx = c->rec[1];
+      void (*kfn)(AcRevArgs) = k_ac_rev_ring<4>;
+      LAUNCHS("ac_rev", kBytesAcRev * CELLS(n), kfn, rgrid, kFB, sm, a);
+    }
+    CK(cudaGetLastError());
+    return reduce_images(c, n, 1);
   } else {
     for (int it = 0; it < d.nt; it++) {
       AcArgs b = ac_args(c, 0, it, 1.f);

@@ -1443,4 +1443,217 @@ __global__ void __launch_bounds__(kFB, 6) k_ac_ring(AcRingArgs a) {
   cp_async_wait<0>();
 }
 
+// ---------------------------------------------------------------------------------------------
+// Reverse step of the acoustic L^T fed by the ring: the adjoint pair with the gradient and the
+// exact reversal of the background, the fused counterpart of k_ac_adj_v, k_ac_adj_s, k_ac_str and
+// k_ac_vel (direction -1) in that order, with the same arithmetic.  At row step r it
+//   A. (row r-4)  y_v += residual; yx -= dt/dx Dx+(lam ys), yz -= dt/dz Dz+(lam ys);
+//   B. (row r-8)  gs = -Dx-(b dt/dx yx) - Dz-(b dt/dz yz), ys += gs,
+//                 grad += -2 lam (Dx- bvx / dx + Dz- bvz / dz) gs (interior),
+//                 s -= lam (dt/dx Dx- bvx + dt/dz Dz- bvz)  (the same two derivatives);
+//   C. (row r-12) v -= b dt/d D+(s + source)  with the reversed s of stage B.
+// The three chained z-stencils need a 12-column halo on each side (kAcRevTZ output columns of
+// 128 threads) and the rows a 10-row lead; both state sets ping-pong between two buffers.
+// Ring fields of slot q: 0 ys, 1 lam of row q; 2 yx, 3 yz, 4 b, 5 bvx, 6 bvz of row q-4;
+// 7 ys, 8 bs, 9 lam, 10 grad of row q-8; 11 b of row q-12.
+// ---------------------------------------------------------------------------------------------
+constexpr int kAcRevRingFields = 12;
+constexpr int kAcRevTZ = kFB - 24;
+
+struct AcRevArgs {
+  Dims d;
+  const ShotDev *shots;
+  const float *yx, *yz, *ys;     // adjoint state (read)
+  float *yx_n, *yz_n, *ys_n;     // adjoint state one step back (written)
+  const float *vx, *vz, *s;      // background at step it (read)
+  float *vx_n, *vz_n, *s_n;      // background at step it - 1 (written)
+  const float *b, *lam;
+  float *grad;                   // [slot][wnx][wnz] (wnx_max stride), accumulated
+  const float *wavelet;
+  int it, tz, xr;
+  const int *rmap;
+  const float *res_vz, *res_vx;  // [slot][max_ntr][nt]
+};
+
+template <int kD>
+__global__ void __launch_bounds__(kFB, 4) k_ac_rev_ring(AcRevArgs a) {
+  static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
+  constexpr int NF = kAcRevRingFields;
+  extern __shared__ float ring[];  // [kD][NF][kFB]
+  __shared__ float s_w[kFB], s_uz[kFB], s_bvz[kFB], s_S[kFB];
+  // receiver column: trace index (16 stage-A rows ahead), residual (8 ahead) per row mod 16
+  __shared__ int s_tr[16], s_has[16];
+  __shared__ float s_rz[16], s_rx[16];
+  const int sl = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[sl]);
+  const int z = blockIdx.x * a.tz - 12 + t;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  const int base = (int)(d.slot * sl);  // cell offsets fit 32 bits (checked on the host)
+  const int ld = d.ld, pml = d.pml;
+  const bool zin = z >= 0 && z < d.nzp;
+  const bool zupd = z >= d.nop && z < d.nzp - d.nop;
+  const bool z_int = z >= pml && z < d.nzp - pml;
+  const bool colA = t >= 5 && t < a.tz + 19 && zupd;   // stage A: rows of the B halo
+  const bool colB = t >= 9 && t < a.tz + 16 && zupd;   // stage B: the C halo
+  const bool colC = t >= 12 && t < a.tz + 12 && zupd;  // stage C: own columns
+  const bool ownB = t >= 12 && t < a.tz + 12;
+  const ShotDev sh = a.shots[sl];
+  const bool rec_col = z == sh.igz;
+  const bool src_col = z == sh.isz;
+  const float sval = a.wavelet[a.it];
+  const float *res_z = a.res_vz + (long long)sl * d.max_ntr * d.nt + a.it;
+  const float *res_x = a.res_vx + (long long)sl * d.max_ntr * d.nt + a.it;
+  const int *rmap = a.rmap + (long long)sl * d.nxp_max;
+  const float cx = d.dt / d.dx, cz = d.dt / d.dz;
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
+  auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kFB + t]; };
+  auto issue = [&](int q) {
+    const int r0 = q, r4 = q - 4, r8 = q - 8, r12 = q - 12;
+    const bool in0 = r0 >= 0 && r0 < d.nxp && zin;
+    const bool in4 = r4 >= 0 && r4 < d.nxp && zin;
+    const bool in8 = r8 >= 0 && r8 < d.nxp && zin;
+    const bool in12 = r12 >= 0 && r12 < d.nxp && zin;
+    const int o0 = base + r0 * ld + z, o4 = base + r4 * ld + z, o8 = base + r8 * ld + z;
+    if (in0) {
+      cp_async4(&R(q, 0), a.ys + o0);
+      cp_async4(&R(q, 1), a.lam + o0);
+    } else {
+      R(q, 0) = R(q, 1) = 0.f;
+    }
+    if (in4) {
+      cp_async4(&R(q, 2), a.yx + o4);
+      cp_async4(&R(q, 3), a.yz + o4);
+      cp_async4(&R(q, 4), a.b + o4);
+      cp_async4(&R(q, 5), a.vx + o4);
+      cp_async4(&R(q, 6), a.vz + o4);
+    } else {
+      R(q, 2) = R(q, 3) = R(q, 4) = R(q, 5) = R(q, 6) = 0.f;
+    }
+    if (in8) {
+      cp_async4(&R(q, 7), a.ys + o8);
+      cp_async4(&R(q, 8), a.s + o8);
+      cp_async4(&R(q, 9), a.lam + o8);
+      if (r8 >= pml && r8 < d.nxp - pml && z_int)
+        cp_async4(&R(q, 10), a.grad + ((sl * d.wnx_max + (r8 - pml)) * d.wnz + (z - pml)));
+    } else {
+      R(q, 7) = R(q, 8) = R(q, 9) = 0.f;
+    }
+    if (in12) cp_async4(&R(q, 11), a.b + (base + r12 * ld + z)); else R(q, 11) = 0.f;
+    cp_async_commit();
+  };
+
+  float w_w[9], w_ux[9], w_uz[5], w_bvx[9], w_bvz[9], w_S[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_w[i] = w_ux[i] = w_bvx[i] = w_bvz[i] = w_S[i] = 0.f;
+#pragma unroll
+  for (int i = 0; i < 5; i++) w_uz[i] = 0.f;
+
+  const int r_first = x0 - 10, r_last = x1 + 12;
+#pragma unroll
+  for (int j = 0; j < kD - 1; j++) issue(r_first + j);
+  if (rec_col) {  // stage-A rows a = r - 4: trace indexes of the first 16, residuals of the first 8
+    const int a0 = r_first - 4;
+    for (int q = a0; q < a0 + 16; q++) s_tr[q & 15] = (q >= 0 && q < d.nxp) ? rmap[q] : -1;
+    for (int q = a0; q < a0 + 8; q++) {
+      const int tr = s_tr[q & 15];
+      s_has[q & 15] = tr >= 0;
+      if (tr >= 0) {
+        s_rz[q & 15] = res_z[(long long)tr * d.nt];
+        s_rx[q & 15] = res_x[(long long)tr * d.nt];
+      }
+    }
+  }
+  for (int r = r_first; r < r_last; r++) {
+    cp_async_wait<kD - 2>();  // slot r has landed (this thread's copies)
+    const int rA = r - 4, rB = r - 8, rC = r - 12;
+    if (rec_col) {  // residual of stage-A row rA + 8, trace index of rA + 16 (landed in time)
+      const int q8 = rA + 8, q16 = rA + 16;
+      const int tr8 = s_tr[q8 & 15];
+      s_has[q8 & 15] = tr8 >= 0;
+      if (tr8 >= 0) {
+        cp_async4(&s_rz[q8 & 15], res_z + (long long)tr8 * d.nt);
+        cp_async4(&s_rx[q8 & 15], res_x + (long long)tr8 * d.nt);
+      }
+      if (q16 >= 0 && q16 < d.nxp)
+        cp_async4((float *)&s_tr[q16 & 15], (const float *)(rmap + q16));
+      else
+        s_tr[q16 & 15] = -1;
+    }
+    push(w_w, R(r, 0) * R(r, 1));  // ys * lam  (k_ac_adj_v: lam[q] * ys[q])
+    push(w_bvx, R(r, 5));           // background velocities of row rA (stage B window)
+    push(w_bvz, R(r, 6));
+    issue(r + kD - 1);
+    // ---- A: adjoint velocities of row rA -------------------------------------------------------
+    s_w[t] = w_w[4];
+    __syncthreads();
+    float uxn = 0.f, uzn = 0.f;
+    if (rA >= 0 && rA < d.nxp && zin) {
+      float yx = R(r, 2), yz = R(r, 3);
+      if (colA && rA >= d.nop && rA < d.nxp - d.nop) {
+        const float tx = dxp_mid(w_w);
+        const float tzv = stencil4([&](int i) { return s_w[t + i] - s_w[t - i + 1]; });
+        if (rec_col && s_has[rA & 15]) {
+          yz += s_rz[rA & 15];
+          yx += s_rx[rA & 15];
+        }
+        yx = yx - cx * tx;
+        yz = yz - cz * tzv;
+        if (ownB && rA >= x0 && rA < x1) {
+          const int k = base + rA * ld + z;
+          a.yx_n[k] = yx;
+          a.yz_n[k] = yz;
+        }
+      }
+      const float bb = R(r, 4);
+      uxn = bb * cx * yx;  // k_ac_adj_s: b[q] * cx * yx[q]
+      uzn = bb * cz * yz;
+    }
+    push(w_ux, uxn);
+    push(w_uz, uzn);
+    // ---- B: ys, gradient and the background stress of row rB ---------------------------------
+    s_uz[t] = w_uz[0];  // 5-deep window: row rB is its oldest entry
+    s_bvz[t] = w_bvz[4];
+    __syncthreads();
+    float Sn = 0.f;
+    if (rB >= 0 && rB < d.nxp && zin) {
+      float bs = R(r, 8);
+      if (colB && rB >= d.nop && rB < d.nxp - d.nop) {
+        const int k = base + rB * ld + z;
+        const bool own = ownB && rB >= x0 && rB < x1;
+        const float gx = dxm_mid(w_ux);
+        const float gz = stencil4([&](int i) { return s_uz[t + i - 1] - s_uz[t - i]; });
+        const float gs = -gx - gz;
+        const float sx = dxm_mid(w_bvx);
+        const float sz = stencil4([&](int i) { return s_bvz[t + i - 1] - s_bvz[t - i]; });
+        const float lam = R(r, 9);
+        if (own) {
+          a.ys_n[k] = R(r, 7) + gs;
+          if (rB >= pml && rB < d.nxp - pml && z_int) {
+            const int o = (sl * d.wnx_max + (rB - pml)) * d.wnz + (z - pml);
+            a.grad[o] = R(r, 10) + -2.0f * lam * (sx * rdx + sz * rdz) * gs;
+          }
+        }
+        bs = bs + -1.0f * lam * (cx * sx + cz * sz);  // k_ac_str, dir = -1
+        if (own) a.s_n[k] = bs;
+      }
+      Sn = bs;
+      if (src_col && rB == sh.isx) Sn += sval;  // the source overlay of k_ac_vel (transient)
+    }
+    push(w_S, Sn);
+    // ---- C: background velocities of row rC ----------------------------------------------------
+    s_S[t] = w_S[4];
+    __syncthreads();
+    if (colC && rC >= x0 && rC < x1 && rC >= d.nop && rC < d.nxp - d.nop) {
+      const int k = base + rC * ld + z;
+      const float ax = dxp_mid(w_S);
+      const float az = stencil4([&](int i) { return s_S[t + i] - s_S[t - i + 1]; });
+      const float bb = R(r, 11);
+      a.vx_n[k] = w_bvx[0] + -1.0f * (bb * cx) * ax;  // k_ac_vel, dir = -1
+      a.vz_n[k] = w_bvz[0] + -1.0f * (bb * cz) * az;
+    }
+  }
+  cp_async_wait<0>();
+}
+
 }  // namespace ds2d
