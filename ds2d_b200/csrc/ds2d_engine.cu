@@ -60,11 +60,16 @@ FwdFn fwd_ring_fn(bool rbc, int depth, int occ = 0, int cta = kFB) {
 // Born-modelling modes of the forward ring kernel (1 background + Born source, 2 first-order
 // scattered set, 3 second-order set), default ring depth and CTA width; their larger rings allow
 // 3-4 CTAs per SM, so the register budget is set for 4.
+#ifndef DS2D_BORN_RING
+#define DS2D_BORN_RING 4
+#endif
+constexpr int kBornRing = DS2D_BORN_RING;  // ring depth of the Born-modelling modes
+
 FwdFn fwd_mode_fn(bool rbc, int mode) {
   switch (mode) {
-    case 1: return rbc ? k_fwd_ring<false, 4, 4, kFB, 1> : k_fwd_ring<true, 4, 4, kFB, 1>;
-    case 2: return rbc ? k_fwd_ring<false, 4, 4, kFB, 2> : k_fwd_ring<true, 4, 4, kFB, 2>;
-    default: return rbc ? k_fwd_ring<false, 4, 4, kFB, 3> : k_fwd_ring<true, 4, 4, kFB, 3>;
+    case 1: return rbc ? k_fwd_ring<false, kBornRing, 4, kFB, 1> : k_fwd_ring<true, kBornRing, 4, kFB, 1>;
+    case 2: return rbc ? k_fwd_ring<false, kBornRing, 4, kFB, 2> : k_fwd_ring<true, kBornRing, 4, kFB, 2>;
+    default: return rbc ? k_fwd_ring<false, kBornRing, 4, kFB, 3> : k_fwd_ring<true, kBornRing, 4, kFB, 3>;
   }
 }
 
@@ -853,7 +858,7 @@ int elsrtm_forward_fused(ds2d_ctx *c, int n, bool strips) {
       }
       if (m < 2) { a.ovo_txx = ov[m][0]; a.ovo_tzz = ov[m][1]; a.ovo_txz = ov[m][2]; }
       const int mode = m + 1;
-      const size_t sm = sizeof(float) * 4 * fwd_ring_fields(!d.rbc, mode) * kFB;
+      const size_t sm = sizeof(float) * kBornRing * fwd_ring_fields(!d.rbc, mode) * kFB;
       FwdFn kfn = fwd_mode_fn(d.rbc != 0, mode);
       LAUNCHS("fwd_born", kBytesBornMode[mode] * CELLS(n), kfn, grid, kFB, sm, a);
     }
@@ -1378,7 +1383,7 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
     for (bool rbc : {false, true})
       for (int mode = 1; mode <= 3 && e == cudaSuccess; mode++)
         e = cudaFuncSetAttribute(fwd_mode_fn(rbc, mode), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(sizeof(float) * 4 * fwd_ring_fields(!rbc, mode) * kFB));
+                                 (int)(sizeof(float) * kBornRing * fwd_ring_fields(!rbc, mode) * kFB));
     if (e != cudaSuccess) {
       g_create_err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
       delete c;
