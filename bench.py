@@ -35,6 +35,7 @@ CFG = dict(allnx=1201, allnz=401, pml=40, nt=4000, dx=10.0, dz=10.0, dt=0.0008, 
 # second-order Born sets forward; background and first-order reconstruction and the adjoint
 # backward); the reference also propagates a scattered adjoint that its runs leave at zero.
 ELSRTM_SHOTS, ELSRTM_NT, ELSRTM_PROPS = 16, 2000, 6
+TRAFFIC_CELLS_PER_SHOT = 1281 * 481  # padded cells of the grid the ncu traffic was captured on
 
 
 def parse():
@@ -176,17 +177,24 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def traffic_for(kernel, shots):
-    """DRAM bytes (read + write) per launch of `kernel` over `shots` resident shots, from the
-    per-shot figure of a committed ncu capture (profiles/traffic.json), else None.  A launch
-    advances every resident shot by one step, so its traffic scales with the shot count."""
+def traffic_for(kernel, cells):
+    """DRAM bytes (read + write) per launch of `kernel` over `cells` padded cells (all resident
+    shots), from a committed ncu capture (profiles/traffic.json: bytes per shot of the captured
+    1281x481 grid), else None.  A launch advances every resident cell by one step, so its traffic
+    scales with the cells of the batch."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
             per_shot = json.load(f)[kernel]["dram_bytes_per_shot"]
-        return round(per_shot * shots)
+        return round(per_shot * cells / TRAFFIC_CELLS_PER_SHOT)
     except Exception:
         return None
+
+
+def batch_cells(c, shots):
+    """Padded cells of all shots of a batch (each shot's own window width)."""
+    nz = c["allnz"] + 2 * c["pml"]
+    return sum(((s.nx or c["nx"]) + 2 * c["pml"]) * nz for s in shots)  # nx 0: the grid's nx
 
 
 def run_ours(args, rank, world, dist):
@@ -293,7 +301,7 @@ def run_ours(args, rank, world, dist):
         achieved = by / n / (kms / n / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": src,
-                "traffic": traffic_for(name, c["shots"]), "share": round(kms / tot, 4),
+                "traffic": traffic_for(name, batch_cells(c, shots)), "share": round(kms / tot, 4),
                 "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
                                 "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] > 0 else None}
                             for k, v in rep.items()}}
@@ -427,7 +435,7 @@ def run_elsrtm(args, rank, world, dist):
         achieved = by / n / (kms / n / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": src,
-                "traffic": traffic_for(name, len(shots)), "share": round(kms / tot, 4),
+                "traffic": traffic_for(name, batch_cells(c, shots)), "share": round(kms / tot, 4),
                 "kernels": {k: {"launches": v[0], "ms": round(v[1], 3),
                                 "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[2] > 0 else None}
                             for k, v in rep.items()}}

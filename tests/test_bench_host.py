@@ -52,6 +52,10 @@ def test_roofline_inputs():
     else:
         assert src == "fallback"
     # committed per-shot DRAM traffic scales with the resident shots of a launch
-    t16, t60 = bench.traffic_for("bwd_fused", 16), bench.traffic_for("bwd_fused", 60)
+    cell = bench.TRAFFIC_CELLS_PER_SHOT
+    t16, t60 = bench.traffic_for("bwd_fused", 16 * cell), bench.traffic_for("bwd_fused", 60 * cell)
     assert t16 and t60 and abs(t60 / t16 - 60 / 16) < 1e-6
-    assert bench.traffic_for("no_such_kernel", 60) is None
+    assert bench.traffic_for("no_such_kernel", 60 * cell) is None
+    # uneven windows: traffic follows the batch's padded cells, not its shot count
+    c, _, _, _, _, _, shots = bench.workload(_Args(workload="uneven", nt=10), 0, 1)
+    assert bench.batch_cells(c, shots) == sum((s.nx + 40) * 441 for s in shots)
