@@ -791,6 +791,11 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
   // and the cell's state without the residual (kept 8 rows for stage 2).
   __shared__ int s_tr[16], s_has[16];
   __shared__ float s_rz[16], s_rx[16], s_ownx[16], s_ownz[16];
+  // PML variants: per ring slot and thread, the predicates issue(q) derives for the rows slot q's
+  // step consumes -- the strip-band offset of row q, and bits 1 / 2 / 4 = PML cell at row q-4,
+  // PML cell at row q-8, inner strip-band cell at row q-8 -- so the march does not derive them
+  // again (same thread, written kD - 1 steps before the read).
+  __shared__ int s_bo[kPML ? kD * kT : 1], s_fl[kPML ? kD * kT : 1];
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int z = blockIdx.x * a.tz - 8 + t;
@@ -819,6 +824,19 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
                                a.p.lam,  a.p.mu,   a.p.kpp,  a.p.kps,  a.p.b};
   auto R = [&](int q, int f) -> float & { return ring[((q & (kD - 1)) * NF + f) * kT + t]; };
   auto strip_elem = [&](int comp, int bo) { return (strip_row0 + comp) * d.lb_max + bo; };
+  // band_offset with this thread's column terms hoisted, as selects
+  const int N = d.nop;
+  const bool zb_up = z >= pml - N && z < pml + N, zb_dn = z >= d.nzp - pml - N && z < d.nzp - pml + N;
+  const int zb_off = zb_up ? z - (pml - N) : d.wnx * 2 * N + z - (d.nzp - pml - N);
+  const bool zP = z < pml || z > d.nzp - pml;
+  auto band_row = [&](int ix) {
+    const bool xint = ix >= pml && ix < d.nxp - pml;
+    const bool xl = ix >= pml - N && ix < pml + N, xr = ix >= d.nxp - pml - N && ix < d.nxp - pml + N;
+    const int a1 = (ix - pml) * 2 * N + zb_off;
+    const int a2 = 4 * N * d.wnx + (xl ? ix - (pml - N) : 2 * N + ix - (d.nxp - pml - N)) * d.wnz + (z - pml);
+    return (xint && (zb_up || zb_dn)) ? a1 : ((z_int && (xl || xr)) ? a2 : -1);
+  };
+  auto pml_row = [&](int ix) { return zP || ix < pml || ix > d.nxp - pml; };
   auto issue = [&](int q) {
     const int r0 = q, r4 = q - 4, r8 = q - 8;
     const bool in0 = r0 >= 0 && r0 < d.nxp && zin;
@@ -827,9 +845,14 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
     const int o0 = base + r0 * ld + z, o4 = base + r4 * ld + z, o8 = base + r8 * ld + z;
     const bool int4 = in4 && r4 >= pml && r4 < d.nxp - pml && z_int;
     const bool int8 = in8 && r8 >= pml && r8 < d.nxp - pml && z_int;
-    const bool pml4 = kPML && in4 && pml_cell(d, r4, z);
-    const bool pml8 = kPML && in8 && pml_cell(d, r8, z);
-    const int bo0 = strips && in0 ? band_offset(d, r0, z) : -1;
+    const bool pml4 = kPML && in4 && pml_row(r4);
+    const bool pml8 = kPML && in8 && pml_row(r8);
+    const int bo0 = strips && in0 ? band_row(r0) : -1;
+    const bool own8 = strips && int8 && band_row(r8) >= 0;
+    if (kPML) {
+      s_bo[(q & (kD - 1)) * kT + t] = bo0;
+      s_fl[(q & (kD - 1)) * kT + t] = (pml4 ? 1 : 0) | (pml8 ? 2 : 0) | (own8 ? 4 : 0);
+    }
     // lag 0: stencil inputs (strip words in the band)
 #pragma unroll
     for (int f = 0; f < 4; f++) {
@@ -879,7 +902,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
       cp_async4(&R(q, 22), a.aa.vz_z + o8);
     } else if (int8) {
       cp_async4(&R(q, 17), img_il + ((img_row + r8 - pml) * d.wnz + (z - pml)));
-      if (strips && band_offset(d, r8, z) >= 0) {
+      if (own8) {
         cp_async4(&R(q, 23), a.ra.vx + o8);
         cp_async4(&R(q, 24), a.ra.vz + o8);
       }
@@ -931,11 +954,12 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
       else
         s_tr[q16 & 15] = -1;
     }
+    const int pfl = kPML ? s_fl[(r & (kD - 1)) * kT + t] : 0;  // cached predicates of slot r
     {
       float n_bvx = R(r, 0), n_bvz = R(r, 1), n_avx = R(r, 2), n_avz = R(r, 3);
       if (r >= 0 && r < d.nxp && zin) {
         if (strips) {
-          const int bo = band_offset(d, r, z);
+          const int bo = s_bo[(r & (kD - 1)) * kT + t];
           if (bo >= 0) {
             n_bvx = strip_unpack(a.st.prec, strip_elem(0, bo), n_bvx, R(r, 25));
             n_bvz = strip_unpack(a.st.prec, strip_elem(1, bo), n_bvz, R(r, 26));
@@ -1002,7 +1026,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float se = stencil4([&](int i) { return s_avx[t + i] - s_avx[t - i + 1]; });
         const float xx = -dtdx * sa, zz = -dtdz * sb, xz_x = -dtdx * sf, xz_z = -dtdz * se;
         const float oxx = R(r, 7), ozz = R(r, 8);
-        if (kPML && pml_cell(d, r1, z)) {
+        if (kPML && (pfl & 1)) {
           // ring slots 9, 12, 13, 14 of a PML cell: atxz_x, atxz_z, dampx, dampz
           const float ddx = R(r, 13) * d.dt * 0.5f, ddz = R(r, 14) * d.dt * 0.5f;
           const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
@@ -1064,7 +1088,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float bz = stencil4([&](int i) { return s_btxz[t + i - 1] - s_btxz[t - i]; });
         const float ez = stencil4([&](int i) { return s_btzz[t + i] - s_btzz[t - i + 1]; });
         float ovx = w_bvx[0], ovz = w_bvz[0];
-        if (strips && band_offset(d, r2, z) >= 0) {  // inner band: own state, not the strip
+        if (strips && (pfl & 4)) {  // inner band: own state, not the strip
           ovx = R(r, 23);
           ovz = R(r, 24);
         }
@@ -1083,7 +1107,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float ux_x = -cbx * t_x, ux_z = -cbz * t_xz;
         const float uz_x = -cbx * s_xz, uz_z = -cbz * s_z;
         float vx, vz;
-        if (kPML && pml_cell(d, r2, z)) {
+        if (kPML && (pfl & 2)) {
           // ring slots 17-22 of a PML cell: dampx, dampz, avx_x, avx_z, avz_x, avz_z
           const float ddx = R(r, 17) * d.dt * 0.5f, ddz = R(r, 18) * d.dt * 0.5f;
           const float d1 = 1.0f - ddx, d3 = 1.0f - ddz;
