@@ -1172,6 +1172,9 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_scat_ring(BwdScatArgs a) {
   constexpr int NF = kBwdScatRingFields;
   extern __shared__ float ring[];  // [kD][NF][kFB]
   __shared__ float s_bvx[kFB], s_bvz[kFB], s_btxz[kFB], s_btzz[kFB];
+  // strips: per ring slot and thread, the band offset of row q and whether row q-8 is an inner
+  // band cell (derived once by issue(q), read by the same thread kD - 1 steps later)
+  __shared__ int s_bo[kPML ? kD * kFB : 1], s_fl[kPML ? kD * kFB : 1];
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int z = blockIdx.x * a.tz - 8 + t;
@@ -1200,6 +1203,11 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_scat_ring(BwdScatArgs a) {
     const bool int4 = in4 && r4 >= pml && r4 < d.nxp - pml && z_int;
     const bool int8 = in8 && r8 >= pml && r8 < d.nxp - pml && z_int;
     const int bo0 = strips && in0 ? band_offset(d, r0, z) : -1;
+    const bool own8 = strips && int8 && band_offset(d, r8, z) >= 0;
+    if (kPML) {
+      s_bo[(q & (kD - 1)) * kFB + t] = bo0;
+      s_fl[(q & (kD - 1)) * kFB + t] = own8 ? 1 : 0;
+    }
 #pragma unroll
     for (int f = 0; f < 2; f++) {
       float *dst = &R(q, f);
@@ -1242,7 +1250,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_scat_ring(BwdScatArgs a) {
       R(q, 14) = R(q, 15) = R(q, 16) = 0.f;  // the Born source is zero outside the interior
     }
     if (in8) cp_async4(&R(q, 17), a.p.b + o8); else R(q, 17) = 0.f;
-    if (strips && int8 && band_offset(d, r8, z) >= 0) {
+    if (own8) {
       cp_async4(&R(q, 18), a.ra.vx + o8);
       cp_async4(&R(q, 19), a.ra.vz + o8);
     }
@@ -1263,7 +1271,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_scat_ring(BwdScatArgs a) {
     {
       float n_bvx = R(r, 0), n_bvz = R(r, 1);
       if (strips && r >= 0 && r < d.nxp && zin) {
-        const int bo = band_offset(d, r, z);
+        const int bo = s_bo[(r & (kD - 1)) * kFB + t];
         if (bo >= 0) {
           n_bvx = strip_unpack(a.st.prec, strip_elem(0, bo), n_bvx, R(r, 20));
           n_bvz = strip_unpack(a.st.prec, strip_elem(1, bo), n_bvz, R(r, 21));
@@ -1328,7 +1336,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_scat_ring(BwdScatArgs a) {
       const float bz = stencil4([&](int i) { return s_btxz[t + i - 1] - s_btxz[t - i]; });
       const float ez = stencil4([&](int i) { return s_btzz[t + i] - s_btzz[t - i + 1]; });
       float ovx = w_bvx[0], ovz = w_bvz[0];
-      if (strips && band_offset(d, r2, z) >= 0) {  // inner band: own state, not the strip
+      if (strips && s_fl[(r & (kD - 1)) * kFB + t]) {  // inner band: own state, not the strip
         ovx = R(r, 18);
         ovz = R(r, 19);
       }
