@@ -149,6 +149,16 @@ def workload(args, rank, world=1):
     return c, vp, vs, vpm, vsm, w, shots
 
 
+def job_updates(upd, dist, dev):
+    """Cell-updates of one step summed over all ranks (shards of uneven windows differ)."""
+    if dist is None:
+        return upd
+    import torch
+    t = torch.tensor([float(upd)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def cells(c):
     return (c["allnx"] + 2 * c["pml"]) * (c["allnz"] + 2 * c["pml"])
 
@@ -213,8 +223,10 @@ def run_ours(args, rank, world, dist):
     if not args.no_autotune:
         # launch shape chosen by the project's autotuner on a short probe of the same batch
         from ds2d_b200.autotune import apply, tune_rtm
-        tuned, _ = tune_rtm(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"],
-                            vpm, vsm, w, shots, max_ntr=ntr, seed=c["seed"], device=dev)
+        tuned, tune_ms = tune_rtm(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"],
+                                  c["dt"], vpm, vsm, w, shots, max_ntr=ntr, seed=c["seed"],
+                                  device=dev)
+        print("autotune ms per probe step: " + json.dumps(tune_ms), file=sys.stderr, flush=True)
     e = Elastic2D(c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
                   boundary="random", max_shots=c["shots"], max_ntr=ntr, seed=c["seed"], device=dev)
     if tuned:
@@ -268,7 +280,7 @@ def run_ours(args, rank, world, dist):
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    total_upd = upd * world * args.steps
+    total_upd = job_updates(upd, dist, dev) * args.steps
     value = total_upd / (ms / 1e3) / 1e9
     # end-to-end: host (pinned) data in, images out, through the public API
     e.read_images(reset=True)
@@ -320,7 +332,7 @@ def run_ours(args, rank, world, dist):
                                        f"-> per-shot windows (nx + {2 * c['pml']}) x "
                                        f"{c['allnz'] + 2 * c['pml']} cells")),
                           "nt": c["nt"], "shots_per_gpu": c["shots"], "propagations_per_shot": 3,
-                          "cell_updates_per_step": upd * world, "parallelism": f"shots x{world}",
+                          "cell_updates_per_step": total_upd / args.steps, "parallelism": f"shots x{world}",
                           "l2": "inputs larger than L2 (wavefields of all resident shots, GBs)",
                           "launch_shape": tuned or "library defaults (autotuner skipped)"},
                "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s",
@@ -402,7 +414,7 @@ def run_elsrtm(args, rank, world, dist):
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    total_upd = upd * world * args.steps
+    total_upd = job_updates(upd, dist, dev) * args.steps
     value = total_upd / (ms / 1e3) / 1e9
     # end to end: observed records from pinned host memory, gradients back to the host
     e.read_images(reset=True)
@@ -453,7 +465,7 @@ def run_elsrtm(args, rank, world, dist):
                                    f"{cells(c)} padded cells",
                           "nt": c["nt"], "shots_per_gpu": len(shots),
                           "propagations_per_shot": ELSRTM_PROPS,
-                          "cell_updates_per_step": upd * world, "parallelism": f"shots x{world}",
+                          "cell_updates_per_step": total_upd / args.steps, "parallelism": f"shots x{world}",
                           "l2": "inputs larger than L2 (wavefields of all resident shots, GBs)"},
                "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s",
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": img_bytes},
@@ -583,8 +595,7 @@ def run_lsrtm(args):
     ds2d_lsrtm_pcg with and without the network on the application grid."""
     import torch
     from ds2d_b200 import Elastic2D, precond, synth
-    from ds2d_b200.unet import UNet, flatten
-    from oracle import unet_oracle
+    from ds2d_b200.unet import UNet, he_normal
 
     def log(msg):
         print(msg, file=sys.stderr, flush=True)
@@ -618,7 +629,7 @@ def run_lsrtm(args):
     anx, anz, ant, ashots = (2001, 601, 5000, 80) if args.lsrtm_size == "full" else (512, 256, 2000, 40)
     hp, wp = (anx + 7) // 8 * 8, (anz + 7) // 8 * 8
     net = UNet(base=32, max_n=8, max_h=max(128, hp), max_w=max(tnz, wp), device=dev)
-    net.set_params(flatten(unet_oracle.init_params(5)))
+    net.set_params(he_normal(5))
     t0 = time.perf_counter()
     hist = precond.train(net, X[:args.pairs], Y[:args.pairs], steps=args.train_steps, batch=8,
                          lr=1e-3, log=log)

@@ -2,7 +2,9 @@
 launches are fixed 32x32 blocks).
 
 The knobs are the rows marched per CTA (`xr`), the depth of the cp.async prefetch ring (`ring`),
-the register / occupancy target (`occ`) and the threads per CTA (`cta`, 128 or 192).  Their best values depend on the grid, the number of
+the register / occupancy target (`occ`) and the threads per CTA (`cta`, 128 or 192) of the
+one-column ring kernels, and, for the random boundary, the pair-blocked bulk-copy kernels
+(`pair`) with their backward CTA width (`pair_cta`, 256 or 160) and rows per CTA (`pair_xr`).  Their best values depend on the grid, the number of
 resident shots and the boundary, so the tuner times each candidate on a probe context with the
 caller's grid and batch but only `probe_nt` time steps (an RTM of the same shots: one forward and
 one backward fused launch per step), and returns the fastest setting; `apply` copies it onto the
@@ -11,12 +13,28 @@ import numpy as np
 
 from .api import Elastic2D
 
-DEFAULT_SPACE = [
+_RING_BASE = {"pair": 0, "pair_cta": 0, "pair_xr": 0}
+_RING_SPACE = [
     {"ring": 4, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 0, "cta": 192},
-    {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 128},
-    {"ring": 4, "xr": 256, "occ": 0, "cta": 192}, {"ring": 2, "xr": 128, "occ": 0, "cta": 128},
-    {"ring": 8, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 1, "cta": 128},
+    {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 192},
+    {"ring": 2, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 1, "cta": 128},
 ]
+# Pair-blocked kernels (random boundary only): backward CTA width x rows per CTA (0 = the
+# library's wave-filling choice).
+_PAIR_SPACE = [{"pair": 1, "pair_cta": cta, "pair_xr": xr}
+               for cta in (256, 160) for xr in (0, 64, 96, 128, 192)]
+_RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0}
+
+
+def default_space(boundary="random"):
+    """Full option sets (every knob named, so no setting carries over between candidates)."""
+    space = [dict(_RING_BASE, **c) for c in _RING_SPACE]
+    if boundary == "random":
+        space = [dict(_RING_DEFAULTS, **c) for c in _PAIR_SPACE] + space
+    return space
+
+
+DEFAULT_SPACE = default_space("random")
 
 
 def tune_rtm(allnx, allnz, nx, pml, dx, dz, dt, vp, vs, wavelet, shots, boundary="random",
@@ -24,7 +42,7 @@ def tune_rtm(allnx, allnz, nx, pml, dx, dz, dt, vp, vs, wavelet, shots, boundary
     """Times every setting of `space` on an RTM of `shots` with probe_nt steps; returns
     (best setting, {setting key: ms per step})."""
     import torch
-    space = space or DEFAULT_SPACE
+    space = space or default_space(boundary)
     max_ntr = max_ntr or max(s.ntr for s in shots)
     w = np.asarray(wavelet, np.float32)[:probe_nt]
     timings = {}

@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(256) k_ac_adj_s(AcAdjArgs a) {
     const float *VX = a.bvx, *VZ = a.bvz;
     const float sx = stencil4([&](int i) { return __ldg(VX + k + (long long)(i - 1) * ld) - __ldg(VX + k - (long long)i * ld); });
     const float sz = stencil4([&](int i) { return __ldg(VZ + k + i - 1) - __ldg(VZ + k - i); });
-    const long long o = ((long long)s * d.wnx_max + (ix - d.pml)) * d.wnz + (iz - d.pml);
+    const long long o = ((long long)s * d.wnx_max + (ix - d.pml)) * d.ild + iz;
     a.grad[o] += -2.0f * a.p.lam[k] * (sx * (1.0f / d.dx) + sz * (1.0f / d.dz)) * gs;
   }
 }

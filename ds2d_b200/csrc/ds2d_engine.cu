@@ -4,6 +4,7 @@
 // "slots" (one per resident shot) with the shot's padded parameters, wavefields, strips and
 // window images.  One call (ds2d_forward / ds2d_elsrtm / ds2d_rtm) processes its shots in
 // batches of opts.max_shots; every kernel launch covers all shots of the batch.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,7 +19,9 @@
 
 #include "../../include/ds2d.h"
 #include "ds2d_acoustic.cuh"
+#include "ds2d_filter.cuh"
 #include "ds2d_fused.cuh"
+#include "ds2d_pair.cuh"
 #include "ds2d_step.cuh"
 
 using namespace ds2d;
@@ -253,6 +256,15 @@ struct ds2d_ctx {
   int opt_occ = 0;           // occupancy target of the ring kernels (see fwd_ring_fn)
   int opt_cta = 0;           // threads per CTA of the ring kernels: 0 auto, 128 or 192
   bool ring_ok = true;       // batch arrays fit the ring kernels' 32-bit offsets
+  // Pair-blocked bulk-copy kernels of the random-boundary RTM step (ds2d_pair.cuh): option
+  // "pair" (1 on where they apply, 0 off: the default until they beat the one-column kernels),
+  // "pair_cta" (backward CTA width: 0 auto, 256 or 160), "pair_xr" (rows per CTA: 0 = chosen to
+  // fill whole waves).
+  int opt_pair = 0, opt_pair_cta = 0, opt_pair_xr = 0;
+  int *d_err = nullptr;      // error word raised by a pair kernel's bounded wait
+  int num_sms = 148;
+  int occ_pair_fwd = 0, occ_pair_bwd256 = 0, occ_pair_bwd160 = 0;  // resident CTAs per SM
+  std::vector<int> h_nxp;    // padded window rows of each slot of the current batch
   int opt_pcg_switch = 970;  // ds2d_lsrtm_pcg: per-mille residual ratio that ends the network phase
   int opt_pcg_m = 8;         // ds2d_lsrtm_pcg: directions kept for explicit conjugation
   // Acoustic Born pair (LSRTM): background, scattered and adjoint states, Born overlay.
@@ -394,7 +406,7 @@ int ensure_rtm(ds2d_ctx *c) {
     if ((rc = alloc_slots(c, p))) return rc;
   if (!c->d.rbc && (rc = alloc_strips(c, c->st_a))) return rc;
   if (!c->img_slot) {
-    size_t n = (size_t)7 * c->B * c->d.wnx * c->d.wnz;
+    size_t n = (size_t)7 * c->B * c->d.wnx * c->d.ild;
     if ((rc = alloc(c, (void **)&c->img_slot, n * sizeof(float)))) return rc;
   }
   c->have_rtm = true;
@@ -463,6 +475,8 @@ int upload_batch(ds2d_ctx *c, const ds2d_shot *shots, int n) {
                     4 * d.nop * (wnx + d.wnz)};
   }
   c->batch_cells = c->batch_wcells = 0;
+  c->h_nxp.assign(n, 0);
+  for (int s = 0; s < n; s++) c->h_nxp[s] = sd[s].nxp;
   for (const ShotDev &x : sd) {
     c->batch_cells += (double)x.nxp * d.nzp;
     c->batch_wcells += (double)x.wnx * d.wnz;
@@ -593,6 +607,69 @@ void strip_split(const Dims &d, int cta, int *nstrips, int *tz) {
   *tz = (d.nzp + *nstrips - 1) / *nstrips;
 }
 
+// ---- pair-blocked kernels (random boundary) ------------------------------------------------
+constexpr int kPairFwdT = 256, kPairFwdD = 4;  // forward: 256 threads, ring of 4 slots
+constexpr int kPairBwdD = 3;                   // backward: ring of 3 slots
+using PairFwdFn = void (*)(FwdFusedArgs);
+using PairBwdFn = void (*)(BwdFusedArgs);
+PairFwdFn pair_fwd_fn() { return k_fwd_pair<kPairFwdT, kPairFwdD>; }
+PairBwdFn pair_bwd_fn(int cta) {
+  return cta == 160 ? k_bwd_pair<160, kPairBwdD, 2> : k_bwd_pair<256, kPairBwdD, 1>;
+}
+constexpr size_t kPairFwdSmem = pair_smem(kPairFwdT, kPairFwdD, kFwdPairFields, kFwdPairZ2);
+constexpr size_t pair_bwd_smem(int cta) {
+  return pair_smem(cta, kPairBwdD, kBwdPairFields, kBwdPairZ2);
+}
+
+bool pair_on(const ds2d_ctx *c) {
+  return c->opt_pair && c->opt_fused && c->ring_ok && c->d.rbc && c->d.nop == 4 &&
+         c->d.ild == c->d.ld && c->d_err && c->occ_pair_fwd > 0;
+}
+// Backward CTA width: the whole column in one 256-thread CTA when it fits (no z-halo recomputed),
+// else strips of 160-thread CTAs (two per SM).
+int pair_bwd_cta(const ds2d_ctx *c) {
+  if (c->opt_pair_cta == 160 || c->opt_pair_cta == 256) return c->opt_pair_cta;
+  return c->d.nzp + 16 <= 2 * 256 ? 256 : 160;
+}
+// z-strips of a pair launch: each CTA computes tz (a multiple of 4) columns, 2 kT - 16 at most.
+void pair_split(const Dims &d, int kT, int *nstrips, int *tz) {
+  const int w = 2 * kT - 16;
+  *nstrips = (d.nzp + w - 1) / w;
+  const int t = (d.nzp + *nstrips - 1) / *nstrips;
+  *tz = (t + 3) / 4 * 4;
+}
+// Rows per CTA: a CTA's time grows with xr + 12 (16 halo steps, 8 of them loads only), and the
+// launch takes as many waves as its CTAs fill; xr minimises waves x (xr + 12) over the batch's
+// own window widths.
+int pair_xr(const ds2d_ctx *c, int nstrips, int per_sm) {
+  if (c->opt_pair_xr > 0) return std::max(8, c->opt_pair_xr);
+  const long long slots = (long long)c->num_sms * std::max(1, per_sm);
+  long long best = -1;
+  int best_xr = 128;
+  for (int xr = 48; xr <= 256; xr++) {
+    long long ctas = 0;
+    for (int nx : c->h_nxp) ctas += (long long)nstrips * ((nx + xr - 1) / xr);
+    const long long cost = (ctas + slots - 1) / slots * (xr + 12);
+    if (best < 0 || cost <= best) {
+      best = cost;
+      best_xr = xr;
+    }
+  }
+  return best_xr;
+}
+
+// Reads and clears the error word of the pair kernels (after the stream has been synchronised).
+int check_pair_err(ds2d_ctx *c) {
+  if (!c->d_err) return DS2D_OK;
+  int h = 0;
+  CK(cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    return fail(c, DS2D_E_CUDA, "a pair kernel's ring wait gave up (error word %d)", h);
+  }
+  return DS2D_OK;
+}
+
 // Fused forward pass: one k_fwd_fused launch per step, ping-ponging fw <-> fw2.
 int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
   const Dims &d = c->d;
@@ -610,7 +687,14 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
     a.d = d; a.a = *cur; a.b = *nxt; a.p = c->par; a.shots = c->d_shots; a.wavelet = c->wavelet;
     a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
     if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
-    if (c->opt_ring && c->ring_ok) {
+    if (pair_on(c)) {
+      int pns, ptz;
+      pair_split(d, kPairFwdT, &pns, &ptz);
+      const int pxr = pair_xr(c, pns, c->occ_pair_fwd);
+      a.tz = ptz; a.xr = pxr; a.err = c->d_err;
+      dim3 pgrid(pns, (d.nxp + pxr - 1) / pxr, n);
+      LAUNCHS("fwd_pair", kBytesFused * CELLS(n), pair_fwd_fn(), pgrid, kPairFwdT, kPairFwdSmem, a);
+    } else if (c->opt_ring && c->ring_ok) {
       const size_t sm = sizeof(float) * c->opt_ring * fwd_ring_fields(!d.rbc) * cta;
       FwdFn kfn = fwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ, cta);
       LAUNCHS("fwd_fused", kBytesFused * CELLS(n), kfn, grid, cta, sm, a);
@@ -649,7 +733,7 @@ int run_forward_pass(ds2d_ctx *c, int n, bool record, bool strips) {
 int reduce_images(ds2d_ctx *c, int n, int nimg) {
   const Dims &d = c->d;
   dim3 grid((d.allnz + 255) / 256, d.allnx);
-  long long plane = (long long)c->B * d.wnx * d.wnz;
+  long long plane = (long long)c->B * d.wnx * d.ild;
   k_image_reduce<<<grid, 256, 0, c->stream>>>(d, c->img_slot, plane, nimg, n, c->d_shots, c->images,
                                               (long long)d.allnx * d.allnz);
   c->last_launches++;
@@ -742,7 +826,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr, (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -752,7 +836,7 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
   if ((rc = setup_batch(c, n, shot_base, false))) return rc;
   if ((rc = zero_wave(c, c->fw, n))) return rc;
   if ((rc = zero_wave(c, c->abk, n))) return rc;
-  size_t plane = (size_t)c->B * d.wnx * d.wnz;
+  size_t plane = (size_t)c->B * d.wnx * d.ild;
   CK(cudaMemsetAsync(c->img_slot, 0, 7 * plane * sizeof(float), c->stream));
   const bool strips = !d.rbc;
   if ((rc = run_forward_pass(c, n, false, strips))) return rc;
@@ -779,7 +863,16 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
       a.shots = c->d_shots; a.rmap = c->d_rmap; a.res_vz = c->rec[0]; a.res_vx = c->rec[1];
       a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
       a.img = c->img_slot; a.img_plane = (long long)plane;
-      if (c->opt_ring && c->ring_ok) {
+      if (pair_on(c)) {
+        const int pc = pair_bwd_cta(c);
+        int pns, ptz;
+        pair_split(d, pc, &pns, &ptz);
+        const int pxr = pair_xr(c, pns, pc == 160 ? c->occ_pair_bwd160 : c->occ_pair_bwd256);
+        a.tz = ptz; a.xr = pxr; a.err = c->d_err;
+        dim3 pgrid(pns, (d.nxp + pxr - 1) / pxr, n);
+        LAUNCHS("bwd_pair", kBytesBwdFused * CELLS(n), pair_bwd_fn(pc), pgrid, pc,
+                pair_bwd_smem(pc), a);
+      } else if (c->opt_ring && c->ring_ok) {
         const size_t sm = sizeof(float) * c->opt_ring * bwd_ring_fields(!d.rbc) * cta;
         BwdFn kfn = bwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ, cta);
         LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, fgrid, cta, sm, a);
@@ -903,7 +996,7 @@ int elsrtm_backward_fused(ds2d_ctx *c, int n, bool strips) {
   const int xr = std::max(8, c->opt_xr);
   dim3 grid(nstrips, (d.nxp + xr - 1) / xr, n);
   dim3 bgrid = cell_grid(d, n), blk(kBX, kBY);
-  const long long plane = (long long)c->B * d.wnx * d.wnz;
+  const long long plane = (long long)c->B * d.wnx * d.ild;
   Wave *fc = &c->fw, *fn = &c->fw2, *ac = &c->abk, *an = &c->abk2, *bc = &c->b1, *bn = &c->b1_2;
   const size_t sm = sizeof(float) * 4 * bwd_ring_fields(!d.rbc) * kFB;
   const size_t sm2 = sizeof(float) * 4 * kBwdScatRingFields * kFB;
@@ -942,7 +1035,7 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
   size_t bytes = sizeof(float) * (size_t)d.slot * n;
   for (int i = 0; i < 3; i++) CK(cudaMemsetAsync(c->ov_s[i], 0, bytes, c->stream));
   for (int i = 0; i < 2; i++) CK(cudaMemsetAsync(c->ov_v[i], 0, bytes, c->stream));
-  size_t plane = (size_t)c->B * d.wnx * d.wnz;
+  size_t plane = (size_t)c->B * d.wnx * d.ild;
   CK(cudaMemsetAsync(c->img_slot, 0, 7 * plane * sizeof(float), c->stream));
   size_t nrec = (size_t)n * d.max_ntr * d.nt;
   for (int i = 2; i < 6; i++) CK(cudaMemsetAsync(c->rec[i], 0, nrec * sizeof(float), c->stream));
@@ -1067,7 +1160,7 @@ int ensure_acoustic(ds2d_ctx *c) {
     for (float *&p : c->ac2)
       if (!p && (rc = alloc_slots(c, &p))) return rc;
   if (!c->img_slot) {  // per-shot gradient planes (same 7-plane size as the RTM images)
-    size_t n = (size_t)7 * c->B * c->d.wnx * c->d.wnz;
+    size_t n = (size_t)7 * c->B * c->d.wnx * c->d.ild;
     if ((rc = alloc(c, (void **)&c->img_slot, n * sizeof(float)))) return rc;
   }
   if (!c->dot_part) {
@@ -1163,7 +1256,7 @@ int ac_LT_batch(ds2d_ctx *c, int n) {
   size_t bytes = sizeof(float) * (size_t)d.slot * n;
   for (int i = 0; i < 9; i++)
     if (i < 3 || i >= 6) CK(cudaMemsetAsync(c->ac[i], 0, bytes, c->stream));
-  size_t plane = (size_t)c->B * d.wnx * d.wnz;
+  size_t plane = (size_t)c->B * d.wnx * d.ild;
   CK(cudaMemsetAsync(c->img_slot, 0, plane * sizeof(float), c->stream));
   dim3 grid = cell_grid(d, n), blk(32, 8);
   const bool fused = c->opt_fused && c->ring_ok && c->ac2[0];
@@ -1331,6 +1424,7 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
   d.nop = nop;
   d.wnx = g.nx;
   d.wnz = g.allnz;
+  d.ild = d.ld;
   d.nt = g.nt;
   d.allnx = g.allnx;
   d.allnz = g.allnz;
@@ -1348,7 +1442,7 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
   // The ring-fed kernels index cells and image pixels with 32-bit offsets; batches whose arrays
   // exceed 2^31 elements fall back to the 64-bit fused kernels.
   c->ring_ok = (long long)c->B * d.slot < (1LL << 31) &&
-               (long long)c->B * d.wnx * d.wnz < (1LL << 31);
+               (long long)c->B * d.wnx * d.ild < (1LL << 31);
   {
     // Ring-fed kernels may use more than the default 48 KB of dynamic shared memory.
     cudaError_t e = cudaSuccess;
@@ -1376,6 +1470,25 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
           }
         }
     }
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(pair_fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kPairFwdSmem);
+    for (int pc : {160, 256})
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(pair_bwd_fn(pc), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_bwd_smem(pc));
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair_fwd, pair_fwd_fn(), kPairFwdT,
+                                                        kPairFwdSmem);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair_bwd256, pair_bwd_fn(256), 256,
+                                                        pair_bwd_smem(256));
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair_bwd160, pair_bwd_fn(160), 160,
+                                                        pair_bwd_smem(160));
+    int dev = 0;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
     for (bool rbc : {false, true})
       if (e == cudaSuccess)
         e = cudaFuncSetAttribute(bwd_scat_fn(rbc), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1401,11 +1514,13 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
   if ((rc = alloc(c, (void **)&c->vp_all, nall * 4)) || (rc = alloc(c, (void **)&c->vs_all, nall * 4)) ||
       (rc = alloc(c, (void **)&c->pp_all, nall * 4)) || (rc = alloc(c, (void **)&c->ps_all, nall * 4)) ||
       (rc = alloc(c, (void **)&c->images, 7 * nall * 4)) ||
-      (rc = alloc(c, (void **)&c->wavelet, (size_t)g.nt * 4))) {
+      (rc = alloc(c, (void **)&c->wavelet, (size_t)g.nt * 4)) ||
+      (rc = alloc(c, (void **)&c->d_err, sizeof(int)))) {
     ds2d_destroy(c);
     return rc;
   }
   if (cudaMemsetAsync(c->images, 0, 7 * nall * 4, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream) != cudaSuccess ||
       cudaStreamSynchronize(c->stream) != cudaSuccess) {
     ds2d_destroy(c);
     return DS2D_E_CUDA;
@@ -1492,7 +1607,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr, (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -1508,7 +1623,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     for (int s = 0; s < m; s++) tb += shots[f + s].ntr;
     c->last_updates += c->batch_cells * c->d.nt;
   }
-  return DS2D_OK;
+  return check_pair_err(c);
 }
 
 static int rtm_common(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *az,
@@ -1529,7 +1644,7 @@ static int rtm_common(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *a
     c->last_updates += 3.0 * c->batch_cells * c->d.nt;
   }
   CK(cudaStreamSynchronize(c->stream));
-  return DS2D_OK;
+  return check_pair_err(c);
 }
 
 int ds2d_rtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *adj_vz, const float *adj_vx) {
@@ -1917,6 +2032,17 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     if (value != 0 && value != kFB && value != kWideCta)
       return fail(c, DS2D_E_ARG, "cta must be 0 (automatic), 128 or 192");
     c->opt_cta = (int)value;
+  } else if (k == "pair") {
+    if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "pair must be 0 or 1");
+    c->opt_pair = (int)value;
+  } else if (k == "pair_cta") {
+    if (value != 0 && value != 160 && value != 256)
+      return fail(c, DS2D_E_ARG, "pair_cta must be 0 (automatic), 160 or 256");
+    c->opt_pair_cta = (int)value;
+  } else if (k == "pair_xr") {
+    if (value != 0 && (value < 8 || value > 4096))
+      return fail(c, DS2D_E_ARG, "pair_xr must be 0 (automatic) or in [8, 4096]");
+    c->opt_pair_xr = (int)value;
   } else if (k == "xr") {
     if (value < 8 || value > 4096) return fail(c, DS2D_E_ARG, "xr must be in [8, 4096]");
     c->opt_xr = (int)value;
@@ -2027,11 +2153,32 @@ __global__ void __launch_bounds__(kDotThreads) k_dot_chunk(const float *a, const
 }
 
 std::mutex g_na_mu;
-double *g_na_ptr[kNaMaxDevices] = {};
+struct NaSlot {
+  CUcontext ctx;  // context the address below belongs to
+  double *ptr;
+};
+NaSlot g_na_slot[kNaMaxDevices] = {};
 
-// Device address of g_na_scratch on the current device, looked up once per device (with that
-// device current, as cudaGetSymbolAddress requires) and cached.  The first call on a device
-// may load this module there, so it should come before any stream capture on that device.
+// cuCtxGetCurrent through the runtime's driver entry point (no link against libcuda).
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+CtxGetCurrentFn na_ctx_fn() {
+  static CtxGetCurrentFn fn = []() -> CtxGetCurrentFn {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
+
+// Device address of g_na_scratch in the current context.  It is looked up (with the device
+// current, as cudaGetSymbolAddress requires) on the first call in a context and cached per
+// device together with the context it belongs to; a call from another context of the same
+// device (a non-primary context, or the primary context re-created after cudaDeviceReset under
+// a new handle) looks it up again.  The first call in a context may load this module there, so
+// it should come before any stream capture on that device.
 int na_scratch(double **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -2044,18 +2191,25 @@ int na_scratch(double **out) {
                    " is beyond the table of " + std::to_string(kNaMaxDevices) + " devices";
     return DS2D_E_ARG;
   }
+  // cudaFree(0) makes the runtime bind (or create) the device's primary context when the
+  // calling thread has none yet; it allocates nothing.
+  CUcontext ctx = nullptr;
+  CtxGetCurrentFn get = na_ctx_fn();
+  if (get && get(&ctx) == CUDA_SUCCESS && !ctx && cudaFree(nullptr) == cudaSuccess) get(&ctx);
   std::lock_guard<std::mutex> lock(g_na_mu);
-  if (!g_na_ptr[dev]) {
+  NaSlot &slot = g_na_slot[dev];
+  if (!slot.ptr || slot.ctx != ctx || !ctx) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_na_scratch);
     if (e != cudaSuccess || !p) {
       g_create_err = std::string("ds2d_dot_f64_noalloc: cudaGetSymbolAddress: ") +
                      cudaGetErrorString(e);
+      slot = NaSlot{};
       return DS2D_E_CUDA;
     }
-    g_na_ptr[dev] = static_cast<double *>(p);
+    slot = NaSlot{ctx, static_cast<double *>(p)};
   }
-  *out = g_na_ptr[dev];
+  *out = slot.ptr;
   return DS2D_OK;
 }
 
@@ -2090,4 +2244,130 @@ extern "C" int ds2d_dot_f64_noalloc(const float *a, const float *b, long long n,
     return DS2D_E_CUDA;
   }
   return DS2D_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gradient band-pass filter (reference bandpass_filter, FD2DGPU.cu:4125-4182; see
+// ds2d_filter.cuh for the arithmetic it reproduces).
+namespace {
+
+struct BandpassScratch {
+  double2 *wz = nullptr, *wzi = nullptr, *wx = nullptr, *wxi = nullptr, *t1 = nullptr,
+          *t2 = nullptr;
+  float *filt = nullptr;
+  std::vector<void *> all;
+  ~BandpassScratch() {
+    for (void *p : all) cudaFree(p);
+  }
+  cudaError_t get(void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) all.push_back(*p);
+    return e;
+  }
+};
+
+int bandpass_images(int nx, int nz, int z1, int z2, float *const imgs[2], cudaStream_t st) {
+  auto err = [&](const char *what, cudaError_t e) {
+    g_create_err = std::string("ds2d_bandpass_filter: ") + what + ": " + cudaGetErrorString(e);
+    return DS2D_E_CUDA;
+  };
+  BandpassScratch sc;
+  const size_t ncell = (size_t)nx * nz;
+  cudaError_t e = cudaSuccess;
+  if ((e = sc.get((void **)&sc.wz, sizeof(double2) * nz * nz)) ||
+      (e = sc.get((void **)&sc.wzi, sizeof(double2) * nz * nz)) ||
+      (e = sc.get((void **)&sc.wx, sizeof(double2) * nx * nx)) ||
+      (e = sc.get((void **)&sc.wxi, sizeof(double2) * nx * nx)) ||
+      (e = sc.get((void **)&sc.t1, sizeof(double2) * ncell)) ||
+      (e = sc.get((void **)&sc.t2, sizeof(double2) * ncell)) ||
+      (e = sc.get((void **)&sc.filt, sizeof(float) * ncell)))
+    return err("cudaMalloc", e);
+  // filter in natural frequency order: k'(j) = k(S(j))
+  const std::vector<float> k = gaussian_bandpass(nx, nz, z1, z2);
+  std::vector<float> kp(ncell);
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) kp[(size_t)ix * nz + iz] = k[quadrant_swap(nx, nz, ix, iz)];
+  const std::vector<double2> wz = dft_matrix(nz, -1), wzi = dft_matrix(nz, 1);
+  const std::vector<double2> wx = dft_matrix(nx, -1), wxi = dft_matrix(nx, 1);
+  if ((e = cudaMemcpyAsync(sc.wz, wz.data(), sizeof(double2) * wz.size(), cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(sc.wzi, wzi.data(), sizeof(double2) * wzi.size(), cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(sc.wx, wx.data(), sizeof(double2) * wx.size(), cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(sc.wxi, wxi.data(), sizeof(double2) * wxi.size(), cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(sc.filt, kp.data(), sizeof(float) * ncell, cudaMemcpyHostToDevice, st)))
+    return err("cudaMemcpyAsync", e);
+  auto gemm = [&](DftArgs a) {
+    dim3 grid((a.N + kDftTile - 1) / kDftTile, (a.M + kDftTile - 1) / kDftTile);
+    k_dft_gemm<<<grid, kDftTile * kDftTile, 0, st>>>(a);
+  };
+  for (int i = 0; i < 2; i++) {
+    if (!imgs[i]) continue;
+    DftArgs a{};
+    // forward along z: t1[x][kz] = sum_z f[x][z] Wz[z][kz]
+    a = DftArgs{};
+    a.M = nx; a.N = nz; a.K = nz; a.a_real = imgs[i]; a.lda = nz; a.b = sc.wz; a.ldb = nz;
+    a.c = sc.t1; a.ldc = nz;
+    gemm(a);
+    // forward along x, times (k', k'): t2[kx][kz] = (k', k') * sum_x Wx[kx][x] t1[x][kz]
+    a = DftArgs{};
+    a.M = nx; a.N = nz; a.K = nx; a.a = sc.wx; a.lda = nx; a.b = sc.t1; a.ldb = nz;
+    a.c = sc.t2; a.ldc = nz; a.filt = sc.filt; a.ldf = nz;
+    gemm(a);
+    // inverse along x: t1[x][kz] = sum_kx Wx*[x][kx] t2[kx][kz]
+    a = DftArgs{};
+    a.M = nx; a.N = nz; a.K = nx; a.a = sc.wxi; a.lda = nx; a.b = sc.t2; a.ldb = nz;
+    a.c = sc.t1; a.ldc = nz;
+    gemm(a);
+    // inverse along z, real part / (nx nz) into the image
+    a = DftArgs{};
+    a.M = nx; a.N = nz; a.K = nz; a.a = sc.t1; a.lda = nz; a.b = sc.wzi; a.ldb = nz;
+    a.out_real = imgs[i]; a.ldo = nz; a.scale = (double)(nx * nz);
+    gemm(a);
+  }
+  if ((e = cudaGetLastError()) || (e = cudaStreamSynchronize(st))) return err("launch", e);
+  return DS2D_OK;
+}
+
+int bandpass_check(int nx, int nz, int z1, int z2) {
+  if (nx < 2 || nz < 2 || z2 <= 0 || z1 < 0) {
+    g_create_err = "ds2d_bandpass_filter: need nx, nz >= 2, high cut-off z2 > 0, low cut-off z1 >= 0";
+    return DS2D_E_ARG;
+  }
+  return DS2D_OK;
+}
+
+}  // namespace
+
+extern "C" int ds2d_bandpass_filter_device(int nx, int nz, int x1, int x2, int z1, int z2,
+                                           float *grad_pp, float *grad_ps, void *stream) {
+  (void)x1;
+  (void)x2;  // accepted for the reference's signature; its live filter uses z1, z2 only
+  int rc = bandpass_check(nx, nz, z1, z2);
+  if (rc) return rc;
+  float *imgs[2] = {grad_pp, grad_ps};
+  return bandpass_images(nx, nz, z1, z2, imgs, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ds2d_bandpass_filter(int nx, int nz, int x1, int x2, int z1, int z2,
+                                    float *grad_pp, float *grad_ps) {
+  int rc = bandpass_check(nx, nz, z1, z2);
+  if (rc) return rc;
+  const size_t bytes = sizeof(float) * (size_t)nx * nz;
+  float *d[2] = {nullptr, nullptr};
+  float *h[2] = {grad_pp, grad_ps};
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && e == cudaSuccess; i++)
+    if (h[i] && (e = cudaMalloc(&d[i], bytes)) == cudaSuccess)
+      e = cudaMemcpy(d[i], h[i], bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = bandpass_images(nx, nz, z1, z2, d, nullptr);
+    for (int i = 0; i < 2 && rc == DS2D_OK && e == cudaSuccess; i++)
+      if (h[i]) e = cudaMemcpy(h[i], d[i], bytes, cudaMemcpyDeviceToHost);
+  }
+  for (float *p : d)
+    if (p) cudaFree(p);
+  if (e != cudaSuccess) {
+    g_create_err = std::string("ds2d_bandpass_filter: ") + cudaGetErrorString(e);
+    return DS2D_E_CUDA;
+  }
+  return rc;
 }

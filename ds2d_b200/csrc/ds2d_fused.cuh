@@ -53,6 +53,7 @@ struct FwdFusedArgs {
   // new velocities for the next set.
   const float *ovi_txx, *ovi_tzz, *ovi_txz;
   float *ovo_txx, *ovo_tzz, *ovo_txz;
+  int *err;  // device error word of the pair kernels' bounded waits (null: none)
 };
 
 template <int N>
@@ -521,8 +522,9 @@ struct BwdFusedArgs {
   int strips_on;
   int it;
   int tz, xr;
-  float *img;        // [3][slot][wnx][wnz]: pp, ps, illumination
+  float *img;        // [3][slot][wnx][ild]: pp, ps, illumination
   long long img_plane;
+  int *err;          // device error word of the pair kernels' bounded waits (null: none)
 };
 
 template <bool kPML>
@@ -667,7 +669,7 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
       Pz = l2m * atzz;
       Lx = lam * atxx;
       if (own && x_int && z_int) {
-        const long long o = ((long long)s * d.wnx_max + (r1 - pml)) * d.wnz + (z - pml);
+        const long long o = ((long long)s * d.wnx_max + (r1 - pml)) * d.ild + z;
         const float kpp = __ldg(a.p.kpp + k), kps = __ldg(a.p.kps + k);
         const float lamda_grad = (gx_vx + gz_vz) * (atxx + atzz);
         const float miu_grad = -2.0f * (gx_vx * atzz + gz_vz * atxx) + (gz_vx + gx_vz) * atxz;
@@ -710,7 +712,7 @@ __global__ void __launch_bounds__(kFB) k_bwd_fused(BwdFusedArgs a) {
         const float vz = ovz + (-cbx * fx + -cbz * ez);
         a.rb.vx[k] = vx;
         a.rb.vz[k] = vz;
-        const long long o = ((long long)s * d.wnx_max + (r2 - pml)) * d.wnz + (z - pml);
+        const long long o = ((long long)s * d.wnx_max + (r2 - pml)) * d.ild + z;
         a.img[2 * a.img_plane + o] += vx * vx + vz * vz;
       }
       if (r2 >= d.nop && r2 < d.nxp - d.nop && z_upd) {
@@ -882,7 +884,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
         if (f == 14) cp_async4(dst, a.p.dampz + o4);
       } else if (f == 14 || f == 15) {
         if (int4)
-          cp_async4(dst, (f == 14 ? img_pp : img_ps) + ((img_row + r4 - pml) * d.wnz + (z - pml)));
+          cp_async4(dst, (f == 14 ? img_pp : img_ps) + ((img_row + r4 - pml) * d.ild + z));
         else
           *dst = 0.f;
       } else if (in4) {
@@ -901,7 +903,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
       cp_async4(&R(q, 21), a.aa.vz_x + o8);
       cp_async4(&R(q, 22), a.aa.vz_z + o8);
     } else if (int8) {
-      cp_async4(&R(q, 17), img_il + ((img_row + r8 - pml) * d.wnz + (z - pml)));
+      cp_async4(&R(q, 17), img_il + ((img_row + r8 - pml) * d.ild + z));
       if (own8) {
         cp_async4(&R(q, 23), a.ra.vx + o8);
         cp_async4(&R(q, 24), a.ra.vz + o8);
@@ -1056,7 +1058,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
       M = mu * atxz;
       PzLx = l2m * atzz + lam * atxx;
       if (own && x_int && z_int) {
-        const int o = (img_row + (r1 - pml)) * d.wnz + (z - pml);
+        const int o = (img_row + (r1 - pml)) * d.ild + z;
         const float kpp = R(r, 12), kps = R(r, 13);
         const float lamda_grad = (gx_vx + gz_vz) * (atxx + atzz);
         const float miu_grad = -2.0f * (gx_vx * atzz + gz_vz * atxx) + (gz_vx + gx_vz) * atxz;
@@ -1096,7 +1098,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
         const float vz = ovz + (-cbx * fx + -cbz * ez);
         a.rb.vx[k] = vx;
         a.rb.vz[k] = vz;
-        const int o = (img_row + (r2 - pml)) * d.wnz + (z - pml);
+        const int o = (img_row + (r2 - pml)) * d.ild + z;
         img_il[o] = R(r, 17) + (vx * vx + vz * vz);
       }
       if (r2 >= d.nop && r2 < d.nxp - d.nop && z_upd) {
@@ -1235,7 +1237,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_scat_ring(BwdScatArgs a) {
       R(q, 2) = R(q, 3) = R(q, 4) = R(q, 5) = R(q, 6) = 0.f;
     }
     if (int4) {
-      const int io = (img_row + r4 - pml) * d.wnz + (z - pml);
+      const int io = (img_row + r4 - pml) * d.ild + z;
       cp_async4(&R(q, 7), a.p.kpp + o4);
       cp_async4(&R(q, 8), a.p.kps + o4);
       cp_async4(&R(q, 9), img_b + io);
@@ -1310,7 +1312,7 @@ __global__ void __launch_bounds__(kFB, kMinB) k_bwd_scat_ring(BwdScatArgs a) {
           const float atxx = R(r, 11), atzz = R(r, 12), atxz = R(r, 13);
           const float lamda_grad = (gx_vx + gz_vz) * (atxx + atzz);
           const float miu_grad = -2.0f * (gx_vx * atzz + gz_vz * atxx) + (gz_vx + gx_vz) * atxz;
-          const int o = (img_row + (r1 - pml)) * d.wnz + (z - pml);
+          const int o = (img_row + (r1 - pml)) * d.ild + z;
           img_b[o] = R(r, 9) + R(r, 7) * lamda_grad;
           img_bs[o] = R(r, 10) + R(r, 8) * miu_grad;
         }
@@ -1567,7 +1569,7 @@ __global__ void __launch_bounds__(kFB, 4) k_ac_rev_ring(AcRevArgs a) {
       cp_async4(&R(q, 8), a.s + o8);
       cp_async4(&R(q, 9), a.lam + o8);
       if (r8 >= pml && r8 < d.nxp - pml && z_int)
-        cp_async4(&R(q, 10), a.grad + ((sl * d.wnx_max + (r8 - pml)) * d.wnz + (z - pml)));
+        cp_async4(&R(q, 10), a.grad + ((sl * d.wnx_max + (r8 - pml)) * d.ild + z));
     } else {
       R(q, 7) = R(q, 8) = R(q, 9) = 0.f;
     }
@@ -1662,7 +1664,7 @@ __global__ void __launch_bounds__(kFB, 4) k_ac_rev_ring(AcRevArgs a) {
         if (own) {
           a.ys_n[k] = R(r, 7) + gs;
           if (rB >= pml && rB < d.nxp - pml && z_int) {
-            const int o = (sl * d.wnx_max + (rB - pml)) * d.wnz + (z - pml);
+            const int o = (sl * d.wnx_max + (rB - pml)) * d.ild + z;
             a.grad[o] = R(r, 10) + -2.0f * lam * (sx * rdx + sz * rdz) * gs;
           }
         }

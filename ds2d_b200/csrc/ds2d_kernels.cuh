@@ -32,6 +32,8 @@ struct Dims {
   int nxp, nzp, ld;  // padded window, leading dimension
   int pml, nop;
   int wnx, wnz;      // interior window (reference nx, nz)
+  int ild;           // row stride of the per-slot window images [slot][wnx][ild]; window
+                     // column iz - pml sits at iz, so rows align like the wavefield rows
   int nt;
   int allnx, allnz;
   long long slot;    // floats per slot of one array (nxp_max * ld)

@@ -1,0 +1,720 @@
+// Pair-blocked, bulk-copy-fed ring kernels of the random-boundary elastic RTM step for sm_100a.
+//
+// Same x-march as the ring kernels of ds2d_fused.cuh (a CTA owns a z-strip, walks xr rows along
+// x, stage 1 runs 4 rows behind the newest loaded row and stage 2 8 rows behind, both half steps
+// of a time step in one pass), with three changes that cut the instructions per cell:
+//
+//  * Two cells per thread.  Thread t owns the adjacent columns z0 = zs - 8 + 2t and z0 + 1 and
+//    moves them as float2.  An 8-tap z-derivative of both cells needs the 10 columns z0-4..z0+5:
+//    five 8-byte shared loads (the thread's own pair and two pairs either side) instead of the
+//    sixteen 4-byte loads two one-column threads issue, and every per-row cost (loop, indexes,
+//    predicates, barrier) is paid once per two cells.
+//  * Rows arrive by bulk copy.  Each ring slot holds, for one row step, every row segment the
+//    step consumes (the newest stencil rows, the z-tap rows of stage 1 and the own-cell operands
+//    of both stages).  One thread issues one cp.async.bulk per field row (global -> shared,
+//    completion counted on the slot's mbarrier) kD - 1 steps ahead; the other threads only wait
+//    on the barrier's phase.  Stage-1 z-taps are read straight from the ring, so a step has a
+//    single CTA barrier (before the stage-2 z-taps, whose rows are computed in registers).
+//  * Injections as corrections.  The explosive source (forward) and the receiver residual
+//    (adjoint) act on the stencil values only (the reference adds them to the summed arrays,
+//    which its split update recomputes, FD2DGPU.cu:2039-2049, :3306-3322).  The owner of the
+//    injected column adds the value to its x-window entry; the z-derivatives of the columns
+//    within 4 of it add c_i * value for the taps that read it.  The own-cell operands come from
+//    the ring, i.e. from memory, without the injection.
+//
+// Scope: random boundary (no PML cells, no strips), RTM forward (optional receiver recording)
+// and backward steps.  The PML / strip / Born variants stay on the one-column ring kernels.
+#pragma once
+#include "ds2d_fused.cuh"
+
+namespace ds2d {
+
+// ---- bulk-copy ring primitives (PTX ISA 8.x, sm_90 and later) ------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// One arrival that also raises the transaction count the phase waits for by `bytes`.
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Global -> shared bulk copy (no multicast); `bytes` and both addresses multiples of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Polls of one phase before a wait gives up (each try_wait may itself suspend for a while):
+// far beyond any copy's latency, short of a hang.  A kernel that gives up raises the error word
+// (code kErrRingWait) and leaves its march; the host turns the word into an error.
+constexpr int kRingWaitPolls = 1 << 22;
+constexpr int kErrRingWait = 1;
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  for (int i = 0; i < kRingWaitPolls; i++)
+    if (mbar_test(bar, parity)) return true;
+  return false;
+}
+
+// Floats per ring row of a kT-thread CTA: two columns per thread plus two pairs of padding on
+// each side, so the z-taps of the edge threads stay inside the row.
+__host__ __device__ constexpr int pair_row(int kT) { return 2 * kT + 8; }
+
+// c_k of the 8th-order staggered stencil for k = 1..4, 0 otherwise (injection corrections).
+__device__ __forceinline__ float coef_or0(int k) {
+  return k == 1 ? kC1 : k == 2 ? kC2 : k == 3 ? kC3 : k == 4 ? kC4 : 0.0f;
+}
+
+// The ten columns z0-4 .. z0+5 around a thread's pair, v[k + 4] = column z0 + k, from a ring row
+// (float2 index i of the thread's own pair).
+struct Z10 {
+  float v[10];
+};
+__device__ __forceinline__ Z10 z10(const float2 *row, int i) {
+  const float2 a = row[i - 2], b = row[i - 1], c = row[i], e = row[i + 1], f = row[i + 2];
+  return Z10{{a.x, a.y, b.x, b.y, c.x, c.y, e.x, e.y, f.x, f.y}};
+}
+// Dz+ f = sum c_i (f[z+i] - f[z-i+1]) and Dz- f = sum c_i (f[z+i-1] - f[z-i]) at column z0 + e.
+template <int e>
+__device__ __forceinline__ float dzp(const Z10 &z) {
+  return stencil4([&](int i) { return z.v[4 + e + i] - z.v[5 + e - i]; });
+}
+template <int e>
+__device__ __forceinline__ float dzm(const Z10 &z) {
+  return stencil4([&](int i) { return z.v[3 + e + i] - z.v[4 + e - i]; });
+}
+
+// x-windows of float2 pairs: w[j] = row (newest - (N-1) + j).  Dx taps at the row 4 below the
+// window's top, in the index pattern both staggered forms share here: sum c_i (w[3+i] - w[4-i]).
+template <int N>
+__device__ __forceinline__ void push2(float2 (&w)[N], float2 v) {
+#pragma unroll
+  for (int i = 0; i < N - 1; i++) w[i] = w[i + 1];
+  w[N - 1] = v;
+}
+template <int N>
+__device__ __forceinline__ float dxw_x(const float2 (&w)[N]) {
+  return stencil4([&](int i) { return w[3 + i].x - w[4 - i].x; });
+}
+template <int N>
+__device__ __forceinline__ float dxw_y(const float2 (&w)[N]) {
+  return stencil4([&](int i) { return w[3 + i].y - w[4 - i].y; });
+}
+
+// Per-step ring bookkeeping shared by the pair kernels: slot / phase of the step being consumed
+// and of the step being refilled (kD - 1 ahead).
+template <int kD>
+struct RingCursor {
+  int slot = 0;
+  unsigned phase = 0;
+  __device__ __forceinline__ void advance() {
+    if (++slot == kD) {
+      slot = 0;
+      phase ^= 1u;
+    }
+  }
+};
+
+// End of a pair kernel's march.  No bulk copy may still be landing in shared memory when the CTA
+// exits, so every thread waits (bounded) for the phases still in flight: after a normal march,
+// the kD - 1 slots issued beyond its last step; after an aborted one (some wait gave up), both
+// phases of every slot.  A thread whose own wait gave up raises the error word.
+template <int kD>
+__device__ __forceinline__ void pair_exit(unsigned long long *bars, RingCursor<kD> cur,
+                                          bool aborted, bool ok, int *err) {
+  if (!aborted) {
+    for (int j = 0; j < kD - 1; j++) {
+      mbar_wait(&bars[cur.slot], cur.phase);
+      cur.advance();
+    }
+    return;
+  }
+  if (!ok && err) atomicExch(err, kErrRingWait);
+  for (int k = 0; k < kD; k++) {
+    mbar_wait(&bars[k], 0);
+    mbar_wait(&bars[k], 1);
+  }
+}
+
+// Copies of one ring slot: field f reads row (q - lag[f]) of an array whose rows are ld floats
+// apart (wavefields, parameters and the per-slot images alike), if that row lies in
+// [lo[f], hi[f]).  The strip's columns [zs - 8, zs - 8 + 2 kT) map to ring floats 4 .. 2 kT + 4;
+// the copy is clipped to [0, ld) (the row's own allocation).
+template <int NF>
+struct SlotPlan {
+  const float *src[NF];  // slot-0 row-0 pointer of each field's array (image rows: see below)
+  int lag[NF], lo[NF], hi[NF];
+  int row0[NF];          // array row of grid row x is x + row0 (image rows: x - pml)
+  bool img[NF];          // per-slot image rows (slot offset ibase) instead of field rows (fbase)
+};
+
+template <int NF, int kT>
+__device__ __forceinline__ void issue_slot(const SlotPlan<NF> &pl, float *slot_base,
+                                           unsigned long long *bar, int q, long long fbase,
+                                           long long ibase, int ld, int zs) {
+  const int glo = max(0, zs - 8), ghi = min(ld, zs - 8 + 2 * kT);
+  const unsigned bytes = (unsigned)(ghi - glo) * 4u;
+  const int dst_off = glo - (zs - 8) + 4;
+  unsigned total = 0;
+#pragma unroll
+  for (int f = 0; f < NF; f++) {
+    const int row = q - pl.lag[f];
+    if (row >= pl.lo[f] && row < pl.hi[f]) total += bytes;
+  }
+  mbar_arrive_tx(bar, total);
+#pragma unroll
+  for (int f = 0; f < NF; f++) {
+    const int row = q - pl.lag[f];
+    if (row >= pl.lo[f] && row < pl.hi[f]) {
+      const long long base = pl.img[f] ? ibase : fbase;
+      bulk_g2s(slot_base + f * pair_row(kT) + dst_off,
+               pl.src[f] + base + (long long)(row + pl.row0[f]) * ld + glo, bytes, bar);
+    }
+  }
+}
+
+// Shared-memory bytes of a pair kernel: the ring, the stage-2 z-tap rows (double-buffered), the
+// slot barriers and the receiver staging.
+__host__ __device__ constexpr size_t pair_smem(int kT, int kD, int NF, int NZ2) {
+  return sizeof(float) * ((size_t)kD * NF + 2 * NZ2) * pair_row(kT) + 8 * 8 + 6 * 16 * 4;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Forward step (background modelling, RTM source side): velocities of row r-4 and stresses of
+// row r-8 at row step r; optional receiver recording.  Ring fields of step r:
+//   0 txx(r)  1 txz(r-1)        x-window inputs (Dx+ txx over rows r-7..r, Dx- txz over r-8..r-1)
+//   2 txz(r-4)  3 tzz(r-4)      stage-1 z-tap rows
+//   4 vx(r-4)  5 vz(r-4)  6 b(r-4)            stage-1 own cells
+//   7 txx(r-8)  8 tzz(r-8)  9 lam(r-8)  10 mu(r-8)   stage-2 own cells (txz(r-8) is w_txz[0])
+constexpr int kFwdPairFields = 11;
+constexpr int kFwdPairZ2 = 2;  // stage-2 z-tap rows: vx, vz of row r-8
+
+template <int kT, int kD>
+__global__ void __launch_bounds__(kT, 2) k_fwd_pair(FwdFusedArgs a) {
+  constexpr int NF = kFwdPairFields, ROW = pair_row(kT);
+  extern __shared__ __align__(16) float smem[];
+  float *ring = smem;                               // [kD][NF][ROW]
+  float *z2 = ring + (size_t)kD * NF * ROW;         // [2][kFwdPairZ2][ROW]
+  unsigned long long *bars = (unsigned long long *)(z2 + 2 * kFwdPairZ2 * ROW);
+  int *s_tr = (int *)(bars + 8);                    // receiver staging [16]
+  const int s = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int zs = blockIdx.x * a.tz;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  const int ld = d.ld, nop = d.nop;
+  const long long fbase = d.slot * s;
+  const int z0 = zs - 8 + 2 * t;
+  const int pi = t + 2;  // float2 index of the own pair in a ring row
+  // column predicates of the pair: stage-1 columns, stage-2 (owned) columns, update masks
+  const bool c1 = z0 >= zs - 4 && z0 < zs + a.tz + 4;
+  const bool c2 = z0 >= zs && z0 < zs + a.tz && z0 < d.nzp;
+  const bool u0 = z0 >= nop && z0 < d.nzp - nop, u1 = z0 + 1 >= nop && z0 + 1 < d.nzp - nop;
+  const ShotDev sh = a.shots[s];
+  const float sval = a.wavelet[a.it];
+  const int se = sh.isz - z0;  // source column relative to the pair (0 / 1: owned here)
+  const bool src_near = se >= -4 && se <= 5;
+  const bool rec_col = a.rec_on && (sh.igz - z0 == 0 || sh.igz - z0 == 1);
+  const int rec_e = sh.igz - z0;
+  const int *rmap = a.rmap + (long long)s * d.nxp_max;
+  const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+
+  SlotPlan<NF> pl;
+  {
+    const float *src[NF] = {a.a.txx, a.a.txz, a.a.txz, a.a.tzz, a.a.vx, a.a.vz,
+                            a.p.b,   a.a.txx, a.a.tzz, a.p.lam, a.p.mu};
+    const int lag[NF] = {0, 1, 4, 4, 4, 4, 4, 8, 8, 8, 8};
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      pl.src[f] = src[f];
+      pl.lag[f] = lag[f];
+      pl.lo[f] = 0;
+      pl.hi[f] = d.nxp;
+      pl.row0[f] = 0;
+      pl.img[f] = false;
+    }
+  }
+  if (t == 0) {
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int rs0 = x0 - 8;
+  if (t == 0)
+    for (int j = 0; j < kD - 1; j++)
+      issue_slot<NF, kT>(pl, ring + (size_t)j * NF * ROW, &bars[j], rs0 + j, fbase, 0, ld, zs);
+
+  float2 w_txx[8], w_txz[8], w_vx[9], w_vz[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) w_txx[i] = w_txz[i] = w_vz[i] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_vx[i] = make_float2(0.f, 0.f);
+
+  RingCursor<kD> cur;
+  bool ok = true, aborted = false;
+#pragma unroll 2
+  for (int r = rs0; r < x1 + 8; r++) {
+    // A wait that gives up skips the step's work; the barrier below is a vote, so every thread
+    // leaves the march together (none is left waiting at a barrier).
+    ok = mbar_wait(&bars[cur.slot], cur.phase);
+    const float *S = ring + (size_t)cur.slot * NF * ROW;
+    auto F2 = [&](int f) -> float2 { return reinterpret_cast<const float2 *>(S + f * ROW)[pi]; };
+    // trace index of velocity row r + 4 (recorded at step r + 8, one commit group per step)
+    if (rec_col && r + 4 < d.nxp && r + 4 >= 0)
+      cp_async4((float *)&s_tr[(r + 4) & 15], (const float *)(rmap + r + 4));
+    if (ok) {
+      float2 n_txx = F2(0);
+      if (r == sh.isx && (se == 0 || se == 1)) {  // FD2DGPU.cu:2039-2049 (transient)
+        if (se == 0) n_txx.x += sval; else n_txx.y += sval;
+      }
+      push2(w_txx, n_txx);
+      push2(w_txz, F2(1));
+    }
+    // ---- stage 1: velocities of row rv = r - 4 ------------------------------------------
+    const int rv = r - 4;
+    float2 vn = make_float2(0.f, 0.f), vzn = make_float2(0.f, 0.f);
+    if (ok && c1 && r >= x0 && rv >= nop && rv < d.nxp - nop) {
+      const Z10 zxz = z10(reinterpret_cast<const float2 *>(S + 2 * ROW), pi);
+      const Z10 zzz = z10(reinterpret_cast<const float2 *>(S + 3 * ROW), pi);
+      float ez0 = dzp<0>(zzz), ez1 = dzp<1>(zzz);
+      if (rv == sh.isx && src_near) {  // tzz of the source cell, read by the z-taps
+        ez0 += sval * (coef_or0(se) - coef_or0(1 - se));
+        ez1 += sval * (coef_or0(se - 1) - coef_or0(2 - se));
+      }
+      const float2 bb = F2(6), ovx = F2(4), ovz = F2(5);
+      const float ax0 = dxw_x(w_txx), ax1 = dxw_y(w_txx);
+      const float fx0 = dxw_x(w_txz), fx1 = dxw_y(w_txz);
+      const float bz0 = dzm<0>(zxz), bz1 = dzm<1>(zxz);
+      {
+        const float cbx = bb.x * dtdx, cbz = bb.x * dtdz;
+        if (u0) {
+          vn.x = ovx.x + (cbx * ax0 + cbz * bz0);
+          vzn.x = ovz.x + (cbx * fx0 + cbz * ez0);
+        }
+      }
+      {
+        const float cbx = bb.y * dtdx, cbz = bb.y * dtdz;
+        if (u1) {
+          vn.y = ovx.y + (cbx * ax1 + cbz * bz1);
+          vzn.y = ovz.y + (cbx * fx1 + cbz * ez1);
+        }
+      }
+      if (c2 && rv >= x0 && rv < x1) {
+        const long long k = fbase + (long long)rv * ld + z0;
+        *reinterpret_cast<float2 *>(a.b.vx + k) = vn;
+        *reinterpret_cast<float2 *>(a.b.vz + k) = vzn;
+        if (rec_col) {
+          const int tr = s_tr[rv & 15];
+          if (tr >= 0) {
+            const long long q = ((long long)s * d.max_ntr + tr) * d.nt + a.it;
+            a.rec_vz[q] = rec_e == 0 ? vzn.x : vzn.y;
+            a.rec_vx[q] = rec_e == 0 ? vn.x : vn.y;
+          }
+        }
+      }
+    }
+    push2(w_vx, vn);
+    push2(w_vz, vzn);
+    // ---- stage-2 z-tap rows (vx, vz of row r - 8), then the step's only barrier --------------
+    float *zb = z2 + (r & 1) * kFwdPairZ2 * ROW;
+    reinterpret_cast<float2 *>(zb)[pi] = w_vx[4];
+    reinterpret_cast<float2 *>(zb + ROW)[pi] = w_vz[3];
+    if (rec_col) cp_async_commit();
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+    // every thread is done with the previous slot: refill it kD - 1 steps ahead
+    if (t == 0) {
+      const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
+      issue_slot<NF, kT>(pl, ring + (size_t)ps * NF * ROW, &bars[ps], r + kD - 1, fbase, 0, ld,
+                         zs);
+    }
+    // ---- stage 2: stresses of row rs = r - 8 ------------------------------------------------
+    const int rs = r - 8;
+    if (c2 && rs >= x0 && rs < x1 && rs >= nop && rs < d.nxp - nop) {
+      const Z10 zvx = z10(reinterpret_cast<const float2 *>(zb), pi);
+      const Z10 zvz = z10(reinterpret_cast<const float2 *>(zb + ROW), pi);
+      const float2 lam = F2(9), mu = F2(10), oxx = F2(7), ozz = F2(8), oxz = w_txz[0];
+      float2 nxx = oxx, nzz = ozz, nxz = oxz;
+      {
+        const float sa = stencil4([&](int i) { return w_vx[3 + i].x - w_vx[4 - i].x; });
+        const float sf = stencil4([&](int i) { return w_vz[3 + i].x - w_vz[4 - i].x; });
+        const float sb = dzm<0>(zvz), sev = dzp<0>(zvx);
+        const float l2m = lam.x + 2.0f * mu.x;
+        if (u0) {
+          nxx.x = oxx.x + (l2m * dtdx * sa + lam.x * dtdz * sb);
+          nzz.x = ozz.x + (lam.x * dtdx * sa + l2m * dtdz * sb);
+          nxz.x = oxz.x + (dtdx * mu.x * sf + dtdz * mu.x * sev);
+        }
+      }
+      {
+        const float sa = stencil4([&](int i) { return w_vx[3 + i].y - w_vx[4 - i].y; });
+        const float sf = stencil4([&](int i) { return w_vz[3 + i].y - w_vz[4 - i].y; });
+        const float sb = dzm<1>(zvz), sev = dzp<1>(zvx);
+        const float l2m = lam.y + 2.0f * mu.y;
+        if (u1) {
+          nxx.y = oxx.y + (l2m * dtdx * sa + lam.y * dtdz * sb);
+          nzz.y = ozz.y + (lam.y * dtdx * sa + l2m * dtdz * sb);
+          nxz.y = oxz.y + (dtdx * mu.y * sf + dtdz * mu.y * sev);
+        }
+      }
+      const long long k = fbase + (long long)rs * ld + z0;
+      *reinterpret_cast<float2 *>(a.b.txx + k) = nxx;
+      *reinterpret_cast<float2 *>(a.b.tzz + k) = nzz;
+      *reinterpret_cast<float2 *>(a.b.txz + k) = nxz;
+    }
+    if (rec_col) cp_async_wait<7>();
+    cur.advance();
+  }
+  pair_exit<kD>(bars, cur, aborted, ok, a.err);
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Backward RTM step (random boundary): interior reconstruction of the source field (direction
+// -1, FD2DGPU.cu:903-1082 via :4769-4772), the adjoint step with the receiver residual
+// (FD2DGPU.cu:591-895, :3306-3322) and the imaging condition (doimage_gradient :3245,
+// doimage_illum :3235).  Stage 1 (stresses and images) at row r-4, stage 2 (velocities and
+// illumination) at row r-8.  Ring fields of step r:
+//   0 bvx(r-1)  1 bvz(r)  2 avx(r-1)  3 avz(r)              x-window inputs
+//   4 bvx(r-4)  5 bvz(r-4)  6 avx(r-4)  7 avz(r-4)          stage-1 z-tap rows
+//   8-10 btxx, btzz, btxz(r-4)  11-13 atxx, atzz, atxz(r-4) stage-1 own cells
+//   14 lam  15 mu  16 kpp  17 kps (r-4)  18 image pp  19 image ps (r-4)
+//   20 b(r-8)  21 bvz(r-8)  22 avx(r-8)  23 avz(r-8)  24 illumination(r-8)   stage-2 own cells
+// (bvx(r-8) is w_bvx[0]; the adjoint own velocities come from the ring because the windows carry
+// the residual.)
+constexpr int kBwdPairFields = 25;
+constexpr int kBwdPairZ2 = 4;  // stage-2 z-tap rows: btxz, btzz, M, PzLx of row r-8
+
+template <int kT, int kD, int kMinB>
+__global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
+  constexpr int NF = kBwdPairFields, ROW = pair_row(kT);
+  extern __shared__ __align__(16) float smem[];
+  float *ring = smem;
+  float *z2 = ring + (size_t)kD * NF * ROW;
+  unsigned long long *bars = (unsigned long long *)(z2 + 2 * kBwdPairZ2 * ROW);
+  int *s_tr = (int *)(bars + 8);
+  int *s_has = s_tr + 16;
+  float *s_rz = (float *)(s_has + 16), *s_rx = s_rz + 16;
+  const int s = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int zs = blockIdx.x * a.tz;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;
+  const int ld = d.ld, nop = d.nop, pml = d.pml;
+  const long long fbase = d.slot * s;
+  const long long ibase = (long long)s * d.wnx_max * d.ild;
+  const int z0 = zs - 8 + 2 * t;
+  const int pi = t + 2;
+  const bool c1 = z0 >= zs - 4 && z0 < zs + a.tz + 4;
+  const bool c2 = z0 >= zs && z0 < zs + a.tz && z0 < d.nzp;
+  const bool u0 = z0 >= nop && z0 < d.nzp - nop, u1 = z0 + 1 >= nop && z0 + 1 < d.nzp - nop;
+  const bool i0 = z0 >= pml && z0 < d.nzp - pml, i1 = z0 + 1 >= pml && z0 + 1 < d.nzp - pml;
+  const ShotDev sh = a.shots[s];
+  const int re = sh.igz - z0;  // receiver column relative to the pair
+  const bool rec_col = re == 0 || re == 1;
+  const bool rec_near = re >= -4 && re <= 5;
+  const float *res_z = a.res_vz + (long long)s * d.max_ntr * d.nt + a.it;
+  const float *res_x = a.res_vx + (long long)s * d.max_ntr * d.nt + a.it;
+  const int *rmap = a.rmap + (long long)s * d.nxp_max;
+  const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
+  float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
+
+  SlotPlan<NF> pl;
+  {
+    const float *src[NF] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.vx,  a.ra.vz,  a.aa.vx,
+                            a.aa.vz,  a.ra.txx, a.ra.tzz, a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz,
+                            a.p.lam,  a.p.mu,   a.p.kpp,  a.p.kps,  img_pp,   img_ps,   a.p.b,
+                            a.ra.vz,  a.aa.vx,  a.aa.vz,  img_il};
+    const int lag[NF] = {1, 0, 1, 0, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 8, 8, 8, 8, 8};
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const bool img = f == 18 || f == 19 || f == 24;
+      pl.src[f] = src[f];
+      pl.lag[f] = lag[f];
+      pl.lo[f] = img ? pml : 0;
+      pl.hi[f] = img ? d.nxp - pml : d.nxp;
+      pl.row0[f] = img ? -pml : 0;
+      pl.img[f] = img;
+    }
+  }
+  if (t == 0) {
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    mbar_fence_init();
+  }
+  if (rec_col) {  // residuals of rows x0-9 .. x0-1 and trace indexes of rows x0 .. x0+7 (direct;
+                  // the march fetches the rest ahead)
+    for (int q = x0 - 9; q < x0; q++) {
+      const int tr = (q >= 0 && q < d.nxp) ? rmap[q] : -1;
+      s_has[q & 15] = tr >= 0;
+      if (tr >= 0) {
+        s_rz[q & 15] = res_z[(long long)tr * d.nt];
+        s_rx[q & 15] = res_x[(long long)tr * d.nt];
+      }
+    }
+    for (int q = x0; q < x0 + 8; q++) s_tr[q & 15] = (q >= 0 && q < d.nxp) ? rmap[q] : -1;
+  }
+  __syncthreads();
+  const int rs0 = x0 - 8;
+  if (t == 0)
+    for (int j = 0; j < kD - 1; j++)
+      issue_slot<NF, kT>(pl, ring + (size_t)j * NF * ROW, &bars[j], rs0 + j, fbase, ibase, ld, zs);
+
+  float2 w_bvx[8], w_bvz[8], w_avx[8], w_avz[8];     // stage-1 x-windows
+  float2 w_btxx[8], w_btxz[9], w_PL[8], w_M[9];       // stage-2 x-windows
+  float2 w_btzz[5], w_PzLx[5];                        // stage-2 z-tap rows, 4 steps deep
+  const float2 zero2 = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+    w_bvx[i] = w_bvz[i] = w_avx[i] = w_avz[i] = w_btxx[i] = w_PL[i] = zero2;
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_btxz[i] = w_M[i] = zero2;
+#pragma unroll
+  for (int i = 0; i < 5; i++) w_btzz[i] = w_PzLx[i] = zero2;
+
+  RingCursor<kD> cur;
+  bool ok = true, aborted = false;
+#pragma unroll 1
+  for (int r = rs0; r < x1 + 8; r++) {
+    // A wait that gives up skips the step's work; the barrier below is a vote, so every thread
+    // leaves the march together (none is left waiting at a barrier).
+    ok = mbar_wait(&bars[cur.slot], cur.phase);
+    const float *S = ring + (size_t)cur.slot * NF * ROW;
+    auto F2 = [&](int f) -> float2 { return reinterpret_cast<const float2 *>(S + f * ROW)[pi]; };
+    if (rec_col) {
+      // residual of row r + 8 (its trace index landed 8 steps ago), trace index of row r + 16;
+      // one commit group per step, waited for 7 steps later
+      const int q8 = r + 8, q16 = r + 16;
+      const int tr8 = s_tr[q8 & 15];
+      s_has[q8 & 15] = tr8 >= 0;
+      if (tr8 >= 0) {
+        cp_async4(&s_rz[q8 & 15], res_z + (long long)tr8 * d.nt);
+        cp_async4(&s_rx[q8 & 15], res_x + (long long)tr8 * d.nt);
+      }
+      if (q16 < d.nxp)
+        cp_async4((float *)&s_tr[q16 & 15], (const float *)(rmap + q16));
+      else
+        s_tr[q16 & 15] = -1;
+      cp_async_commit();
+    }
+    if (ok) {
+      float2 n_bvx = F2(0), n_bvz = F2(1), n_avx = F2(2), n_avz = F2(3);
+      if (rec_col) {  // the residual enters the stencil values of the receiver column
+        const int qa = r - 1, qz = r;
+        if (qa >= 0 && qa < d.nxp && s_has[qa & 15]) {
+          if (re == 0) n_avx.x += s_rx[qa & 15]; else n_avx.y += s_rx[qa & 15];
+        }
+        if (qz >= 0 && qz < d.nxp && s_has[qz & 15]) {
+          if (re == 0) n_avz.x += s_rz[qz & 15]; else n_avz.y += s_rz[qz & 15];
+        }
+      }
+      push2(w_bvx, n_bvx);
+      push2(w_bvz, n_bvz);
+      push2(w_avx, n_avx);
+      push2(w_avz, n_avz);
+    }
+    // ---- stage 1: stresses of row r1 = r - 4, images ----------------------------------------
+    const int r1 = r - 4;
+    float2 btxx = zero2, btzz = zero2, btxz = zero2, PL = zero2, M = zero2, PzLx = zero2;
+    if (ok && c1 && r >= x0 && r1 >= 0 && r1 < d.nxp) {
+      const bool own = c2 && r1 >= x0 && r1 < x1;
+      const bool x_int = r1 >= pml && r1 < d.nxp - pml;
+      const float2 lam = F2(14), mu = F2(15);
+      btxx = F2(8);
+      btzz = F2(9);
+      btxz = F2(10);
+      float2 gxx = zero2, gzz = zero2, gsh = zero2;  // strains: Dx vx, Dz vz, Dz vx + Dx vz
+      if (x_int) {
+        const Z10 zbx = z10(reinterpret_cast<const float2 *>(S + 4 * ROW), pi);
+        const Z10 zbz = z10(reinterpret_cast<const float2 *>(S + 5 * ROW), pi);
+        const float sa0 = dxw_x(w_bvx), sa1 = dxw_y(w_bvx);
+        const float sf0 = dxw_x(w_bvz), sf1 = dxw_y(w_bvz);
+        const float sb0 = dzm<0>(zbz), sb1 = dzm<1>(zbz);
+        const float se0 = dzp<0>(zbx), se1 = dzp<1>(zbx);
+        const float dir = -1.0f;
+        if (i0) {
+          const float l2m = lam.x + 2.0f * mu.x;
+          btxx.x = btxx.x + (dir * l2m * dtdx * sa0 + dir * lam.x * dtdz * sb0);
+          btzz.x = btzz.x + (dir * lam.x * dtdx * sa0 + dir * l2m * dtdz * sb0);
+          btxz.x = btxz.x + (dir * mu.x * dtdx * sf0 + dir * mu.x * dtdz * se0);
+          gxx.x = sa0 * rdx;
+          gzz.x = sb0 * rdz;
+          gsh.x = se0 * rdz + sf0 * rdx;
+        }
+        if (i1) {
+          const float l2m = lam.y + 2.0f * mu.y;
+          btxx.y = btxx.y + (dir * l2m * dtdx * sa1 + dir * lam.y * dtdz * sb1);
+          btzz.y = btzz.y + (dir * lam.y * dtdx * sa1 + dir * l2m * dtdz * sb1);
+          btxz.y = btxz.y + (dir * mu.y * dtdx * sf1 + dir * mu.y * dtdz * se1);
+          gxx.y = sa1 * rdx;
+          gzz.y = sb1 * rdz;
+          gsh.y = se1 * rdz + sf1 * rdx;
+        }
+        if (own) {
+          const long long k = fbase + (long long)r1 * ld + z0;
+          *reinterpret_cast<float2 *>(a.rb.txx + k) = btxx;
+          *reinterpret_cast<float2 *>(a.rb.tzz + k) = btzz;
+          *reinterpret_cast<float2 *>(a.rb.txz + k) = btxz;
+        }
+      }
+      float2 atxx = zero2, atzz = zero2, atxz = zero2;
+      if (r1 >= nop && r1 < d.nxp - nop) {
+        const Z10 zax = z10(reinterpret_cast<const float2 *>(S + 6 * ROW), pi);
+        const Z10 zaz = z10(reinterpret_cast<const float2 *>(S + 7 * ROW), pi);
+        float sb0 = dzm<0>(zaz), sb1 = dzm<1>(zaz);
+        float se0 = dzp<0>(zax), se1 = dzp<1>(zax);
+        if (rec_near && s_has[r1 & 15]) {  // residual of the receiver cell in the z-taps
+          const float rz = s_rz[r1 & 15], rx = s_rx[r1 & 15];
+          sb0 += rz * (coef_or0(re + 1) - coef_or0(-re));
+          sb1 += rz * (coef_or0(re) - coef_or0(1 - re));
+          se0 += rx * (coef_or0(re) - coef_or0(1 - re));
+          se1 += rx * (coef_or0(re - 1) - coef_or0(2 - re));
+        }
+        const float sa0 = dxw_x(w_avx), sa1 = dxw_y(w_avx);
+        const float sf0 = dxw_x(w_avz), sf1 = dxw_y(w_avz);
+        const float2 oxx = F2(11), ozz = F2(12), oxz = F2(13);
+        if (u0) {
+          atxx.x = oxx.x + -dtdx * sa0;
+          atzz.x = ozz.x + -dtdz * sb0;
+          atxz.x = oxz.x + (-dtdx * sf0 + -dtdz * se0);
+        }
+        if (u1) {
+          atxx.y = oxx.y + -dtdx * sa1;
+          atzz.y = ozz.y + -dtdz * sb1;
+          atxz.y = oxz.y + (-dtdx * sf1 + -dtdz * se1);
+        }
+        if (own) {
+          const long long k = fbase + (long long)r1 * ld + z0;
+          *reinterpret_cast<float2 *>(a.ab.txx + k) = atxx;
+          *reinterpret_cast<float2 *>(a.ab.tzz + k) = atzz;
+          *reinterpret_cast<float2 *>(a.ab.txz + k) = atxz;
+        }
+      }
+      {
+        const float l2m0 = lam.x + 2.0f * mu.x, l2m1 = lam.y + 2.0f * mu.y;
+        PL = make_float2(l2m0 * atxx.x + lam.x * atzz.x, l2m1 * atxx.y + lam.y * atzz.y);
+        M = make_float2(mu.x * atxz.x, mu.y * atxz.y);
+        PzLx = make_float2(l2m0 * atzz.x + lam.x * atxx.x, l2m1 * atzz.y + lam.y * atxx.y);
+      }
+      if (own && x_int) {  // doimage_gradient, FD2DGPU.cu:3245-3263
+        const float2 kpp = F2(16), kps = F2(17), ipp = F2(18), ips = F2(19);
+        float2 npp = ipp, nps = ips;
+        if (i0) {
+          npp.x = ipp.x + kpp.x * ((gxx.x + gzz.x) * (atxx.x + atzz.x));
+          nps.x = ips.x + kps.x * (-2.0f * (gxx.x * atzz.x + gzz.x * atxx.x) + gsh.x * atxz.x);
+        }
+        if (i1) {
+          npp.y = ipp.y + kpp.y * ((gxx.y + gzz.y) * (atxx.y + atzz.y));
+          nps.y = ips.y + kps.y * (-2.0f * (gxx.y * atzz.y + gzz.y * atxx.y) + gsh.y * atxz.y);
+        }
+        const long long o = ibase + (long long)(r1 - pml) * d.ild + z0;
+        *reinterpret_cast<float2 *>(img_pp + o) = npp;
+        *reinterpret_cast<float2 *>(img_ps + o) = nps;
+      }
+    }
+    push2(w_btxx, btxx);
+    push2(w_btxz, btxz);
+    push2(w_btzz, btzz);
+    push2(w_PL, PL);
+    push2(w_M, M);
+    push2(w_PzLx, PzLx);
+    // ---- stage-2 z-tap rows of row r - 8, the step's barrier, the refill -----------------------
+    float *zb = z2 + (r & 1) * kBwdPairZ2 * ROW;
+    reinterpret_cast<float2 *>(zb)[pi] = w_btxz[4];
+    reinterpret_cast<float2 *>(zb + ROW)[pi] = w_btzz[0];
+    reinterpret_cast<float2 *>(zb + 2 * ROW)[pi] = w_M[4];
+    reinterpret_cast<float2 *>(zb + 3 * ROW)[pi] = w_PzLx[0];
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+    if (t == 0) {
+      const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
+      issue_slot<NF, kT>(pl, ring + (size_t)ps * NF * ROW, &bars[ps], r + kD - 1, fbase, ibase,
+                         ld, zs);
+    }
+    // ---- stage 2: velocities of row r2 = r - 8, illumination ---------------------------------
+    const int r2 = r - 8;
+    if (c2 && r2 >= x0 && r2 < x1) {
+      const long long k = fbase + (long long)r2 * ld + z0;
+      const bool x_int = r2 >= pml && r2 < d.nxp - pml;
+      const float2 bb = F2(20);
+      if (x_int) {
+        const Z10 ztxz = z10(reinterpret_cast<const float2 *>(zb), pi);
+        const Z10 ztzz = z10(reinterpret_cast<const float2 *>(zb + ROW), pi);
+        const float2 ovx = w_bvx[0], ovz = F2(21), il = F2(24);
+        float2 vx = ovx, vz = ovz, nil = il;
+        if (i0) {
+          const float cbx = bb.x * dtdx, cbz = bb.x * dtdz;
+          const float ax = dxw_x(w_btxx), fx = dxw_x(w_btxz);
+          const float bz = dzm<0>(ztxz), ez = dzp<0>(ztzz);
+          vx.x = ovx.x + (-cbx * ax + -cbz * bz);
+          vz.x = ovz.x + (-cbx * fx + -cbz * ez);
+          nil.x = il.x + (vx.x * vx.x + vz.x * vz.x);
+        }
+        if (i1) {
+          const float cbx = bb.y * dtdx, cbz = bb.y * dtdz;
+          const float ax = dxw_y(w_btxx), fx = dxw_y(w_btxz);
+          const float bz = dzm<1>(ztxz), ez = dzp<1>(ztzz);
+          vx.y = ovx.y + (-cbx * ax + -cbz * bz);
+          vz.y = ovz.y + (-cbx * fx + -cbz * ez);
+          nil.y = il.y + (vx.y * vx.y + vz.y * vz.y);
+        }
+        *reinterpret_cast<float2 *>(a.rb.vx + k) = vx;
+        *reinterpret_cast<float2 *>(a.rb.vz + k) = vz;
+        *reinterpret_cast<float2 *>(img_il + ibase + (long long)(r2 - pml) * d.ild + z0) = nil;
+      }
+      if (r2 >= nop && r2 < d.nxp - nop) {
+        const Z10 zm = z10(reinterpret_cast<const float2 *>(zb + 2 * ROW), pi);
+        const Z10 zp = z10(reinterpret_cast<const float2 *>(zb + 3 * ROW), pi);
+        float2 vx = zero2, vz = zero2;
+        const float2 ovx = F2(22), ovz = F2(23);
+        if (u0) {
+          const float cbx = bb.x * dtdx, cbz = bb.x * dtdz;
+          const float t_x = dxw_x(w_PL), s_xz = dxw_x(w_M);
+          const float t_xz = dzm<0>(zm), s_z = dzp<0>(zp);
+          vx.x = ovx.x + (-cbx * t_x + -cbz * t_xz);
+          vz.x = ovz.x + (-cbx * s_xz + -cbz * s_z);
+        }
+        if (u1) {
+          const float cbx = bb.y * dtdx, cbz = bb.y * dtdz;
+          const float t_x = dxw_y(w_PL), s_xz = dxw_y(w_M);
+          const float t_xz = dzm<1>(zm), s_z = dzp<1>(zp);
+          vx.y = ovx.y + (-cbx * t_x + -cbz * t_xz);
+          vz.y = ovz.y + (-cbx * s_xz + -cbz * s_z);
+        }
+        *reinterpret_cast<float2 *>(a.ab.vx + k) = vx;
+        *reinterpret_cast<float2 *>(a.ab.vz + k) = vz;
+      }
+    }
+    if (rec_col) cp_async_wait<6>();
+    cur.advance();
+  }
+  pair_exit<kD>(bars, cur, aborted, ok, a.err);
+  cp_async_wait<0>();
+}
+
+}  // namespace ds2d

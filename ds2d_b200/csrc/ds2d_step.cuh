@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(kBX *kBY) k_image(ImgArgs a) {
   const int ix = blockIdx.y * kBY + threadIdx.y;
   if (ix >= d.wnx || iz >= d.wnz) return;
   const long long k = d.slot * s + (long long)(ix + d.pml) * d.ld + iz + d.pml;
-  const long long o = ((long long)s * d.wnx_max + ix) * d.wnz + iz;
+  const long long o = ((long long)s * d.wnx_max + ix) * d.ild + (iz + d.pml);
   const float kpp = a.p.kpp[k], kps = a.p.kps[k];
   float pp, ps;
   image_pair(a.e.gx_vx, a.e.gz_vz, a.e.gz_vx, a.e.gx_vz, a.atxx, a.atzz, a.atxz, k, kpp, kps, pp, ps);
@@ -472,7 +472,7 @@ __global__ void k_image_reduce(Dims d, const float *img, long long img_plane, in
     for (int s = 0; s < nslots; s++) {
       const int c = col - shots[s].win_left;
       if (c >= 0 && c < shots[s].wnx)
-        acc += img[a * img_plane + ((long long)s * d.wnx_max + c) * d.wnz + iz];
+        acc += img[a * img_plane + ((long long)s * d.wnx_max + c) * d.ild + (iz + d.pml)];
     }
     full[a * full_plane + (long long)col * d.allnz + iz] = acc;
   }

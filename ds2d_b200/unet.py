@@ -33,6 +33,20 @@ def flatten(params, base=32):
     return np.concatenate(parts).astype(np.float32)
 
 
+def he_normal(seed, base=32):
+    """Initial parameters as one flat FP32 vector: He-normal 3x3 weights (std sqrt(2 / fan_in)),
+    std sqrt(1 / fan_in) for the 1x1 output layer, zero biases; seeded, in layer_shapes order."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for name, ws, bs in layer_shapes(base):
+        k, _, cout, cin = ws
+        fan_in = cin * k * k
+        std = np.sqrt((1.0 if name == "out" else 2.0) / fan_in)
+        parts.append((rng.standard_normal(ws) * std).ravel())
+        parts.append(np.zeros(bs).ravel())
+    return np.concatenate(parts).astype(np.float32)
+
+
 def unflatten(vec, base=32):
     out, off = {}, 0
     for name, ws, bs in layer_shapes(base):

@@ -171,8 +171,11 @@ int ds2d_dot_f64(ds2d_ctx *ctx, const float *a, const float *b, long long n, dou
  * in a static device array of the library (256 KiB per device), so:
  *  - n is limited to 536,870,912 elements (32768 partial sums of 16384 elements each); a larger
  *    n returns DS2D_E_ARG with a message, and nothing is launched;
- *  - the first call on a device looks up that array's address with the device current (and may
- *    load the library's module there), so make it before any stream capture on that device;
+ *  - the first call in a CUDA context of a device looks up that array's address with the device
+ *    current (and may load the library's module there), so make it before any stream capture
+ *    on that device; the address is cached per device with the context it belongs to, and a
+ *    call from a different context (a non-primary one, or the primary context re-created after
+ *    cudaDeviceReset) looks it up again;
  *  - calls on the same device that overlap in time (other host threads, or streams whose work
  *    runs concurrently) share the array and race: serialise them.
  * Runs on `stream` (NULL = the legacy default stream) of the current device and returns after
@@ -181,6 +184,21 @@ int ds2d_dot_f64(ds2d_ctx *ctx, const float *a, const float *b, long long n, dou
  * FP64 rounding, not bit for bit. */
 int ds2d_dot_f64_noalloc(const float *a, const float *b, long long n, void *stream,
                          double *result);
+
+/* Gradient band-pass filter, replacing the reference's bandpass_filter (FD2DGPU.cu:4125-4182,
+ * which main.cpp:1074-1089 applies to the summed gradients when enabled): each [nx][nz] image
+ * (z fastest) is transformed to the 2D spectrum in FP64, multiplied by the Gaussian band-pass of
+ * construct_gaussian_bandpass_filter (FD2DGPU.cu:4038-4077) with low cut-off z1 (0 = low-pass)
+ * and high cut-off z2, and transformed back, reproducing the reference's quadrant swaps and its
+ * complex (k, k) multiply.  x1, x2 are accepted for the reference's signature and unused, as in
+ * its live filter.  ds2d_bandpass_filter takes host arrays (copied in and out, like the
+ * reference); ds2d_bandpass_filter_device filters device arrays in place on `stream`.  Either
+ * image pointer may be NULL.  Both allocate their scratch per call (two DFT matrices and three
+ * work planes, about 16 (nx^2 + nz^2 + 3 nx nz) bytes).  Errors via ds2d_last_error(NULL). */
+int ds2d_bandpass_filter(int nx, int nz, int x1, int x2, int z1, int z2, float *grad_pp,
+                         float *grad_ps);
+int ds2d_bandpass_filter_device(int nx, int nz, int x1, int x2, int z1, int z2, float *grad_pp,
+                                float *grad_ps, void *stream);
 
 /* Tuning knobs (no counterpart in the reference, whose launch shape is fixed at 32x32 blocks,
  * FD2DGPU.cuh:8-9): "fused" (1 = single-pass fused time step, 0 = one launch per half step),

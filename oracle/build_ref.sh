@@ -3,8 +3,21 @@
 # reference tree) plus oracle/ref_harness.cu into oracle/_ref/libds2dref.so.  Test
 # infrastructure only: the library is the parity checker, never the product.  Flags follow the
 # reference Makefile (nvcc -O3 -w -DELASTIC -DORDER=12) with an explicit sm_100a target.
+#
+#   oracle/build_ref.sh [--if-present]
+#
+# The reference tree is read from $DS2D_REFERENCE, default /root/reference.  With --if-present a
+# missing tree is not an error (nothing is built), so build steps can call the recipe anywhere.
 set -euo pipefail
 REF="${DS2D_REFERENCE:-/root/reference}"
+if [ ! -f "$REF/FD2DGPU.cu" ]; then
+  if [ "${1:-}" = "--if-present" ]; then
+    echo "reference tree not found at $REF: oracle/_ref not built"
+    exit 0
+  fi
+  echo "reference tree not found at $REF (set DS2D_REFERENCE)" >&2
+  exit 1
+fi
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 mkdir -p "$OUT"

@@ -440,6 +440,34 @@ int forward_impl(const orc_grid *gg, const float *const model[7], const float *w
   return 0;
 }
 
+// First-order Born modelling, FD2DGPU.cu:1820-1831 (born_modeling mode 1) after the explosive
+// source: background step, add_born_source of the new background velocities into the scattered
+// stresses (born.cu:351-405), scattered step; the scattered velocities are recorded.  With
+// vs = 0 (mu = 0) this is the acoustic Born operator of the elastic scheme.
+template <class R>
+int born_impl(const orc_grid *gg, const float *const model[7], const float *dmp,
+              const float *dms, const float *wav, int nt, const orc_shot *s, double *rec_vz,
+              double *rec_vx) {
+  Geo<R> g(gg);
+  Model<R> M = load_model(g, model, dmp, dms);
+  Wave<R> w(g.n), b(g.n);
+  Vec<R> rz((size_t)s->ntr * nt), rx((size_t)s->ntr * nt);
+  for (int it = 0; it < nt; it++) {
+    fwd_background_step(g, w, M, wav, s, it);
+    k_born_source(g, w, b, M, 1);
+    k_update_vx(g, b, M, 1, g.nop);
+    k_update_vz(g, b, M, 1, g.nop);
+    k_update_txx_tzz(g, b, M, 1, g.nop, (Strain<R> *)nullptr);
+    k_update_txz(g, b, M, 1, g.nop, (Strain<R> *)nullptr);
+    k_record(g, s, nt, it, b.vz, b.vx, rz, rx);
+  }
+  for (size_t i = 0; i < rz.size(); i++) {
+    rec_vz[i] = rz[i];
+    rec_vx[i] = rx[i];
+  }
+  return 0;
+}
+
 // FD2DGPU.cu:4556-4664: NCC adjoint source (double host arithmetic).
 void ncc_residual(int ntr, int nt, const std::vector<double> &sz, const std::vector<double> &sx,
                   const float *dz_obs, const float *dx_obs, int iter, std::vector<double> &rz,
@@ -876,6 +904,16 @@ int orc_forward_f64(const orc_grid *g, const float *const model[7], const float 
 int orc_forward_f32(const orc_grid *g, const float *const model[7], const float *wavelet, int nt,
                     const orc_shot *s, double *rec_vz, double *rec_vx) {
   return forward_impl<float>(g, model, wavelet, nt, s, rec_vz, rec_vx);
+}
+int orc_born_f64(const orc_grid *g, const float *const model[7], const float *dm_p,
+                 const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
+                 double *rec_vz, double *rec_vx) {
+  return born_impl<double>(g, model, dm_p, dm_s, wavelet, nt, s, rec_vz, rec_vx);
+}
+int orc_born_f32(const orc_grid *g, const float *const model[7], const float *dm_p,
+                 const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
+                 double *rec_vz, double *rec_vx) {
+  return born_impl<float>(g, model, dm_p, dm_s, wavelet, nt, s, rec_vz, rec_vx);
 }
 
 int orc_elsrtm_f64(const orc_grid *g, const float *const model[7], const float *dm_p,

@@ -72,6 +72,13 @@ int orc_forward_f32(const orc_grid *g, const float *const model[7], const float 
  *   img[7]             window images [nx][nz] in imagebuffer_resettozero order:
  *                      pp_grad, ps_grad, illumination, b_pp, b_ps, b_pp2, b_ps2
  *   misfit             accumulated exactly as FD2DGPU.cu:4615-4618 (iter > 0 only) */
+/* First-order Born records (scattered vz, vx) of born_modeling mode 1 (FD2DGPU.cu:1820-1831). */
+int orc_born_f64(const orc_grid *g, const float *const model[7], const float *dm_p,
+                 const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
+                 double *rec_vz, double *rec_vx);
+int orc_born_f32(const orc_grid *g, const float *const model[7], const float *dm_p,
+                 const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
+                 double *rec_vz, double *rec_vx);
 int orc_elsrtm_f64(const orc_grid *g, const float *const model[7], const float *dm_p,
                    const float *dm_s, const float *wavelet, int nt, const orc_shot *s,
                    const float *obs_vz, const float *obs_vx, int iter, int rbc, int adjoint_born,

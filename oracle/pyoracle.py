@@ -52,6 +52,7 @@ def lib():
         L.orc_ricker.restype = None
         for p in ("f64", "f32"):
             getattr(L, f"orc_forward_{p}").argtypes = [G, M, fp, ctypes.c_int, S, dp, dp]
+            getattr(L, f"orc_born_{p}").argtypes = [G, M, fp, fp, fp, ctypes.c_int, S, dp, dp]
             getattr(L, f"orc_elsrtm_{p}").argtypes = [G, M, fp, fp, fp, ctypes.c_int, S, fp, fp,
                                                        ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                        dp, dp, dp, dp, ctypes.POINTER(dp), dp]
@@ -132,6 +133,21 @@ def forward(st, model, wavelet, shot, precision="f64"):
     rx = np.zeros((shot.ntr, nt))
     getattr(lib(), f"orc_forward_{precision}")(ctypes.byref(st.g), mp, _p(w), nt,
                                                ctypes.byref(sh), _p(rz, dp), _p(rx, dp))
+    return rz, rx
+
+
+def born(st, model, dm_p, dm_s, wavelet, shot, precision="f64"):
+    """First-order elastic Born records (rec_vz, rec_vx) [ntr][nt] of one shot: the reference's
+    born_modeling mode 1 (FD2DGPU.cu:1820-1831).  dm_p / dm_s are padded windows
+    (window_image); with vs = 0 this is the acoustic Born operator of the elastic scheme."""
+    sh, keep = _shot(shot)
+    mp, keep2 = _model_ptrs(model)
+    w = _f(wavelet)
+    nt = len(w)
+    rz = np.zeros((shot.ntr, nt))
+    rx = np.zeros((shot.ntr, nt))
+    getattr(lib(), f"orc_born_{precision}")(ctypes.byref(st.g), mp, _p(_f(dm_p)), _p(_f(dm_s)),
+                                            _p(w), nt, ctypes.byref(sh), _p(rz, dp), _p(rx, dp))
     return rz, rx
 
 
@@ -239,6 +255,9 @@ def ref_lib():
                                  fp, I, fp, fp, ctypes.POINTER(fp), dp, fp]
         L.ref_rtm.argtypes = [I, I, I, I, I, F, F, F, fp, fp, fp, I, ip, ip, I, I, I, ip, fp, fp, I,
                               fp, fp, ctypes.POINTER(fp), fp]
+        L.ref_born.argtypes = [I, I, I, I, I, F, F, F, fp, fp, fp, fp, fp, I, I, I, I, I, ip, I,
+                               fp, fp, fp, fp]
+        L.ref_release.argtypes = []
         _ref = L
     return _ref
 
@@ -253,6 +272,29 @@ def ref_forward(allnx, allnz, nx, pml, nt, dx, dz, dt, vp, vs, wavelet, shot):
     if rc != 0:
         raise RuntimeError(f"ref_forward: CUDA error {rc}")
     return rz, rx
+
+
+def ref_born(allnx, allnz, nx, pml, nt, dx, dz, dt, vp, vs, wavelet, img_pp, img_ps, shot,
+             rbc=0, vp_pad=None, vs_pad=None):
+    """First-order Born records (rec_vz, rec_vx) of one shot by the reference's own kernels
+    (born_modeling mode 1); rbc = 1 injects the padded model vp_pad / vs_pad with zero damping."""
+    gx = np.ascontiguousarray(shot.igx, np.int32)
+    rz = np.zeros((len(gx), nt), np.float32)
+    rx = np.zeros((len(gx), nt), np.float32)
+    rc = ref_lib().ref_born(allnx, allnz, nx, pml, nt, dx, dz, dt, _p(_f(vp)), _p(_f(vs)),
+                            _p(_f(wavelet)), _p(_f(img_pp)), _p(_f(img_ps)), shot.win_left,
+                            shot.isx, shot.isz, shot.igz, len(gx), _p(gx, ip), int(rbc),
+                            _p(None if vp_pad is None else _f(vp_pad)),
+                            _p(None if vs_pad is None else _f(vs_pad)), _p(rz), _p(rx))
+    if rc != 0:
+        raise RuntimeError(f"ref_born: CUDA error {rc}")
+    return rz, rx
+
+
+def ref_release():
+    """Frees the reference object the harness keeps between calls."""
+    if _ref is not None:
+        _ref.ref_release()
 
 
 def ref_elsrtm(allnx, allnz, nx, pml, nt, dx, dz, dt, vp, vs, wavelet, img_pp, img_ps, shot,

@@ -1,4 +1,5 @@
 // Harness around the reference's own CUDA build -- TEST INFRASTRUCTURE ONLY.
+// (The parity checker and the reference arm of the benchmark; never the product.)
 //
 // Compiles the reference translation unit FD2DGPU.cu in place (it is #included from the
 // reference tree by oracle/build_ref.sh; nothing is copied) and drives its FD2DGPU_ELASTIC class
@@ -10,6 +11,7 @@
 #include "FD2DGPU.cu"
 #undef private
 
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 
@@ -37,6 +39,42 @@ FD2DGPU_ELASTIC *make(const RefGeom &g, const float *wavelet, int ntr) {
                              g.nt, 4, ntr);
 }
 
+// The reference builds one FD2DGPU_ELASTIC per worker and reuses it for every shot and
+// iteration (main.cpp:939-1035); the harness does the same: one object per process, rebuilt only
+// when the geometry, the trace count or the wavelet (copied to the device by the constructor,
+// FD2DGPU.cu:56-57) changes.  The strip buffers of ref_rtm's PML mode are kept with it.
+struct Cached {
+  RefGeom g{};
+  int ntr = -1;
+  std::vector<float> wav;
+  FD2DGPU_ELASTIC *f = nullptr;
+  float *strips[8] = {};
+};
+Cached g_cached;
+
+void release_strips() {
+  for (float *&p : g_cached.strips) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+}
+
+FD2DGPU_ELASTIC *obtain(const RefGeom &g, const float *wavelet, int ntr) {
+  Cached &c = g_cached;
+  const bool same = c.f && c.ntr == ntr && c.g.allnx == g.allnx && c.g.allnz == g.allnz &&
+                    c.g.nx == g.nx && c.g.pml == g.pml && c.g.nt == g.nt && c.g.dx == g.dx &&
+                    c.g.dz == g.dz && c.g.dt == g.dt && (int)c.wav.size() == g.nt &&
+                    std::equal(c.wav.begin(), c.wav.end(), wavelet);
+  if (same) return c.f;
+  release_strips();
+  delete c.f;
+  c.f = make(g, wavelet, ntr);
+  c.g = g;
+  c.ntr = ntr;
+  c.wav.assign(wavelet, wavelet + g.nt);
+  return c.f;
+}
+
 // Receiver coordinates such that pml + (int)((float)(gc - ngx_left)/dx) == igx exactly.
 std::vector<int> coords_from_cells(const RefGeom &g, const int *igx, int ntr) {
   std::vector<int> gc(ntr);
@@ -56,7 +94,7 @@ int ref_forward(int allnx, int allnz, int nx, int pml, int nt, float dx, float d
                 int isx, int isz, int igz, int ntr, const int *igx, float *rec_vz,
                 float *rec_vx) {
   RefGeom g{allnx, allnz, nx, pml, nt, dx, dz, dt};
-  FD2DGPU_ELASTIC *f = make(g, wavelet, ntr);
+  FD2DGPU_ELASTIC *f = obtain(g, wavelet, ntr);
   std::vector<float> vp(vp_all, vp_all + (size_t)allnx * allnz), vs(vs_all, vs_all + (size_t)allnx * allnz);
   f->GPUbufferVPVS(vp.data(), vs.data());
   f->bufferVpVsHtoD(win_left);
@@ -83,9 +121,7 @@ int ref_forward(int allnx, int allnz, int nx, int pml, int nt, float dx, float d
   cudaFree(d_igx);
   cudaFree(d_rz);
   cudaFree(d_rx);
-  int rc = last_error();
-  delete f;
-  return rc;
+  return last_error();
 }
 
 // One reference-mode ELSRTM shot through the reference driver itself (rbc = 0, cpu_mem = 0),
@@ -98,7 +134,7 @@ int ref_elsrtm(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz
                float *elapsed_ms) {
   RefGeom g{allnx, allnz, nx, pml, nt, dx, dz, dt};
   size_t nall = (size_t)allnx * allnz, nrec = (size_t)ntr * nt;
-  FD2DGPU_ELASTIC *f = make(g, wavelet, ntr);
+  FD2DGPU_ELASTIC *f = obtain(g, wavelet, ntr);
   std::vector<float> vp(vp_all, vp_all + nall), vs(vs_all, vs_all + nall);
   std::vector<float> ipp(image_pp, image_pp + nall), ips(image_ps, image_ps + nall);
   std::vector<float> rz(obs_vz, obs_vz + nrec), rx(obs_vx, obs_vx + nrec);
@@ -136,9 +172,7 @@ int ref_elsrtm(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz
   if (res_vx) cudaMemcpy(res_vx, f->GPUrecord_scatter_x, nrec * sizeof(float), cudaMemcpyDeviceToHost);
   f->imagebuffer_resettozero(img7[0], img7[1], img7[2], img7[3], img7[4], img7[5], img7[6]);
   if (misfit) *misfit = mis;
-  int rc = last_error();
-  delete f;
-  return rc;
+  return last_error();
 }
 
 // Elastic RTM with the reference's kernels in the reference driver's order (forward:
@@ -156,19 +190,17 @@ int ref_rtm(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz, f
             const float *vs_pad, float *const img3[3], float *elapsed_ms) {
   RefGeom g{allnx, allnz, nx, pml, nt, dx, dz, dt};
   size_t nall = (size_t)allnx * allnz, nrec = (size_t)ntr * nt;
-  FD2DGPU_ELASTIC *f = make(g, wavelet, ntr);
+  FD2DGPU_ELASTIC *f = obtain(g, wavelet, ntr);
   std::vector<float> vp(vp_all, vp_all + nall), vs(vs_all, vs_all + nall);
   f->GPUbufferVPVS(vp.data(), vs.data());
   int nxpml = f->nxpml, nzpml = f->nzpml, N = f->nop, nDim = nxpml * nzpml;
   size_t ud = (size_t)2 * N * nx * nt, lr = (size_t)2 * N * allnz * nt;
-  float *up_x = nullptr, *up_z = nullptr, *dn_x = nullptr, *dn_z = nullptr;
-  float *lf_x = nullptr, *lf_z = nullptr, *rt_x = nullptr, *rt_z = nullptr;
-  if (!rbc) {
-    cudaMalloc(&up_x, ud * 4); cudaMalloc(&up_z, ud * 4);
-    cudaMalloc(&dn_x, ud * 4); cudaMalloc(&dn_z, ud * 4);
-    cudaMalloc(&lf_x, lr * 4); cudaMalloc(&lf_z, lr * 4);
-    cudaMalloc(&rt_x, lr * 4); cudaMalloc(&rt_z, lr * 4);
+  float **sb = g_cached.strips;
+  if (!rbc && !sb[0]) {
+    for (int i = 0; i < 8; i++) cudaMalloc(&sb[i], (i < 4 ? ud : lr) * 4);
   }
+  float *up_x = sb[0], *up_z = sb[1], *dn_x = sb[2], *dn_z = sb[3];
+  float *lf_x = sb[4], *lf_z = sb[5], *rt_x = sb[6], *rt_z = sb[7];
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -241,15 +273,76 @@ int ref_rtm(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz, f
     if (img3[1]) cudaMemcpy(img3[1], f->ps_gradient, nall * 4, cudaMemcpyDeviceToHost);
     if (img3[2]) cudaMemcpy(img3[2], f->allimageGPU_denominator, nall * 4, cudaMemcpyDeviceToHost);
   }
-  if (!rbc) {
-    cudaFree(up_x); cudaFree(up_z); cudaFree(dn_x); cudaFree(dn_z);
-    cudaFree(lf_x); cudaFree(lf_z); cudaFree(rt_x); cudaFree(rt_z);
-  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  int rc = last_error();
-  delete f;
-  return rc;
+  return last_error();
+}
+
+// First-order Born modelling with the reference's own kernels: per step the explosive source
+// (FD2DGPU.cu:2046-2049), then born_modeling(direction 1, mode 1) -- background step,
+// add_born_source of the new background velocities, scattered step (:1820-1831) -- and the
+// scattered velocities b_vz / b_vx sampled at the receivers.  The model perturbation images
+// image_pp / image_ps are windowed by buffer_image_extrapolation (:1324-1333) as in the ELSRTM
+// driver.  rbc = 1 takes a pre-randomised padded model (vp_pad / vs_pad) with zero damping, as
+// ref_rtm does; rbc = 0 uses the reference's PML (calculate_elastic_damp_C).  With vs = 0 this
+// is the reference's acoustic Born operator: mu = 0 removes every shear term.
+int ref_born(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz, float dt,
+             const float *vp_all, const float *vs_all, const float *wavelet,
+             const float *image_pp, const float *image_ps, int win_left, int isx, int isz,
+             int igz, int ntr, const int *igx, int rbc, const float *vp_pad, const float *vs_pad,
+             float *rec_vz, float *rec_vx) {
+  RefGeom g{allnx, allnz, nx, pml, nt, dx, dz, dt};
+  const size_t nall = (size_t)allnx * allnz;
+  FD2DGPU_ELASTIC *f = obtain(g, wavelet, ntr);
+  std::vector<float> vp(vp_all, vp_all + nall), vs(vs_all, vs_all + nall);
+  std::vector<float> ipp(image_pp, image_pp + nall), ips(image_ps, image_ps + nall);
+  f->GPUbufferVPVS(vp.data(), vs.data());
+  f->GPUbufferM(ipp.data(), ips.data());
+  f->bufferVpVsHtoD(win_left);
+  f->isx = isx;
+  f->isz = isz;
+  f->igz = igz;
+  const int nxpml = f->nxpml, nzpml = f->nzpml, nDim = nxpml * nzpml;
+  f->FD_ELASTIC_initial(nDim);
+  f->BK_ELASTIC_initial(nDim);
+  f->LSRTM_initial(nDim);
+  f->buffer_image_extrapolation(win_left);
+  if (rbc) {
+    cudaMemcpy(f->vp, vp_pad, (size_t)nDim * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(f->vs, vs_pad, (size_t)nDim * 4, cudaMemcpyHostToDevice);
+    cudaMemset(f->d_damp, 0, (size_t)nDim * 4);
+    cudaMemset(f->d_dampz, 0, (size_t)nDim * 4);
+    GPUcalculate_elastic_rho_C<<<f->Grid_Block.grid, f->Grid_Block.block>>>(
+        f->d_rho, f->vp, f->vs, f->lamda, f->miu, nxpml, nzpml);
+  } else {
+    f->calculate_elastic_damp_C();
+  }
+  int *d_igx;
+  float *d_rz, *d_rx;
+  cudaMalloc(&d_igx, ntr * sizeof(int));
+  cudaMalloc(&d_rz, (size_t)ntr * nt * sizeof(float));
+  cudaMalloc(&d_rx, (size_t)ntr * nt * sizeof(float));
+  cudaMemcpy(d_igx, igx, ntr * sizeof(int), cudaMemcpyHostToDevice);
+  for (int it = 0; it < nt; ++it) {
+    f->elastic_rotation_addS_for(it, 0);
+    f->born_modeling(1, 1);
+    harness_record<<<(ntr + 127) / 128, 128>>>(f->b_vz, f->b_vx, d_rz, d_rx, d_igx, igz, nzpml,
+                                                ntr, nt, it);
+  }
+  cudaMemcpy(rec_vz, d_rz, (size_t)ntr * nt * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(rec_vx, d_rx, (size_t)ntr * nt * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(d_igx);
+  cudaFree(d_rz);
+  cudaFree(d_rx);
+  return last_error();
+}
+
+// Frees the cached reference object (and its strip buffers).
+int ref_release() {
+  release_strips();
+  delete g_cached.f;
+  g_cached = Cached{};
+  return last_error();
 }
 
 }  // extern "C"

@@ -174,3 +174,35 @@ def test_acoustic_fused_steps_match_half_steps(cuda_device):
             out[fused] = (dz, dx, g)
     for a, b in zip(out[1], out[0]):
         assert rel(a, b) < 1e-6, rel(a, b)
+
+
+def test_ac_born_vs_reference_golden(cuda_device):
+    """The acoustic Born operator against the reference itself: first-order Born records of the
+    reference's born_modeling (mode 1) with vs = 0 (mu = 0 removes every shear term), the random
+    band injected and no damping, made by tests/golden/make_golden.py.  Born records are
+    reproducible only to the FP32 floor of the scheme, measured per case on the oracle."""
+    from tests.helpers import case_of, gate, load, shots_of
+    fx = load("born_acoustic_random.npz")
+    assert fx is not None, "golden fixture born_acoustic_random.npz missing"
+    c = case_of(fx)
+    shots = shots_of(fx)
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    seed = int(fx["seed"])
+    with Elastic2D(c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                   boundary="random", seed=seed, max_shots=len(shots),
+                   max_ntr=max(s.ntr for s in shots)) as e:
+        e.set_models(fx["vp"], fx["vs"])
+        e.set_wavelet(fx["wavelet"])
+        dz, dx = e.ac_born(shots, fx["img_pp"])
+    ntr = shots[0].ntr
+    zero = np.zeros_like(fx["img_pp"])
+    for i, s in enumerate(shots):
+        m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left, rbc=1, seed=seed, shot_id=i)
+        dmp = po.window_image(st, fx["img_pp"], s.win_left)
+        dms = po.window_image(st, zero, s.win_left)
+        b64 = po.born(st, m, dmp, dms, fx["wavelet"], s, "f64")
+        b32 = po.born(st, m, dmp, dms, fx["wavelet"], s, "f32")
+        for got, key, j in ((dz, "rec_vz", 0), (dx, "rec_vx", 1)):
+            floor = rel(b32[j], b64[j])
+            err = rel(got[i * ntr:(i + 1) * ntr], fx[key][i])
+            assert err < gate(floor), (key, i, err, f"FP32 floor {floor:.3e}")

@@ -204,6 +204,7 @@ def test_fused_step_matches_half_steps(cuda_device, boundary, xr, ring):
     out = {}
     for fused in (0, 1):
         with _ctx(c, shots, boundary=boundary, seed=5) as e:
+            e.set_option("pair", 0)  # the one-column kernels (the pair kernels have their own test)
             e.set_option("fused", fused)
             e.set_option("ring", ring)
             e.set_option("xr", xr)
@@ -231,6 +232,7 @@ def test_ring_occupancy_variants_agree(cuda_device, boundary):
     out = {}
     for occ in (0, 1):
         with _ctx(c, shots, boundary=boundary, seed=5) as e:
+            e.set_option("pair", 0)
             e.set_option("occ", occ)
             e.set_models(vp, vs)
             e.set_wavelet(w)
@@ -254,6 +256,7 @@ def test_ring_cta_widths_agree(cuda_device, boundary):
     out = {}
     for cta in (128, 192):
         with _ctx(c, shots, boundary=boundary, seed=5) as e:
+            e.set_option("pair", 0)
             e.set_option("cta", cta)
             e.set_models(vp, vs)
             e.set_wavelet(w)
@@ -401,5 +404,203 @@ def test_live_reference_rtm_random(cuda_device):
         e.set_wavelet(w)
         e.rtm(shots, az, ax)
         imgs = e.read_images()
+    tot64 = np.zeros((3, c["allnx"], c["allnz"]))
+    tot32 = np.zeros((3, c["allnx"], c["allnz"]))
+    ntr = shots[0].ntr
+    for i, s in enumerate(shots):
+        sl = slice(i * ntr, (i + 1) * ntr)
+        for tot, prec in ((tot64, "f64"), (tot32, "f32")):
+            o = po.rtm(st, pads[i], w, s, az[sl], ax[sl], 1, prec)
+            for k in range(3):
+                tot[k] += po.place(o[k], c["allnx"], c["allnz"], s.win_left)
     for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
-        assert rel(imgs[key], ref_imgs[k]) < 2e-5, (key, rel(imgs[key], ref_imgs[k]))
+        floor = rel(tot32[k], tot64[k])
+        err = rel(imgs[key], ref_imgs[k])
+        assert err < gate(floor), f"{key}: vs reference {err:.3e}, FP32 floor {floor:.3e}"
+
+
+@pytest.mark.parametrize("pair_cta", [160, 256])
+@pytest.mark.parametrize("pair_xr", [0, 24])
+def test_pair_kernels_match_ring_and_oracle(cuda_device, pair_cta, pair_xr):
+    """Pair-blocked bulk-copy kernels of the random-boundary RTM step (forward with receiver
+    records, backward with the residual injection and the imaging condition) against the
+    one-column ring kernels and the FP64 oracle.  The 320-deep grid makes the 160-thread CTAs run
+    two z-strips; xr 24 gives each shot four row blocks (x-halos between CTAs)."""
+    c, _, _, w, _ = small_case(nt=200)
+    c["allnz"] = 300
+    vp, vs = synth.layered(c["allnx"], c["allnz"], seed=4)
+    shots = synth.surface_shots(c["allnx"], c["nx"], c["pml"], 3)
+    with _ctx(c, shots, boundary="pml") as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        oz, ox = e.forward(shots)
+    vpm, vsm = synth.smooth(vp, 3.0), synth.smooth(vs, 3.0)
+    out = {}
+    for pair in (0, 1):
+        with _ctx(c, shots, boundary="random", seed=5) as e:
+            e.set_option("pair", pair)
+            if pair:
+                e.set_option("pair_cta", pair_cta)
+                e.set_option("pair_xr", pair_xr)
+            e.set_models(vpm, vsm)
+            e.set_wavelet(w)
+            rz, rx = e.forward(shots)
+            e.rtm(shots, oz, ox)
+            out[pair] = (rz, rx, e.read_images())
+    assert np.abs(out[1][0]).max() > 0
+    assert rel(out[1][0], out[0][0]) < GATE and rel(out[1][1], out[0][1]) < GATE
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    ntr = shots[0].ntr
+    tot64 = np.zeros((3, c["allnx"], c["allnz"]))
+    tot32 = np.zeros((3, c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        m = po.build_model(st, vpm, vsm, None, s.win_left, rbc=1, seed=5, shot_id=i)
+        fz, fx = po.forward(st, m, w, s, "f64")
+        sl = slice(i * ntr, (i + 1) * ntr)
+        assert rel(out[1][0][sl], fz) < GATE and rel(out[1][1][sl], fx) < GATE
+        for tot, prec in ((tot64, "f64"), (tot32, "f32")):
+            o = po.rtm(st, m, w, s, oz[sl], ox[sl], 1, prec)
+            for k in range(3):
+                tot[k] += po.place(o[k], c["allnx"], c["allnz"], s.win_left)
+    for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
+        floor = rel(tot32[k], tot64[k])
+        err_ring = rel(out[1][2][key], out[0][2][key])
+        err64 = rel(out[1][2][key], tot64[k])
+        assert err_ring < gate(floor), (key, err_ring, f"FP32 floor {floor:.3e}")
+        assert err64 < gate(floor), (key, err64, f"FP32 floor {floor:.3e}")
+
+
+def test_pair_kernels_uneven_windows(cuda_device):
+    """Shots of different aperture in one batch on the pair kernels (per-slot row counts, CTAs
+    beyond a slot's window return at once) against the FP64 oracle."""
+    c, vp, vs, w, _ = small_case(nt=200)
+    shots = synth.uneven_shots(c["allnx"], c["pml"], 4, 20, c["allnx"], seed=9)
+    wmax = max(s.nx for s in shots)
+    with Elastic2D(c["allnx"], c["allnz"], wmax, c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                   boundary="random", seed=8, max_shots=len(shots), max_ntr=wmax) as e:
+        e.set_option("pair", 1)
+        e.set_option("pair_xr", 16)
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        rz, rx = e.forward(shots)
+        e.rtm(shots, rz, rx)
+        imgs = e.read_images()
+    off = 0
+    tot = np.zeros((3, c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        st = po.Setup(c["allnx"], c["allnz"], s.nx, c["pml"], c["dx"], c["dz"], c["dt"])
+        m = po.build_model(st, vp, vs, None, s.win_left, rbc=1, seed=8, shot_id=i)
+        oz, ox = po.forward(st, m, w, s)
+        assert rel(rz[off:off + s.ntr], oz) < GATE
+        o = po.rtm(st, m, w, s, rz[off:off + s.ntr], rx[off:off + s.ntr], 1)
+        for k in range(3):
+            tot[k] += po.place(o[k], c["allnx"], c["allnz"], s.win_left)
+        off += s.ntr
+    for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
+        assert rel(imgs[key], tot[k]) < 1e-4, (key, rel(imgs[key], tot[k]))
+
+
+def _headline_survey(nt):
+    """The RTM benchmark's grid (1201x401 model, 40-cell band, dt 0.8 ms), its seeded model pair
+    and two of its 60 surface shots."""
+    c = dict(allnx=1201, allnz=401, nx=1201, pml=40, nt=nt, dx=10.0, dz=10.0, dt=0.0008)
+    vp, vs = synth.dipping_lenses(c["allnx"], c["allnz"], seed=2024)
+    vpm, vsm = synth.smooth(vp, 15.0), synth.smooth(vs, 15.0)
+    w = synth.ricker(nt, 15.0, c["dt"])
+    survey = synth.surface_shots(c["allnx"], c["nx"], c["pml"], 60)
+    return c, vp, vs, vpm, vsm, w, [survey[7], survey[41]]
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_live_reference_rtm_headline(cuda_device):
+    """Elastic RTM at the benchmark's full size (1201x401 + 40-cell random band, nt 4000, two
+    shots) against the reference's own CUDA kernels on the same padded model, and one shot against
+    the FP64 oracle.  In the undamped band every rounding difference stays in the grid for 4000
+    steps: the reference's FP32 result itself lies about 1.5e-3 from the FP64 restatement of its
+    scheme (its split-field update rounds differently), so the gate against it is the FP32 floor
+    of the scheme (|oracle f32 - oracle f64|), which every assertion prints.  Against the FP64
+    oracle this path must be at least as close as the reference is."""
+    c, vp, vs, vpm, vsm, w, shots = _headline_survey(4000)
+    g = tuple(c.values())
+    with _ctx(c, shots, boundary="pml") as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        az, ax = e.forward(shots)
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    pads = [po.build_model(st, vpm, vsm, None, s.win_left, rbc=1, seed=77, shot_id=i)
+            for i, s in enumerate(shots)]
+    vpp, vsp = np.stack([p[0] for p in pads]), np.stack([p[1] for p in pads])
+    ntr = shots[0].ntr
+    ref2, _ = po.ref_rtm(*g, vpm, vsm, w, shots, az, ax, rbc=1, vp_pad=vpp, vs_pad=vsp)
+    ref1, _ = po.ref_rtm(*g, vpm, vsm, w, shots[:1], az[:ntr], ax[:ntr], rbc=1, vp_pad=vpp[:1],
+                         vs_pad=vsp[:1])
+    with _ctx(c, shots, boundary="random", seed=77) as e:
+        e.set_models(vpm, vsm)
+        e.set_wavelet(w)
+        e.rtm(shots, az, ax)
+        ours2 = e.read_images()
+        e.rtm(shots[:1], az[:ntr], ax[:ntr])
+        ours1 = e.read_images()
+    o64 = po.rtm(st, pads[0], w, shots[0], az[:ntr], ax[:ntr], 1, "f64")
+    o32 = po.rtm(st, pads[0], w, shots[0], az[:ntr], ax[:ntr], 1, "f32")
+    for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
+        f64 = po.place(o64[k], c["allnx"], c["allnz"], shots[0].win_left)
+        f32 = po.place(o32[k], c["allnx"], c["allnz"], shots[0].win_left)
+        floor = rel(f32, f64)
+        e_ref = rel(ours2[key], ref2[k])
+        e_64, r_64 = rel(ours1[key], f64), rel(ref1[k], f64)
+        msg = (f"{key}: vs reference {e_ref:.3e}, vs FP64 {e_64:.3e} (reference vs FP64 "
+               f"{r_64:.3e}), FP32 floor {floor:.3e}")
+        assert e_ref < gate(floor), msg
+        assert e_64 < gate(floor) and e_64 <= r_64 + GATE, msg
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_live_reference_elsrtm_full_size(cuda_device):
+    """Reference-mode ELSRTM (PML + FP32 strips, Born modelling, NCC adjoint source, seven
+    gradients) at 1201x401, nt 2000, one shot, against the reference's own per-shot driver and
+    the FP64 oracle.  Receivers within 300 columns of the source: the wavefield reaches all of
+    them in 2000 steps (the reference's NCC divides by each trace's norm, FD2DGPU.cu:4567-4572,
+    so an all-zero trace would give NaN in both).  Each output must be within the FP32 floor of
+    the FP64 oracle, and within that floor plus the reference's own distance to the FP64 oracle of
+    the reference."""
+    from ds2d_b200.api import ShotGeom
+    c, vp, vs, vpm, vsm, w, _ = _headline_survey(2000)
+    g = tuple(c.values())
+    s0 = synth.surface_shots(c["allnx"], c["nx"], c["pml"], 16)[5]
+    igx = np.arange(max(c["pml"], s0.isx - 300), min(c["pml"] + c["nx"], s0.isx + 301),
+                    dtype=np.int32)
+    s = ShotGeom(s0.win_left, s0.isx, s0.isz, s0.igz, igx)
+    with _ctx(c, [s], boundary="pml") as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        oz, ox = e.forward([s])
+    pp = synth.reflectivity(c["allnx"], c["allnz"], seed=5, density=0.05, std=0.05)
+    ps = 0.5 * synth.reflectivity(c["allnx"], c["allnz"], seed=6, density=0.05, std=0.05)
+    r = po.ref_elsrtm(*g, vpm, vsm, w, pp, ps, s, oz, ox, 1)
+    with _ctx(c, [s], boundary="pml", strips="f32") as e:
+        e.set_models(vpm, vsm)
+        e.set_wavelet(w)
+        e.set_image(pp, ps)
+        mis, (_, _, rz, rx) = e.elsrtm([s], oz, ox, 1, want_records=True)
+        imgs = e.read_images()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    m = po.build_model(st, vpm, vsm, None, s.win_left)
+    args = (st, m, po.window_image(st, pp, s.win_left), po.window_image(st, ps, s.win_left), w, s,
+            oz, ox, 1)
+    r64 = po.elsrtm(*args, precision="f64")
+    r32 = po.elsrtm(*args, precision="f32")
+    outs = [(rz, r["res_vz"], r64["res_vz"], r32["res_vz"], "res_vz"),
+            (rx, r["res_vx"], r64["res_vx"], r32["res_vx"], "res_vx")]
+    for k, key in enumerate(Elastic2D.IMAGE_NAMES[:5]):
+        outs.append((imgs[key], r["images"][k],
+                     po.place(r64["images"][k], c["allnx"], c["allnz"], s.win_left),
+                     po.place(r32["images"][k], c["allnx"], c["allnz"], s.win_left), key))
+    for got, ref, f64, f32, key in outs:
+        floor = rel(f32, f64)
+        e_ref, e_64, r_64 = rel(got, ref), rel(got, f64), rel(ref, f64)
+        msg = (f"{key}: vs reference {e_ref:.3e}, vs FP64 {e_64:.3e} (reference vs FP64 "
+               f"{r_64:.3e}), FP32 floor {floor:.3e}")
+        assert e_64 < gate(floor), msg
+        assert e_ref < gate(floor) + r_64, msg
+    assert mis == pytest.approx(r["misfit"], rel=1e-4) and mis == pytest.approx(r64["misfit"], rel=1e-4)

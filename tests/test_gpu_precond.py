@@ -12,8 +12,7 @@ pytestmark = pytest.mark.gpu
 
 def test_trained_network_beats_plain_cg(cuda_device):
     import torch
-    from ds2d_b200.unet import UNet, flatten
-    from oracle import unet_oracle as uo
+    from ds2d_b200.unet import UNet, he_normal
     nx, nz, band, nt, dx, dt = 96, 48, 12, 500, 10.0, 0.0008
     shots = synth.surface_shots(nx, nx, band, 8)
     with Elastic2D(nx, nz, nx, band, nt, dx, dx, dt, boundary="random", max_shots=len(shots),
@@ -23,7 +22,7 @@ def test_trained_network_beats_plain_cg(cuda_device):
         e.set_wavelet(synth.ricker(nt, 15.0, dt))
         X, Y = precond.make_trajectory_pairs(e, shots, nmodels=8, iters=8, seed=5)
         with UNet(max_n=8, max_h=nx, max_w=nz) as net:
-            net.set_params(flatten(uo.init_params(2)))
+            net.set_params(he_normal(2))
             hist = precond.train(net, X, Y, steps=800, batch=8, crop=(48, None), lr=1e-3)
             assert hist[-1] < 0.8 * hist[0]
             # held-out reflectivity (the configs' sparse kind), Born data by the same operator

@@ -71,3 +71,44 @@ def test_rtm_golden(name):
     for k in range(3):
         floor = rel(tot32[k], tot64[k])
         assert rel(fx["images"][k], tot64[k]) < gate(floor), (k, rel(fx["images"][k], tot64[k]), floor)
+
+
+def test_forward_c1_golden():
+    """First benchmark configuration at full size (251x101, 20-cell PML, nt 2000): the FP64 oracle
+    against the reference's records at every fifth receiver."""
+    fx = _need("forward_c1.npz")
+    c, st = _setup(fx)
+    s = shots_of(fx)[0]
+    m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left)
+    rz, rx = po.forward(st, m, fx["wavelet"], s, "f64")
+    keep = fx["traces"]
+    ez, ex = rel(fx["rec_vz"], rz[keep]), rel(fx["rec_vx"], rx[keep])
+    assert ez < gate() and ex < gate(), (ez, ex)
+
+
+@pytest.mark.parametrize("name", ["born_acoustic_random.npz", "born_elastic_pml.npz"])
+def test_born_golden(name):
+    """First-order Born records of the reference's born_modeling (mode 1) against the oracle's
+    restatement; for vs = 0 also against the acoustic Born oracle, which must be the same operator
+    (mu = 0 removes every shear term of the elastic scheme)."""
+    fx = _need(name)
+    c, st = _setup(fx)
+    acoustic = "acoustic" in name
+    img_ps = np.zeros_like(fx["img_pp"]) if acoustic else fx["img_ps"]
+    for i, s in enumerate(shots_of(fx)):
+        rbc = 1 if acoustic else 0
+        m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left, rbc=rbc,
+                           seed=int(fx.get("seed", 0)), shot_id=i)
+        if acoustic:
+            np.testing.assert_array_equal(m[0], fx["vp_pad"][i])
+        dmp = po.window_image(st, fx["img_pp"], s.win_left)
+        dms = po.window_image(st, img_ps, s.win_left)
+        b64 = po.born(st, m, dmp, dms, fx["wavelet"], s, "f64")
+        b32 = po.born(st, m, dmp, dms, fx["wavelet"], s, "f32")
+        for j in range(2):
+            floor = rel(b32[j], b64[j])
+            got = rel(fx["rec_vz" if j == 0 else "rec_vx"][i], b64[j])
+            assert got < gate(floor), (i, j, got, floor)
+        if acoustic:
+            az, ax = po.ac_born(st, m, fx["wavelet"], s, dmp)
+            assert rel(az, b64[0]) < 1e-10 and rel(ax, b64[1]) < 1e-10
