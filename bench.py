@@ -51,12 +51,18 @@ def parse():
     p.add_argument("--ref-shots", type=int, default=2, help="shots per reference-arm step")
     p.add_argument("--no-autotune", action="store_true",
                    help="skip the launch-shape autotuner (library defaults)")
-    p.add_argument("--workload", default="rtm", choices=["rtm", "uneven", "lsrtm", "elsrtm"],
+    p.add_argument("--set", default="",
+                   help="library options applied after the autotuner, e.g. pair=1,pair_xr=96 "
+                        "(profiling runs of one kernel variant)")
+    p.add_argument("--workload", default="rtm",
+                   choices=["rtm", "uneven", "lsrtm", "elsrtm", "acoustic", "unet"],
                    help="rtm: elastic RTM throughput, 60 shots 1201x401 (default); uneven: 256 "
                         "shots with their own aperture windows from a 4001x401 model; lsrtm: "
                         "learned vs plain CG-LSRTM; elsrtm: reference-mode ELSRTM iteration "
                         "(PML + boundary strips, Born modelling, NCC adjoint source), 16 shots "
-                        "1201x401, nt 2000")
+                        "1201x401, nt 2000; acoustic: the CG-LSRTM normal operator L^T L on the "
+                        "2001x601 grid (+20 band), 16 shots by default; unet: the preconditioner "
+                        "network's forward pass and training step on one 2008x608 image")
     p.add_argument("--lsrtm-size", default="full", choices=["small", "full"],
                    help="full: 2001x601, 80 shots, nt 5000; small: 512x256, 40 shots, nt 2000")
     p.add_argument("--pairs", type=int, default=192, help="training pairs of the preconditioner")
@@ -149,6 +155,15 @@ def workload(args, rank, world=1):
     return c, vp, vs, vpm, vsm, w, shots
 
 
+def parse_set(text):
+    """'k=v,k2=v2' -> {k: int(v)} (library options of --set)."""
+    out = {}
+    for item in filter(None, (x.strip() for x in text.split(","))):
+        k, v = item.split("=")
+        out[k.strip()] = int(v)
+    return out
+
+
 def job_updates(upd, dist, dev):
     """Cell-updates of one step summed over all ranks (shards of uneven windows differ)."""
     if dist is None:
@@ -231,6 +246,9 @@ def run_ours(args, rank, world, dist):
                   boundary="random", max_shots=c["shots"], max_ntr=ntr, seed=c["seed"], device=dev)
     if tuned:
         apply(e, tuned)
+    for k, v in parse_set(args.set).items():
+        e.set_option(k, v)
+        tuned = dict(tuned or {}, **{k: v})
     e.set_models(vpm, vsm)
     e.set_wavelet(w)
     # A non-default stream: the library captures each batch (time loops included) into a CUDA
@@ -250,12 +268,15 @@ def run_ours(args, rank, world, dist):
             dist.barrier()
         torch.cuda.synchronize()
 
+    red_buf = torch.empty((3, c["allnx"], c["allnz"]), dtype=torch.float32, device=dev)
+
     def allreduce_images():
-        # the one exchange step of the path: the images summed over every rank's shots
+        # the one exchange step of the path: the images summed over every rank's shots, device
+        # to device into red_buf and one in-place NCCL all-reduce (the library's stream is
+        # torch's current stream)
         if dist is not None:
-            from ds2d_b200.shard import reduce_images
-            imgs = e.read_images(reset=True, which=("pp_grad", "ps_grad", "illumination"))
-            return reduce_images(imgs, dist, device=dev)
+            from ds2d_b200.shard import reduce_images_device
+            return reduce_images_device(e, dist, red_buf)
         return None
 
     # warm-up
@@ -290,8 +311,9 @@ def run_ours(args, rank, world, dist):
     for _ in range(args.steps):
         e.rtm(shots, h_z.numpy(), h_x.numpy())
         if dist is not None:
-            allreduce_images()
-        e.read_images(reset=True, which=("pp_grad", "ps_grad", "illumination"))
+            allreduce_images().cpu()  # the job's images, read back once per step
+        else:
+            e.read_images(reset=True, which=("pp_grad", "ps_grad", "illumination"))
     e1.record(stream)
     barrier()
     ms_e2e = e0.elapsed_time(e1)
@@ -389,10 +411,12 @@ def run_elsrtm(args, rank, world, dist):
             dist.barrier()
         torch.cuda.synchronize()
 
+    red_buf = torch.empty((len(names), c["allnx"], c["allnz"]), dtype=torch.float32, device=dev)
+
     def reduce_grads():
         if dist is not None:
-            from ds2d_b200.shard import reduce_images
-            reduce_images(e.read_images(reset=True, which=names), dist, device=dev)
+            from ds2d_b200.shard import reduce_images_device
+            reduce_images_device(e, dist, red_buf, which=names)
 
     for _ in range(args.warmup):
         e.elsrtm_device(shots, d_z.data_ptr(), d_x.data_ptr(), 1)
@@ -425,6 +449,7 @@ def run_elsrtm(args, rank, world, dist):
         e.elsrtm(shots, h_z.numpy(), h_x.numpy(), 1)
         if dist is not None:
             reduce_grads()
+            red_buf.cpu()
         else:
             e.read_images(reset=True, which=names)
     e1.record(stream)
@@ -589,6 +614,87 @@ def run_reference(args, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_acoustic(args):
+    """The acoustic Born pair of CG-LSRTM (configs 3 / 5): L^T L (ds2d_ac_normal: background with
+    the Born source, scattered set with records, background replay, fused reverse step) on the
+    2001x601 grid with a 20-cell random band; shots evenly spread, nt from --nt (default 60 here,
+    the profiling case).  Timed with CUDA events on the library's stream."""
+    import torch
+    from ds2d_b200 import Elastic2D, synth
+    allnx, allnz, band = 2001, 601, 20
+    nt = args.nt if args.nt != CFG["nt"] else 60
+    nshots = args.shots if args.shots != CFG["shots"] else 16
+    vp = np.broadcast_to(np.linspace(1800, 4500, allnz, dtype=np.float32), (allnx, allnz)).copy()
+    w = synth.ricker(nt, 15.0, 0.0008)
+    shots = synth.surface_shots(allnx, allnx, band, nshots)
+    m = torch.from_numpy(synth.reflectivity(allnx, allnz, seed=4, density=0.05, std=0.05)).cuda()
+    img = torch.zeros_like(m)
+    with Elastic2D(allnx, allnz, allnx, band, nt, 10.0, 10.0, 0.0008, boundary="random",
+                   max_shots=nshots, max_ntr=allnx, seed=3) as e:
+        e.set_models(vp, 0 * vp)
+        e.set_wavelet(w)
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        e.set_stream(stream.cuda_stream)
+        for _ in range(args.warmup):
+            e.ac_normal_device(shots, m.data_ptr(), img.data_ptr())
+        upd = e.last_cell_updates
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            e.ac_normal_device(shots, m.data_ptr(), img.data_ptr())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+    return {"metric": "Gcell-updates/s (acoustic L^T L)", "value": round(upd * args.steps / ms / 1e6, 3),
+            "unit": "Gcell-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (linear 1800-4500 m/s background, seeded sparse reflectivity)",
+            "config": {"workload": "acoustic normal operator L^T L", "grid": "2001x601 (+20 band)",
+                       "shots": nshots, "nt": nt, "cell_updates_per_step": upd}}
+
+
+def run_unet(args):
+    """The preconditioner network (4-level U-Net, 32 base channels, BF16 tensor cores) on one
+    2008x608 image: forward pass and one training step (loss gradient + Adam), CUDA events."""
+    import torch
+    from ds2d_b200.unet import UNet, he_normal, layer_shapes
+    h, w = 2008, 608
+    x = torch.randn((1, h, w), device="cuda")
+    t = torch.randn((1, h, w), device="cuda")
+    y = torch.empty_like(x)
+    flops = 0.0
+    for lvl, (name, ws, _) in enumerate(layer_shapes(32)):
+        k, _, co, ci = ws
+        scale = 4 ** int(name[1]) // 4 if name[0] in "ed" else 1  # level l runs at 1/4^(l-1) pixels
+        flops += 2.0 * h * w / scale * co * ci * k * k
+    with UNet(base=32, max_n=1, max_h=h, max_w=w) as net:
+        net.set_params(he_normal(5))
+        for _ in range(args.warmup):
+            net.forward(x.data_ptr(), y.data_ptr(), 1, h, w)
+            net.loss_grad(x.data_ptr(), t.data_ptr(), 1, h, w)
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        for _ in range(args.steps):
+            net.forward(x.data_ptr(), y.data_ptr(), 1, h, w)
+        e1.record()
+        for _ in range(args.steps):
+            net.loss_grad(x.data_ptr(), t.data_ptr(), 1, h, w)
+            net.adam_step()
+        e2.record()
+        torch.cuda.synchronize()
+        fwd_ms = e0.elapsed_time(e1) / args.steps
+        train_ms = e1.elapsed_time(e2) / args.steps
+    return {"metric": "U-Net forward TFLOP/s (BF16 tensor cores)", "value": round(flops / fwd_ms / 1e9, 2),
+            "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(fwd_ms, 3), "higher_is_better": True, "dtype": "bf16 (fp32 accumulate)",
+            "data": "synthetic (random image)",
+            "config": {"workload": "U-Net preconditioner", "image": f"{h}x{w}", "base_channels": 32,
+                       "forward_gflop": round(flops / 1e9, 2), "train_step_ms": round(train_ms, 3)}}
+
+
 def run_lsrtm(args):
     """Learned vs plain acoustic CG-LSRTM on one GPU: training pairs (random reflectivity -> Born
     data -> RTM image, 512x256, 40 shots) made by this code, U-Net training on the GPU, then
@@ -713,9 +819,10 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
-    if args.workload == "lsrtm":
+    if args.workload in ("lsrtm", "acoustic", "unet"):
         if rank == 0:
-            print(json.dumps(run_lsrtm(args)))
+            fn = {"lsrtm": run_lsrtm, "acoustic": run_acoustic, "unet": run_unet}[args.workload]
+            print(json.dumps(fn(args)))
         return
     if world > 1:
         import datetime

@@ -85,6 +85,7 @@ def load():
         "ds2d_rtm": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp], ctypes.c_int),
         "ds2d_rtm_device": ([P, ctypes.POINTER(Shot), ctypes.c_int, P, P], ctypes.c_int),
         "ds2d_read_images": ([P, ctypes.POINTER(fp), ctypes.c_int], ctypes.c_int),
+        "ds2d_read_images_device": ([P, ctypes.POINTER(P), ctypes.c_int], ctypes.c_int),
         "ds2d_last_cell_updates": ([P], ctypes.c_double),
         "ds2d_last_launches": ([P], ctypes.c_longlong),
         "ds2d_profile": ([P, ctypes.c_int], ctypes.c_int),
@@ -110,6 +111,8 @@ def load():
         "ds2d_lsrtm": ([P, ctypes.POINTER(Shot), ctypes.c_int, fp, fp, ctypes.c_int,
                         ctypes.c_double, fp, dp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "ds2d_profile_report": ([P, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
+        "ds2d_bandpass_filter": ([ctypes.c_int] * 6 + [fp, fp], ctypes.c_int),
+        "ds2d_bandpass_filter_device": ([ctypes.c_int] * 6 + [P, P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -252,6 +252,19 @@ class Elastic2D:
         self._check(self.lib.ds2d_read_images(self.h, ptrs, int(bool(reset))))
         return out
 
+    def read_images_device(self, out, reset=True, which=None):
+        """Device read-out: copies the named images into `out` (a CUDA tensor [len(which)][allnx]
+        [allnz], FP32) on the context stream, then zeroes them when reset."""
+        which = self.IMAGE_NAMES if which is None else which
+        if tuple(out.shape) != (len(which), self.allnx, self.allnz) or not out.is_contiguous():
+            raise ValueError("out must be a contiguous [len(which)][allnx][allnz] tensor")
+        ptrs = (ctypes.c_void_p * 7)()
+        plane = self.allnx * self.allnz * 4
+        for i, k in enumerate(which):
+            ptrs[self.IMAGE_NAMES.index(k)] = out.data_ptr() + i * plane
+        self._check(self.lib.ds2d_read_images_device(self.h, ptrs, int(bool(reset))))
+        return out
+
     def set_option(self, key, value):
         """Tuning knob: "fused" (0/1) or "xr" (rows per CTA of the fused kernels)."""
         self._check(self.lib.ds2d_set_option(self.h, key.encode(), int(value)))
@@ -277,3 +290,27 @@ class Elastic2D:
     @property
     def last_launches(self):
         return self.lib.ds2d_last_launches(self.h)
+
+
+def bandpass_filter(grad_pp, grad_ps, z1, z2, x1=0, x2=0):
+    """Band-pass filter of two [nx][nz] gradient images (reference bandpass_filter,
+    FD2DGPU.cu:4125-4182) on the GPU; returns the filtered copies.  z1 = low cut-off (0: low-pass),
+    z2 = high cut-off; x1, x2 are unused, as in the reference's live filter."""
+    lib = _lib.load()
+    pp = _f32(grad_pp).copy()
+    ps = _f32(grad_ps).copy()
+    nx, nz = pp.shape
+    rc = lib.ds2d_bandpass_filter(nx, nz, int(x1), int(x2), int(z1), int(z2), _fptr(pp), _fptr(ps))
+    if rc != 0:
+        raise _lib.DS2DError(rc, lib.ds2d_last_error(None).decode())
+    return pp, ps
+
+
+def bandpass_filter_device(pp_ptr, ps_ptr, nx, nz, z1, z2, stream=0, x1=0, x2=0):
+    """In-place band-pass of two device images (either pointer may be 0) on `stream`."""
+    lib = _lib.load()
+    rc = lib.ds2d_bandpass_filter_device(nx, nz, int(x1), int(x2), int(z1), int(z2),
+                                         ctypes.c_void_p(pp_ptr or None),
+                                         ctypes.c_void_p(ps_ptr or None), ctypes.c_void_p(stream))
+    if rc != 0:
+        raise _lib.DS2DError(rc, lib.ds2d_last_error(None).decode())

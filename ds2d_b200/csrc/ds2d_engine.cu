@@ -260,10 +260,11 @@ struct ds2d_ctx {
   // "pair" (1 on where they apply, 0 off: the default until they beat the one-column kernels),
   // "pair_cta" (backward CTA width: 0 auto, 256 or 160), "pair_xr" (rows per CTA: 0 = chosen to
   // fill whole waves).
-  int opt_pair = 0, opt_pair_cta = 0, opt_pair_xr = 0;
+  int opt_pair = 0, opt_pair_cta = 0, opt_pair_fcta = 0, opt_pair_xr = 0;
   int *d_err = nullptr;      // error word raised by a pair kernel's bounded wait
   int num_sms = 148;
-  int occ_pair_fwd = 0, occ_pair_bwd256 = 0, occ_pair_bwd160 = 0;  // resident CTAs per SM
+  // resident CTAs per SM: forward 256 / 64, backward 256 / 160 / 64
+  int occ_pair[5] = {0, 0, 0, 0, 0};
   std::vector<int> h_nxp;    // padded window rows of each slot of the current batch
   int opt_pcg_switch = 970;  // ds2d_lsrtm_pcg: per-mille residual ratio that ends the network phase
   int opt_pcg_m = 8;         // ds2d_lsrtm_pcg: directions kept for explicit conjugation
@@ -608,28 +609,40 @@ void strip_split(const Dims &d, int cta, int *nstrips, int *tz) {
 }
 
 // ---- pair-blocked kernels (random boundary) ------------------------------------------------
-constexpr int kPairFwdT = 256, kPairFwdD = 4;  // forward: 256 threads, ring of 4 slots
-constexpr int kPairBwdD = 3;                   // backward: ring of 3 slots
+// CTA widths: 256 threads cover a whole 481-deep column (no z-halo recomputed) at 2 forward / 1
+// backward CTAs per SM; 64 threads (z-strips of 100 columns) give 8 forward / 4 backward CTAs per
+// SM, each barrier syncing two warps; 160 threads: two strips of a 481-deep column.
+constexpr int kPairFwdD = 4;  // forward ring: 4 slots
+constexpr int kPairBwdD = 3;  // backward ring: 3 slots
 using PairFwdFn = void (*)(FwdFusedArgs);
 using PairBwdFn = void (*)(BwdFusedArgs);
-PairFwdFn pair_fwd_fn() { return k_fwd_pair<kPairFwdT, kPairFwdD>; }
-PairBwdFn pair_bwd_fn(int cta) {
-  return cta == 160 ? k_bwd_pair<160, kPairBwdD, 2> : k_bwd_pair<256, kPairBwdD, 1>;
+PairFwdFn pair_fwd_fn(int cta) {
+  return cta == 64 ? k_fwd_pair<64, kPairFwdD, 8> : k_fwd_pair<256, kPairFwdD, 2>;
 }
-constexpr size_t kPairFwdSmem = pair_smem(kPairFwdT, kPairFwdD, kFwdPairFields, kFwdPairZ2);
+PairBwdFn pair_bwd_fn(int cta) {
+  return cta == 64    ? k_bwd_pair<64, kPairBwdD, 4>
+         : cta == 160 ? k_bwd_pair<160, kPairBwdD, 2>
+                      : k_bwd_pair<256, kPairBwdD, 1>;
+}
+constexpr size_t pair_fwd_smem(int cta) {
+  return pair_smem(cta, kPairFwdD, kFwdPairFields, kFwdPairZ2Rows);
+}
 constexpr size_t pair_bwd_smem(int cta) {
-  return pair_smem(cta, kPairBwdD, kBwdPairFields, kBwdPairZ2);
+  return pair_smem(cta, kPairBwdD, kBwdPairFields, kBwdPairZ2Rows);
 }
 
 bool pair_on(const ds2d_ctx *c) {
   return c->opt_pair && c->opt_fused && c->ring_ok && c->d.rbc && c->d.nop == 4 &&
-         c->d.ild == c->d.ld && c->d_err && c->occ_pair_fwd > 0;
+         c->d.ild == c->d.ld && c->d_err && c->occ_pair[0] > 0;
 }
-// Backward CTA width: the whole column in one 256-thread CTA when it fits (no z-halo recomputed),
-// else strips of 160-thread CTAs (two per SM).
-int pair_bwd_cta(const ds2d_ctx *c) {
-  if (c->opt_pair_cta == 160 || c->opt_pair_cta == 256) return c->opt_pair_cta;
-  return c->d.nzp + 16 <= 2 * 256 ? 256 : 160;
+// CTA widths (options "pair_cta" backward, "pair_fcta" forward; 0 = automatic): narrow 64-thread
+// strips by default (more CTAs per SM, barriers of two warps).
+int pair_bwd_cta(const ds2d_ctx *c) { return c->opt_pair_cta ? c->opt_pair_cta : 64; }
+int pair_fwd_cta(const ds2d_ctx *c) { return c->opt_pair_fcta ? c->opt_pair_fcta : 64; }
+// resident CTAs per SM of each variant (queried at create)
+int pair_occ(const ds2d_ctx *c, bool fwd, int cta) {
+  if (fwd) return cta == 64 ? c->occ_pair[1] : c->occ_pair[0];
+  return cta == 64 ? c->occ_pair[4] : cta == 160 ? c->occ_pair[3] : c->occ_pair[2];
 }
 // z-strips of a pair launch: each CTA computes tz (a multiple of 4) columns, 2 kT - 16 at most.
 void pair_split(const Dims &d, int kT, int *nstrips, int *tz) {
@@ -688,12 +701,13 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
     a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
     if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
     if (pair_on(c)) {
+      const int pc = pair_fwd_cta(c);
       int pns, ptz;
-      pair_split(d, kPairFwdT, &pns, &ptz);
-      const int pxr = pair_xr(c, pns, c->occ_pair_fwd);
+      pair_split(d, pc, &pns, &ptz);
+      const int pxr = pair_xr(c, pns, pair_occ(c, true, pc));
       a.tz = ptz; a.xr = pxr; a.err = c->d_err;
       dim3 pgrid(pns, (d.nxp + pxr - 1) / pxr, n);
-      LAUNCHS("fwd_pair", kBytesFused * CELLS(n), pair_fwd_fn(), pgrid, kPairFwdT, kPairFwdSmem, a);
+      LAUNCHS("fwd_pair", kBytesFused * CELLS(n), pair_fwd_fn(pc), pgrid, pc, pair_fwd_smem(pc), a);
     } else if (c->opt_ring && c->ring_ok) {
       const size_t sm = sizeof(float) * c->opt_ring * fwd_ring_fields(!d.rbc) * cta;
       FwdFn kfn = fwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ, cta);
@@ -826,7 +840,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64) + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -867,7 +881,7 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
         const int pc = pair_bwd_cta(c);
         int pns, ptz;
         pair_split(d, pc, &pns, &ptz);
-        const int pxr = pair_xr(c, pns, pc == 160 ? c->occ_pair_bwd160 : c->occ_pair_bwd256);
+        const int pxr = pair_xr(c, pns, pair_occ(c, false, pc));
         a.tz = ptz; a.xr = pxr; a.err = c->d_err;
         dim3 pgrid(pns, (d.nxp + pxr - 1) / pxr, n);
         LAUNCHS("bwd_pair", kBytesBwdFused * CELLS(n), pair_bwd_fn(pc), pgrid, pc,
@@ -1470,22 +1484,24 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
           }
         }
     }
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(pair_fwd_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kPairFwdSmem);
-    for (int pc : {160, 256})
-      if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(pair_bwd_fn(pc), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)pair_bwd_smem(pc));
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair_fwd, pair_fwd_fn(), kPairFwdT,
-                                                        kPairFwdSmem);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair_bwd256, pair_bwd_fn(256), 256,
-                                                        pair_bwd_smem(256));
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair_bwd160, pair_bwd_fn(160), 160,
-                                                        pair_bwd_smem(160));
+    {
+      const int fctas[2] = {256, 64}, bctas[3] = {256, 160, 64};
+      for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+        e = cudaFuncSetAttribute(pair_fwd_fn(fctas[i]), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_fwd_smem(fctas[i]));
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair[i], pair_fwd_fn(fctas[i]),
+                                                            fctas[i], pair_fwd_smem(fctas[i]));
+      }
+      for (int i = 0; i < 3 && e == cudaSuccess; i++) {
+        e = cudaFuncSetAttribute(pair_bwd_fn(bctas[i]), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_bwd_smem(bctas[i]));
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair[2 + i],
+                                                            pair_bwd_fn(bctas[i]), bctas[i],
+                                                            pair_bwd_smem(bctas[i]));
+      }
+    }
     int dev = 0;
     if (e == cudaSuccess) e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1607,7 +1623,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64) + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -1692,6 +1708,16 @@ int ds2d_read_images(ds2d_ctx *c, float *const images[7], int reset) {
       CK(cudaMemcpyAsync(images[a], c->images + a * n, n * 4, cudaMemcpyDeviceToHost, c->stream));
   if (reset) CK(cudaMemsetAsync(c->images, 0, 7 * n * 4, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return DS2D_OK;
+}
+
+int ds2d_read_images_device(ds2d_ctx *c, float *const images[7], int reset) {
+  if (!c || !images) return DS2D_E_ARG;
+  size_t n = (size_t)c->g.allnx * c->g.allnz;
+  for (int a = 0; a < 7; a++)
+    if (images[a])
+      CK(cudaMemcpyAsync(images[a], c->images + a * n, n * 4, cudaMemcpyDeviceToDevice, c->stream));
+  if (reset) CK(cudaMemsetAsync(c->images, 0, 7 * n * 4, c->stream));
   return DS2D_OK;
 }
 
@@ -2036,9 +2062,13 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "pair must be 0 or 1");
     c->opt_pair = (int)value;
   } else if (k == "pair_cta") {
-    if (value != 0 && value != 160 && value != 256)
-      return fail(c, DS2D_E_ARG, "pair_cta must be 0 (automatic), 160 or 256");
+    if (value != 0 && value != 64 && value != 160 && value != 256)
+      return fail(c, DS2D_E_ARG, "pair_cta must be 0 (automatic), 64, 160 or 256");
     c->opt_pair_cta = (int)value;
+  } else if (k == "pair_fcta") {
+    if (value != 0 && value != 64 && value != 256)
+      return fail(c, DS2D_E_ARG, "pair_fcta must be 0 (automatic), 64 or 256");
+    c->opt_pair_fcta = (int)value;
   } else if (k == "pair_xr") {
     if (value != 0 && (value < 8 || value > 4096))
       return fail(c, DS2D_E_ARG, "pair_xr must be 0 (automatic) or in [8, 4096]");

@@ -157,47 +157,37 @@ __device__ __forceinline__ void pair_exit(unsigned long long *bars, RingCursor<k
   }
 }
 
-// Copies of one ring slot: field f reads row (q - lag[f]) of an array whose rows are ld floats
-// apart (wavefields, parameters and the per-slot images alike), if that row lies in
-// [lo[f], hi[f]).  The strip's columns [zs - 8, zs - 8 + 2 kT) map to ring floats 4 .. 2 kT + 4;
-// the copy is clipped to [0, ld) (the row's own allocation).
-template <int NF>
-struct SlotPlan {
-  const float *src[NF];  // slot-0 row-0 pointer of each field's array (image rows: see below)
-  int lag[NF], lo[NF], hi[NF];
-  int row0[NF];          // array row of grid row x is x + row0 (image rows: x - pml)
-  bool img[NF];          // per-slot image rows (slot offset ibase) instead of field rows (fbase)
+// Copies of one ring slot, issued by the 32 lanes of one warp at once: lane f (f < NF) owns ring
+// field f, which reads row (q - lag) of an array whose rows are ld floats apart (wavefields,
+// parameters and the per-slot images alike) if that row lies in [lo, hi).  The strip's columns
+// [zs - 8, zs - 8 + 2 kT) map to ring floats 4 .. 2 kT + 4; the copy is clipped to [0, ld) (the
+// row's own allocation).  Lane 0 arrives on the slot's barrier with the bytes of all the copies
+// (counted by ballot) before any is issued, so the phase cannot complete early.
+struct RingField {
+  const float *src;  // this lane's field: array row x starts at src + x * ld (0 for lanes >= NF)
+  int lag, lo, hi;
 };
 
-template <int NF, int kT>
-__device__ __forceinline__ void issue_slot(const SlotPlan<NF> &pl, float *slot_base,
-                                           unsigned long long *bar, int q, long long fbase,
-                                           long long ibase, int ld, int zs) {
+template <int kT>
+__device__ __forceinline__ void issue_slot_warp(const RingField &fd, float *slot_base, int f,
+                                                unsigned long long *bar, int q, int ld, int zs,
+                                                int lane) {
   const int glo = max(0, zs - 8), ghi = min(ld, zs - 8 + 2 * kT);
   const unsigned bytes = (unsigned)(ghi - glo) * 4u;
-  const int dst_off = glo - (zs - 8) + 4;
-  unsigned total = 0;
-#pragma unroll
-  for (int f = 0; f < NF; f++) {
-    const int row = q - pl.lag[f];
-    if (row >= pl.lo[f] && row < pl.hi[f]) total += bytes;
-  }
-  mbar_arrive_tx(bar, total);
-#pragma unroll
-  for (int f = 0; f < NF; f++) {
-    const int row = q - pl.lag[f];
-    if (row >= pl.lo[f] && row < pl.hi[f]) {
-      const long long base = pl.img[f] ? ibase : fbase;
-      bulk_g2s(slot_base + f * pair_row(kT) + dst_off,
-               pl.src[f] + base + (long long)(row + pl.row0[f]) * ld + glo, bytes, bar);
-    }
-  }
+  const int row = q - fd.lag;
+  const bool mine = fd.src != nullptr && row >= fd.lo && row < fd.hi;
+  const unsigned n = __popc(__ballot_sync(0xffffffffu, mine));
+  if (lane == 0) mbar_arrive_tx(bar, n * bytes);
+  __syncwarp();
+  if (mine)
+    bulk_g2s(slot_base + f * pair_row(kT) + (glo - (zs - 8) + 4),
+             fd.src + (long long)row * ld + glo, bytes, bar);
 }
 
-// Shared-memory bytes of a pair kernel: the ring, the stage-2 z-tap rows (double-buffered), the
-// slot barriers and the receiver staging.
-__host__ __device__ constexpr size_t pair_smem(int kT, int kD, int NF, int NZ2) {
-  return sizeof(float) * ((size_t)kD * NF + 2 * NZ2) * pair_row(kT) + 8 * 8 + 6 * 16 * 4;
+// Shared-memory bytes of a pair kernel: the ring, `rows` rows of stage-2 z-taps, the slot
+// barriers and the receiver staging.
+__host__ __device__ constexpr size_t pair_smem(int kT, int kD, int NF, int rows) {
+  return sizeof(float) * ((size_t)kD * NF + rows) * pair_row(kT) + 8 * 8 + 6 * 16 * 4;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -209,14 +199,15 @@ __host__ __device__ constexpr size_t pair_smem(int kT, int kD, int NF, int NZ2) 
 //   7 txx(r-8)  8 tzz(r-8)  9 lam(r-8)  10 mu(r-8)   stage-2 own cells (txz(r-8) is w_txz[0])
 constexpr int kFwdPairFields = 11;
 constexpr int kFwdPairZ2 = 2;  // stage-2 z-tap rows: vx, vz of row r-8
+constexpr int kFwdPairZ2Rows = 2 * kFwdPairZ2;  // double-buffered
 
-template <int kT, int kD>
-__global__ void __launch_bounds__(kT, 2) k_fwd_pair(FwdFusedArgs a) {
+template <int kT, int kD, int kMinB>
+__global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
   constexpr int NF = kFwdPairFields, ROW = pair_row(kT);
   extern __shared__ __align__(16) float smem[];
   float *ring = smem;                               // [kD][NF][ROW]
   float *z2 = ring + (size_t)kD * NF * ROW;         // [2][kFwdPairZ2][ROW]
-  unsigned long long *bars = (unsigned long long *)(z2 + 2 * kFwdPairZ2 * ROW);
+  unsigned long long *bars = (unsigned long long *)(z2 + kFwdPairZ2Rows * ROW);
   int *s_tr = (int *)(bars + 8);                    // receiver staging [16]
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
@@ -240,20 +231,19 @@ __global__ void __launch_bounds__(kT, 2) k_fwd_pair(FwdFusedArgs a) {
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
 
-  SlotPlan<NF> pl;
+  // ring field of this lane (warp 0 issues the copies; lane f owns field f)
+  const int lane = t & 31;
+  RingField fd{nullptr, 0, 0, d.nxp};
   {
     const float *src[NF] = {a.a.txx, a.a.txz, a.a.txz, a.a.tzz, a.a.vx, a.a.vz,
                             a.p.b,   a.a.txx, a.a.tzz, a.p.lam, a.p.mu};
     const int lag[NF] = {0, 1, 4, 4, 4, 4, 4, 8, 8, 8, 8};
 #pragma unroll
-    for (int f = 0; f < NF; f++) {
-      pl.src[f] = src[f];
-      pl.lag[f] = lag[f];
-      pl.lo[f] = 0;
-      pl.hi[f] = d.nxp;
-      pl.row0[f] = 0;
-      pl.img[f] = false;
-    }
+    for (int f = 0; f < NF; f++)
+      if (lane == f) {
+        fd.src = src[f] + fbase;
+        fd.lag = lag[f];
+      }
   }
   if (t == 0) {
     for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
@@ -261,9 +251,9 @@ __global__ void __launch_bounds__(kT, 2) k_fwd_pair(FwdFusedArgs a) {
   }
   __syncthreads();
   const int rs0 = x0 - 8;
-  if (t == 0)
+  if (t < 32)
     for (int j = 0; j < kD - 1; j++)
-      issue_slot<NF, kT>(pl, ring + (size_t)j * NF * ROW, &bars[j], rs0 + j, fbase, 0, ld, zs);
+      issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], rs0 + j, ld, zs, lane);
 
   float2 w_txx[8], w_txz[8], w_vx[9], w_vz[8];
 #pragma unroll
@@ -346,10 +336,10 @@ __global__ void __launch_bounds__(kT, 2) k_fwd_pair(FwdFusedArgs a) {
       break;
     }
     // every thread is done with the previous slot: refill it kD - 1 steps ahead
-    if (t == 0) {
+    if (t < 32) {
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
-      issue_slot<NF, kT>(pl, ring + (size_t)ps * NF * ROW, &bars[ps], r + kD - 1, fbase, 0, ld,
-                         zs);
+      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps], r + kD - 1, ld, zs,
+                          lane);
     }
     // ---- stage 2: stresses of row rs = r - 8 ------------------------------------------------
     const int rs = r - 8;
@@ -406,15 +396,19 @@ __global__ void __launch_bounds__(kT, 2) k_fwd_pair(FwdFusedArgs a) {
 // (bvx(r-8) is w_bvx[0]; the adjoint own velocities come from the ring because the windows carry
 // the residual.)
 constexpr int kBwdPairFields = 25;
-constexpr int kBwdPairZ2 = 4;  // stage-2 z-tap rows: btxz, btzz, M, PzLx of row r-8
+// Stage-2 z-tap rows btxz, btzz, M, PzLx, written by stage 1 for its row and read by stage 2 four
+// steps later: a circular buffer of 6 rows (rows r-9 .. r-4 are distinct slots, so the write of
+// step r never meets a read of step r-1 still in flight).
+constexpr int kBwdPairZ2 = 4, kBwdPairZDepth = 6;
+constexpr int kBwdPairZ2Rows = kBwdPairZ2 * kBwdPairZDepth;
 
 template <int kT, int kD, int kMinB>
 __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   constexpr int NF = kBwdPairFields, ROW = pair_row(kT);
   extern __shared__ __align__(16) float smem[];
   float *ring = smem;
-  float *z2 = ring + (size_t)kD * NF * ROW;
-  unsigned long long *bars = (unsigned long long *)(z2 + 2 * kBwdPairZ2 * ROW);
+  float *zc = ring + (size_t)kD * NF * ROW;  // [kBwdPairZDepth][kBwdPairZ2][ROW]
+  unsigned long long *bars = (unsigned long long *)(zc + kBwdPairZ2Rows * ROW);
   int *s_tr = (int *)(bars + 8);
   int *s_has = s_tr + 16;
   float *s_rz = (float *)(s_has + 16), *s_rx = s_rz + 16;
@@ -443,7 +437,8 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
   float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
 
-  SlotPlan<NF> pl;
+  const int lane = t & 31;
+  RingField fd{nullptr, 0, 0, d.nxp};
   {
     const float *src[NF] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.vx,  a.ra.vz,  a.aa.vx,
                             a.aa.vz,  a.ra.txx, a.ra.tzz, a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz,
@@ -451,15 +446,15 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
                             a.ra.vz,  a.aa.vx,  a.aa.vz,  img_il};
     const int lag[NF] = {1, 0, 1, 0, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 8, 8, 8, 8, 8};
 #pragma unroll
-    for (int f = 0; f < NF; f++) {
-      const bool img = f == 18 || f == 19 || f == 24;
-      pl.src[f] = src[f];
-      pl.lag[f] = lag[f];
-      pl.lo[f] = img ? pml : 0;
-      pl.hi[f] = img ? d.nxp - pml : d.nxp;
-      pl.row0[f] = img ? -pml : 0;
-      pl.img[f] = img;
-    }
+    for (int f = 0; f < NF; f++)
+      if (lane == f) {
+        const bool img = f == 18 || f == 19 || f == 24;
+        // image rows: grid row x is image row x - pml of the slot's plane
+        fd.src = img ? src[f] + ibase - (long long)pml * ld : src[f] + fbase;
+        fd.lag = lag[f];
+        fd.lo = img ? pml : 0;
+        fd.hi = img ? d.nxp - pml : d.nxp;
+      }
   }
   if (t == 0) {
     for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
@@ -479,21 +474,20 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   }
   __syncthreads();
   const int rs0 = x0 - 8;
-  if (t == 0)
+  if (t < 32)
     for (int j = 0; j < kD - 1; j++)
-      issue_slot<NF, kT>(pl, ring + (size_t)j * NF * ROW, &bars[j], rs0 + j, fbase, ibase, ld, zs);
+      issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], rs0 + j, ld, zs, lane);
 
   float2 w_bvx[8], w_bvz[8], w_avx[8], w_avz[8];     // stage-1 x-windows
   float2 w_btxx[8], w_btxz[9], w_PL[8], w_M[9];       // stage-2 x-windows
-  float2 w_btzz[5], w_PzLx[5];                        // stage-2 z-tap rows, 4 steps deep
   const float2 zero2 = make_float2(0.f, 0.f);
 #pragma unroll
   for (int i = 0; i < 8; i++)
     w_bvx[i] = w_bvz[i] = w_avx[i] = w_avz[i] = w_btxx[i] = w_PL[i] = zero2;
 #pragma unroll
   for (int i = 0; i < 9; i++) w_btxz[i] = w_M[i] = zero2;
-#pragma unroll
-  for (int i = 0; i < 5; i++) w_btzz[i] = w_PzLx[i] = zero2;
+  // circular z-tap slot of stage 1's row r-4 (stage 2 reads row r-8, two slots further on)
+  int zw = ((rs0 - 4) % kBwdPairZDepth + kBwdPairZDepth) % kBwdPairZDepth;
 
   RingCursor<kD> cur;
   bool ok = true, aborted = false;
@@ -637,24 +631,26 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
     }
     push2(w_btxx, btxx);
     push2(w_btxz, btxz);
-    push2(w_btzz, btzz);
     push2(w_PL, PL);
     push2(w_M, M);
-    push2(w_PzLx, PzLx);
-    // ---- stage-2 z-tap rows of row r - 8, the step's barrier, the refill -----------------------
-    float *zb = z2 + (r & 1) * kBwdPairZ2 * ROW;
-    reinterpret_cast<float2 *>(zb)[pi] = w_btxz[4];
-    reinterpret_cast<float2 *>(zb + ROW)[pi] = w_btzz[0];
-    reinterpret_cast<float2 *>(zb + 2 * ROW)[pi] = w_M[4];
-    reinterpret_cast<float2 *>(zb + 3 * ROW)[pi] = w_PzLx[0];
+    {  // z-tap rows of row r - 4 for stage 2 four steps on
+      float *zwb = zc + zw * kBwdPairZ2 * ROW;
+      reinterpret_cast<float2 *>(zwb)[pi] = btxz;
+      reinterpret_cast<float2 *>(zwb + ROW)[pi] = btzz;
+      reinterpret_cast<float2 *>(zwb + 2 * ROW)[pi] = M;
+      reinterpret_cast<float2 *>(zwb + 3 * ROW)[pi] = PzLx;
+    }
+    const float *zb = zc + (zw >= kBwdPairZDepth - 2 ? zw - (kBwdPairZDepth - 2) : zw + 2) * kBwdPairZ2 * ROW;
+    zw = zw == kBwdPairZDepth - 1 ? 0 : zw + 1;
+    // ---- the step's barrier, the refill -------------------------------------------------------
     if (__syncthreads_or(!ok)) {
       aborted = true;
       break;
     }
-    if (t == 0) {
+    if (t < 32) {
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
-      issue_slot<NF, kT>(pl, ring + (size_t)ps * NF * ROW, &bars[ps], r + kD - 1, fbase, ibase,
-                         ld, zs);
+      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps], r + kD - 1, ld, zs,
+                          lane);
     }
     // ---- stage 2: velocities of row r2 = r - 8, illumination ---------------------------------
     const int r2 = r - 8;

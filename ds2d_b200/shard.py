@@ -58,6 +58,17 @@ def reduce_images(images, dist, device="cpu"):
     return {k: out[i] for i, k in enumerate(names)}
 
 
+def reduce_images_device(ctx, dist, buf, which=("pp_grad", "ps_grad", "illumination")):
+    """The GPU path of the reduction: the context's images are copied device to device into
+    `buf` (a CUDA tensor [len(which)][allnx][allnz]) and summed over all ranks by one in-place
+    NCCL all-reduce; nothing crosses PCIe.  The context stream must be torch's current stream
+    (or synchronised with it) so the all-reduce sees the copies."""
+    ctx.read_images_device(buf, reset=True, which=which)
+    if dist is not None:
+        dist.all_reduce(buf)
+    return buf
+
+
 def reduce_scalar_f64(value, dist, device="cpu"):
     """FP64 sum of one scalar over all ranks (misfit, CG dot products)."""
     if dist is None:

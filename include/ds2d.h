@@ -116,6 +116,12 @@ int ds2d_rtm_device(ds2d_ctx *ctx, const ds2d_shot *shots, int n, const float *a
  * host arrays that are not NULL, then zeroes them when reset != 0. */
 int ds2d_read_images(ds2d_ctx *ctx, float *const images[7], int reset);
 
+/* The same read-out into DEVICE arrays (no counterpart in the reference, whose gradients cross
+ * to the host and MPI_Reduce there, main.cpp:1038-1060): the non-NULL images are copied device
+ * to device on the context stream, then zeroed when reset != 0; returns without synchronising.
+ * For one process per GPU, the caller all-reduces those arrays in place over NCCL. */
+int ds2d_read_images_device(ds2d_ctx *ctx, float *const images[7], int reset);
+
 /* Cell-updates performed by the last ds2d_forward / ds2d_elsrtm / ds2d_rtm call (padded cells x
  * steps x propagations), for throughput reporting. */
 double ds2d_last_cell_updates(const ds2d_ctx *ctx);

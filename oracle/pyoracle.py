@@ -210,6 +210,50 @@ def ac_born_adj(st, model, wavelet, shot, rz, rx):
     return g
 
 
+def gaussian_bandpass(nx, nz, low, high):
+    """construct_gaussian_bandpass_filter(filter, width = nz, height = nx, low, high) as the
+    reference's bandpass_filter calls it (FD2DGPU.cu:4038-4077, :4135): FP32 distance with the
+    width / height scale on the x offset, FP64 exponentials stored as FP32, clamped at 0,
+    normalised to a maximum of 1; low == 0 is the low-pass form.  [nx][nz]."""
+    cx, cy = nz // 2, nx // 2
+    dz = (np.arange(nz) - cx)[None, :]
+    dx = (np.arange(nx) - cy)[:, None]
+    scale = np.float32(np.float32(nz) / np.float32(nx))
+    t = (scale * dx.astype(np.float32)).astype(np.float32)
+    dist = np.sqrt((dz * dz).astype(np.float32) + t * t).astype(np.float32)
+    d2 = ((-dist) * dist).astype(np.float64)
+    if low == 0:
+        g = np.exp(d2 / (2.0 * high * high)).astype(np.float32)
+    else:
+        g = (np.exp(d2 / (2.0 * high * high)) - np.exp(d2 / (2.0 * low * low))).astype(np.float32)
+    g = np.where(g < 0, np.float32(0), g).astype(np.float32)
+    return (g / g.max()).astype(np.float32)
+
+
+def quadrant_swap(a):
+    """fft_shift / ifft_shift of FD2DGPU.cu:3922-3965 on [nx][nz]: quadrant (y, x) <-> (y + nx/2,
+    x + nz/2) and (y, x + nz/2) <-> (y + nx/2, x) for y < nx/2, x < nz/2 (odd sizes keep the last
+    row and column in place)."""
+    nx, nz = a.shape
+    hx, hz = nx // 2, nz // 2
+    out = a.copy()
+    out[:hx, :hz], out[hx:2 * hx, hz:2 * hz] = a[hx:2 * hx, hz:2 * hz], a[:hx, :hz]
+    out[:hx, hz:2 * hz], out[hx:2 * hx, :hz] = a[hx:2 * hx, :hz], a[:hx, hz:2 * hz]
+    return out
+
+
+def bandpass(img, z1, z2):
+    """The reference's bandpass_filter (FD2DGPU.cu:4125-4182) on one [nx][nz] image, step by
+    step in FP64: FFT2 (cuFFT Z2Z forward, unnormalised), quadrant swap, multiply by the complex
+    number (k, k) (GPU_lowpass), swap back, inverse FFT2, divide by nx*nz, real part as FP32."""
+    nx, nz = img.shape
+    k = gaussian_bandpass(nx, nz, z1, z2).astype(np.float64)
+    f = np.fft.fft2(np.asarray(img, np.float64))
+    f = quadrant_swap(f) * (k + 1j * k)
+    g = np.fft.ifft2(quadrant_swap(f))  # numpy's inverse includes the 1 / (nx nz) of GPU_divide
+    return g.real.astype(np.float32)
+
+
 def ricker(nt, f0, dt):
     s = np.zeros(nt, np.float32)
     lib().orc_ricker(nt, f0, dt, _p(s))
@@ -258,6 +302,7 @@ def ref_lib():
         L.ref_born.argtypes = [I, I, I, I, I, F, F, F, fp, fp, fp, fp, fp, I, I, I, I, I, ip, I,
                                fp, fp, fp, fp]
         L.ref_release.argtypes = []
+        L.ref_bandpass.argtypes = [I, I, I, I, I, I, fp, fp]
         _ref = L
     return _ref
 
@@ -289,6 +334,17 @@ def ref_born(allnx, allnz, nx, pml, nt, dx, dz, dt, vp, vs, wavelet, img_pp, img
     if rc != 0:
         raise RuntimeError(f"ref_born: CUDA error {rc}")
     return rz, rx
+
+
+def ref_bandpass(img_pp, img_ps, z1, z2, x1=0, x2=0):
+    """The reference's own bandpass_filter (cuFFT) on two [nx][nz] images; returns copies."""
+    pp = np.array(img_pp, np.float32, order="C")
+    ps = np.array(img_ps, np.float32, order="C")
+    nx, nz = pp.shape
+    rc = ref_lib().ref_bandpass(nx, nz, x1, x2, z1, z2, _p(pp), _p(ps))
+    if rc != 0:
+        raise RuntimeError(f"ref_bandpass: CUDA error {rc}")
+    return pp, ps
 
 
 def ref_release():

@@ -337,6 +337,12 @@ int ref_born(int allnx, int allnz, int nx, int pml, int nt, float dx, float dz, 
   return last_error();
 }
 
+// The reference's gradient band-pass filter itself (FD2DGPU.cu:4125-4182, cuFFT), host arrays.
+int ref_bandpass(int nx, int nz, int x1, int x2, int z1, int z2, float *pp, float *ps) {
+  bandpass_filter(nx, nz, x1, x2, z1, z2, pp, ps);
+  return last_error();
+}
+
 // Frees the cached reference object (and its strip buffers).
 int ref_release() {
   release_strips();

@@ -99,6 +99,23 @@ def make_born(outdir):
                         rec_vx=np.stack([r[1] for r in recs]), **common)
 
 
+BANDPASS_CASES = [(80, 40, 0, 8), (81, 41, 3, 12), (121, 41, 0, 10)]  # nx, nz, z1, z2
+
+
+def make_bandpass(outdir):
+    """The reference's bandpass_filter (cuFFT) on seeded random images: even and odd sizes, the
+    low-pass (z1 = 0) and band-pass forms."""
+    rng = np.random.default_rng(41)
+    out = {}
+    for i, (nx, nz, z1, z2) in enumerate(BANDPASS_CASES):
+        pp = rng.standard_normal((nx, nz)).astype(np.float32)
+        ps = rng.standard_normal((nx, nz)).astype(np.float32)
+        fpp, fps = po.ref_bandpass(pp, ps, z1, z2)
+        out.update({f"in_pp{i}": pp, f"in_ps{i}": ps, f"out_pp{i}": fpp, f"out_ps{i}": fps})
+    np.savez_compressed(os.path.join(outdir, "bandpass.npz"),
+                        cases=np.array(BANDPASS_CASES, np.int32), **out)
+
+
 def main(outdir):
     os.makedirs(outdir, exist_ok=True)
     c = CASE
@@ -152,7 +169,7 @@ if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--only")]
     only = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")), None)
     out = args[0] if args else os.path.dirname(os.path.abspath(__file__))
-    makers = {"base": main, "c1": make_c1, "born": make_born}
+    makers = {"base": main, "c1": make_c1, "born": make_born, "bandpass": make_bandpass}
     for name in (only.split(",") if only else list(makers)):
         makers[name](out)
     print("golden fixtures written to", out)

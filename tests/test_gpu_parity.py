@@ -419,13 +419,14 @@ def test_live_reference_rtm_random(cuda_device):
         assert err < gate(floor), f"{key}: vs reference {err:.3e}, FP32 floor {floor:.3e}"
 
 
-@pytest.mark.parametrize("pair_cta", [160, 256])
+@pytest.mark.parametrize("pair_cta,pair_fcta", [(64, 64), (256, 256), (160, 64)])
 @pytest.mark.parametrize("pair_xr", [0, 24])
-def test_pair_kernels_match_ring_and_oracle(cuda_device, pair_cta, pair_xr):
+def test_pair_kernels_match_ring_and_oracle(cuda_device, pair_cta, pair_fcta, pair_xr):
     """Pair-blocked bulk-copy kernels of the random-boundary RTM step (forward with receiver
     records, backward with the residual injection and the imaging condition) against the
-    one-column ring kernels and the FP64 oracle.  The 320-deep grid makes the 160-thread CTAs run
-    two z-strips; xr 24 gives each shot four row blocks (x-halos between CTAs)."""
+    one-column ring kernels and the FP64 oracle.  On the 320-deep grid the 64-thread CTAs run four
+    z-strips and the 160-thread ones two; xr 24 gives each shot four row blocks (x-halos between
+    CTAs)."""
     c, _, _, w, _ = small_case(nt=200)
     c["allnz"] = 300
     vp, vs = synth.layered(c["allnx"], c["allnz"], seed=4)
@@ -441,6 +442,7 @@ def test_pair_kernels_match_ring_and_oracle(cuda_device, pair_cta, pair_xr):
             e.set_option("pair", pair)
             if pair:
                 e.set_option("pair_cta", pair_cta)
+                e.set_option("pair_fcta", pair_fcta)
                 e.set_option("pair_xr", pair_xr)
             e.set_models(vpm, vsm)
             e.set_wavelet(w)

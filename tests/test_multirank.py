@@ -9,7 +9,8 @@ import pytest
 import torch.multiprocessing as mp
 
 from ds2d_b200 import synth
-from ds2d_b200.shard import reduce_images, reduce_scalar_f64, shard_loads, shard_shots
+from ds2d_b200.shard import (reduce_images, reduce_images_device, reduce_scalar_f64, shard_loads,
+                             shard_shots)
 from oracle import pyoracle as po
 
 ALLNX, ALLNZ, PML, NT, DX, DT = 48, 24, 8, 80, 10.0, 0.0008
@@ -56,8 +57,21 @@ def _rank_main(rank, world, port, outdir):
         imgs, misfit = _images_of(mine, vp, vs, shots, w, adj)
         red = reduce_images({k: v.astype(np.float32) for k, v in imgs.items()}, dist)
         mis = reduce_scalar_f64(misfit, dist)
+        # the in-place path the GPU ranks take (device read-out, then one all-reduce of the
+        # buffer), with a stand-in context whose read-out fills the buffer from this rank's sums
+        import torch
+
+        class _Ctx:
+            def read_images_device(self, out, reset=True, which=None):
+                for i, k in enumerate(which):
+                    out[i].copy_(torch.from_numpy(imgs[k].astype(np.float32)))
+                return out
+
+        buf = torch.zeros((3, ALLNX, ALLNZ), dtype=torch.float32)
+        reduce_images_device(_Ctx(), dist, buf, which=("pp", "ps", "il"))
         if rank == 0:
-            np.savez(os.path.join(outdir, "red.npz"), misfit=mis, **red)
+            np.savez(os.path.join(outdir, "red.npz"), misfit=mis,
+                     dev=buf.numpy(), **red)
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -88,7 +102,8 @@ def test_two_gloo_ranks_reduce_to_single_process_images(tmp_path):
         p.join(timeout=300)
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
     got = np.load(tmp_path / "red.npz")
-    for k in ("pp", "ps", "il"):
+    for i, k in enumerate(("pp", "ps", "il")):
         ref = want[k].astype(np.float32)
         assert np.linalg.norm(got[k] - ref) <= 1e-6 * np.linalg.norm(ref)
+        assert np.linalg.norm(got["dev"][i] - ref) <= 1e-6 * np.linalg.norm(ref)
     assert abs(float(got["misfit"]) - want_mis) <= 1e-12 * abs(want_mis)

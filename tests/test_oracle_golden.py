@@ -112,3 +112,12 @@ def test_born_golden(name):
         if acoustic:
             az, ax = po.ac_born(st, m, fx["wavelet"], s, dmp)
             assert rel(az, b64[0]) < 1e-10 and rel(ax, b64[1]) < 1e-10
+
+
+def test_bandpass_golden():
+    """The FP64 restatement of the reference's band-pass filter against its cuFFT results."""
+    fx = _need("bandpass.npz")
+    for i, (nx, nz, z1, z2) in enumerate(fx["cases"]):
+        for key in ("pp", "ps"):
+            got = po.bandpass(fx[f"in_{key}{i}"], int(z1), int(z2))
+            assert rel(got, fx[f"out_{key}{i}"]) < 1e-6, (i, key, rel(got, fx[f"out_{key}{i}"]))
