@@ -65,6 +65,11 @@ def parse():
                         "network's forward pass and training step on one 2008x608 image")
     p.add_argument("--lsrtm-size", default="full", choices=["small", "full"],
                    help="full: 2001x601, 80 shots, nt 5000; small: 512x256, 40 shots, nt 2000")
+    p.add_argument("--lsrtm-boundary", default="random", choices=["random", "pml"],
+                   help="boundary of the LSRTM operators: random band (exact background "
+                        "reversal) or the reference's PML with the background rebuilt from strips")
+    p.add_argument("--lsrtm-strips", default="bf16", choices=["f32", "f16", "bf16"],
+                   help="storage of the background's boundary strips with --lsrtm-boundary pml")
     p.add_argument("--pairs", type=int, default=192, help="training pairs of the preconditioner")
     p.add_argument("--train-steps", type=int, default=2000)
     p.add_argument("--trajectory", type=int, default=16,
@@ -647,12 +652,38 @@ def run_acoustic(args):
         ev1.record(stream)
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1)
-    return {"metric": "Gcell-updates/s (acoustic L^T L)", "value": round(upd * args.steps / ms / 1e6, 3),
+    out = {"metric": "Gcell-updates/s (acoustic L^T L)", "value": round(upd * args.steps / ms / 1e6, 3),
             "unit": "Gcell-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (linear 1800-4500 m/s background, seeded sparse reflectivity)",
             "config": {"workload": "acoustic normal operator L^T L", "grid": "2001x601 (+20 band)",
                        "shots": nshots, "nt": nt, "cell_updates_per_step": upd}}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_acoustic(allnx, allnz, band, vp, w, shots[0])
+    return out
+
+
+def cpu_baseline_acoustic(allnx, allnz, pml, vp, w, shot):
+    """The reference's own CPU acoustic stepper (main.cpp:602-727, OpenMP on all host threads) on
+    the same padded grid with a 20-cell PML, a bounded number of steps (about 10 s of host work,
+    from a 20-step probe); cell-updates per second of one propagation."""
+    from oracle import pyoracle as po
+    if not po.ref_available():
+        return None
+    st = po.Setup(allnx, allnz, allnx, pml, 10.0, 10.0, 0.0008)
+    m = po.build_model(st, vp, 0 * vp, None, shot.win_left)
+    damp = np.maximum(m[5], m[6])
+    wave = np.tile(w, 200)  # long enough for any sample length
+    _, probe = po.ref_cpu_acoustic(m[0], m[2], damp, wave[:20], shot.isx, shot.isz, 0.0008, 10.0, 10.0)
+    steps = int(min(3000, max(50, 20 * 6.0 / max(probe, 1e-3))))
+    _, sec = po.ref_cpu_acoustic(m[0], m[2], damp, wave[:steps], shot.isx, shot.isz, 0.0008, 10.0,
+                                 10.0)
+    cells = m[0].size
+    return {"value": round(cells * steps / sec / 1e9, 4), "unit": "Gcell-updates/s",
+            "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"the reference's staggered_grid_extrapolation_2d_pml (main.cpp:602), one "
+                      f"acoustic propagation on the {m[0].shape[0]}x{m[0].shape[1]} padded grid, "
+                      f"{steps} steps, OpenMP on {os.cpu_count()} threads, {sec:.1f} s"}
 
 
 def run_unet(args):
@@ -717,8 +748,9 @@ def run_lsrtm(args):
     else:
         tnx, tnz, tnt, tshots = 512, 256, 2000, 40
     tr_shots = synth.surface_shots(tnx, tnx, band, tshots)
-    et = Elastic2D(tnx, tnz, tnx, band, tnt, dx, dx, dt, boundary="random", max_shots=tshots,
-                   max_ntr=tnx, seed=7, device=dev)
+    bkw = dict(boundary=args.lsrtm_boundary, strips=args.lsrtm_strips)
+    et = Elastic2D(tnx, tnz, tnx, band, tnt, dx, dx, dt, max_shots=tshots, max_ntr=tnx, seed=7,
+                   device=dev, **bkw)
     vpt = precond.background(tnx, tnz, seed=1)
     et.set_models(vpt, np.zeros_like(vpt))
     et.set_wavelet(synth.ricker(tnt, f0, dt))
@@ -746,8 +778,8 @@ def run_lsrtm(args):
     del X, Y
     # ---- application: observed Born data of a sparse random reflectivity -------------------
     shots = synth.surface_shots(anx, anx, band, ashots)
-    ea = Elastic2D(anx, anz, anx, band, ant, dx, dx, dt, boundary="random", max_shots=ashots,
-                   max_ntr=anx, seed=9, device=dev)
+    ea = Elastic2D(anx, anz, anx, band, ant, dx, dx, dt, max_shots=ashots, max_ntr=anx, seed=9,
+                   device=dev, **bkw)
     vpa = precond.background(anx, anz, seed=2)
     ea.set_models(vpa, np.zeros_like(vpa))
     ea.set_wavelet(synth.ricker(ant, f0, dt))
@@ -792,7 +824,9 @@ def run_lsrtm(args):
             "value": round(speedup, 3) if speedup else None, "unit": "x", "basis": basis,
             "higher_is_better": True, "n_gpus": 1, "dtype": "f32 stencils, bf16 network, f64 CG",
             "data": "synthetic (seeded sparse reflectivity on a smooth 1800-4500 m/s background)",
-            "config": {"workload": "acoustic CG-LSRTM", "grid": f"{anx}x{anz} (+{band} band)",
+            "config": {"workload": "acoustic CG-LSRTM", "grid": f"{anx}x{anz} (+{band} "
+                       + ("random band)" if args.lsrtm_boundary == "random" else
+                          f"PML, {args.lsrtm_strips} boundary strips with FP32 scales)"),
                        "shots": ashots, "nt": ant, "cg_iterations": args.cg_iters,
                        "target": args.target},
             "plain": res["plain"], "learned": res["learned"],

@@ -4,8 +4,8 @@ launches are fixed 32x32 blocks).
 The knobs are the rows marched per CTA (`xr`), the depth of the cp.async prefetch ring (`ring`),
 the register / occupancy target (`occ`) and the threads per CTA (`cta`, 128 or 192) of the
 one-column ring kernels, and, for the random boundary, the pair-blocked bulk-copy kernels
-(`pair`) with their CTA widths (`pair_cta` backward, `pair_fcta` forward) and rows per CTA
-(`pair_xr`).  Their best values depend on the grid, the number of
+(`pair`) with their CTA widths (`pair_cta` backward, `pair_fcta` forward), rows per CTA
+(`pair_xr`) and the backward step fused or split in two launches (`pair_split`).  Their best values depend on the grid, the number of
 resident shots and the boundary, so the tuner times each candidate on a probe context with the
 caller's grid and batch but only `probe_nt` time steps (an RTM of the same shots: one forward and
 one backward fused launch per step), and returns the fastest setting; `apply` copies it onto the
@@ -14,7 +14,7 @@ import numpy as np
 
 from .api import Elastic2D
 
-_RING_BASE = {"pair": 0, "pair_cta": 0, "pair_fcta": 0, "pair_xr": 0}
+_RING_BASE = {"pair": 0, "pair_split": 0, "pair_cta": 0, "pair_fcta": 0, "pair_xr": 0}
 _RING_SPACE = [
     {"ring": 4, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 0, "cta": 192},
     {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 192},
@@ -22,8 +22,10 @@ _RING_SPACE = [
 ]
 # Pair-blocked kernels (random boundary only): backward CTA width x rows per CTA (0 = the
 # library's wave-filling choice).
-_PAIR_SPACE = [{"pair": 1, "pair_cta": cta, "pair_fcta": fcta, "pair_xr": xr}
-               for cta, fcta in ((64, 64), (256, 256), (256, 64)) for xr in (0, 96, 160)]
+_PAIR_SPACE = ([{"pair": 1, "pair_split": 0, "pair_cta": cta, "pair_fcta": fcta, "pair_xr": xr}
+                for cta, fcta in ((64, 64), (256, 256), (256, 64)) for xr in (0, 96, 160)] +
+               [{"pair": 1, "pair_split": 1, "pair_cta": 0, "pair_fcta": fcta, "pair_xr": xr}
+                for fcta in (64, 256) for xr in (0, 96, 160)])
 _RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0}
 
 

@@ -6,8 +6,12 @@
 // transient read overlay of the scattered stress.  L m records the scattered vz, vx after every
 // step; L^T is its exact discrete transpose (no reference counterpart: the reference's adjoint is
 // not the transpose of its Born modelling and its CG helpers, main.cpp:1224-1320, are unused).
-// The boundary is the random band without damping, so the background field is rebuilt by exact
-// time reversal of the whole grid (source included) instead of saved strips.
+// With the random band (no damping) the background field is rebuilt by exact time reversal of the
+// whole grid (source included).  With a PML the update is the reference's split form with mu = 0
+// (vx damped in x only, vz in z only, s = s_x + s_z split in the PML cells, born.cu:215-349), L^T
+// is the exact transpose of that damped scheme, and the background is rebuilt backward on the
+// interior from boundary strips of vx, vz saved during a forward replay (the reference's
+// reconstruction, FD2DGPU.cu:3674-3731, 4769-4772), in FP32, FP16 or BF16.
 #pragma once
 #include "ds2d_kernels.cuh"
 
@@ -18,6 +22,8 @@ struct AcArgs {
   const ShotDev *shots;
   Par p;
   float *vx, *vz, *s;      // state updated in place
+  float *sx, *sz;          // split stress of the PML cells (null without a PML)
+  int interior;            // update only the interior [pml, n - pml)^2 (reconstruction)
   const float *e;          // additive stress overlay (Born source) or null
   const float *wavelet;
   int it;
@@ -34,6 +40,14 @@ __device__ __forceinline__ bool in_upd(const Dims &d, int ix, int iz) {
 __device__ __forceinline__ bool in_int(const Dims &d, int ix, int iz) {
   return ix >= d.pml && ix < d.nxp - d.pml && iz >= d.pml && iz < d.nzp - d.pml;
 }
+// Damping factors of a PML cell: d1 = 1 - dt d / 2 and 1 / d2 = 1 / (1 + dt d / 2).
+struct AcDamp {
+  float d1x, r2x, d1z, r2z;
+};
+__device__ __forceinline__ AcDamp ac_damp(const Dims &d, const Par &p, long long k) {
+  const float hx = p.dampx[k] * d.dt * 0.5f, hz = p.dampz[k] * d.dt * 0.5f;
+  return AcDamp{1.0f - hx, __frcp_rn(1.0f + hx), 1.0f - hz, __frcp_rn(1.0f + hz)};
+}
 
 // v += dir * b dt/d * D+(s + e + source)
 __global__ void __launch_bounds__(256) k_ac_vel(AcArgs a) {
@@ -41,6 +55,7 @@ __global__ void __launch_bounds__(256) k_ac_vel(AcArgs a) {
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y;
   if (ix >= d.nxp || iz >= d.nzp || !in_upd(d, ix, iz)) return;
+  if (a.interior && !in_int(d, ix, iz)) return;
   const int ld = d.ld;
   const long long base = d.slot * s, k = base + (long long)ix * ld + iz;
   long long ksrc = -1;
@@ -60,8 +75,15 @@ __global__ void __launch_bounds__(256) k_ac_vel(AcArgs a) {
   const float ax = stencil4([&](int i) { return rd(k + (long long)i * ld) - rd(k + (long long)(1 - i) * ld); });
   const float az = stencil4([&](int i) { return rd(k + i) - rd(k - i + 1); });
   const float bb = a.p.b[k];
-  const float vx = a.vx[k] + a.dir * (bb * (d.dt / d.dx)) * ax;
-  const float vz = a.vz[k] + a.dir * (bb * (d.dt / d.dz)) * az;
+  float vx, vz;
+  if (a.sx && pml_cell(d, ix, iz)) {  // damped (forward only): (d1 v + b dt/d D+ S) / d2
+    const AcDamp q = ac_damp(d, a.p, k);
+    vx = fmaf(q.d1x, a.vx[k], bb * (d.dt / d.dx) * ax) * q.r2x;
+    vz = fmaf(q.d1z, a.vz[k], bb * (d.dt / d.dz) * az) * q.r2z;
+  } else {
+    vx = a.vx[k] + a.dir * (bb * (d.dt / d.dx)) * ax;
+    vz = a.vz[k] + a.dir * (bb * (d.dt / d.dz)) * az;
+  }
   a.vx[k] = vx;
   a.vz[k] = vz;
   if (a.rec_on && iz == a.shots[s].igz) {
@@ -80,12 +102,42 @@ __global__ void __launch_bounds__(256) k_ac_str(AcArgs a) {
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int iz = blockIdx.x * 32 + threadIdx.x, ix = blockIdx.y * 8 + threadIdx.y;
   if (ix >= d.nxp || iz >= d.nzp || !in_upd(d, ix, iz)) return;
+  if (a.interior && !in_int(d, ix, iz)) return;
   const int ld = d.ld;
   const long long k = d.slot * s + (long long)ix * ld + iz;
   const float *VX = a.vx, *VZ = a.vz;
   const float sx = stencil4([&](int i) { return __ldg(VX + k + (long long)(i - 1) * ld) - __ldg(VX + k - (long long)i * ld); });
   const float sz = stencil4([&](int i) { return __ldg(VZ + k + i - 1) - __ldg(VZ + k - i); });
+  if (a.sx && pml_cell(d, ix, iz)) {  // split and damped (forward only)
+    const AcDamp q = ac_damp(d, a.p, k);
+    const float lam = a.p.lam[k];
+    const float nx = fmaf(q.d1x, a.sx[k], lam * (d.dt / d.dx) * sx) * q.r2x;
+    const float nz = fmaf(q.d1z, a.sz[k], lam * (d.dt / d.dz) * sz) * q.r2z;
+    a.sx[k] = nx;
+    a.sz[k] = nz;
+    a.s[k] = nx + nz;
+    return;
+  }
   a.s[k] = a.s[k] + a.dir * a.p.lam[k] * ((d.dt / d.dx) * sx + (d.dt / d.dz) * sz);
+}
+
+// Interior reconstruction of the background with a PML: the band of vx, vz around the PML edge
+// (the 2-field strips of FD2DGPU.cu:3674-3731) restored from the step's saved strips.
+struct AcStripArgs {
+  Dims d;
+  const ShotDev *shots;
+  float *vx, *vz;
+  Strips st;
+  int it;
+};
+__global__ void __launch_bounds__(256) k_ac_strip_load(AcStripArgs a) {
+  const int s = blockIdx.z, comp = blockIdx.y;
+  const Dims d = slot_dims(a.d, a.shots[s]);
+  const int bo = blockIdx.x * 256 + threadIdx.x;
+  if (bo >= d.lb) return;
+  int ix, iz;
+  band_cell(d, bo, ix, iz);
+  (comp ? a.vz : a.vx)[d.slot * s + (long long)ix * d.ld + iz] = strip_get(a.st, d, s, a.it, comp, bo);
 }
 
 // e = -2 lam m (Dx- vx / dx + Dz- vz / dz) on the interior (m = the windowed model in p.dmp).
@@ -115,7 +167,8 @@ struct AcAdjArgs {
   const float *res_vz, *res_vx;  // [slot][max_ntr][nt]
   int it;
   const float *bvx, *bvz;        // background velocities at this step (gradient)
-  float *grad;                   // [slot][wnx][wnz] (wnx_max stride)
+  float *grad;                   // [slot][wnx][ild] (wnx_max stride)
+  float *ysx, *ysz;              // adjoint of the split stress of the PML cells (null: none)
 };
 
 __global__ void __launch_bounds__(256) k_ac_adj_v(AcAdjArgs a) {
@@ -126,10 +179,33 @@ __global__ void __launch_bounds__(256) k_ac_adj_v(AcAdjArgs a) {
   const int ld = d.ld;
   const long long k = d.slot * s + (long long)ix * ld + iz;
   const float *lam = a.p.lam, *ys = a.ys;
-  auto w = [&](long long q) { return __ldg(lam + q) * __ldg(ys + q); };
-  const float tx = stencil4([&](int i) { return w(k + (long long)i * ld) - w(k + (long long)(1 - i) * ld); });
-  const float tz = stencil4([&](int i) { return w(k + i) - w(k - i + 1); });
+  float tx, tz;
   float yx = a.yx[k], yz = a.yz[k];
+  if (a.ysx) {
+    // With a PML: the stress stage's transpose reads y_sx / d2x (x part) and y_sz / d2z (z part)
+    // on split cells, and the velocity decay d1/d2 of the previous reverse step's velocity-stage
+    // transpose is applied here, where y_v is read only at its own cell.
+    const float *ysx = a.ysx, *ysz = a.ysz, *dpx = a.p.dampx, *dpz = a.p.dampz;
+    auto wx = [&](long long q, int qx, int qz) {
+      if (!pml_cell(d, qx, qz)) return __ldg(lam + q) * __ldg(ys + q);
+      return __ldg(lam + q) * __ldg(ysx + q) * __frcp_rn(1.0f + __ldg(dpx + q) * d.dt * 0.5f);
+    };
+    auto wz = [&](long long q, int qx, int qz) {
+      if (!pml_cell(d, qx, qz)) return __ldg(lam + q) * __ldg(ys + q);
+      return __ldg(lam + q) * __ldg(ysz + q) * __frcp_rn(1.0f + __ldg(dpz + q) * d.dt * 0.5f);
+    };
+    tx = stencil4([&](int i) { return wx(k + (long long)i * ld, ix + i, iz) - wx(k + (long long)(1 - i) * ld, ix + 1 - i, iz); });
+    tz = stencil4([&](int i) { return wz(k + i, ix, iz + i) - wz(k - i + 1, ix, iz - i + 1); });
+    if (pml_cell(d, ix, iz)) {
+      const AcDamp q = ac_damp(d, a.p, k);
+      yx *= q.d1x * q.r2x;
+      yz *= q.d1z * q.r2z;
+    }
+  } else {
+    auto w = [&](long long q) { return __ldg(lam + q) * __ldg(ys + q); };
+    tx = stencil4([&](int i) { return w(k + (long long)i * ld) - w(k + (long long)(1 - i) * ld); });
+    tz = stencil4([&](int i) { return w(k + i) - w(k - i + 1); });
+  }
   if (iz == a.shots[s].igz) {
     const int tr = a.rmap[(long long)s * d.nxp_max + ix];
     if (tr >= 0) {
@@ -153,12 +229,33 @@ __global__ void __launch_bounds__(256) k_ac_adj_s(AcAdjArgs a) {
   const long long k = d.slot * s + (long long)ix * ld + iz;
   const float *b = a.p.b, *yx = a.yx, *yz = a.yz;
   const float cx = d.dt / d.dx, cz = d.dt / d.dz;
-  auto ux = [&](long long q) { return __ldg(b + q) * cx * __ldg(yx + q); };
-  auto uz = [&](long long q) { return __ldg(b + q) * cz * __ldg(yz + q); };
-  const float gx = stencil4([&](int i) { return ux(k + (long long)(i - 1) * ld) - ux(k - (long long)i * ld); });
-  const float gz = stencil4([&](int i) { return uz(k + i - 1) - uz(k - i); });
+  float gx, gz;
+  if (a.ysx) {  // velocity-stage transpose with the PML's 1 / d2 on split cells
+    const float *dpx = a.p.dampx, *dpz = a.p.dampz;
+    auto ux = [&](long long q, int qx, int qz) {
+      const float u = __ldg(b + q) * cx * __ldg(yx + q);
+      return pml_cell(d, qx, qz) ? u * __frcp_rn(1.0f + __ldg(dpx + q) * d.dt * 0.5f) : u;
+    };
+    auto uz = [&](long long q, int qx, int qz) {
+      const float u = __ldg(b + q) * cz * __ldg(yz + q);
+      return pml_cell(d, qx, qz) ? u * __frcp_rn(1.0f + __ldg(dpz + q) * d.dt * 0.5f) : u;
+    };
+    gx = stencil4([&](int i) { return ux(k + (long long)(i - 1) * ld, ix + i - 1, iz) - ux(k - (long long)i * ld, ix - i, iz); });
+    gz = stencil4([&](int i) { return uz(k + i - 1, ix, iz + i - 1) - uz(k - i, ix, iz - i); });
+  } else {
+    auto ux = [&](long long q) { return __ldg(b + q) * cx * __ldg(yx + q); };
+    auto uz = [&](long long q) { return __ldg(b + q) * cz * __ldg(yz + q); };
+    gx = stencil4([&](int i) { return ux(k + (long long)(i - 1) * ld) - ux(k - (long long)i * ld); });
+    gz = stencil4([&](int i) { return uz(k + i - 1) - uz(k - i); });
+  }
   const float gs = -gx - gz;
-  a.ys[k] = a.ys[k] + gs;
+  if (a.ysx && pml_cell(d, ix, iz)) {  // S = s_x + s_z: y_S reaches both split parts
+    const AcDamp q = ac_damp(d, a.p, k);
+    a.ysx[k] = fmaf(q.d1x * q.r2x, a.ysx[k], gs);
+    a.ysz[k] = fmaf(q.d1z * q.r2z, a.ysz[k], gs);
+  } else {
+    a.ys[k] = a.ys[k] + gs;
+  }
   if (in_int(d, ix, iz)) {
     const float *VX = a.bvx, *VZ = a.bvz;
     const float sx = stencil4([&](int i) { return __ldg(VX + k + (long long)(i - 1) * ld) - __ldg(VX + k - (long long)i * ld); });

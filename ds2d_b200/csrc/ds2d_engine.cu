@@ -260,16 +260,21 @@ struct ds2d_ctx {
   // "pair" (1 on where they apply, 0 off: the default until they beat the one-column kernels),
   // "pair_cta" (backward CTA width: 0 auto, 256 or 160), "pair_xr" (rows per CTA: 0 = chosen to
   // fill whole waves).
-  int opt_pair = 0, opt_pair_cta = 0, opt_pair_fcta = 0, opt_pair_xr = 0;
+  int opt_pair = 0, opt_pair_cta = 0, opt_pair_fcta = 0, opt_pair_xr = 0, opt_pair_split = 0;
+  // split backward: the two launches of a step as parallel branches (second stream, fork / join
+  // events; parallel nodes in a captured graph)
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int *d_err = nullptr;      // error word raised by a pair kernel's bounded wait
   int num_sms = 148;
-  // resident CTAs per SM: forward 256 / 64, backward 256 / 160 / 64
-  int occ_pair[5] = {0, 0, 0, 0, 0};
+  // resident CTAs per SM: forward 256 / 64, backward 256 / 160 / 64, split parts 1 / 2
+  int occ_pair[7] = {0, 0, 0, 0, 0, 0, 0};
   std::vector<int> h_nxp;    // padded window rows of each slot of the current batch
   int opt_pcg_switch = 970;  // ds2d_lsrtm_pcg: per-mille residual ratio that ends the network phase
   int opt_pcg_m = 8;         // ds2d_lsrtm_pcg: directions kept for explicit conjugation
   // Acoustic Born pair (LSRTM): background, scattered and adjoint states, Born overlay.
   float *ac[10] = {};        // bvx bvz bs | dvx dvz ds | yx yz ys | e
+  float *ac_split[6] = {};   // with a PML: split stress s_x, s_z of background | scattered | adjoint
   float *ac2[6] = {};        // second (ping-pong) buffers of bvx bvz bs | dvx dvz ds (fused steps)
   double *dot_part = nullptr, *dot_out = nullptr;  // FP64 inner-product scratch
   // Work vectors of the LSRTM solver (model- and data-space), grown on demand.
@@ -624,11 +629,24 @@ PairBwdFn pair_bwd_fn(int cta) {
          : cta == 160 ? k_bwd_pair<160, kPairBwdD, 2>
                       : k_bwd_pair<256, kPairBwdD, 1>;
 }
+// The backward step split in two launches (option "pair_split"): reconstruction + illumination,
+// then adjoint + imaging, both on 64-thread strips.
+constexpr int kPairSplitT = 64;
+PairBwdFn pair_split_fn(int part) {
+  return part == 1 ? k_bwd_pair<kPairSplitT, kPairBwdD, 8, 1> : k_bwd_pair<kPairSplitT, kPairBwdD, 5, 2>;
+}
+constexpr size_t pair_split_smem(int part) {
+  return pair_smem(kPairSplitT, kPairBwdD, bwd_pair_fields(part), bwd_pair_z2_rows(part));
+}
+// Algorithmic bytes per padded cell of the two parts: reconstruction 5 fields r/w + b, lam, mu +
+// illumination r/w (60); adjoint 5 fields r/w + b, lam, mu + the reconstruction's input
+// velocities + imaging weights + two images r/w (84).
+constexpr double kBytesBwdRec = 60, kBytesBwdAdj = 84;
 constexpr size_t pair_fwd_smem(int cta) {
   return pair_smem(cta, kPairFwdD, kFwdPairFields, kFwdPairZ2Rows);
 }
 constexpr size_t pair_bwd_smem(int cta) {
-  return pair_smem(cta, kPairBwdD, kBwdPairFields, kBwdPairZ2Rows);
+  return pair_smem(cta, kPairBwdD, kBwdPairFields, bwd_pair_z2_rows(0));
 }
 
 bool pair_on(const ds2d_ctx *c) {
@@ -840,7 +858,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64) + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -877,7 +895,28 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
       a.shots = c->d_shots; a.rmap = c->d_rmap; a.res_vz = c->rec[0]; a.res_vx = c->rec[1];
       a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
       a.img = c->img_slot; a.img_plane = (long long)plane;
-      if (pair_on(c)) {
+      if (pair_on(c) && c->opt_pair_split) {
+        int pns, ptz;
+        pair_split(d, kPairSplitT, &pns, &ptz);
+        const int pxr = pair_xr(c, pns, std::min(c->occ_pair[5], c->occ_pair[6]));
+        a.tz = ptz; a.xr = pxr; a.err = c->d_err;
+        dim3 pgrid(pns, (d.nxp + pxr - 1) / pxr, n);
+        // independent launches (both read the step's input states, write their own buffers):
+        // the adjoint part runs on the second stream between a fork and a join event
+        CK(cudaEventRecord(c->ev_fork, c->stream));
+        CK(cudaStreamWaitEvent(c->aux, c->ev_fork, 0));
+        LAUNCHS("bwd_rec", kBytesBwdRec * CELLS(n), pair_split_fn(1), pgrid, kPairSplitT,
+                pair_split_smem(1), a);
+        {
+          cudaStream_t main = c->stream;
+          c->stream = c->aux;
+          LAUNCHS("bwd_adj", kBytesBwdAdj * CELLS(n), pair_split_fn(2), pgrid, kPairSplitT,
+                  pair_split_smem(2), a);
+          c->stream = main;
+        }
+        CK(cudaEventRecord(c->ev_join, c->aux));
+        CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+      } else if (pair_on(c)) {
         const int pc = pair_bwd_cta(c);
         int pns, ptz;
         pair_split(d, pc, &pns, &ptz);
@@ -1158,10 +1197,11 @@ int elsrtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base, int 
 int ensure_acoustic(ds2d_ctx *c) {
   int rc;
   if ((rc = ensure_common(c))) return rc;
-  if (!c->d.rbc)
-    return fail(c, DS2D_E_STATE,
-                "the acoustic LSRTM operators need boundary = DS2D_BOUNDARY_RANDOM (exact time "
-                "reversal of an undamped grid)");
+  if (!c->d.rbc) {  // PML: split stress in the damped cells, background strips for L^T
+    for (float *&p : c->ac_split)
+      if (!p && (rc = alloc_slots(c, &p))) return rc;
+    if (!c->st_a.data && (rc = alloc_strips(c, c->st_a))) return rc;
+  }
   if (!c->p_dmp) {
     if ((rc = alloc_slots(c, &c->p_dmp))) return rc;
     if ((rc = alloc_slots(c, &c->p_dms))) return rc;
@@ -1188,6 +1228,10 @@ AcArgs ac_args(ds2d_ctx *c, int set, int it, float dir) {
   AcArgs a{};
   a.d = c->d; a.shots = c->d_shots; a.p = c->par;
   a.vx = c->ac[3 * set]; a.vz = c->ac[3 * set + 1]; a.s = c->ac[3 * set + 2];
+  if (!c->d.rbc && set < 2) {
+    a.sx = c->ac_split[2 * set];
+    a.sz = c->ac_split[2 * set + 1];
+  }
   a.wavelet = c->wavelet; a.it = it; a.dir = dir; a.rmap = c->d_rmap;
   return a;
 }
@@ -1224,7 +1268,9 @@ int ac_ring_step(ds2d_ctx *c, int n, int set, int cur, int it, bool born_out, bo
 int ac_L_batch(ds2d_ctx *c, int n) {
   const Dims &d = c->d;
   size_t bytes = sizeof(float) * (size_t)d.slot * n;
-  if (c->opt_fused && c->ring_ok && c->ac2[0]) {
+  if (!d.rbc)
+    for (float *p : c->ac_split) CK(cudaMemsetAsync(p, 0, bytes, c->stream));
+  if (d.rbc && c->opt_fused && c->ring_ok && c->ac2[0]) {
     // fused: per step one background launch (Born source out) and one scattered launch
     for (int i = 0; i < 10; i++)
       if (i < 6 || i == 9) CK(cudaMemsetAsync(c->ac[i], 0, bytes, c->stream));
@@ -1263,6 +1309,45 @@ int ac_L_batch(ds2d_ctx *c, int n) {
   return DS2D_OK;
 }
 
+// L^T r with a PML (half steps): forward replay of the background (damped) saving the strips of
+// vx, vz each step, then per step in reverse: the step's strips restored into the band, the
+// transpose of the damped scattered step (records injected, gradient with the background
+// velocities after the step), and the interior reconstruction of the background one step back.
+int ac_LT_batch_pml(ds2d_ctx *c, int n) {
+  const Dims &d = c->d;
+  size_t bytes = sizeof(float) * (size_t)d.slot * n;
+  for (float *p : c->ac_split) CK(cudaMemsetAsync(p, 0, bytes, c->stream));
+  dim3 grid = cell_grid(d, n), blk(32, 8);
+  for (int it = 0; it < d.nt; it++) {
+    AcArgs b = ac_args(c, 0, it, 1.f);
+    b.src_on = 1;
+    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
+    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+    StripSaveArgs sv{d, c->d_shots, c->ac[0], c->ac[1], c->st_a, it};
+    LAUNCH(k_strip_save, dim3((d.lb + 255) / 256, 2, n), 256, sv);
+  }
+  for (int it = d.nt - 1; it >= 0; --it) {
+    AcStripArgs ld{d, c->d_shots, c->ac[0], c->ac[1], c->st_a, it};
+    LAUNCH(k_ac_strip_load, dim3((d.lb + 255) / 256, 2, n), 256, ld);
+    AcAdjArgs y{};
+    y.d = d; y.shots = c->d_shots; y.p = c->par;
+    y.yx = c->ac[6]; y.yz = c->ac[7]; y.ys = c->ac[8];
+    y.ysx = c->ac_split[4]; y.ysz = c->ac_split[5];
+    y.rmap = c->d_rmap; y.res_vz = c->rec[0]; y.res_vx = c->rec[1]; y.it = it;
+    y.bvx = c->ac[0]; y.bvz = c->ac[1]; y.grad = c->img_slot;
+    LAUNCHP("ac_adj_v", 0, k_ac_adj_v, grid, blk, y);
+    LAUNCHP("ac_adj_s", 0, k_ac_adj_s, grid, blk, y);
+    AcArgs b = ac_args(c, 0, it, -1.f);  // background back to step it-1 on the interior
+    b.src_on = 1;
+    b.interior = 1;
+    b.sx = b.sz = nullptr;
+    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
+  }
+  CK(cudaGetLastError());
+  return reduce_images(c, n, 1);
+}
+
 // L^T r for the uploaded batch (r in rec[0] / rec[1]); the windowed gradients are added into
 // the model-size image 0.
 int ac_LT_batch(ds2d_ctx *c, int n) {
@@ -1273,6 +1358,7 @@ int ac_LT_batch(ds2d_ctx *c, int n) {
   size_t plane = (size_t)c->B * d.wnx * d.ild;
   CK(cudaMemsetAsync(c->img_slot, 0, plane * sizeof(float), c->stream));
   dim3 grid = cell_grid(d, n), blk(32, 8);
+  if (!d.rbc) return ac_LT_batch_pml(c, n);
   const bool fused = c->opt_fused && c->ring_ok && c->ac2[0];
   if (fused) {
     // fused forward replay of the background, final state left in ac[0..2]
@@ -1493,6 +1579,14 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
           e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair[i], pair_fwd_fn(fctas[i]),
                                                             fctas[i], pair_fwd_smem(fctas[i]));
       }
+      for (int part = 1; part <= 2 && e == cudaSuccess; part++) {
+        e = cudaFuncSetAttribute(pair_split_fn(part), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_split_smem(part));
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair[4 + part],
+                                                            pair_split_fn(part), kPairSplitT,
+                                                            pair_split_smem(part));
+      }
       for (int i = 0; i < 3 && e == cudaSuccess; i++) {
         e = cudaFuncSetAttribute(pair_bwd_fn(bctas[i]), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)pair_bwd_smem(bctas[i]));
@@ -1525,6 +1619,13 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
     return DS2D_E_CUDA;
   }
   c->stream = c->own;
+  if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    fail(c, DS2D_E_CUDA, "cudaStreamCreate / cudaEventCreate failed");
+    ds2d_destroy(c);
+    return DS2D_E_CUDA;
+  }
   size_t nall = (size_t)g.allnx * g.allnz;
   int rc = 0;
   if ((rc = alloc(c, (void **)&c->vp_all, nall * 4)) || (rc = alloc(c, (void **)&c->vs_all, nall * 4)) ||
@@ -1549,11 +1650,15 @@ int ds2d_destroy(ds2d_ctx *c) {
   if (!c) return DS2D_OK;
   if (c->own) cudaStreamSynchronize(c->own);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->aux) cudaStreamSynchronize(c->aux);
   for (auto &g : c->graphs) cudaGraphExecDestroy(g.exec);
   c->graphs.clear();
   for (auto &v : c->vecs)
     if (v.p) cudaFree(v.p);
   c->arena.release();
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->aux) cudaStreamDestroy(c->aux);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
   return DS2D_OK;
@@ -1623,7 +1728,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64) + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -2065,6 +2170,9 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     if (value != 0 && value != 64 && value != 160 && value != 256)
       return fail(c, DS2D_E_ARG, "pair_cta must be 0 (automatic), 64, 160 or 256");
     c->opt_pair_cta = (int)value;
+  } else if (k == "pair_split") {
+    if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "pair_split must be 0 or 1");
+    c->opt_pair_split = (int)value;
   } else if (k == "pair_fcta") {
     if (value != 0 && value != 64 && value != 256)
       return fail(c, DS2D_E_ARG, "pair_fcta must be 0 (automatic), 64 or 256");

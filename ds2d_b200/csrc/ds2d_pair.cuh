@@ -387,28 +387,66 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
 // -1, FD2DGPU.cu:903-1082 via :4769-4772), the adjoint step with the receiver residual
 // (FD2DGPU.cu:591-895, :3306-3322) and the imaging condition (doimage_gradient :3245,
 // doimage_illum :3235).  Stage 1 (stresses and images) at row r-4, stage 2 (velocities and
-// illumination) at row r-8.  Ring fields of step r:
-//   0 bvx(r-1)  1 bvz(r)  2 avx(r-1)  3 avz(r)              x-window inputs
-//   4 bvx(r-4)  5 bvz(r-4)  6 avx(r-4)  7 avz(r-4)          stage-1 z-tap rows
-//   8-10 btxx, btzz, btxz(r-4)  11-13 atxx, atzz, atxz(r-4) stage-1 own cells
-//   14 lam  15 mu  16 kpp  17 kps (r-4)  18 image pp  19 image ps (r-4)
-//   20 b(r-8)  21 bvz(r-8)  22 avx(r-8)  23 avz(r-8)  24 illumination(r-8)   stage-2 own cells
+// illumination) at row r-8.
+//
+// kPart selects what one launch does: 0 everything (one pass, 124 B per cell), 1 the
+// reconstruction and the illumination (60 B), 2 the adjoint and the imaging, the latter with the
+// strains of the reconstruction's input state (t), which part 1 does not change (84 B).  Parts 1
+// and 2 of a step are independent; split, each needs far fewer registers than the fused pass, so
+// more CTAs stay resident per SM.
+//
+// Ring fields of step r (the rows each stage consumes), by part:
+//   x-windows:  bvx(r-1) bvz(r) [0, 1, 2]   avx(r-1) avz(r) [0, 2]
+//   stage-1 z-tap rows (r-4): bvx bvz [0, 1, 2]   avx avz [0, 2]
+//   stage-1 own (r-4): btxx btzz btxz [0, 1]  atxx atzz atxz [0, 2]  lam mu [all]
+//                      kpp kps, images pp ps [0, 2]
+//   stage-2 own (r-8): b [all]  bvz, illumination [0, 1]  avx avz [0, 2]
 // (bvx(r-8) is w_bvx[0]; the adjoint own velocities come from the ring because the windows carry
 // the residual.)
-constexpr int kBwdPairFields = 25;
-// Stage-2 z-tap rows btxz, btzz, M, PzLx, written by stage 1 for its row and read by stage 2 four
-// steps later: a circular buffer of 6 rows (rows r-9 .. r-4 are distinct slots, so the write of
-// step r never meets a read of step r-1 still in flight).
-constexpr int kBwdPairZ2 = 4, kBwdPairZDepth = 6;
-constexpr int kBwdPairZ2Rows = kBwdPairZ2 * kBwdPairZDepth;
+template <int P>
+struct BwdPairLayout;
+template <>
+struct BwdPairLayout<0> {
+  enum : int { BVXW = 0, BVZW, AVXW, AVZW, BVX4, BVZ4, AVX4, AVZ4, BTXX, BTZZ, BTXZ, ATXX, ATZZ,
+               ATXZ, LAM, MU, KPP, KPS, IPP, IPS, B8, BVZ8, AVX8, AVZ8, IL8, NF };
+};
+template <>
+struct BwdPairLayout<1> {
+  enum : int { BVXW = 0, BVZW, BVX4, BVZ4, BTXX, BTZZ, BTXZ, LAM, MU, B8, BVZ8, IL8, NF,
+               AVXW = -1, AVZW = -1, AVX4 = -1, AVZ4 = -1, ATXX = -1, ATZZ = -1, ATXZ = -1,
+               KPP = -1, KPS = -1, IPP = -1, IPS = -1, AVX8 = -1, AVZ8 = -1 };
+};
+template <>
+struct BwdPairLayout<2> {
+  enum : int { AVXW = 0, AVZW, BVXW, BVZW, AVX4, AVZ4, BVX4, BVZ4, ATXX, ATZZ, ATXZ, LAM, MU, KPP,
+               KPS, IPP, IPS, B8, AVX8, AVZ8, NF, BTXX = -1, BTZZ = -1, BTXZ = -1, BVZ8 = -1,
+               IL8 = -1 };
+};
+__host__ __device__ constexpr int bwd_pair_fields(int part) {
+  return part == 0 ? (int)BwdPairLayout<0>::NF
+                   : part == 1 ? (int)BwdPairLayout<1>::NF : (int)BwdPairLayout<2>::NF;
+}
+constexpr int kBwdPairFields = BwdPairLayout<0>::NF;
+// Stage-2 z-tap rows (btxz, btzz of the reconstruction; M, PzLx of the adjoint), written by stage
+// 1 for its row and read by stage 2 four steps later: a circular buffer of 6 rows (rows r-9 ..
+// r-4 are distinct slots, so the write of step r never meets a read of step r-1 still in flight).
+constexpr int kBwdPairZDepth = 6;
+__host__ __device__ constexpr int bwd_pair_z2(int part) { return part == 0 ? 4 : 2; }
+__host__ __device__ constexpr int bwd_pair_z2_rows(int part) {
+  return bwd_pair_z2(part) * kBwdPairZDepth;
+}
 
-template <int kT, int kD, int kMinB>
+template <int kT, int kD, int kMinB, int kPart = 0>
 __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
-  constexpr int NF = kBwdPairFields, ROW = pair_row(kT);
+  using L = BwdPairLayout<kPart>;
+  constexpr bool kRec = kPart != 2, kAdj = kPart != 1;
+  constexpr int NF = L::NF, ROW = pair_row(kT), NZ2 = bwd_pair_z2(kPart);
+  // z-tap rows of the circular buffer: reconstruction at 0-1, adjoint after them
+  constexpr int ZR = 0, ZA = kRec ? 2 : 0;
   extern __shared__ __align__(16) float smem[];
   float *ring = smem;
-  float *zc = ring + (size_t)kD * NF * ROW;  // [kBwdPairZDepth][kBwdPairZ2][ROW]
-  unsigned long long *bars = (unsigned long long *)(zc + kBwdPairZ2Rows * ROW);
+  float *zc = ring + (size_t)kD * NF * ROW;  // [kBwdPairZDepth][NZ2][ROW]
+  unsigned long long *bars = (unsigned long long *)(zc + NZ2 * kBwdPairZDepth * ROW);
   int *s_tr = (int *)(bars + 8);
   int *s_has = s_tr + 16;
   float *s_rz = (float *)(s_has + 16), *s_rx = s_rz + 16;
@@ -428,8 +466,8 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   const bool i0 = z0 >= pml && z0 < d.nzp - pml, i1 = z0 + 1 >= pml && z0 + 1 < d.nzp - pml;
   const ShotDev sh = a.shots[s];
   const int re = sh.igz - z0;  // receiver column relative to the pair
-  const bool rec_col = re == 0 || re == 1;
-  const bool rec_near = re >= -4 && re <= 5;
+  const bool rec_col = kAdj && (re == 0 || re == 1);
+  const bool rec_near = kAdj && re >= -4 && re <= 5;
   const float *res_z = a.res_vz + (long long)s * d.max_ntr * d.nt + a.it;
   const float *res_x = a.res_vx + (long long)s * d.max_ntr * d.nt + a.it;
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
@@ -437,23 +475,37 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
   float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
 
+  // ring field of this lane (warp 0 issues the copies; lane f owns field f)
   const int lane = t & 31;
   RingField fd{nullptr, 0, 0, d.nxp};
   {
-    const float *src[NF] = {a.ra.vx,  a.ra.vz,  a.aa.vx,  a.aa.vz,  a.ra.vx,  a.ra.vz,  a.aa.vx,
-                            a.aa.vz,  a.ra.txx, a.ra.tzz, a.ra.txz, a.aa.txx, a.aa.tzz, a.aa.txz,
-                            a.p.lam,  a.p.mu,   a.p.kpp,  a.p.kps,  img_pp,   img_ps,   a.p.b,
-                            a.ra.vz,  a.aa.vx,  a.aa.vz,  img_il};
-    const int lag[NF] = {1, 0, 1, 0, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 4, 8, 8, 8, 8, 8};
+    struct Src {
+      int f;
+      const float *p;
+      int lag;
+      bool img;
+    };
+    const Src tab[25] = {{L::BVXW, a.ra.vx, 1, false},  {L::BVZW, a.ra.vz, 0, false},
+                         {L::AVXW, a.aa.vx, 1, false},  {L::AVZW, a.aa.vz, 0, false},
+                         {L::BVX4, a.ra.vx, 4, false},  {L::BVZ4, a.ra.vz, 4, false},
+                         {L::AVX4, a.aa.vx, 4, false},  {L::AVZ4, a.aa.vz, 4, false},
+                         {L::BTXX, a.ra.txx, 4, false}, {L::BTZZ, a.ra.tzz, 4, false},
+                         {L::BTXZ, a.ra.txz, 4, false}, {L::ATXX, a.aa.txx, 4, false},
+                         {L::ATZZ, a.aa.tzz, 4, false}, {L::ATXZ, a.aa.txz, 4, false},
+                         {L::LAM, a.p.lam, 4, false},   {L::MU, a.p.mu, 4, false},
+                         {L::KPP, a.p.kpp, 4, false},   {L::KPS, a.p.kps, 4, false},
+                         {L::IPP, img_pp, 4, true},     {L::IPS, img_ps, 4, true},
+                         {L::B8, a.p.b, 8, false},      {L::BVZ8, a.ra.vz, 8, false},
+                         {L::AVX8, a.aa.vx, 8, false},  {L::AVZ8, a.aa.vz, 8, false},
+                         {L::IL8, img_il, 8, true}};
 #pragma unroll
-    for (int f = 0; f < NF; f++)
-      if (lane == f) {
-        const bool img = f == 18 || f == 19 || f == 24;
+    for (int q = 0; q < 25; q++)
+      if (tab[q].f >= 0 && lane == tab[q].f) {
         // image rows: grid row x is image row x - pml of the slot's plane
-        fd.src = img ? src[f] + ibase - (long long)pml * ld : src[f] + fbase;
-        fd.lag = lag[f];
-        fd.lo = img ? pml : 0;
-        fd.hi = img ? d.nxp - pml : d.nxp;
+        fd.src = tab[q].img ? tab[q].p + ibase - (long long)pml * ld : tab[q].p + fbase;
+        fd.lag = tab[q].lag;
+        fd.lo = tab[q].img ? pml : 0;
+        fd.hi = tab[q].img ? d.nxp - pml : d.nxp;
       }
   }
   if (t == 0) {
@@ -478,14 +530,25 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
     for (int j = 0; j < kD - 1; j++)
       issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], rs0 + j, ld, zs, lane);
 
-  float2 w_bvx[8], w_bvz[8], w_avx[8], w_avz[8];     // stage-1 x-windows
-  float2 w_btxx[8], w_btxz[9], w_PL[8], w_M[9];       // stage-2 x-windows
   const float2 zero2 = make_float2(0.f, 0.f);
+  float2 w_bvx[8], w_bvz[8];               // stage-1 x-windows (strains / reconstruction)
+  float2 w_avx[kAdj ? 8 : 1], w_avz[kAdj ? 8 : 1];
+  float2 w_btxx[kRec ? 8 : 1], w_btxz[kRec ? 9 : 1];  // stage-2 x-windows
+  float2 w_PL[kAdj ? 8 : 1], w_M[kAdj ? 9 : 1];
 #pragma unroll
-  for (int i = 0; i < 8; i++)
-    w_bvx[i] = w_bvz[i] = w_avx[i] = w_avz[i] = w_btxx[i] = w_PL[i] = zero2;
+  for (int i = 0; i < 8; i++) w_bvx[i] = w_bvz[i] = zero2;
+  if constexpr (kAdj) {
 #pragma unroll
-  for (int i = 0; i < 9; i++) w_btxz[i] = w_M[i] = zero2;
+    for (int i = 0; i < 8; i++) w_avx[i] = w_avz[i] = w_PL[i] = zero2;
+#pragma unroll
+    for (int i = 0; i < 9; i++) w_M[i] = zero2;
+  }
+  if constexpr (kRec) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) w_btxx[i] = zero2;
+#pragma unroll
+    for (int i = 0; i < 9; i++) w_btxz[i] = zero2;
+  }
   // circular z-tap slot of stage 1's row r-4 (stage 2 reads row r-8, two slots further on)
   int zw = ((rs0 - 4) % kBwdPairZDepth + kBwdPairZDepth) % kBwdPairZDepth;
 
@@ -498,6 +561,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
     ok = mbar_wait(&bars[cur.slot], cur.phase);
     const float *S = ring + (size_t)cur.slot * NF * ROW;
     auto F2 = [&](int f) -> float2 { return reinterpret_cast<const float2 *>(S + f * ROW)[pi]; };
+    auto ROWP = [&](int f) { return reinterpret_cast<const float2 *>(S + f * ROW); };
     if (rec_col) {
       // residual of row r + 8 (its trace index landed 8 steps ago), trace index of row r + 16;
       // one commit group per step, waited for 7 steps later
@@ -515,20 +579,22 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
       cp_async_commit();
     }
     if (ok) {
-      float2 n_bvx = F2(0), n_bvz = F2(1), n_avx = F2(2), n_avz = F2(3);
-      if (rec_col) {  // the residual enters the stencil values of the receiver column
-        const int qa = r - 1, qz = r;
-        if (qa >= 0 && qa < d.nxp && s_has[qa & 15]) {
-          if (re == 0) n_avx.x += s_rx[qa & 15]; else n_avx.y += s_rx[qa & 15];
+      push2(w_bvx, F2(L::BVXW));
+      push2(w_bvz, F2(L::BVZW));
+      if constexpr (kAdj) {
+        float2 n_avx = F2(L::AVXW), n_avz = F2(L::AVZW);
+        if (rec_col) {  // the residual enters the stencil values of the receiver column
+          const int qa = r - 1, qz = r;
+          if (qa >= 0 && qa < d.nxp && s_has[qa & 15]) {
+            if (re == 0) n_avx.x += s_rx[qa & 15]; else n_avx.y += s_rx[qa & 15];
+          }
+          if (qz >= 0 && qz < d.nxp && s_has[qz & 15]) {
+            if (re == 0) n_avz.x += s_rz[qz & 15]; else n_avz.y += s_rz[qz & 15];
+          }
         }
-        if (qz >= 0 && qz < d.nxp && s_has[qz & 15]) {
-          if (re == 0) n_avz.x += s_rz[qz & 15]; else n_avz.y += s_rz[qz & 15];
-        }
+        push2(w_avx, n_avx);
+        push2(w_avz, n_avz);
       }
-      push2(w_bvx, n_bvx);
-      push2(w_bvz, n_bvz);
-      push2(w_avx, n_avx);
-      push2(w_avz, n_avz);
     }
     // ---- stage 1: stresses of row r1 = r - 4, images ----------------------------------------
     const int r1 = r - 4;
@@ -536,111 +602,132 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
     if (ok && c1 && r >= x0 && r1 >= 0 && r1 < d.nxp) {
       const bool own = c2 && r1 >= x0 && r1 < x1;
       const bool x_int = r1 >= pml && r1 < d.nxp - pml;
-      const float2 lam = F2(14), mu = F2(15);
-      btxx = F2(8);
-      btzz = F2(9);
-      btxz = F2(10);
+      const float2 lam = F2(L::LAM), mu = F2(L::MU);
+      if constexpr (kRec) {
+        btxx = F2(L::BTXX);
+        btzz = F2(L::BTZZ);
+        btxz = F2(L::BTXZ);
+      }
       float2 gxx = zero2, gzz = zero2, gsh = zero2;  // strains: Dx vx, Dz vz, Dz vx + Dx vz
       if (x_int) {
-        const Z10 zbx = z10(reinterpret_cast<const float2 *>(S + 4 * ROW), pi);
-        const Z10 zbz = z10(reinterpret_cast<const float2 *>(S + 5 * ROW), pi);
+        const Z10 zbx = z10(ROWP(L::BVX4), pi);
+        const Z10 zbz = z10(ROWP(L::BVZ4), pi);
         const float sa0 = dxw_x(w_bvx), sa1 = dxw_y(w_bvx);
         const float sf0 = dxw_x(w_bvz), sf1 = dxw_y(w_bvz);
         const float sb0 = dzm<0>(zbz), sb1 = dzm<1>(zbz);
         const float se0 = dzp<0>(zbx), se1 = dzp<1>(zbx);
-        const float dir = -1.0f;
-        if (i0) {
-          const float l2m = lam.x + 2.0f * mu.x;
-          btxx.x = btxx.x + (dir * l2m * dtdx * sa0 + dir * lam.x * dtdz * sb0);
-          btzz.x = btzz.x + (dir * lam.x * dtdx * sa0 + dir * l2m * dtdz * sb0);
-          btxz.x = btxz.x + (dir * mu.x * dtdx * sf0 + dir * mu.x * dtdz * se0);
-          gxx.x = sa0 * rdx;
-          gzz.x = sb0 * rdz;
-          gsh.x = se0 * rdz + sf0 * rdx;
+        if constexpr (kRec) {
+          const float dir = -1.0f;
+          if (i0) {
+            const float l2m = lam.x + 2.0f * mu.x;
+            btxx.x = btxx.x + (dir * l2m * dtdx * sa0 + dir * lam.x * dtdz * sb0);
+            btzz.x = btzz.x + (dir * lam.x * dtdx * sa0 + dir * l2m * dtdz * sb0);
+            btxz.x = btxz.x + (dir * mu.x * dtdx * sf0 + dir * mu.x * dtdz * se0);
+          }
+          if (i1) {
+            const float l2m = lam.y + 2.0f * mu.y;
+            btxx.y = btxx.y + (dir * l2m * dtdx * sa1 + dir * lam.y * dtdz * sb1);
+            btzz.y = btzz.y + (dir * lam.y * dtdx * sa1 + dir * l2m * dtdz * sb1);
+            btxz.y = btxz.y + (dir * mu.y * dtdx * sf1 + dir * mu.y * dtdz * se1);
+          }
+          if (own) {
+            const long long k = fbase + (long long)r1 * ld + z0;
+            *reinterpret_cast<float2 *>(a.rb.txx + k) = btxx;
+            *reinterpret_cast<float2 *>(a.rb.tzz + k) = btzz;
+            *reinterpret_cast<float2 *>(a.rb.txz + k) = btxz;
+          }
         }
-        if (i1) {
-          const float l2m = lam.y + 2.0f * mu.y;
-          btxx.y = btxx.y + (dir * l2m * dtdx * sa1 + dir * lam.y * dtdz * sb1);
-          btzz.y = btzz.y + (dir * lam.y * dtdx * sa1 + dir * l2m * dtdz * sb1);
-          btxz.y = btxz.y + (dir * mu.y * dtdx * sf1 + dir * mu.y * dtdz * se1);
-          gxx.y = sa1 * rdx;
-          gzz.y = sb1 * rdz;
-          gsh.y = se1 * rdz + sf1 * rdx;
-        }
-        if (own) {
-          const long long k = fbase + (long long)r1 * ld + z0;
-          *reinterpret_cast<float2 *>(a.rb.txx + k) = btxx;
-          *reinterpret_cast<float2 *>(a.rb.tzz + k) = btzz;
-          *reinterpret_cast<float2 *>(a.rb.txz + k) = btxz;
-        }
-      }
-      float2 atxx = zero2, atzz = zero2, atxz = zero2;
-      if (r1 >= nop && r1 < d.nxp - nop) {
-        const Z10 zax = z10(reinterpret_cast<const float2 *>(S + 6 * ROW), pi);
-        const Z10 zaz = z10(reinterpret_cast<const float2 *>(S + 7 * ROW), pi);
-        float sb0 = dzm<0>(zaz), sb1 = dzm<1>(zaz);
-        float se0 = dzp<0>(zax), se1 = dzp<1>(zax);
-        if (rec_near && s_has[r1 & 15]) {  // residual of the receiver cell in the z-taps
-          const float rz = s_rz[r1 & 15], rx = s_rx[r1 & 15];
-          sb0 += rz * (coef_or0(re + 1) - coef_or0(-re));
-          sb1 += rz * (coef_or0(re) - coef_or0(1 - re));
-          se0 += rx * (coef_or0(re) - coef_or0(1 - re));
-          se1 += rx * (coef_or0(re - 1) - coef_or0(2 - re));
-        }
-        const float sa0 = dxw_x(w_avx), sa1 = dxw_y(w_avx);
-        const float sf0 = dxw_x(w_avz), sf1 = dxw_y(w_avz);
-        const float2 oxx = F2(11), ozz = F2(12), oxz = F2(13);
-        if (u0) {
-          atxx.x = oxx.x + -dtdx * sa0;
-          atzz.x = ozz.x + -dtdz * sb0;
-          atxz.x = oxz.x + (-dtdx * sf0 + -dtdz * se0);
-        }
-        if (u1) {
-          atxx.y = oxx.y + -dtdx * sa1;
-          atzz.y = ozz.y + -dtdz * sb1;
-          atxz.y = oxz.y + (-dtdx * sf1 + -dtdz * se1);
-        }
-        if (own) {
-          const long long k = fbase + (long long)r1 * ld + z0;
-          *reinterpret_cast<float2 *>(a.ab.txx + k) = atxx;
-          *reinterpret_cast<float2 *>(a.ab.tzz + k) = atzz;
-          *reinterpret_cast<float2 *>(a.ab.txz + k) = atxz;
+        if constexpr (kAdj) {
+          if (i0) {
+            gxx.x = sa0 * rdx;
+            gzz.x = sb0 * rdz;
+            gsh.x = se0 * rdz + sf0 * rdx;
+          }
+          if (i1) {
+            gxx.y = sa1 * rdx;
+            gzz.y = sb1 * rdz;
+            gsh.y = se1 * rdz + sf1 * rdx;
+          }
         }
       }
-      {
-        const float l2m0 = lam.x + 2.0f * mu.x, l2m1 = lam.y + 2.0f * mu.y;
-        PL = make_float2(l2m0 * atxx.x + lam.x * atzz.x, l2m1 * atxx.y + lam.y * atzz.y);
-        M = make_float2(mu.x * atxz.x, mu.y * atxz.y);
-        PzLx = make_float2(l2m0 * atzz.x + lam.x * atxx.x, l2m1 * atzz.y + lam.y * atxx.y);
-      }
-      if (own && x_int) {  // doimage_gradient, FD2DGPU.cu:3245-3263
-        const float2 kpp = F2(16), kps = F2(17), ipp = F2(18), ips = F2(19);
-        float2 npp = ipp, nps = ips;
-        if (i0) {
-          npp.x = ipp.x + kpp.x * ((gxx.x + gzz.x) * (atxx.x + atzz.x));
-          nps.x = ips.x + kps.x * (-2.0f * (gxx.x * atzz.x + gzz.x * atxx.x) + gsh.x * atxz.x);
+      if constexpr (kAdj) {
+        float2 atxx = zero2, atzz = zero2, atxz = zero2;
+        if (r1 >= nop && r1 < d.nxp - nop) {
+          const Z10 zax = z10(ROWP(L::AVX4), pi);
+          const Z10 zaz = z10(ROWP(L::AVZ4), pi);
+          float sb0 = dzm<0>(zaz), sb1 = dzm<1>(zaz);
+          float se0 = dzp<0>(zax), se1 = dzp<1>(zax);
+          if (rec_near && s_has[r1 & 15]) {  // residual of the receiver cell in the z-taps
+            const float rz = s_rz[r1 & 15], rx = s_rx[r1 & 15];
+            sb0 += rz * (coef_or0(re + 1) - coef_or0(-re));
+            sb1 += rz * (coef_or0(re) - coef_or0(1 - re));
+            se0 += rx * (coef_or0(re) - coef_or0(1 - re));
+            se1 += rx * (coef_or0(re - 1) - coef_or0(2 - re));
+          }
+          const float sa0 = dxw_x(w_avx), sa1 = dxw_y(w_avx);
+          const float sf0 = dxw_x(w_avz), sf1 = dxw_y(w_avz);
+          const float2 oxx = F2(L::ATXX), ozz = F2(L::ATZZ), oxz = F2(L::ATXZ);
+          if (u0) {
+            atxx.x = oxx.x + -dtdx * sa0;
+            atzz.x = ozz.x + -dtdz * sb0;
+            atxz.x = oxz.x + (-dtdx * sf0 + -dtdz * se0);
+          }
+          if (u1) {
+            atxx.y = oxx.y + -dtdx * sa1;
+            atzz.y = ozz.y + -dtdz * sb1;
+            atxz.y = oxz.y + (-dtdx * sf1 + -dtdz * se1);
+          }
+          if (own) {
+            const long long k = fbase + (long long)r1 * ld + z0;
+            *reinterpret_cast<float2 *>(a.ab.txx + k) = atxx;
+            *reinterpret_cast<float2 *>(a.ab.tzz + k) = atzz;
+            *reinterpret_cast<float2 *>(a.ab.txz + k) = atxz;
+          }
         }
-        if (i1) {
-          npp.y = ipp.y + kpp.y * ((gxx.y + gzz.y) * (atxx.y + atzz.y));
-          nps.y = ips.y + kps.y * (-2.0f * (gxx.y * atzz.y + gzz.y * atxx.y) + gsh.y * atxz.y);
+        {
+          const float l2m0 = lam.x + 2.0f * mu.x, l2m1 = lam.y + 2.0f * mu.y;
+          PL = make_float2(l2m0 * atxx.x + lam.x * atzz.x, l2m1 * atxx.y + lam.y * atzz.y);
+          M = make_float2(mu.x * atxz.x, mu.y * atxz.y);
+          PzLx = make_float2(l2m0 * atzz.x + lam.x * atxx.x, l2m1 * atzz.y + lam.y * atxx.y);
         }
-        const long long o = ibase + (long long)(r1 - pml) * d.ild + z0;
-        *reinterpret_cast<float2 *>(img_pp + o) = npp;
-        *reinterpret_cast<float2 *>(img_ps + o) = nps;
+        if (own && x_int) {  // doimage_gradient, FD2DGPU.cu:3245-3263
+          const float2 kpp = F2(L::KPP), kps = F2(L::KPS), ipp = F2(L::IPP), ips = F2(L::IPS);
+          float2 npp = ipp, nps = ips;
+          if (i0) {
+            npp.x = ipp.x + kpp.x * ((gxx.x + gzz.x) * (atxx.x + atzz.x));
+            nps.x = ips.x + kps.x * (-2.0f * (gxx.x * atzz.x + gzz.x * atxx.x) + gsh.x * atxz.x);
+          }
+          if (i1) {
+            npp.y = ipp.y + kpp.y * ((gxx.y + gzz.y) * (atxx.y + atzz.y));
+            nps.y = ips.y + kps.y * (-2.0f * (gxx.y * atzz.y + gzz.y * atxx.y) + gsh.y * atxz.y);
+          }
+          const long long o = ibase + (long long)(r1 - pml) * d.ild + z0;
+          *reinterpret_cast<float2 *>(img_pp + o) = npp;
+          *reinterpret_cast<float2 *>(img_ps + o) = nps;
+        }
       }
     }
-    push2(w_btxx, btxx);
-    push2(w_btxz, btxz);
-    push2(w_PL, PL);
-    push2(w_M, M);
+    if constexpr (kRec) {
+      push2(w_btxx, btxx);
+      push2(w_btxz, btxz);
+    }
+    if constexpr (kAdj) {
+      push2(w_PL, PL);
+      push2(w_M, M);
+    }
     {  // z-tap rows of row r - 4 for stage 2 four steps on
-      float *zwb = zc + zw * kBwdPairZ2 * ROW;
-      reinterpret_cast<float2 *>(zwb)[pi] = btxz;
-      reinterpret_cast<float2 *>(zwb + ROW)[pi] = btzz;
-      reinterpret_cast<float2 *>(zwb + 2 * ROW)[pi] = M;
-      reinterpret_cast<float2 *>(zwb + 3 * ROW)[pi] = PzLx;
+      float *zwb = zc + zw * NZ2 * ROW;
+      if constexpr (kRec) {
+        reinterpret_cast<float2 *>(zwb + ZR * ROW)[pi] = btxz;
+        reinterpret_cast<float2 *>(zwb + (ZR + 1) * ROW)[pi] = btzz;
+      }
+      if constexpr (kAdj) {
+        reinterpret_cast<float2 *>(zwb + ZA * ROW)[pi] = M;
+        reinterpret_cast<float2 *>(zwb + (ZA + 1) * ROW)[pi] = PzLx;
+      }
     }
-    const float *zb = zc + (zw >= kBwdPairZDepth - 2 ? zw - (kBwdPairZDepth - 2) : zw + 2) * kBwdPairZ2 * ROW;
+    const float *zb =
+        zc + (zw >= kBwdPairZDepth - 2 ? zw - (kBwdPairZDepth - 2) : zw + 2) * NZ2 * ROW;
     zw = zw == kBwdPairZDepth - 1 ? 0 : zw + 1;
     // ---- the step's barrier, the refill -------------------------------------------------------
     if (__syncthreads_or(!ok)) {
@@ -656,54 +743,57 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
     const int r2 = r - 8;
     if (c2 && r2 >= x0 && r2 < x1) {
       const long long k = fbase + (long long)r2 * ld + z0;
-      const bool x_int = r2 >= pml && r2 < d.nxp - pml;
-      const float2 bb = F2(20);
-      if (x_int) {
-        const Z10 ztxz = z10(reinterpret_cast<const float2 *>(zb), pi);
-        const Z10 ztzz = z10(reinterpret_cast<const float2 *>(zb + ROW), pi);
-        const float2 ovx = w_bvx[0], ovz = F2(21), il = F2(24);
-        float2 vx = ovx, vz = ovz, nil = il;
-        if (i0) {
-          const float cbx = bb.x * dtdx, cbz = bb.x * dtdz;
-          const float ax = dxw_x(w_btxx), fx = dxw_x(w_btxz);
-          const float bz = dzm<0>(ztxz), ez = dzp<0>(ztzz);
-          vx.x = ovx.x + (-cbx * ax + -cbz * bz);
-          vz.x = ovz.x + (-cbx * fx + -cbz * ez);
-          nil.x = il.x + (vx.x * vx.x + vz.x * vz.x);
+      const float2 bb = F2(L::B8);
+      if constexpr (kRec) {
+        if (r2 >= pml && r2 < d.nxp - pml) {
+          const Z10 ztxz = z10(reinterpret_cast<const float2 *>(zb + ZR * ROW), pi);
+          const Z10 ztzz = z10(reinterpret_cast<const float2 *>(zb + (ZR + 1) * ROW), pi);
+          const float2 ovx = w_bvx[0], ovz = F2(L::BVZ8), il = F2(L::IL8);
+          float2 vx = ovx, vz = ovz, nil = il;
+          if (i0) {
+            const float cbx = bb.x * dtdx, cbz = bb.x * dtdz;
+            const float ax = dxw_x(w_btxx), fx = dxw_x(w_btxz);
+            const float bz = dzm<0>(ztxz), ez = dzp<0>(ztzz);
+            vx.x = ovx.x + (-cbx * ax + -cbz * bz);
+            vz.x = ovz.x + (-cbx * fx + -cbz * ez);
+            nil.x = il.x + (vx.x * vx.x + vz.x * vz.x);
+          }
+          if (i1) {
+            const float cbx = bb.y * dtdx, cbz = bb.y * dtdz;
+            const float ax = dxw_y(w_btxx), fx = dxw_y(w_btxz);
+            const float bz = dzm<1>(ztxz), ez = dzp<1>(ztzz);
+            vx.y = ovx.y + (-cbx * ax + -cbz * bz);
+            vz.y = ovz.y + (-cbx * fx + -cbz * ez);
+            nil.y = il.y + (vx.y * vx.y + vz.y * vz.y);
+          }
+          *reinterpret_cast<float2 *>(a.rb.vx + k) = vx;
+          *reinterpret_cast<float2 *>(a.rb.vz + k) = vz;
+          *reinterpret_cast<float2 *>(img_il + ibase + (long long)(r2 - pml) * d.ild + z0) = nil;
         }
-        if (i1) {
-          const float cbx = bb.y * dtdx, cbz = bb.y * dtdz;
-          const float ax = dxw_y(w_btxx), fx = dxw_y(w_btxz);
-          const float bz = dzm<1>(ztxz), ez = dzp<1>(ztzz);
-          vx.y = ovx.y + (-cbx * ax + -cbz * bz);
-          vz.y = ovz.y + (-cbx * fx + -cbz * ez);
-          nil.y = il.y + (vx.y * vx.y + vz.y * vz.y);
-        }
-        *reinterpret_cast<float2 *>(a.rb.vx + k) = vx;
-        *reinterpret_cast<float2 *>(a.rb.vz + k) = vz;
-        *reinterpret_cast<float2 *>(img_il + ibase + (long long)(r2 - pml) * d.ild + z0) = nil;
       }
-      if (r2 >= nop && r2 < d.nxp - nop) {
-        const Z10 zm = z10(reinterpret_cast<const float2 *>(zb + 2 * ROW), pi);
-        const Z10 zp = z10(reinterpret_cast<const float2 *>(zb + 3 * ROW), pi);
-        float2 vx = zero2, vz = zero2;
-        const float2 ovx = F2(22), ovz = F2(23);
-        if (u0) {
-          const float cbx = bb.x * dtdx, cbz = bb.x * dtdz;
-          const float t_x = dxw_x(w_PL), s_xz = dxw_x(w_M);
-          const float t_xz = dzm<0>(zm), s_z = dzp<0>(zp);
-          vx.x = ovx.x + (-cbx * t_x + -cbz * t_xz);
-          vz.x = ovz.x + (-cbx * s_xz + -cbz * s_z);
+      if constexpr (kAdj) {
+        if (r2 >= nop && r2 < d.nxp - nop) {
+          const Z10 zm = z10(reinterpret_cast<const float2 *>(zb + ZA * ROW), pi);
+          const Z10 zp = z10(reinterpret_cast<const float2 *>(zb + (ZA + 1) * ROW), pi);
+          float2 vx = zero2, vz = zero2;
+          const float2 ovx = F2(L::AVX8), ovz = F2(L::AVZ8);
+          if (u0) {
+            const float cbx = bb.x * dtdx, cbz = bb.x * dtdz;
+            const float t_x = dxw_x(w_PL), s_xz = dxw_x(w_M);
+            const float t_xz = dzm<0>(zm), s_z = dzp<0>(zp);
+            vx.x = ovx.x + (-cbx * t_x + -cbz * t_xz);
+            vz.x = ovz.x + (-cbx * s_xz + -cbz * s_z);
+          }
+          if (u1) {
+            const float cbx = bb.y * dtdx, cbz = bb.y * dtdz;
+            const float t_x = dxw_y(w_PL), s_xz = dxw_y(w_M);
+            const float t_xz = dzm<1>(zm), s_z = dzp<1>(zp);
+            vx.y = ovx.y + (-cbx * t_x + -cbz * t_xz);
+            vz.y = ovz.y + (-cbx * s_xz + -cbz * s_z);
+          }
+          *reinterpret_cast<float2 *>(a.ab.vx + k) = vx;
+          *reinterpret_cast<float2 *>(a.ab.vz + k) = vz;
         }
-        if (u1) {
-          const float cbx = bb.y * dtdx, cbz = bb.y * dtdz;
-          const float t_x = dxw_y(w_PL), s_xz = dxw_y(w_M);
-          const float t_xz = dzm<1>(zm), s_z = dzp<1>(zp);
-          vx.y = ovx.y + (-cbx * t_x + -cbz * t_xz);
-          vz.y = ovz.y + (-cbx * s_xz + -cbz * s_z);
-        }
-        *reinterpret_cast<float2 *>(a.ab.vx + k) = vx;
-        *reinterpret_cast<float2 *>(a.ab.vz + k) = vz;
       }
     }
     if (rec_col) cp_async_wait<6>();

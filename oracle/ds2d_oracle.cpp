@@ -658,18 +658,34 @@ int rtm_impl(const orc_grid *gg, const float *const model[7], const float *wav, 
 
 // ---- acoustic Born operator pair (exact discrete adjoint), FP64 -----------------------------
 // Fields vx, vz, s (s = txx = tzz of the mu = 0 elastic scheme).  U = [nop, n-nop)^2 is the
-// updated set, I = [pml, n-pml)^2 the interior carrying the Born source.
+// updated set, I = [pml, n-pml)^2 the interior carrying the Born source.  With a PML (non-zero
+// damping) the update is the reference's split form with mu = 0 (born.cu:215-349): vx is damped
+// in x only and vz in z only (their z / x parts are driven by txz = 0), and s = s_x + s_z with
+// s_x <- (d1x s_x + lam dt/dx Dx- vx) / d2x, s_z likewise in z, d1 = 1 - dt d / 2, d2 = 1 + dt d / 2.
+// PML cells are those of the geometric PML (ix < pml, ix > nx - pml, likewise in z) and carry
+// s_x, s_z; the other cells carry only s.  Without damping (random band) no cell is split.
 struct AcOp {
   Geo<double> g;
-  Vec<double> b, lam;
+  Vec<double> b, lam, d1x, d2x, d1z, d2z;
+  Vec<char> split;
+  bool has_pml = false;
   double cx, cz;  // dt/dx, dt/dz
   explicit AcOp(const orc_grid *gg, const float *const model[7]) : g(gg) {
     b.resize(g.n);
     lam.resize(g.n);
+    d1x.resize(g.n); d2x.resize(g.n); d1z.resize(g.n); d2z.resize(g.n);
+    split.assign(g.n, 0);
     for (size_t k = 0; k < g.n; k++) {
       b[k] = 1.0 / (double)model[2][k];
       lam[k] = model[3][k];
+      const double hx = g.dt * (double)model[5][k] * 0.5, hz = g.dt * (double)model[6][k] * 0.5;
+      d1x[k] = 1.0 - hx; d2x[k] = 1.0 + hx; d1z[k] = 1.0 - hz; d2z[k] = 1.0 + hz;
+      if (model[5][k] != 0.f || model[6][k] != 0.f) has_pml = true;
     }
+    if (has_pml)
+      for (int ix = 0; ix < g.nx; ix++)
+        for (int iz = 0; iz < g.nz; iz++)
+          split[I(ix, iz)] = ix < g.pml || ix > g.nx - g.pml || iz < g.pml || iz > g.nz - g.pml;
     cx = g.dt / g.dx;
     cz = g.dt / g.dz;
   }
@@ -695,10 +711,11 @@ struct AcOp {
     for (int i = 1; i <= 4; i++) t += g.c[i] * (f(I(ix, iz + i - 1)) - f(I(ix, iz - i)));
     return t;
   }
-  // One step: v += b dt/d D+ (s + e + source), then s += lam (dt/dx Dx- vx + dt/dz Dz- vz).
-  // dir = -1 undoes a dir = +1 step exactly (stress first, then velocities).
-  void step(Vec<double> &vx, Vec<double> &vz, Vec<double> &s, const Vec<double> *e, long ksrc,
-            double sval, int dir) const {
+  // One step: v += b dt/d D+ (s + e + source), then s += lam (dt/dx Dx- vx + dt/dz Dz- vz);
+  // split (damped) in PML cells.  dir = -1 undoes a dir = +1 step exactly (stress first, then
+  // velocities) on a grid without damping.
+  void step(Vec<double> &vx, Vec<double> &vz, Vec<double> &s, Vec<double> &sx, Vec<double> &sz,
+            const Vec<double> *e, long ksrc, double sval, int dir) const {
     const int lo = g.nop;
     auto S = [&](size_t q) {
       double v = s[q];
@@ -709,8 +726,13 @@ struct AcOp {
     auto vstage = [&]() {
       FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {
         size_t k = I(ix, iz);
-        vx[k] += dir * b[k] * cx * dxp(S, ix, iz);
-        vz[k] += dir * b[k] * cz * dzp(S, ix, iz);
+        if (split[k]) {
+          vx[k] = (d1x[k] * vx[k] + b[k] * cx * dxp(S, ix, iz)) / d2x[k];
+          vz[k] = (d1z[k] * vz[k] + b[k] * cz * dzp(S, ix, iz)) / d2z[k];
+        } else {
+          vx[k] += dir * b[k] * cx * dxp(S, ix, iz);
+          vz[k] += dir * b[k] * cz * dzp(S, ix, iz);
+        }
       }
     };
     auto sstage = [&]() {
@@ -718,7 +740,13 @@ struct AcOp {
       auto VZ = [&](size_t q) { return vz[q]; };
       FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {
         size_t k = I(ix, iz);
-        s[k] += dir * lam[k] * (cx * dxm(VX, ix, iz) + cz * dzm(VZ, ix, iz));
+        if (split[k]) {
+          sx[k] = (d1x[k] * sx[k] + lam[k] * cx * dxm(VX, ix, iz)) / d2x[k];
+          sz[k] = (d1z[k] * sz[k] + lam[k] * cz * dzm(VZ, ix, iz)) / d2z[k];
+          s[k] = sx[k] + sz[k];
+        } else {
+          s[k] += dir * lam[k] * (cx * dxm(VX, ix, iz) + cz * dzm(VZ, ix, iz));
+        }
       }
     };
     if (dir > 0) { vstage(); sstage(); } else { sstage(); vstage(); }
@@ -732,29 +760,54 @@ struct AcOp {
       e[k] = -2.0 * lam[k] * m[k] * (dxm(VX, ix, iz) / g.dx + dzm(VZ, ix, iz) / g.dz);
     }
   }
-  // Transpose of one dir = +1 step acting on the adjoint state; returns the gradient with
-  // respect to the injected e in ge (on U).
-  void adj_step(Vec<double> &yx, Vec<double> &yz, Vec<double> &ys, Vec<double> &ge) const {
+  // Transpose of one dir = +1 step acting on the adjoint state (y_s on unsplit cells, y_sx / y_sz
+  // on split ones); returns the gradient with respect to the injected e in ge (on U).
+  // Stress stage v' -> s': y_v' -= D+(lam dt/d y_s' [/ d2]), y_sx <- d1x / d2x y_sx'.
+  // Velocity stage (v, S) -> v': y_S = -Dx-(b dt/dx y_vx' [/ d2x]) - Dz-(...), y_v <- d1/d2 y_v',
+  // and S = s + e adds y_S to y_s (both parts on split cells) and to ge.
+  void adj_step(Vec<double> &yx, Vec<double> &yz, Vec<double> &ys, Vec<double> &ysx,
+                Vec<double> &ysz, Vec<double> &ge) const {
     const int lo = g.nop;
-    Vec<double> w(g.n, 0.0), ux(g.n, 0.0), uz(g.n, 0.0);
-    FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) { size_t k = I(ix, iz); w[k] = lam[k] * ys[k]; }
-    auto W = [&](size_t q) { return w[q]; };
+    Vec<double> wx(g.n, 0.0), wz(g.n, 0.0), ux(g.n, 0.0), uz(g.n, 0.0);
+    FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {
+      size_t k = I(ix, iz);
+      if (split[k]) {
+        wx[k] = lam[k] * cx * ysx[k] / d2x[k];
+        wz[k] = lam[k] * cz * ysz[k] / d2z[k];
+      } else {
+        wx[k] = lam[k] * cx * ys[k];
+        wz[k] = lam[k] * cz * ys[k];
+      }
+    }
+    auto WX = [&](size_t q) { return wx[q]; };
+    auto WZ = [&](size_t q) { return wz[q]; };
     FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {  // transpose of the stress stage
       size_t k = I(ix, iz);
-      yx[k] -= cx * dxp(W, ix, iz);
-      yz[k] -= cz * dzp(W, ix, iz);
+      yx[k] -= dxp(WX, ix, iz);
+      yz[k] -= dzp(WZ, ix, iz);
+      if (split[k]) {
+        ysx[k] *= d1x[k] / d2x[k];
+        ysz[k] *= d1z[k] / d2z[k];
+      }
     }
     FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {
       size_t k = I(ix, iz);
-      ux[k] = b[k] * cx * yx[k];
-      uz[k] = b[k] * cz * yz[k];
+      ux[k] = b[k] * cx * yx[k] / (split[k] ? d2x[k] : 1.0);
+      uz[k] = b[k] * cz * yz[k] / (split[k] ? d2z[k] : 1.0);
     }
     auto UX = [&](size_t q) { return ux[q]; };
     auto UZ = [&](size_t q) { return uz[q]; };
     FOR_CELLS(lo, g.nx - lo, lo, g.nz - lo) {  // transpose of the velocity stage
       size_t k = I(ix, iz);
       const double gs = -dxm(UX, ix, iz) - dzm(UZ, ix, iz);
-      ys[k] += gs;
+      if (split[k]) {
+        ysx[k] += gs;
+        ysz[k] += gs;
+        yx[k] *= d1x[k] / d2x[k];
+        yz[k] *= d1z[k] / d2z[k];
+      } else {
+        ys[k] += gs;
+      }
       ge[k] = gs;
     }
   }
@@ -764,12 +817,13 @@ int ac_born(const orc_grid *gg, const float *const model[7], const float *wav, i
             const orc_shot *s, const double *m, double *rz, double *rx) {
   AcOp op(gg, model);
   const Geo<double> &g = op.g;
-  Vec<double> vx(g.n, 0), vz(g.n, 0), sg(g.n, 0), dvx(g.n, 0), dvz(g.n, 0), ds(g.n, 0), e(g.n, 0);
+  Vec<double> vx(g.n, 0), vz(g.n, 0), sg(g.n, 0), sgx(g.n, 0), sgz(g.n, 0);
+  Vec<double> dvx(g.n, 0), dvz(g.n, 0), ds(g.n, 0), dsx(g.n, 0), dsz(g.n, 0), e(g.n, 0);
   const long ks = (long)g.I(s->isx, s->isz);
   for (int it = 0; it < nt; it++) {
-    op.step(vx, vz, sg, nullptr, ks, wav[it], 1);
+    op.step(vx, vz, sg, sgx, sgz, nullptr, ks, wav[it], 1);
     op.born(vx, vz, m, e);
-    op.step(dvx, dvz, ds, &e, -1, 0.0, 1);
+    op.step(dvx, dvz, ds, dsx, dsz, &e, -1, 0.0, 1);
     for (int tr = 0; tr < s->ntr; tr++) {
       size_t k = g.I(s->igx[tr], s->igz);
       rz[(size_t)tr * nt + it] = dvz[k];
@@ -779,29 +833,41 @@ int ac_born(const orc_grid *gg, const float *const model[7], const float *wav, i
   return 0;
 }
 
+// Exact transpose of ac_born.  The background at each step comes from exact time reversal
+// without damping, and from the stored forward history with a PML (damping cannot be reversed).
 int ac_born_adj(const orc_grid *gg, const float *const model[7], const float *wav, int nt,
                 const orc_shot *s, const double *rz, const double *rx, double *grad) {
   AcOp op(gg, model);
   const Geo<double> &g = op.g;
-  Vec<double> vx(g.n, 0), vz(g.n, 0), sg(g.n, 0), yx(g.n, 0), yz(g.n, 0), ys(g.n, 0), ge(g.n, 0);
+  Vec<double> vx(g.n, 0), vz(g.n, 0), sg(g.n, 0), sgx(g.n, 0), sgz(g.n, 0);
+  Vec<double> yx(g.n, 0), yz(g.n, 0), ys(g.n, 0), ysx(g.n, 0), ysz(g.n, 0), ge(g.n, 0);
   const long ks = (long)g.I(s->isx, s->isz);
-  for (int it = 0; it < nt; it++) op.step(vx, vz, sg, nullptr, ks, wav[it], 1);
+  std::vector<Vec<double>> hist;  // background velocities after each step (PML only)
+  for (int it = 0; it < nt; it++) {
+    op.step(vx, vz, sg, sgx, sgz, nullptr, ks, wav[it], 1);
+    if (op.has_pml) {
+      hist.push_back(vx);
+      hist.push_back(vz);
+    }
+  }
   std::fill(grad, grad + g.n, 0.0);
-  auto VX = [&](size_t q) { return vx[q]; };
-  auto VZ = [&](size_t q) { return vz[q]; };
   for (int it = nt - 1; it >= 0; --it) {
     for (int tr = 0; tr < s->ntr; tr++) {  // transpose of the recording after step it
       size_t k = g.I(s->igx[tr], s->igz);
       yz[k] += rz[(size_t)tr * nt + it];
       yx[k] += rx[(size_t)tr * nt + it];
     }
-    op.adj_step(yx, yz, ys, ge);
+    op.adj_step(yx, yz, ys, ysx, ysz, ge);
+    const Vec<double> &bx = op.has_pml ? hist[2 * it] : vx;
+    const Vec<double> &bz = op.has_pml ? hist[2 * it + 1] : vz;
+    auto VX = [&](size_t q) { return bx[q]; };
+    auto VZ = [&](size_t q) { return bz[q]; };
     for (int ix = g.pml; ix < g.nx - g.pml; ix++)  // transpose of the Born source at step it
       for (int iz = g.pml; iz < g.nz - g.pml; iz++) {
         size_t k = g.I(ix, iz);
         grad[k] += -2.0 * op.lam[k] * (op.dxm(VX, ix, iz) / g.dx + op.dzm(VZ, ix, iz) / g.dz) * ge[k];
       }
-    op.step(vx, vz, sg, nullptr, ks, wav[it], -1);  // background back to step it-1
+    if (!op.has_pml) op.step(vx, vz, sg, sgx, sgz, nullptr, ks, wav[it], -1);  // back to it-1
   }
   return 0;
 }

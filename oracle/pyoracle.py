@@ -303,6 +303,7 @@ def ref_lib():
                                fp, fp, fp, fp]
         L.ref_release.argtypes = []
         L.ref_bandpass.argtypes = [I, I, I, I, I, I, fp, fp]
+        L.ref_cpu_acoustic.argtypes = [I, I, I, F, F, F, fp, fp, fp, I, I, fp, fp, dp]
         _ref = L
     return _ref
 
@@ -345,6 +346,22 @@ def ref_bandpass(img_pp, img_ps, z1, z2, x1=0, x2=0):
     if rc != 0:
         raise RuntimeError(f"ref_bandpass: CUDA error {rc}")
     return pp, ps
+
+
+def ref_cpu_acoustic(vp_pad, rho_pad, damp_pad, wavelet, isx, isz, dt, dx, dz):
+    """The reference's own CPU acoustic stepper (main.cpp:602-727, OpenMP, all host threads)
+    driven for len(wavelet) steps with the source split over px, pz at (isx, isz); padded
+    [nxpml][nzpml] inputs.  Returns (final p, seconds)."""
+    nxpml, nzpml = vp_pad.shape
+    out = np.zeros((nxpml, nzpml), np.float32)
+    sec = ctypes.c_double(0.0)
+    w = _f(wavelet)
+    rc = ref_lib().ref_cpu_acoustic(nxpml, nzpml, len(w), dt, dx, dz, _p(_f(vp_pad)),
+                                    _p(_f(rho_pad)), _p(_f(damp_pad)), isx, isz, _p(w), _p(out),
+                                    ctypes.byref(sec))
+    if rc != 0:
+        raise RuntimeError(f"ref_cpu_acoustic: {rc}")
+    return out, sec.value
 
 
 def ref_release():

@@ -68,8 +68,8 @@ def make_c1(outdir):
 
 def make_born(outdir):
     """First-order Born records by the reference's own born_modeling (mode 1), small case, two
-    shots each: vs = 0 with an injected random band and zero damping (the acoustic Born operator
-    of the elastic scheme, mu = 0), and the elastic model with the reference's PML."""
+    shots each: vs = 0 (the acoustic Born operator of the elastic scheme, mu = 0) with an injected
+    random band and zero damping, and with the reference's PML; the elastic model with the PML."""
     c = CASE
     g = (c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"])
     shots = geometry()
@@ -90,6 +90,11 @@ def make_born(outdir):
             for s, p in zip(shots, pads)]
     np.savez_compressed(os.path.join(outdir, "born_acoustic_random.npz"), vp=vp_mig, vs=vs0,
                         seed=np.uint64(1234), vp_pad=np.stack([p[0] for p in pads]),
+                        rec_vz=np.stack([r[0] for r in recs]), rec_vx=np.stack([r[1] for r in recs]),
+                        **common)
+    # acoustic with the reference's PML (vs = 0)
+    recs = [po.ref_born(*g, vp_mig, vs0, w, img_pp, zero, s) for s in shots]
+    np.savez_compressed(os.path.join(outdir, "born_acoustic_pml.npz"), vp=vp_mig, vs=vs0,
                         rec_vz=np.stack([r[0] for r in recs]), rec_vx=np.stack([r[1] for r in recs]),
                         **common)
     # elastic with PML, both perturbations
