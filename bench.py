@@ -66,7 +66,8 @@ def parse():
     p.add_argument("--lsrtm-size", default="full", choices=["small", "full"],
                    help="full: 2001x601, 80 shots, nt 5000; small: 512x256, 40 shots, nt 2000")
     p.add_argument("--lsrtm-boundary", default="random", choices=["random", "pml"],
-                   help="boundary of the LSRTM operators: random band (exact background "
+                   help="boundary of the LSRTM and acoustic workloads' operators: random band "
+                        "(exact background "
                         "reversal) or the reference's PML with the background rebuilt from strips")
     p.add_argument("--lsrtm-strips", default="bf16", choices=["f32", "f16", "bf16"],
                    help="storage of the background's boundary strips with --lsrtm-boundary pml")
@@ -622,8 +623,9 @@ def run_reference(args, rank, world):
 def run_acoustic(args):
     """The acoustic Born pair of CG-LSRTM (configs 3 / 5): L^T L (ds2d_ac_normal: background with
     the Born source, scattered set with records, background replay, fused reverse step) on the
-    2001x601 grid with a 20-cell random band; shots evenly spread, nt from --nt (default 60 here,
-    the profiling case).  Timed with CUDA events on the library's stream."""
+    2001x601 grid with a 20-cell random band (or, with --lsrtm-boundary pml, the reference's PML
+    and the background rebuilt from --lsrtm-strips boundary strips); shots evenly spread, nt from
+    --nt (default 60 here, the profiling case).  Timed with CUDA events on the library's stream."""
     import torch
     from ds2d_b200 import Elastic2D, synth
     allnx, allnz, band = 2001, 601, 20
@@ -634,7 +636,8 @@ def run_acoustic(args):
     shots = synth.surface_shots(allnx, allnx, band, nshots)
     m = torch.from_numpy(synth.reflectivity(allnx, allnz, seed=4, density=0.05, std=0.05)).cuda()
     img = torch.zeros_like(m)
-    with Elastic2D(allnx, allnz, allnx, band, nt, 10.0, 10.0, 0.0008, boundary="random",
+    with Elastic2D(allnx, allnz, allnx, band, nt, 10.0, 10.0, 0.0008,
+                   boundary=args.lsrtm_boundary, strips=args.lsrtm_strips,
                    max_shots=nshots, max_ntr=allnx, seed=3) as e:
         e.set_models(vp, 0 * vp)
         e.set_wavelet(w)
@@ -657,6 +660,8 @@ def run_acoustic(args):
             "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (linear 1800-4500 m/s background, seeded sparse reflectivity)",
             "config": {"workload": "acoustic normal operator L^T L", "grid": "2001x601 (+20 band)",
+                       "boundary": args.lsrtm_boundary,
+                       "strips": args.lsrtm_strips if args.lsrtm_boundary == "pml" else None,
                        "shots": nshots, "nt": nt, "cell_updates_per_step": upd}}
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_acoustic(allnx, allnz, band, vp, w, shots[0])
@@ -801,7 +806,8 @@ def run_lsrtm(args):
             h = [t for t, v in zip(ms, r) if v <= level]
             return round(h[0] / 1e3, 2) if h else None
         res[name] = {"time_to_target_s": round(hit[0] / 1e3, 3) if hit else None,
-                     "time_to_residual_s": {str(lv): time_to(lv) for lv in (0.5, 0.3, 0.2, 0.15, 0.1)},
+                     "time_to_residual_s": {str(lv): time_to(lv)
+                                            for lv in (0.5, 0.3, 0.2, 0.15, 0.1, 0.05, 0.02, 0.01)},
                      "iterations": len(r), "residual": [round(float(v), 5) for v in r],
                      "elapsed_s": [round(float(t) / 1e3, 2) for t in ms],
                      "image_rel_error_vs_true": round(err, 4)}

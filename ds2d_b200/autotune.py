@@ -5,11 +5,12 @@ The knobs are the rows marched per CTA (`xr`), the depth of the cp.async prefetc
 the register / occupancy target (`occ`) and the threads per CTA (`cta`, 128 or 192) of the
 one-column ring kernels, and, for the random boundary, the pair-blocked bulk-copy kernels
 (`pair`) with their CTA widths (`pair_cta` backward, `pair_fcta` forward), rows per CTA
-(`pair_xr`) and the backward step fused or split in two launches (`pair_split`).  Their best values depend on the grid, the number of
-resident shots and the boundary, so the tuner times each candidate on a probe context with the
-caller's grid and batch but only `probe_nt` time steps (an RTM of the same shots: one forward and
-one backward fused launch per step), and returns the fastest setting; `apply` copies it onto the
-production context.  Everything runs through the public API on the GPU."""
+(`pair_xr`) and the backward step fused or split in two launches (`pair_split`); `pair` 2
+takes the pair kernel for the forward step only, with the backward on the one-column kernel.
+Their best values depend on the grid, the number of resident shots and the boundary, so the
+tuner times each candidate on a probe context with the caller's grid and batch but only
+`probe_nt` time steps (an RTM of the same shots: one forward and one backward fused launch per
+step), and returns the fastest setting; `apply` copies it onto the production context.  Everything runs through the public API on the GPU."""
 import numpy as np
 
 from .api import Elastic2D
@@ -22,10 +23,13 @@ _RING_SPACE = [
 ]
 # Pair-blocked kernels (random boundary only): backward CTA width x rows per CTA (0 = the
 # library's wave-filling choice).
-_PAIR_SPACE = ([{"pair": 1, "pair_split": 0, "pair_cta": cta, "pair_fcta": fcta, "pair_xr": xr}
-                for cta, fcta in ((64, 64), (256, 256), (256, 64)) for xr in (0, 96, 160)] +
-               [{"pair": 1, "pair_split": 1, "pair_cta": 0, "pair_fcta": fcta, "pair_xr": xr}
-                for fcta in (64, 256) for xr in (0, 96, 160)])
+_PAIR_SPACE = ([{"pair": 2, "pair_split": 0, "pair_cta": 0, "pair_fcta": fcta, "pair_xr": xr,
+                 "cta": cta}
+                for fcta in (256, 64) for xr in (0, 143) for cta in (192, 128)] +
+               [{"pair": 1, "pair_split": 0, "pair_cta": cta, "pair_fcta": 256, "pair_xr": xr}
+                for cta in (256, 64) for xr in (0, 96)] +
+               [{"pair": 1, "pair_split": 1, "pair_cta": 0, "pair_fcta": 256, "pair_xr": xr}
+                for xr in (0, 96)])
 _RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0}
 
 

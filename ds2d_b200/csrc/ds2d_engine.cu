@@ -649,14 +649,18 @@ constexpr size_t pair_bwd_smem(int cta) {
   return pair_smem(cta, kPairBwdD, kBwdPairFields, bwd_pair_z2_rows(0));
 }
 
-bool pair_on(const ds2d_ctx *c) {
-  return c->opt_pair && c->opt_fused && c->ring_ok && c->d.rbc && c->d.nop == 4 &&
-         c->d.ild == c->d.ld && c->d_err && c->occ_pair[0] > 0;
+bool pair_ok(const ds2d_ctx *c) {
+  return c->opt_fused && c->ring_ok && c->d.rbc && c->d.nop == 4 && c->d.ild == c->d.ld &&
+         c->d_err && c->occ_pair[0] > 0;
 }
+// option "pair": 0 none, 1 forward and backward, 2 forward only (the backward stays on the
+// one-column ring kernel)
+bool pair_fwd_on(const ds2d_ctx *c) { return c->opt_pair && pair_ok(c); }
+bool pair_bwd_on(const ds2d_ctx *c) { return c->opt_pair == 1 && pair_ok(c); }
 // CTA widths (options "pair_cta" backward, "pair_fcta" forward; 0 = automatic): narrow 64-thread
 // strips by default (more CTAs per SM, barriers of two warps).
 int pair_bwd_cta(const ds2d_ctx *c) { return c->opt_pair_cta ? c->opt_pair_cta : 64; }
-int pair_fwd_cta(const ds2d_ctx *c) { return c->opt_pair_fcta ? c->opt_pair_fcta : 64; }
+int pair_fwd_cta(const ds2d_ctx *c) { return c->opt_pair_fcta ? c->opt_pair_fcta : 256; }
 // resident CTAs per SM of each variant (queried at create)
 int pair_occ(const ds2d_ctx *c, bool fwd, int cta) {
   if (fwd) return cta == 64 ? c->occ_pair[1] : c->occ_pair[0];
@@ -718,7 +722,7 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
     a.d = d; a.a = *cur; a.b = *nxt; a.p = c->par; a.shots = c->d_shots; a.wavelet = c->wavelet;
     a.it = it; a.tz = tz; a.xr = xr; a.rmap = c->d_rmap;
     if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
-    if (pair_on(c)) {
+    if (pair_fwd_on(c)) {
       const int pc = pair_fwd_cta(c);
       int pns, ptz;
       pair_split(d, pc, &pns, &ptz);
@@ -895,7 +899,7 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
       a.shots = c->d_shots; a.rmap = c->d_rmap; a.res_vz = c->rec[0]; a.res_vx = c->rec[1];
       a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
       a.img = c->img_slot; a.img_plane = (long long)plane;
-      if (pair_on(c) && c->opt_pair_split) {
+      if (pair_bwd_on(c) && c->opt_pair_split) {
         int pns, ptz;
         pair_split(d, kPairSplitT, &pns, &ptz);
         const int pxr = pair_xr(c, pns, std::min(c->occ_pair[5], c->occ_pair[6]));
@@ -916,7 +920,7 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
         }
         CK(cudaEventRecord(c->ev_join, c->aux));
         CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
-      } else if (pair_on(c)) {
+      } else if (pair_bwd_on(c)) {
         const int pc = pair_bwd_cta(c);
         int pns, ptz;
         pair_split(d, pc, &pns, &ptz);
@@ -2164,7 +2168,8 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
       return fail(c, DS2D_E_ARG, "cta must be 0 (automatic), 128 or 192");
     c->opt_cta = (int)value;
   } else if (k == "pair") {
-    if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "pair must be 0 or 1");
+    if (value < 0 || value > 2)
+      return fail(c, DS2D_E_ARG, "pair must be 0, 1 (forward and backward) or 2 (forward only)");
     c->opt_pair = (int)value;
   } else if (k == "pair_cta") {
     if (value != 0 && value != 64 && value != 160 && value != 256)

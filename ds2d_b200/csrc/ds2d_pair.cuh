@@ -11,9 +11,9 @@
 //    predicates, barrier) is paid once per two cells.
 //  * Rows arrive by bulk copy.  Each ring slot holds, for one row step, every row segment the
 //    step consumes (the newest stencil rows, the z-tap rows of stage 1 and the own-cell operands
-//    of both stages).  One thread issues one cp.async.bulk per field row (global -> shared,
-//    completion counted on the slot's mbarrier) kD - 1 steps ahead; the other threads only wait
-//    on the barrier's phase.  Stage-1 z-taps are read straight from the ring, so a step has a
+//    of both stages).  The lanes of warp 0 issue one cp.async.bulk per field row (global ->
+//    shared, completion counted on the slot's mbarrier) kD - 1 steps ahead; every thread then
+//    waits on the barrier's phase before it reads the slot.  Stage-1 z-taps are read straight from the ring, so a step has a
 //    single CTA barrier (before the stage-2 z-taps, whose rows are computed in registers).
 //  * Injections as corrections.  The explosive source (forward) and the receiver residual
 //    (adjoint) act on the stencil values only (the reference adds them to the summed arrays,
@@ -46,13 +46,16 @@ __device__ __forceinline__ void mbar_arrive_tx(unsigned long long *bar, unsigned
                "r"(bytes)
                : "memory");
 }
+// One bounded poll: the thread may be suspended for up to kSuspendNs while the phase is open, so
+// a waiting warp sleeps instead of re-issuing the poll.
+constexpr unsigned kSuspendNs = 200000;
 __device__ __forceinline__ bool mbar_test(unsigned long long *bar, unsigned parity) {
   unsigned ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "n"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
@@ -66,15 +69,23 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
       : "memory");
 }
 
-// Polls of one phase before a wait gives up (each try_wait may itself suspend for a while):
-// far beyond any copy's latency, short of a hang.  A kernel that gives up raises the error word
-// (code kErrRingWait) and leaves its march; the host turns the word into an error.
-constexpr int kRingWaitPolls = 1 << 22;
+// A wait gives up once kRingWaitNs of device time have passed with the phase still open (read
+// from %globaltimer, so the bound holds whatever the suspend hint does): far beyond any copy's
+// latency, short of a hang.  A kernel that gives up raises the error word (code kErrRingWait)
+// and leaves its march; the host turns the word into an error.
+constexpr unsigned long long kRingWaitNs = 2000000000ull;
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 constexpr int kErrRingWait = 1;
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
-  for (int i = 0; i < kRingWaitPolls; i++)
-    if (mbar_test(bar, parity)) return true;
-  return false;
+  if (mbar_test(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_test(bar, parity))
+    if (global_ns() - t0 > kRingWaitNs) return false;
+  return true;
 }
 
 // Floats per ring row of a kT-thread CTA: two columns per thread plus two pairs of padding on
@@ -554,7 +565,10 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
 
   RingCursor<kD> cur;
   bool ok = true, aborted = false;
-#pragma unroll 1
+  // Two row steps per loop iteration let the compiler rename half of the window shifts away
+  // where the registers allow it (the split parts); the fused pass is at its register limit.
+  constexpr int kUnroll = kPart == 0 ? 1 : 2;
+#pragma unroll kUnroll
   for (int r = rs0; r < x1 + 8; r++) {
     // A wait that gives up skips the step's work; the barrier below is a vote, so every thread
     // leaves the march together (none is left waiting at a barrier).

@@ -206,3 +206,101 @@ def test_ac_born_vs_reference_golden(cuda_device):
             floor = rel(b32[j], b64[j])
             err = rel(got[i * ntr:(i + 1) * ntr], fx[key][i])
             assert err < gate(floor), (key, i, err, f"FP32 floor {floor:.3e}")
+
+
+def _pml_case(nt=300):
+    c = dict(allnx=64, allnz=36, nx=64, pml=12, nt=nt, dx=10.0, dz=10.0, dt=0.0008, f0=15.0)
+    vp = np.broadcast_to(np.linspace(1800, 4500, c["allnz"], dtype=np.float32),
+                         (c["allnx"], c["allnz"])).copy()
+    w = synth.ricker(nt, c["f0"], c["dt"])
+    shots = synth.surface_shots(c["allnx"], c["nx"], c["pml"], 3)
+    m = synth.reflectivity(c["allnx"], c["allnz"], seed=4, density=0.05, std=0.05)
+    m[:, :3] = 0
+    return c, vp, w, shots, m
+
+
+def _pml_run(c, vp, w, shots, m, strips, rz=None, rx=None):
+    with Elastic2D(c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                   boundary="pml", strips=strips, max_shots=len(shots), max_ntr=c["nx"]) as e:
+        e.set_models(vp, 0 * vp)
+        e.set_wavelet(w)
+        dz, dx = e.ac_born(shots, m)
+        g = e.ac_born_adj(shots, dz if rz is None else rz, dx if rx is None else rx)
+    return dz, dx, g
+
+
+def test_ac_born_pml_vs_oracle_and_adjoint(cuda_device):
+    """The acoustic Born pair with the reference's PML (split, damped update with mu = 0) and the
+    background rebuilt on the interior from FP32 strips: L against the FP64 oracle, L^T against the
+    oracle's exact transpose (which keeps the whole background history), and the dot-product test
+    <L m, d> = <m, L^T d> in FP32."""
+    c, vp, w, shots, m = _pml_case()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    rng = np.random.default_rng(3)
+    ntr = shots[0].ntr
+    rz = rng.normal(size=(len(shots) * ntr, c["nt"])).astype(np.float32)
+    rx = rng.normal(size=rz.shape).astype(np.float32)
+    dz, dx, g = _pml_run(c, vp, w, shots, m, "f32", rz, rx)
+    gref = np.zeros((c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        model = po.build_model(st, vp, 0 * vp, None, s.win_left)
+        assert model[5].max() > 0  # a damped PML
+        oz, ox = po.ac_born(st, model, w, s, pad(st, m, s, c))
+        assert rel(dz[i * ntr:(i + 1) * ntr], oz) < BORN_GATE
+        assert rel(dx[i * ntr:(i + 1) * ntr], ox) < BORN_GATE
+        gp = po.ac_born_adj(st, model, w, s, rz[i * ntr:(i + 1) * ntr], rx[i * ntr:(i + 1) * ntr])
+        gref[s.win_left:s.win_left + c["nx"]] += gp[c["pml"]:c["pml"] + c["nx"], c["pml"]:-c["pml"]]
+    assert rel(g, gref) < BORN_GATE, rel(g, gref)
+    lhs = float(np.dot(dz.ravel().astype(np.float64), rz.ravel()) +
+                np.dot(dx.ravel().astype(np.float64), rx.ravel()))
+    rhs = float(np.dot(m.ravel().astype(np.float64), g.ravel()))
+    assert abs(lhs - rhs) <= 1e-4 * abs(lhs), (lhs, rhs)
+
+
+@pytest.mark.parametrize("strips,gate", [("f16", 2e-3), ("bf16", 2e-2)])
+def test_ac_born_adj_pml_half_precision_strips(cuda_device, strips, gate):
+    """L^T with the background's boundary strips stored in FP16 / BF16 (one FP32 scale per
+    32-cell segment) against the FP64 oracle's exact transpose: the error the storage format adds
+    to the gradient (gates: FP16 2e-3, BF16 2e-2 relative L2)."""
+    c, vp, w, shots, m = _pml_case()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    rng = np.random.default_rng(8)
+    ntr = shots[0].ntr
+    rz = rng.normal(size=(len(shots) * ntr, c["nt"])).astype(np.float32)
+    rx = rng.normal(size=rz.shape).astype(np.float32)
+    _, _, g16 = _pml_run(c, vp, w, shots, m, strips, rz, rx)
+    gref = np.zeros((c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        model = po.build_model(st, vp, 0 * vp, None, s.win_left)
+        gp = po.ac_born_adj(st, model, w, s, rz[i * ntr:(i + 1) * ntr], rx[i * ntr:(i + 1) * ntr])
+        gref[s.win_left:s.win_left + c["nx"]] += gp[c["pml"]:c["pml"] + c["nx"], c["pml"]:-c["pml"]]
+    err = rel(g16, gref)
+    assert err < gate, f"{strips} strips: L^T vs FP64 oracle {err:.3e}"
+
+
+def test_ac_born_pml_vs_reference_golden(cuda_device):
+    """The acoustic Born operator with the PML against the reference's own born_modeling (mode 1)
+    with vs = 0 and its PML (tests/golden/born_acoustic_pml.npz), at the FP32 floor of the
+    scheme."""
+    from tests.helpers import case_of, gate, load, shots_of
+    fx = load("born_acoustic_pml.npz")
+    assert fx is not None, "golden fixture born_acoustic_pml.npz missing"
+    c = case_of(fx)
+    shots = shots_of(fx)
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    with Elastic2D(c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
+                   boundary="pml", max_shots=len(shots), max_ntr=max(s.ntr for s in shots)) as e:
+        e.set_models(fx["vp"], fx["vs"])
+        e.set_wavelet(fx["wavelet"])
+        dz, dx = e.ac_born(shots, fx["img_pp"])
+    ntr = shots[0].ntr
+    zero = np.zeros_like(fx["img_pp"])
+    for i, s in enumerate(shots):
+        model = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left)
+        dmp = po.window_image(st, fx["img_pp"], s.win_left)
+        b64 = po.born(st, model, dmp, po.window_image(st, zero, s.win_left), fx["wavelet"], s, "f64")
+        b32 = po.born(st, model, dmp, po.window_image(st, zero, s.win_left), fx["wavelet"], s, "f32")
+        for got, key, j in ((dz, "rec_vz", 0), (dx, "rec_vx", 1)):
+            floor = rel(b32[j], b64[j])
+            err = rel(got[i * ntr:(i + 1) * ntr], fx[key][i])
+            assert err < gate(floor), (key, i, err, f"FP32 floor {floor:.3e}")

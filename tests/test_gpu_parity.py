@@ -419,14 +419,18 @@ def test_live_reference_rtm_random(cuda_device):
         assert err < gate(floor), f"{key}: vs reference {err:.3e}, FP32 floor {floor:.3e}"
 
 
-@pytest.mark.parametrize("pair_cta,pair_fcta", [(64, 64), (256, 256), (160, 64)])
+@pytest.mark.parametrize("mode,pair_cta,pair_fcta,pair_split", [(1, 64, 64, 0), (1, 256, 256, 0),
+                                                              (1, 160, 64, 0), (1, 0, 64, 1),
+                                                              (2, 0, 256, 0)])
 @pytest.mark.parametrize("pair_xr", [0, 24])
-def test_pair_kernels_match_ring_and_oracle(cuda_device, pair_cta, pair_fcta, pair_xr):
+def test_pair_kernels_match_ring_and_oracle(cuda_device, mode, pair_cta, pair_fcta, pair_split,
+                                            pair_xr):
     """Pair-blocked bulk-copy kernels of the random-boundary RTM step (forward with receiver
     records, backward with the residual injection and the imaging condition) against the
-    one-column ring kernels and the FP64 oracle.  On the 320-deep grid the 64-thread CTAs run four
-    z-strips and the 160-thread ones two; xr 24 gives each shot four row blocks (x-halos between
-    CTAs)."""
+    one-column ring kernels and the FP64 oracle; fused, or split into a reconstruction launch and
+    an adjoint + imaging launch.  On the 320-deep grid the 64-thread CTAs run four z-strips and
+    the 160-thread ones two; xr 24 gives each shot four row blocks (x-halos between CTAs).  Mode
+    2 runs the pair kernel for the forward step only and the one-column kernel backward."""
     c, _, _, w, _ = small_case(nt=200)
     c["allnz"] = 300
     vp, vs = synth.layered(c["allnx"], c["allnz"], seed=4)
@@ -439,10 +443,11 @@ def test_pair_kernels_match_ring_and_oracle(cuda_device, pair_cta, pair_fcta, pa
     out = {}
     for pair in (0, 1):
         with _ctx(c, shots, boundary="random", seed=5) as e:
-            e.set_option("pair", pair)
+            e.set_option("pair", mode if pair else 0)
             if pair:
                 e.set_option("pair_cta", pair_cta)
                 e.set_option("pair_fcta", pair_fcta)
+                e.set_option("pair_split", pair_split)
                 e.set_option("pair_xr", pair_xr)
             e.set_models(vpm, vsm)
             e.set_wavelet(w)

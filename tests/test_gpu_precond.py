@@ -6,6 +6,8 @@ import numpy as np
 import pytest
 
 from ds2d_b200 import Elastic2D, precond, synth
+from oracle import pyoracle as po
+from tests.helpers import rel
 
 pytestmark = pytest.mark.gpu
 
@@ -40,3 +42,80 @@ def test_trained_network_beats_plain_cg(cuda_device):
     # the gain: a clearly lower residual after the first iterations
     assert learned[0] < 0.95 * plain[0], (learned, plain)
     assert learned[-1] < plain[-1], (learned, plain)
+
+
+def _oracle_cgls(st, models, w, shots, d, niter):
+    """CGLS in FP64 on the oracle's Born pair (the least-squares reference)."""
+    L = lambda mm: [po.ac_born(st, models[i], w, s, mm) for i, s in enumerate(shots)]
+    LT = lambda dd: sum(po.ac_born_adj(st, models[i], w, s, *dd[i]) for i, s in enumerate(shots))
+    dot = lambda a, b: sum((x * y).sum() + (u * v).sum() for (x, u), (y, v) in zip(a, b))
+    mm = np.zeros(st.shape)
+    r = [(a.copy(), b.copy()) for a, b in d]
+    s_ = LT(r)
+    p = s_.copy()
+    gam = (s_ * s_).sum()
+    for _ in range(niter):
+        q = L(p)
+        al = gam / dot(q, q)
+        mm += al * p
+        r = [(a - al * x, b - al * y) for (a, b), (x, y) in zip(r, q)]
+        s_ = LT(r)
+        gn = (s_ * s_).sum()
+        p = s_ + (gn / gam) * p
+        gam = gn
+    return mm
+
+
+def test_learned_and_plain_image_error_vs_fp64_oracle(cuda_device):
+    """Final image error of plain CG-LSRTM and of the learned-preconditioned solver, both run on
+    the GPU for the same number of iterations, against the FP64 oracle's least-squares image
+    (oracle CGLS run five times as long on the same Born data) and against the true reflectivity.
+    The plain run must match the oracle's CGLS after the same iterations to FP32 rounding; both
+    images must be closer to the least-squares image than the zero image is.  The learned solver
+    lowers the data residual faster (test_trained_network_beats_plain_cg) but walks a different
+    path than CGLS through an under-determined problem, so it is not required to be closer to
+    CGLS's own limit: the two errors are reported side by side."""
+    import torch
+    from ds2d_b200.unet import UNet, he_normal
+    nx, nz, band, nt, dx, dt, iters = 96, 48, 12, 500, 10.0, 0.0008, 4
+    shots = synth.surface_shots(nx, nx, band, 8)
+    st = po.Setup(nx, nz, nx, band, dx, dx, dt)
+    with Elastic2D(nx, nz, nx, band, nt, dx, dx, dt, boundary="random", max_shots=len(shots),
+                   max_ntr=nx, seed=3) as e:
+        vp = precond.background(nx, nz, seed=1)
+        w = synth.ricker(nt, 15.0, dt)
+        e.set_models(vp, np.zeros_like(vp))
+        e.set_wavelet(w)
+        X, Y = precond.make_trajectory_pairs(e, shots, nmodels=8, iters=8, seed=5)
+        models = [po.build_model(st, vp, 0 * vp, None, s.win_left, rbc=1, seed=3, shot_id=i)
+                  for i, s in enumerate(shots)]
+        rng = np.random.default_rng(99)
+        m_true = precond.random_reflectivity(nx, nz, rng, reflectors=0)
+        mp = np.zeros(st.shape)
+        mp[band:band + nx, band:-band] = m_true
+        d = [po.ac_born(st, models[i], w, s, mp) for i, s in enumerate(shots)]  # FP64 data
+        dz = torch.from_numpy(np.concatenate([a for a, _ in d]).astype(np.float32)).cuda()
+        dxr = torch.from_numpy(np.concatenate([b for _, b in d]).astype(np.float32)).cuda()
+        with UNet(max_n=8, max_h=nx, max_w=nz) as net:
+            net.set_params(he_normal(2))
+            precond.train(net, X, Y, steps=800, batch=8, crop=(48, None), lr=1e-3)
+            m = torch.zeros((nx, nz), device="cuda")
+            res_p, _ = e.lsrtm_pcg(shots, dz.data_ptr(), dxr.data_ptr(), m.data_ptr(), iters)
+            m_plain = m.cpu().numpy().astype(np.float64)
+            m.zero_()
+            res_l, _ = e.lsrtm_pcg(shots, dz.data_ptr(), dxr.data_ptr(), m.data_ptr(), iters,
+                                   net=net)
+            m_learned = m.cpu().numpy().astype(np.float64)
+    crop = lambda a: a[band:band + nx, band:-band]
+    m_same = crop(_oracle_cgls(st, models, w, shots, d, iters))
+    m_ls = crop(_oracle_cgls(st, models, w, shots, d, 5 * iters))
+    err_same = rel(m_plain, m_same)
+    e_plain, e_learned = rel(m_plain, m_ls), rel(m_learned, m_ls)
+    t_plain, t_learned = rel(m_plain, m_true), rel(m_learned, m_true)
+    print(f"after {iters} iterations: image error vs FP64 oracle LS image: plain {e_plain:.3f}, "
+          f"learned {e_learned:.3f}; vs true reflectivity: plain {t_plain:.3f}, learned "
+          f"{t_learned:.3f}; data residual: plain {res_p[-1]:.3f}, learned {res_l[-1]:.3f}; "
+          f"plain vs oracle CGLS after {iters} iterations {err_same:.2e}")
+    assert err_same < 5e-3, err_same
+    assert e_plain < 1.0 and e_learned < 1.0, (e_plain, e_learned)
+    assert res_l[-1] < res_p[-1], (res_l, res_p)
