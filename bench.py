@@ -639,6 +639,9 @@ def run_acoustic(args):
     with Elastic2D(allnx, allnz, allnx, band, nt, 10.0, 10.0, 0.0008,
                    boundary=args.lsrtm_boundary, strips=args.lsrtm_strips,
                    max_shots=nshots, max_ntr=allnx, seed=3) as e:
+        opts = parse_set(args.set)
+        for k, v in opts.items():
+            e.set_option(k, v)
         e.set_models(vp, 0 * vp)
         e.set_wavelet(w)
         stream = torch.cuda.Stream()
@@ -662,7 +665,8 @@ def run_acoustic(args):
             "config": {"workload": "acoustic normal operator L^T L", "grid": "2001x601 (+20 band)",
                        "boundary": args.lsrtm_boundary,
                        "strips": args.lsrtm_strips if args.lsrtm_boundary == "pml" else None,
-                       "shots": nshots, "nt": nt, "cell_updates_per_step": upd}}
+                       "shots": nshots, "nt": nt, "cell_updates_per_step": upd,
+                       "options": opts}}
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_acoustic(allnx, allnz, band, vp, w, shots[0])
     return out

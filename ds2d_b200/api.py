@@ -266,7 +266,8 @@ class Elastic2D:
         return out
 
     def set_option(self, key, value):
-        """Tuning knob: "fused" (0/1) or "xr" (rows per CTA of the fused kernels)."""
+        """Tuning knob by name ("fused", "xr", "ring", "occ", "cta", "graph", "pair", "pair_xr",
+        "ac_pair", ...; the list and ranges are documented at ds2d_set_option in ds2d.h)."""
         self._check(self.lib.ds2d_set_option(self.h, key.encode(), int(value)))
 
     def profile(self, enable=True):

@@ -261,6 +261,7 @@ struct ds2d_ctx {
   // "pair_cta" (backward CTA width: 0 auto, 256 or 160), "pair_xr" (rows per CTA: 0 = chosen to
   // fill whole waves).
   int opt_pair = 0, opt_pair_cta = 0, opt_pair_fcta = 0, opt_pair_xr = 0, opt_pair_split = 0;
+  int opt_ac_pair = 1, opt_ac_pair_cta = 0;  // acoustic steps on k_ac_pair / k_ac_rev_pair
   // split backward: the two launches of a step as parallel branches (second stream, fork / join
   // events; parallel nodes in a captured graph)
   cudaStream_t aux = nullptr;
@@ -269,6 +270,8 @@ struct ds2d_ctx {
   int num_sms = 148;
   // resident CTAs per SM: forward 256 / 64, backward 256 / 160 / 64, split parts 1 / 2
   int occ_pair[7] = {0, 0, 0, 0, 0, 0, 0};
+  int occ_ac_pair[3] = {0, 0, 0};  // k_ac_pair, 256 / 192 / 128 threads
+  int occ_ac_rev[2] = {0, 0};      // k_ac_rev_pair, 192 / 128 threads
   std::vector<int> h_nxp;    // padded window rows of each slot of the current batch
   int opt_pcg_switch = 970;  // ds2d_lsrtm_pcg: per-mille residual ratio that ends the network phase
   int opt_pcg_m = 8;         // ds2d_lsrtm_pcg: directions kept for explicit conjugation
@@ -703,6 +706,61 @@ int check_pair_err(ds2d_ctx *c) {
     return fail(c, DS2D_E_CUDA, "a pair kernel's ring wait gave up (error word %d)", h);
   }
   return DS2D_OK;
+}
+
+// Acoustic pair kernels (k_ac_pair): 256 / 192 / 128 threads at 2 / 3 / 4 CTAs per SM.
+constexpr int kAcPairCtas[3] = {256, 192, 128};
+using AcPairFn = void (*)(AcRingArgs);
+AcPairFn ac_pair_fn(int mode, int cta) {
+  if (cta == 256) return mode ? k_ac_pair<1, 256, 2> : k_ac_pair<0, 256, 2>;
+  if (cta == 192) return mode ? k_ac_pair<1, 192, 3> : k_ac_pair<0, 192, 3>;
+  return mode ? k_ac_pair<1, 128, 4> : k_ac_pair<0, 128, 4>;
+}
+int ac_pair_idx(int cta) { return cta == 256 ? 0 : cta == 192 ? 1 : 2; }
+// CTA width: option "ac_pair_cta", else the width with the fewest threads per grid row (z-strips
+// x threads; the wider on a tie), so the z-halo recomputed and the idle columns stay small.
+int ac_pair_cta(const ds2d_ctx *c) {
+  if (c->opt_ac_pair_cta) return c->opt_ac_pair_cta;
+  int best = 256, best_thr = 1 << 30;
+  for (int cta : kAcPairCtas) {
+    int ns, tz;
+    pair_split(c->d, cta, &ns, &tz);
+    if (ns * cta < best_thr) {
+      best_thr = ns * cta;
+      best = cta;
+    }
+  }
+  return best;
+}
+bool ac_pair_on(const ds2d_ctx *c) {
+  return c->opt_ac_pair && pair_ok(c) && c->occ_ac_pair[ac_pair_idx(ac_pair_cta(c))] > 0;
+}
+// Reverse step (k_ac_rev_pair): 192 / 128 threads at 2 / 3 CTAs per SM, strips with a
+// 12-column halo (each CTA computes tz <= 2 kT - 24 columns); the width with the fewest threads
+// per grid row, the wider on a tie.
+constexpr int kAcRevCtas[2] = {192, 128};
+using AcRevFn = void (*)(AcRevArgs);
+AcRevFn ac_rev_fn(int cta) { return cta == 192 ? k_ac_rev_pair<192, 2> : k_ac_rev_pair<128, 3>; }
+void ac_rev_split(const Dims &d, int kT, int *nstrips, int *tz) {
+  const int w = 2 * kT - 2 * kAcRevHalo;
+  *nstrips = (d.nzp + w - 1) / w;
+  const int t = (d.nzp + *nstrips - 1) / *nstrips;
+  *tz = (t + 3) / 4 * 4;
+}
+int ac_rev_cta(const ds2d_ctx *c) {
+  int best = 192, best_thr = 1 << 30;
+  for (int cta : kAcRevCtas) {
+    int ns, tz;
+    ac_rev_split(c->d, cta, &ns, &tz);
+    if (ns * cta < best_thr) {
+      best_thr = ns * cta;
+      best = cta;
+    }
+  }
+  return best;
+}
+bool ac_rev_pair_on(const ds2d_ctx *c) {
+  return ac_pair_on(c) && c->occ_ac_rev[ac_rev_cta(c) == 192 ? 0 : 1] > 0;
 }
 
 // Fused forward pass: one k_fwd_fused launch per step, ping-ponging fw <-> fw2.
@@ -1262,6 +1320,16 @@ int ac_ring_step(ds2d_ctx *c, int n, int set, int cur, int it, bool born_out, bo
     a.e_in = c->ac[9];
     if (record) { a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
   }
+  if (ac_pair_on(c)) {
+    const int pc = ac_pair_cta(c);
+    int pns, ptz;
+    pair_split(d, pc, &pns, &ptz);
+    const int pxr = pair_xr(c, pns, c->occ_ac_pair[ac_pair_idx(pc)]);
+    a.tz = ptz; a.xr = pxr; a.err = c->d_err;
+    dim3 pgrid(pns, (d.nxp + pxr - 1) / pxr, n);
+    LAUNCHS("ac_pair", 0, ac_pair_fn(set, pc), pgrid, pc, ac_pair_smem(pc), a);
+    return DS2D_OK;
+  }
   const size_t sm = sizeof(float) * 4 * kAcRingFields * kFB;
   void (*kfn)(AcRingArgs) = set == 0 ? k_ac_ring<0, 4> : k_ac_ring<1, 4>;
   LAUNCHS("ac_ring", 0, kfn, grid, kFB, sm, a);
@@ -1377,6 +1445,31 @@ int ac_LT_batch(ds2d_ctx *c, int n) {
     // ac[0..2] and ac2[0..2], the adjoint state between ac[6..8] and ac2[3..5] (both start at
     // zero; cells outside the updated band are never written in either)
     for (int i = 3; i < 6; i++) CK(cudaMemsetAsync(c->ac2[i], 0, bytes, c->stream));
+    if (ac_rev_pair_on(c)) {
+      const int pc = ac_rev_cta(c);
+      int pns, ptz;
+      ac_rev_split(d, pc, &pns, &ptz);
+      const int pxr = pair_xr(c, pns, c->occ_ac_rev[pc == 192 ? 0 : 1]);
+      dim3 pgrid(pns, (d.nxp + pxr - 1) / pxr, n);
+      float *bk[2][3] = {{c->ac[0], c->ac[1], c->ac[2]}, {c->ac2[0], c->ac2[1], c->ac2[2]}};
+      float *yk[2][3] = {{c->ac[6], c->ac[7], c->ac[8]}, {c->ac2[3], c->ac2[4], c->ac2[5]}};
+      cur = 0;
+      for (int it = d.nt - 1; it >= 0; --it, cur ^= 1) {
+        AcRevArgs a{};
+        a.d = d; a.shots = c->d_shots;
+        a.yx = yk[cur][0]; a.yz = yk[cur][1]; a.ys = yk[cur][2];
+        a.yx_n = yk[cur ^ 1][0]; a.yz_n = yk[cur ^ 1][1]; a.ys_n = yk[cur ^ 1][2];
+        a.vx = bk[cur][0]; a.vz = bk[cur][1]; a.s = bk[cur][2];
+        a.vx_n = bk[cur ^ 1][0]; a.vz_n = bk[cur ^ 1][1]; a.s_n = bk[cur ^ 1][2];
+        a.b = c->par.b; a.lam = c->par.lam; a.grad = c->img_slot; a.wavelet = c->wavelet;
+        a.it = it; a.tz = ptz; a.xr = pxr; a.rmap = c->d_rmap;
+        a.res_vz = c->rec[0]; a.res_vx = c->rec[1]; a.err = c->d_err;
+        LAUNCHS("ac_rev_pair", kBytesAcRev * CELLS(n), ac_rev_fn(pc), pgrid, pc,
+                ac_rev_pair_smem(pc), a);
+      }
+      CK(cudaGetLastError());
+      return reduce_images(c, n, 1);
+    }
     const int nstrips = (d.nzp + kAcRevTZ - 1) / kAcRevTZ;
     const int tz = (d.nzp + nstrips - 1) / nstrips;
     const int xr = std::max(8, c->opt_xr);
@@ -1582,6 +1675,24 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
         if (e == cudaSuccess)
           e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_pair[i], pair_fwd_fn(fctas[i]),
                                                             fctas[i], pair_fwd_smem(fctas[i]));
+      }
+      for (int i = 0; i < 3 && e == cudaSuccess; i++) {
+        const int cta = kAcPairCtas[i];
+        for (int mode = 0; mode < 2 && e == cudaSuccess; mode++)
+          e = cudaFuncSetAttribute(ac_pair_fn(mode, cta),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)ac_pair_smem(cta));
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_ac_pair[i], ac_pair_fn(1, cta),
+                                                            cta, ac_pair_smem(cta));
+      }
+      for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+        const int cta = kAcRevCtas[i];
+        e = cudaFuncSetAttribute(ac_rev_fn(cta), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ac_rev_pair_smem(cta));
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_ac_rev[i], ac_rev_fn(cta), cta,
+                                                            ac_rev_pair_smem(cta));
       }
       for (int part = 1; part <= 2 && e == cudaSuccess; part++) {
         e = cudaFuncSetAttribute(pair_split_fn(part), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1871,7 +1982,7 @@ int ds2d_ac_born(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *m, flo
   if ((rc = data_io(c, shots, n, dz, rec_vz, false)) || (rc = data_io(c, shots, n, dx, rec_vx, false)))
     return rc;
   CK(cudaStreamSynchronize(c->stream));
-  return DS2D_OK;
+  return check_pair_err(c);
 }
 
 int ds2d_ac_born_adj(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *rec_vz,
@@ -1894,7 +2005,7 @@ int ds2d_ac_born_adj(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *re
   if ((rc = ac_apply(c, shots, n, true, nullptr, dz, dx, gv))) return rc;
   CK(cudaMemcpyAsync(grad, gv, nall * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return DS2D_OK;
+  return check_pair_err(c);
 }
 
 int ds2d_lsrtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *obs_vz,
@@ -1959,7 +2070,7 @@ int ds2d_lsrtm(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *obs_vz,
   if (iters_done) *iters_done = k;
   CK(cudaMemcpyAsync(m_out, m, nall * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return DS2D_OK;
+  return check_pair_err(c);
 }
 
 int ds2d_ac_normal(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *m, float *img) {
@@ -1979,7 +2090,7 @@ int ds2d_ac_normal(ds2d_ctx *c, const ds2d_shot *shots, int n, const float *m, f
   if ((rc = ac_apply(c, shots, n, true, nullptr, dz, dx, gv))) return rc;
   CK(cudaMemcpyAsync(img, gv, nall * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return DS2D_OK;
+  return check_pair_err(c);
 }
 
 }  // extern "C"
@@ -2127,7 +2238,7 @@ int ds2d_lsrtm_pcg(ds2d_ctx *c, ds2d_unet *net, const ds2d_shot *shots, int n, c
   if (iters_done) *iters_done = k;
   CK(cudaMemcpyAsync(m_out, m, nall * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  return DS2D_OK;
+  return check_pair_err(c);
 }
 
 int ds2d_dot_f64(ds2d_ctx *c, const float *a, const float *b, long long n, double *result) {
@@ -2175,6 +2286,13 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     if (value != 0 && value != 64 && value != 160 && value != 256)
       return fail(c, DS2D_E_ARG, "pair_cta must be 0 (automatic), 64, 160 or 256");
     c->opt_pair_cta = (int)value;
+  } else if (k == "ac_pair") {
+    if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "ac_pair must be 0 or 1");
+    c->opt_ac_pair = (int)value;
+  } else if (k == "ac_pair_cta") {
+    if (value != 0 && value != 128 && value != 192 && value != 256)
+      return fail(c, DS2D_E_ARG, "ac_pair_cta must be 0 (automatic), 128, 192 or 256");
+    c->opt_ac_pair_cta = (int)value;
   } else if (k == "pair_split") {
     if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "pair_split must be 0 or 1");
     c->opt_pair_split = (int)value;

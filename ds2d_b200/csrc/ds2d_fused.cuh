@@ -1376,6 +1376,7 @@ struct AcRingArgs {
   int it, tz, xr;
   const int *rmap;
   float *rec_vz, *rec_vx;    // mode 1: records [slot][max_ntr][nt]
+  int *err;                  // pair kernels: error word (a ring wait that gave up)
 };
 
 template <int kMode, int kD>
@@ -1507,6 +1508,7 @@ struct AcRevArgs {
   int it, tz, xr;
   const int *rmap;
   const float *res_vz, *res_vx;  // [slot][max_ntr][nt]
+  int *err;                      // pair kernel: error word (a ring wait that gave up)
 };
 
 template <int kD>

@@ -15,12 +15,13 @@
 //    shared, completion counted on the slot's mbarrier) kD - 1 steps ahead; every thread then
 //    waits on the barrier's phase before it reads the slot.  Stage-1 z-taps are read straight from the ring, so a step has a
 //    single CTA barrier (before the stage-2 z-taps, whose rows are computed in registers).
-//  * Injections as corrections.  The explosive source (forward) and the receiver residual
-//    (adjoint) act on the stencil values only (the reference adds them to the summed arrays,
-//    which its split update recomputes, FD2DGPU.cu:2039-2049, :3306-3322).  The owner of the
-//    injected column adds the value to its x-window entry; the z-derivatives of the columns
-//    within 4 of it add c_i * value for the taps that read it.  The own-cell operands come from
-//    the ring, i.e. from memory, without the injection.
+//  * Injections on the stencil values only.  The explosive source (forward) and the receiver
+//    residual (adjoint) act on the stencil values, not on the stored state (the reference adds
+//    them to the summed arrays, which its split update recomputes, FD2DGPU.cu:2039-2049,
+//    :3306-3322).  The owner of the injected column adds the value to its x-window entry; the
+//    threads whose z-taps read that column add it to their copy of the tap (the source, so the
+//    sum rounds as in the one-column kernels) or add c_i * value to the derivative (the
+//    residual).  The own-cell operands come from the ring, i.e. from memory, without it.
 //
 // Scope: random boundary (no PML cells, no strips), RTM forward (optional receiver recording)
 // and backward steps.  The PML / strip / Born variants stay on the one-column ring kernels.
@@ -80,6 +81,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 constexpr int kErrRingWait = 1;
+// True once a pair kernel of this context has given up a wait: later launches return at once, so
+// a failed step does not cost every later step its own wait bound before the host sees the word.
+__device__ __forceinline__ bool pair_err_raised(const int *err) {
+  return err && *(const volatile int *)err != 0;
+}
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
   if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
@@ -179,11 +185,12 @@ struct RingField {
   int lag, lo, hi;
 };
 
-template <int kT>
+template <int kT, int kHalo = 8>
 __device__ __forceinline__ void issue_slot_warp(const RingField &fd, float *slot_base, int f,
                                                 unsigned long long *bar, int q, int ld, int zs,
                                                 int lane) {
-  const int glo = max(0, zs - 8), ghi = min(ld, zs - 8 + 2 * kT);
+  // (strips with a kHalo-column halo: columns [zs - kHalo, zs - kHalo + 2 kT))
+  const int glo = max(0, zs - kHalo), ghi = min(ld, zs - kHalo + 2 * kT);
   const unsigned bytes = (unsigned)(ghi - glo) * 4u;
   const int row = q - fd.lag;
   const bool mine = fd.src != nullptr && row >= fd.lo && row < fd.hi;
@@ -191,7 +198,7 @@ __device__ __forceinline__ void issue_slot_warp(const RingField &fd, float *slot
   if (lane == 0) mbar_arrive_tx(bar, n * bytes);
   __syncwarp();
   if (mine)
-    bulk_g2s(slot_base + f * pair_row(kT) + (glo - (zs - 8) + 4),
+    bulk_g2s(slot_base + f * pair_row(kT) + (glo - (zs - kHalo) + 4),
              fd.src + (long long)row * ld + glo, bytes, bar);
 }
 
@@ -225,6 +232,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
   const int zs = blockIdx.x * a.tz;
   const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
   if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  if (__syncthreads_or(t == 0 && pair_err_raised(a.err))) return;  // whole CTA
   const int ld = d.ld, nop = d.nop;
   const long long fbase = d.slot * s;
   const int z0 = zs - 8 + 2 * t;
@@ -273,6 +281,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
   for (int i = 0; i < 9; i++) w_vx[i] = make_float2(0.f, 0.f);
 
   RingCursor<kD> cur;
+  int iw = 0;  // warp that issues the copies of this step
   bool ok = true, aborted = false;
 #pragma unroll 2
   for (int r = rs0; r < x1 + 8; r++) {
@@ -297,12 +306,9 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
     float2 vn = make_float2(0.f, 0.f), vzn = make_float2(0.f, 0.f);
     if (ok && c1 && r >= x0 && rv >= nop && rv < d.nxp - nop) {
       const Z10 zxz = z10(reinterpret_cast<const float2 *>(S + 2 * ROW), pi);
-      const Z10 zzz = z10(reinterpret_cast<const float2 *>(S + 3 * ROW), pi);
-      float ez0 = dzp<0>(zzz), ez1 = dzp<1>(zzz);
-      if (rv == sh.isx && src_near) {  // tzz of the source cell, read by the z-taps
-        ez0 += sval * (coef_or0(se) - coef_or0(1 - se));
-        ez1 += sval * (coef_or0(se - 1) - coef_or0(2 - se));
-      }
+      Z10 zzz = z10(reinterpret_cast<const float2 *>(S + 3 * ROW), pi);
+      if (rv == sh.isx && src_near) zzz.v[se + 4] += sval;  // tzz + source, as the ring kernel
+      const float ez0 = dzp<0>(zzz), ez1 = dzp<1>(zzz);
       const float2 bb = F2(6), ovx = F2(4), ovz = F2(5);
       const float ax0 = dxw_x(w_txx), ax1 = dxw_y(w_txx);
       const float fx0 = dxw_x(w_txz), fx1 = dxw_y(w_txz);
@@ -347,7 +353,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
       break;
     }
     // every thread is done with the previous slot: refill it kD - 1 steps ahead
-    if (t < 32) {
+    if ((t >> 5) == iw) {  // the step's issuing warp (round robin spreads the extra work)
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
       issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps], r + kD - 1, ld, zs,
                           lane);
@@ -388,6 +394,457 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
     }
     if (rec_col) cp_async_wait<7>();
     cur.advance();
+    if (++iw == kT / 32) iw = 0;
+  }
+  pair_exit<kD>(bars, cur, aborted, ok, a.err);
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Acoustic forward step (vs = 0: one stress s), pair-blocked: the counterpart of k_ac_ring with
+// the same arithmetic per cell (its modes, its overlay and source, its Born source and records).
+// At row step r the velocities of row r - 4 and the stress of row r - 8 are updated.  Ring fields
+// of step r:
+//   0 s(r)  1 e(r)                   x-window of S = s (+ e, mode 1)
+//   2 s(r-4)  3 e(r-4)               stage-1 z-tap rows of S
+//   4 vx(r-4)  5 vz(r-4)  6 b(r-4)   stage-1 own cells
+//   7 s(r-8)  8 lam(r-8)  9 m(r-8)   stage-2 own cells (m: mode 0 with the Born source written)
+// The e rows (mode 1) and m (mode 0 without a Born source) are not copied.  In mode 1 the z-taps
+// of S add the s and e rows column by column, so S is rounded as in k_ac_ring; in mode 0 the
+// source enters the x-window at its row and the z-tap copies of the columns within 4 of it.
+// ---------------------------------------------------------------------------------------------
+constexpr int kAcPairFields = 10;
+constexpr int kAcPairZ2Rows = 2;  // stage-2 z-tap row (vz of row r-8), double-buffered
+constexpr int kAcPairD = 4;
+__host__ __device__ constexpr size_t ac_pair_smem(int kT) {
+  return pair_smem(kT, kAcPairD, kAcPairFields, kAcPairZ2Rows);
+}
+
+template <int kMode, int kT, int kMinB>
+__global__ void __launch_bounds__(kT, kMinB) k_ac_pair(AcRingArgs a) {
+  constexpr int kD = kAcPairD, NF = kAcPairFields, ROW = pair_row(kT);
+  extern __shared__ __align__(16) float smem[];
+  float *ring = smem;                               // [kD][NF][ROW]
+  float *z2 = ring + (size_t)kD * NF * ROW;         // [2][ROW]
+  unsigned long long *bars = (unsigned long long *)(z2 + kAcPairZ2Rows * ROW);
+  int *s_tr = (int *)(bars + 8);                    // receiver staging [16]
+  const int sl = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[sl]);
+  const int zs = blockIdx.x * a.tz;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  if (__syncthreads_or(t == 0 && pair_err_raised(a.err))) return;  // whole CTA
+  const int ld = d.ld, nop = d.nop, pml = d.pml;
+  const long long fbase = d.slot * sl;
+  const int z0 = zs - 8 + 2 * t;
+  const int pi = t + 2;  // float2 index of the own pair in a ring row
+  const bool c1 = z0 >= zs - 4 && z0 < zs + a.tz + 4;
+  const bool c2 = z0 >= zs && z0 < zs + a.tz && z0 < d.nzp;
+  const bool u0 = z0 >= nop && z0 < d.nzp - nop, u1 = z0 + 1 >= nop && z0 + 1 < d.nzp - nop;
+  const bool zi0 = z0 >= pml && z0 < d.nzp - pml, zi1 = z0 + 1 >= pml && z0 + 1 < d.nzp - pml;
+  const ShotDev sh = a.shots[sl];
+  const float sval = kMode == 0 ? a.wavelet[a.it] : 0.f;
+  const int se = sh.isz - z0;  // source column relative to the pair (0 / 1: owned here)
+  const bool src_near = kMode == 0 && se >= -4 && se <= 5;
+  const bool rec_col = kMode == 1 && a.rec_vz && (sh.igz - z0 == 0 || sh.igz - z0 == 1);
+  const int rec_e = sh.igz - z0;
+  const int *rmap = a.rmap + (long long)sl * d.nxp_max;
+  const float cx = d.dt / d.dx, cz = d.dt / d.dz;
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
+  const bool born_out = kMode == 0 && a.e_out != nullptr;
+
+  const int lane = t & 31;
+  RingField fd{nullptr, 0, 0, d.nxp};
+  {
+    const float *src[NF] = {a.s, kMode == 1 ? a.e_in : nullptr, a.s, kMode == 1 ? a.e_in : nullptr,
+                            a.vx, a.vz, a.b, a.s, a.lam, born_out ? a.m : nullptr};
+    const int lag[NF] = {0, 0, 4, 4, 4, 4, 4, 8, 8, 8};
+#pragma unroll
+    for (int f = 0; f < NF; f++)
+      if (lane == f && src[f]) {
+        fd.src = src[f] + fbase;
+        fd.lag = lag[f];
+      }
+  }
+  if (t == 0) {
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int rs0 = x0 - 8;
+  if (t < 32)
+    for (int j = 0; j < kD - 1; j++)
+      issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], rs0 + j, ld, zs, lane);
+
+  float2 w_S[8], w_vx[9], w_vz[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) w_S[i] = w_vz[i] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_vx[i] = make_float2(0.f, 0.f);
+
+  RingCursor<kD> cur;
+  int iw = 0;  // warp that issues the copies of this step
+  bool ok = true, aborted = false;
+#pragma unroll 2
+  for (int r = rs0; r < x1 + 8; r++) {
+    ok = mbar_wait(&bars[cur.slot], cur.phase);
+    const float *S = ring + (size_t)cur.slot * NF * ROW;
+    auto F2 = [&](int f) -> float2 { return reinterpret_cast<const float2 *>(S + f * ROW)[pi]; };
+    if (rec_col && r + 4 < d.nxp && r + 4 >= 0)
+      cp_async4((float *)&s_tr[(r + 4) & 15], (const float *)(rmap + r + 4));
+    if (ok) {
+      float2 nS = F2(0);
+      if (kMode == 1) {
+        const float2 e = F2(1);
+        nS.x += e.x;
+        nS.y += e.y;
+      }
+      if (kMode == 0 && r == sh.isx && (se == 0 || se == 1)) {  // FD2DGPU.cu:2039-2049
+        if (se == 0) nS.x += sval; else nS.y += sval;
+      }
+      push2(w_S, nS);
+    }
+    // ---- stage 1: velocities of row rv = r - 4 ------------------------------------------
+    const int rv = r - 4;
+    float2 vxn = make_float2(0.f, 0.f), vzn = make_float2(0.f, 0.f);
+    if (ok && c1 && r >= x0 && rv >= nop && rv < d.nxp - nop) {
+      Z10 zS = z10(reinterpret_cast<const float2 *>(S + 2 * ROW), pi);
+      if (kMode == 1) {
+        const Z10 zE = z10(reinterpret_cast<const float2 *>(S + 3 * ROW), pi);
+#pragma unroll
+        for (int k = 0; k < 10; k++) zS.v[k] += zE.v[k];
+      }
+      if (kMode == 0 && rv == sh.isx && src_near) zS.v[se + 4] += sval;  // S + source
+      const float az0 = dzp<0>(zS), az1 = dzp<1>(zS);
+      const float2 bb = F2(6), ovx = F2(4), ovz = F2(5);
+      const float ax0 = dxw_x(w_S), ax1 = dxw_y(w_S);
+      if (u0) {  // k_ac_vel: v + dir (b dt/d) D+ S, dir = +1
+        vxn.x = ovx.x + (bb.x * cx) * ax0;
+        vzn.x = ovz.x + (bb.x * cz) * az0;
+      }
+      if (u1) {
+        vxn.y = ovx.y + (bb.y * cx) * ax1;
+        vzn.y = ovz.y + (bb.y * cz) * az1;
+      }
+      if (c2 && rv >= x0 && rv < x1) {
+        const long long k = fbase + (long long)rv * ld + z0;
+        *reinterpret_cast<float2 *>(a.vx_n + k) = vxn;
+        *reinterpret_cast<float2 *>(a.vz_n + k) = vzn;
+        if (rec_col) {
+          const int tr = s_tr[rv & 15];
+          if (tr >= 0) {
+            const long long q = ((long long)sl * d.max_ntr + tr) * d.nt + a.it;
+            a.rec_vz[q] = rec_e == 0 ? vzn.x : vzn.y;
+            a.rec_vx[q] = rec_e == 0 ? vxn.x : vxn.y;
+          }
+        }
+      }
+    }
+    push2(w_vx, vxn);
+    push2(w_vz, vzn);
+    // ---- stage-2 z-tap row (vz of row r - 8), then the step's only barrier ------------------
+    float *zb = z2 + (r & 1) * ROW;
+    reinterpret_cast<float2 *>(zb)[pi] = w_vz[3];
+    if (rec_col) cp_async_commit();
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+    if ((t >> 5) == iw) {  // the step's issuing warp (round robin spreads the extra work)
+      const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
+      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps], r + kD - 1, ld, zs,
+                          lane);
+    }
+    // ---- stage 2: stress of row rs = r - 8 --------------------------------------------------
+    const int rs = r - 8;
+    if (c2 && rs >= x0 && rs < x1 && rs >= nop && rs < d.nxp - nop) {
+      const Z10 zvz = z10(reinterpret_cast<const float2 *>(zb), pi);
+      const float2 lam = F2(8), os = F2(7);
+      const float sx0 = stencil4([&](int i) { return w_vx[3 + i].x - w_vx[4 - i].x; });
+      const float sx1 = stencil4([&](int i) { return w_vx[3 + i].y - w_vx[4 - i].y; });
+      const float sz0 = dzm<0>(zvz), sz1 = dzm<1>(zvz);
+      float2 ns = os;
+      if (u0) ns.x = os.x + lam.x * (cx * sx0 + cz * sz0);  // k_ac_str, dir = +1
+      if (u1) ns.y = os.y + lam.y * (cx * sx1 + cz * sz1);
+      const long long k = fbase + (long long)rs * ld + z0;
+      *reinterpret_cast<float2 *>(a.s_n + k) = ns;
+      if (born_out && rs >= pml && rs < d.nxp - pml && (zi0 || zi1)) {
+        const float2 mm = F2(9);
+        float2 e = make_float2(0.f, 0.f);  // the band's cells stay zero (k_ac_born)
+        if (zi0) e.x = -2.0f * lam.x * mm.x * (sx0 * rdx + sz0 * rdz);
+        if (zi1) e.y = -2.0f * lam.y * mm.y * (sx1 * rdx + sz1 * rdz);
+        *reinterpret_cast<float2 *>(a.e_out + k) = e;
+      }
+    }
+    if (rec_col) cp_async_wait<7>();
+    cur.advance();
+    if (++iw == kT / 32) iw = 0;
+  }
+  pair_exit<kD>(bars, cur, aborted, ok, a.err);
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Reverse step of the acoustic L^T, pair-blocked: the counterpart of k_ac_rev_ring, with the same
+// three chained stages and the same arithmetic per cell,
+//   A. (row r-4)  y_v += residual; yx -= dt/dx Dx+(lam ys), yz -= dt/dz Dz+(lam ys);
+//   B. (row r-8)  gs = -Dx-(b dt/dx yx) - Dz-(b dt/dz yz), ys += gs, the gradient, and
+//                 s -= lam (dt/dx Dx- bvx + dt/dz Dz- bvz);
+//   C. (row r-12) v -= b dt/d D+(s + source),
+// on strips with a 12-column halo (stage A runs on the halo of B, B on the halo of C).  Ring
+// fields of step r:
+//   0 ys(r)  1 lam(r)                  x-window of w = ys lam
+//   2 ys(r-4)  3 lam(r-4)              stage-A z-taps of w (the products formed per tap)
+//   4 yx(r-4)  5 yz(r-4)  6 b(r-4)     stage-A own cells
+//   7 vx(r-4)  8 vz(r-4)               background velocities (x-window of vx; vz kept 8 rows)
+//   9 vz(r-8)                          stage-B z-taps of the background vz
+//   10 ys(r-8)  11 s(r-8)  12 lam(r-8)  13 gradient(r-8)   stage-B own cells
+//   14 b(r-12)                         stage-C own cells
+// The stage-B z-taps of b dt/dz yz and the stage-C z-taps of s + source are values the kernel
+// computed 4 row steps earlier (stages A and B); they go through two circular row buffers in
+// shared memory, written at step r and read at step r + 4, so one barrier per step suffices
+// (k_ac_rev_ring needs three).  The residual enters stage A's own cells (as in k_ac_rev_ring),
+// the source stage B's computed S values, so neither needs a z-tap correction.
+// ---------------------------------------------------------------------------------------------
+constexpr int kAcRevPairFields = 15;
+constexpr int kAcRevPairD = 3;
+constexpr int kAcRevPairZ = 8;  // rows of each z-tap buffer (written at r, read at r + 4)
+constexpr int kAcRevHalo = 12;
+__host__ __device__ constexpr size_t ac_rev_pair_smem(int kT) {
+  return pair_smem(kT, kAcRevPairD, kAcRevPairFields, 2 * kAcRevPairZ);
+}
+
+template <int kT, int kMinB>
+__global__ void __launch_bounds__(kT, kMinB) k_ac_rev_pair(AcRevArgs a) {
+  constexpr int kD = kAcRevPairD, NF = kAcRevPairFields, ROW = pair_row(kT), ZD = kAcRevPairZ;
+  extern __shared__ __align__(16) float smem[];
+  float *ring = smem;                               // [kD][NF][ROW]
+  float *zu = ring + (size_t)kD * NF * ROW;         // [ZD][ROW]  b dt/dz yz of stage A
+  float *zS = zu + (size_t)ZD * ROW;                // [ZD][ROW]  s + source of stage B
+  unsigned long long *bars = (unsigned long long *)(zS + (size_t)ZD * ROW);
+  int *s_tr = (int *)(bars + 8), *s_has = s_tr + 16;  // receiver staging [16] each
+  float *s_rz = (float *)(s_has + 16), *s_rx = s_rz + 16;
+  const int sl = blockIdx.z, t = threadIdx.x;
+  const Dims d = slot_dims(a.d, a.shots[sl]);
+  const int zs = blockIdx.x * a.tz;
+  const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
+  if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  if (__syncthreads_or(t == 0 && pair_err_raised(a.err))) return;  // whole CTA
+  const int ld = d.ld, nop = d.nop, pml = d.pml;
+  const long long fbase = d.slot * sl;
+  const long long ibase = (long long)sl * d.wnx_max * d.ild;
+  const int z0 = zs - kAcRevHalo + 2 * t;
+  const int pi = t + 2;  // float2 index of the own pair in a ring row
+  const bool cA = z0 >= zs - 8 && z0 < zs + a.tz + 8;
+  const bool cB = z0 >= zs - 4 && z0 < zs + a.tz + 4;
+  const bool cC = z0 >= zs && z0 < zs + a.tz && z0 < d.nzp;
+  const bool u0 = z0 >= nop && z0 < d.nzp - nop, u1 = z0 + 1 >= nop && z0 + 1 < d.nzp - nop;
+  const bool i0 = z0 >= pml && z0 < d.nzp - pml, i1 = z0 + 1 >= pml && z0 + 1 < d.nzp - pml;
+  const ShotDev sh = a.shots[sl];
+  const int re = sh.igz - z0, se = sh.isz - z0;
+  const bool rec_col = re == 0 || re == 1;
+  const float sval = a.wavelet[a.it];
+  const float *res_z = a.res_vz + (long long)sl * d.max_ntr * d.nt + a.it;
+  const float *res_x = a.res_vx + (long long)sl * d.max_ntr * d.nt + a.it;
+  const int *rmap = a.rmap + (long long)sl * d.nxp_max;
+  const float cx = d.dt / d.dx, cz = d.dt / d.dz;
+  const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
+
+  const int lane = t & 31;
+  RingField fd{nullptr, 0, 0, d.nxp};
+  {
+    const float *src[NF] = {a.ys, a.lam, a.ys, a.lam, a.yx, a.yz, a.b, a.vx,
+                            a.vz, a.vz,  a.ys, a.s,   a.lam, a.grad, a.b};
+    const int lag[NF] = {0, 0, 4, 4, 4, 4, 4, 4, 4, 8, 8, 8, 8, 8, 12};
+#pragma unroll
+    for (int f = 0; f < NF; f++)
+      if (lane == f) {
+        // gradient rows: grid row x is image row x - pml of the slot's plane
+        fd.src = f == 13 ? src[f] + ibase - (long long)pml * ld : src[f] + fbase;
+        fd.lag = lag[f];
+        fd.lo = f == 13 ? pml : 0;
+        fd.hi = f == 13 ? d.nxp - pml : d.nxp;
+      }
+  }
+  const int r_first = x0 - 10, r_last = x1 + 12;
+  if (t == 0) {
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    mbar_fence_init();
+  }
+  if (rec_col) {  // stage-A rows r_first-4 ..: residuals of the first 8 rows and trace indexes
+                  // of the 8 after them (direct; the march fetches the rest ahead)
+    const int a0 = r_first - 4;
+    for (int q = a0; q < a0 + 8; q++) {
+      const int tr = (q >= 0 && q < d.nxp) ? rmap[q] : -1;
+      s_has[q & 15] = tr >= 0;
+      if (tr >= 0) {
+        s_rz[q & 15] = res_z[(long long)tr * d.nt];
+        s_rx[q & 15] = res_x[(long long)tr * d.nt];
+      }
+    }
+    for (int q = a0 + 8; q < a0 + 16; q++) s_tr[q & 15] = (q >= 0 && q < d.nxp) ? rmap[q] : -1;
+  }
+  __syncthreads();
+  if (t < 32)
+    for (int j = 0; j < kD - 1; j++)
+      issue_slot_warp<kT, kAcRevHalo>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], r_first + j,
+                                      ld, zs, lane);
+
+  const float2 zero2 = make_float2(0.f, 0.f);
+  float2 w_w[8], w_ux[9], w_bvx[9], w_bvz[9], w_S[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) w_w[i] = w_S[i] = zero2;
+#pragma unroll
+  for (int i = 0; i < 9; i++) w_ux[i] = w_bvx[i] = w_bvz[i] = zero2;
+
+  RingCursor<kD> cur;
+  int iw = 0;  // warp that issues the copies of this step
+  bool ok = true, aborted = false;
+  for (int r = r_first; r < r_last; r++) {
+    ok = mbar_wait(&bars[cur.slot], cur.phase);
+    const float *S = ring + (size_t)cur.slot * NF * ROW;
+    auto F2 = [&](int f) -> float2 { return reinterpret_cast<const float2 *>(S + f * ROW)[pi]; };
+    const int rA = r - 4, rB = r - 8, rC = r - 12;
+    if (rec_col) {  // residual of stage-A row rA + 8, trace index of rA + 16 (landed in time)
+      const int q8 = rA + 8, q16 = rA + 16;
+      const int tr8 = s_tr[q8 & 15];
+      s_has[q8 & 15] = tr8 >= 0;
+      if (tr8 >= 0) {
+        cp_async4(&s_rz[q8 & 15], res_z + (long long)tr8 * d.nt);
+        cp_async4(&s_rx[q8 & 15], res_x + (long long)tr8 * d.nt);
+      }
+      if (q16 >= 0 && q16 < d.nxp)
+        cp_async4((float *)&s_tr[q16 & 15], (const float *)(rmap + q16));
+      else
+        s_tr[q16 & 15] = -1;
+      cp_async_commit();
+    }
+    if (ok) {
+      const float2 ys = F2(0), lam = F2(1);
+      push2(w_w, make_float2(ys.x * lam.x, ys.y * lam.y));  // k_ac_adj_v: lam[q] * ys[q]
+      push2(w_bvx, F2(7));
+      push2(w_bvz, F2(8));
+    }
+    // ---- A: adjoint velocities of row rA -------------------------------------------------------
+    float2 uxn = zero2, uzn = zero2;
+    if (ok && cA && rA >= 0 && rA < d.nxp) {
+      float2 yx = F2(4), yz = F2(5);
+      if (rA >= nop && rA < d.nxp - nop) {
+        const Z10 zy = z10(reinterpret_cast<const float2 *>(S + 2 * ROW), pi);
+        const Z10 zl = z10(reinterpret_cast<const float2 *>(S + 3 * ROW), pi);
+        Z10 zw;
+#pragma unroll
+        for (int k = 0; k < 10; k++) zw.v[k] = zy.v[k] * zl.v[k];
+        if (rec_col && s_has[rA & 15]) {
+          if (re == 0) {
+            yz.x += s_rz[rA & 15];
+            yx.x += s_rx[rA & 15];
+          } else {
+            yz.y += s_rz[rA & 15];
+            yx.y += s_rx[rA & 15];
+          }
+        }
+        if (u0) {
+          yx.x = yx.x - cx * dxw_x(w_w);
+          yz.x = yz.x - cz * dzp<0>(zw);
+        }
+        if (u1) {
+          yx.y = yx.y - cx * dxw_y(w_w);
+          yz.y = yz.y - cz * dzp<1>(zw);
+        }
+        if (cC && rA >= x0 && rA < x1) {
+          const long long k = fbase + (long long)rA * ld + z0;
+          *reinterpret_cast<float2 *>(a.yx_n + k) = yx;
+          *reinterpret_cast<float2 *>(a.yz_n + k) = yz;
+        }
+      }
+      const float2 bb = F2(6);
+      uxn = make_float2(bb.x * cx * yx.x, bb.y * cx * yx.y);  // k_ac_adj_s: b[q] * cx * yx[q]
+      uzn = make_float2(bb.x * cz * yz.x, bb.y * cz * yz.y);
+    }
+    push2(w_ux, uxn);
+    reinterpret_cast<float2 *>(zu + ((r + 16) & (ZD - 1)) * ROW)[pi] = uzn;
+    // ---- B: ys, gradient and the background stress of row rB ---------------------------------
+    float2 Sn = zero2;
+    if (ok && cB && rB >= 0 && rB < d.nxp) {
+      float2 bs = F2(11);
+      if (rB >= nop && rB < d.nxp - nop) {
+        const Z10 zuz = z10(reinterpret_cast<const float2 *>(zu + ((r + 12) & (ZD - 1)) * ROW), pi);
+        const Z10 zbv = z10(reinterpret_cast<const float2 *>(S + 9 * ROW), pi);
+        const float2 lam = F2(12), ys_o = F2(10);
+        float2 ys_n = ys_o, gr = zero2;
+        const bool own = cC && rB >= x0 && rB < x1;
+        if (own && rB >= pml && rB < d.nxp - pml) gr = F2(13);
+        const float2 g_o = gr;
+        {
+          const float gx = stencil4([&](int i) { return w_ux[3 + i].x - w_ux[4 - i].x; });
+          const float gs = -gx - dzm<0>(zuz);
+          const float sx = stencil4([&](int i) { return w_bvx[3 + i].x - w_bvx[4 - i].x; });
+          const float sz = dzm<0>(zbv);
+          if (u0) {
+            ys_n.x = ys_o.x + gs;
+            if (i0) gr.x = g_o.x + -2.0f * lam.x * (sx * rdx + sz * rdz) * gs;
+            bs.x = bs.x + -1.0f * lam.x * (cx * sx + cz * sz);  // k_ac_str, dir = -1
+          }
+        }
+        {
+          const float gx = stencil4([&](int i) { return w_ux[3 + i].y - w_ux[4 - i].y; });
+          const float gs = -gx - dzm<1>(zuz);
+          const float sx = stencil4([&](int i) { return w_bvx[3 + i].y - w_bvx[4 - i].y; });
+          const float sz = dzm<1>(zbv);
+          if (u1) {
+            ys_n.y = ys_o.y + gs;
+            if (i1) gr.y = g_o.y + -2.0f * lam.y * (sx * rdx + sz * rdz) * gs;
+            bs.y = bs.y + -1.0f * lam.y * (cx * sx + cz * sz);
+          }
+        }
+        if (own) {
+          const long long k = fbase + (long long)rB * ld + z0;
+          *reinterpret_cast<float2 *>(a.ys_n + k) = ys_n;
+          *reinterpret_cast<float2 *>(a.s_n + k) = bs;
+          if (rB >= pml && rB < d.nxp - pml && (i0 || i1))
+            *reinterpret_cast<float2 *>(a.grad + ibase + (long long)(rB - pml) * d.ild + z0) = gr;
+        }
+      }
+      Sn = bs;
+      if (rB == sh.isx) {  // the source overlay of k_ac_vel (transient)
+        if (se == 0) Sn.x += sval;
+        if (se == 1) Sn.y += sval;
+      }
+    }
+    push2(w_S, Sn);
+    reinterpret_cast<float2 *>(zS + ((r + 16) & (ZD - 1)) * ROW)[pi] = Sn;
+    // ---- C: background velocities of row rC ----------------------------------------------------
+    if (ok && cC && rC >= x0 && rC < x1 && rC >= nop && rC < d.nxp - nop) {
+      const Z10 zsn = z10(reinterpret_cast<const float2 *>(zS + ((r + 12) & (ZD - 1)) * ROW), pi);
+      const float2 bb = F2(14), ovx = w_bvx[0], ovz = w_bvz[0];
+      float2 vx = ovx, vz = ovz;
+      if (u0) {
+        vx.x = ovx.x + -1.0f * (bb.x * cx) * dxw_x(w_S);  // k_ac_vel, dir = -1
+        vz.x = ovz.x + -1.0f * (bb.x * cz) * dzp<0>(zsn);
+      }
+      if (u1) {
+        vx.y = ovx.y + -1.0f * (bb.y * cx) * dxw_y(w_S);
+        vz.y = ovz.y + -1.0f * (bb.y * cz) * dzp<1>(zsn);
+      }
+      const long long k = fbase + (long long)rC * ld + z0;
+      *reinterpret_cast<float2 *>(a.vx_n + k) = vx;
+      *reinterpret_cast<float2 *>(a.vz_n + k) = vz;
+    }
+    // one barrier per step: the z-tap rows written above are read 4 steps on; the ring slot of
+    // the previous step is free once every thread has passed it
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+    if ((t >> 5) == iw) {  // the step's issuing warp (round robin spreads the extra work)
+      const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
+      issue_slot_warp<kT, kAcRevHalo>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps],
+                                      r + kD - 1, ld, zs, lane);
+    }
+    if (rec_col) cp_async_wait<7>();
+    cur.advance();
+    if (++iw == kT / 32) iw = 0;
   }
   pair_exit<kD>(bars, cur, aborted, ok, a.err);
   cp_async_wait<0>();
@@ -466,6 +923,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   const int zs = blockIdx.x * a.tz;
   const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
   if (x0 >= d.nxp) return;
+  if (__syncthreads_or(t == 0 && pair_err_raised(a.err))) return;  // whole CTA
   const int ld = d.ld, nop = d.nop, pml = d.pml;
   const long long fbase = d.slot * s;
   const long long ibase = (long long)s * d.wnx_max * d.ild;
@@ -564,6 +1022,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   int zw = ((rs0 - 4) % kBwdPairZDepth + kBwdPairZDepth) % kBwdPairZDepth;
 
   RingCursor<kD> cur;
+  int iw = 0;  // warp that issues the copies of this step
   bool ok = true, aborted = false;
   // Two row steps per loop iteration let the compiler rename half of the window shifts away
   // where the registers allow it (the split parts); the fused pass is at its register limit.
@@ -748,7 +1207,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
       aborted = true;
       break;
     }
-    if (t < 32) {
+    if ((t >> 5) == iw) {  // the step's issuing warp (round robin spreads the extra work)
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
       issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps], r + kD - 1, ld, zs,
                           lane);
@@ -812,6 +1271,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
     }
     if (rec_col) cp_async_wait<6>();
     cur.advance();
+    if (++iw == kT / 32) iw = 0;
   }
   pair_exit<kD>(bars, cur, aborted, ok, a.err);
   cp_async_wait<0>();

@@ -213,7 +213,14 @@ int ds2d_bandpass_filter_device(int nx, int nz, int x1, int x2, int z1, int z2, 
  * forward and 3 / 4 backward CTAs per SM), "cta" (threads per CTA of the ring kernels: 128,
  * 192, or 0 = the one whose z-strips leave fewer threads idle for this grid; 192 needs ring 4 and
  * occ 0), "graph" (0 / 1: capture batches in CUDA graphs),
- * "adjoint_born" (see ds2d_elsrtm), "pcg_switch" and "pcg_m" (1..15, see ds2d_lsrtm_pcg). */
+ * "adjoint_born" (see ds2d_elsrtm), "pcg_switch" and "pcg_m" (1..15, see ds2d_lsrtm_pcg).
+ * Pair-blocked bulk-copy kernels (random boundary; two z-columns per thread, rows fed by
+ * cp.async.bulk into an mbarrier ring): "pair" (0 off, 1 forward and backward RTM steps, 2 the
+ * forward step only), "pair_fcta" (forward CTA width 64 / 256, 0 = 256), "pair_cta" (backward
+ * 64 / 160 / 256, 0 = 64), "pair_split" (0 / 1: backward in one or two launches), "pair_xr" (rows
+ * per CTA, 0 = the count that fills the SMs' waves best), "ac_pair" (0 / 1: acoustic forward
+ * steps of the Born pair on k_ac_pair) and "ac_pair_cta" (128 / 192 / 256, 0 = the width with the
+ * fewest threads per grid row). */
 int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
 
 /* Profiling (no counterpart in the reference, which has only a commented-out host timer,

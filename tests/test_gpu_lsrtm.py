@@ -4,7 +4,7 @@ import pytest
 
 from ds2d_b200 import Elastic2D, synth
 from oracle import pyoracle as po
-from tests.helpers import rel
+from tests.helpers import gate, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -81,10 +81,62 @@ def test_ac_born_and_adjoint_vs_oracle(cuda_device):
     assert rel(g, gref) < BORN_GATE, rel(g, gref)
 
 
-def test_ac_dot_product_fp32(cuda_device):
-    """<L m, d> = <m, L^T d> for the sm_100a pair (FP32 arithmetic, FP64 sums)."""
+@pytest.mark.parametrize("cta,xr", [(0, 0), (128, 24), (192, 0), (256, 40)])
+def test_ac_pair_kernels_match_ring_and_oracle(cuda_device, cta, xr):
+    """Pair-blocked acoustic forward steps (k_ac_pair: background with the Born source written,
+    scattered set with records, and the background replay of L^T) against the one-column ring
+    kernels and the FP64 oracle.  The 300-deep grid gives the 128-thread CTAs two z-strips; xr
+    24 / 40 gives every shot several row blocks (x-halos between CTAs)."""
+    c, vp, vs, w, shots, m = acoustic_case(nt=300)
+    c["allnz"] = 300
+    vp = np.broadcast_to(np.linspace(1800, 4500, c["allnz"], dtype=np.float32),
+                         (c["allnx"], c["allnz"])).copy()
+    vs = np.zeros_like(vp)
+    m = synth.reflectivity(c["allnx"], c["allnz"], seed=4, density=0.05, std=0.05)
+    m[:, :3] = 0
+    rng = np.random.default_rng(3)
+    out = {}
+    for pair in (0, 1):
+        with ctx(c, shots) as e:
+            e.set_option("ac_pair", pair)
+            e.set_option("ac_pair_cta", cta)
+            e.set_option("pair_xr", xr)
+            e.set_models(vp, vs)
+            e.set_wavelet(w)
+            dz, dx = e.ac_born(shots, m)
+            if pair == 0:
+                rz = rng.normal(size=dz.shape).astype(np.float32)
+                rx = rng.normal(size=dx.shape).astype(np.float32)
+            g = e.ac_born_adj(shots, rz, rx)
+            out[pair] = (dz, dx, g)
+    assert np.abs(out[1][0]).max() > 0
+    # FP32 floor of the Born records: the oracle's elastic Born step at vs = 0 (the same operator)
+    # in FP32 against FP64
+    st, models = oracle_models(c, vp, vs, shots)
+    ntr = shots[0].ntr
+    floor = 0.0
+    for i, s in enumerate(shots[:2]):
+        dmp = po.window_image(st, m, s.win_left)
+        dms = po.window_image(st, np.zeros_like(m), s.win_left)
+        b64 = po.born(st, models[i], dmp, dms, w, s, "f64")
+        b32 = po.born(st, models[i], dmp, dms, w, s, "f32")
+        fl = max(rel(b32[0], b64[0]), rel(b32[1], b64[1]))
+        floor = max(floor, fl)
+        for j in range(2):
+            err = rel(out[1][j][i * ntr:(i + 1) * ntr], b64[j])
+            assert err < gate(fl), (i, j, err, f"FP32 floor {fl:.3e}")
+    for k in range(3):
+        err = rel(out[1][k], out[0][k])
+        assert err < gate(floor), (k, err, f"FP32 floor {floor:.3e}")
+
+
+@pytest.mark.parametrize("ac_pair", [0, 1])
+def test_ac_dot_product_fp32(cuda_device, ac_pair):
+    """<L m, d> = <m, L^T d> for the sm_100a pair (FP32 arithmetic, FP64 sums), on the
+    one-column ring kernels and on the pair-blocked ones."""
     c, vp, vs, w, shots, m = acoustic_case(nt=400)
     with ctx(c, shots) as e:
+        e.set_option("ac_pair", ac_pair)
         e.set_models(vp, vs)
         e.set_wavelet(w)
         dz, dx = e.ac_born(shots, m)
