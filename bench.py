@@ -760,6 +760,9 @@ def run_lsrtm(args):
     bkw = dict(boundary=args.lsrtm_boundary, strips=args.lsrtm_strips)
     et = Elastic2D(tnx, tnz, tnx, band, tnt, dx, dx, dt, max_shots=tshots, max_ntr=tnx, seed=7,
                    device=dev, **bkw)
+    opts = parse_set(args.set)  # library options of both contexts (e.g. ac_ckpt=500)
+    for k, v in opts.items():
+        et.set_option(k, v)
     vpt = precond.background(tnx, tnz, seed=1)
     et.set_models(vpt, np.zeros_like(vpt))
     et.set_wavelet(synth.ricker(tnt, f0, dt))
@@ -789,6 +792,8 @@ def run_lsrtm(args):
     shots = synth.surface_shots(anx, anx, band, ashots)
     ea = Elastic2D(anx, anz, anx, band, ant, dx, dx, dt, max_shots=ashots, max_ntr=anx, seed=9,
                    device=dev, **bkw)
+    for k, v in opts.items():
+        ea.set_option(k, v)
     vpa = precond.background(anx, anz, seed=2)
     ea.set_models(vpa, np.zeros_like(vpa))
     ea.set_wavelet(synth.ricker(ant, f0, dt))
@@ -838,7 +843,7 @@ def run_lsrtm(args):
                        + ("random band)" if args.lsrtm_boundary == "random" else
                           f"PML, {args.lsrtm_strips} boundary strips with FP32 scales)"),
                        "shots": ashots, "nt": ant, "cg_iterations": args.cg_iters,
-                       "target": args.target},
+                       "target": args.target, "options": opts},
             "plain": res["plain"], "learned": res["learned"],
             "training": {"pairs": args.pairs, "grid": f"{tnx}x{tnz}", "shots": tshots, "nt": tnt,
                          "pair_generation_s": round(t_pairs, 1),

@@ -140,6 +140,70 @@ __global__ void __launch_bounds__(256) k_ac_strip_load(AcStripArgs a) {
   (comp ? a.vz : a.vx)[d.slot * s + (long long)ix * d.ld + iz] = strip_get(a.st, d, s, a.it, comp, bo);
 }
 
+// ---- background checkpoints of the PML L^T --------------------------------------------------
+// With option "ac_ckpt" = K the forward replay of L^T keeps, instead of every step's boundary
+// strips, a snapshot of the whole background state (vx, vz, s and the PML split stress sx, sz)
+// every K steps, stored in the context's strip precision with one FP32 scale per field, shot and
+// snapshot (scale = max|f| / 2^15 as for the strips, so FP16 stays in range; BF16 takes the same
+// scale).  The reverse pass then works segment by segment from the last: decode the segment's
+// snapshot, replay its steps saving their strips (a K-step strip buffer), reverse through them.
+constexpr int kCkptFields = 5;
+struct CkptArgs {
+  long long slot;          // floats per shot slot
+  const float *f[kCkptFields];
+  float *fw[kCkptFields];  // the same arrays, written by the decode
+  void *data;              // this snapshot: [kCkptFields][B][slot] elements
+  float *scale;            // this snapshot: [kCkptFields][B]
+  unsigned *amax;          // scratch [kCkptFields][B]: max |f| as float bits (non-negative)
+  int prec, B;
+};
+
+__global__ void __launch_bounds__(256) k_ckpt_absmax(CkptArgs a) {
+  const int s = blockIdx.z, f = blockIdx.y;
+  const float *src = a.f[f] + a.slot * s;
+  float m = 0.f;
+  for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < a.slot;
+       i += (long long)gridDim.x * 256)
+    m = fmaxf(m, fabsf(src[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  // non-negative floats order like their bit patterns
+  if ((threadIdx.x & 31) == 0) atomicMax(&a.amax[f * a.B + s], __float_as_uint(m));
+}
+
+__device__ __forceinline__ float ckpt_scale(unsigned bits) {
+  const float m = __uint_as_float(bits);
+  return m > 0.f ? fmaxf(m * (1.0f / 32768.0f), 1.17549435e-38f) : 1.0f;
+}
+
+__global__ void __launch_bounds__(256) k_ckpt_encode(CkptArgs a) {
+  const int s = blockIdx.z, f = blockIdx.y;
+  const float *src = a.f[f] + a.slot * s;
+  const long long base = ((long long)f * a.B + s) * a.slot;
+  const float sc = a.prec == 0 ? 1.0f : ckpt_scale(a.amax[f * a.B + s]);
+  if (a.prec != 0 && blockIdx.x == 0 && threadIdx.x == 0) a.scale[f * a.B + s] = sc;
+  for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < a.slot;
+       i += (long long)gridDim.x * 256) {
+    const float v = src[i];
+    if (a.prec == 0) ((float *)a.data)[base + i] = v;
+    else if (a.prec == 1) ((__half *)a.data)[base + i] = __float2half_rn(v / sc);
+    else ((__nv_bfloat16 *)a.data)[base + i] = __float2bfloat16_rn(v / sc);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_ckpt_decode(CkptArgs a) {
+  const int s = blockIdx.z, f = blockIdx.y;
+  float *dst = a.fw[f] + a.slot * s;
+  const long long base = ((long long)f * a.B + s) * a.slot;
+  const float sc = a.prec == 0 ? 1.0f : a.scale[f * a.B + s];
+  for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < a.slot;
+       i += (long long)gridDim.x * 256) {
+    if (a.prec == 0) dst[i] = ((const float *)a.data)[base + i];
+    else if (a.prec == 1) dst[i] = __half2float(((const __half *)a.data)[base + i]) * sc;
+    else dst[i] = __bfloat162float(((const __nv_bfloat16 *)a.data)[base + i]) * sc;
+  }
+}
+
 // e = -2 lam m (Dx- vx / dx + Dz- vz / dz) on the interior (m = the windowed model in p.dmp).
 __global__ void __launch_bounds__(256) k_ac_born(Dims d0, const ShotDev *shots, Par p,
                                                  const float *vx, const float *vz, float *e) {

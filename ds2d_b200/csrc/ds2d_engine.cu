@@ -242,6 +242,13 @@ struct ds2d_ctx {
   Strain e{}, be{};
   float *ov_s[3] = {nullptr, nullptr, nullptr}, *ov_v[2] = {nullptr, nullptr};
   Strips st_a{}, st_b{};
+  int st_a_steps = 0, st_b_steps = 0;  // time steps the strip buffers hold
+  // background checkpoints of the PML L^T (option "ac_ckpt")
+  int opt_ac_ckpt = 0;
+  void *ckpt = nullptr;
+  float *ckpt_scale = nullptr;
+  unsigned *ckpt_amax = nullptr;
+  size_t ckpt_bytes = 0;
   ShotDev *d_shots = nullptr;
   int *d_rmap = nullptr;
   float *rec[8] = {};          // obs/adj z,x | scattered z,x | scattered2 z,x | residual z,x
@@ -370,16 +377,39 @@ int zero_wave(ds2d_ctx *c, const Wave &w, int nslots) {
   return DS2D_OK;
 }
 
-int alloc_strips(ds2d_ctx *c, Strips &st) {
+int alloc_strips(ds2d_ctx *c, Strips &st, int steps) {
   int rc;
   st.prec = c->o.strip_precision;
-  size_t elems = (size_t)c->B * c->d.nt * 2 * c->d.lb;
+  size_t elems = (size_t)c->B * steps * 2 * c->d.lb;
   size_t esz = st.prec == DS2D_STRIPS_F32 ? 4 : 2;
   if ((rc = alloc(c, &st.data, elems * esz))) return rc;
   if (st.prec != DS2D_STRIPS_F32) {
-    size_t ns = (size_t)c->B * c->d.nt * 2 * c->d.nseg;
+    size_t ns = (size_t)c->B * steps * 2 * c->d.nseg;
     if ((rc = alloc(c, (void **)&st.scale, ns * sizeof(float)))) return rc;
   }
+  return DS2D_OK;
+}
+
+// Frees one arena allocation before the context's end (buffers whose size follows an option).
+void release(ds2d_ctx *c, void *p) {
+  if (!p) return;
+  cudaFree(p);
+  auto &v = c->arena.ptrs;
+  v.erase(std::remove(v.begin(), v.end(), p), v.end());
+}
+
+// A strip buffer holding at least `steps` time steps (strips are indexed by the step within the
+// buffer, so a larger one serves a shorter use).
+int ensure_strips(ds2d_ctx *c, Strips &st, int &have, int steps) {
+  if (st.data && have >= steps) return DS2D_OK;
+  release(c, st.data);
+  release(c, st.scale);
+  st.data = nullptr;
+  st.scale = nullptr;
+  have = 0;
+  int rc;
+  if ((rc = alloc_strips(c, st, steps))) return rc;
+  have = steps;
   return DS2D_OK;
 }
 
@@ -413,7 +443,7 @@ int ensure_rtm(ds2d_ctx *c) {
   float **es[4] = {&c->e.gx_vx, &c->e.gz_vz, &c->e.gz_vx, &c->e.gx_vz};
   for (float **p : es)
     if ((rc = alloc_slots(c, p))) return rc;
-  if (!c->d.rbc && (rc = alloc_strips(c, c->st_a))) return rc;
+  if (!c->d.rbc && (rc = ensure_strips(c, c->st_a, c->st_a_steps, c->d.nt))) return rc;
   if (!c->img_slot) {
     size_t n = (size_t)7 * c->B * c->d.wnx * c->d.ild;
     if ((rc = alloc(c, (void **)&c->img_slot, n * sizeof(float)))) return rc;
@@ -440,7 +470,7 @@ int ensure_elsrtm(ds2d_ctx *c) {
     if ((rc = alloc_slots(c, &c->ov_s[i]))) return rc;
   for (int i = 0; i < 2; i++)
     if ((rc = alloc_slots(c, &c->ov_v[i]))) return rc;
-  if (!c->d.rbc && (rc = alloc_strips(c, c->st_b))) return rc;
+  if (!c->d.rbc && (rc = ensure_strips(c, c->st_b, c->st_b_steps, c->d.nt))) return rc;
   size_t nrec = (size_t)c->B * c->d.max_ntr * c->d.nt;
   for (int i = 2; i < 8; i++)
     if ((rc = alloc(c, (void **)&c->rec[i], nrec * sizeof(float)))) return rc;
@@ -1262,7 +1292,10 @@ int ensure_acoustic(ds2d_ctx *c) {
   if (!c->d.rbc) {  // PML: split stress in the damped cells, background strips for L^T
     for (float *&p : c->ac_split)
       if (!p && (rc = alloc_slots(c, &p))) return rc;
-    if (!c->st_a.data && (rc = alloc_strips(c, c->st_a))) return rc;
+    // the L^T replay saves the strips of every step, or with checkpoints of one segment
+    const int k = c->opt_ac_ckpt;
+    const int steps = k > 0 && k < c->d.nt ? k : c->d.nt;
+    if ((rc = ensure_strips(c, c->st_a, c->st_a_steps, steps))) return rc;
   }
   if (!c->p_dmp) {
     if ((rc = alloc_slots(c, &c->p_dmp))) return rc;
@@ -1385,10 +1418,119 @@ int ac_L_batch(ds2d_ctx *c, int n) {
 // vx, vz each step, then per step in reverse: the step's strips restored into the band, the
 // transpose of the damped scattered step (records injected, gradient with the background
 // velocities after the step), and the interior reconstruction of the background one step back.
+// Saves (save) or restores background snapshot `snap` of the PML L^T: vx, vz, s and the split
+// stress sx, sz of every slot, in the strip precision with per-field, per-shot FP32 scales.
+int ac_ckpt_io(ds2d_ctx *c, int n, int snap, bool save) {
+  const Dims &d = c->d;
+  CkptArgs a{};
+  a.slot = (long long)d.slot;
+  a.prec = c->o.strip_precision;
+  a.B = c->B;
+  float *f[kCkptFields] = {c->ac[0], c->ac[1], c->ac[2], c->ac_split[0], c->ac_split[1]};
+  for (int i = 0; i < kCkptFields; i++) {
+    a.f[i] = f[i];
+    a.fw[i] = f[i];
+  }
+  const size_t esz = a.prec == DS2D_STRIPS_F32 ? 4 : 2;
+  const size_t per = (size_t)kCkptFields * c->B * d.slot;
+  a.data = (char *)c->ckpt + (size_t)snap * per * esz;
+  a.scale = c->ckpt_scale + (size_t)snap * kCkptFields * c->B;
+  a.amax = c->ckpt_amax;
+  dim3 grid((unsigned)std::min<long long>(((long long)d.slot + 255) / 256, 64), kCkptFields, n);
+  if (save) {
+    if (a.prec != DS2D_STRIPS_F32) {
+      CK(cudaMemsetAsync(c->ckpt_amax, 0, sizeof(unsigned) * kCkptFields * c->B, c->stream));
+      LAUNCH(k_ckpt_absmax, grid, 256, a);
+    }
+    LAUNCH(k_ckpt_encode, grid, 256, a);
+  } else {
+    LAUNCH(k_ckpt_decode, grid, 256, a);
+  }
+  return DS2D_OK;
+}
+
+// One reverse step of the PML L^T: the band of the background from the strips (row `srow` of
+// the strip buffer described by `ds`), the adjoint step with the gradient, the interior of the
+// background one step back.
+void ac_LT_pml_reverse_step(ds2d_ctx *c, int n, const Dims &ds, int srow, int it) {
+  const Dims &d = c->d;
+  dim3 grid = cell_grid(d, n), blk(32, 8);
+  AcStripArgs ld{ds, c->d_shots, c->ac[0], c->ac[1], c->st_a, srow};
+  LAUNCH(k_ac_strip_load, dim3((d.lb + 255) / 256, 2, n), 256, ld);
+  AcAdjArgs y{};
+  y.d = d; y.shots = c->d_shots; y.p = c->par;
+  y.yx = c->ac[6]; y.yz = c->ac[7]; y.ys = c->ac[8];
+  y.ysx = c->ac_split[4]; y.ysz = c->ac_split[5];
+  y.rmap = c->d_rmap; y.res_vz = c->rec[0]; y.res_vx = c->rec[1]; y.it = it;
+  y.bvx = c->ac[0]; y.bvz = c->ac[1]; y.grad = c->img_slot;
+  LAUNCHP("ac_adj_v", 0, k_ac_adj_v, grid, blk, y);
+  LAUNCHP("ac_adj_s", 0, k_ac_adj_s, grid, blk, y);
+  AcArgs b = ac_args(c, 0, it, -1.f);  // background back to step it-1 on the interior
+  b.src_on = 1;
+  b.interior = 1;
+  b.sx = b.sz = nullptr;
+  LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+  LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
+}
+
+// PML L^T with background checkpoints every K steps (option "ac_ckpt"): a forward pass keeps
+// snapshots 0 .. nseg-2 (the state before steps 0, K, 2K, ...); then, from the last segment to the
+// first, the segment's start state (the exact state for the last, a decoded snapshot for the
+// others) is replayed over its steps saving their strips into a K-step buffer, and the segment is
+// reversed with them.  Forward work: (nseg - 1) K + nt steps instead of nt.
+int ac_LT_batch_pml_ckpt(ds2d_ctx *c, int n, int K) {
+  const Dims &d = c->d;
+  const int nseg = (d.nt + K - 1) / K;
+  const size_t esz = c->o.strip_precision == DS2D_STRIPS_F32 ? 4 : 2;
+  const int nsnap = std::max(1, nseg - 1);
+  const size_t need = (size_t)nsnap * kCkptFields * c->B * d.slot * esz;
+  int rc;
+  if (c->ckpt_bytes < need) {
+    release(c, c->ckpt);
+    release(c, c->ckpt_scale);
+    c->ckpt = nullptr;
+    c->ckpt_scale = nullptr;
+    c->ckpt_bytes = 0;
+    if ((rc = alloc(c, &c->ckpt, need))) return rc;
+    if ((rc = alloc(c, (void **)&c->ckpt_scale, sizeof(float) * nsnap * kCkptFields * c->B)))
+      return rc;
+    c->ckpt_bytes = need;
+  }
+  if (!c->ckpt_amax &&
+      (rc = alloc(c, (void **)&c->ckpt_amax, sizeof(unsigned) * kCkptFields * c->B)))
+    return rc;
+  dim3 grid = cell_grid(d, n), blk(32, 8);
+  auto fwd_step = [&](int it) {
+    AcArgs b = ac_args(c, 0, it, 1.f);
+    b.src_on = 1;
+    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
+    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
+  };
+  for (int it = 0; it < (nseg - 1) * K; it++) {
+    if (it % K == 0 && (rc = ac_ckpt_io(c, n, it / K, true))) return rc;
+    fwd_step(it);
+  }
+  Dims dk = d;
+  dk.nt = K;  // strip rows of one segment
+  for (int j = nseg - 1; j >= 0; --j) {
+    const int t0 = j * K, t1 = std::min(d.nt, t0 + K);
+    if (j < nseg - 1 && (rc = ac_ckpt_io(c, n, j, false))) return rc;
+    for (int it = t0; it < t1; it++) {
+      fwd_step(it);
+      StripSaveArgs sv{dk, c->d_shots, c->ac[0], c->ac[1], c->st_a, it - t0};
+      LAUNCH(k_strip_save, dim3((d.lb + 255) / 256, 2, n), 256, sv);
+    }
+    for (int it = t1 - 1; it >= t0; --it) ac_LT_pml_reverse_step(c, n, dk, it - t0, it);
+  }
+  CK(cudaGetLastError());
+  return reduce_images(c, n, 1);
+}
+
 int ac_LT_batch_pml(ds2d_ctx *c, int n) {
   const Dims &d = c->d;
   size_t bytes = sizeof(float) * (size_t)d.slot * n;
   for (float *p : c->ac_split) CK(cudaMemsetAsync(p, 0, bytes, c->stream));
+  if (c->opt_ac_ckpt > 0 && c->opt_ac_ckpt < d.nt) return ac_LT_batch_pml_ckpt(c, n, c->opt_ac_ckpt);
   dim3 grid = cell_grid(d, n), blk(32, 8);
   for (int it = 0; it < d.nt; it++) {
     AcArgs b = ac_args(c, 0, it, 1.f);
@@ -1398,24 +1540,7 @@ int ac_LT_batch_pml(ds2d_ctx *c, int n) {
     StripSaveArgs sv{d, c->d_shots, c->ac[0], c->ac[1], c->st_a, it};
     LAUNCH(k_strip_save, dim3((d.lb + 255) / 256, 2, n), 256, sv);
   }
-  for (int it = d.nt - 1; it >= 0; --it) {
-    AcStripArgs ld{d, c->d_shots, c->ac[0], c->ac[1], c->st_a, it};
-    LAUNCH(k_ac_strip_load, dim3((d.lb + 255) / 256, 2, n), 256, ld);
-    AcAdjArgs y{};
-    y.d = d; y.shots = c->d_shots; y.p = c->par;
-    y.yx = c->ac[6]; y.yz = c->ac[7]; y.ys = c->ac[8];
-    y.ysx = c->ac_split[4]; y.ysz = c->ac_split[5];
-    y.rmap = c->d_rmap; y.res_vz = c->rec[0]; y.res_vx = c->rec[1]; y.it = it;
-    y.bvx = c->ac[0]; y.bvz = c->ac[1]; y.grad = c->img_slot;
-    LAUNCHP("ac_adj_v", 0, k_ac_adj_v, grid, blk, y);
-    LAUNCHP("ac_adj_s", 0, k_ac_adj_s, grid, blk, y);
-    AcArgs b = ac_args(c, 0, it, -1.f);  // background back to step it-1 on the interior
-    b.src_on = 1;
-    b.interior = 1;
-    b.sx = b.sz = nullptr;
-    LAUNCHP("ac_str", 0, k_ac_str, grid, blk, b);
-    LAUNCHP("ac_vel", 0, k_ac_vel, grid, blk, b);
-  }
+  for (int it = d.nt - 1; it >= 0; --it) ac_LT_pml_reverse_step(c, n, d, it, it);
   CK(cudaGetLastError());
   return reduce_images(c, n, 1);
 }
@@ -2286,6 +2411,9 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     if (value != 0 && value != 64 && value != 160 && value != 256)
       return fail(c, DS2D_E_ARG, "pair_cta must be 0 (automatic), 64, 160 or 256");
     c->opt_pair_cta = (int)value;
+  } else if (k == "ac_ckpt") {
+    if (value < 0 || value > (1 << 30)) return fail(c, DS2D_E_ARG, "ac_ckpt must be >= 0");
+    c->opt_ac_ckpt = (int)value;
   } else if (k == "ac_pair") {
     if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "ac_pair must be 0 or 1");
     c->opt_ac_pair = (int)value;

@@ -220,7 +220,11 @@ int ds2d_bandpass_filter_device(int nx, int nz, int x1, int x2, int z1, int z2, 
  * 64 / 160 / 256, 0 = 64), "pair_split" (0 / 1: backward in one or two launches), "pair_xr" (rows
  * per CTA, 0 = the count that fills the SMs' waves best), "ac_pair" (0 / 1: acoustic forward
  * steps of the Born pair on k_ac_pair) and "ac_pair_cta" (128 / 192 / 256, 0 = the width with the
- * fewest threads per grid row). */
+ * fewest threads per grid row).  "ac_ckpt" (K, 0 = off; PML acoustic L^T): keep a snapshot of
+ * the whole background state every K steps, in the strip precision with one FP32 scale per field,
+ * shot and snapshot, and replay each K-step segment from its snapshot with strips before
+ * reversing it: snapshots plus K steps of strips instead of nt steps of strips, for one more
+ * forward propagation per L^T. */
 int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
 
 /* Profiling (no counterpart in the reference, which has only a commented-out host timer,

@@ -271,9 +271,11 @@ def _pml_case(nt=300):
     return c, vp, w, shots, m
 
 
-def _pml_run(c, vp, w, shots, m, strips, rz=None, rx=None):
+def _pml_run(c, vp, w, shots, m, strips, rz=None, rx=None, opts=None):
     with Elastic2D(c["allnx"], c["allnz"], c["nx"], c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
                    boundary="pml", strips=strips, max_shots=len(shots), max_ntr=c["nx"]) as e:
+        for k, v in (opts or {}).items():
+            e.set_option(k, v)
         e.set_models(vp, 0 * vp)
         e.set_wavelet(w)
         dz, dx = e.ac_born(shots, m)
@@ -328,6 +330,34 @@ def test_ac_born_adj_pml_half_precision_strips(cuda_device, strips, gate):
         gref[s.win_left:s.win_left + c["nx"]] += gp[c["pml"]:c["pml"] + c["nx"], c["pml"]:-c["pml"]]
     err = rel(g16, gref)
     assert err < gate, f"{strips} strips: L^T vs FP64 oracle {err:.3e}"
+
+
+@pytest.mark.parametrize("strips,gate_", [("f32", 1e-6), ("f16", 2e-3), ("bf16", 2e-2)])
+def test_ac_born_adj_pml_checkpoints(cuda_device, strips, gate_):
+    """L^T with the background checkpointed every 37 steps (option ac_ckpt: whole-state snapshots
+    in the strip precision with one FP32 scale per field, shot and snapshot; each 37-step segment
+    replayed from its snapshot with strips, then reversed; 300 steps give 8 full segments and a
+    4-step one).  FP32 snapshots replay the same states bit for bit, so the gradient equals the
+    all-strips path's; FP16 / BF16 snapshots and strips are gated against the FP64 oracle's exact
+    transpose like the strips alone."""
+    c, vp, w, shots, m = _pml_case()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    rng = np.random.default_rng(8)
+    ntr = shots[0].ntr
+    rz = rng.normal(size=(len(shots) * ntr, c["nt"])).astype(np.float32)
+    rx = rng.normal(size=rz.shape).astype(np.float32)
+    _, _, g_ck = _pml_run(c, vp, w, shots, m, strips, rz, rx, opts={"ac_ckpt": 37})
+    if strips == "f32":
+        _, _, g_all = _pml_run(c, vp, w, shots, m, strips, rz, rx)
+        assert rel(g_ck, g_all) < gate_, rel(g_ck, g_all)
+        return
+    gref = np.zeros((c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        model = po.build_model(st, vp, 0 * vp, None, s.win_left)
+        gp = po.ac_born_adj(st, model, w, s, rz[i * ntr:(i + 1) * ntr], rx[i * ntr:(i + 1) * ntr])
+        gref[s.win_left:s.win_left + c["nx"]] += gp[c["pml"]:c["pml"] + c["nx"], c["pml"]:-c["pml"]]
+    err = rel(g_ck, gref)
+    assert err < gate_, f"{strips} checkpoints + strips: L^T vs FP64 oracle {err:.3e}"
 
 
 def test_ac_born_pml_vs_reference_golden(cuda_device):
