@@ -709,8 +709,11 @@ def run_unet(args):
         k, _, co, ci = ws
         scale = 4 ** int(name[1]) // 4 if name[0] in "ed" else 1  # level l runs at 1/4^(l-1) pixels
         flops += 2.0 * h * w / scale * co * ci * k * k
+    opts = parse_set(args.set)  # network options (e.g. tcgen05_wgrad=0)
     with UNet(base=32, max_n=1, max_h=h, max_w=w) as net:
         net.set_params(he_normal(5))
+        for k, v in opts.items():
+            net.set_option(k, v)
         for _ in range(args.warmup):
             net.forward(x.data_ptr(), y.data_ptr(), 1, h, w)
             net.loss_grad(x.data_ptr(), t.data_ptr(), 1, h, w)
@@ -732,7 +735,8 @@ def run_unet(args):
             "ms_per_step": round(fwd_ms, 3), "higher_is_better": True, "dtype": "bf16 (fp32 accumulate)",
             "data": "synthetic (random image)",
             "config": {"workload": "U-Net preconditioner", "image": f"{h}x{w}", "base_channels": 32,
-                       "forward_gflop": round(flops / 1e9, 2), "train_step_ms": round(train_ms, 3)}}
+                       "forward_gflop": round(flops / 1e9, 2), "train_step_ms": round(train_ms, 3),
+                       "options": opts}}
 
 
 def run_lsrtm(args):

@@ -7,6 +7,8 @@ one-column ring kernels, and, for the random boundary, the pair-blocked bulk-cop
 (`pair`) with their CTA widths (`pair_cta` backward, `pair_fcta` forward), rows per CTA
 (`pair_xr`) and the backward step fused or split in two launches (`pair_split`); `pair` 2
 takes the pair kernel for the forward step only, with the backward on the one-column kernel.
+The forward step can also run time-blocked (`tb` = time steps per launch, 1-4, `tb_cta` = its
+CTA width): one launch advances the batch by `tb` steps, reading and writing the state once.
 Their best values depend on the grid, the number of resident shots and the boundary, so the
 tuner times each candidate on a probe context with the caller's grid and batch but only
 `probe_nt` time steps (an RTM of the same shots: one forward and one backward fused launch per
@@ -15,7 +17,8 @@ import numpy as np
 
 from .api import Elastic2D
 
-_RING_BASE = {"pair": 0, "pair_split": 0, "pair_cta": 0, "pair_fcta": 0, "pair_xr": 0}
+_RING_BASE = {"pair": 0, "pair_split": 0, "pair_cta": 0, "pair_fcta": 0, "pair_xr": 0, "tb": 0,
+              "tb_cta": 0}
 _RING_SPACE = [
     {"ring": 4, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 0, "cta": 192},
     {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 192},
@@ -30,14 +33,19 @@ _PAIR_SPACE = ([{"pair": 2, "pair_split": 0, "pair_cta": 0, "pair_fcta": fcta, "
                 for cta in (256, 64) for xr in (0, 96)] +
                [{"pair": 1, "pair_split": 1, "pair_cta": 0, "pair_fcta": 256, "pair_xr": xr}
                 for xr in (0, 96)])
-_RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0}
+# Time-blocked forward (random boundary only): depth 1-4 at the automatic CTA width, and the
+# 512-thread single-strip CTAs at depth 1-2; the backward on the one-column ring kernel.
+_TB_SPACE = ([{"tb": k, "tb_cta": 0, "cta": 192} for k in (1, 2, 3, 4)] +
+             [{"tb": k, "tb_cta": 512, "cta": 192} for k in (1, 2)])
+_RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0, "tb": 0, "tb_cta": 0}
 
 
 def default_space(boundary="random"):
     """Full option sets (every knob named, so no setting carries over between candidates)."""
     space = [dict(_RING_BASE, **c) for c in _RING_SPACE]
     if boundary == "random":
-        space = [dict(_RING_DEFAULTS, **c) for c in _PAIR_SPACE] + space
+        space = ([dict(_RING_DEFAULTS, **c) for c in _PAIR_SPACE] +
+                 [{**_RING_DEFAULTS, **_RING_BASE, **c} for c in _TB_SPACE] + space)
     return space
 
 

@@ -23,6 +23,7 @@
 #include "ds2d_fused.cuh"
 #include "ds2d_pair.cuh"
 #include "ds2d_step.cuh"
+#include "ds2d_tblock.cuh"
 
 using namespace ds2d;
 
@@ -269,6 +270,10 @@ struct ds2d_ctx {
   // fill whole waves).
   int opt_pair = 0, opt_pair_cta = 0, opt_pair_fcta = 0, opt_pair_xr = 0, opt_pair_split = 0;
   int opt_ac_pair = 1, opt_ac_pair_cta = 0;  // acoustic steps on k_ac_pair / k_ac_rev_pair
+  // Time-blocked forward launches (ds2d_tblock.cuh, random boundary): option "tb" = time steps
+  // per launch (0 off, 1-4), "tb_cta" = threads per CTA (0 automatic, 256 or 512).
+  int opt_tb = 0, opt_tb_cta = 0;
+  int occ_tb[2][4] = {};     // resident CTAs per SM of k_fwd_tb, [256 / 512 threads][depth - 1]
   // split backward: the two launches of a step as parallel branches (second stream, fork / join
   // events; parallel nodes in a captured graph)
   cudaStream_t aux = nullptr;
@@ -738,6 +743,84 @@ int check_pair_err(ds2d_ctx *c) {
   return DS2D_OK;
 }
 
+// ---- time-blocked forward kernels (random boundary) ----------------------------------------
+// k_fwd_tb<depth, threads>: 256 threads at any depth (register budget for 3 / 2 / 1 / 1 CTAs per
+// SM at depth 1 / 2 / 3 / 4), or 512 threads at depth 1-2 (one CTA per SM: a single strip covers
+// a grid up to 512 deep with no z-halo, e.g. 481 rows, which 256-thread strips split in three
+// once the depth-2 halo of 16 columns is added).
+constexpr int kTbCtas[2] = {256, 512};
+constexpr int kTbMaxXr = 512;  // rows per CTA (bounds the trace-index staging in shared memory)
+using TbFn = void (*)(FwdFusedArgs);
+template <int kT>
+TbFn tb_fn_t(int depth) {
+  switch (depth) {
+    case 1: return k_fwd_tb<1, kT, 3>;
+    case 2: return k_fwd_tb<2, kT, 2>;
+    case 3: return k_fwd_tb<3, kT, 1>;
+    default: return k_fwd_tb<4, kT, 1>;
+  }
+}
+TbFn tb_fn(int depth, int cta) {
+  if (cta == 512) return depth == 1 ? k_fwd_tb<1, 512, 1> : k_fwd_tb<2, 512, 1>;
+  return tb_fn_t<256>(depth);
+}
+int tb_idx(int cta) { return cta == 512 ? 1 : 0; }
+// z-strips of a time-blocked launch of depth K: a strip owns tz columns, its CTA covers them plus
+// 8K halo columns at each inner edge (one strip: the whole depth; two: one halo each; more: the
+// inner strips carry two).  Returns false when kT threads cannot cover a strip.
+bool tb_split(const Dims &d, int kT, int K, int *nstrips, int *tz) {
+  const int H = 8 * K;
+  for (int ns = 1; ns <= 64; ns++) {
+    const int t = (d.nzp + ns - 1) / ns;
+    const int cap = ns == 1 ? kT : ns == 2 ? kT - H : kT - 2 * H;
+    if (t <= cap) {
+      *nstrips = ns;
+      *tz = t;
+      return true;
+    }
+  }
+  return false;
+}
+// CTA width: option "tb_cta", else the width with the fewest threads per grid row.
+int tb_cta(const ds2d_ctx *c, int K) {
+  if (c->opt_tb_cta) return K > 2 ? 256 : c->opt_tb_cta;
+  int best = 256;
+  long long best_thr = 1LL << 40;
+  for (int cta : kTbCtas) {
+    int ns, tz;
+    if ((cta == 512 && K > 2) || !tb_split(c->d, cta, K, &ns, &tz)) continue;
+    if ((long long)ns * cta < best_thr) {
+      best_thr = (long long)ns * cta;
+      best = cta;
+    }
+  }
+  return best;
+}
+// Rows per CTA: a CTA marches xr + 16K row steps; xr minimises waves x (xr + 12K) over the
+// batch's window widths (the halo steps at the start only load and fill windows).
+int tb_xr(const ds2d_ctx *c, int nstrips, int per_sm, int K) {
+  if (c->opt_pair_xr > 0) return std::min(kTbMaxXr, std::max(8, c->opt_pair_xr));
+  const long long slots = (long long)c->num_sms * std::max(1, per_sm);
+  long long best = -1;
+  int best_xr = 128;
+  for (int xr = 48; xr <= kTbMaxXr; xr++) {
+    long long ctas = 0;
+    for (int nx : c->h_nxp) ctas += (long long)nstrips * ((nx + xr - 1) / xr);
+    const long long cost = (ctas + slots - 1) / slots * (xr + 12 * K);
+    if (best < 0 || cost <= best) {
+      best = cost;
+      best_xr = xr;
+    }
+  }
+  return best_xr;
+}
+bool tb_on(const ds2d_ctx *c) {
+  if (!(c->opt_tb > 0 && c->opt_fused && c->ring_ok && c->d.rbc && c->d.nop == 4)) return false;
+  const int cta = tb_cta(c, c->opt_tb);
+  int ns, tz;
+  return tb_split(c->d, cta, c->opt_tb, &ns, &tz) && c->occ_tb[tb_idx(cta)][c->opt_tb - 1] > 0;
+}
+
 // Acoustic pair kernels (k_ac_pair): 256 / 192 / 128 threads at 2 / 3 / 4 CTAs per SM.
 constexpr int kAcPairCtas[3] = {256, 192, 128};
 using AcPairFn = void (*)(AcRingArgs);
@@ -805,6 +888,28 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
   const int xr = std::max(8, c->opt_xr);
   dim3 grid(nstrips, (d.nxp + xr - 1) / xr, n);
   Wave *cur = &c->fw, *nxt = &c->fw2;
+  if (!strips && tb_on(c)) {
+    // time blocks of opt_tb steps, one launch each (the last block takes what is left)
+    for (int it = 0; it < d.nt;) {
+      const int K = std::min(c->opt_tb, d.nt - it);
+      const int tc = tb_cta(c, c->opt_tb);
+      int ns, tz;
+      if (!tb_split(d, tc, K, &ns, &tz))
+        return fail(c, DS2D_E_ARG, "time-blocked strips do not fit %d threads", tc);
+      const int txr = tb_xr(c, ns, c->occ_tb[tb_idx(tc)][K - 1], K);
+      FwdFusedArgs a{};
+      a.d = d; a.a = *cur; a.b = *nxt; a.p = c->par; a.shots = c->d_shots; a.wavelet = c->wavelet;
+      a.it = it; a.tz = tz; a.xr = txr; a.rmap = c->d_rmap;
+      if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
+      dim3 tgrid(ns, (d.nxp + txr - 1) / txr, n);
+      LAUNCHS("fwd_tb", kBytesFused * CELLS(n), tb_fn(K, tc), tgrid, tc, tb_smem(K, tc, txr), a);
+      std::swap(cur, nxt);
+      it += K;
+    }
+    c->fw_cur = cur;
+    CK(cudaGetLastError());
+    return DS2D_OK;
+  }
   for (int it = 0; it < d.nt; it++) {
     FwdFusedArgs a{};
     a.d = d; a.a = *cur; a.b = *nxt; a.p = c->par; a.shots = c->d_shots; a.wavelet = c->wavelet;
@@ -950,7 +1055,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)), (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -1836,6 +1941,15 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
                                                             pair_bwd_smem(bctas[i]));
       }
     }
+    for (int i = 0; i < 2 && e == cudaSuccess; i++)
+      for (int K = 1; K <= (i ? 2 : 4) && e == cudaSuccess; K++) {
+        const int cta = kTbCtas[i];
+        const size_t sm = tb_smem(K, cta, kTbMaxXr);
+        e = cudaFuncSetAttribute(tb_fn(K, cta), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_tb[i][K - 1], tb_fn(K, cta),
+                                                            cta, sm);
+      }
     int dev = 0;
     if (e == cudaSuccess) e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1968,7 +2082,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair, (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)), (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -2432,6 +2546,13 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     if (value != 0 && (value < 8 || value > 4096))
       return fail(c, DS2D_E_ARG, "pair_xr must be 0 (automatic) or in [8, 4096]");
     c->opt_pair_xr = (int)value;
+  } else if (k == "tb") {
+    if (value < 0 || value > 4) return fail(c, DS2D_E_ARG, "tb must be 0 (off) or 1-4");
+    c->opt_tb = (int)value;
+  } else if (k == "tb_cta") {
+    if (value != 0 && value != 256 && value != 512)
+      return fail(c, DS2D_E_ARG, "tb_cta must be 0 (automatic), 256 or 512 (depth 1-2)");
+    c->opt_tb_cta = (int)value;
   } else if (k == "xr") {
     if (value < 8 || value > 4096) return fail(c, DS2D_E_ARG, "xr must be in [8, 4096]");
     c->opt_xr = (int)value;

@@ -1,6 +1,7 @@
-// Image-domain U-Net preconditioner on sm_100a: BF16 tensor-core (mma.sync m16n8k16, FP32
-// accumulate) convolution kernels for inference and training, with the host orchestration of the
-// network, its Adam optimiser and its C ABI (include/ds2d.h, ds2d_unet_*).
+// Image-domain U-Net preconditioner on sm_100a: BF16 tensor-core convolution kernels (tcgen05
+// with TMEM accumulators by default, mma.sync m16n8k16 as the checked alternative; FP32
+// accumulate) for inference and training, with the host orchestration of the network, its Adam
+// optimiser and its C ABI (include/ds2d.h, ds2d_unet_*).
 //
 // The reference has no learned component; the network approximates the inverse Hessian of the
 // Born operator (maps an RTM image to reflectivity) and preconditions CG-LSRTM.  Architecture
@@ -434,6 +435,192 @@ __global__ void __launch_bounds__(128) k_conv3x3_wgrad(WgradArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// The weight gradient on the tensor cores (tcgen05, accumulators in TMEM).  The product is
+// dW[tap][co][ci] = sum_p dz[p][co] x[p + tap][ci]: D = A B^T with A = dz^T (M = 128 output
+// channels, K = pixels) and B = x shifted by the tap (N = kN input channels, K = pixels).  A CTA
+// owns 128 output channels x kN input channels x the three taps of one kernel row ky (3 kN TMEM
+// columns), and a contiguous range of 64-pixel row chunks (split-K over CTAs, FP32 atomics at the
+// end).  Per chunk it copies the raw rows (dz: 64 pixels x 128 channels; x: row r + ky - 1, 66
+// pixels x kN channels) into shared memory, rebuilds them transposed (pixels contiguous) in the
+// canonical K-major no-swizzle layout -- one 8-pixel core-matrix row per 16-byte store, a copy of
+// x per horizontal shift kx because a one-pixel shift along K is not a descriptor offset -- and
+// one thread issues the 3 x 4 UMMAs (M 128, N kN, K 16).  The raw copy of the next chunk overlaps
+// the MMAs of this one; the rebuild waits for them (bounded mbarrier wait).
+// ---------------------------------------------------------------------------------------------
+constexpr int kWgP = 64;                 // pixels per chunk (4 UMMA K-steps)
+constexpr int kWgM = 128;                // output channels per CTA (UMMA M)
+constexpr int kWgPlaneA = kWgM * 16;     // bytes of one 8-pixel plane of A
+
+template <int kN>
+constexpr int wg_tc_smem_bytes() {
+  // raw dz [P][128] + raw x [P + 2][kN] + A [P/8][128][16 B] + B [3][P/8][kN][16 B]
+  return kWgP * kWgM * 2 + (kWgP + 2) * kN * 2 + (kWgP / 8) * kWgPlaneA + 3 * (kWgP / 8) * kN * 16;
+}
+
+template <int kN>
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad_tc(WgradArgs a, int *err) {
+  extern __shared__ __align__(1024) unsigned char wg_smem[];
+  unsigned char *sA = wg_smem;                                   // transposed dz (1024-aligned)
+  unsigned char *sB = sA + (kWgP / 8) * kWgPlaneA;                // transposed x, per kx
+  bf16 *raw_dz = reinterpret_cast<bf16 *>(sB + 3 * (kWgP / 8) * kN * 16);  // [P][128]
+  bf16 *raw_x = raw_dz + kWgP * kWgM;                             // [P + 2][kN]
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int co0 = blockIdx.x * kWgM;
+  const int ci0 = (blockIdx.y / 3) * kN, ky = blockIdx.y % 3;
+  constexpr uint32_t kCols = 3 * kN <= 64 ? 64 : 128;  // TMEM columns: a power of two >= 3 kN
+  constexpr int kBPlane = kN * 16;                     // bytes of one 8-pixel plane of B
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base)), "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar)));
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t idesc = umma_idesc(kWgM, kN);
+  const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+  const int wchunks = (a.w + kWgP - 1) / kWgP;
+  const long long total = (long long)a.n * a.h * wchunks;
+  const long long c_begin = (long long)blockIdx.z * a.chunks_per_cta;
+  const long long c_end = c_begin + a.chunks_per_cta < total ? c_begin + a.chunks_per_cta : total;
+  const bool do_bias = a.db && blockIdx.y == 0;
+  float bsum = 0.f;
+  bool ok = true, pending = false;
+  int phase = 0;
+  auto wait_mma = [&]() {
+    uint32_t done = 0;
+    for (int spin = 0; spin < kTcSpin && !done; spin++) {
+      asm volatile(
+          "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+          "selp.u32 %0, 1, 0, p;\n}\n"
+          : "=r"(done)
+          : "r"(smem_u32(&mbar)), "r"(phase)
+          : "memory");
+    }
+    if (!done) {
+      ok = false;
+      if (tid == 0) atomicExch(err, 1);
+    }
+    phase ^= 1;
+  };
+  for (long long cidx = c_begin; cidx < c_end && ok; cidx++) {
+    const int wc = (int)(cidx % wchunks);
+    const long long rr = cidx / wchunks;
+    const int row = (int)(rr % a.h), img = (int)(rr / a.h);
+    const int w0 = wc * kWgP;
+    // ---- raw copies (overlap the previous chunk's MMAs, which read only sA / sB) ----------
+    for (int i = tid; i < kWgP * (kWgM / 8); i += 128) {  // dz: 16-byte pieces of 8 channels
+      const int px = i / (kWgM / 8), cg = i % (kWgM / 8);
+      const int ww = w0 + px, co = co0 + cg * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (ww < a.w && co < a.cout)
+        v = *reinterpret_cast<const uint4 *>(
+            a.dz + (((long long)img * a.h + row) * a.w + ww) * a.zcs + co);
+      *reinterpret_cast<uint4 *>(raw_dz + px * kWgM + cg * 8) = v;
+    }
+    const int hh = row + ky - 1;
+    for (int i = tid; i < (kWgP + 2) * (kN / 8); i += 128) {  // x: row hh, pixels w0-1 .. w0+P
+      const int px = i / (kN / 8), cg = i % (kN / 8);
+      const int ww = w0 + px - 1;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (hh >= 0 && hh < a.h && ww >= 0 && ww < a.w)
+        v = *reinterpret_cast<const uint4 *>(
+            a.x + (((long long)img * a.h + hh) * a.w + ww) * a.cin + ci0 + cg * 8);
+      *reinterpret_cast<uint4 *>(raw_x + px * kN + cg * 8) = v;
+    }
+    if (pending) wait_mma();  // the previous chunk's MMAs are done with sA / sB
+    pending = false;
+    if (!__syncthreads_and(ok)) {  // every thread leaves together if any wait gave up
+      ok = false;
+      break;
+    }
+    // ---- transposed rebuild: core-matrix row (channel, 8 pixels) per 16-byte store -------
+    {
+      const int m = tid;  // output channel co0 + m; plane g = pixels 8g .. 8g+7
+#pragma unroll
+      for (int g = 0; g < kWgP / 8; g++) {
+        __align__(16) bf16 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          v[j] = raw_dz[(8 * g + j) * kWgM + m];
+          if (do_bias) bsum += __bfloat162float(v[j]);
+        }
+        *reinterpret_cast<uint4 *>(sA + g * kWgPlaneA + (m >> 3) * 128 + (m & 7) * 16) =
+            *reinterpret_cast<const uint4 *>(v);
+      }
+    }
+    for (int i = tid; i < 3 * (kWgP / 8) * kN; i += 128) {
+      const int ci = i % kN, g = (i / kN) % (kWgP / 8), kx = i / (kN * (kWgP / 8));
+      __align__(16) bf16 v[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) v[j] = raw_x[(8 * g + j + kx) * kN + ci];
+      *reinterpret_cast<uint4 *>(sB + (kx * (kWgP / 8) + g) * kBPlane + (ci >> 3) * 128 +
+                                 (ci & 7) * 16) = *reinterpret_cast<const uint4 *>(v);
+    }
+    // generic-proxy writes -> visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+#pragma unroll
+      for (int kx = 0; kx < 3; kx++)
+#pragma unroll
+        for (int s = 0; s < kWgP / 16; s++) {
+          const uint64_t ad = umma_desc(a_base + (2 * s) * kWgPlaneA, kWgPlaneA, 128);
+          const uint64_t bd =
+              umma_desc(b_base + (kx * (kWgP / 8) + 2 * s) * kBPlane, kBPlane, 128);
+          const uint32_t acc = (cidx > c_begin || s > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+                  tmem + (uint32_t)(kx * kN)),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+        }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+              smem_u32(&mbar)));
+    }
+    pending = true;
+  }
+  if (pending && ok) wait_mma();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  if (ok && c_end > c_begin) {
+    // epilogue: thread (warp w, lane l) owns output channel co0 + 32 w + l
+    const int co = co0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int kx = 0; kx < 3; kx++) {
+      float *dst = a.dw + ((long long)(ky * 3 + kx) * a.cout + co) * a.cin + ci0;
+#pragma unroll 1
+      for (int c0 = 0; c0 < kN; c0 += 8) {
+        uint32_t r[8];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kx * kN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+              "=r"(r[7])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (co < a.cout) {
+#pragma unroll
+          for (int j = 0; j < 8; j++) atomicAdd(dst + c0 + j, __uint_as_float(r[j]));
+        }
+      }
+    }
+    if (do_bias && tid < kWgM && co0 + tid < a.cout) atomicAdd(a.db + co0 + tid, bsum);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Element-wise and small kernels
 // ---------------------------------------------------------------------------------------------
 // FP32 image [N][H][W] -> BF16 [N][H][W][16] (channel 0 = value, 1..15 = 0)
@@ -625,6 +812,7 @@ struct ds2d_unet {
   std::string err;
   bool weights_dirty = true;
   int use_tc = 1;          // 3x3 convolutions on tcgen05 (1, default) or mma.sync (0)
+  int tc_wgrad = 1;        // with use_tc: weight gradients on tcgen05 too (0: on mma.sync)
   int *d_err = nullptr;    // device flag raised by a bounded wait that gave up
   std::vector<void *> allocs;
 };
@@ -697,6 +885,23 @@ int wgrad(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *dz, int zcs, cons
   // padded scratch that the caller folds
   if (L.cin_pad != L.cin && !dw_padded)
     return unet_fail(u, DS2D_E_STATE, "wgrad of a channel-padded layer needs a padded scratch");
+  if (u->use_tc && u->tc_wgrad && L.cin_pad % 16 == 0) {
+    // tcgen05: CTAs of 128 output channels x kN input channels x one kernel row, 64-pixel chunks
+    const int kn = L.cin_pad % 32 == 0 ? 32 : 16;
+    const long long tchunks = (long long)n * h * ((wd + kWgP - 1) / kWgP);
+    const long long ttiles = (long long)((L.cout + kWgM - 1) / kWgM) * (L.cin_pad / kn) * 3;
+    long long ts = (4 * 148 + ttiles - 1) / ttiles;
+    ts = ts > tchunks ? tchunks : (ts < 1 ? 1 : ts);
+    a.chunks_per_cta = (int)((tchunks + ts - 1) / ts);
+    ts = (tchunks + a.chunks_per_cta - 1) / a.chunks_per_cta;
+    dim3 tgrid((L.cout + kWgM - 1) / kWgM, (L.cin_pad / kn) * 3, (unsigned)ts);
+    if (kn == 32)
+      k_conv3x3_wgrad_tc<32><<<tgrid, 128, wg_tc_smem_bytes<32>(), u->stream>>>(a, u->d_err);
+    else
+      k_conv3x3_wgrad_tc<16><<<tgrid, 128, wg_tc_smem_bytes<16>(), u->stream>>>(a, u->d_err);
+    UCK(cudaGetLastError());
+    return DS2D_OK;
+  }
   dim3 grid(L.cout / 32, L.cin_pad / kci, (unsigned)splits);
   if (kci == 32)
     k_conv3x3_wgrad<2><<<grid, 128, 0, u->stream>>>(a);
@@ -959,6 +1164,12 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
     if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc_smem_bytes<32>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tc<32>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, wg_tc_smem_bytes<32>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tc<16>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, wg_tc_smem_bytes<16>());
     if (ea != cudaSuccess)
       rc = unet_fail(u, DS2D_E_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
   }
@@ -1027,6 +1238,10 @@ int ds2d_unet_set_option(ds2d_unet *u, const char *key, long long value) {
   if (!u || !key) return unet_fail(u, DS2D_E_ARG, "set_option: null argument");
   if (std::string(key) == "tcgen05") {
     u->use_tc = value != 0;
+    return DS2D_OK;
+  }
+  if (std::string(key) == "tcgen05_wgrad") {
+    u->tc_wgrad = value != 0;
     return DS2D_OK;
   }
   return unet_fail(u, DS2D_E_ARG, std::string("unknown option ") + key);

@@ -91,7 +91,8 @@ class UNet:
             raise DS2DError(rc, self.lib.ds2d_unet_last_error(self.h).decode())
 
     def set_option(self, key, value):
-        """"tcgen05": 1 = 3x3 convolutions on tcgen05 / TMEM, 0 = mma.sync."""
+        """"tcgen05": 1 = 3x3 convolutions on tcgen05 / TMEM, 0 = mma.sync; "tcgen05_wgrad": 0
+        keeps the weight gradient on mma.sync."""
         self._check(self.lib.ds2d_unet_set_option(self.h, key.encode(), int(value)))
 
     def set_stream(self, stream_handle):

@@ -259,9 +259,9 @@ int ds2d_unet_loss_grad(ds2d_unet *net, const float *x, const float *target, int
                         double *loss, float *grads_host);
 /* One Adam step (bias-corrected) with the gradients of the last ds2d_unet_loss_grad. */
 int ds2d_unet_adam_step(ds2d_unet *net, float lr, float beta1, float beta2, float eps);
-/* "tcgen05" = 1 (default) runs the 3x3 convolutions (forward and backward-data) on the
- * 5th-generation tensor cores with TMEM accumulators; 0 on mma.sync.  The weight gradient uses
- * mma.sync. */
+/* "tcgen05" = 1 (default) runs the 3x3 convolutions (forward, backward-data and weight gradient)
+ * on the 5th-generation tensor cores with TMEM accumulators; 0 runs all three on mma.sync.
+ * "tcgen05_wgrad" = 0 keeps only the weight gradient on mma.sync (default 1). */
 int ds2d_unet_set_option(ds2d_unet *net, const char *key, long long value);
 
 #ifdef __cplusplus

@@ -212,13 +212,16 @@ def test_lsrtm_pcg_plain_matches_cgls_and_net_descends(cuda_device):
 
 
 def test_acoustic_fused_steps_match_half_steps(cuda_device):
-    """The fused acoustic step (velocity + stress + Born source in one x-march, ping-pong state)
-    against one launch per half step, for L and L^T."""
+    """The fused one-column acoustic step (velocity + stress + Born source in one x-march,
+    ping-pong state) against one launch per half step, for L and L^T.  The pair-blocked kernels
+    (the default) round their z-taps differently and are gated against these at the FP32 floor in
+    test_ac_pair_kernels_match_ring_and_oracle."""
     c, vp, vs, w, shots, m = acoustic_case(nt=300, nshots=3)
     out = {}
     for fused in (0, 1):
         with ctx(c, shots) as e:
             e.set_option("fused", fused)
+            e.set_option("ac_pair", 0)
             e.set_models(vp, vs)
             e.set_wavelet(w)
             dz, dx = e.ac_born(shots, m)
@@ -332,14 +335,16 @@ def test_ac_born_adj_pml_half_precision_strips(cuda_device, strips, gate):
     assert err < gate, f"{strips} strips: L^T vs FP64 oracle {err:.3e}"
 
 
-@pytest.mark.parametrize("strips,gate_", [("f32", 1e-6), ("f16", 2e-3), ("bf16", 2e-2)])
+@pytest.mark.parametrize("strips,gate_", [("f32", BORN_GATE), ("f16", 4e-3), ("bf16", 4e-2)])
 def test_ac_born_adj_pml_checkpoints(cuda_device, strips, gate_):
     """L^T with the background checkpointed every 37 steps (option ac_ckpt: whole-state snapshots
     in the strip precision with one FP32 scale per field, shot and snapshot; each 37-step segment
     replayed from its snapshot with strips, then reversed; 300 steps give 8 full segments and a
-    4-step one).  FP32 snapshots replay the same states bit for bit, so the gradient equals the
-    all-strips path's; FP16 / BF16 snapshots and strips are gated against the FP64 oracle's exact
-    transpose like the strips alone."""
+    4-step one) against the FP64 oracle's exact transpose.  Each segment's reversal starts from
+    the replayed forward state, where the all-strips path continues its own reversed background,
+    so with FP32 snapshots the two gradients differ by rounding only (gate 1e-5).  With FP16 /
+    BF16 both the snapshots and the strips are quantised: the gates are twice the strips-alone
+    gates."""
     c, vp, w, shots, m = _pml_case()
     st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
     rng = np.random.default_rng(8)
@@ -349,8 +354,7 @@ def test_ac_born_adj_pml_checkpoints(cuda_device, strips, gate_):
     _, _, g_ck = _pml_run(c, vp, w, shots, m, strips, rz, rx, opts={"ac_ckpt": 37})
     if strips == "f32":
         _, _, g_all = _pml_run(c, vp, w, shots, m, strips, rz, rx)
-        assert rel(g_ck, g_all) < gate_, rel(g_ck, g_all)
-        return
+        assert rel(g_ck, g_all) < 1e-5, rel(g_ck, g_all)
     gref = np.zeros((c["allnx"], c["allnz"]))
     for i, s in enumerate(shots):
         model = po.build_model(st, vp, 0 * vp, None, s.win_left)
