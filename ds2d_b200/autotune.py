@@ -9,6 +9,8 @@ one-column ring kernels, and, for the random boundary, the pair-blocked bulk-cop
 takes the pair kernel for the forward step only, with the backward on the one-column kernel.
 The forward step can also run time-blocked (`tb` = time steps per launch, 1-4, `tb_cta` = its
 CTA width): one launch advances the batch by `tb` steps, reading and writing the state once.
+The backward step can run warp-specialised (`bwd_ws` = threads per role, 96 / 128 / 192): the
+source and adjoint wavefields on separate warps of one CTA.
 Their best values depend on the grid, the number of resident shots and the boundary, so the
 tuner times each candidate on a probe context with the caller's grid and batch but only
 `probe_nt` time steps (an RTM of the same shots: one forward and one backward fused launch per
@@ -18,7 +20,7 @@ import numpy as np
 from .api import Elastic2D
 
 _RING_BASE = {"pair": 0, "pair_split": 0, "pair_cta": 0, "pair_fcta": 0, "pair_xr": 0, "tb": 0,
-              "tb_cta": 0}
+              "tb_cta": 0, "bwd_ws": 0}
 _RING_SPACE = [
     {"ring": 4, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 0, "cta": 192},
     {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 192},
@@ -37,7 +39,10 @@ _PAIR_SPACE = ([{"pair": 2, "pair_split": 0, "pair_cta": 0, "pair_fcta": fcta, "
 # 512-thread single-strip CTAs at depth 1-2; the backward on the one-column ring kernel.
 _TB_SPACE = ([{"tb": k, "tb_cta": 0, "cta": 192} for k in (1, 2, 3, 4)] +
              [{"tb": k, "tb_cta": 512, "cta": 192} for k in (1, 2)])
-_RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0, "tb": 0, "tb_cta": 0}
+# Warp-specialised backward (random boundary only) behind the two best forward kernels.
+_WS_SPACE = ([{"tb": 2, "tb_cta": 0, "bwd_ws": kt} for kt in (96, 128, 192)] +
+             [{"pair": 2, "pair_fcta": 256, "bwd_ws": kt} for kt in (96, 128, 192)])
+_RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0, "tb": 0, "tb_cta": 0, "bwd_ws": 0}
 
 
 def default_space(boundary="random"):
@@ -45,7 +50,7 @@ def default_space(boundary="random"):
     space = [dict(_RING_BASE, **c) for c in _RING_SPACE]
     if boundary == "random":
         space = ([dict(_RING_DEFAULTS, **c) for c in _PAIR_SPACE] +
-                 [{**_RING_DEFAULTS, **_RING_BASE, **c} for c in _TB_SPACE] + space)
+                 [{**_RING_DEFAULTS, **_RING_BASE, **c} for c in _TB_SPACE + _WS_SPACE] + space)
     return space
 
 

@@ -24,6 +24,7 @@
 #include "ds2d_pair.cuh"
 #include "ds2d_step.cuh"
 #include "ds2d_tblock.cuh"
+#include "ds2d_bwdws.cuh"
 
 using namespace ds2d;
 
@@ -273,6 +274,10 @@ struct ds2d_ctx {
   // Time-blocked forward launches (ds2d_tblock.cuh, random boundary): option "tb" = time steps
   // per launch (0 off, 1-4), "tb_cta" = threads per CTA (0 automatic, 256 or 512).
   int opt_tb = 0, opt_tb_cta = 0;
+  // Warp-specialised backward step (ds2d_bwdws.cuh, random boundary): option "bwd_ws" = threads
+  // per role (0 off, 96, 128 or 192; a CTA holds both roles).
+  int opt_bwd_ws = 0;
+  int occ_ws[3] = {};        // resident CTAs per SM of k_bwd_ws, 96 / 128 / 192 threads per role
   int occ_tb[2][4] = {};     // resident CTAs per SM of k_fwd_tb, [256 / 512 threads][depth - 1]
   // split backward: the two launches of a step as parallel branches (second stream, fork / join
   // events; parallel nodes in a captured graph)
@@ -814,6 +819,17 @@ int tb_xr(const ds2d_ctx *c, int nstrips, int per_sm, int K) {
   }
   return best_xr;
 }
+// ---- warp-specialised backward (random boundary) ------------------------------------------
+constexpr int kWsRoles[3] = {96, 128, 192};
+BwdFn ws_fn(int kt) {
+  return kt == 96 ? k_bwd_ws<96, 4> : kt == 128 ? k_bwd_ws<128, 3> : k_bwd_ws<192, 2>;
+}
+int ws_idx(int kt) { return kt == 96 ? 0 : kt == 128 ? 1 : 2; }
+bool ws_on(const ds2d_ctx *c) {
+  return c->opt_bwd_ws > 0 && c->opt_fused && c->ring_ok && c->d.rbc &&
+         c->occ_ws[ws_idx(c->opt_bwd_ws)] > 0;
+}
+
 bool tb_on(const ds2d_ctx *c) {
   if (!(c->opt_tb > 0 && c->opt_fused && c->ring_ok && c->d.rbc && c->d.nop == 4)) return false;
   const int cta = tb_cta(c, c->opt_tb);
@@ -1055,7 +1071,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)), (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32), (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -1113,6 +1129,13 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
         }
         CK(cudaEventRecord(c->ev_join, c->aux));
         CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+      } else if (ws_on(c)) {
+        const int kt = c->opt_bwd_ws;
+        int wns, wtz;
+        strip_split(d, kt, &wns, &wtz);
+        a.tz = wtz;
+        dim3 wgrid(wns, (d.nxp + xr - 1) / xr, n);
+        LAUNCHS("bwd_ws", kBytesBwdFused * CELLS(n), ws_fn(kt), wgrid, 2 * kt, ws_smem(kt), a);
       } else if (pair_bwd_on(c)) {
         const int pc = pair_bwd_cta(c);
         int pns, ptz;
@@ -1941,6 +1964,14 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
                                                             pair_bwd_smem(bctas[i]));
       }
     }
+    for (int i = 0; i < 3 && e == cudaSuccess; i++) {
+      const int kt = kWsRoles[i];
+      e = cudaFuncSetAttribute(ws_fn(kt), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)ws_smem(kt));
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_ws[i], ws_fn(kt), 2 * kt,
+                                                          ws_smem(kt));
+    }
     for (int i = 0; i < 2 && e == cudaSuccess; i++)
       for (int K = 1; K <= (i ? 2 : 4) && e == cudaSuccess; K++) {
         const int cta = kTbCtas[i];
@@ -2082,7 +2113,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)), (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32), (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -2549,6 +2580,10 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
   } else if (k == "tb") {
     if (value < 0 || value > 4) return fail(c, DS2D_E_ARG, "tb must be 0 (off) or 1-4");
     c->opt_tb = (int)value;
+  } else if (k == "bwd_ws") {
+    if (value != 0 && value != 96 && value != 128 && value != 192)
+      return fail(c, DS2D_E_ARG, "bwd_ws must be 0 (off) or 96, 128, 192 threads per role");
+    c->opt_bwd_ws = (int)value;
   } else if (k == "tb_cta") {
     if (value != 0 && value != 256 && value != 512)
       return fail(c, DS2D_E_ARG, "tb_cta must be 0 (automatic), 256 or 512 (depth 1-2)");

@@ -371,6 +371,10 @@ def test_elsrtm_batched_equals_one_by_one(cuda_device):
 
 @pytest.mark.parametrize("strips", ["f16", "bf16"])
 def test_half_precision_strips(cuda_device, strips):
+    """RTM with the PML and the source field rebuilt from FP16 / BF16 boundary strips (one FP32
+    scale per 32-cell segment) against the FP64 oracle, which keeps its strips exact: the error
+    the storage format adds to the images (gates: FP16 2e-3, BF16 2e-2 relative L2), next to the
+    FP32-strip run's own distance from the oracle."""
     fx = _need("rtm_pml.npz")
     c = case_of(fx)
     shots = shots_of(fx)
@@ -381,9 +385,18 @@ def test_half_precision_strips(cuda_device, strips):
             e.set_wavelet(fx["wavelet"])
             e.rtm(shots, fx["adj_vz"].reshape(-1, c["nt"]), fx["adj_vx"].reshape(-1, c["nt"]))
             out[prec] = e.read_images()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    tot64 = np.zeros((3, c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        m = po.build_model(st, fx["vp"], fx["vs"], None, s.win_left)
+        o = po.rtm(st, m, fx["wavelet"], s, fx["adj_vz"][i], fx["adj_vx"][i], 0, "f64")
+        for k in range(3):
+            tot64[k] += po.place(o[k], c["allnx"], c["allnz"], s.win_left)
     tol = 2e-3 if strips == "f16" else 2e-2
-    for key in ("pp_grad", "ps_grad", "illumination"):
-        assert rel(out[strips][key], out["f32"][key]) < tol, (key, rel(out[strips][key], out["f32"][key]))
+    for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
+        err = rel(out[strips][key], tot64[k])
+        err32 = rel(out["f32"][key], tot64[k])
+        assert err < tol, (key, err, f"FP32 strips: {err32:.3e}")
 
 
 @pytest.mark.skipif(not po.ref_available(), reason="reference build (oracle/_ref) not present")
@@ -611,3 +624,48 @@ def test_live_reference_elsrtm_full_size(cuda_device):
         assert e_64 < gate(floor), msg
         assert e_ref < gate(floor) + r_64, msg
     assert mis == pytest.approx(r["misfit"], rel=1e-4) and mis == pytest.approx(r64["misfit"], rel=1e-4)
+
+
+@pytest.mark.parametrize("kt,xr", [(96, 128), (128, 24), (192, 24), (192, 128)])
+def test_ws_backward_matches_ring_and_oracle(cuda_device, kt, xr):
+    """Warp-specialised backward step (k_bwd_ws: the source field and the adjoint field on
+    separate warps of one CTA, strains handed over in shared memory for the imaging condition)
+    against the one-column ring kernel and the FP64 oracle, random boundary.  The 320-deep grid
+    gives every role width two or more z-strips; xr 24 gives each shot several row blocks."""
+    c, _, _, w, _ = small_case(nt=200)
+    c["allnz"] = 300
+    vp, vs = synth.layered(c["allnx"], c["allnz"], seed=4)
+    shots = synth.surface_shots(c["allnx"], c["nx"], c["pml"], 3)
+    with _ctx(c, shots, boundary="pml") as e:
+        e.set_models(vp, vs)
+        e.set_wavelet(w)
+        oz, ox = e.forward(shots)
+    vpm, vsm = synth.smooth(vp, 3.0), synth.smooth(vs, 3.0)
+    out = {}
+    for ws in (0, kt):
+        with _ctx(c, shots, boundary="random", seed=5) as e:
+            e.set_option("pair", 0)
+            e.set_option("xr", xr)
+            e.set_option("bwd_ws", ws)
+            e.set_models(vpm, vsm)
+            e.set_wavelet(w)
+            e.rtm(shots, oz, ox)
+            out[ws] = e.read_images()
+    st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
+    ntr = shots[0].ntr
+    tot64 = np.zeros((3, c["allnx"], c["allnz"]))
+    tot32 = np.zeros((3, c["allnx"], c["allnz"]))
+    for i, s in enumerate(shots):
+        m = po.build_model(st, vpm, vsm, None, s.win_left, rbc=1, seed=5, shot_id=i)
+        sl = slice(i * ntr, (i + 1) * ntr)
+        for tot, prec in ((tot64, "f64"), (tot32, "f32")):
+            o = po.rtm(st, m, w, s, oz[sl], ox[sl], 1, prec)
+            for k in range(3):
+                tot[k] += po.place(o[k], c["allnx"], c["allnz"], s.win_left)
+    for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
+        assert np.abs(out[kt][key]).max() > 0
+        floor = rel(tot32[k], tot64[k])
+        err_ring = rel(out[kt][key], out[0][key])
+        err64 = rel(out[kt][key], tot64[k])
+        assert err_ring < gate(floor), (key, err_ring, f"FP32 floor {floor:.3e}")
+        assert err64 < gate(floor), (key, err64, f"FP32 floor {floor:.3e}")
