@@ -25,6 +25,7 @@
 #include "ds2d_step.cuh"
 #include "ds2d_tblock.cuh"
 #include "ds2d_bwdws.cuh"
+#include "ds2d_bwdbulk.cuh"
 
 using namespace ds2d;
 
@@ -81,7 +82,9 @@ FwdFn fwd_mode_fn(bool rbc, int mode) {
 using ScatFn = void (*)(BwdScatArgs);
 ScatFn bwd_scat_fn(bool rbc) { return rbc ? k_bwd_scat_ring<false, 4, 4> : k_bwd_scat_ring<true, 4, 4>; }
 
-BwdFn bwd_ring_fn(bool rbc, int depth, int occ = 0, int cta = kFB) {
+BwdFn bwd_ring_fn(bool rbc, int depth, int occ = 0, int cta = kFB, bool one = false) {
+  if (one && rbc && depth == 4 && occ == 0)  // one barrier per row step (random boundary)
+    return cta == kWideCta ? k_bwd_ring<false, 4, 2, kWideCta, true> : k_bwd_ring<false, 4, 3, kFB, true>;
   if (cta == kWideCta && depth == 4 && occ == 0)
     return rbc ? k_bwd_ring<false, 4, 2, kWideCta> : k_bwd_ring<true, 4, 2, kWideCta>;
   switch (depth * 2 + (occ ? 1 : 0)) {
@@ -277,6 +280,9 @@ struct ds2d_ctx {
   // Warp-specialised backward step (ds2d_bwdws.cuh, random boundary): option "bwd_ws" = threads
   // per role (0 off, 96, 128 or 192; a CTA holds both roles).
   int opt_bwd_ws = 0;
+  int opt_bwd_1b = 0;        // option "bwd_1b": one barrier per row step in k_bwd_ring (random boundary)
+  int opt_bwd_bulk = 0;      // option "bwd_bulk": k_bwd_bulk, operand rows by bulk copy (random boundary)
+  int occ_bulk[4] = {};      // resident CTAs per SM of k_bwd_bulk: [128 / 192 threads][one barrier]
   int occ_ws[3] = {};        // resident CTAs per SM of k_bwd_ws, 96 / 128 / 192 threads per role
   int occ_tb[2][4] = {};     // resident CTAs per SM of k_fwd_tb, [256 / 512 threads][depth - 1]
   // split backward: the two launches of a step as parallel branches (second stream, fork / join
@@ -825,6 +831,24 @@ BwdFn ws_fn(int kt) {
   return kt == 96 ? k_bwd_ws<96, 4> : kt == 128 ? k_bwd_ws<128, 3> : k_bwd_ws<192, 2>;
 }
 int ws_idx(int kt) { return kt == 96 ? 0 : kt == 128 ? 1 : 2; }
+// ---- bulk-copy-fed one-column backward (random boundary) ------------------------------------
+BwdFn bulk_fn(int cta, bool one) {
+  if (cta == kWideCta) return one ? k_bwd_bulk<kWideCta, 2, true> : k_bwd_bulk<kWideCta, 2, false>;
+  return one ? k_bwd_bulk<kFB, 3, true> : k_bwd_bulk<kFB, 3, false>;
+}
+int bulk_idx(int cta, bool one) { return (cta == kWideCta ? 2 : 0) + (one ? 1 : 0); }
+// z-strips whose width is a multiple of 4 (16-byte aligned copy rows), at most cta - 16 columns
+void bulk_split(const Dims &d, int cta, int *nstrips, int *tz) {
+  for (int ns = (d.nzp + cta - 17) / (cta - 16);; ns++) {
+    const int t = ((d.nzp + ns - 1) / ns + 3) / 4 * 4;
+    if (t <= cta - 16) {
+      *nstrips = ns;
+      *tz = t;
+      return;
+    }
+  }
+}
+
 bool ws_on(const ds2d_ctx *c) {
   return c->opt_bwd_ws > 0 && c->opt_fused && c->ring_ok && c->d.rbc &&
          c->occ_ws[ws_idx(c->opt_bwd_ws)] > 0;
@@ -1071,7 +1095,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32), (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk), (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -1129,6 +1153,14 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
         }
         CK(cudaEventRecord(c->ev_join, c->aux));
         CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+      } else if (c->opt_bwd_bulk && pair_ok(c) &&
+                 c->occ_bulk[bulk_idx(cta, c->opt_bwd_1b != 0)] > 0) {
+        int bns, btz;
+        bulk_split(d, cta, &bns, &btz);
+        a.tz = btz; a.err = c->d_err;
+        dim3 bgrid(bns, (d.nxp + xr - 1) / xr, n);
+        LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), bulk_fn(cta, c->opt_bwd_1b != 0), bgrid,
+                cta, bwd_bulk_smem(cta), a);
       } else if (ws_on(c)) {
         const int kt = c->opt_bwd_ws;
         int wns, wtz;
@@ -1147,7 +1179,7 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
                 pair_bwd_smem(pc), a);
       } else if (c->opt_ring && c->ring_ok) {
         const size_t sm = sizeof(float) * c->opt_ring * bwd_ring_fields(!d.rbc) * cta;
-        BwdFn kfn = bwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ, cta);
+        BwdFn kfn = bwd_ring_fn(d.rbc != 0, c->opt_ring, c->opt_occ, cta, c->opt_bwd_1b != 0);
         LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, fgrid, cta, sm, a);
       } else if (d.rbc) {
         LAUNCHP("bwd_fused", kBytesBwdFused * CELLS(n), k_bwd_fused<false>, fgrid, kFB, a);
@@ -1917,6 +1949,13 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
               e = cudaFuncSetAttribute(bwd_ring_fn(rbc, depth, occ, kWideCta),
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        bwd_sm / kFB * kWideCta);
+            if (rbc) {
+              for (int cta : {kFB, kWideCta})
+                if (e == cudaSuccess)
+                  e = cudaFuncSetAttribute(bwd_ring_fn(rbc, depth, occ, cta, true),
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           bwd_sm / kFB * cta);
+            }
           }
         }
     }
@@ -1963,6 +2002,16 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
                                                             pair_bwd_fn(bctas[i]), bctas[i],
                                                             pair_bwd_smem(bctas[i]));
       }
+    }
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) {
+      const int cta = i < 2 ? kFB : kWideCta;
+      const bool one = (i & 1) != 0;
+      e = cudaFuncSetAttribute(bulk_fn(cta, one), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)bwd_bulk_smem(cta));
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_bulk[bulk_idx(cta, one)],
+                                                          bulk_fn(cta, one), cta,
+                                                          bwd_bulk_smem(cta));
     }
     for (int i = 0; i < 3 && e == cudaSuccess; i++) {
       const int kt = kWsRoles[i];
@@ -2113,7 +2162,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32), (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk), (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -2580,6 +2629,12 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
   } else if (k == "tb") {
     if (value < 0 || value > 4) return fail(c, DS2D_E_ARG, "tb must be 0 (off) or 1-4");
     c->opt_tb = (int)value;
+  } else if (k == "bwd_bulk") {
+    if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "bwd_bulk must be 0 or 1");
+    c->opt_bwd_bulk = (int)value;
+  } else if (k == "bwd_1b") {
+    if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "bwd_1b must be 0 or 1");
+    c->opt_bwd_1b = (int)value;
   } else if (k == "bwd_ws") {
     if (value != 0 && value != 96 && value != 128 && value != 192)
       return fail(c, DS2D_E_ARG, "bwd_ws must be 0 (off) or 96, 128, 192 threads per role");

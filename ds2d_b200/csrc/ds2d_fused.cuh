@@ -781,13 +781,19 @@ __device__ __forceinline__ float strip_unpack(int prec, long long e, float word,
   return __bfloat162float(__ushort_as_bfloat16(h)) * sc;
 }
 
-template <bool kPML, int kD, int kMinB, int kT = kFB>
+// kOne (random boundary only): one barrier per row step instead of two.  Every z-tap row of a step
+// exists at its top -- stage 1's rows are this step's inputs at row r - 4, stage 2's are stage-1
+// outputs of row r - 8, computed four steps earlier -- so all eight are published there, into one
+// of two buffers (a thread running ahead writes the other), and the two stages then run without
+// a barrier between them.
+template <bool kPML, int kD, int kMinB, int kT = kFB, bool kOne = false>
 __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
   static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
+  static_assert(!(kOne && kPML), "the one-barrier step is built for the random boundary");
   constexpr int NF = bwd_ring_fields(kPML);
   extern __shared__ float ring[];  // [kD][NF][kT]
-  __shared__ float s_bvx[kT], s_bvz[kT], s_avx[kT], s_avz[kT];
-  __shared__ float s_btxz[kT], s_btzz[kT], s_m[kT], s_pzlx[kT];
+  // z-tap rows: bvx bvz avx avz (stage 1), btxz btzz M PzLx (stage 2); two buffers with kOne
+  __shared__ float s_zt[kOne ? 2 : 1][8][kT];
   // Receiver column (one thread of the CTA, if any): per row mod 16, the trace index (fetched 16
   // rows ahead), whether a trace sits there and its residual at this step (fetched 8 rows ahead)
   // and the cell's state without the residual (kept 8 rows for stage 2).
@@ -985,10 +991,20 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
     issue(r + kD - 1);
     // ---- stage 1: stresses of row r1 = r - 4 -----------------------------------------------
     const int r1 = r - 4;
+    float *const s_bvx = s_zt[kOne ? (r & 1) : 0][0], *const s_bvz = s_zt[kOne ? (r & 1) : 0][1];
+    float *const s_avx = s_zt[kOne ? (r & 1) : 0][2], *const s_avz = s_zt[kOne ? (r & 1) : 0][3];
+    float *const s_btxz = s_zt[kOne ? (r & 1) : 0][4], *const s_btzz = s_zt[kOne ? (r & 1) : 0][5];
+    float *const s_m = s_zt[kOne ? (r & 1) : 0][6], *const s_pzlx = s_zt[kOne ? (r & 1) : 0][7];
     s_bvx[t] = w_bvx[4];
     s_bvz[t] = w_bvz[4];
     s_avx[t] = w_avx[4];
     s_avz[t] = w_avz[4];
+    if (kOne) {  // stage-2 rows of row r - 8 (before this step's stage-1 push: index 5 / 1)
+      s_btxz[t] = w_btxz[5];
+      s_btzz[t] = w_btzz[1];
+      s_m[t] = w_M[5];
+      s_pzlx[t] = w_PzLx[1];
+    }
     __syncthreads();
     float btxx = 0.f, btzz = 0.f, btxz = 0.f, PL = 0.f, M = 0.f, PzLx = 0.f;
     if (c1 && zin && r >= x0 && r1 >= 0 && r1 < d.nxp) {
@@ -1074,11 +1090,13 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
     push(w_PzLx, PzLx);
     // ---- stage 2: velocities of row r2 = r - 8 ---------------------------------------------
     const int r2 = r - 8;
-    s_btxz[t] = w_btxz[4];
-    s_btzz[t] = w_btzz[0];
-    s_m[t] = w_M[4];
-    s_pzlx[t] = w_PzLx[0];
-    __syncthreads();
+    if (!kOne) {
+      s_btxz[t] = w_btxz[4];
+      s_btzz[t] = w_btzz[0];
+      s_m[t] = w_M[4];
+      s_pzlx[t] = w_PzLx[0];
+      __syncthreads();
+    }
     if (c2 && zin && r2 >= x0 && r2 < x1) {
       const int k = base + r2 * ld + z;
       const bool x_int = r2 >= pml && r2 < d.nxp - pml;

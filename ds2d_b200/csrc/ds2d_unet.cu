@@ -187,44 +187,37 @@ __host__ __device__ constexpr uint32_t umma_idesc(int m, int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
-// Bytes of one staging buffer (3 halo rows x 2 channel halves + 9 taps x 2 halves x kN rows),
-// rounded to 1 KiB; the kernel holds two.
-template <int kN>
-__host__ __device__ constexpr int tc_stage_bytes() {
-  return (6 * kTcPlaneA + 9 * 2 * kN * 16 + 1023) / 1024 * 1024;
-}
-
 template <int kN>
 __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  // two staging buffers, each: A planes [3 rows][2 halves][130 px][16 B], B planes [9 taps]
-  // [2 halves][kN][16 B]; chunk c is staged in buffer c & 1 while the MMAs of chunk c - 1 run
-  __shared__ __align__(8) uint64_t mbar[2];
+  // layout: A planes [3 rows][2 halves][130 px][16 B], B planes [9 taps][2 halves][kN][16 B]
+  unsigned char *sA = tc_smem;
+  unsigned char *sB = tc_smem + 6 * kTcPlaneA;
+  __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int w0 = blockIdx.x * kTcM, row = blockIdx.y;
   const int ngrp = a.cout / kN;
   const int img = blockIdx.z / ngrp, co0 = (blockIdx.z % ngrp) * kN;
   constexpr uint32_t kCols = kN < 32 ? 32 : kN;  // TMEM columns: a power of two >= 32
-  constexpr int kStage = tc_stage_bytes<kN>();
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&tmem_base)), "r"(kCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[0])));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[1])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar)));
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const uint32_t tmem = tmem_base;
   constexpr uint32_t idesc = umma_idesc(kTcM, kN);
-  // stage the 3 halo rows (pixel px of row ky, channel half kh -> plane (ky, kh)) and the weights
-  // (tap, half, cout row) of the 16-channel chunk at ci0 into buffer `buf`
-  auto stage = [&](int ci0, unsigned char *buf) {
-    unsigned char *sA = buf, *sB = buf + 6 * kTcPlaneA;
+  const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
+  bool ok = true;
+  int phase = 0;
+  for (int ci0 = 0; ci0 < a.cin && ok; ci0 += 16) {
+    // stage the 3 halo rows: pixel px of row ky, channel half kh -> plane (ky, kh), offset 16 px
     for (int i = tid; i < 3 * 2 * kTcHalo; i += 128) {
       const int px = i % kTcHalo, kh = (i / kTcHalo) & 1, ky = i / (2 * kTcHalo);
       const int hh = row + ky - 1, ww = w0 + px - 1;
@@ -234,74 +227,51 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
             a.in + (((long long)img * a.h + hh) * a.w + ww) * a.cin + ci0 + kh * 8);
       *reinterpret_cast<uint4 *>(sA + (ky * 2 + kh) * kTcPlaneA + px * 16) = v;
     }
+    // stage the weights: tap, half, cout row
     for (int i = tid; i < 9 * 2 * kN; i += 128) {
       const int co = i % kN, kh = (i / kN) & 1, tap = i / (2 * kN);
       const uint4 v = *reinterpret_cast<const uint4 *>(
           a.wt + ((long long)tap * a.cout + co0 + co) * a.cin + ci0 + kh * 8);
       *reinterpret_cast<uint4 *>(sB + (tap * 2 + kh) * (kN * 16) + co * 16) = v;
     }
-  };
-  // bounded wait for the next completion of barrier b (its phase bit flips per completion)
-  int phase[2] = {0, 0};
-  bool ok = true;
-  auto wait_bar = [&](int b) {
+    // generic-proxy writes -> visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+#pragma unroll
+      for (int tap = 0; tap < 9; tap++) {
+        const int ky = tap / 3, kx = tap % 3;
+        const uint64_t ad = umma_desc(a_base + (ky * 2) * kTcPlaneA + kx * 16, kTcPlaneA, 128);
+        const uint64_t bd = umma_desc(b_base + (tap * 2) * (kN * 16), kN * 16, 128);
+        const uint32_t acc = (ci0 > 0 || tap > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+          smem_u32(&mbar)));
+    }
+    // every thread waits until the MMAs of this chunk have read shared memory and finished
     uint32_t done = 0;
     for (int spin = 0; spin < kTcSpin && !done; spin++) {
       asm volatile(
           "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
           "selp.u32 %0, 1, 0, p;\n}\n"
           : "=r"(done)
-          : "r"(smem_u32(&mbar[b])), "r"(phase[b])
+          : "r"(smem_u32(&mbar)), "r"(phase)
           : "memory");
     }
     if (!done) {
       ok = false;
       if (tid == 0) atomicExch(err, 1);
     }
-    phase[b] ^= 1;
-  };
-  const int nch = a.cin / 16;
-  stage(0, tc_smem);
-  int waited = 0;  // chunks whose MMAs are known complete
-  for (int c = 0; c < nch; c++) {
-    unsigned char *cur = tc_smem + (c & 1) * kStage;
-    // generic-proxy writes of chunk c -> visible to the tensor core (async proxy)
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    if (!__syncthreads_and(ok)) {
-      ok = false;
-      break;
-    }
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-      const uint32_t a_base = smem_u32(cur), b_base = smem_u32(cur + 6 * kTcPlaneA);
-#pragma unroll
-      for (int tap = 0; tap < 9; tap++) {
-        const int ky = tap / 3, kx = tap % 3;
-        const uint64_t ad = umma_desc(a_base + (ky * 2) * kTcPlaneA + kx * 16, kTcPlaneA, 128);
-        const uint64_t bd = umma_desc(b_base + (tap * 2) * (kN * 16), kN * 16, 128);
-        const uint32_t acc = (c > 0 || tap > 0) ? 1u : 0u;
-        asm volatile(
-            "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
-      }
-      asm volatile(
-          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-              smem_u32(&mbar[c & 1])));
-    }
-    if (c + 1 < nch) {
-      // buffer (c + 1) & 1 was read by chunk c - 1's MMAs: wait for them, then stage into it
-      if (c >= 1) {
-        wait_bar((c - 1) & 1);
-        waited = c;
-      }
-      stage((c + 1) * 16, tc_smem + ((c + 1) & 1) * kStage);
-    }
+    phase ^= 1;
+    __syncthreads();
   }
-  // the last (up to two) chunks' completions, in commit order
-  for (int c = waited; c < nch && ok; c++) wait_bar(c & 1);
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-  if (__syncthreads_and(ok)) {
+  if (ok) {
     // epilogue: thread (warp w, lane l) owns output pixel 32 w + l, reads 8 columns at a time
     const int m = warp * 32 + lane;
     const int ww = w0 + m;
@@ -350,7 +320,7 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
 
 template <int kN>
 constexpr int tc_smem_bytes() {
-  return 2 * tc_stage_bytes<kN>();
+  return 6 * kTcPlaneA + 9 * 2 * kN * 16;
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -626,12 +626,20 @@ def test_live_reference_elsrtm_full_size(cuda_device):
     assert mis == pytest.approx(r["misfit"], rel=1e-4) and mis == pytest.approx(r64["misfit"], rel=1e-4)
 
 
-@pytest.mark.parametrize("kt,xr", [(96, 128), (128, 24), (192, 24), (192, 128)])
-def test_ws_backward_matches_ring_and_oracle(cuda_device, kt, xr):
-    """Warp-specialised backward step (k_bwd_ws: the source field and the adjoint field on
-    separate warps of one CTA, strains handed over in shared memory for the imaging condition)
-    against the one-column ring kernel and the FP64 oracle, random boundary.  The 320-deep grid
-    gives every role width two or more z-strips; xr 24 gives each shot several row blocks."""
+@pytest.mark.parametrize("opts,xr", [({"bwd_ws": 96}, 128), ({"bwd_ws": 128}, 24),
+                                     ({"bwd_ws": 192}, 24), ({"bwd_ws": 192}, 128),
+                                     ({"bwd_1b": 1, "cta": 128}, 24),
+                                     ({"bwd_1b": 1, "cta": 192}, 128),
+                                     ({"bwd_bulk": 1, "cta": 128}, 24),
+                                     ({"bwd_bulk": 1, "cta": 192}, 128),
+                                     ({"bwd_bulk": 1, "bwd_1b": 1, "cta": 192}, 24)])
+def test_backward_variants_match_ring_and_oracle(cuda_device, opts, xr):
+    """Variants of the backward RTM step against the one-column ring kernel and the FP64 oracle,
+    random boundary: the warp-specialised step (k_bwd_ws: the source field and the adjoint field
+    on separate warps of one CTA, strains handed over in shared memory for the imaging
+    condition), the ring kernel with one barrier per row step (bwd_1b) and the ring fed by bulk
+    copies (k_bwd_bulk, with either barrier count).  The 320-deep grid gives every CTA width two
+    or more z-strips; xr 24 gives each shot several row blocks."""
     c, _, _, w, _ = small_case(nt=200)
     c["allnz"] = 300
     vp, vs = synth.layered(c["allnx"], c["allnz"], seed=4)
@@ -642,15 +650,16 @@ def test_ws_backward_matches_ring_and_oracle(cuda_device, kt, xr):
         oz, ox = e.forward(shots)
     vpm, vsm = synth.smooth(vp, 3.0), synth.smooth(vs, 3.0)
     out = {}
-    for ws in (0, kt):
+    for var in (0, 1):
         with _ctx(c, shots, boundary="random", seed=5) as e:
             e.set_option("pair", 0)
             e.set_option("xr", xr)
-            e.set_option("bwd_ws", ws)
+            for k, v in (opts if var else {}).items():
+                e.set_option(k, v)
             e.set_models(vpm, vsm)
             e.set_wavelet(w)
             e.rtm(shots, oz, ox)
-            out[ws] = e.read_images()
+            out[var] = e.read_images()
     st = po.Setup(c["allnx"], c["allnz"], c["nx"], c["pml"], c["dx"], c["dz"], c["dt"])
     ntr = shots[0].ntr
     tot64 = np.zeros((3, c["allnx"], c["allnz"]))
@@ -663,9 +672,9 @@ def test_ws_backward_matches_ring_and_oracle(cuda_device, kt, xr):
             for k in range(3):
                 tot[k] += po.place(o[k], c["allnx"], c["allnz"], s.win_left)
     for k, key in enumerate(("pp_grad", "ps_grad", "illumination")):
-        assert np.abs(out[kt][key]).max() > 0
+        assert np.abs(out[1][key]).max() > 0
         floor = rel(tot32[k], tot64[k])
-        err_ring = rel(out[kt][key], out[0][key])
-        err64 = rel(out[kt][key], tot64[k])
+        err_ring = rel(out[1][key], out[0][key])
+        err64 = rel(out[1][key], tot64[k])
         assert err_ring < gate(floor), (key, err_ring, f"FP32 floor {floor:.3e}")
         assert err64 < gate(floor), (key, err64, f"FP32 floor {floor:.3e}")
