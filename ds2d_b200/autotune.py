@@ -21,7 +21,7 @@ import numpy as np
 from .api import Elastic2D
 
 _RING_BASE = {"pair": 0, "pair_split": 0, "pair_cta": 0, "pair_fcta": 0, "pair_xr": 0, "tb": 0,
-              "tb_cta": 0, "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0}
+              "tb_cta": 0, "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0}  # every knob named
 _RING_SPACE = [
     {"ring": 4, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 0, "cta": 192},
     {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 192},

@@ -280,7 +280,7 @@ struct ds2d_ctx {
   // Warp-specialised backward step (ds2d_bwdws.cuh, random boundary): option "bwd_ws" = threads
   // per role (0 off, 96, 128 or 192; a CTA holds both roles).
   int opt_bwd_ws = 0;
-  int opt_bwd_1b = 0;        // option "bwd_1b": one barrier per row step in k_bwd_ring (random boundary)
+  int opt_bwd_1b = 1;        // option "bwd_1b": one barrier per row step in k_bwd_ring (random boundary)
   int opt_bwd_bulk = 0;      // option "bwd_bulk": k_bwd_bulk, operand rows by bulk copy (random boundary)
   int occ_bulk[4] = {};      // resident CTAs per SM of k_bwd_bulk: [128 / 192 threads][one barrier]
   int occ_ws[3] = {};        // resident CTAs per SM of k_bwd_ws, 96 / 128 / 192 threads per role

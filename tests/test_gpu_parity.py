@@ -654,6 +654,7 @@ def test_backward_variants_match_ring_and_oracle(cuda_device, opts, xr):
         with _ctx(c, shots, boundary="random", seed=5) as e:
             e.set_option("pair", 0)
             e.set_option("xr", xr)
+            e.set_option("bwd_1b", 0)  # the two-barrier ring kernel as the reference
             for k, v in (opts if var else {}).items():
                 e.set_option(k, v)
             e.set_models(vpm, vsm)
