@@ -3,15 +3,16 @@
 // The one-column backward step executes most of its instructions on per-row work rather than on
 // the stencils: every thread issues its own 18 cp.async copies a row step (addresses, range
 // predicates, zero stores for rows outside the window) and waits on its own commit groups.  Here
-// the lanes of one warp issue one cp.async.bulk per field row for the whole CTA (global ->
-// shared, completion counted on the ring slot's mbarrier, the issuing warp rotating over the CTA
-// step by step), as the pair kernels of ds2d_pair.cuh do, and every thread waits on the slot's
-// phase (bounded by device time; a wait that gives up raises the error word and the CTA leaves the
+// one cp.async.bulk per field row copies it for the whole CTA (global -> shared, completion
+// counted on the ring slot's mbarrier), as in the pair kernels of ds2d_pair.cuh, and every
+// thread waits on the slot's phase (bounded by device time; a wait that gives up raises the error word and the CTA leaves the
 // march together).  The ring layout, the stages and the arithmetic are k_bwd_ring's, expression
 // for expression; rows outside the window are skipped rather than zeroed, because no update
 // reads them (the stencils of updated rows stay inside the grid, and imaging rows inside the
 // interior).  kOne: one barrier per row step (all eight z-tap rows published at the top of the
-// step, into one of two buffers), as k_bwd_ring's kOne.
+// step, into one of two buffers), as k_bwd_ring's kOne.  The copies of a slot are spread over
+// all warps of the CTA (warp w issues the fields f with f mod W = w, W warps; every warp arrives
+// on the slot's barrier with its own bytes), so no warp carries a step's whole copy issue.
 //
 // z-strips: a CTA's columns [zs - 8, zs - 8 + kT) start on a 16-byte boundary, so the strips'
 // width tz is a multiple of 4 (copies are clipped to the row's allocation [0, ld)).
@@ -26,10 +27,10 @@ __host__ __device__ constexpr size_t bwd_bulk_smem(int kT) {
   return sizeof(float) * (size_t)kBulkRing * kBwdBulkFields * kT + 8 * kBulkRing;
 }
 
-// Copies of one ring slot for one-column CTAs: lane f (f < NF) owns ring field f (row q - lag of
-// its array if that row lies in [lo, hi)); strip columns [zs - 8, zs - 8 + kT) map to ring floats
-// 0 .. kT, clipped to [0, ld).  Lane 0 arrives on the slot's barrier with the bytes of all the
-// copies before any is issued.
+// Copies of one ring slot for one-column CTAs, by one warp: its lane owning ring field f (row
+// q - lag of its array if that row lies in [lo, hi)) copies it; strip columns
+// [zs - 8, zs - 8 + kT) map to ring floats 0 .. kT, clipped to [0, ld).  Lane 0 arrives on the
+// slot's barrier with the bytes of the warp's copies before any is issued.
 template <int kT>
 __device__ __forceinline__ void issue_slot_col(const RingField &fd, float *slot_base, int f,
                                                unsigned long long *bar, int q, int ld, int zs,
@@ -78,9 +79,11 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
   const int img_row = s * d.wnx_max;  // image row of model row r: img_row + r - pml
   float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
 
-  // ring field of this lane (the issuing warp's lane f owns field f); the per-slot images share
-  // the wavefields' row stride (ild == ld), model row x at image row x - pml
+  // ring field of this lane: warp w, lane l owns field f = w + W l (W warps); the per-slot images
+  // share the wavefields' row stride (ild == ld), model row x at image row x - pml
+  constexpr int W = kT / 32;
   const int lane = t & 31;
+  const int my_f = (t >> 5) + W * lane;
   RingField fd{nullptr, 0, 0, d.nxp};
   {
     const long long fbase = d.slot * s;
@@ -90,7 +93,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
                             a.p.kpp,  a.p.kps,  img_pp,   img_ps,   a.p.b,    img_il};
 #pragma unroll
     for (int f = 0; f < NF; f++)
-      if (lane == f) {
+      if (my_f == f) {
         const bool img = f == 14 || f == 15 || f == 17;
         fd.src = src[f] + (img ? ibase : fbase);
         fd.lag = f < 4 ? 0 : (f < 16 ? 4 : 8);
@@ -99,7 +102,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
       }
   }
   if (t == 0) {
-    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], W);  // one arrival per warp and phase
     mbar_fence_init();
   }
   if (rec_col) {  // trace indexes of the first 16 rows, residuals of the first 8 (direct loads)
@@ -115,9 +118,8 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
   }
   __syncthreads();
   const int rs0 = x0 - 8;
-  if (t < 32)
-    for (int j = 0; j < kD - 1; j++)
-      issue_slot_col<kT>(fd, ring + (size_t)j * NF * kT, lane, &bars[j], rs0 + j, ld, zs, lane);
+  for (int j = 0; j < kD - 1; j++)
+    issue_slot_col<kT>(fd, ring + (size_t)j * NF * kT, my_f, &bars[j], rs0 + j, ld, zs, lane);
 
   float w_bvx[9], w_bvz[9], w_avx[9], w_avz[9];
   // adjoint-velocity operands, as k_bwd_ring: PL = (l+2m) atxx + l atzz, PzLx = (l+2m) atzz + l atxx
@@ -129,7 +131,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
   for (int i = 0; i < 5; i++) w_btzz[i] = w_PzLx[i] = 0.f;
 
   RingCursor<kD> cur;
-  int iw = 0;  // warp that issues the copies of this step
   bool ok = true, aborted = false;
 #pragma unroll kRingUnrollBwd
   for (int r = rs0; r < x1 + 8; r++) {
@@ -194,9 +195,9 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
       break;
     }
     // every thread is done with the previous slot: refill it kD - 1 steps ahead
-    if ((t >> 5) == iw) {
+    {
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
-      issue_slot_col<kT>(fd, ring + (size_t)ps * NF * kT, lane, &bars[ps], r + kD - 1, ld, zs,
+      issue_slot_col<kT>(fd, ring + (size_t)ps * NF * kT, my_f, &bars[ps], r + kD - 1, ld, zs,
                          lane);
     }
     // ---- stage 1: stresses of row r1 = r - 4 -----------------------------------------------
@@ -309,7 +310,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
     }
     if (rec_col) cp_async_wait<7>();
     cur.advance();
-    if (++iw == kT / 32) iw = 0;
   }
   pair_exit<kD>(bars, cur, aborted, ok, a.err);
   cp_async_wait<0>();
