@@ -48,6 +48,8 @@ _WS_SPACE = ([{"tb": 2, "tb_cta": 0, "bwd_ws": kt} for kt in (96, 128, 192)] +
              [{"tb": 2, "tb_cta": 0, "bwd_1b": 1, "cta": cta} for cta in (128, 192)] +
              [{"pair": 2, "pair_fcta": 256, "bwd_1b": 1, "cta": cta} for cta in (128, 192)] +
              [{"tb": 2, "tb_cta": 0, "bwd_bulk": 1, "bwd_1b": one, "cta": cta}
+              for one in (0, 1) for cta in (128, 192)] +
+             [{"pair": 2, "pair_fcta": 256, "bwd_bulk": 1, "bwd_1b": one, "cta": cta}
               for one in (0, 1) for cta in (128, 192)])
 _RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0, "tb": 0, "tb_cta": 0, "bwd_ws": 0,
                   "bwd_1b": 0, "bwd_bulk": 0}

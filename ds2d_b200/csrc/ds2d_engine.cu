@@ -269,10 +269,9 @@ struct ds2d_ctx {
   int opt_cta = 0;           // threads per CTA of the ring kernels: 0 auto, 128 or 192
   bool ring_ok = true;       // batch arrays fit the ring kernels' 32-bit offsets
   // Pair-blocked bulk-copy kernels of the random-boundary RTM step (ds2d_pair.cuh): option
-  // "pair" (1 on where they apply, 0 off: the default until they beat the one-column kernels),
-  // "pair_cta" (backward CTA width: 0 auto, 256 or 160), "pair_xr" (rows per CTA: 0 = chosen to
-  // fill whole waves).
-  int opt_pair = 0, opt_pair_cta = 0, opt_pair_fcta = 0, opt_pair_xr = 0, opt_pair_split = 0;
+  // "pair" (2 forward only: the default; 1 forward and backward; 0 off), "pair_cta" (backward CTA
+  // width: 0 auto, 256 or 160), "pair_xr" (rows per CTA: 0 = chosen to fill whole waves).
+  int opt_pair = 2, opt_pair_cta = 0, opt_pair_fcta = 0, opt_pair_xr = 0, opt_pair_split = 0;
   int opt_ac_pair = 1, opt_ac_pair_cta = 0;  // acoustic steps on k_ac_pair / k_ac_rev_pair
   // Time-blocked forward launches (ds2d_tblock.cuh, random boundary): option "tb" = time steps
   // per launch (0 off, 1-4), "tb_cta" = threads per CTA (0 automatic, 256 or 512).
@@ -280,8 +279,9 @@ struct ds2d_ctx {
   // Warp-specialised backward step (ds2d_bwdws.cuh, random boundary): option "bwd_ws" = threads
   // per role (0 off, 96, 128 or 192; a CTA holds both roles).
   int opt_bwd_ws = 0;
-  int opt_bwd_1b = 1;        // option "bwd_1b": one barrier per row step in k_bwd_ring (random boundary)
-  int opt_bwd_bulk = 0;      // option "bwd_bulk": k_bwd_bulk, operand rows by bulk copy (random boundary)
+  int opt_bwd_1b = 0;        // option "bwd_1b": one barrier per row step in k_bwd_ring / k_bwd_bulk
+  int opt_bwd_bulk = 1;      // option "bwd_bulk": k_bwd_bulk, operand rows by bulk copy (random
+                             // boundary; the default, 0 = the per-thread cp.async ring of k_bwd_ring)
   int occ_bulk[4] = {};      // resident CTAs per SM of k_bwd_bulk: [128 / 192 threads][one barrier]
   int occ_ws[3] = {};        // resident CTAs per SM of k_bwd_ws, 96 / 128 / 192 threads per role
   int occ_tb[2][4] = {};     // resident CTAs per SM of k_fwd_tb, [256 / 512 threads][depth - 1]

@@ -11,9 +11,11 @@
 //    predicates, barrier) is paid once per two cells.
 //  * Rows arrive by bulk copy.  Each ring slot holds, for one row step, every row segment the
 //    step consumes (the newest stencil rows, the z-tap rows of stage 1 and the own-cell operands
-//    of both stages).  The lanes of warp 0 issue one cp.async.bulk per field row (global ->
-//    shared, completion counted on the slot's mbarrier) kD - 1 steps ahead; every thread then
-//    waits on the barrier's phase before it reads the slot.  Stage-1 z-taps are read straight from the ring, so a step has a
+//    of both stages).  One cp.async.bulk per field row (global -> shared, completion counted on
+//    the slot's mbarrier) fills it kD - 1 steps ahead; the copies are spread over all warps of
+//    the CTA (warp w issues the fields f with f mod W = w, and every warp arrives on the slot's
+//    barrier with its own bytes), so no warp carries a step's whole copy issue to the next
+//    barrier.  Every thread waits on the barrier's phase before it reads the slot.  Stage-1 z-taps are read straight from the ring, so a step has a
 //    single CTA barrier (before the stage-2 z-taps, whose rows are computed in registers).
 //  * Injections on the stencil values only.  The explosive source (forward) and the receiver
 //    residual (adjoint) act on the stencil values, not on the stored state (the reference adds
@@ -174,11 +176,11 @@ __device__ __forceinline__ void pair_exit(unsigned long long *bars, RingCursor<k
   }
 }
 
-// Copies of one ring slot, issued by the 32 lanes of one warp at once: lane f (f < NF) owns ring
-// field f, which reads row (q - lag) of an array whose rows are ld floats apart (wavefields,
-// parameters and the per-slot images alike) if that row lies in [lo, hi).  The strip's columns
-// [zs - 8, zs - 8 + 2 kT) map to ring floats 4 .. 2 kT + 4; the copy is clipped to [0, ld) (the
-// row's own allocation).  Lane 0 arrives on the slot's barrier with the bytes of all the copies
+// One warp's share of the copies of a ring slot: the lane owning ring field f reads row
+// (q - lag) of an array whose rows are ld floats apart (wavefields, parameters and the per-slot
+// images alike) if that row lies in [lo, hi).  The strip's columns [zs - 8, zs - 8 + 2 kT) map to
+// ring floats 4 .. 2 kT + 4; the copy is clipped to [0, ld) (the row's own allocation).  Lane 0
+// arrives on the slot's barrier (one arrival per warp) with the bytes of the warp's copies
 // (counted by ballot) before any is issued, so the phase cannot complete early.
 struct RingField {
   const float *src;  // this lane's field: array row x starts at src + x * ld (0 for lanes >= NF)
@@ -250,8 +252,11 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
   const int *rmap = a.rmap + (long long)s * d.nxp_max;
   const float dtdx = d.dt / d.dx, dtdz = d.dt / d.dz;
 
-  // ring field of this lane (warp 0 issues the copies; lane f owns field f)
+  // ring fields (the thread owning field f issues its row copies)
   const int lane = t & 31;
+  // ring field of this thread: warp w, lane l owns field w + W l (W warps), so every warp issues
+  // a share of a slot's copies
+  const int my_f = (t >> 5) + (kT / 32) * lane;
   RingField fd{nullptr, 0, 0, d.nxp};
   {
     const float *src[NF] = {a.a.txx, a.a.txz, a.a.txz, a.a.tzz, a.a.vx, a.a.vz,
@@ -259,20 +264,19 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
     const int lag[NF] = {0, 1, 4, 4, 4, 4, 4, 8, 8, 8, 8};
 #pragma unroll
     for (int f = 0; f < NF; f++)
-      if (lane == f) {
+      if (my_f == f) {
         fd.src = src[f] + fbase;
         fd.lag = lag[f];
       }
   }
   if (t == 0) {
-    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], kT / 32);  // one arrival per warp
     mbar_fence_init();
   }
   __syncthreads();
   const int rs0 = x0 - 8;
-  if (t < 32)
-    for (int j = 0; j < kD - 1; j++)
-      issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], rs0 + j, ld, zs, lane);
+  for (int j = 0; j < kD - 1; j++)
+    issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, my_f, &bars[j], rs0 + j, ld, zs, lane);
 
   float2 w_txx[8], w_txz[8], w_vx[9], w_vz[8];
 #pragma unroll
@@ -281,7 +285,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
   for (int i = 0; i < 9; i++) w_vx[i] = make_float2(0.f, 0.f);
 
   RingCursor<kD> cur;
-  int iw = 0;  // warp that issues the copies of this step
   bool ok = true, aborted = false;
 #pragma unroll 2
   for (int r = rs0; r < x1 + 8; r++) {
@@ -353,9 +356,9 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
       break;
     }
     // every thread is done with the previous slot: refill it kD - 1 steps ahead
-    if ((t >> 5) == iw) {  // the step's issuing warp (round robin spreads the extra work)
+    {  // every warp issues its share of the slot's copies
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
-      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps], r + kD - 1, ld, zs,
+      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, my_f, &bars[ps], r + kD - 1, ld, zs,
                           lane);
     }
     // ---- stage 2: stresses of row rs = r - 8 ------------------------------------------------
@@ -394,7 +397,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_pair(FwdFusedArgs a) {
     }
     if (rec_col) cp_async_wait<7>();
     cur.advance();
-    if (++iw == kT / 32) iw = 0;
   }
   pair_exit<kD>(bars, cur, aborted, ok, a.err);
   cp_async_wait<0>();
@@ -454,6 +456,9 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_pair(AcRingArgs a) {
   const bool born_out = kMode == 0 && a.e_out != nullptr;
 
   const int lane = t & 31;
+  // ring field of this thread: warp w, lane l owns field w + W l (W warps), so every warp issues
+  // a share of a slot's copies
+  const int my_f = (t >> 5) + (kT / 32) * lane;
   RingField fd{nullptr, 0, 0, d.nxp};
   {
     const float *src[NF] = {a.s, kMode == 1 ? a.e_in : nullptr, a.s, kMode == 1 ? a.e_in : nullptr,
@@ -461,20 +466,19 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_pair(AcRingArgs a) {
     const int lag[NF] = {0, 0, 4, 4, 4, 4, 4, 8, 8, 8};
 #pragma unroll
     for (int f = 0; f < NF; f++)
-      if (lane == f && src[f]) {
+      if (my_f == f && src[f]) {
         fd.src = src[f] + fbase;
         fd.lag = lag[f];
       }
   }
   if (t == 0) {
-    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], kT / 32);  // one arrival per warp
     mbar_fence_init();
   }
   __syncthreads();
   const int rs0 = x0 - 8;
-  if (t < 32)
-    for (int j = 0; j < kD - 1; j++)
-      issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], rs0 + j, ld, zs, lane);
+  for (int j = 0; j < kD - 1; j++)
+    issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, my_f, &bars[j], rs0 + j, ld, zs, lane);
 
   float2 w_S[8], w_vx[9], w_vz[8];
 #pragma unroll
@@ -483,7 +487,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_pair(AcRingArgs a) {
   for (int i = 0; i < 9; i++) w_vx[i] = make_float2(0.f, 0.f);
 
   RingCursor<kD> cur;
-  int iw = 0;  // warp that issues the copies of this step
   bool ok = true, aborted = false;
 #pragma unroll 2
   for (int r = rs0; r < x1 + 8; r++) {
@@ -550,9 +553,9 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_pair(AcRingArgs a) {
       aborted = true;
       break;
     }
-    if ((t >> 5) == iw) {  // the step's issuing warp (round robin spreads the extra work)
+    {  // every warp issues its share of the slot's copies
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
-      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps], r + kD - 1, ld, zs,
+      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, my_f, &bars[ps], r + kD - 1, ld, zs,
                           lane);
     }
     // ---- stage 2: stress of row rs = r - 8 --------------------------------------------------
@@ -578,7 +581,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_pair(AcRingArgs a) {
     }
     if (rec_col) cp_async_wait<7>();
     cur.advance();
-    if (++iw == kT / 32) iw = 0;
   }
   pair_exit<kD>(bars, cur, aborted, ok, a.err);
   cp_async_wait<0>();
@@ -651,6 +653,9 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_rev_pair(AcRevArgs a) {
   const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
 
   const int lane = t & 31;
+  // ring field of this thread: warp w, lane l owns field w + W l (W warps), so every warp issues
+  // a share of a slot's copies
+  const int my_f = (t >> 5) + (kT / 32) * lane;
   RingField fd{nullptr, 0, 0, d.nxp};
   {
     const float *src[NF] = {a.ys, a.lam, a.ys, a.lam, a.yx, a.yz, a.b, a.vx,
@@ -658,7 +663,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_rev_pair(AcRevArgs a) {
     const int lag[NF] = {0, 0, 4, 4, 4, 4, 4, 4, 4, 8, 8, 8, 8, 8, 12};
 #pragma unroll
     for (int f = 0; f < NF; f++)
-      if (lane == f) {
+      if (my_f == f) {
         // gradient rows: grid row x is image row x - pml of the slot's plane
         fd.src = f == 13 ? src[f] + ibase - (long long)pml * ld : src[f] + fbase;
         fd.lag = lag[f];
@@ -668,7 +673,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_rev_pair(AcRevArgs a) {
   }
   const int r_first = x0 - 10, r_last = x1 + 12;
   if (t == 0) {
-    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], kT / 32);  // one arrival per warp
     mbar_fence_init();
   }
   if (rec_col) {  // stage-A rows r_first-4 ..: residuals of the first 8 rows and trace indexes
@@ -685,9 +690,8 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_rev_pair(AcRevArgs a) {
     for (int q = a0 + 8; q < a0 + 16; q++) s_tr[q & 15] = (q >= 0 && q < d.nxp) ? rmap[q] : -1;
   }
   __syncthreads();
-  if (t < 32)
-    for (int j = 0; j < kD - 1; j++)
-      issue_slot_warp<kT, kAcRevHalo>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], r_first + j,
+  for (int j = 0; j < kD - 1; j++)
+    issue_slot_warp<kT, kAcRevHalo>(fd, ring + (size_t)j * NF * ROW, my_f, &bars[j], r_first + j,
                                       ld, zs, lane);
 
   const float2 zero2 = make_float2(0.f, 0.f);
@@ -698,7 +702,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_rev_pair(AcRevArgs a) {
   for (int i = 0; i < 9; i++) w_ux[i] = w_bvx[i] = w_bvz[i] = zero2;
 
   RingCursor<kD> cur;
-  int iw = 0;  // warp that issues the copies of this step
   bool ok = true, aborted = false;
   for (int r = r_first; r < r_last; r++) {
     ok = mbar_wait(&bars[cur.slot], cur.phase);
@@ -837,14 +840,13 @@ __global__ void __launch_bounds__(kT, kMinB) k_ac_rev_pair(AcRevArgs a) {
       aborted = true;
       break;
     }
-    if ((t >> 5) == iw) {  // the step's issuing warp (round robin spreads the extra work)
+    {  // every warp issues its share of the slot's copies
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
-      issue_slot_warp<kT, kAcRevHalo>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps],
+      issue_slot_warp<kT, kAcRevHalo>(fd, ring + (size_t)ps * NF * ROW, my_f, &bars[ps],
                                       r + kD - 1, ld, zs, lane);
     }
     if (rec_col) cp_async_wait<7>();
     cur.advance();
-    if (++iw == kT / 32) iw = 0;
   }
   pair_exit<kD>(bars, cur, aborted, ok, a.err);
   cp_async_wait<0>();
@@ -944,8 +946,11 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   const float rdx = 1.0f / d.dx, rdz = 1.0f / d.dz;
   float *img_pp = a.img, *img_ps = a.img + a.img_plane, *img_il = a.img + 2 * a.img_plane;
 
-  // ring field of this lane (warp 0 issues the copies; lane f owns field f)
+  // ring fields (the thread owning field f issues its row copies)
   const int lane = t & 31;
+  // ring field of this thread: warp w, lane l owns field w + W l (W warps), so every warp issues
+  // a share of a slot's copies
+  const int my_f = (t >> 5) + (kT / 32) * lane;
   RingField fd{nullptr, 0, 0, d.nxp};
   {
     struct Src {
@@ -969,7 +974,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
                          {L::IL8, img_il, 8, true}};
 #pragma unroll
     for (int q = 0; q < 25; q++)
-      if (tab[q].f >= 0 && lane == tab[q].f) {
+      if (tab[q].f >= 0 && my_f == tab[q].f) {
         // image rows: grid row x is image row x - pml of the slot's plane
         fd.src = tab[q].img ? tab[q].p + ibase - (long long)pml * ld : tab[q].p + fbase;
         fd.lag = tab[q].lag;
@@ -978,7 +983,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
       }
   }
   if (t == 0) {
-    for (int k = 0; k < kD; k++) mbar_init(&bars[k], 1);
+    for (int k = 0; k < kD; k++) mbar_init(&bars[k], kT / 32);  // one arrival per warp
     mbar_fence_init();
   }
   if (rec_col) {  // residuals of rows x0-9 .. x0-1 and trace indexes of rows x0 .. x0+7 (direct;
@@ -995,9 +1000,8 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   }
   __syncthreads();
   const int rs0 = x0 - 8;
-  if (t < 32)
-    for (int j = 0; j < kD - 1; j++)
-      issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, lane, &bars[j], rs0 + j, ld, zs, lane);
+  for (int j = 0; j < kD - 1; j++)
+    issue_slot_warp<kT>(fd, ring + (size_t)j * NF * ROW, my_f, &bars[j], rs0 + j, ld, zs, lane);
 
   const float2 zero2 = make_float2(0.f, 0.f);
   float2 w_bvx[8], w_bvz[8];               // stage-1 x-windows (strains / reconstruction)
@@ -1022,7 +1026,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
   int zw = ((rs0 - 4) % kBwdPairZDepth + kBwdPairZDepth) % kBwdPairZDepth;
 
   RingCursor<kD> cur;
-  int iw = 0;  // warp that issues the copies of this step
   bool ok = true, aborted = false;
   // Two row steps per loop iteration let the compiler rename half of the window shifts away
   // where the registers allow it (the split parts); the fused pass is at its register limit.
@@ -1207,9 +1210,9 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
       aborted = true;
       break;
     }
-    if ((t >> 5) == iw) {  // the step's issuing warp (round robin spreads the extra work)
+    {  // every warp issues its share of the slot's copies
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
-      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, lane, &bars[ps], r + kD - 1, ld, zs,
+      issue_slot_warp<kT>(fd, ring + (size_t)ps * NF * ROW, my_f, &bars[ps], r + kD - 1, ld, zs,
                           lane);
     }
     // ---- stage 2: velocities of row r2 = r - 8, illumination ---------------------------------
@@ -1271,7 +1274,6 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_pair(BwdFusedArgs a) {
     }
     if (rec_col) cp_async_wait<6>();
     cur.advance();
-    if (++iw == kT / 32) iw = 0;
   }
   pair_exit<kD>(bars, cur, aborted, ok, a.err);
   cp_async_wait<0>();

@@ -216,7 +216,7 @@ int ds2d_bandpass_filter_device(int nx, int nz, int x1, int x2, int z1, int z2, 
  * "adjoint_born" (see ds2d_elsrtm), "pcg_switch" and "pcg_m" (1..15, see ds2d_lsrtm_pcg).
  * Pair-blocked bulk-copy kernels (random boundary; two z-columns per thread, rows fed by
  * cp.async.bulk into an mbarrier ring): "pair" (0 off, 1 forward and backward RTM steps, 2 the
- * forward step only), "pair_fcta" (forward CTA width 64 / 256, 0 = 256), "pair_cta" (backward
+ * forward step only: the default), "pair_fcta" (forward CTA width 64 / 256, 0 = 256), "pair_cta" (backward
  * 64 / 160 / 256, 0 = 64), "pair_split" (0 / 1: backward in one or two launches), "pair_xr" (rows
  * per CTA, 0 = the count that fills the SMs' waves best), "ac_pair" (0 / 1: acoustic forward
  * steps of the Born pair on k_ac_pair) and "ac_pair_cta" (128 / 192 / 256, 0 = the width with the
@@ -224,7 +224,11 @@ int ds2d_bandpass_filter_device(int nx, int nz, int x1, int x2, int z1, int z2, 
  * the whole background state every K steps, in the strip precision with one FP32 scale per field,
  * shot and snapshot, and replay each K-step segment from its snapshot with strips before
  * reversing it: snapshots plus K steps of strips instead of nt steps of strips, for one more
- * forward propagation per L^T. */
+ * forward propagation per L^T.  Random-boundary RTM steps: "tb" (K = 1-4 forward time steps
+ * per launch, 0 = off: the default), "tb_cta" (256 / 512, 0 = automatic); the backward step
+ * "bwd_bulk" (1 = operand rows by bulk copy, the copy issue spread over all warps: the default;
+ * 0 = per-thread cp.async), "bwd_1b" (0 / 1: one barrier per row step), "bwd_ws" (0 off, or
+ * 96 / 128 / 192 threads per role of the warp-specialised step). */
 int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
 
 /* Profiling (no counterpart in the reference, which has only a commented-out host timer,

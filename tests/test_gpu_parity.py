@@ -628,8 +628,8 @@ def test_live_reference_elsrtm_full_size(cuda_device):
 
 @pytest.mark.parametrize("opts,xr", [({"bwd_ws": 96}, 128), ({"bwd_ws": 128}, 24),
                                      ({"bwd_ws": 192}, 24), ({"bwd_ws": 192}, 128),
-                                     ({"bwd_1b": 1, "cta": 128}, 24),
                                      ({"bwd_1b": 1, "cta": 192}, 128),
+                                     ({"bwd_1b": 1, "bwd_bulk": 0, "cta": 128}, 24),
                                      ({"bwd_bulk": 1, "cta": 128}, 24),
                                      ({"bwd_bulk": 1, "cta": 192}, 128),
                                      ({"bwd_bulk": 1, "bwd_1b": 1, "cta": 192}, 24)])
@@ -654,7 +654,8 @@ def test_backward_variants_match_ring_and_oracle(cuda_device, opts, xr):
         with _ctx(c, shots, boundary="random", seed=5) as e:
             e.set_option("pair", 0)
             e.set_option("xr", xr)
-            e.set_option("bwd_1b", 0)  # the two-barrier ring kernel as the reference
+            e.set_option("bwd_1b", 0)  # the two-barrier per-thread ring kernel as the reference
+            e.set_option("bwd_bulk", 0)
             for k, v in (opts if var else {}).items():
                 e.set_option(k, v)
             e.set_models(vpm, vsm)
