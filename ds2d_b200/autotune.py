@@ -8,7 +8,8 @@ one-column ring kernels, and, for the random boundary, the pair-blocked bulk-cop
 (`pair_xr`) and the backward step fused or split in two launches (`pair_split`); `pair` 2
 takes the pair kernel for the forward step only, with the backward on the one-column kernel.
 The forward step can also run time-blocked (`tb` = time steps per launch, 1-4, `tb_cta` = its
-CTA width): one launch advances the batch by `tb` steps, reading and writing the state once.
+CTA width, `tb_bulk` = operand rows by bulk copy at depth 1-2): one launch advances the batch by
+`tb` steps, reading and writing the state once.
 The backward step can run warp-specialised (`bwd_ws` = threads per role, 96 / 128 / 192: the
 source and adjoint wavefields on separate warps of one CTA), with one barrier per row step
 (`bwd_1b`), and with its operand rows fed by bulk copies (`bwd_bulk`).
@@ -21,7 +22,7 @@ import numpy as np
 from .api import Elastic2D
 
 _RING_BASE = {"pair": 0, "pair_split": 0, "pair_cta": 0, "pair_fcta": 0, "pair_xr": 0, "tb": 0,
-              "tb_cta": 0, "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0}  # every knob named
+              "tb_cta": 0, "tb_bulk": 1, "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0}  # every knob named
 _RING_SPACE = [
     {"ring": 4, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 0, "cta": 192},
     {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 192},
@@ -39,7 +40,8 @@ _PAIR_SPACE = ([{"pair": 2, "pair_split": 0, "pair_cta": 0, "pair_fcta": fcta, "
 # Time-blocked forward (random boundary only): depth 1-4 at the automatic CTA width, and the
 # 512-thread single-strip CTAs at depth 1-2; the backward on the one-column ring kernel.
 _TB_SPACE = ([{"tb": k, "tb_cta": 0, "cta": 192} for k in (1, 2, 3, 4)] +
-             [{"tb": k, "tb_cta": 512, "cta": 192} for k in (1, 2)])
+             [{"tb": k, "tb_cta": 512, "cta": 192} for k in (1, 2)] +
+             [{"tb": 2, "tb_cta": 0, "tb_bulk": 0, "cta": 192}])
 # Backward variants (random boundary only) behind the two best forward kernels: warp-specialised
 # (`bwd_ws` threads per role), the ring kernel with one barrier per row step (`bwd_1b`), and the
 # ring fed by bulk copies (`bwd_bulk`, with either barrier count).
@@ -49,10 +51,11 @@ _WS_SPACE = ([{"tb": 2, "tb_cta": 0, "bwd_ws": kt} for kt in (96, 128, 192)] +
              [{"pair": 2, "pair_fcta": 256, "bwd_1b": 1, "cta": cta} for cta in (128, 192)] +
              [{"tb": 2, "tb_cta": 0, "bwd_bulk": 1, "bwd_1b": one, "cta": cta}
               for one in (0, 1) for cta in (128, 192)] +
+             [{"tb": k, "tb_cta": tc, "bwd_bulk": 1, "cta": 192} for k in (1, 2) for tc in (256, 512)] +
              [{"pair": 2, "pair_fcta": 256, "bwd_bulk": 1, "bwd_1b": one, "cta": cta}
               for one in (0, 1) for cta in (128, 192)])
-_RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0, "tb": 0, "tb_cta": 0, "bwd_ws": 0,
-                  "bwd_1b": 0, "bwd_bulk": 0}
+_RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0, "tb": 0, "tb_cta": 0, "tb_bulk": 1,
+                  "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0}
 
 
 def default_space(boundary="random"):

@@ -274,8 +274,10 @@ struct ds2d_ctx {
   int opt_pair = 2, opt_pair_cta = 0, opt_pair_fcta = 0, opt_pair_xr = 0, opt_pair_split = 0;
   int opt_ac_pair = 1, opt_ac_pair_cta = 0;  // acoustic steps on k_ac_pair / k_ac_rev_pair
   // Time-blocked forward launches (ds2d_tblock.cuh, random boundary): option "tb" = time steps
-  // per launch (0 off, 1-4), "tb_cta" = threads per CTA (0 automatic, 256 or 512).
-  int opt_tb = 0, opt_tb_cta = 0;
+  // per launch (0 off, 1-4; default 2), "tb_cta" = threads per CTA (0 automatic, 256 or 512).
+  int opt_tb = 2, opt_tb_cta = 0;
+  int opt_tb_bulk = 1;       // option "tb_bulk": depth 1-2 rows by bulk copy (0 = per-thread cp.async)
+  int occ_tb_bulk[2][2] = {};  // resident CTAs per SM of k_fwd_tb with bulk copies [256 / 512][depth - 1]
   // Warp-specialised backward step (ds2d_bwdws.cuh, random boundary): option "bwd_ws" = threads
   // per role (0 off, 96, 128 or 192; a CTA holds both roles).
   int opt_bwd_ws = 0;
@@ -771,7 +773,11 @@ TbFn tb_fn_t(int depth) {
     default: return k_fwd_tb<4, kT, 1>;
   }
 }
-TbFn tb_fn(int depth, int cta) {
+TbFn tb_fn(int depth, int cta, bool bulk = false) {
+  if (bulk && depth <= 2) {  // operand rows by bulk copy (depth 1-2)
+    if (cta == 512) return depth == 1 ? k_fwd_tb<1, 512, 1, true> : k_fwd_tb<2, 512, 1, true>;
+    return depth == 1 ? k_fwd_tb<1, 256, 3, true> : k_fwd_tb<2, 256, 2, true>;
+  }
   if (cta == 512) return depth == 1 ? k_fwd_tb<1, 512, 1> : k_fwd_tb<2, 512, 1>;
   return tb_fn_t<256>(depth);
 }
@@ -782,7 +788,8 @@ int tb_idx(int cta) { return cta == 512 ? 1 : 0; }
 bool tb_split(const Dims &d, int kT, int K, int *nstrips, int *tz) {
   const int H = 8 * K;
   for (int ns = 1; ns <= 64; ns++) {
-    const int t = (d.nzp + ns - 1) / ns;
+    // several strips: widths a multiple of 4, so every strip starts on a 16-byte boundary
+    const int t = ns == 1 ? d.nzp : ((d.nzp + ns - 1) / ns + 3) / 4 * 4;
     const int cap = ns == 1 ? kT : ns == 2 ? kT - H : kT - 2 * H;
     if (t <= cap) {
       *nstrips = ns;
@@ -939,10 +946,13 @@ int run_forward_fused(ds2d_ctx *c, int n, bool record, bool strips) {
       const int txr = tb_xr(c, ns, c->occ_tb[tb_idx(tc)][K - 1], K);
       FwdFusedArgs a{};
       a.d = d; a.a = *cur; a.b = *nxt; a.p = c->par; a.shots = c->d_shots; a.wavelet = c->wavelet;
-      a.it = it; a.tz = tz; a.xr = txr; a.rmap = c->d_rmap;
+      a.it = it; a.tz = tz; a.xr = txr; a.rmap = c->d_rmap; a.err = c->d_err;
       if (record) { a.rec_on = 1; a.rec_vz = c->rec[0]; a.rec_vx = c->rec[1]; }
       dim3 tgrid(ns, (d.nxp + txr - 1) / txr, n);
-      LAUNCHS("fwd_tb", kBytesFused * CELLS(n), tb_fn(K, tc), tgrid, tc, tb_smem(K, tc, txr), a);
+      const bool bulk = c->opt_tb_bulk && K <= 2 && c->d_err && d.ild == d.ld &&
+                        c->occ_tb_bulk[tb_idx(tc)][K - 1] > 0;
+      LAUNCHS("fwd_tb", kBytesFused * CELLS(n), tb_fn(K, tc, bulk), tgrid, tc, tb_smem(K, tc, txr),
+              a);
       std::swap(cur, nxt);
       it += K;
     }
@@ -1095,7 +1105,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk), (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk + 32 * c->opt_tb_bulk), (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -2029,6 +2039,12 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
         if (e == cudaSuccess)
           e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_tb[i][K - 1], tb_fn(K, cta),
                                                             cta, sm);
+        if (K <= 2 && e == cudaSuccess)
+          e = cudaFuncSetAttribute(tb_fn(K, cta, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sm);
+        if (K <= 2 && e == cudaSuccess)
+          e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->occ_tb_bulk[i][K - 1],
+                                                            tb_fn(K, cta, true), cta, sm);
       }
     int dev = 0;
     if (e == cudaSuccess) e = cudaGetDevice(&dev);
@@ -2162,7 +2178,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk), (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk + 32 * c->opt_tb_bulk), (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -2639,6 +2655,9 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
     if (value != 0 && value != 96 && value != 128 && value != 192)
       return fail(c, DS2D_E_ARG, "bwd_ws must be 0 (off) or 96, 128, 192 threads per role");
     c->opt_bwd_ws = (int)value;
+  } else if (k == "tb_bulk") {
+    if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "tb_bulk must be 0 or 1");
+    c->opt_tb_bulk = (int)value;
   } else if (k == "tb_cta") {
     if (value != 0 && value != 256 && value != 512)
       return fail(c, DS2D_E_ARG, "tb_cta must be 0 (automatic), 256 or 512 (depth 1-2)");

@@ -24,13 +24,21 @@
 // columns beyond are zero), so a kT-thread CTA owns up to kT - 16 kK columns (kT - 8 kK at an
 // edge, kT when one strip covers the whole depth).
 //
+// kBulk: the operand rows arrive by bulk copy instead of per-thread cp.async -- one
+// cp.async.bulk per field row for the whole CTA into the same ring layout, the copies of a slot
+// spread over all warps (warp w issues the fields f with f mod W = w and arrives on the slot's
+// mbarrier with its own bytes), every thread waiting (bounded) on the slot's phase, the slot of
+// step r - 1 refilled after the step's barrier.  Rows outside the window are skipped, not
+// zeroed: no updated row reads them.  A strip's first column is then a multiple of 4 (16-byte
+// aligned copy rows).
+//
 // Injections are the one-step kernels': the explosive source of time t + k (FD2DGPU.cu:2039-2049)
 // is added to the stress values that enter V_k (window entry and z-tap copy); the injected cell
 // keeps its un-injected stresses in registers for S_k.  Receivers record the V_k output of rows
 // and columns the CTA owns at time index it + k.  Results are bit-identical to kK launches of
 // k_fwd_ring.
 #pragma once
-#include "ds2d_fused.cuh"
+#include "ds2d_pair.cuh"
 
 namespace ds2d {
 
@@ -44,7 +52,26 @@ __host__ __device__ constexpr int tb_row(int kT) { return kT + 2 * kTbPad; }
 // CTA's rows (xr ints).
 __host__ __device__ constexpr size_t tb_smem(int K, int kT, int xr) {
   return sizeof(float) * ((size_t)kTbRing * tb_fields(K) * kT + 2 * 4 * K * tb_row(kT)) +
-         sizeof(int) * (size_t)xr;
+         (sizeof(int) * (size_t)xr + 7) / 8 * 8 + 8 * kTbRing;  // + the slot barriers (kBulk)
+}
+
+// One warp's share of the bulk copies of a ring slot: the lane owning ring field f copies row
+// q - lag of its array (if that row lies in [lo, hi)) over the strip columns [c0, c0 + kT),
+// clipped to the row's allocation [0, ld), into ring floats 0 .. kT; lane 0 arrives on the
+// slot's barrier with the bytes of the warp's copies first.
+template <int kT>
+__device__ __forceinline__ void tb_issue_warp(const RingField &fd, float *slot_base, int f,
+                                              unsigned long long *bar, int q, int ld, int c0,
+                                              int lane) {
+  const int glo = max(0, c0), ghi = min(ld, c0 + kT);
+  const unsigned bytes = (unsigned)(ghi - glo) * 4u;
+  const int row = q - fd.lag;
+  const bool mine = fd.src != nullptr && row >= fd.lo && row < fd.hi;
+  const unsigned n = __popc(__ballot_sync(0xffffffffu, mine));
+  if (lane == 0) mbar_arrive_tx(bar, n * bytes);
+  __syncwarp();
+  if (mine)
+    bulk_g2s(slot_base + f * kT + (glo - c0), fd.src + (long long)row * ld + glo, bytes, bar);
 }
 
 template <int K>
@@ -53,7 +80,7 @@ struct TbWin {
   float vx[K][9], vz[K][9];               // V_k outputs entering S_k
 };
 
-template <int kK, int kT, int kMinB>
+template <int kK, int kT, int kMinB, bool kBulk = false>
 __global__ void __launch_bounds__(kT, kMinB) k_fwd_tb(FwdFusedArgs a) {
   constexpr int kD = kTbRing, NF = tb_fields(kK), ROW = tb_row(kT);
   constexpr int H = 8 * kK;  // halo columns at an inner strip edge, halo rows at each x end
@@ -61,11 +88,14 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_tb(FwdFusedArgs a) {
   float *ring = smem;                          // [kD][NF][kT]
   float *ztap = ring + (size_t)kD * NF * kT;   // [2][4 kK][ROW]
   int *s_tr = (int *)(ztap + 2 * 4 * kK * ROW);  // [xr] trace index of row x0 + i, or -1
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(  // [kD] slot barriers (kBulk)
+      (char *)smem + ((size_t)((char *)(s_tr + a.xr) - (char *)smem) + 7) / 8 * 8);
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int zs = blockIdx.x * a.tz, ze = min(zs + a.tz, d.nzp);
   const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
   if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
+  if (kBulk && __syncthreads_or(t == 0 && pair_err_raised(a.err))) return;  // whole CTA
   const int hl = zs > 0 ? H : 0;
   const int z = zs - hl + t;
   const int base = (int)(d.slot * s);  // cell offsets fit 32 bits (checked on the host)
@@ -114,6 +144,27 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_tb(FwdFusedArgs a) {
     }
     cp_async_commit();
   };
+  // kBulk: ring field of this thread (warp w, lane l owns field w + W l) and the slot barriers
+  const int lane = t & 31;
+  const int my_f = (t >> 5) + (kT / 32) * lane;
+  RingField fd{nullptr, 0, 0, d.nxp};
+  if (kBulk) {
+    const long long fbase = d.slot * s;
+#pragma unroll
+    for (int f = 0; f < NF; f++)
+      if (my_f == f) {
+        const float *src = f == 0 ? a.a.txx : f == 1 ? a.a.tzz : f == 2 ? a.a.txz
+                         : f == 3 ? a.a.vx : f == 4 ? a.a.vz
+                         : f < 5 + kK ? a.p.b : ((f - 5 - kK) & 1) ? a.p.mu : a.p.lam;
+        fd.src = src + fbase;
+        fd.lag = f < 3 ? 0 : f < 5 ? 4 : f < 5 + kK ? 4 + 8 * (f - 5) : 8 + 8 * ((f - 5 - kK) >> 1);
+      }
+    if (t == 0) {
+      for (int k = 0; k < kD; k++) mbar_init(&bars[k], kT / 32);  // one arrival per warp
+      mbar_fence_init();
+    }
+  }
+  const int c0 = zs - hl;  // first column of the CTA (a multiple of 4 with kBulk)
 
   // trace indexes of the CTA's own rows (receiver column only reads them; everyone copies)
   if (a.rec_on) {
@@ -142,16 +193,28 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_tb(FwdFusedArgs a) {
   __syncthreads();
 
   const int r_begin = x0 - H, r_end = x1 + H;
+  if (kBulk) {
+    for (int j = 0; j < kD - 1; j++)
+      tb_issue_warp<kT>(fd, ring + (size_t)j * NF * kT, my_f, &bars[j], r_begin + j, ld, c0, lane);
+  } else {
 #pragma unroll
-  for (int j = 0; j < kD - 1; j++) issue(r_begin + j);
+    for (int j = 0; j < kD - 1; j++) issue(r_begin + j);
+  }
+  RingCursor<kD> cur;  // kBulk: slot and phase of the step being consumed
+  bool ok = true, aborted = false;
   // two row steps per iteration let the compiler rename half of the window shifts away
   constexpr int kUnroll = kK <= 2 ? 2 : 1;
 #pragma unroll kUnroll
   for (int r = r_begin; r < r_end; r++) {
-    cp_async_wait<kD - 2>();  // row step r has landed (this thread's copies)
+    // row step r has landed: this thread's copies, or (kBulk) the slot's phase, bounded
+    if (kBulk)
+      ok = mbar_wait(&bars[cur.slot], cur.phase);
+    else
+      cp_async_wait<kD - 2>();
+    const float *S = ring + (size_t)(kBulk ? cur.slot : (r & (kD - 1))) * NF * kT + t;
     {
-      float n_txx = R(r, 0), n_tzz = R(r, 1);
-      const float n_txz = R(r, 2);
+      float n_txx = S[0], n_tzz = S[kT];
+      const float n_txz = S[2 * kT];
       if (src_col && r == sh.isx) {  // FD2DGPU.cu:2039-2049 (transient)
         own_txx[0] = n_txx;
         own_tzz[0] = n_tzz;
@@ -164,15 +227,15 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_tb(FwdFusedArgs a) {
       push(w.txz[0], n_txz);
     }
     // own operands of this step (read before the refill below can reuse ring slots)
-    const float ovx0 = R(r, 3), ovz0 = R(r, 4);
+    const float ovx0 = S[3 * kT], ovz0 = S[4 * kT];
     float bb[kK], lam[kK], mu[kK];
 #pragma unroll
     for (int k = 0; k < kK; k++) {
-      bb[k] = R(r, 5 + k);
-      lam[k] = R(r, 5 + kK + 2 * k);
-      mu[k] = R(r, 6 + kK + 2 * k);
+      bb[k] = S[(5 + k) * kT];
+      lam[k] = S[(5 + kK + 2 * k) * kT];
+      mu[k] = S[(6 + kK + 2 * k) * kT];
     }
-    issue(r + kD - 1);  // into the slot of row step r - 1 (mod kD), finished last step
+    if (!kBulk) issue(r + kD - 1);  // into the slot of row step r - 1 (mod kD), finished last step
     // ---- publish this step's z-tap rows -----------------------------------------------------
     float *zb = ztap + (r & 1) * 4 * kK * ROW + kTbPad;
 #pragma unroll
@@ -186,7 +249,19 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_tb(FwdFusedArgs a) {
       zb[(4 * k + 2) * ROW + t] = w.vx[k][5];
       zb[(4 * k + 3) * ROW + t] = w.vz[k][5];
     }
-    __syncthreads();
+    if (kBulk) {
+      // a wait that gave up ends the march for the whole CTA (the barrier is a vote); otherwise
+      // every thread is done with slot r - 1: refill it kD - 1 steps ahead
+      if (__syncthreads_or(!ok)) {
+        aborted = true;
+        break;
+      }
+      const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
+      tb_issue_warp<kT>(fd, ring + (size_t)ps * NF * kT, my_f, &bars[ps], r + kD - 1, ld, c0, lane);
+      cur.advance();
+    } else {
+      __syncthreads();
+    }
 #pragma unroll
     for (int k = 0; k < kK; k++) {
       const float *zt_txz = zb + (4 * k + 0) * ROW + t;
@@ -274,6 +349,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_fwd_tb(FwdFusedArgs a) {
       }
     }
   }
+  if (kBulk) pair_exit<kD>(bars, cur, aborted, ok, a.err);
   cp_async_wait<0>();
 }
 

@@ -225,7 +225,8 @@ int ds2d_bandpass_filter_device(int nx, int nz, int x1, int x2, int z1, int z2, 
  * shot and snapshot, and replay each K-step segment from its snapshot with strips before
  * reversing it: snapshots plus K steps of strips instead of nt steps of strips, for one more
  * forward propagation per L^T.  Random-boundary RTM steps: "tb" (K = 1-4 forward time steps
- * per launch, 0 = off: the default), "tb_cta" (256 / 512, 0 = automatic); the backward step
+ * per launch, default 2; 0 = one step per launch on the pair / ring kernels), "tb_cta" (256 / 512,
+ * 0 = automatic), "tb_bulk" (1 = operand rows by bulk copy at depth 1-2, the default); the backward step
  * "bwd_bulk" (1 = operand rows by bulk copy, the copy issue spread over all warps: the default;
  * 0 = per-thread cp.async), "bwd_1b" (0 / 1: one barrier per row step), "bwd_ws" (0 off, or
  * 96 / 128 / 192 threads per role of the warp-specialised step). */

@@ -205,6 +205,7 @@ def test_fused_step_matches_half_steps(cuda_device, boundary, xr, ring):
     for fused in (0, 1):
         with _ctx(c, shots, boundary=boundary, seed=5) as e:
             e.set_option("pair", 0)  # the one-column kernels (the pair kernels have their own test)
+            e.set_option("tb", 0)  # one forward step per launch
             e.set_option("fused", fused)
             e.set_option("ring", ring)
             e.set_option("xr", xr)
@@ -233,6 +234,7 @@ def test_ring_occupancy_variants_agree(cuda_device, boundary):
     for occ in (0, 1):
         with _ctx(c, shots, boundary=boundary, seed=5) as e:
             e.set_option("pair", 0)
+            e.set_option("tb", 0)  # one forward step per launch
             e.set_option("occ", occ)
             e.set_models(vp, vs)
             e.set_wavelet(w)
@@ -257,6 +259,7 @@ def test_ring_cta_widths_agree(cuda_device, boundary):
     for cta in (128, 192):
         with _ctx(c, shots, boundary=boundary, seed=5) as e:
             e.set_option("pair", 0)
+            e.set_option("tb", 0)  # one forward step per launch
             e.set_option("cta", cta)
             e.set_models(vp, vs)
             e.set_wavelet(w)
@@ -457,6 +460,7 @@ def test_pair_kernels_match_ring_and_oracle(cuda_device, mode, pair_cta, pair_fc
     for pair in (0, 1):
         with _ctx(c, shots, boundary="random", seed=5) as e:
             e.set_option("pair", mode if pair else 0)
+            e.set_option("tb", 0)  # one forward step per launch
             if pair:
                 e.set_option("pair_cta", pair_cta)
                 e.set_option("pair_fcta", pair_fcta)
@@ -499,6 +503,7 @@ def test_pair_kernels_uneven_windows(cuda_device):
     with Elastic2D(c["allnx"], c["allnz"], wmax, c["pml"], c["nt"], c["dx"], c["dz"], c["dt"],
                    boundary="random", seed=8, max_shots=len(shots), max_ntr=wmax) as e:
         e.set_option("pair", 1)
+        e.set_option("tb", 0)  # one forward step per launch
         e.set_option("pair_xr", 16)
         e.set_models(vp, vs)
         e.set_wavelet(w)

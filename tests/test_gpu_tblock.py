@@ -39,12 +39,15 @@ def _case(allnz, nt):
     return c, vp, vs, w, shots, obs
 
 
-# (depth, CTA width, rows per CTA, model depth): 320 padded rows give 256-thread CTAs two z-strips
-# (one inner edge each), 460 give depth 3-4 three strips (an inner strip with two halos), 512
-# threads cover the 320 rows in one strip; xr 24 gives each shot several row blocks.  nt 203 is
-# no multiple of the depth, so the last block of a pass is shorter.
-CASES = [(1, 256, 0, 300), (2, 256, 24, 300), (3, 256, 24, 300), (4, 256, 0, 300),
-         (1, 512, 24, 300), (2, 512, 0, 300), (3, 256, 24, 440), (4, 256, 24, 440)]
+# (depth, CTA width, rows per CTA, model depth, operand rows by bulk copy): 320 padded rows give
+# 256-thread CTAs two z-strips (one inner edge each), 460 give depth 3-4 three strips (an inner
+# strip with two halos), 512 threads cover the 320 rows in one strip; xr 24 gives each shot
+# several row blocks.  nt 203 is no multiple of the depth, so the last block of a pass is shorter.
+# Depth 1-2 run with bulk-copied operand rows (the default) and with per-thread cp.async; depth
+# 3-4 have only the latter.
+CASES = [(1, 256, 0, 300, 1), (2, 256, 24, 300, 1), (3, 256, 24, 300, 0), (4, 256, 0, 300, 0),
+         (1, 512, 24, 300, 1), (2, 512, 0, 300, 1), (3, 256, 24, 440, 0), (4, 256, 24, 440, 0),
+         (1, 256, 24, 300, 0), (2, 256, 0, 300, 0), (2, 512, 24, 300, 0), (2, 256, 24, 440, 1)]
 
 
 _FLOOR = {}
@@ -69,14 +72,14 @@ def _image_floor(c, vp, vs, w, shots, obs):
     return _FLOOR[c["allnz"]]
 
 
-@pytest.mark.parametrize("depth,cta,xr,allnz", CASES)
-def test_time_blocked_forward_matches_one_step(cuda_device, depth, cta, xr, allnz):
+@pytest.mark.parametrize("depth,cta,xr,allnz,bulk", CASES)
+def test_time_blocked_forward_matches_one_step(cuda_device, depth, cta, xr, allnz, bulk):
     """Receiver records of the forward modelling (to 1e-6) and the RTM images (to the FP32 floor
     of the images) with the forward pass on the time-blocked kernel against the one-step ring
     kernels."""
     c, vp, vs, w, shots, obs = _case(allnz, nt=203)
     ref = _run(c, shots, vp, vs, w, obs, tb=0, pair=0)
-    got = _run(c, shots, vp, vs, w, obs, tb=depth, tb_cta=cta, pair_xr=xr)
+    got = _run(c, shots, vp, vs, w, obs, tb=depth, tb_cta=cta, pair_xr=xr, tb_bulk=bulk)
     assert np.abs(got[0]).max() > 0
     for j in range(2):
         err = rel(got[j], ref[j])
