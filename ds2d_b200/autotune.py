@@ -12,7 +12,7 @@ CTA width, `tb_bulk` = operand rows by bulk copy at depth 1-2): one launch advan
 `tb` steps, reading and writing the state once.
 The backward step can run warp-specialised (`bwd_ws` = threads per role, 96 / 128 / 192: the
 source and adjoint wavefields on separate warps of one CTA), with one barrier per row step
-(`bwd_1b`), and with its operand rows fed by bulk copies (`bwd_bulk`).
+(`bwd_1b`), and with its operand rows fed by bulk copies (`bwd_bulk`, CTA width `bwd_cta`).
 Their best values depend on the grid, the number of resident shots and the boundary, so the
 tuner times each candidate on a probe context with the caller's grid and batch but only
 `probe_nt` time steps (an RTM of the same shots: one forward and one backward fused launch per
@@ -22,7 +22,7 @@ import numpy as np
 from .api import Elastic2D
 
 _RING_BASE = {"pair": 0, "pair_split": 0, "pair_cta": 0, "pair_fcta": 0, "pair_xr": 0, "tb": 0,
-              "tb_cta": 0, "tb_bulk": 1, "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0}  # every knob named
+              "tb_cta": 0, "tb_bulk": 1, "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0, "bwd_cta": 0}
 _RING_SPACE = [
     {"ring": 4, "xr": 128, "occ": 0, "cta": 128}, {"ring": 4, "xr": 128, "occ": 0, "cta": 192},
     {"ring": 4, "xr": 64, "occ": 0, "cta": 128}, {"ring": 4, "xr": 256, "occ": 0, "cta": 192},
@@ -49,13 +49,13 @@ _WS_SPACE = ([{"tb": 2, "tb_cta": 0, "bwd_ws": kt} for kt in (96, 128, 192)] +
              [{"pair": 2, "pair_fcta": 256, "bwd_ws": kt} for kt in (96, 128, 192)] +
              [{"tb": 2, "tb_cta": 0, "bwd_1b": 1, "cta": cta} for cta in (128, 192)] +
              [{"pair": 2, "pair_fcta": 256, "bwd_1b": 1, "cta": cta} for cta in (128, 192)] +
-             [{"tb": 2, "tb_cta": 0, "bwd_bulk": 1, "bwd_1b": one, "cta": cta}
-              for one in (0, 1) for cta in (128, 192)] +
-             [{"tb": k, "tb_cta": tc, "bwd_bulk": 1, "cta": 192} for k in (1, 2) for tc in (256, 512)] +
-             [{"pair": 2, "pair_fcta": 256, "bwd_bulk": 1, "bwd_1b": one, "cta": cta}
-              for one in (0, 1) for cta in (128, 192)])
+             [{"tb": 2, "tb_cta": 0, "bwd_bulk": 1, "bwd_1b": one, "bwd_cta": bc}
+              for one in (0, 1) for bc in (128, 192, 256)] +
+             [{"tb": k, "tb_cta": tc, "bwd_bulk": 1, "bwd_cta": 0} for k in (1, 2) for tc in (256, 512)] +
+             [{"pair": 2, "pair_fcta": 256, "bwd_bulk": 1, "bwd_1b": one, "bwd_cta": bc}
+              for one in (0, 1) for bc in (128, 192, 256)])
 _RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0, "tb": 0, "tb_cta": 0, "tb_bulk": 1,
-                  "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0}
+                  "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0, "bwd_cta": 0}
 
 
 def default_space(boundary="random"):

@@ -14,8 +14,12 @@
 // all warps of the CTA (warp w issues the fields f with f mod W = w, W warps; every warp arrives
 // on the slot's barrier with its own bytes), so no warp carries a step's whole copy issue.
 //
-// z-strips: a CTA's columns [zs - 8, zs - 8 + kT) start on a 16-byte boundary, so the strips'
-// width tz is a multiple of 4 (copies are clipped to the row's allocation [0, ld)).
+// z-strips: strip j owns columns [zs, zs + tz), zs = j tz; its CTA's threads cover them plus the
+// 8 halo columns of each side that borders another strip (none at the grid's edges, where the
+// columns beyond are zero), from c0 = zs - 8 (or 0 for the first strip).  tz is a multiple of 4,
+// so every copy row starts on a 16-byte boundary (copies are clipped to the row's allocation
+// [0, ld)).  Without halo columns at the edges, 2 strips of 256 threads cover a 481-deep grid
+// (512 threads for 481 columns, 128 registers: 16 warps per SM).
 #pragma once
 #include "ds2d_pair.cuh"
 
@@ -28,14 +32,14 @@ __host__ __device__ constexpr size_t bwd_bulk_smem(int kT) {
 }
 
 // Copies of one ring slot for one-column CTAs, by one warp: its lane owning ring field f (row
-// q - lag of its array if that row lies in [lo, hi)) copies it; strip columns
-// [zs - 8, zs - 8 + kT) map to ring floats 0 .. kT, clipped to [0, ld).  Lane 0 arrives on the
-// slot's barrier with the bytes of the warp's copies before any is issued.
+// q - lag of its array if that row lies in [lo, hi)) copies it; the CTA's columns
+// [c0, c0 + kT) map to ring floats 0 .. kT, clipped to [0, ld).  Lane 0 arrives on the slot's
+// barrier with the bytes of the warp's copies before any is issued.
 template <int kT>
 __device__ __forceinline__ void issue_slot_col(const RingField &fd, float *slot_base, int f,
-                                               unsigned long long *bar, int q, int ld, int zs,
+                                               unsigned long long *bar, int q, int ld, int c0,
                                                int lane) {
-  const int glo = max(0, zs - 8), ghi = min(ld, zs - 8 + kT);
+  const int glo = max(0, c0), ghi = min(ld, c0 + kT);
   const unsigned bytes = (unsigned)(ghi - glo) * 4u;
   const int row = q - fd.lag;
   const bool mine = fd.src != nullptr && row >= fd.lo && row < fd.hi;
@@ -43,7 +47,7 @@ __device__ __forceinline__ void issue_slot_col(const RingField &fd, float *slot_
   if (lane == 0) mbar_arrive_tx(bar, n * bytes);
   __syncwarp();
   if (mine)
-    bulk_g2s(slot_base + f * kT + (glo - (zs - 8)), fd.src + (long long)row * ld + glo, bytes, bar);
+    bulk_g2s(slot_base + f * kT + (glo - c0), fd.src + (long long)row * ld + glo, bytes, bar);
 }
 
 template <int kT, int kMinB, bool kOne>
@@ -58,15 +62,16 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
   const int s = blockIdx.z, t = threadIdx.x;
   const Dims d = slot_dims(a.d, a.shots[s]);
   const int zs = blockIdx.x * a.tz;
-  const int z = zs - 8 + t;
+  const int c0 = zs > 0 ? zs - 8 : 0;  // first column of the CTA: 8 halo columns inside the grid
+  const int z = c0 + t;
   const int x0 = blockIdx.y * a.xr, x1 = min(x0 + a.xr, d.nxp);
   if (x0 >= d.nxp) return;  // beyond this slot's window (uneven batches), whole CTA
   if (__syncthreads_or(t == 0 && pair_err_raised(a.err))) return;  // whole CTA
   const int base = (int)(d.slot * s);  // cell offsets fit 32 bits (checked on the host)
   const int ld = d.ld, pml = d.pml;
   const bool zin = z >= 0 && z < d.nzp;
-  const bool c1 = t >= 4 && t < a.tz + 12;
-  const bool c2 = t >= 8 && t < a.tz + 8;
+  const bool c1 = z >= zs - 4 && z < zs + a.tz + 4;  // stage-1 columns: the strip and 4 each side
+  const bool c2 = z >= zs && z < zs + a.tz;          // stage-2 columns: the strip
   const bool z_int = z >= pml && z < d.nzp - pml;
   const bool z_upd = z >= d.nop && z < d.nzp - d.nop;
   const ShotDev sh = a.shots[s];
@@ -119,7 +124,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
   __syncthreads();
   const int rs0 = x0 - 8;
   for (int j = 0; j < kD - 1; j++)
-    issue_slot_col<kT>(fd, ring + (size_t)j * NF * kT, my_f, &bars[j], rs0 + j, ld, zs, lane);
+    issue_slot_col<kT>(fd, ring + (size_t)j * NF * kT, my_f, &bars[j], rs0 + j, ld, c0, lane);
 
   float w_bvx[9], w_bvz[9], w_avx[9], w_avz[9];
   // adjoint-velocity operands, as k_bwd_ring: PL = (l+2m) atxx + l atzz, PzLx = (l+2m) atzz + l atxx
@@ -197,7 +202,7 @@ __global__ void __launch_bounds__(kT, kMinB) k_bwd_bulk(BwdFusedArgs a) {
     // every thread is done with the previous slot: refill it kD - 1 steps ahead
     {
       const int ps = cur.slot == 0 ? kD - 1 : cur.slot - 1;
-      issue_slot_col<kT>(fd, ring + (size_t)ps * NF * kT, my_f, &bars[ps], r + kD - 1, ld, zs,
+      issue_slot_col<kT>(fd, ring + (size_t)ps * NF * kT, my_f, &bars[ps], r + kD - 1, ld, c0,
                          lane);
     }
     // ---- stage 1: stresses of row r1 = r - 4 -----------------------------------------------

@@ -284,7 +284,8 @@ struct ds2d_ctx {
   int opt_bwd_1b = 0;        // option "bwd_1b": one barrier per row step in k_bwd_ring / k_bwd_bulk
   int opt_bwd_bulk = 1;      // option "bwd_bulk": k_bwd_bulk, operand rows by bulk copy (random
                              // boundary; the default, 0 = the per-thread cp.async ring of k_bwd_ring)
-  int occ_bulk[4] = {};      // resident CTAs per SM of k_bwd_bulk: [128 / 192 threads][one barrier]
+  int opt_bwd_cta = 0;       // option "bwd_cta": threads per CTA of k_bwd_bulk (0 automatic, 128 / 192 / 256)
+  int occ_bulk[6] = {};      // resident CTAs per SM of k_bwd_bulk: [128 / 192 / 256 threads][one barrier]
   int occ_ws[3] = {};        // resident CTAs per SM of k_bwd_ws, 96 / 128 / 192 threads per role
   int occ_tb[2][4] = {};     // resident CTAs per SM of k_fwd_tb, [256 / 512 threads][depth - 1]
   // split backward: the two launches of a step as parallel branches (second stream, fork / join
@@ -839,21 +840,30 @@ BwdFn ws_fn(int kt) {
 }
 int ws_idx(int kt) { return kt == 96 ? 0 : kt == 128 ? 1 : 2; }
 // ---- bulk-copy-fed one-column backward (random boundary) ------------------------------------
+// 128 threads at 4 CTAs per SM and 256 at 2 (128 registers, 16 warps per SM), 192 at 2 (12).
+constexpr int kBulkCtas[3] = {128, 192, 256};
 BwdFn bulk_fn(int cta, bool one) {
+  if (cta == 256) return one ? k_bwd_bulk<256, 2, true> : k_bwd_bulk<256, 2, false>;
   if (cta == kWideCta) return one ? k_bwd_bulk<kWideCta, 2, true> : k_bwd_bulk<kWideCta, 2, false>;
-  return one ? k_bwd_bulk<kFB, 3, true> : k_bwd_bulk<kFB, 3, false>;
+  return one ? k_bwd_bulk<kFB, 4, true> : k_bwd_bulk<kFB, 4, false>;
 }
-int bulk_idx(int cta, bool one) { return (cta == kWideCta ? 2 : 0) + (one ? 1 : 0); }
-// z-strips whose width is a multiple of 4 (16-byte aligned copy rows), at most cta - 16 columns
-void bulk_split(const Dims &d, int cta, int *nstrips, int *tz) {
-  for (int ns = (d.nzp + cta - 17) / (cta - 16);; ns++) {
-    const int t = ((d.nzp + ns - 1) / ns + 3) / 4 * 4;
-    if (t <= cta - 16) {
-      *nstrips = ns;
-      *tz = t;
-      return;
+int bulk_idx(int cta, bool one) { return (cta == 256 ? 4 : cta == kWideCta ? 2 : 0) + (one ? 1 : 0); }
+
+// CTA width of k_bwd_bulk: option "bwd_cta", else the width with the fewest threads per grid row
+// (edge-aware strips), the wider on a tie.
+int bulk_cta(const ds2d_ctx *c) {
+  if (c->opt_bwd_cta) return c->opt_bwd_cta;
+  int best = kWideCta;
+  long long best_thr = 1LL << 40;
+  for (int cta : kBulkCtas) {
+    int ns, tz;
+    if (!tb_split(c->d, cta, 1, &ns, &tz)) continue;
+    if ((long long)ns * cta <= best_thr) {
+      best_thr = (long long)ns * cta;
+      best = cta;
     }
   }
+  return best;
 }
 
 bool ws_on(const ds2d_ctx *c) {
@@ -1105,7 +1115,7 @@ int rtm_batch(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
     if (!c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
     if (!c->abk2.vx && (rc = alloc_wave(c, c->abk2, true))) return rc;
   }
-  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk + 32 * c->opt_tb_bulk), (long long)(size_t)c->stream};
+  const long long key[6] = {2, n, shot_base, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk + 32 * c->opt_tb_bulk + 64 * (c->opt_bwd_cta / 64)), (long long)(size_t)c->stream};
   return run_graph(c, key, [&]() { return rtm_batch_body(c, shots, n, shot_base); });
 }
 
@@ -1164,13 +1174,14 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
         CK(cudaEventRecord(c->ev_join, c->aux));
         CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
       } else if (c->opt_bwd_bulk && pair_ok(c) &&
-                 c->occ_bulk[bulk_idx(cta, c->opt_bwd_1b != 0)] > 0) {
+                 c->occ_bulk[bulk_idx(bulk_cta(c), c->opt_bwd_1b != 0)] > 0) {
+        const int bc = bulk_cta(c);
         int bns, btz;
-        bulk_split(d, cta, &bns, &btz);
+        tb_split(d, bc, 1, &bns, &btz);  // edge-aware strips, widths a multiple of 4
         a.tz = btz; a.err = c->d_err;
         dim3 bgrid(bns, (d.nxp + xr - 1) / xr, n);
-        LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), bulk_fn(cta, c->opt_bwd_1b != 0), bgrid,
-                cta, bwd_bulk_smem(cta), a);
+        LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), bulk_fn(bc, c->opt_bwd_1b != 0), bgrid,
+                bc, bwd_bulk_smem(bc), a);
       } else if (ws_on(c)) {
         const int kt = c->opt_bwd_ws;
         int wns, wtz;
@@ -2013,8 +2024,8 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
                                                             pair_bwd_smem(bctas[i]));
       }
     }
-    for (int i = 0; i < 4 && e == cudaSuccess; i++) {
-      const int cta = i < 2 ? kFB : kWideCta;
+    for (int i = 0; i < 6 && e == cudaSuccess; i++) {
+      const int cta = kBulkCtas[i / 2];
       const bool one = (i & 1) != 0;
       e = cudaFuncSetAttribute(bulk_fn(cta, one), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)bwd_bulk_smem(cta));
@@ -2178,7 +2189,7 @@ int ds2d_forward(ds2d_ctx *c, const ds2d_shot *shots, int n, float *rec_vz, floa
     int m = std::min(c->B, n - f);
     if ((rc = upload_batch(c, shots + f, m))) return rc;
     if (c->opt_fused && !c->fw2.vx && (rc = alloc_wave(c, c->fw2, false))) return rc;
-    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk + 32 * c->opt_tb_bulk), (long long)(size_t)c->stream};
+    const long long key[6] = {1, m, f, c->opt_fused + 2 * c->opt_ring + 32 * c->opt_occ + 64 * c->opt_cta, c->opt_xr + 1000LL * c->opt_pair_xr + 1000000LL * c->opt_pair_cta + 100000000LL * (c->opt_pair_fcta / 64 + 5 * c->opt_pair_split) + 1000000000LL * c->opt_pair + 10000000000LL * (c->opt_tb + 5 * (c->opt_tb_cta / 32)) + 1000000000000LL * (c->opt_bwd_ws / 32 + 8 * c->opt_bwd_1b + 16 * c->opt_bwd_bulk + 32 * c->opt_tb_bulk + 64 * (c->opt_bwd_cta / 64)), (long long)(size_t)c->stream};
     rc = run_graph(c, key, [&]() {
       int r;
       if ((r = setup_batch(c, m, f, false))) return r;
@@ -2648,6 +2659,10 @@ int ds2d_set_option(ds2d_ctx *c, const char *key, long long value) {
   } else if (k == "bwd_bulk") {
     if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "bwd_bulk must be 0 or 1");
     c->opt_bwd_bulk = (int)value;
+  } else if (k == "bwd_cta") {
+    if (value != 0 && value != 128 && value != 192 && value != 256)
+      return fail(c, DS2D_E_ARG, "bwd_cta must be 0 (automatic), 128, 192 or 256");
+    c->opt_bwd_cta = (int)value;
   } else if (k == "bwd_1b") {
     if (value != 0 && value != 1) return fail(c, DS2D_E_ARG, "bwd_1b must be 0 or 1");
     c->opt_bwd_1b = (int)value;

@@ -631,22 +631,24 @@ def test_live_reference_elsrtm_full_size(cuda_device):
     assert mis == pytest.approx(r["misfit"], rel=1e-4) and mis == pytest.approx(r64["misfit"], rel=1e-4)
 
 
-@pytest.mark.parametrize("opts,xr", [({"bwd_ws": 96}, 128), ({"bwd_ws": 128}, 24),
-                                     ({"bwd_ws": 192}, 24), ({"bwd_ws": 192}, 128),
-                                     ({"bwd_1b": 1, "cta": 192}, 128),
-                                     ({"bwd_1b": 1, "bwd_bulk": 0, "cta": 128}, 24),
-                                     ({"bwd_bulk": 1, "cta": 128}, 24),
-                                     ({"bwd_bulk": 1, "cta": 192}, 128),
-                                     ({"bwd_bulk": 1, "bwd_1b": 1, "cta": 192}, 24)])
-def test_backward_variants_match_ring_and_oracle(cuda_device, opts, xr):
+@pytest.mark.parametrize("opts,xr,allnz", [
+    ({"bwd_ws": 96}, 128, 300), ({"bwd_ws": 128}, 24, 300), ({"bwd_ws": 192}, 24, 300),
+    ({"bwd_ws": 192}, 128, 300), ({"bwd_1b": 1, "bwd_bulk": 0, "cta": 128}, 24, 300),
+    ({"bwd_1b": 1, "bwd_bulk": 0, "cta": 192}, 128, 300),
+    ({"bwd_bulk": 1, "bwd_cta": 128}, 24, 300), ({"bwd_bulk": 1, "bwd_cta": 192}, 128, 300),
+    ({"bwd_bulk": 1, "bwd_cta": 256}, 24, 300), ({"bwd_bulk": 1, "bwd_cta": 256}, 128, 200),
+    ({"bwd_bulk": 1, "bwd_1b": 1, "bwd_cta": 192}, 24, 300),
+    ({"bwd_bulk": 1, "bwd_1b": 1, "bwd_cta": 256}, 128, 300)])
+def test_backward_variants_match_ring_and_oracle(cuda_device, opts, xr, allnz):
     """Variants of the backward RTM step against the one-column ring kernel and the FP64 oracle,
     random boundary: the warp-specialised step (k_bwd_ws: the source field and the adjoint field
     on separate warps of one CTA, strains handed over in shared memory for the imaging
     condition), the ring kernel with one barrier per row step (bwd_1b) and the ring fed by bulk
-    copies (k_bwd_bulk, with either barrier count).  The 320-deep grid gives every CTA width two
-    or more z-strips; xr 24 gives each shot several row blocks."""
+    copies (k_bwd_bulk, with either barrier count, halo columns only at inner strip edges).  The
+    320-deep grid gives every CTA width two or more z-strips, the 220-deep one a single
+    256-thread strip; xr 24 gives each shot several row blocks."""
     c, _, _, w, _ = small_case(nt=200)
-    c["allnz"] = 300
+    c["allnz"] = allnz
     vp, vs = synth.layered(c["allnx"], c["allnz"], seed=4)
     shots = synth.surface_shots(c["allnx"], c["nx"], c["pml"], 3)
     with _ctx(c, shots, boundary="pml") as e:
