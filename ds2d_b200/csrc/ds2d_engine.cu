@@ -281,7 +281,7 @@ struct ds2d_ctx {
   // Warp-specialised backward step (ds2d_bwdws.cuh, random boundary): option "bwd_ws" = threads
   // per role (0 off, 96, 128 or 192; a CTA holds both roles).
   int opt_bwd_ws = 0;
-  int opt_bwd_1b = 0;        // option "bwd_1b": one barrier per row step in k_bwd_ring / k_bwd_bulk
+  int opt_bwd_1b = 1;        // option "bwd_1b": one barrier per row step in k_bwd_ring / k_bwd_bulk
   int opt_bwd_bulk = 1;      // option "bwd_bulk": k_bwd_bulk, operand rows by bulk copy (random
                              // boundary; the default, 0 = the per-thread cp.async ring of k_bwd_ring)
   int opt_bwd_cta = 0;       // option "bwd_cta": threads per CTA of k_bwd_bulk (0 automatic, 128 / 192 / 256)

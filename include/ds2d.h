@@ -228,8 +228,10 @@ int ds2d_bandpass_filter_device(int nx, int nz, int x1, int x2, int z1, int z2, 
  * per launch, default 2; 0 = one step per launch on the pair / ring kernels), "tb_cta" (256 / 512,
  * 0 = automatic), "tb_bulk" (1 = operand rows by bulk copy at depth 1-2, the default); the backward step
  * "bwd_bulk" (1 = operand rows by bulk copy, the copy issue spread over all warps: the default;
- * 0 = per-thread cp.async), "bwd_1b" (0 / 1: one barrier per row step), "bwd_ws" (0 off, or
- * 96 / 128 / 192 threads per role of the warp-specialised step). */
+ * 0 = per-thread cp.async), "bwd_cta" (threads per CTA of the bulk-copy step: 128 / 192 / 256,
+ * 0 = the width with the fewest threads per grid row), "bwd_1b" (1 = one barrier per row step:
+ * the default; 0 = two), "bwd_ws" (0 off, or 96 / 128 / 192 threads per role of the
+ * warp-specialised step). */
 int ds2d_set_option(ds2d_ctx *ctx, const char *key, long long value);
 
 /* Profiling (no counterpart in the reference, which has only a commented-out host timer,
