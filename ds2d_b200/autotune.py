@@ -53,7 +53,9 @@ _WS_SPACE = ([{"tb": 2, "tb_cta": 0, "bwd_ws": kt} for kt in (96, 128, 192)] +
               for one in (0, 1) for bc in (128, 192, 256)] +
              [{"tb": k, "tb_cta": tc, "bwd_bulk": 1, "bwd_cta": 0} for k in (1, 2) for tc in (256, 512)] +
              [{"pair": 2, "pair_fcta": 256, "bwd_bulk": 1, "bwd_1b": one, "bwd_cta": bc}
-              for one in (0, 1) for bc in (128, 192, 256)])
+              for one in (0, 1) for bc in (128, 192, 256)] +
+             [{"tb": 2, "tb_cta": 0, "bwd_bulk": 1, "bwd_1b": 1, "bwd_cta": 256, "pair_xr": pxr}
+              for pxr in (96, 128, 192)])
 _RING_DEFAULTS = {"ring": 4, "xr": 128, "occ": 0, "cta": 0, "tb": 0, "tb_cta": 0, "tb_bulk": 1,
                   "bwd_ws": 0, "bwd_1b": 0, "bwd_bulk": 0, "bwd_cta": 0}
 

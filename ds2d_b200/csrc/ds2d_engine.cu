@@ -1178,8 +1178,10 @@ int rtm_batch_body(ds2d_ctx *c, const ds2d_shot *shots, int n, int shot_base) {
         const int bc = bulk_cta(c);
         int bns, btz;
         tb_split(d, bc, 1, &bns, &btz);  // edge-aware strips, widths a multiple of 4
-        a.tz = btz; a.err = c->d_err;
-        dim3 bgrid(bns, (d.nxp + xr - 1) / xr, n);
+        // rows per CTA: option "pair_xr", else the count that fills the SMs' waves best
+        const int bxr = pair_xr(c, bns, c->occ_bulk[bulk_idx(bc, c->opt_bwd_1b != 0)]);
+        a.tz = btz; a.xr = bxr; a.err = c->d_err;
+        dim3 bgrid(bns, (d.nxp + bxr - 1) / bxr, n);
         LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), bulk_fn(bc, c->opt_bwd_1b != 0), bgrid,
                 bc, bwd_bulk_smem(bc), a);
       } else if (ws_on(c)) {

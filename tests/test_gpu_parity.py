@@ -660,7 +660,8 @@ def test_backward_variants_match_ring_and_oracle(cuda_device, opts, xr, allnz):
     for var in (0, 1):
         with _ctx(c, shots, boundary="random", seed=5) as e:
             e.set_option("pair", 0)
-            e.set_option("xr", xr)
+            e.set_option("xr", xr)  # rows per CTA of the one-column ring kernels
+            e.set_option("pair_xr", xr)  # and of the bulk-copy ones
             e.set_option("bwd_1b", 0)  # the two-barrier per-thread ring kernel as the reference
             e.set_option("bwd_bulk", 0)
             for k, v in (opts if var else {}).items():
