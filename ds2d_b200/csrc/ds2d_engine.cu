@@ -83,8 +83,11 @@ using ScatFn = void (*)(BwdScatArgs);
 ScatFn bwd_scat_fn(bool rbc) { return rbc ? k_bwd_scat_ring<false, 4, 4> : k_bwd_scat_ring<true, 4, 4>; }
 
 BwdFn bwd_ring_fn(bool rbc, int depth, int occ = 0, int cta = kFB, bool one = false) {
-  if (one && rbc && depth == 4 && occ == 0)  // one barrier per row step (random boundary)
-    return cta == kWideCta ? k_bwd_ring<false, 4, 2, kWideCta, true> : k_bwd_ring<false, 4, 3, kFB, true>;
+  if (one && depth == 4 && occ == 0) {  // one barrier per row step
+    if (rbc)
+      return cta == kWideCta ? k_bwd_ring<false, 4, 2, kWideCta, true> : k_bwd_ring<false, 4, 3, kFB, true>;
+    return cta == kWideCta ? k_bwd_ring<true, 4, 2, kWideCta, true> : k_bwd_ring<true, 4, 3, kFB, true>;
+  }
   if (cta == kWideCta && depth == 4 && occ == 0)
     return rbc ? k_bwd_ring<false, 4, 2, kWideCta> : k_bwd_ring<true, 4, 2, kWideCta>;
   switch (depth * 2 + (occ ? 1 : 0)) {
@@ -282,6 +285,7 @@ struct ds2d_ctx {
   // per role (0 off, 96, 128 or 192; a CTA holds both roles).
   int opt_bwd_ws = 0;
   int opt_bwd_1b = 1;        // option "bwd_1b": one barrier per row step in k_bwd_ring / k_bwd_bulk
+                             // (PML and random boundary)
   int opt_bwd_bulk = 1;      // option "bwd_bulk": k_bwd_bulk, operand rows by bulk copy (random
                              // boundary; the default, 0 = the per-thread cp.async ring of k_bwd_ring)
   int opt_bwd_cta = 0;       // option "bwd_cta": threads per CTA of k_bwd_bulk (0 automatic, 128 / 192 / 256)
@@ -1334,7 +1338,7 @@ int elsrtm_backward_fused(ds2d_ctx *c, int n, bool strips) {
     a.shots = c->d_shots; a.rmap = c->d_rmap; a.res_vz = c->rec[6]; a.res_vx = c->rec[7];
     a.st = c->st_a; a.strips_on = strips; a.it = it; a.tz = tz; a.xr = xr;
     a.img = c->img_slot; a.img_plane = plane;
-    BwdFn kfn = bwd_ring_fn(d.rbc != 0, 4, 0, kFB);
+    BwdFn kfn = bwd_ring_fn(d.rbc != 0, 4, 0, kFB, c->opt_bwd_1b != 0);
     LAUNCHS("bwd_fused", kBytesBwdFused * CELLS(n), kfn, grid, kFB, sm, a);
     BornArgs bs{d, c->d_shots, fn->vx, fn->vz, c->par, c->ov_s[0], c->ov_s[1], c->ov_s[2]};
     LAUNCH(k_born, bgrid, blk, bs);
@@ -1972,13 +1976,11 @@ int ds2d_create(const ds2d_grid *grid, const ds2d_opts *opts, ds2d_ctx **out) {
               e = cudaFuncSetAttribute(bwd_ring_fn(rbc, depth, occ, kWideCta),
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        bwd_sm / kFB * kWideCta);
-            if (rbc) {
-              for (int cta : {kFB, kWideCta})
-                if (e == cudaSuccess)
-                  e = cudaFuncSetAttribute(bwd_ring_fn(rbc, depth, occ, cta, true),
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           bwd_sm / kFB * cta);
-            }
+            for (int cta : {kFB, kWideCta})
+              if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(bwd_ring_fn(rbc, depth, occ, cta, true),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bwd_sm / kFB * cta);
           }
         }
     }

@@ -781,7 +781,7 @@ __device__ __forceinline__ float strip_unpack(int prec, long long e, float word,
   return __bfloat162float(__ushort_as_bfloat16(h)) * sc;
 }
 
-// kOne (random boundary only): one barrier per row step instead of two.  Every z-tap row of a step
+// kOne: one barrier per row step instead of two.  Every z-tap row of a step
 // exists at its top -- stage 1's rows are this step's inputs at row r - 4, stage 2's are stage-1
 // outputs of row r - 8, computed four steps earlier -- so all eight are published there, into one
 // of two buffers (a thread running ahead writes the other), and the two stages then run without
@@ -789,7 +789,6 @@ __device__ __forceinline__ float strip_unpack(int prec, long long e, float word,
 template <bool kPML, int kD, int kMinB, int kT = kFB, bool kOne = false>
 __global__ void __launch_bounds__(kT, kMinB) k_bwd_ring(BwdFusedArgs a) {
   static_assert(kD >= 2 && kD <= 8 && (kD & (kD - 1)) == 0, "ring depth: 2, 4 or 8");
-  static_assert(!(kOne && kPML), "the one-barrier step is built for the random boundary");
   constexpr int NF = bwd_ring_fields(kPML);
   extern __shared__ float ring[];  // [kD][NF][kT]
   // z-tap rows: bvx bvz avx avz (stage 1), btxz btzz M PzLx (stage 2); two buffers with kOne

@@ -59,3 +59,19 @@ def test_roofline_inputs():
     # uneven windows: traffic follows the batch's padded cells, not its shot count
     c, _, _, _, _, _, shots = bench.workload(_Args(workload="uneven", nt=10), 0, 1)
     assert bench.batch_cells(c, shots) == sum((s.nx + 40) * 441 for s in shots)
+
+
+def test_autotuner_candidates_name_every_knob():
+    """Every candidate of the launch-shape autotuner sets every knob the space uses, so no
+    setting carries over from the candidate timed before it; the space holds the time-blocking
+    depths 1-4 and the backward variants."""
+    from ds2d_b200 import autotune
+    for boundary in ("random", "pml"):
+        space = autotune.default_space(boundary)
+        keys = {tuple(sorted(c)) for c in space}
+        assert len(keys) == 1, keys
+        assert len({autotune.key(c) for c in space}) == len(space)  # no candidate twice
+    space = autotune.default_space("random")
+    assert {c["tb"] for c in space} == {0, 1, 2, 3, 4}
+    assert {c["bwd_bulk"] for c in space} == {0, 1} and {c["bwd_1b"] for c in space} == {0, 1}
+    assert {c["bwd_cta"] for c in space} >= {128, 192, 256}
