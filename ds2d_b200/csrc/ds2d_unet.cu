@@ -187,19 +187,23 @@ __host__ __device__ constexpr uint32_t umma_idesc(int m, int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
-template <int kN>
+// kR output rows per CTA (1 or 2): the staged weights of a chunk serve kR rows of pixels (kR + 2
+// halo rows staged, one accumulator tile of kN TMEM columns per row), halving the weight staging
+// per output pixel at kR = 2.
+template <int kN, int kR = 1>
 __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  // layout: A planes [3 rows][2 halves][130 px][16 B], B planes [9 taps][2 halves][kN][16 B]
+  // layout: A planes [kR + 2 rows][2 halves][130 px][16 B], B planes [9 taps][2 halves][kN][16 B]
   unsigned char *sA = tc_smem;
-  unsigned char *sB = tc_smem + 6 * kTcPlaneA;
+  unsigned char *sB = tc_smem + (kR + 2) * 2 * kTcPlaneA;
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int w0 = blockIdx.x * kTcM, row = blockIdx.y;
+  const int w0 = blockIdx.x * kTcM, row0 = blockIdx.y * kR;
   const int ngrp = a.cout / kN;
   const int img = blockIdx.z / ngrp, co0 = (blockIdx.z % ngrp) * kN;
-  constexpr uint32_t kCols = kN < 32 ? 32 : kN;  // TMEM columns: a power of two >= 32
+  // TMEM columns: a power of two >= 32 holding kR accumulator tiles of kN columns
+  constexpr uint32_t kCols = kR * kN <= 32 ? 32 : kR * kN <= 64 ? 64 : kR * kN <= 128 ? 128 : 256;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&tmem_base)), "r"(kCols));
@@ -217,10 +221,10 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
   bool ok = true;
   int phase = 0;
   for (int ci0 = 0; ci0 < a.cin && ok; ci0 += 16) {
-    // stage the 3 halo rows: pixel px of row ky, channel half kh -> plane (ky, kh), offset 16 px
-    for (int i = tid; i < 3 * 2 * kTcHalo; i += 128) {
+    // stage the kR + 2 halo rows: pixel px of row ky, channel half kh -> plane (ky, kh)
+    for (int i = tid; i < (kR + 2) * 2 * kTcHalo; i += 128) {
       const int px = i % kTcHalo, kh = (i / kTcHalo) & 1, ky = i / (2 * kTcHalo);
-      const int hh = row + ky - 1, ww = w0 + px - 1;
+      const int hh = row0 + ky - 1, ww = w0 + px - 1;
       uint4 v = make_uint4(0, 0, 0, 0);
       if (hh >= 0 && hh < a.h && ww >= 0 && ww < a.w)
         v = *reinterpret_cast<const uint4 *>(
@@ -240,16 +244,20 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
 #pragma unroll
-      for (int tap = 0; tap < 9; tap++) {
-        const int ky = tap / 3, kx = tap % 3;
-        const uint64_t ad = umma_desc(a_base + (ky * 2) * kTcPlaneA + kx * 16, kTcPlaneA, 128);
-        const uint64_t bd = umma_desc(b_base + (tap * 2) * (kN * 16), kN * 16, 128);
-        const uint32_t acc = (ci0 > 0 || tap > 0) ? 1u : 0u;
-        asm volatile(
-            "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
-      }
+      for (int j = 0; j < kR; j++)
+#pragma unroll
+        for (int tap = 0; tap < 9; tap++) {
+          const int ky = tap / 3, kx = tap % 3;
+          const uint64_t ad =
+              umma_desc(a_base + ((j + ky) * 2) * kTcPlaneA + kx * 16, kTcPlaneA, 128);
+          const uint64_t bd = umma_desc(b_base + (tap * 2) * (kN * 16), kN * 16, 128);
+          const uint32_t acc = (ci0 > 0 || tap > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+                  tmem + (uint32_t)(j * kN)),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+        }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
           smem_u32(&mbar)));
     }
@@ -271,22 +279,24 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
     __syncthreads();
   }
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-  if (ok) {
-    // epilogue: thread (warp w, lane l) owns output pixel 32 w + l, reads 8 columns at a time
+  for (int j = 0; j < kR && ok; j++) {
+    // epilogue of output row row0 + j: thread (warp w, lane l) owns output pixel 32 w + l, reads
+    // 8 columns of the row's accumulator tile at a time
+    const int row = row0 + j;
     const int m = warp * 32 + lane;
     const int ww = w0 + m;
     const long long obase = (((long long)img * a.h + row) * a.w + ww) * a.ocs + a.oco + co0;
 #pragma unroll 1
     for (int c0 = 0; c0 < kN; c0 += 8) {
       uint32_t r[8];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * kN + c0);
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
           : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
             "=r"(r[7])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      if (ww < a.w) {
+      if (ww < a.w && row < a.h) {
         float v[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) {
@@ -318,9 +328,15 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
   }
 }
 
-template <int kN>
+// Dynamic shared memory of k_conv3x3_tc: the staged operands, raised where needed so that no more
+// CTAs fit on an SM than its 512 TMEM columns hold (a CTA beyond that would wait in tcgen05.alloc
+// holding an SM slot).
+template <int kN, int kR = 1>
 constexpr int tc_smem_bytes() {
-  return 6 * kTcPlaneA + 9 * 2 * kN * 16;
+  constexpr int kCols = kR * kN <= 32 ? 32 : kR * kN <= 64 ? 64 : kR * kN <= 128 ? 128 : 256;
+  constexpr int operands = (kR + 2) * 2 * kTcPlaneA + 9 * 2 * kN * 16;
+  constexpr int fit = 228 * 1024 / (512 / kCols + 1) + 2048;  // over (512 / kCols) CTAs per SM
+  return operands > fit ? operands : fit;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -813,6 +829,7 @@ struct ds2d_unet {
   bool weights_dirty = true;
   int use_tc = 1;          // 3x3 convolutions on tcgen05 (1, default) or mma.sync (0)
   int tc_wgrad = 1;        // with use_tc: weight gradients on tcgen05 too (0: on mma.sync)
+  int tc_rows = 2;         // output rows per CTA of the tcgen05 convolution (1 or 2)
   int *d_err = nullptr;    // device flag raised by a bounded wait that gave up
   std::vector<void *> allocs;
 };
@@ -848,13 +865,22 @@ int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w,
   (void)L;
   if (u->use_tc && cout % 32 == 0) {
     const int kn = cout % 128 == 0 ? 128 : (cout % 64 == 0 ? 64 : 32);
-    dim3 grid((wd + kTcM - 1) / kTcM, h, n * (cout / kn));
-    if (kn == 128)
+    const int kr = u->tc_rows;
+    dim3 grid((wd + kTcM - 1) / kTcM, (h + kr - 1) / kr, n * (cout / kn));
+    if (kr == 2) {
+      if (kn == 128)
+        k_conv3x3_tc<128, 2><<<grid, 128, tc_smem_bytes<128, 2>(), u->stream>>>(a, u->d_err);
+      else if (kn == 64)
+        k_conv3x3_tc<64, 2><<<grid, 128, tc_smem_bytes<64, 2>(), u->stream>>>(a, u->d_err);
+      else
+        k_conv3x3_tc<32, 2><<<grid, 128, tc_smem_bytes<32, 2>(), u->stream>>>(a, u->d_err);
+    } else if (kn == 128) {
       k_conv3x3_tc<128><<<grid, 128, tc_smem_bytes<128>(), u->stream>>>(a, u->d_err);
-    else if (kn == 64)
+    } else if (kn == 64) {
       k_conv3x3_tc<64><<<grid, 128, tc_smem_bytes<64>(), u->stream>>>(a, u->d_err);
-    else
+    } else {
       k_conv3x3_tc<32><<<grid, 128, tc_smem_bytes<32>(), u->stream>>>(a, u->d_err);
+    }
   } else if (cout % 64 == 0) {
     dim3 grid((wd + kPx - 1) / kPx, h, n * (cout / 64));
     k_conv3x3<64><<<grid, 128, 0, u->stream>>>(a);
@@ -1165,6 +1191,15 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
       ea = cudaFuncSetAttribute(k_conv3x3_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc_smem_bytes<32>());
     if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tc<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc_smem_bytes<128, 2>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tc<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc_smem_bytes<64, 2>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tc<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc_smem_bytes<32, 2>());
+    if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tc<32>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, wg_tc_smem_bytes<32>());
     if (ea == cudaSuccess)
@@ -1242,6 +1277,12 @@ int ds2d_unet_set_option(ds2d_unet *u, const char *key, long long value) {
   }
   if (std::string(key) == "tcgen05_wgrad") {
     u->tc_wgrad = value != 0;
+    return DS2D_OK;
+  }
+  if (std::string(key) == "tcgen05_rows") {
+    if (value != 1 && value != 2)
+      return unet_fail(u, DS2D_E_ARG, "tcgen05_rows must be 1 or 2");
+    u->tc_rows = (int)value;
     return DS2D_OK;
   }
   return unet_fail(u, DS2D_E_ARG, std::string("unknown option ") + key);

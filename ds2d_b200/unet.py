@@ -92,7 +92,7 @@ class UNet:
 
     def set_option(self, key, value):
         """"tcgen05": 1 = 3x3 convolutions on tcgen05 / TMEM, 0 = mma.sync; "tcgen05_wgrad": 0
-        keeps the weight gradient on mma.sync."""
+        keeps the weight gradient on mma.sync; "tcgen05_rows": output rows per CTA (1 or 2)."""
         self._check(self.lib.ds2d_unet_set_option(self.h, key.encode(), int(value)))
 
     def set_stream(self, stream_handle):

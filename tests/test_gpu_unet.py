@@ -132,3 +132,32 @@ def test_unet_tcgen05_weight_gradients_agree_with_mma_sync(cuda_device):
     for k, v in grads[0].items():
         if np.linalg.norm(v) > 0:
             assert rel(grads[1][k], v) < 1e-4, (k, rel(grads[1][k], v))
+
+
+def test_unet_tcgen05_two_rows_per_cta_equal_one(cuda_device):
+    """The tcgen05 convolution with two output rows per CTA (the staged weights of a chunk shared
+    by both rows, one TMEM accumulator tile per row) against one row per CTA: every output sums
+    the same products in the same order, so the forward pass agrees bit for bit, and the
+    gradients up to the order of the weight gradient's split-K atomics; an odd row count at the
+    coarsest level leaves its last CTA one row past the image."""
+    import torch
+    from ds2d_b200.unet import UNet, flatten
+    p = uo.init_params(7)
+    rng = np.random.default_rng(7)
+    n, h, w = 2, 40, 200  # 40, 20, 10, 5 rows at the four levels
+    x = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32) * 0.5).cuda()
+    out, grads = [], []
+    with UNet(max_n=n, max_h=h, max_w=w) as net:
+        net.set_params(flatten(p))
+        net.set_option("tcgen05", 1)
+        for rows in (1, 2):
+            net.set_option("tcgen05_rows", rows)
+            y = torch.zeros_like(x)
+            net.forward(x.data_ptr(), y.data_ptr(), n, h, w)
+            torch.cuda.synchronize()
+            out.append(y.cpu().numpy())
+            _, g = net.loss_grad(x.data_ptr(), t.data_ptr(), n, h, w, want_grads=True)
+            grads.append(g)
+    np.testing.assert_array_equal(out[1], out[0])
+    assert rel(grads[1], grads[0]) < 1e-5, rel(grads[1], grads[0])
