@@ -187,9 +187,9 @@ __host__ __device__ constexpr uint32_t umma_idesc(int m, int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
-// kR output rows per CTA (1 or 2): the staged weights of a chunk serve kR rows of pixels (kR + 2
-// halo rows staged, one accumulator tile of kN TMEM columns per row), halving the weight staging
-// per output pixel at kR = 2.
+// kR output rows per CTA (1, 2 or 4): the staged weights of a chunk serve kR rows of pixels
+// (kR + 2 halo rows staged, one accumulator tile of kN TMEM columns per row), so the weight
+// staging per output pixel falls as 1 / kR and the halo rows' as (kR + 2) / (3 kR).
 template <int kN, int kR = 1>
 __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
@@ -203,7 +203,8 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
   const int ngrp = a.cout / kN;
   const int img = blockIdx.z / ngrp, co0 = (blockIdx.z % ngrp) * kN;
   // TMEM columns: a power of two >= 32 holding kR accumulator tiles of kN columns
-  constexpr uint32_t kCols = kR * kN <= 32 ? 32 : kR * kN <= 64 ? 64 : kR * kN <= 128 ? 128 : 256;
+  constexpr uint32_t kCols = kR * kN <= 32 ? 32 : kR * kN <= 64 ? 64 : kR * kN <= 128 ? 128
+                           : kR * kN <= 256 ? 256 : 512;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&tmem_base)), "r"(kCols));
@@ -333,7 +334,8 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(ConvArgs a, int *err) {
 // holding an SM slot).
 template <int kN, int kR = 1>
 constexpr int tc_smem_bytes() {
-  constexpr int kCols = kR * kN <= 32 ? 32 : kR * kN <= 64 ? 64 : kR * kN <= 128 ? 128 : 256;
+  constexpr int kCols = kR * kN <= 32 ? 32 : kR * kN <= 64 ? 64 : kR * kN <= 128 ? 128
+                      : kR * kN <= 256 ? 256 : 512;
   constexpr int operands = (kR + 2) * 2 * kTcPlaneA + 9 * 2 * kN * 16;
   constexpr int fit = 228 * 1024 / (512 / kCols + 1) + 2048;  // over (512 / kCols) CTAs per SM
   return operands > fit ? operands : fit;
@@ -865,9 +867,16 @@ int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w,
   (void)L;
   if (u->use_tc && cout % 32 == 0) {
     const int kn = cout % 128 == 0 ? 128 : (cout % 64 == 0 ? 64 : 32);
-    const int kr = u->tc_rows;
+    // rows per CTA: option "tcgen05_rows" (4 applies to tiles of up to 64 output channels; 128
+    // channels take 2, keeping two CTAs per SM within the TMEM columns)
+    const int kr = u->tc_rows == 4 && kn == 128 ? 2 : u->tc_rows;
     dim3 grid((wd + kTcM - 1) / kTcM, (h + kr - 1) / kr, n * (cout / kn));
-    if (kr == 2) {
+    if (kr == 4) {
+      if (kn == 64)
+        k_conv3x3_tc<64, 4><<<grid, 128, tc_smem_bytes<64, 4>(), u->stream>>>(a, u->d_err);
+      else
+        k_conv3x3_tc<32, 4><<<grid, 128, tc_smem_bytes<32, 4>(), u->stream>>>(a, u->d_err);
+    } else if (kr == 2) {
       if (kn == 128)
         k_conv3x3_tc<128, 2><<<grid, 128, tc_smem_bytes<128, 2>(), u->stream>>>(a, u->d_err);
       else if (kn == 64)
@@ -1200,6 +1209,12 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
       ea = cudaFuncSetAttribute(k_conv3x3_tc<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc_smem_bytes<32, 2>());
     if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tc<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc_smem_bytes<64, 4>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tc<32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tc_smem_bytes<32, 4>());
+    if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tc<32>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, wg_tc_smem_bytes<32>());
     if (ea == cudaSuccess)
@@ -1280,8 +1295,8 @@ int ds2d_unet_set_option(ds2d_unet *u, const char *key, long long value) {
     return DS2D_OK;
   }
   if (std::string(key) == "tcgen05_rows") {
-    if (value != 1 && value != 2)
-      return unet_fail(u, DS2D_E_ARG, "tcgen05_rows must be 1 or 2");
+    if (value != 1 && value != 2 && value != 4)
+      return unet_fail(u, DS2D_E_ARG, "tcgen05_rows must be 1, 2 or 4");
     u->tc_rows = (int)value;
     return DS2D_OK;
   }

@@ -135,7 +135,7 @@ def test_unet_tcgen05_weight_gradients_agree_with_mma_sync(cuda_device):
 
 
 def test_unet_tcgen05_two_rows_per_cta_equal_one(cuda_device):
-    """The tcgen05 convolution with two output rows per CTA (the staged weights of a chunk shared
+    """The tcgen05 convolution with two (or four) output rows per CTA (the staged weights of a chunk shared
     by both rows, one TMEM accumulator tile per row) against one row per CTA: every output sums
     the same products in the same order, so the forward pass agrees bit for bit, and the
     gradients up to the order of the weight gradient's split-K atomics; an odd row count at the
@@ -151,7 +151,7 @@ def test_unet_tcgen05_two_rows_per_cta_equal_one(cuda_device):
     with UNet(max_n=n, max_h=h, max_w=w) as net:
         net.set_params(flatten(p))
         net.set_option("tcgen05", 1)
-        for rows in (1, 2):
+        for rows in (1, 2, 4):
             net.set_option("tcgen05_rows", rows)
             y = torch.zeros_like(x)
             net.forward(x.data_ptr(), y.data_ptr(), n, h, w)
@@ -159,5 +159,6 @@ def test_unet_tcgen05_two_rows_per_cta_equal_one(cuda_device):
             out.append(y.cpu().numpy())
             _, g = net.loss_grad(x.data_ptr(), t.data_ptr(), n, h, w, want_grads=True)
             grads.append(g)
-    np.testing.assert_array_equal(out[1], out[0])
-    assert rel(grads[1], grads[0]) < 1e-5, rel(grads[1], grads[0])
+    for k in (1, 2):
+        np.testing.assert_array_equal(out[k], out[0])
+        assert rel(grads[k], grads[0]) < 1e-5, (k, rel(grads[k], grads[0]))
