@@ -17,6 +17,7 @@
 //   backward     dx[p][ci]   = sum_{tap,co} dz[p - tap][co] * W[tap][co][ci]  (= forward with the
 //                              flipped, transposed weights)
 //   weight grad  dW[tap][co][ci] = sum_p dz[p][co] * x[p + tap][ci]   (K = pixels, split over CTAs)
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched through the runtime)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -342,6 +343,203 @@ constexpr int tc_smem_bytes() {
 }
 
 // ---------------------------------------------------------------------------------------------
+// The same convolution fed by the tensor-memory accelerator through a kS-stage ring (option
+// "tcgen05_tma").  Per 16-channel chunk, one thread issues the tiled bulk-tensor loads of the
+// kR + 2 halo rows (box: 8 channels x 130 pixels per channel half, out-of-image pixels and rows
+// filled with zeros by the copy engine) and of the 9 x 2 weight planes (box: 8 input channels x
+// kN output channels) into a free stage, counted on the stage's "full" mbarrier; a second thread
+// waits for the stage, issues the stage's 9 kR UMMAs and commits them to its "empty" mbarrier,
+// which frees the stage for the loads kS chunks later.  The boxes land in the K-major no-swizzle
+// layout the descriptors of k_conv3x3_tc read (16-byte rows, one plane per channel half), so the
+// MMAs and the epilogue are that kernel's.  Every wait is bounded.
+// ---------------------------------------------------------------------------------------------
+constexpr int kTmaStages = 3;
+// A plane of a halo row in the ring: the 130 x 16-byte box rows, padded to a multiple of 128 bytes
+// so every bulk-tensor destination starts on a 128-byte boundary (the descriptors' LBO).
+constexpr int kTmaPlaneA = (kTcPlaneA + 127) / 128 * 128;
+// Bytes the loads of one stage deliver (the mbarrier's transaction count) and the stage's size.
+template <int kN, int kR>
+__host__ __device__ constexpr int tma_tx_bytes() {
+  return (kR + 2) * 2 * kTcPlaneA + 9 * 2 * kN * 16;
+}
+template <int kN, int kR>
+__host__ __device__ constexpr int tma_stage_bytes() {
+  return (kR + 2) * 2 * kTmaPlaneA + 9 * 2 * kN * 16;
+}
+template <int kN, int kR>
+__host__ __device__ constexpr int tma_smem_bytes() {
+  // stages, 1024-aligned, then the barriers (2 per stage + 1)
+  return kTmaStages * ((tma_stage_bytes<kN, kR>() + 1023) / 1024 * 1024) + 8 * (2 * kTmaStages + 1);
+}
+
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done = 0;
+  for (int spin = 0; spin < kTcSpin && !done; spin++) {
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+  }
+  return done != 0;
+}
+
+template <int kN, int kR>
+__global__ void __launch_bounds__(128) k_conv3x3_tma(ConvArgs a, const __grid_constant__ CUtensorMap tmA,
+                                                     const __grid_constant__ CUtensorMap tmB,
+                                                     int *err) {
+  extern __shared__ __align__(1024) unsigned char tm_smem[];
+  constexpr int kStage = (tma_stage_bytes<kN, kR>() + 1023) / 1024 * 1024;
+  uint64_t *full = reinterpret_cast<uint64_t *>(tm_smem + kTmaStages * kStage);
+  uint64_t *empty = full + kTmaStages;
+  uint64_t *done = empty + kTmaStages;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int w0 = blockIdx.x * kTcM, row0 = blockIdx.y * kR;
+  const int ngrp = a.cout / kN;
+  const int img = blockIdx.z / ngrp, co0 = (blockIdx.z % ngrp) * kN;
+  constexpr uint32_t kCols = kR * kN <= 32 ? 32 : kR * kN <= 64 ? 64 : kR * kN <= 128 ? 128
+                           : kR * kN <= 256 ? 256 : 512;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base)), "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int k = 0; k < 2 * kTmaStages + 1; k++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(full + k)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t idesc = umma_idesc(kTcM, kN);
+  const int nch = a.cin / 16;
+  if (tid == 0) {
+    // producer: tiled bulk-tensor loads of chunk c into stage c mod kS
+    const uint64_t ta = reinterpret_cast<uint64_t>(&tmA), tb = reinterpret_cast<uint64_t>(&tmB);
+    for (int c = 0; c < nch; c++) {
+      const int st = c % kTmaStages, k = c / kTmaStages;
+      if (c >= kTmaStages && !tc_wait(empty + st, (k - 1) & 1)) {
+        s_fail = 1;
+        break;
+      }
+      unsigned char *sA = tm_smem + st * kStage, *sB = sA + (kR + 2) * 2 * kTmaPlaneA;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                       smem_u32(full + st)),
+                   "r"((uint32_t)tma_tx_bytes<kN, kR>())
+                   : "memory");
+      const int ci0 = c * 16;
+      for (int r = 0; r < kR + 2; r++)
+        for (int kh = 0; kh < 2; kh++)
+          asm volatile(
+              "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+              " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(
+                  smem_u32(sA + (r * 2 + kh) * kTmaPlaneA)),
+              "l"(ta), "r"(ci0 + 8 * kh), "r"(w0 - 1), "r"(row0 + r - 1), "r"(img),
+              "r"(smem_u32(full + st))
+              : "memory");
+      for (int tap = 0; tap < 9; tap++)
+        for (int kh = 0; kh < 2; kh++)
+          asm volatile(
+              "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+              " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+                  smem_u32(sB + (tap * 2 + kh) * (kN * 16))),
+              "l"(tb), "r"(ci0 + 8 * kh), "r"(co0), "r"(tap), "r"(smem_u32(full + st))
+              : "memory");
+    }
+  } else if (tid == 32) {
+    // MMA issuer: the stage's 9 kR UMMAs, then a commit that frees the stage
+    for (int c = 0; c < nch; c++) {
+      const int st = c % kTmaStages, k = c / kTmaStages;
+      if (!tc_wait(full + st, k & 1)) {
+        s_fail = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint32_t a_base = smem_u32(tm_smem + st * kStage);
+      const uint32_t b_base = a_base + (kR + 2) * 2 * kTmaPlaneA;
+#pragma unroll
+      for (int j = 0; j < kR; j++)
+#pragma unroll
+        for (int tap = 0; tap < 9; tap++) {
+          const int ky = tap / 3, kx = tap % 3;
+          const uint64_t ad =
+              umma_desc(a_base + ((j + ky) * 2) * kTmaPlaneA + kx * 16, kTmaPlaneA, 128);
+          const uint64_t bd = umma_desc(b_base + (tap * 2) * (kN * 16), kN * 16, 128);
+          const uint32_t acc = (c > 0 || tap > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+                  tmem + (uint32_t)(j * kN)),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+        }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+              smem_u32(empty + st)));
+    }
+    // completion of every MMA issued
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+            smem_u32(done)));
+  }
+  bool ok = tc_wait(done, 0);
+  __syncwarp();
+  ok = __syncthreads_and(ok && !s_fail);
+  if (!ok && tid == 0) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  for (int j = 0; j < kR && ok; j++) {
+    const int row = row0 + j;
+    const int m = warp * 32 + lane;
+    const int ww = w0 + m;
+    const long long obase = (((long long)img * a.h + row) * a.w + ww) * a.ocs + a.oco + co0;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kN; c0 += 8) {
+      uint32_t r[8];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * kN + c0);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+            "=r"(r[7])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (ww < a.w && row < a.h) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          v[q] = __uint_as_float(r[q]) + (a.bias ? a.bias[co0 + c0 + q] : 0.f);
+          if (a.relu) v[q] = fmaxf(v[q], 0.f);
+        }
+        const long long o = obase + c0;
+        if (a.mask) {
+#pragma unroll
+          for (int q = 0; q < 8; q++)
+            if (!(__bfloat162float(a.mask[o + q]) > 0.f)) v[q] = 0.f;
+        }
+        __nv_bfloat162 pk[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) pk[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+        *reinterpret_cast<uint4 *>(a.out + o) = *reinterpret_cast<uint4 *>(pk);
+        if (a.out_f32) {
+#pragma unroll
+          for (int q = 0; q < 8; q++) a.out_f32[o + q] = v[q];
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Weight gradient dW[tap][co][ci] += sum_p dz[p][co] x[p + tap][ci] and bias gradient.  CTA:
 // 32 couts x 16*kCiT input channels, all 9 taps, over a contiguous range of 32-pixel row chunks
 // (split-K over CTAs, FP32 atomics at the end).  Operands are staged transposed (channel-major,
@@ -639,81 +837,329 @@ __global__ void __launch_bounds__(128) k_conv3x3_wgrad_tc(WgradArgs a, int *err)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Element-wise and small kernels
+// The weight gradient with both operands MN-major (option "tcgen05_wgrad_tma"): in the product
+// dW[tap][co][ci] = sum_p dz[p][co] x[p + tap][ci] the reduction runs over pixels, and the NHWC
+// activations hold the M (co) and N (ci) indices contiguous, so a tiled bulk-tensor box of
+// 8 channels x P pixels lands as one 8-channel column of the canonical MN-major no-swizzle layout
+// (16-byte rows of 8 channels, one per pixel; 8-pixel core matrices 128 bytes apart along K,
+// channel groups one box (x: one 128-byte-padded box) apart along M / N).  No transposition passes through the threads: one
+// thread issues the boxes of a 64-pixel row chunk into a kS-stage ring (dz: up to 16 channel
+// groups; x: the kN / 8 groups of 66 pixels, w0 - 1 .. w0 + 64, of row r + ky - 1, the copy engine
+// filling pixels and rows outside the image with zeros), a second thread issues the chunk's
+// 3 x 4 UMMAs (M 128 output channels, N kN input channels, K 16 pixels; the shift kx is a
+// 16-byte offset of the B descriptor along K) and commits them to the stage's "empty" barrier.
+// A CTA owns 128 output channels x kN input channels x the three taps of one kernel row and a
+// contiguous range of chunks (split-K, FP32 atomics at the end).  The bias gradient is
+// k_bias_grad's.  Every wait is bounded.
 // ---------------------------------------------------------------------------------------------
-// FP32 image [N][H][W] -> BF16 [N][H][W][16] (channel 0 = value, 1..15 = 0)
-__global__ void k_pack_input(const float *x, bf16 *out, long long npx) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= npx * 16) return;
-  out[i] = __float2bfloat16((i & 15) == 0 ? x[i >> 4] : 0.f);
+constexpr int kWtStages = 4;
+constexpr int kWtHalo = kWgP + 2;                // x pixels per chunk
+// ring space of one x box (66 pixels x 16 B), padded so every box lands on a 128-byte boundary
+constexpr int kWtXPlane = (kWtHalo * 16 + 127) / 128 * 128;
+template <int kN>
+__host__ __device__ constexpr int wt_stage_bytes() {
+  return ((16 * kWgP * 16 + (kN / 8) * kWtXPlane) + 1023) / 1024 * 1024;
+}
+template <int kN>
+__host__ __device__ constexpr int wt_smem_bytes() {
+  return kWtStages * wt_stage_bytes<kN>() + 8 * (2 * kWtStages + 1);
 }
 
-// 2x2 average pooling, [N][H][W][C] -> [N][H/2][W/2][C]
+template <int kN>
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad_tma(WgradArgs a,
+                                                           const __grid_constant__ CUtensorMap tmZ,
+                                                           const __grid_constant__ CUtensorMap tmX,
+                                                           int *err) {
+  extern __shared__ __align__(1024) unsigned char wt_smem[];
+  constexpr int kStage = wt_stage_bytes<kN>();
+  constexpr int kZBytes = 16 * kWgP * 16;   // dz: 16 channel groups x 64 pixels x 16 B
+  uint64_t *full = reinterpret_cast<uint64_t *>(wt_smem + kWtStages * kStage);
+  uint64_t *empty = full + kWtStages;
+  uint64_t *done = empty + kWtStages;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int co0 = blockIdx.x * kWgM;
+  const int ci0 = (blockIdx.y / 3) * kN, ky = blockIdx.y % 3;
+  const int gz = (a.cout - co0) / 8 < 16 ? (a.cout - co0) / 8 : 16;  // dz channel groups loaded
+  constexpr uint32_t kCols = 3 * kN <= 32 ? 32 : 3 * kN <= 64 ? 64 : 3 * kN <= 128 ? 128
+                           : 3 * kN <= 256 ? 256 : 512;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_base)), "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int k = 0; k < 2 * kWtStages + 1; k++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(full + k)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = tmem_base;
+  // both operands MN-major (instruction descriptor bits 15 and 16)
+  constexpr uint32_t idesc = umma_idesc(kWgM, kN) | (1u << 15) | (1u << 16);
+  const int wchunks = (a.w + kWgP - 1) / kWgP;
+  const long long total = (long long)a.n * a.h * wchunks;
+  const long long c_begin = (long long)blockIdx.z * a.chunks_per_cta;
+  const long long c_end = c_begin + a.chunks_per_cta < total ? c_begin + a.chunks_per_cta : total;
+  const int nck = c_end > c_begin ? (int)(c_end - c_begin) : 0;
+  if (tid == 0) {
+    // producer
+    const uint64_t tz = reinterpret_cast<uint64_t>(&tmZ), tx = reinterpret_cast<uint64_t>(&tmX);
+    const uint32_t tx_bytes = (uint32_t)(gz * kWgP * 16 + (kN / 8) * kWtHalo * 16);
+    for (int i = 0; i < nck; i++) {
+      const int st = i % kWtStages, k = i / kWtStages;
+      if (i >= kWtStages && !tc_wait(empty + st, (k - 1) & 1)) {
+        s_fail = 1;
+        break;
+      }
+      const long long cidx = c_begin + i;
+      const int wc = (int)(cidx % wchunks);
+      const long long rr = cidx / wchunks;
+      const int row = (int)(rr % a.h), img = (int)(rr / a.h);
+      const int w0 = wc * kWgP;
+      unsigned char *sZ = wt_smem + st * kStage, *sX = sZ + kZBytes;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                       smem_u32(full + st)),
+                   "r"(tx_bytes)
+                   : "memory");
+      for (int g = 0; g < gz; g++)
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(smem_u32(sZ + g * (kWgP * 16))),
+            "l"(tz), "r"(co0 + 8 * g), "r"(w0), "r"(row), "r"(img), "r"(smem_u32(full + st))
+            : "memory");
+      for (int g = 0; g < kN / 8; g++)
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(smem_u32(sX + g * kWtXPlane)),
+            "l"(tx), "r"(ci0 + 8 * g), "r"(w0 - 1), "r"(row + ky - 1), "r"(img),
+            "r"(smem_u32(full + st))
+            : "memory");
+    }
+  } else if (tid == 32) {
+    // MMA issuer
+    for (int i = 0; i < nck; i++) {
+      const int st = i % kWtStages, k = i / kWtStages;
+      if (!tc_wait(full + st, k & 1)) {
+        s_fail = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint32_t z_base = smem_u32(wt_smem + st * kStage);
+      const uint32_t x_base = z_base + kZBytes;
+#pragma unroll
+      for (int kx = 0; kx < 3; kx++)
+#pragma unroll
+        for (int s = 0; s < kWgP / 16; s++) {
+          const uint64_t ad = umma_desc(z_base + s * 256, 128, kWgP * 16);
+          const uint64_t bd = umma_desc(x_base + kx * 16 + s * 256, 128, kWtXPlane);
+          const uint32_t acc = (i > 0 || s > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+                  tmem + (uint32_t)(kx * kN)),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+        }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+              smem_u32(empty + st)));
+    }
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+            smem_u32(done)));
+  }
+  bool ok = tc_wait(done, 0);
+  __syncwarp();
+  ok = __syncthreads_and(ok && !s_fail);
+  if (!ok && tid == 0) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  if (ok && nck > 0) {
+    // epilogue: thread (warp w, lane l) owns output channel co0 + 32 w + l
+    const int co = co0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int kx = 0; kx < 3; kx++) {
+      float *dst = a.dw + ((long long)(ky * 3 + kx) * a.cout + co) * a.cin + ci0;
+#pragma unroll 1
+      for (int c0 = 0; c0 < kN; c0 += 8) {
+        uint32_t r[8];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kx * kN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+              "=r"(r[7])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (co < a.cout) {
+#pragma unroll
+          for (int j = 0; j < 8; j++) atomicAdd(dst + c0 + j, __uint_as_float(r[j]));
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols));
+  }
+}
+
+// Bias gradient db[co] += sum_p dz[p][co] (dz [P][zcs], cout channels): each thread sums one
+// 8-channel group over a strided set of pixels, then shared and global atomics.
+__global__ void __launch_bounds__(256) k_bias_grad(const bf16 *dz, int zcs, int cout, long long npx,
+                                                   float *db) {
+  __shared__ float s_db[512];  // cout <= 512 (base channels <= 64)
+  for (int i = threadIdx.x; i < cout; i += blockDim.x) s_db[i] = 0.f;
+  __syncthreads();
+  const int g = cout / 8, per = blockDim.x / g;  // threads per channel group
+  const int cg = threadIdx.x % g, lp = threadIdx.x / g;
+  float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (lp < per) {
+    for (long long p = (long long)blockIdx.x * per + lp; p < npx; p += (long long)gridDim.x * per) {
+      const uint4 v = *reinterpret_cast<const uint4 *>(dz + p * zcs + cg * 8);
+      const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+        acc[q] += __uint_as_float((q & 1) ? (wv[q >> 1] & 0xffff0000u) : (wv[q >> 1] << 16));
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) atomicAdd(&s_db[cg * 8 + q], acc[q]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < cout; i += blockDim.x) atomicAdd(db + i, s_db[i]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Element-wise and small kernels
+// ---------------------------------------------------------------------------------------------
+// The layout kernels below move 8 channels (16 bytes) per thread: a CTA row of threads covers
+// one image row (pixel x channel group), blockIdx.y strides over the rows of all images, so every
+// index is one 64-bit division per row and one 32-bit division per thread.  Channel counts are
+// multiples of 8 (base 32 or 64).  The arithmetic per element is the one of the scalar
+// definitions in the comments, in the same order.
+__device__ __forceinline__ uint4 ld16(const bf16 *p) { return *reinterpret_cast<const uint4 *>(p); }
+__device__ __forceinline__ void st16(bf16 *p, uint4 v) { *reinterpret_cast<uint4 *>(p) = v; }
+__device__ __forceinline__ float bfe(const uint4 &v, int q) {
+  const uint32_t w = (&v.x)[q >> 1];
+  return __uint_as_float((q & 1) ? (w & 0xffff0000u) : (w << 16));
+}
+__device__ __forceinline__ uint4 pack8(const float *f) {
+  uint4 v;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const __nv_bfloat162 b = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
+    (&v.x)[q] = *reinterpret_cast<const uint32_t *>(&b);
+  }
+  return v;
+}
+
+// FP32 image [N][H][W] -> BF16 [N][H][W][16] (channel 0 = value, 1..15 = 0)
+__global__ void k_pack_input(const float *x, bf16 *out, long long npx) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npx) return;
+  float f[8] = {x[p], 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  st16(out + p * 16, pack8(f));
+  st16(out + p * 16 + 8, make_uint4(0, 0, 0, 0));
+}
+
+// 2x2 average pooling, [N][H][W][C] -> [N][H/2][W/2][C]:
+// y = 0.25 (x[2y][2x] + x[2y][2x+1] + x[2y+1][2x] + x[2y+1][2x+1])
 __global__ void k_pool(const bf16 *x, bf16 *y, int n, int h, int w, int c) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int h2 = h / 2, w2 = w / 2;
-  if (i >= (long long)n * h2 * w2 * c) return;
-  const int ch = (int)(i % c);
-  long long r = i / c;
-  const int xx = (int)(r % w2), yy = (int)((r / w2) % h2), im = (int)(r / ((long long)w2 * h2));
-  const long long b = (((long long)im * h + 2 * yy) * w + 2 * xx) * c + ch;
-  const float s = __bfloat162float(x[b]) + __bfloat162float(x[b + c]) +
-                  __bfloat162float(x[b + (long long)w * c]) + __bfloat162float(x[b + (long long)w * c + c]);
-  y[i] = __float2bfloat16(0.25f * s);
+  const int h2 = h / 2, w2 = w / 2, g = c / 8;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w2 * g) return;
+  const int xx = t / g, cg = t - xx * g;
+  for (long long r = blockIdx.y; r < (long long)n * h2; r += gridDim.y) {
+    const long long im = r / h2;
+    const int yy = (int)(r - im * h2);
+    const long long b = ((im * h + 2 * yy) * w + 2 * xx) * c + cg * 8;
+    const uint4 v0 = ld16(x + b), v1 = ld16(x + b + c), v2 = ld16(x + b + (long long)w * c),
+                v3 = ld16(x + b + (long long)w * c + c);
+    float f[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) f[q] = 0.25f * (bfe(v0, q) + bfe(v1, q) + bfe(v2, q) + bfe(v3, q));
+    st16(y + (r * w2 + xx) * c + cg * 8, pack8(f));
+  }
 }
 
 // d(skip) = pool_grad(dy) * (s > 0) + extra, where extra (the skip's gradient through the
 // decoder concatenation, already masked) is read at channel offset `eco` of stride `ecs`.
 __global__ void k_pool_grad(const bf16 *dy, const bf16 *s, const bf16 *extra, int ecs, int eco,
                             bf16 *dx, int n, int h, int w, int c) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)n * h * w * c) return;
-  const int ch = (int)(i % c);
-  long long r = i / c;
-  const int xx = (int)(r % w), yy = (int)((r / w) % h), im = (int)(r / ((long long)w * h));
-  const long long j = (((long long)im * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c + ch;
-  float v = __bfloat162float(s[i]) > 0.f ? 0.25f * __bfloat162float(dy[j]) : 0.f;
-  if (extra) v += __bfloat162float(extra[r * ecs + eco + ch]);
-  dx[i] = __float2bfloat16(v);
+  const int g = c / 8;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w * g) return;
+  const int xx = t / g, cg = t - xx * g;
+  for (long long r = blockIdx.y; r < (long long)n * h; r += gridDim.y) {
+    const long long im = r / h;
+    const int yy = (int)(r - im * h);
+    const long long px = r * w + xx;
+    const long long j = ((im * (h / 2) + yy / 2) * (w / 2) + xx / 2) * c + cg * 8;
+    const uint4 vs = ld16(s + px * c + cg * 8), vd = ld16(dy + j);
+    uint4 ve = make_uint4(0, 0, 0, 0);
+    if (extra) ve = ld16(extra + px * ecs + eco + cg * 8);
+    float f[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      f[q] = bfe(vs, q) > 0.f ? 0.25f * bfe(vd, q) : 0.f;
+      if (extra) f[q] += bfe(ve, q);
+    }
+    st16(dx + px * c + cg * 8, pack8(f));
+  }
 }
 
 // Decoder input: out[.., 0:cu] = up2(u) (nearest), out[.., cu:cu+cs] = s; out [N][H][W][cu+cs]
 __global__ void k_up_concat(const bf16 *u, int cu, const bf16 *s, int cs, bf16 *out, int n, int h,
                             int w) {
-  const int c = cu + cs;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)n * h * w * c) return;
-  const int ch = (int)(i % c);
-  long long r = i / c;
-  const int xx = (int)(r % w), yy = (int)((r / w) % h), im = (int)(r / ((long long)w * h));
-  if (ch < cu)
-    out[i] = u[(((long long)im * (h / 2) + yy / 2) * (w / 2) + xx / 2) * cu + ch];
-  else
-    out[i] = s[r * cs + ch - cu];
+  const int gu = cu / 8, g = (cu + cs) / 8;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w * g) return;
+  const int xx = t / g, cg = t - xx * g;
+  for (long long r = blockIdx.y; r < (long long)n * h; r += gridDim.y) {
+    const long long im = r / h;
+    const int yy = (int)(r - im * h);
+    const long long px = r * w + xx;
+    const uint4 v = cg < gu ? ld16(u + ((im * (h / 2) + yy / 2) * (w / 2) + xx / 2) * cu + cg * 8)
+                            : ld16(s + px * cs + (cg - gu) * 8);
+    st16(out + px * (cu + cs) + cg * 8, v);
+  }
 }
 
 // d(u) = up2_grad(d(cat)[.., 0:cu]): sum of the 4 children
 __global__ void k_up_grad(const bf16 *dcat, int c, bf16 *du, int cu, int n, int h, int w) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int h2 = h / 2, w2 = w / 2;
-  if (i >= (long long)n * h2 * w2 * cu) return;
-  const int ch = (int)(i % cu);
-  long long r = i / cu;
-  const int xx = (int)(r % w2), yy = (int)((r / w2) % h2), im = (int)(r / ((long long)w2 * h2));
-  const long long b = (((long long)im * h + 2 * yy) * w + 2 * xx) * c + ch;
-  const float s = __bfloat162float(dcat[b]) + __bfloat162float(dcat[b + c]) +
-                  __bfloat162float(dcat[b + (long long)w * c]) +
-                  __bfloat162float(dcat[b + (long long)w * c + c]);
-  du[i] = __float2bfloat16(s);
+  const int h2 = h / 2, w2 = w / 2, g = cu / 8;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w2 * g) return;
+  const int xx = t / g, cg = t - xx * g;
+  for (long long r = blockIdx.y; r < (long long)n * h2; r += gridDim.y) {
+    const long long im = r / h2;
+    const int yy = (int)(r - im * h2);
+    const long long b = ((im * h + 2 * yy) * w + 2 * xx) * c + cg * 8;
+    const uint4 v0 = ld16(dcat + b), v1 = ld16(dcat + b + c), v2 = ld16(dcat + b + (long long)w * c),
+                v3 = ld16(dcat + b + (long long)w * c + c);
+    float f[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) f[q] = bfe(v0, q) + bfe(v1, q) + bfe(v2, q) + bfe(v3, q);
+    st16(du + (r * w2 + xx) * cu + cg * 8, pack8(f));
+  }
 }
 
-// 1x1 output convolution (c -> 1): y[p] = b + sum_c x[p][c] w[c]
-__global__ void k_out_fwd(const bf16 *x, const float *w, const float *b, float *y, long long npx,
-                          int c) {
+// 1x1 output convolution (c -> 1): y[p] = b + sum_c x[p][c] w[c], channels in ascending order
+template <int kC>
+__global__ void k_out_fwd(const bf16 *x, const float *w, const float *b, float *y, long long npx) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npx) return;
   float s = b[0];
-  for (int ch = 0; ch < c; ch++) s = fmaf(__bfloat162float(x[p * c + ch]), w[ch], s);
+#pragma unroll
+  for (int cg = 0; cg < kC / 8; cg++) {
+    const uint4 v = ld16(x + p * kC + cg * 8);
+#pragma unroll
+    for (int q = 0; q < 8; q++) s = fmaf(bfe(v, q), __ldg(w + cg * 8 + q), s);
+  }
   y[p] = s;
 }
 
@@ -736,27 +1182,51 @@ __global__ void k_mse(const float *y, const float *t, float *dy, long long npx, 
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
-// Backward of the 1x1 output convolution: dx[p][c] = dy[p] w[c] (x > 0), dw[c] += dy x, db += dy
-__global__ void k_out_bwd(const bf16 *x, const float *dy, const float *w, bf16 *dx, float *dw,
-                          float *db, long long npx, int c) {
-  __shared__ float s_dw[64];
-  __shared__ float s_db;
-  if (threadIdx.x < c) s_dw[threadIdx.x] = 0.f;
-  if (threadIdx.x == 0) s_db = 0.f;
+// Backward of the 1x1 output convolution: dx[p][c] = dy[p] w[c] (x > 0), dw[c] += dy x, db += dy.
+// Grid-stride over pixels with the kC + 1 sums in registers, reduced over the warp by shuffles,
+// over the CTA in shared memory, and once per CTA into the global gradients.
+template <int kC>
+__global__ void __launch_bounds__(256) k_out_bwd(const bf16 *x, const float *dy, const float *w,
+                                                 bf16 *dx, float *dw, float *db, long long npx) {
+  __shared__ float s_dw[kC + 1];
+  for (int i = threadIdx.x; i <= kC; i += blockDim.x) s_dw[i] = 0.f;
   __syncthreads();
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < npx) {
-    const float d = dy[p];
-    for (int ch = 0; ch < c; ch++) {
-      const float xv = __bfloat162float(x[p * c + ch]);
-      dx[p * c + ch] = __float2bfloat16(xv > 0.f ? d * w[ch] : 0.f);
-      atomicAdd(&s_dw[ch], d * xv);
-    }
-    atomicAdd(&s_db, d);
+  float acc[kC], accb = 0.f, wr[kC];
+#pragma unroll
+  for (int ch = 0; ch < kC; ch++) {
+    acc[ch] = 0.f;
+    wr[ch] = __ldg(w + ch);
   }
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npx;
+       p += (long long)gridDim.x * blockDim.x) {
+    const float d = dy[p];
+    accb += d;
+#pragma unroll
+    for (int cg = 0; cg < kC / 8; cg++) {
+      const uint4 v = ld16(x + p * kC + cg * 8);
+      float f[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const float xv = bfe(v, q);
+        f[q] = xv > 0.f ? d * wr[cg * 8 + q] : 0.f;
+        acc[cg * 8 + q] += d * xv;
+      }
+      st16(dx + p * kC + cg * 8, pack8(f));
+    }
+  }
+#pragma unroll
+  for (int ch = 0; ch < kC; ch++) {
+    float v = acc[ch];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_dw[ch], v);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) accb += __shfl_xor_sync(0xffffffffu, accb, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&s_dw[kC], accb);
   __syncthreads();
-  if (threadIdx.x < c) atomicAdd(dw + threadIdx.x, s_dw[threadIdx.x]);
-  if (threadIdx.x == 0) atomicAdd(db, s_db);
+  if (threadIdx.x < kC) atomicAdd(dw + threadIdx.x, s_dw[threadIdx.x]);
+  if (threadIdx.x == kC) atomicAdd(db, s_dw[kC]);
 }
 
 // Adam step on the FP32 master parameters (bias-corrected, as Kingma & Ba 2015).
@@ -796,6 +1266,11 @@ __global__ void k_fold_first(const float *g0, float *g, int rows, int cin_pad) {
 
 inline unsigned nblk(long long n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
+// Grid of the row-wise layout kernels: x covers one row's (pixel, channel group) pairs, y the rows.
+inline dim3 row_grid(long long rows, int per_row) {
+  return dim3(nblk(per_row), (unsigned)(rows < 65535 ? rows : 65535));
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------
@@ -831,7 +1306,9 @@ struct ds2d_unet {
   bool weights_dirty = true;
   int use_tc = 1;          // 3x3 convolutions on tcgen05 (1, default) or mma.sync (0)
   int tc_wgrad = 1;        // with use_tc: weight gradients on tcgen05 too (0: on mma.sync)
-  int tc_rows = 2;         // output rows per CTA of the tcgen05 convolution (1 or 2)
+  int tc_wgrad_tma = 1;    // the weight gradient with MN-major bulk-tensor operands
+  int tc_rows = 2;         // output rows per CTA of the tcgen05 convolution (1, 2 or 4)
+  int tc_tma = 1;          // the tcgen05 convolution fed by tiled bulk-tensor loads (k_conv3x3_tma)
   int *d_err = nullptr;    // device flag raised by a bounded wait that gave up
   std::vector<void *> allocs;
 };
@@ -860,11 +1337,88 @@ int ualloc(ds2d_unet *u, void **p, size_t bytes) {
   return DS2D_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+using TmEncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+TmEncodeFn tm_encode_fn() {
+  static TmEncodeFn fn = []() -> TmEncodeFn {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<TmEncodeFn>(p);
+  }();
+  return fn;
+}
+
+// Tensor maps of one convolution: the input [n][h][w][cin] (box 8 channels x 130 pixels, zero
+// fill outside the image) and the weights [9][cout][cin] (box 8 input x kn output channels).
+bool conv_tensor_maps(const ConvArgs &a, int kn, CUtensorMap *ta, CUtensorMap *tb) {
+  TmEncodeFn enc = tm_encode_fn();
+  if (!enc) return false;
+  const cuuint64_t dA[4] = {(cuuint64_t)a.cin, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
+  const cuuint64_t sA[3] = {(cuuint64_t)a.cin * 2, (cuuint64_t)a.w * a.cin * 2,
+                            (cuuint64_t)a.h * a.w * a.cin * 2};
+  const cuuint32_t bA[4] = {8, (cuuint32_t)kTcHalo, 1, 1}, e4[4] = {1, 1, 1, 1};
+  if (enc(ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.in, dA, sA, bA, e4,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  const cuuint64_t dB[3] = {(cuuint64_t)a.cin, (cuuint64_t)a.cout, 9};
+  const cuuint64_t sB[2] = {(cuuint64_t)a.cin * 2, (cuuint64_t)a.cout * a.cin * 2};
+  const cuuint32_t bB[3] = {8, (cuuint32_t)kn, 1}, e3[3] = {1, 1, 1};
+  return enc(tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)a.wt, dB, sB, bB, e3,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps of one weight gradient: dz [n][h][w][zcs] (cout channels; box 8 channels x 64
+// pixels) and x [n][h][w][cin] (box 8 channels x 66 pixels), zero fill outside the image.
+bool wgrad_tensor_maps(const WgradArgs &a, CUtensorMap *tz, CUtensorMap *tx) {
+  TmEncodeFn enc = tm_encode_fn();
+  if (!enc) return false;
+  const cuuint32_t e4[4] = {1, 1, 1, 1};
+  const cuuint64_t dZ[4] = {(cuuint64_t)a.cout, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
+  const cuuint64_t sZ[3] = {(cuuint64_t)a.zcs * 2, (cuuint64_t)a.w * a.zcs * 2,
+                            (cuuint64_t)a.h * a.w * a.zcs * 2};
+  const cuuint32_t bZ[4] = {8, (cuuint32_t)kWgP, 1, 1};
+  if (enc(tz, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.dz, dZ, sZ, bZ, e4,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  const cuuint64_t dX[4] = {(cuuint64_t)a.cin, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
+  const cuuint64_t sX[3] = {(cuuint64_t)a.cin * 2, (cuuint64_t)a.w * a.cin * 2,
+                            (cuuint64_t)a.h * a.w * a.cin * 2};
+  const cuuint32_t bX[4] = {8, (cuuint32_t)kWtHalo, 1, 1};
+  return enc(tx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.x, dX, sX, bX, e4,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w, int cin, int cout,
          const float *bias, bf16 *out, int ocs, int oco, float *out_f32, const bf16 *mask, int relu,
          int n, int h, int wd) {
   ConvArgs a{in, w, bias, out, out_f32, mask, n, h, wd, cin, cout, ocs, oco, relu};
   (void)L;
+  if (u->use_tc && u->tc_tma && cout % 32 == 0 && cin % 16 == 0) {
+    // tcgen05, operands by tiled bulk-tensor loads through a 3-stage ring, two rows per CTA
+    const int kn = cout % 128 == 0 ? 128 : (cout % 64 == 0 ? 64 : 32);
+    CUtensorMap ta, tb;
+    if (!conv_tensor_maps(a, kn, &ta, &tb))
+      return unet_fail(u, DS2D_E_CUDA, "conv: cuTensorMapEncodeTiled failed");
+    dim3 grid((wd + kTcM - 1) / kTcM, (h + 1) / 2, n * (cout / kn));
+    if (kn == 128)
+      k_conv3x3_tma<128, 2><<<grid, 128, tma_smem_bytes<128, 2>(), u->stream>>>(a, ta, tb, u->d_err);
+    else if (kn == 64)
+      k_conv3x3_tma<64, 2><<<grid, 128, tma_smem_bytes<64, 2>(), u->stream>>>(a, ta, tb, u->d_err);
+    else
+      k_conv3x3_tma<32, 2><<<grid, 128, tma_smem_bytes<32, 2>(), u->stream>>>(a, ta, tb, u->d_err);
+    UCK(cudaGetLastError());
+    return DS2D_OK;
+  }
   if (u->use_tc && cout % 32 == 0) {
     const int kn = cout % 128 == 0 ? 128 : (cout % 64 == 0 ? 64 : 32);
     // rows per CTA: option "tcgen05_rows" (4 applies to tiles of up to 64 output channels; 128
@@ -920,6 +1474,35 @@ int wgrad(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *dz, int zcs, cons
   // padded scratch that the caller folds
   if (L.cin_pad != L.cin && !dw_padded)
     return unet_fail(u, DS2D_E_STATE, "wgrad of a channel-padded layer needs a padded scratch");
+  if (u->use_tc && u->tc_wgrad && u->tc_wgrad_tma && L.cin_pad % 16 == 0 && L.cout % 32 == 0 &&
+      zcs % 8 == 0) {
+    // tcgen05, MN-major operands by tiled bulk-tensor loads: CTAs of 128 output channels x kN
+    // input channels x one kernel row over a range of 64-pixel chunks; bias by k_bias_grad
+    const int kn = L.cin_pad % 128 == 0 ? 128 : L.cin_pad % 64 == 0 ? 64 : L.cin_pad % 32 == 0 ? 32 : 16;
+    CUtensorMap tz, tx;
+    if (!wgrad_tensor_maps(a, &tz, &tx))
+      return unet_fail(u, DS2D_E_CUDA, "wgrad: cuTensorMapEncodeTiled failed");
+    const long long tchunks = (long long)n * h * ((wd + kWgP - 1) / kWgP);
+    const long long ttiles = (long long)((L.cout + kWgM - 1) / kWgM) * (L.cin_pad / kn) * 3;
+    long long ts = (4 * 148 + ttiles - 1) / ttiles;
+    ts = ts > tchunks ? tchunks : (ts < 1 ? 1 : ts);
+    a.chunks_per_cta = (int)((tchunks + ts - 1) / ts);
+    ts = (tchunks + a.chunks_per_cta - 1) / a.chunks_per_cta;
+    dim3 tgrid((L.cout + kWgM - 1) / kWgM, (L.cin_pad / kn) * 3, (unsigned)ts);
+    if (kn == 128)
+      k_conv3x3_wgrad_tma<128><<<tgrid, 128, wt_smem_bytes<128>(), u->stream>>>(a, tz, tx, u->d_err);
+    else if (kn == 64)
+      k_conv3x3_wgrad_tma<64><<<tgrid, 128, wt_smem_bytes<64>(), u->stream>>>(a, tz, tx, u->d_err);
+    else if (kn == 32)
+      k_conv3x3_wgrad_tma<32><<<tgrid, 128, wt_smem_bytes<32>(), u->stream>>>(a, tz, tx, u->d_err);
+    else
+      k_conv3x3_wgrad_tma<16><<<tgrid, 128, wt_smem_bytes<16>(), u->stream>>>(a, tz, tx, u->d_err);
+    const long long npx = (long long)n * h * wd;
+    const unsigned bb = nblk(npx * (L.cout / 8)) < 148u * 4 ? nblk(npx * (L.cout / 8)) : 148u * 4;
+    k_bias_grad<<<bb, 256, 0, u->stream>>>(dz, zcs, L.cout, npx, a.db);
+    UCK(cudaGetLastError());
+    return DS2D_OK;
+  }
   if (u->use_tc && u->tc_wgrad && L.cin_pad % 16 == 0) {
     // tcgen05: CTAs of 128 output channels x kN input channels x one kernel row, 64-pixel chunks
     const int kn = L.cin_pad % 32 == 0 ? 32 : 16;
@@ -985,7 +1568,7 @@ int forward(ds2d_unet *u, const float *x, int n, int h, int w) {
   if ((rc = refresh_weights(u))) return rc;
   using U = ds2d_unet;
   const long long npx = (long long)n * h * w;
-  k_pack_input<<<nblk(npx * 16), 256, 0, u->stream>>>(x, u->act[U::IN].p, npx);
+  k_pack_input<<<nblk(npx), 256, 0, u->stream>>>(x, u->act[U::IN].p, npx);
   const int c[4] = {u->base, 2 * u->base, 4 * u->base, 8 * u->base};
   const int ea[4] = {U::E1A, U::E2A, U::E3A, U::E4A}, eb[4] = {U::E1B, U::E2B, U::E3B, U::E4B};
   const int pl[3] = {U::P1, U::P2, U::P3};
@@ -999,8 +1582,8 @@ int forward(ds2d_unet *u, const float *x, int n, int h, int w) {
                    u->act[eb[l]].p, c[l], 0, nullptr, nullptr, 1, n, hh, ww)))
       return rc;
     if (l < 3) {
-      const long long np = (long long)n * (hh / 2) * (ww / 2) * c[l];
-      k_pool<<<nblk(np), 256, 0, u->stream>>>(u->act[eb[l]].p, u->act[pl[l]].p, n, hh, ww, c[l]);
+      k_pool<<<row_grid((long long)n * (hh / 2), (ww / 2) * (c[l] / 8)), 256, 0, u->stream>>>(
+          u->act[eb[l]].p, u->act[pl[l]].p, n, hh, ww, c[l]);
       src = pl[l];
       hh /= 2;
       ww /= 2;
@@ -1014,9 +1597,8 @@ int forward(ds2d_unet *u, const float *x, int n, int h, int w) {
     hh *= 2;
     ww *= 2;
     const int cc = cprev + c[l];
-    const long long np = (long long)n * hh * ww * cc;
-    k_up_concat<<<nblk(np), 256, 0, u->stream>>>(u->act[prev].p, cprev, u->act[eb[l]].p, c[l],
-                                                 u->act[ca[l]].p, n, hh, ww);
+    k_up_concat<<<row_grid((long long)n * hh, ww * (cc / 8)), 256, 0, u->stream>>>(
+        u->act[prev].p, cprev, u->act[eb[l]].p, c[l], u->act[ca[l]].p, n, hh, ww);
     const int li = 8 + 2 * (2 - l);
     const auto &La = u->layers[li], &Lb = u->layers[li + 1];
     if ((rc = conv(u, La, u->act[ca[l]].p, La.wf, cc, c[l], u->params + La.b_off, u->act[da[l]].p,
@@ -1029,8 +1611,12 @@ int forward(ds2d_unet *u, const float *x, int n, int h, int w) {
     cprev = c[l];
   }
   const auto &Lo = u->layers.back();
-  k_out_fwd<<<nblk(npx), 256, 0, u->stream>>>(u->act[U::D1B].p, u->params + Lo.w_off,
-                                              u->params + Lo.b_off, u->y, npx, c[0]);
+  if (c[0] == 32)
+    k_out_fwd<32><<<nblk(npx), 256, 0, u->stream>>>(u->act[U::D1B].p, u->params + Lo.w_off,
+                                                    u->params + Lo.b_off, u->y, npx);
+  else
+    k_out_fwd<64><<<nblk(npx), 256, 0, u->stream>>>(u->act[U::D1B].p, u->params + Lo.w_off,
+                                                    u->params + Lo.b_off, u->y, npx);
   UCK(cudaGetLastError());
   return DS2D_OK;
 }
@@ -1043,9 +1629,17 @@ int backward(ds2d_unet *u, int n, int h, int w) {
   const int c[4] = {u->base, 2 * u->base, 4 * u->base, 8 * u->base};
   UCK(cudaMemsetAsync(u->grads, 0, sizeof(float) * u->nparam, u->stream));
   const auto &Lo = u->layers.back();
-  k_out_bwd<<<nblk(npx), 256, 0, u->stream>>>(u->act[U::D1B].p, u->dy, u->params + Lo.w_off,
-                                              u->grad[U::D1B].p, u->grads + Lo.w_off,
-                                              u->grads + Lo.b_off, npx, c[0]);
+  {
+    const unsigned ob = nblk(npx) < 148u * 8 ? nblk(npx) : 148u * 8;  // grid-stride over pixels
+    if (c[0] == 32)
+      k_out_bwd<32><<<ob, 256, 0, u->stream>>>(u->act[U::D1B].p, u->dy, u->params + Lo.w_off,
+                                               u->grad[U::D1B].p, u->grads + Lo.w_off,
+                                               u->grads + Lo.b_off, npx);
+    else
+      k_out_bwd<64><<<ob, 256, 0, u->stream>>>(u->act[U::D1B].p, u->dy, u->params + Lo.w_off,
+                                               u->grad[U::D1B].p, u->grads + Lo.w_off,
+                                               u->grads + Lo.b_off, npx);
+  }
   const int ca[3] = {U::C1, U::C2, U::C3}, da[3] = {U::D1A, U::D2A, U::D3A},
             db[3] = {U::D1B, U::D2B, U::D3B};
   const int ea[4] = {U::E1A, U::E2A, U::E3A, U::E4A}, eb[4] = {U::E1B, U::E2B, U::E3B, U::E4B};
@@ -1069,9 +1663,8 @@ int backward(ds2d_unet *u, int n, int h, int w) {
       return rc;
     // up part -> gradient of the coarser level's output
     const int prev = l == 2 ? U::E4B : db[l + 1];
-    const long long np = (long long)n * (hh / 2) * (ww / 2) * cprev;
-    k_up_grad<<<nblk(np), 256, 0, u->stream>>>(u->grad[ca[l]].p, cc, u->grad[prev].p, cprev, n,
-                                                hh, ww);
+    k_up_grad<<<row_grid((long long)n * (hh / 2), (ww / 2) * (cprev / 8)), 256, 0, u->stream>>>(
+        u->grad[ca[l]].p, cc, u->grad[prev].p, cprev, n, hh, ww);
     hh /= 2;
     ww /= 2;
   }
@@ -1081,10 +1674,9 @@ int backward(ds2d_unet *u, int n, int h, int w) {
     if (l < 3) {
       // skip gradient: pool path (from level l+1's input) + concat path (channels cprev..)
       const int cprev = l == 2 ? c[3] : c[l + 1];
-      const long long np = (long long)n * hh * ww * c[l];
-      k_pool_grad<<<nblk(np), 256, 0, u->stream>>>(u->grad[pl[l]].p, u->act[eb[l]].p,
-                                                   u->grad[ca[l]].p, cprev + c[l], cprev,
-                                                   u->grad[eb[l]].p, n, hh, ww, c[l]);
+      k_pool_grad<<<row_grid((long long)n * hh, ww * (c[l] / 8)), 256, 0, u->stream>>>(
+          u->grad[pl[l]].p, u->act[eb[l]].p, u->grad[ca[l]].p, cprev + c[l], cprev,
+          u->grad[eb[l]].p, n, hh, ww, c[l]);
     }
     const int src = l == 0 ? U::IN : pl[l - 1];
     const int cin = l == 0 ? 16 : c[l - 1];
@@ -1212,6 +1804,15 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
       ea = cudaFuncSetAttribute(k_conv3x3_tc<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc_smem_bytes<64, 4>());
     if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tma<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tma_smem_bytes<128, 2>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tma<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tma_smem_bytes<64, 2>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_tma<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tma_smem_bytes<32, 2>());
+    if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_tc<32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc_smem_bytes<32, 4>());
     if (ea == cudaSuccess)
@@ -1220,6 +1821,18 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
     if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tc<16>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, wg_tc_smem_bytes<16>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tma<128>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem_bytes<128>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tma<64>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem_bytes<64>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tma<32>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem_bytes<32>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tma<16>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem_bytes<16>());
     if (ea != cudaSuccess)
       rc = unet_fail(u, DS2D_E_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
   }
@@ -1292,6 +1905,14 @@ int ds2d_unet_set_option(ds2d_unet *u, const char *key, long long value) {
   }
   if (std::string(key) == "tcgen05_wgrad") {
     u->tc_wgrad = value != 0;
+    return DS2D_OK;
+  }
+  if (std::string(key) == "tcgen05_wgrad_tma") {
+    u->tc_wgrad_tma = value != 0;
+    return DS2D_OK;
+  }
+  if (std::string(key) == "tcgen05_tma") {
+    u->tc_tma = value != 0;
     return DS2D_OK;
   }
   if (std::string(key) == "tcgen05_rows") {

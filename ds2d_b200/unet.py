@@ -92,7 +92,10 @@ class UNet:
 
     def set_option(self, key, value):
         """"tcgen05": 1 = 3x3 convolutions on tcgen05 / TMEM, 0 = mma.sync; "tcgen05_wgrad": 0
-        keeps the weight gradient on mma.sync; "tcgen05_rows": output rows per CTA (1 or 2)."""
+        keeps the weight gradient on mma.sync; "tcgen05_tma": 1 = convolution operands by tiled
+        bulk-tensor loads, 0 = staged by the threads with "tcgen05_rows" (1, 2 or 4) output rows
+        per CTA; "tcgen05_wgrad_tma": 1 = weight-gradient operands MN-major by bulk-tensor boxes,
+        0 = transposed through the threads."""
         self._check(self.lib.ds2d_unet_set_option(self.h, key.encode(), int(value)))
 
     def set_stream(self, stream_handle):

@@ -151,6 +151,7 @@ def test_unet_tcgen05_two_rows_per_cta_equal_one(cuda_device):
     with UNet(max_n=n, max_h=h, max_w=w) as net:
         net.set_params(flatten(p))
         net.set_option("tcgen05", 1)
+        net.set_option("tcgen05_tma", 0)  # rows per CTA of the thread-staged kernel
         for rows in (1, 2, 4):
             net.set_option("tcgen05_rows", rows)
             y = torch.zeros_like(x)
@@ -162,3 +163,69 @@ def test_unet_tcgen05_two_rows_per_cta_equal_one(cuda_device):
     for k in (1, 2):
         np.testing.assert_array_equal(out[k], out[0])
         assert rel(grads[k], grads[0]) < 1e-5, (k, rel(grads[k], grads[0]))
+
+
+def test_unet_tcgen05_tma_pipeline_equals_staged(cuda_device):
+    """The tcgen05 convolution fed by tiled bulk-tensor loads through a 3-stage mbarrier ring
+    (option tcgen05_tma; the copy engine fills the pixels outside the image with zeros) against
+    the same convolution staged by the threads: the same products summed in the same order, so
+    the forward pass agrees bit for bit and the gradients up to the weight gradient's split-K
+    atomics; then the pipelined network's gradients against the FP64 oracle."""
+    import torch
+    from ds2d_b200.unet import UNet, flatten, unflatten
+    p = uo.init_params(8)
+    rng = np.random.default_rng(8)
+    n, h, w = 2, 40, 200
+    x = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32) * 0.5).cuda()
+    out, grads = [], []
+    with UNet(max_n=n, max_h=h, max_w=w) as net:
+        net.set_params(flatten(p))
+        net.set_option("tcgen05", 1)
+        for tma in (0, 1):
+            net.set_option("tcgen05_tma", tma)
+            y = torch.zeros_like(x)
+            net.forward(x.data_ptr(), y.data_ptr(), n, h, w)
+            torch.cuda.synchronize()
+            out.append(y.cpu().numpy())
+            _, g = net.loss_grad(x.data_ptr(), t.data_ptr(), n, h, w, want_grads=True)
+            grads.append(g)
+    np.testing.assert_array_equal(out[1], out[0])
+    assert rel(grads[1], grads[0]) < 1e-5, rel(grads[1], grads[0])
+    ps, xs, ts = _case(seed=9)
+    ns, hs, ws = xs.shape[:3]
+    _, g_want, _ = uo.loss_and_grads(ps, xs, ts)
+    with UNet(max_n=ns, max_h=hs, max_w=ws) as net:
+        net.set_option("tcgen05_tma", 1)
+        net.set_params(flatten(ps))
+        dx = torch.from_numpy(xs[..., 0].astype(np.float32)).cuda()
+        dt = torch.from_numpy(ts[..., 0].astype(np.float32)).cuda()
+        _, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), ns, hs, ws, want_grads=True)
+    assert rel(g, flatten(g_want)) < GRAD_GATE_TOTAL, rel(g, flatten(g_want))
+
+
+def test_unet_mn_major_weight_gradients_agree_with_mma_sync(cuda_device):
+    """The weight and bias gradients of every layer from the tcgen05 kernel fed MN-major by tiled
+    bulk-tensor boxes (option tcgen05_wgrad_tma: input-channel tiles of 16, 32, 64 and 128 over
+    the network's layers, two 128-channel output tiles on the 256-channel layers, 64-pixel chunks
+    with a ragged last one on the 200-pixel rows) against the mma.sync kernel: the same BF16
+    products summed in FP32, equal up to summation order."""
+    import torch
+    from ds2d_b200.unet import UNet, flatten, unflatten
+    p = uo.init_params(10)
+    rng = np.random.default_rng(10)
+    n, h, w = 2, 24, 200
+    x = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32) * 0.5).cuda()
+    grads = []
+    with UNet(max_n=n, max_h=h, max_w=w) as net:
+        net.set_params(flatten(p))
+        net.set_option("tcgen05", 1)
+        for tc, tma in ((0, 0), (1, 1)):
+            net.set_option("tcgen05_wgrad", tc)
+            net.set_option("tcgen05_wgrad_tma", tma)
+            _, g = net.loss_grad(x.data_ptr(), t.data_ptr(), n, h, w, want_grads=True)
+            grads.append(unflatten(g))
+    for k, v in grads[0].items():
+        if np.linalg.norm(v) > 0:
+            assert rel(grads[1][k], v) < 1e-4, (k, rel(grads[1][k], v))
