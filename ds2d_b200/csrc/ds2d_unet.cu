@@ -346,14 +346,14 @@ constexpr int tc_smem_bytes() {
 // The same convolution fed by the tensor-memory accelerator through a kS-stage ring (option
 // "tcgen05_tma").  Per 16-channel chunk, one thread issues the tiled bulk-tensor loads of the
 // kR + 2 halo rows (box: 8 channels x 130 pixels per channel half, out-of-image pixels and rows
-// filled with zeros by the copy engine) and of the 9 x 2 weight planes (box: 8 input channels x
-// kN output channels) into a free stage, counted on the stage's "full" mbarrier; a second thread
+// filled with zeros by the copy engine) and of the 9 x 2 weight planes (one box of the blocked
+// weights: 8 input channels x kN output channels x 18 planes) into a free stage, counted on the
+// stage's "full" mbarrier; a second thread
 // waits for the stage, issues the stage's 9 kR UMMAs and commits them to its "empty" mbarrier,
 // which frees the stage for the loads kS chunks later.  The boxes land in the K-major no-swizzle
 // layout the descriptors of k_conv3x3_tc read (16-byte rows, one plane per channel half), so the
 // MMAs and the epilogue are that kernel's.  Every wait is bounded.
 // ---------------------------------------------------------------------------------------------
-constexpr int kTmaStages = 3;
 // A plane of a halo row in the ring: the 130 x 16-byte box rows, padded to a multiple of 128 bytes
 // so every bulk-tensor destination starts on a 128-byte boundary (the descriptors' LBO).
 constexpr int kTmaPlaneA = (kTcPlaneA + 127) / 128 * 128;
@@ -366,10 +366,10 @@ template <int kN, int kR>
 __host__ __device__ constexpr int tma_stage_bytes() {
   return (kR + 2) * 2 * kTmaPlaneA + 9 * 2 * kN * 16;
 }
-template <int kN, int kR>
+template <int kN, int kR, int kS>
 __host__ __device__ constexpr int tma_smem_bytes() {
   // stages, 1024-aligned, then the barriers (2 per stage + 1)
-  return kTmaStages * ((tma_stage_bytes<kN, kR>() + 1023) / 1024 * 1024) + 8 * (2 * kTmaStages + 1);
+  return kS * ((tma_stage_bytes<kN, kR>() + 1023) / 1024 * 1024) + 8 * (2 * kS + 1);
 }
 
 __device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity) {
@@ -385,15 +385,15 @@ __device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity) {
   return done != 0;
 }
 
-template <int kN, int kR>
+template <int kN, int kR, int kS>
 __global__ void __launch_bounds__(128) k_conv3x3_tma(ConvArgs a, const __grid_constant__ CUtensorMap tmA,
                                                      const __grid_constant__ CUtensorMap tmB,
                                                      int *err) {
   extern __shared__ __align__(1024) unsigned char tm_smem[];
   constexpr int kStage = (tma_stage_bytes<kN, kR>() + 1023) / 1024 * 1024;
-  uint64_t *full = reinterpret_cast<uint64_t *>(tm_smem + kTmaStages * kStage);
-  uint64_t *empty = full + kTmaStages;
-  uint64_t *done = empty + kTmaStages;
+  uint64_t *full = reinterpret_cast<uint64_t *>(tm_smem + kS * kStage);
+  uint64_t *empty = full + kS;
+  uint64_t *done = empty + kS;
   __shared__ uint32_t tmem_base;
   __shared__ int s_fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(128) k_conv3x3_tma(ConvArgs a, const __grid_co
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    for (int k = 0; k < 2 * kTmaStages + 1; k++)
+    for (int k = 0; k < 2 * kS + 1; k++)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(full + k)));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_fail = 0;
@@ -423,8 +423,8 @@ __global__ void __launch_bounds__(128) k_conv3x3_tma(ConvArgs a, const __grid_co
     // producer: tiled bulk-tensor loads of chunk c into stage c mod kS
     const uint64_t ta = reinterpret_cast<uint64_t>(&tmA), tb = reinterpret_cast<uint64_t>(&tmB);
     for (int c = 0; c < nch; c++) {
-      const int st = c % kTmaStages, k = c / kTmaStages;
-      if (c >= kTmaStages && !tc_wait(empty + st, (k - 1) & 1)) {
+      const int st = c % kS, k = c / kS;
+      if (c >= kS && !tc_wait(empty + st, (k - 1) & 1)) {
         s_fail = 1;
         break;
       }
@@ -443,19 +443,17 @@ __global__ void __launch_bounds__(128) k_conv3x3_tma(ConvArgs a, const __grid_co
               "l"(ta), "r"(ci0 + 8 * kh), "r"(w0 - 1), "r"(row0 + r - 1), "r"(img),
               "r"(smem_u32(full + st))
               : "memory");
-      for (int tap = 0; tap < 9; tap++)
-        for (int kh = 0; kh < 2; kh++)
-          asm volatile(
-              "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-              " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
-                  smem_u32(sB + (tap * 2 + kh) * (kN * 16))),
-              "l"(tb), "r"(ci0 + 8 * kh), "r"(co0), "r"(tap), "r"(smem_u32(full + st))
-              : "memory");
+      // the chunk's 9 x 2 weight planes of this output tile: one box of the blocked weights
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(sB)),
+          "l"(tb), "r"(0), "r"(co0), "r"(18 * c), "r"(smem_u32(full + st))
+          : "memory");
     }
   } else if (tid == 32) {
     // MMA issuer: the stage's 9 kR UMMAs, then a commit that frees the stage
     for (int c = 0; c < nch; c++) {
-      const int st = c % kTmaStages, k = c / kTmaStages;
+      const int st = c % kS, k = c / kS;
       if (!tc_wait(full + st, k & 1)) {
         s_fail = 1;
         break;
@@ -1243,17 +1241,29 @@ __global__ void k_adam(float *p, const float *g, float *m, float *v, long long n
 }
 
 // BF16 weight copies from the FP32 master [tap][co][ci_real]: forward [tap][co][cin_pad] and
-// backward-data [tap'][ci][co] with tap' = 8 - tap (spatial flip).
+// backward-data [tap'][ci][co] with tap' = 8 - tap (spatial flip), and both blocked for the
+// bulk-tensor-fed convolution as [16-channel input chunk][tap][8-channel half][output ch][8], so
+// the B operand of one chunk and output tile (18 planes of kN x 16 bytes) is one box.
 __global__ void k_weights_bf16(const float *w, int k2, int co_n, int ci_real, int cin_pad,
-                               bf16 *wf, bf16 *wb) {
+                               bf16 *wf, bf16 *wb, bf16 *wfb, bf16 *wbb) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)k2 * co_n * cin_pad) return;
   const int ci = (int)(i % cin_pad);
   const int co = (int)((i / cin_pad) % co_n);
   const int tap = (int)(i / ((long long)cin_pad * co_n));
   const float v = ci < ci_real ? w[((long long)tap * co_n + co) * ci_real + ci] : 0.f;
-  wf[i] = __float2bfloat16(v);
-  if (wb && ci < ci_real) wb[((long long)(k2 - 1 - tap) * ci_real + ci) * co_n + co] = __float2bfloat16(v);
+  const bf16 b = __float2bfloat16(v);
+  wf[i] = b;
+  // blocked [ci / 16][tap][(ci / 8) & 1][co][ci & 7] (cin_pad a multiple of 16)
+  if (wfb && cin_pad % 16 == 0)
+    wfb[(((long long)(ci / 16) * k2 + tap) * 2 + ((ci >> 3) & 1)) * co_n * 8 + co * 8 + (ci & 7)] = b;
+  if (ci < ci_real) {
+    const int tb = k2 - 1 - tap;
+    if (wb) wb[((long long)tb * ci_real + ci) * co_n + co] = b;
+    // backward-data weights blocked the same way, input channels = co, output channels = ci
+    if (wbb && co_n % 16 == 0)
+      wbb[(((long long)(co / 16) * k2 + tb) * 2 + ((co >> 3) & 1)) * ci_real * 8 + ci * 8 + (co & 7)] = b;
+  }
 }
 
 constexpr int kRedBlocks = 296;
@@ -1282,6 +1292,8 @@ struct ds2d_unet {
     int cin, cout, k, cin_pad;
     long long w_off, b_off, nw;  // offsets into the flat FP32 parameter vector
     bf16 *wf = nullptr, *wb = nullptr;  // BF16 forward / backward-data weights
+    // the same, blocked for the bulk-tensor-fed convolution: [cin/16][9][2][cout][8]
+    bf16 *wfb = nullptr, *wbb = nullptr;
   };
   struct Act {
     bf16 *p = nullptr;
@@ -1307,8 +1319,9 @@ struct ds2d_unet {
   int use_tc = 1;          // 3x3 convolutions on tcgen05 (1, default) or mma.sync (0)
   int tc_wgrad = 1;        // with use_tc: weight gradients on tcgen05 too (0: on mma.sync)
   int tc_wgrad_tma = 1;    // the weight gradient with MN-major bulk-tensor operands
-  int tc_rows = 2;         // output rows per CTA of the tcgen05 convolution (1, 2 or 4)
+  int tc_rows = 4;         // output rows per CTA of the tcgen05 convolution (1, 2 or 4)
   int tc_tma = 1;          // the tcgen05 convolution fed by tiled bulk-tensor loads (k_conv3x3_tma)
+  int tc_stages = 2;       // ring stages of k_conv3x3_tma (2 or 3)
   int *d_err = nullptr;    // device flag raised by a bounded wait that gave up
   std::vector<void *> allocs;
 };
@@ -1355,8 +1368,10 @@ TmEncodeFn tm_encode_fn() {
 }
 
 // Tensor maps of one convolution: the input [n][h][w][cin] (box 8 channels x 130 pixels, zero
-// fill outside the image) and the weights [9][cout][cin] (box 8 input x kn output channels).
-bool conv_tensor_maps(const ConvArgs &a, int kn, CUtensorMap *ta, CUtensorMap *tb) {
+// fill outside the image) and the blocked weights [cin/16][9][2][cout][8] viewed as
+// {8, cout, 18 cin/16} (box 8 x kn x 18: the whole B operand of a chunk and output tile).
+bool conv_tensor_maps(const ConvArgs &a, const bf16 *wblk, int kn, CUtensorMap *ta,
+                      CUtensorMap *tb) {
   TmEncodeFn enc = tm_encode_fn();
   if (!enc) return false;
   const cuuint64_t dA[4] = {(cuuint64_t)a.cin, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
@@ -1367,10 +1382,10 @@ bool conv_tensor_maps(const ConvArgs &a, int kn, CUtensorMap *ta, CUtensorMap *t
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
-  const cuuint64_t dB[3] = {(cuuint64_t)a.cin, (cuuint64_t)a.cout, 9};
-  const cuuint64_t sB[2] = {(cuuint64_t)a.cin * 2, (cuuint64_t)a.cout * a.cin * 2};
-  const cuuint32_t bB[3] = {8, (cuuint32_t)kn, 1}, e3[3] = {1, 1, 1};
-  return enc(tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)a.wt, dB, sB, bB, e3,
+  const cuuint64_t dB[3] = {8, (cuuint64_t)a.cout, (cuuint64_t)18 * (a.cin / 16)};
+  const cuuint64_t sB[2] = {16, (cuuint64_t)a.cout * 16};
+  const cuuint32_t bB[3] = {8, (cuuint32_t)kn, 18}, e3[3] = {1, 1, 1};
+  return enc(tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)wblk, dB, sB, bB, e3,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -1398,24 +1413,48 @@ bool wgrad_tensor_maps(const WgradArgs &a, CUtensorMap *tz, CUtensorMap *tx) {
              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+template <int kN, int kR, int kS>
+void launch_tma(dim3 grid, const ConvArgs &a, const CUtensorMap &ta, const CUtensorMap &tb,
+                ds2d_unet *u) {
+  k_conv3x3_tma<kN, kR, kS><<<grid, 128, tma_smem_bytes<kN, kR, kS>(), u->stream>>>(a, ta, tb,
+                                                                                    u->d_err);
+}
+
+template <int kN, int kR, int kS>
+cudaError_t tma_attr() {
+  return cudaFuncSetAttribute(k_conv3x3_tma<kN, kR, kS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              tma_smem_bytes<kN, kR, kS>());
+}
+
 int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w, int cin, int cout,
          const float *bias, bf16 *out, int ocs, int oco, float *out_f32, const bf16 *mask, int relu,
          int n, int h, int wd) {
   ConvArgs a{in, w, bias, out, out_f32, mask, n, h, wd, cin, cout, ocs, oco, relu};
-  (void)L;
   if (u->use_tc && u->tc_tma && cout % 32 == 0 && cin % 16 == 0) {
     // tcgen05, operands by tiled bulk-tensor loads through a 3-stage ring, two rows per CTA
     const int kn = cout % 128 == 0 ? 128 : (cout % 64 == 0 ? 64 : 32);
+    const bf16 *wblk = w == L.wf ? L.wfb : (w == L.wb ? L.wbb : nullptr);
     CUtensorMap ta, tb;
-    if (!conv_tensor_maps(a, kn, &ta, &tb))
+    if (!wblk || !conv_tensor_maps(a, wblk, kn, &ta, &tb))
       return unet_fail(u, DS2D_E_CUDA, "conv: cuTensorMapEncodeTiled failed");
-    dim3 grid((wd + kTcM - 1) / kTcM, (h + 1) / 2, n * (cout / kn));
-    if (kn == 128)
-      k_conv3x3_tma<128, 2><<<grid, 128, tma_smem_bytes<128, 2>(), u->stream>>>(a, ta, tb, u->d_err);
-    else if (kn == 64)
-      k_conv3x3_tma<64, 2><<<grid, 128, tma_smem_bytes<64, 2>(), u->stream>>>(a, ta, tb, u->d_err);
-    else
-      k_conv3x3_tma<32, 2><<<grid, 128, tma_smem_bytes<32, 2>(), u->stream>>>(a, ta, tb, u->d_err);
+    // rows per CTA: 4 with option "tcgen05_rows" 4, else 2; ring stages: option "tcgen05_stages"
+    const int kr = u->tc_rows == 4 ? 4 : 2, ks = u->tc_stages;
+    dim3 grid((wd + kTcM - 1) / kTcM, (h + kr - 1) / kr, n * (cout / kn));
+    const int v = (kn == 128 ? 0 : kn == 64 ? 4 : 8) + (kr == 4 ? 2 : 0) + (ks == 2 ? 1 : 0);
+    switch (v) {
+      case 0: launch_tma<128, 2, 3>(grid, a, ta, tb, u); break;
+      case 1: launch_tma<128, 2, 2>(grid, a, ta, tb, u); break;
+      case 2: launch_tma<128, 4, 3>(grid, a, ta, tb, u); break;
+      case 3: launch_tma<128, 4, 2>(grid, a, ta, tb, u); break;
+      case 4: launch_tma<64, 2, 3>(grid, a, ta, tb, u); break;
+      case 5: launch_tma<64, 2, 2>(grid, a, ta, tb, u); break;
+      case 6: launch_tma<64, 4, 3>(grid, a, ta, tb, u); break;
+      case 7: launch_tma<64, 4, 2>(grid, a, ta, tb, u); break;
+      case 8: launch_tma<32, 2, 3>(grid, a, ta, tb, u); break;
+      case 9: launch_tma<32, 2, 2>(grid, a, ta, tb, u); break;
+      case 10: launch_tma<32, 4, 3>(grid, a, ta, tb, u); break;
+      default: launch_tma<32, 4, 2>(grid, a, ta, tb, u); break;
+    }
     UCK(cudaGetLastError());
     return DS2D_OK;
   }
@@ -1535,7 +1574,7 @@ int refresh_weights(ds2d_unet *u) {
     if (L.k != 3) continue;
     const long long n = 9LL * L.cout * L.cin_pad;
     k_weights_bf16<<<nblk(n), 256, 0, u->stream>>>(u->params + L.w_off, 9, L.cout, L.cin,
-                                                   L.cin_pad, L.wf, L.wb);
+                                                   L.cin_pad, L.wf, L.wb, L.wfb, L.wbb);
   }
   UCK(cudaGetLastError());
   u->weights_dirty = false;
@@ -1759,6 +1798,8 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
     if (L.k == 3) {
       A((void **)&L.wf, sizeof(bf16) * 9 * L.cout * L.cin_pad);
       A((void **)&L.wb, sizeof(bf16) * 9 * L.cout * L.cin);
+      A((void **)&L.wfb, sizeof(bf16) * 9 * L.cout * L.cin_pad);
+      A((void **)&L.wbb, sizeof(bf16) * 9 * L.cout * L.cin);
     }
   using U = ds2d_unet;
   const long long px0 = (long long)max_n * max_h * max_w;
@@ -1803,15 +1844,11 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
     if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_tc<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc_smem_bytes<64, 4>());
-    if (ea == cudaSuccess)
-      ea = cudaFuncSetAttribute(k_conv3x3_tma<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tma_smem_bytes<128, 2>());
-    if (ea == cudaSuccess)
-      ea = cudaFuncSetAttribute(k_conv3x3_tma<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tma_smem_bytes<64, 2>());
-    if (ea == cudaSuccess)
-      ea = cudaFuncSetAttribute(k_conv3x3_tma<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tma_smem_bytes<32, 2>());
+    for (cudaError_t (*f)() : {tma_attr<128, 2, 3>, tma_attr<128, 2, 2>, tma_attr<128, 4, 3>,
+                              tma_attr<128, 4, 2>, tma_attr<64, 2, 3>, tma_attr<64, 2, 2>,
+                              tma_attr<64, 4, 3>, tma_attr<64, 4, 2>, tma_attr<32, 2, 3>,
+                              tma_attr<32, 2, 2>, tma_attr<32, 4, 3>, tma_attr<32, 4, 2>})
+      if (ea == cudaSuccess) ea = f();
     if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_tc<32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 tc_smem_bytes<32, 4>());
@@ -1913,6 +1950,12 @@ int ds2d_unet_set_option(ds2d_unet *u, const char *key, long long value) {
   }
   if (std::string(key) == "tcgen05_tma") {
     u->tc_tma = value != 0;
+    return DS2D_OK;
+  }
+  if (std::string(key) == "tcgen05_stages") {
+    if (value != 2 && value != 3)
+      return unet_fail(u, DS2D_E_ARG, "tcgen05_stages must be 2 or 3");
+    u->tc_stages = (int)value;
     return DS2D_OK;
   }
   if (std::string(key) == "tcgen05_rows") {

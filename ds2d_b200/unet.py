@@ -93,8 +93,8 @@ class UNet:
     def set_option(self, key, value):
         """"tcgen05": 1 = 3x3 convolutions on tcgen05 / TMEM, 0 = mma.sync; "tcgen05_wgrad": 0
         keeps the weight gradient on mma.sync; "tcgen05_tma": 1 = convolution operands by tiled
-        bulk-tensor loads, 0 = staged by the threads with "tcgen05_rows" (1, 2 or 4) output rows
-        per CTA; "tcgen05_wgrad_tma": 1 = weight-gradient operands MN-major by bulk-tensor boxes,
+        bulk-tensor loads through a ring of "tcgen05_stages" (2 or 3) stages, 0 = staged by the
+        threads; "tcgen05_rows": output rows per CTA (1, 2 or 4); "tcgen05_wgrad_tma": 1 = weight-gradient operands MN-major by bulk-tensor boxes,
         0 = transposed through the threads."""
         self._check(self.lib.ds2d_unet_set_option(self.h, key.encode(), int(value)))
 

@@ -269,10 +269,12 @@ int ds2d_unet_adam_step(ds2d_unet *net, float lr, float beta1, float beta2, floa
 /* "tcgen05" = 1 (default) runs the 3x3 convolutions (forward, backward-data and weight gradient)
  * on the 5th-generation tensor cores with TMEM accumulators; 0 runs all three on mma.sync.
  * "tcgen05_wgrad" = 0 keeps only the weight gradient on mma.sync (default 1).  "tcgen05_tma" = 1
- * (default) feeds the tcgen05 convolution by tiled bulk-tensor loads through a 3-stage ring (two
- * output rows per CTA); 0 stages the operands through the threads with "tcgen05_rows" = 1, 2
- * (default) or 4 output rows per CTA.  "tcgen05_wgrad_tma" = 1 (default) loads the weight
- * gradient's operands MN-major by bulk-tensor boxes; 0 transposes them through the threads. */
+ * (default) feeds the tcgen05 convolution by tiled bulk-tensor loads through a ring of
+ * "tcgen05_stages" = 2 (default) or 3 stages; 0 stages the operands through the threads.
+ * "tcgen05_rows" = 1, 2 or 4 (default) output rows per CTA (the bulk-tensor kernel takes 2 or 4;
+ * the thread-staged one keeps 2 for 128-channel tiles).  "tcgen05_wgrad_tma" = 1 (default) loads
+ * the weight gradient's operands MN-major by bulk-tensor boxes; 0 transposes them through the
+ * threads. */
 int ds2d_unet_set_option(ds2d_unet *net, const char *key, long long value);
 
 #ifdef __cplusplus

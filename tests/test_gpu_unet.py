@@ -125,6 +125,7 @@ def test_unet_tcgen05_weight_gradients_agree_with_mma_sync(cuda_device):
     with UNet(max_n=n, max_h=h, max_w=w) as net:
         net.set_params(flatten(p))
         net.set_option("tcgen05", 1)
+        net.set_option("tcgen05_wgrad_tma", 0)  # the kernel that transposes through the threads
         for tc in (0, 1):
             net.set_option("tcgen05_wgrad", tc)
             _, g = net.loss_grad(x.data_ptr(), t.data_ptr(), n, h, w, want_grads=True)
@@ -167,8 +168,9 @@ def test_unet_tcgen05_two_rows_per_cta_equal_one(cuda_device):
 
 def test_unet_tcgen05_tma_pipeline_equals_staged(cuda_device):
     """The tcgen05 convolution fed by tiled bulk-tensor loads through a 3-stage mbarrier ring
-    (option tcgen05_tma; the copy engine fills the pixels outside the image with zeros) against
-    the same convolution staged by the threads: the same products summed in the same order, so
+    (option tcgen05_tma; the copy engine fills the pixels outside the image with zeros; two or
+    four rows per CTA, two or three ring stages) against the same convolution staged by the
+    threads: the same products summed in the same order, so
     the forward pass agrees bit for bit and the gradients up to the weight gradient's split-K
     atomics; then the pipelined network's gradients against the FP64 oracle."""
     import torch
@@ -179,19 +181,24 @@ def test_unet_tcgen05_tma_pipeline_equals_staged(cuda_device):
     x = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32)).cuda()
     t = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32) * 0.5).cuda()
     out, grads = [], []
+    # (bulk-tensor loads, rows per CTA, ring stages): the thread-staged kernel first
+    variants = ((0, 2, 3), (1, 2, 3), (1, 2, 2), (1, 4, 3), (1, 4, 2))
     with UNet(max_n=n, max_h=h, max_w=w) as net:
         net.set_params(flatten(p))
         net.set_option("tcgen05", 1)
-        for tma in (0, 1):
+        for tma, rows, stages in variants:
             net.set_option("tcgen05_tma", tma)
+            net.set_option("tcgen05_rows", rows)
+            net.set_option("tcgen05_stages", stages)
             y = torch.zeros_like(x)
             net.forward(x.data_ptr(), y.data_ptr(), n, h, w)
             torch.cuda.synchronize()
             out.append(y.cpu().numpy())
             _, g = net.loss_grad(x.data_ptr(), t.data_ptr(), n, h, w, want_grads=True)
             grads.append(g)
-    np.testing.assert_array_equal(out[1], out[0])
-    assert rel(grads[1], grads[0]) < 1e-5, rel(grads[1], grads[0])
+    for k in range(1, len(variants)):
+        np.testing.assert_array_equal(out[k], out[0], err_msg=str(variants[k]))
+        assert rel(grads[k], grads[0]) < 1e-5, (variants[k], rel(grads[k], grads[0]))
     ps, xs, ts = _case(seed=9)
     ns, hs, ws = xs.shape[:3]
     _, g_want, _ = uo.loss_and_grads(ps, xs, ts)
