@@ -1431,8 +1431,9 @@ int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w,
          int n, int h, int wd) {
   ConvArgs a{in, w, bias, out, out_f32, mask, n, h, wd, cin, cout, ocs, oco, relu};
   if (u->use_tc && u->tc_tma && cout % 32 == 0 && cin % 16 == 0) {
-    // tcgen05, operands by tiled bulk-tensor loads through a 3-stage ring, two rows per CTA
-    const int kn = cout % 128 == 0 ? 128 : (cout % 64 == 0 ? 64 : 32);
+    // tcgen05, operands by tiled bulk-tensor loads through a ring; output tiles of 128, 64, 96
+    // (one tile for a 96-channel output, so its input is read once) or 32 channels
+    const int kn = cout % 128 == 0 ? 128 : cout % 64 == 0 ? 64 : cout % 96 == 0 ? 96 : 32;
     const bf16 *wblk = w == L.wf ? L.wfb : (w == L.wb ? L.wbb : nullptr);
     CUtensorMap ta, tb;
     if (!wblk || !conv_tensor_maps(a, wblk, kn, &ta, &tb))
@@ -1440,7 +1441,9 @@ int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w,
     // rows per CTA: 4 with option "tcgen05_rows" 4, else 2; ring stages: option "tcgen05_stages"
     const int kr = u->tc_rows == 4 ? 4 : 2, ks = u->tc_stages;
     dim3 grid((wd + kTcM - 1) / kTcM, (h + kr - 1) / kr, n * (cout / kn));
-    const int v = (kn == 128 ? 0 : kn == 64 ? 4 : 8) + (kr == 4 ? 2 : 0) + (ks == 2 ? 1 : 0);
+    const int v = kn == 96 ? (ks == 2 ? 12 : 13)  // 96 channels: two rows per CTA (TMEM)
+                           : (kn == 128 ? 0 : kn == 64 ? 4 : 8) + (kr == 4 ? 2 : 0) + (ks == 2 ? 1 : 0);
+    if (kn == 96) grid.y = (h + 1) / 2;
     switch (v) {
       case 0: launch_tma<128, 2, 3>(grid, a, ta, tb, u); break;
       case 1: launch_tma<128, 2, 2>(grid, a, ta, tb, u); break;
@@ -1453,7 +1456,9 @@ int conv(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *in, const bf16 *w,
       case 8: launch_tma<32, 2, 3>(grid, a, ta, tb, u); break;
       case 9: launch_tma<32, 2, 2>(grid, a, ta, tb, u); break;
       case 10: launch_tma<32, 4, 3>(grid, a, ta, tb, u); break;
-      default: launch_tma<32, 4, 2>(grid, a, ta, tb, u); break;
+      case 11: launch_tma<32, 4, 2>(grid, a, ta, tb, u); break;
+      case 12: launch_tma<96, 2, 2>(grid, a, ta, tb, u); break;
+      default: launch_tma<96, 2, 3>(grid, a, ta, tb, u); break;
     }
     UCK(cudaGetLastError());
     return DS2D_OK;
@@ -1517,7 +1522,8 @@ int wgrad(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *dz, int zcs, cons
       zcs % 8 == 0) {
     // tcgen05, MN-major operands by tiled bulk-tensor loads: CTAs of 128 output channels x kN
     // input channels x one kernel row over a range of 64-pixel chunks; bias by k_bias_grad
-    const int kn = L.cin_pad % 128 == 0 ? 128 : L.cin_pad % 64 == 0 ? 64 : L.cin_pad % 32 == 0 ? 32 : 16;
+    const int kn = L.cin_pad % 128 == 0 ? 128 : L.cin_pad % 64 == 0 ? 64
+                 : L.cin_pad % 96 == 0 ? 96 : L.cin_pad % 32 == 0 ? 32 : 16;
     CUtensorMap tz, tx;
     if (!wgrad_tensor_maps(a, &tz, &tx))
       return unet_fail(u, DS2D_E_CUDA, "wgrad: cuTensorMapEncodeTiled failed");
@@ -1532,6 +1538,8 @@ int wgrad(ds2d_unet *u, const ds2d_unet::Layer &L, const bf16 *dz, int zcs, cons
       k_conv3x3_wgrad_tma<128><<<tgrid, 128, wt_smem_bytes<128>(), u->stream>>>(a, tz, tx, u->d_err);
     else if (kn == 64)
       k_conv3x3_wgrad_tma<64><<<tgrid, 128, wt_smem_bytes<64>(), u->stream>>>(a, tz, tx, u->d_err);
+    else if (kn == 96)
+      k_conv3x3_wgrad_tma<96><<<tgrid, 128, wt_smem_bytes<96>(), u->stream>>>(a, tz, tx, u->d_err);
     else if (kn == 32)
       k_conv3x3_wgrad_tma<32><<<tgrid, 128, wt_smem_bytes<32>(), u->stream>>>(a, tz, tx, u->d_err);
     else
@@ -1847,7 +1855,8 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
     for (cudaError_t (*f)() : {tma_attr<128, 2, 3>, tma_attr<128, 2, 2>, tma_attr<128, 4, 3>,
                               tma_attr<128, 4, 2>, tma_attr<64, 2, 3>, tma_attr<64, 2, 2>,
                               tma_attr<64, 4, 3>, tma_attr<64, 4, 2>, tma_attr<32, 2, 3>,
-                              tma_attr<32, 2, 2>, tma_attr<32, 4, 3>, tma_attr<32, 4, 2>})
+                              tma_attr<32, 2, 2>, tma_attr<32, 4, 3>, tma_attr<32, 4, 2>,
+                              tma_attr<96, 2, 2>, tma_attr<96, 2, 3>})
       if (ea == cudaSuccess) ea = f();
     if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_tc<32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1864,6 +1873,9 @@ int ds2d_unet_create(int base, int max_n, int max_h, int max_w, int device, ds2d
     if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tma<64>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem_bytes<64>());
+    if (ea == cudaSuccess)
+      ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tma<96>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem_bytes<96>());
     if (ea == cudaSuccess)
       ea = cudaFuncSetAttribute(k_conv3x3_wgrad_tma<32>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem_bytes<32>());
