@@ -208,6 +208,16 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def measured_tensor_peak():
+    """Dense BF16 tensor-core peak in TFLOP/s: the measured burst figure (a cuBLAS GEMM timed
+    alone, the right denominator for a pass timed alone), else the earlier pool measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 def traffic_for(kernel, cells):
     """DRAM bytes (read + write) per launch of `kernel` over `cells` padded cells (all resident
     shots), from a committed ncu capture (profiles/traffic.json: bytes per shot of the captured
@@ -730,9 +740,15 @@ def run_unet(args):
         torch.cuda.synchronize()
         fwd_ms = e0.elapsed_time(e1) / args.steps
         train_ms = e1.elapsed_time(e2) / args.steps
-    return {"metric": "U-Net forward TFLOP/s (BF16 tensor cores)", "value": round(flops / fwd_ms / 1e9, 2),
+    tflops = flops / fwd_ms / 1e9
+    peak, src = measured_tensor_peak()
+    return {"metric": "U-Net forward TFLOP/s (BF16 tensor cores)", "value": round(tflops, 2),
             "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(fwd_ms, 3), "higher_is_better": True, "dtype": "bf16 (fp32 accumulate)",
+            "roofline": {"bound": "tensor", "achieved": round(tflops, 2), "peak": peak, "unit": "TFLOP/s",
+                         "frac": round(tflops / peak, 4), "peak_source": src, "traffic": None,
+                         "scope": "whole forward pass (convolutions, layout kernels, output layer), "
+                                  "CUDA events; the per-kernel split is in profiles/"},
             "data": "synthetic (random image)",
             "config": {"workload": "U-Net preconditioner", "image": f"{h}x{w}", "base_channels": 32,
                        "forward_gflop": round(flops / 1e9, 2), "train_step_ms": round(train_ms, 3),

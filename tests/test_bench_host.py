@@ -75,3 +75,12 @@ def test_autotuner_candidates_name_every_knob():
     assert {c["tb"] for c in space} == {0, 1, 2, 3, 4}
     assert {c["bwd_bulk"] for c in space} == {0, 1} and {c["bwd_1b"] for c in space} == {0, 1}
     assert {c["bwd_cta"] for c in space} >= {128, 192, 256}
+
+
+def test_tensor_peak_reads_the_measured_burst_figure():
+    """The U-Net line's roofline denominator: the measured BF16 burst figure when the peaks file
+    is there, the earlier pool measurement otherwise; a plausible B200 dense figure either way."""
+    import bench
+    peak, src = bench.measured_tensor_peak()
+    assert src in ("measured", "fallback")
+    assert 1000.0 < peak < 2500.0
